@@ -1,0 +1,266 @@
+// The extern "C" entry points of include/einfold_b200.h.
+#include <cstring>
+#include <mutex>
+
+#include "fold.h"
+#include "gemm.cuh"
+
+struct einfold_context : ef::Context {};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+void set_message(einfold_result* r, const std::string& m) {
+  std::snprintf(r->message, sizeof r->message, "%s", m.c_str());
+}
+
+// Runs `body` with the context's lock and device, mapping failures to a status.
+template <class F>
+int32_t guarded(einfold_context* ctx, einfold_result* result, F&& body) {
+  if (result) {
+    std::memset(result, 0, sizeof *result);
+  }
+  if (!ctx) {
+    if (result) set_message(result, "no context");
+    return EINFOLD_INVALID;
+  }
+  ef::Context* c = static_cast<ef::Context*>(ctx);
+  std::lock_guard<std::mutex> lock(c->lock);
+  int32_t status = EINFOLD_OK;
+  try {
+    ef::DeviceGuard dev(c->device);
+    c->kernels = 0;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    cudaEventRecord(t0, c->stream);
+    status = body(*c);
+    cudaEventRecord(t1, c->stream);
+    cudaEventSynchronize(t1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (result) {
+      result->device_ms = ms;
+      result->kernels_launched = c->kernels;
+    }
+  } catch (const ef::Declined& d) {
+    status = EINFOLD_DECLINED;
+    if (result) set_message(result, d.why);
+  } catch (const ef::Failure& f) {
+    status = f.status;
+    if (result) set_message(result, f.what());
+    g_last_error = f.what();
+  } catch (const std::exception& e) {
+    status = EINFOLD_COMPUTE;
+    if (result) set_message(result, e.what());
+    g_last_error = e.what();
+  }
+  if (status != EINFOLD_OK && result) ef::release_result(result);
+  if (result) result->status = status;
+  return status;
+}
+
+einfold_options defaults(const einfold_options* o) {
+  einfold_options d;
+  std::memset(&d, 0, sizeof d);
+  d.threads = 1;
+  return o ? *o : d;
+}
+
+int32_t run_fold(einfold_context* ctx, const einfold_fold_desc* fold, const einfold_relation* a,
+                 const einfold_relation* b, const einfold_relation* domain, const einfold_options* options,
+                 einfold_result* result, bool dense_only) {
+  return guarded(ctx, result, [&](ef::Context& c) -> int32_t {
+    einfold_options o = defaults(options);
+    ef::Budget budget;
+    budget.o = &o;
+    ef::FoldD f = ef::parse_fold(fold);
+    ef::Relation ra = ef::import_relation(a), rb = ef::import_relation(b);
+    ef::Relation rd;
+    if (domain) rd = ef::import_relation(domain);
+    std::vector<const std::vector<ef::Field>*> ops = {&ra.fields, &rb.fields};
+    std::vector<ef::Field> schema = ef::fold_schema(f, ops, domain ? &rd.fields : nullptr);
+    if (!dense_only && o.domain_rows == 1)
+      ef::fail(EINFOLD_INVALID, "only fold_dense checks that a domain's keys are unique");
+    ef::FoldOutput out;
+    try {
+      out = ef::dense_fold(c, f, ra, rb, domain ? &rd : nullptr, schema, o, budget);
+    } catch (const ef::Declined& d) {
+      if (dense_only) throw;
+      if (!f.conditions.empty()) ef::fail(EINFOLD_INVALID, "the discrimination algorithm computes no masks");
+      out = ef::discriminate_fold(c, f, ra, rb, domain ? &rd : nullptr, schema, o, budget);
+    }
+    result->algorithm = out.algorithm;
+    ef::export_result(std::move(out.batches), schema, result);
+    return EINFOLD_OK;
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* einfold_version(void) { return "einfold_b200 0.1.0 (sm_100a)"; }
+
+const char* einfold_last_error(void) { return g_last_error.c_str(); }
+
+einfold_context* einfold_context_create(int32_t device) {
+  try {
+    auto* c = new einfold_context();
+    c->device = device;
+    ef::DeviceGuard dev(device);
+    EF_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    EF_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
+    // Keep freed blocks in the stream-ordered pool across calls instead of
+    // returning them to the driver at every synchronization.
+    cudaMemPool_t pool;
+    EF_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = UINT64_MAX;
+    EF_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    return c;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return nullptr;
+  }
+}
+
+void einfold_context_destroy(einfold_context* ctx) {
+  if (!ctx) return;
+  {
+    ef::DeviceGuard dev(ctx->device);
+    if (ctx->stream) {
+      cudaStreamSynchronize(ctx->stream);
+      cudaStreamDestroy(ctx->stream);
+    }
+  }
+  delete ctx;
+}
+
+int32_t einfold_fold(einfold_context* ctx, const einfold_fold_desc* fold, const einfold_relation* a,
+                     const einfold_relation* b, const einfold_relation* domain, const einfold_options* options,
+                     einfold_result* result) {
+  return run_fold(ctx, fold, a, b, domain, options, result, false);
+}
+
+int32_t einfold_fold_dense(einfold_context* ctx, const einfold_fold_desc* fold, const einfold_relation* a,
+                           const einfold_relation* b, const einfold_relation* domain,
+                           const einfold_options* options, einfold_result* result) {
+  return run_fold(ctx, fold, a, b, domain, options, result, true);
+}
+
+int32_t einfold_fold_chain(einfold_context* ctx, const einfold_fold_desc* fold, const einfold_relation* operands,
+                           const einfold_options* options, einfold_result* result) {
+  return guarded(ctx, result, [&](ef::Context& c) -> int32_t {
+    einfold_options o = defaults(options);
+    ef::Budget budget;
+    budget.o = &o;
+    ef::FoldD f = ef::parse_fold(fold);
+    std::vector<ef::Relation> rels;
+    for (int i = 0; i < 3; i++) rels.push_back(ef::import_relation(&operands[i]));
+    std::vector<const std::vector<ef::Field>*> ops;
+    for (auto& r : rels) ops.push_back(&r.fields);
+    if (f.operands.size() != 3) throw ef::Declined{"not three operands"};
+    std::vector<ef::Field> schema = ef::fold_schema(f, ops, nullptr);
+    std::vector<const ef::Relation*> rp = {&rels[0], &rels[1], &rels[2]};
+    ef::FoldOutput out = ef::chain_fold(c, f, rp, schema, o, budget);
+    result->algorithm = out.algorithm;
+    ef::export_result(std::move(out.batches), schema, result);
+    return EINFOLD_OK;
+  });
+}
+
+int32_t einfold_pipeline(einfold_context* ctx, const einfold_pipeline_desc* pipeline,
+                         const einfold_relation* operands, const einfold_options* options,
+                         einfold_result* result) {
+  return guarded(ctx, result, [&](ef::Context& c) -> int32_t {
+    einfold_options o = defaults(options);
+    ef::Budget budget;
+    budget.o = &o;
+    ef::PipelineD p = ef::parse_pipeline(pipeline);
+    std::vector<ef::Relation> rels;
+    for (int i = 0; i < 3; i++) rels.push_back(ef::import_relation(&operands[i]));
+    std::vector<const std::vector<ef::Field>*> ins = {&rels[0].fields, &rels[1].fields, &rels[2].fields};
+    std::vector<ef::Field> schema = ef::pipeline_schema(p, ins);
+    ef::FoldOutput out = ef::fused_pipeline(c, p, rels[0], rels[1], rels[2], schema, o, budget);
+    result->algorithm = EINFOLD_ALG_FUSED;
+    result->tiles_visited = out.tiles_visited;
+    result->tiles = out.tiles;
+    ef::export_result(std::move(out.batches), schema, result);
+    return EINFOLD_OK;
+  });
+}
+
+int32_t einfold_schema(const einfold_fold_desc* fold, const struct ArrowSchema* const* operands, int32_t n_operands,
+                       const struct ArrowSchema* domain, struct ArrowSchema* out, char* message,
+                       int32_t message_len) {
+  try {
+    ef::FoldD f = ef::parse_fold(fold);
+    if (f.row_expr) ef::fail(EINFOLD_INVALID, "EinFold computes SUM of products only");
+    std::vector<std::vector<ef::Field>> fields;
+    for (int i = 0; i < n_operands; i++) fields.push_back(ef::import_schema(operands[i]));
+    std::vector<const std::vector<ef::Field>*> ops;
+    for (auto& fl : fields) ops.push_back(&fl);
+    std::vector<ef::Field> dom;
+    if (domain) dom = ef::import_schema(domain);
+    ef::export_schema(ef::fold_schema(f, ops, domain ? &dom : nullptr), out);
+    return EINFOLD_OK;
+  } catch (const ef::Failure& e) {
+    if (message && message_len > 0) std::snprintf(message, (size_t)message_len, "%s", e.what());
+    return e.status;
+  }
+}
+
+int32_t einfold_pipeline_schema(const einfold_pipeline_desc* pipeline, const struct ArrowSchema* const* inputs,
+                                struct ArrowSchema* out, char* message, int32_t message_len) {
+  try {
+    ef::PipelineD p = ef::parse_pipeline(pipeline);
+    std::vector<std::vector<ef::Field>> fields;
+    for (int i = 0; i < 3; i++) fields.push_back(ef::import_schema(inputs[i]));
+    std::vector<const std::vector<ef::Field>*> ins = {&fields[0], &fields[1], &fields[2]};
+    ef::export_schema(ef::pipeline_schema(p, ins), out);
+    return EINFOLD_OK;
+  } catch (const ef::Failure& e) {
+    if (message && message_len > 0) std::snprintf(message, (size_t)message_len, "%s", e.what());
+    return e.status;
+  }
+}
+
+void einfold_result_release(einfold_result* result) { ef::release_result(result); }
+
+int32_t einfold_split_gemm(einfold_context* ctx, const double* a, const double* b, double* c, int64_t batches,
+                           int64_t m, int64_t n, int64_t k, int32_t b_transposed, int32_t slices, void* stream) {
+  einfold_result r;
+  return guarded(ctx, &r, [&](ef::Context& cx) -> int32_t {
+    cudaStream_t s = stream ? (cudaStream_t)stream : cx.stream;
+    if (b_transposed) {
+      ef::split_gemm(cx, a, b, c, batches, m, n, k, slices ? slices : ef::kDefaultSlices, s);
+    } else {
+      ef::DeviceBuffer<double> bt((size_t)(batches * n * k), s);
+      ef::transpose(b, bt.get(), batches, k, n, s);
+      ef::split_gemm(cx, a, bt.get(), c, batches, m, n, k, slices ? slices : ef::kDefaultSlices, s);
+    }
+    return EINFOLD_OK;
+  });
+}
+
+int32_t einfold_fp64_gemm(einfold_context* ctx, const double* a, const double* b, double* c, int64_t batches,
+                          int64_t m, int64_t n, int64_t k, int32_t b_transposed, void* stream) {
+  einfold_result r;
+  return guarded(ctx, &r, [&](ef::Context& cx) -> int32_t {
+    cudaStream_t s = stream ? (cudaStream_t)stream : cx.stream;
+    if (b_transposed) {
+      ef::fp64_gemm(cx, a, nullptr, b, c, batches, m, n, k, 0, 0, false, s);
+    } else {
+      ef::DeviceBuffer<double> bt((size_t)(batches * n * k), s);
+      ef::transpose(b, bt.get(), batches, k, n, s);
+      ef::fp64_gemm(cx, a, nullptr, bt.get(), c, batches, m, n, k, 0, 0, false, s);
+    }
+    EF_CUDA(cudaStreamSynchronize(s));
+    return EINFOLD_OK;
+  });
+}
+
+}  // extern "C"

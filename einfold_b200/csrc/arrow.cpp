@@ -1,0 +1,324 @@
+// Arrow C Data Interface import and export for the einfold_b200 library.
+#include "arrow.h"
+
+#include <cstring>
+
+namespace ef {
+
+Kind kind_of(const char* f) {
+  if (!f) return Kind::Other;
+  if (f[0] && f[1] == 0) {
+    switch (f[0]) {
+      case 'c': return Kind::Int8;
+      case 'C': return Kind::UInt8;
+      case 's': return Kind::Int16;
+      case 'S': return Kind::UInt16;
+      case 'i': return Kind::Int32;
+      case 'I': return Kind::UInt32;
+      case 'l': return Kind::Int64;
+      case 'L': return Kind::UInt64;
+      case 'e': return Kind::Float16;
+      case 'f': return Kind::Float32;
+      case 'g': return Kind::Float64;
+      case 'b': return Kind::Bool;
+      case 'u': return Kind::Utf8;
+      case 'U': return Kind::LargeUtf8;
+      case 'z': return Kind::Binary;
+      case 'Z': return Kind::LargeBinary;
+      case 'n': return Kind::Null;
+    }
+  }
+  return Kind::Other;
+}
+
+int width_of(Kind k) {
+  switch (k) {
+    case Kind::Int8: case Kind::UInt8: return 1;
+    case Kind::Int16: case Kind::UInt16: case Kind::Float16: return 2;
+    case Kind::Int32: case Kind::UInt32: case Kind::Float32: return 4;
+    case Kind::Int64: case Kind::UInt64: case Kind::Float64: return 8;
+    default: return 0;
+  }
+}
+
+const char* format_of(Kind k) {
+  switch (k) {
+    case Kind::Int8: return "c";
+    case Kind::UInt8: return "C";
+    case Kind::Int16: return "s";
+    case Kind::UInt16: return "S";
+    case Kind::Int32: return "i";
+    case Kind::UInt32: return "I";
+    case Kind::Int64: return "l";
+    case Kind::UInt64: return "L";
+    case Kind::Float16: return "e";
+    case Kind::Float32: return "f";
+    case Kind::Float64: return "g";
+    case Kind::Bool: return "b";
+    case Kind::Utf8: return "u";
+    case Kind::LargeUtf8: return "U";
+    case Kind::Binary: return "z";
+    case Kind::LargeBinary: return "Z";
+    case Kind::Null: return "n";
+    default: return "";
+  }
+}
+
+int64_t Column::nulls() const {
+  if (!validity) return 0;
+  if (null_count >= 0) return null_count;
+  int64_t n = 0;
+  for (int64_t i = 0; i < length; i++) n += !valid(i);
+  return n;
+}
+
+const uint8_t* Column::bytes(int64_t i, int64_t* len) const {
+  int64_t r = offset + i;
+  if (kind == Kind::LargeUtf8 || kind == Kind::LargeBinary) {
+    const int64_t* o = (const int64_t*)values;
+    *len = o[r + 1] - o[r];
+    return data + o[r];
+  }
+  const int32_t* o = (const int32_t*)values;
+  *len = o[r + 1] - o[r];
+  return data + o[r];
+}
+
+static Field field_of(const ArrowSchema* s) {
+  Field f;
+  f.format = s->format ? s->format : "";
+  f.name = s->name ? s->name : "";
+  f.nullable = (s->flags & ARROW_FLAG_NULLABLE) != 0;
+  if (s->dictionary) {
+    f.dictionary = std::make_shared<Field>(field_of(s->dictionary));
+    f.kind = f.dictionary->kind;  // logically the values' type
+  } else {
+    f.kind = kind_of(s->format);
+  }
+  return f;
+}
+
+std::vector<Field> import_schema(const ArrowSchema* s) {
+  if (!s || !s->format || std::strcmp(s->format, "+s") != 0)
+    fail(EINFOLD_INVALID, "a relation's schema must be a struct schema");
+  std::vector<Field> out;
+  for (int64_t i = 0; i < s->n_children; i++) out.push_back(field_of(s->children[i]));
+  return out;
+}
+
+static Column column_of(const ArrowArray* a, const ArrowSchema* s, int64_t parent_offset) {
+  Column c;
+  c.length = a->length;
+  c.offset = a->offset + parent_offset;
+  c.null_count = a->null_count;
+  if (s->dictionary) {
+    c.index_kind = kind_of(s->format);
+    c.kind = kind_of(s->dictionary->format);
+    c.validity = a->n_buffers > 0 ? (const uint8_t*)a->buffers[0] : nullptr;
+    c.values = a->n_buffers > 1 ? (const uint8_t*)a->buffers[1] : nullptr;
+    if (!a->dictionary) fail(EINFOLD_INVALID, "a dictionary column without its dictionary");
+    c.dictionary = std::make_shared<Column>(column_of(a->dictionary, s->dictionary, 0));
+    return c;
+  }
+  c.kind = kind_of(s->format);
+  if (c.kind == Kind::Other) fail(EINFOLD_INVALID, "unsupported Arrow format '%s'", s->format);
+  if (c.kind == Kind::Null) {
+    c.null_count = c.length;
+    return c;
+  }
+  c.validity = a->n_buffers > 0 ? (const uint8_t*)a->buffers[0] : nullptr;
+  c.values = a->n_buffers > 1 ? (const uint8_t*)a->buffers[1] : nullptr;
+  if (is_var(c.kind)) c.data = a->n_buffers > 2 ? (const uint8_t*)a->buffers[2] : nullptr;
+  if (!c.validity) c.null_count = 0;
+  return c;
+}
+
+Relation import_relation(const einfold_relation* r) {
+  Relation rel;
+  if (!r) return rel;
+  rel.fields = import_schema(r->schema);
+  for (int64_t i = 0; i < r->n_batches; i++) {
+    const ArrowArray* b = r->batches[i];
+    if (!b || b->n_children != (int64_t)rel.fields.size())
+      fail(EINFOLD_INVALID, "batch %lld doesn't have the schema's %zu columns", (long long)i, rel.fields.size());
+    Batch batch;
+    batch.rows = b->length;
+    for (int64_t c = 0; c < b->n_children; c++) {
+      Column col = column_of(b->children[c], r->schema->children[c], b->offset);
+      if (b->children[c]->length < b->offset + b->length)
+        fail(EINFOLD_INVALID, "a column shorter than its batch");
+      col.length = b->length;
+      batch.columns.push_back(col);
+    }
+    rel.batches.push_back(std::move(batch));
+  }
+  return rel;
+}
+
+// ---- Export ----
+
+struct ArrayPrivate {
+  std::vector<OutColumn> columns;
+  std::vector<ArrowArray> children;
+  std::vector<ArrowArray*> child_ptrs;
+  std::vector<std::vector<const void*>> child_buffers;
+  std::vector<const void*> buffers;
+};
+
+static void release_child(ArrowArray* a) { a->release = nullptr; }
+
+static void release_array(ArrowArray* a) {
+  if (!a || !a->release) return;
+  delete (ArrayPrivate*)a->private_data;
+  a->release = nullptr;
+}
+
+static void fill_array(OutBatch&& batch, ArrowArray* out) {
+  auto* p = new ArrayPrivate();
+  p->columns = std::move(batch.columns);
+  size_t n = p->columns.size();
+  p->children.resize(n);
+  p->child_ptrs.resize(n);
+  p->child_buffers.resize(n);
+  for (size_t i = 0; i < n; i++) {
+    OutColumn& c = p->columns[i];
+    auto& bufs = p->child_buffers[i];
+    bufs.push_back(c.null_count ? c.validity.ptr : nullptr);
+    bufs.push_back(c.values.ptr);
+    if (is_var(c.kind)) bufs.push_back(c.data.ptr);
+    ArrowArray& a = p->children[i];
+    std::memset(&a, 0, sizeof a);
+    a.length = c.length;
+    a.null_count = c.null_count;
+    a.n_buffers = (int64_t)bufs.size();
+    a.buffers = bufs.data();
+    a.release = release_child;
+    p->child_ptrs[i] = &a;
+  }
+  p->buffers.push_back(nullptr);
+  std::memset(out, 0, sizeof *out);
+  out->length = batch.rows;
+  out->null_count = 0;
+  out->n_buffers = 1;
+  out->buffers = p->buffers.data();
+  out->n_children = (int64_t)n;
+  out->children = p->child_ptrs.data();
+  out->release = release_array;
+  out->private_data = p;
+}
+
+struct SchemaPrivate {
+  std::vector<std::string> formats, names;
+  std::vector<ArrowSchema> children;
+  std::vector<ArrowSchema*> child_ptrs;
+};
+
+static void release_child_schema(ArrowSchema* s) { s->release = nullptr; }
+
+static void release_schema(ArrowSchema* s) {
+  if (!s || !s->release) return;
+  delete (SchemaPrivate*)s->private_data;
+  s->release = nullptr;
+}
+
+void export_schema(const std::vector<Field>& fields, ArrowSchema* out) {
+  auto* p = new SchemaPrivate();
+  size_t n = fields.size();
+  p->formats.resize(n);
+  p->names.resize(n);
+  p->children.resize(n);
+  p->child_ptrs.resize(n);
+  for (size_t i = 0; i < n; i++) {
+    p->formats[i] = fields[i].format;
+    p->names[i] = fields[i].name;
+    ArrowSchema& s = p->children[i];
+    std::memset(&s, 0, sizeof s);
+    s.format = p->formats[i].c_str();
+    s.name = p->names[i].c_str();
+    s.flags = fields[i].nullable ? ARROW_FLAG_NULLABLE : 0;
+    s.release = release_child_schema;
+    p->child_ptrs[i] = &s;
+  }
+  std::memset(out, 0, sizeof *out);
+  out->format = "+s";
+  out->name = "";
+  out->n_children = (int64_t)n;
+  out->children = p->child_ptrs.data();
+  out->release = release_schema;
+  out->private_data = p;
+}
+
+void export_result(std::vector<OutBatch>&& batches, const std::vector<Field>& schema, einfold_result* out) {
+  out->n_batches = (int64_t)batches.size();
+  out->batches = (ArrowArray*)std::calloc(batches.size() ? batches.size() : 1, sizeof(ArrowArray));
+  for (size_t i = 0; i < batches.size(); i++) fill_array(std::move(batches[i]), &out->batches[i]);
+  out->schema = (ArrowSchema*)std::calloc(1, sizeof(ArrowSchema));
+  export_schema(schema, out->schema);
+}
+
+void release_result(einfold_result* r) {
+  if (!r) return;
+  if (r->batches) {
+    for (int64_t i = 0; i < r->n_batches; i++)
+      if (r->batches[i].release) r->batches[i].release(&r->batches[i]);
+    std::free(r->batches);
+    r->batches = nullptr;
+  }
+  if (r->schema) {
+    if (r->schema->release) r->schema->release(r->schema);
+    std::free(r->schema);
+    r->schema = nullptr;
+  }
+  r->n_batches = 0;
+}
+
+OutColumn copy_column(const Column& c, const Field& f) {
+  OutColumn o;
+  o.format = f.format;
+  o.nullable = f.nullable;
+  o.length = c.length;
+  if (c.dictionary) fail(EINFOLD_INVALID, "carrying a dictionary column is not supported");
+  o.kind = c.kind;
+  int64_t nulls = c.nulls();
+  o.null_count = nulls;
+  if (nulls) {
+    o.validity = HostBuffer((size_t)((c.length + 7) / 8));
+    std::memset(o.validity.ptr, 0, o.validity.bytes);
+    uint8_t* v = o.validity.as<uint8_t>();
+    for (int64_t i = 0; i < c.length; i++)
+      if (c.valid(i)) v[i >> 3] |= (uint8_t)(1u << (i & 7));
+  }
+  if (c.kind == Kind::Bool) {
+    o.values = HostBuffer((size_t)((c.length + 7) / 8));
+    std::memset(o.values.ptr, 0, o.values.bytes);
+    uint8_t* v = o.values.as<uint8_t>();
+    for (int64_t i = 0; i < c.length; i++) {
+      int64_t b = c.offset + i;
+      if ((c.values[b >> 3] >> (b & 7)) & 1) v[i >> 3] |= (uint8_t)(1u << (i & 7));
+    }
+  } else if (is_var(c.kind)) {
+    bool large = c.kind == Kind::LargeUtf8 || c.kind == Kind::LargeBinary;
+    int64_t total = 0;
+    for (int64_t i = 0; i < c.length; i++) { int64_t l; c.bytes(i, &l); total += l; }
+    o.values = HostBuffer((size_t)(c.length + 1) * (large ? 8 : 4));
+    o.data = HostBuffer((size_t)(total ? total : 1));
+    int64_t pos = 0;
+    for (int64_t i = 0; i < c.length; i++) {
+      int64_t l;
+      const uint8_t* src = c.bytes(i, &l);
+      if (large) o.values.as<int64_t>()[i] = pos; else o.values.as<int32_t>()[i] = (int32_t)pos;
+      std::memcpy(o.data.as<uint8_t>() + pos, src, (size_t)l);
+      pos += l;
+    }
+    if (large) o.values.as<int64_t>()[c.length] = pos; else o.values.as<int32_t>()[c.length] = (int32_t)pos;
+  } else if (c.kind == Kind::Null) {
+    o.null_count = c.length;
+  } else {
+    int w = width_of(c.kind);
+    o.values = HostBuffer((size_t)(c.length * w));
+    if (c.length) std::memcpy(o.values.ptr, c.values + c.offset * w, (size_t)(c.length * w));
+  }
+  return o;
+}
+
+}  // namespace ef

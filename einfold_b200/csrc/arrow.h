@@ -1,0 +1,121 @@
+// Arrow C Data Interface: reading the caller's batches, and exporting the
+// library's results as struct arrays the caller releases.
+#pragma once
+
+#include <cstdint>
+#include <cstdlib>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.h"
+
+namespace ef {
+
+// A column's logical type, from its Arrow format string.
+enum class Kind : uint8_t {
+  Int8, UInt8, Int16, UInt16, Int32, UInt32, Int64, UInt64,
+  Float16, Float32, Float64, Bool, Utf8, LargeUtf8, Binary, LargeBinary, Null, Other
+};
+
+Kind kind_of(const char* format);
+int width_of(Kind k);  // bytes per value of a fixed-width kind (Bool: 0)
+inline bool is_integer(Kind k) { return k <= Kind::UInt64; }
+inline bool is_signed(Kind k) { return k == Kind::Int8 || k == Kind::Int16 || k == Kind::Int32 || k == Kind::Int64; }
+inline bool is_float(Kind k) { return k == Kind::Float16 || k == Kind::Float32 || k == Kind::Float64; }
+inline bool is_var(Kind k) { return k == Kind::Utf8 || k == Kind::LargeUtf8 || k == Kind::Binary || k == Kind::LargeBinary; }
+const char* format_of(Kind k);
+
+struct Field {
+  std::string format;
+  std::string name;
+  bool nullable = true;
+  Kind kind = Kind::Other;
+  std::shared_ptr<Field> dictionary;  // value type of a dictionary column
+};
+
+// A view of one column of one batch; buffers stay the caller's.
+struct Column {
+  Kind kind = Kind::Other;
+  int64_t length = 0, offset = 0, null_count = 0;
+  const uint8_t* validity = nullptr;  // bitmap, or null when every value is valid
+  const uint8_t* values = nullptr;    // fixed-width values, or var-length offsets
+  const uint8_t* data = nullptr;      // var-length bytes
+  std::shared_ptr<Column> dictionary; // a dictionary column's values; `values` holds indices
+  Kind index_kind = Kind::Other;
+
+  bool valid(int64_t i) const {
+    if (!validity) return true;
+    int64_t b = offset + i;
+    return (validity[b >> 3] >> (b & 7)) & 1;
+  }
+  // The number of NULLs, counted when the producer left it unknown.
+  int64_t nulls() const;
+  // Row i as bytes (var-length kinds).
+  const uint8_t* bytes(int64_t i, int64_t* len) const;
+};
+
+struct Batch {
+  int64_t rows = 0;
+  std::vector<Column> columns;
+};
+
+struct Relation {
+  std::vector<Field> fields;
+  std::vector<Batch> batches;
+  int64_t rows() const {
+    int64_t n = 0;
+    for (auto& b : batches) n += b.rows;
+    return n;
+  }
+};
+
+std::vector<Field> import_schema(const ArrowSchema* s);
+Relation import_relation(const einfold_relation* r);
+
+// malloc'd host memory handed to an exported array.
+struct HostBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  HostBuffer() = default;
+  explicit HostBuffer(size_t n) : ptr(n ? std::malloc(n) : nullptr), bytes(n) {
+    if (n && !ptr) fail(EINFOLD_BUDGET, "out of host memory for %zu bytes", n);
+  }
+  HostBuffer(const HostBuffer&) = delete;
+  HostBuffer(HostBuffer&& o) noexcept : ptr(o.ptr), bytes(o.bytes) { o.ptr = nullptr; o.bytes = 0; }
+  HostBuffer& operator=(HostBuffer&& o) noexcept {
+    std::free(ptr);
+    ptr = o.ptr; bytes = o.bytes; o.ptr = nullptr; o.bytes = 0;
+    return *this;
+  }
+  ~HostBuffer() { std::free(ptr); }
+  template <class T> T* as() const { return (T*)ptr; }
+};
+
+// One column of a result: values, optional validity bitmap, and var-length data.
+struct OutColumn {
+  std::string format;
+  std::string name;
+  bool nullable = true;
+  int64_t length = 0;
+  int64_t null_count = 0;
+  HostBuffer validity;  // empty when there are no NULLs
+  HostBuffer values;
+  HostBuffer data;      // var-length kinds only
+  Kind kind = Kind::Other;
+};
+
+struct OutBatch {
+  int64_t rows = 0;
+  std::vector<OutColumn> columns;
+};
+
+// Exports batches (moved in) and a schema into the result.
+void export_result(std::vector<OutBatch>&& batches, const std::vector<Field>& schema, einfold_result* out);
+void export_schema(const std::vector<Field>& fields, ArrowSchema* out);
+void release_result(einfold_result* r);
+
+// A deep copy of rows [0, length) of a column, for carried domain columns.
+OutColumn copy_column(const Column& c, const Field& f);
+
+}  // namespace ef

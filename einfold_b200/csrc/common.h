@@ -1,0 +1,174 @@
+// Shared host-side machinery of the einfold_b200 library: errors, the
+// budget, device buffers, the per-device context and its stream.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/einfold_b200.h"
+
+namespace ef {
+
+// An outcome other than success, carried to the ABI boundary.
+struct Failure : std::runtime_error {
+  int32_t status;
+  Failure(int32_t s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+[[noreturn]] inline void fail(int32_t status, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  throw Failure(status, buf);
+}
+
+// The kernels' requirements don't hold: the caller runs the host's plan.
+struct Declined {
+  std::string why;
+};
+[[noreturn]] inline void decline(const std::string& why) { throw Declined{why}; }
+
+#define EF_CUDA(call)                                                                          \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess)                                                                     \
+      ::ef::fail(EINFOLD_DEVICE, "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+#define EF_LAUNCH_CHECK() EF_CUDA(cudaGetLastError())
+
+// The memory a call may take beyond its inputs (options.rs:56-65). Asked
+// before allocating; a refusal fails the call with EINFOLD_BUDGET.
+struct Budget {
+  const einfold_options* o = nullptr;
+  uint64_t taken = 0;
+  bool try_reserve(uint64_t bytes) {
+    if (!o || !o->budget_grow) return true;
+    if (o->budget_grow(o->budget_ctx, bytes)) {
+      taken += bytes;
+      return true;
+    }
+    return false;
+  }
+  void reserve(uint64_t bytes, const char* what) {
+    if (!try_reserve(bytes))
+      fail(EINFOLD_BUDGET, "EinFold's budget can't give %llu bytes for %s", (unsigned long long)bytes, what);
+  }
+  void release(uint64_t bytes) {
+    if (o && o->budget_shrink) o->budget_shrink(o->budget_ctx, bytes);
+    taken = bytes > taken ? 0 : taken - bytes;
+  }
+};
+
+// Saturating arithmetic on sizes, as the reference's usize::saturating_*.
+inline uint64_t sat_add(uint64_t a, uint64_t b) { return a + b < a ? UINT64_MAX : a + b; }
+inline uint64_t sat_mul(uint64_t a, uint64_t b) {
+  if (a == 0 || b == 0) return 0;
+  return a > UINT64_MAX / b ? UINT64_MAX : a * b;
+}
+// a * b, or false on overflow (checked_mul).
+inline bool checked_mul(uint64_t a, uint64_t b, uint64_t* out) {
+  if (a != 0 && b > UINT64_MAX / a) return false;
+  *out = a * b;
+  return true;
+}
+
+struct Context;
+
+// A device allocation from the context's stream-ordered pool, freed on the
+// same stream when it goes out of scope.
+template <class T>
+struct DeviceBuffer {
+  T* ptr = nullptr;
+  size_t count = 0;
+  cudaStream_t stream = nullptr;
+  DeviceBuffer() = default;
+  DeviceBuffer(size_t n, cudaStream_t s) { allocate(n, s); }
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  DeviceBuffer(DeviceBuffer&& o) noexcept { *this = std::move(o); }
+  DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
+    reset();
+    ptr = o.ptr; count = o.count; stream = o.stream;
+    o.ptr = nullptr; o.count = 0;
+    return *this;
+  }
+  void allocate(size_t n, cudaStream_t s) {
+    reset();
+    stream = s;
+    count = n;
+    if (n) EF_CUDA(cudaMallocAsync((void**)&ptr, n * sizeof(T), s));
+  }
+  void zero() {
+    if (count) EF_CUDA(cudaMemsetAsync(ptr, 0, count * sizeof(T), stream));
+  }
+  void reset() {
+    if (ptr) cudaFreeAsync(ptr, stream);
+    ptr = nullptr;
+    count = 0;
+  }
+  ~DeviceBuffer() { reset(); }
+  T* get() const { return ptr; }
+  size_t bytes() const { return count * sizeof(T); }
+};
+
+// Pinned host memory for staging copies, grown on demand and kept.
+struct PinnedArena {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  void* get(size_t n) {
+    if (n > bytes) {
+      if (ptr) cudaFreeHost(ptr);
+      ptr = nullptr;
+      size_t want = n < (64u << 20) ? (64u << 20) : n;
+      EF_CUDA(cudaHostAlloc(&ptr, want, cudaHostAllocDefault));
+      bytes = want;
+    }
+    return ptr;
+  }
+  ~PinnedArena() {
+    if (ptr) cudaFreeHost(ptr);
+  }
+};
+
+struct Context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::mutex lock;
+  int sm_count = 148;
+  uint64_t kernels = 0;  // kernels launched by the current call
+  PinnedArena pinned;
+  // Device-resident scratch kept across calls.
+  void* status_word = nullptr;  // int32 status set by bounded device waits
+};
+
+// Makes `ctx`'s device current for the scope.
+struct DeviceGuard {
+  int old = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&old);
+    if (old != dev) EF_CUDA(cudaSetDevice(dev));
+  }
+  ~DeviceGuard() {
+    if (old >= 0) cudaSetDevice(old);
+  }
+};
+
+inline unsigned blocks_for(uint64_t n, unsigned threads, unsigned cap = 148u * 32u) {
+  uint64_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  return (unsigned)(b > cap ? cap : b);
+}
+
+}  // namespace ef

@@ -1,0 +1,531 @@
+// The dense fold on the device (crates/einfold-kernels/src/dense.rs:176-578).
+//
+// Host side: the reference's control logic, dimension roles W/X/Z/Y, the
+// decline rules, the budget. Device side: every pass over rows or cells:
+// keys to int64 with their extents, positions, the scatter of both operands
+// into dense matrices with duplicate detection (integer atomics on flags
+// only), the product, each domain row's cell, and the output's columns.
+//
+// Layout in HBM: a[x][z] (z contiguous: the product's K-major A), held[x][z]
+// as int32 (0 absent, 1 NULL, 2 valued), b transposed as bt[w][y][z] (each
+// column of b contiguous: the product's K-major B), reached[x] and valued[x]
+// as bytes, and the product out[x][y].
+#include <cmath>
+
+#include "fold.h"
+#include "gemm.cuh"
+#include "stage.cuh"
+
+namespace ef {
+namespace {
+
+enum : unsigned { F_DUP_A = 1, F_DUP_B = 2, F_NONFINITE_A = 4, F_NONFINITE_B = 8, F_REPEATED = 16 };
+constexpr int64_t kFewCells = 4096;
+constexpr int64_t kZBlock = 4096;
+constexpr int64_t kNoGroup = -1;
+
+__global__ void scatter_a_kernel(Role xs, Role zs, int64_t rows, const double* __restrict__ vals,
+                                 const uint8_t* __restrict__ valid, int64_t nz, double* __restrict__ a,
+                                 int32_t* __restrict__ held, uint8_t* __restrict__ reached,
+                                 uint8_t* __restrict__ valued, unsigned* flags) {
+  unsigned f = 0;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t x = role_position(xs, r), z = role_position(zs, r);
+    const int64_t p = x * nz + z;
+    const bool v = valid ? valid[r] != 0 : true;
+    if (atomicExch(&held[p], v ? 2 : 1) != 0) f |= F_DUP_A;
+    reached[x] = 1;
+    if (v) {
+      const double val = vals[r];
+      a[p] = val;
+      valued[x] = 1;
+      if (!isfinite(val)) f |= F_NONFINITE_A;
+    }
+  }
+  if (f) atomicOr(flags, f);
+}
+
+__global__ void scatter_b_kernel(Role wzs, Role ys, int64_t rows, const double* __restrict__ vals,
+                                 const uint8_t* __restrict__ valid, int64_t nz, int64_t ny, double* __restrict__ bt,
+                                 int32_t* __restrict__ present, unsigned* flags) {
+  unsigned f = 0;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t wz = role_position(wzs, r), y = role_position(ys, r);
+    const int64_t w = wz / nz, z = wz % nz;
+    const int64_t p = (w * ny + y) * nz + z;
+    if (atomicExch(&present[p], 1) != 0) f |= F_DUP_B;
+    if (!valid || valid[r]) {
+      const double val = vals[r];
+      bt[p] = val;
+      if (!isfinite(val)) f |= F_NONFINITE_B;
+    }
+  }
+  if (f) atomicOr(flags, f);
+}
+
+// Where output keys come from: position x (in_x) or y, their stride and extent.
+struct KeyAt {
+  int in_x;
+  int64_t stride, extent;
+  __device__ __forceinline__ int64_t at(int64_t x, int64_t y) const { return ((in_x ? x : y) / stride) % extent; }
+};
+
+struct Conds {
+  int n = 0;
+  KeyAt left[kMaxDims], right[kMaxDims];
+  int cmp[kMaxDims];
+  int64_t offset[kMaxDims];
+  __device__ bool allowed(int64_t x, int64_t y) const {
+    for (int i = 0; i < n; i++) {
+      const __int128 l = left[i].at(x, y), r = (__int128)right[i].at(x, y) + offset[i];
+      bool ok;
+      switch (cmp[i]) {
+        case 0: ok = l < r; break;
+        case 1: ok = l <= r; break;
+        case 2: ok = l > r; break;
+        default: ok = l >= r; break;
+      }
+      if (!ok) return false;
+    }
+    return true;
+  }
+};
+
+struct OutKeys {
+  int n = 0;
+  KeyAt key[kMaxDims];
+  int width[kMaxDims];
+  void* out[kMaxDims];
+};
+
+__global__ void select_cells(int64_t nx, int64_t ny, const uint8_t* __restrict__ reached, Conds c,
+                             uint8_t* __restrict__ sel) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nx * ny; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t x = i / ny, y = i % ny;
+    sel[i] = reached[x] && (c.n == 0 || c.allowed(x, y));
+  }
+}
+
+__device__ __forceinline__ void store_key(void* base, int width, int64_t i, int64_t v) {
+  switch (width) {
+    case 1: ((uint8_t*)base)[i] = (uint8_t)v; break;
+    case 2: ((uint16_t*)base)[i] = (uint16_t)v; break;
+    case 4: ((uint32_t*)base)[i] = (uint32_t)v; break;
+    default: ((int64_t*)base)[i] = v; break;
+  }
+}
+
+__global__ void emit_cells(int64_t nx, int64_t ny, const uint8_t* __restrict__ sel, const int64_t* __restrict__ pos,
+                           OutKeys keys, const double* __restrict__ out, const uint8_t* __restrict__ valued,
+                           double* __restrict__ val_out, uint8_t* __restrict__ valid_out,
+                           unsigned long long* nulls) {
+  unsigned long long local = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nx * ny; i += (int64_t)gridDim.x * blockDim.x) {
+    if (!sel[i]) continue;
+    const int64_t x = i / ny, y = i % ny, o = pos[i];
+    for (int k = 0; k < keys.n; k++) store_key(keys.out[k], keys.width[k], o, keys.key[k].at(x, y));
+    val_out[o] = out[i];
+    const uint8_t v = valued[x];
+    valid_out[o] = v;
+    local += !v;
+  }
+  if (local) atomicAdd(nulls, local);
+}
+
+struct DomainKeys {
+  int n = 0;
+  const int64_t* key[kMaxDims];
+  const uint8_t* valid[kMaxDims];
+  int64_t extent[kMaxDims], stride[kMaxDims];
+};
+
+__global__ void locate_kernel(DomainKeys k, int64_t rows, int64_t* __restrict__ cell) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    int64_t c = 0;
+    for (int i = 0; i < k.n && c != kNoGroup; i++) {
+      const int64_t v = k.key[i][r];
+      const bool ok = (!k.valid[i] || k.valid[i][r]) && v >= 0 && v < k.extent[i];
+      c = ok ? c + v * k.stride[i] : kNoGroup;
+    }
+    cell[r] = c;
+  }
+}
+
+__global__ void unique_cells(int64_t rows, const int64_t* __restrict__ cell, int32_t* __restrict__ seen,
+                             unsigned* flags) {
+  unsigned f = 0;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = cell[r];
+    if (c != kNoGroup && atomicExch(&seen[c], 1) != 0) f |= F_REPEATED;
+  }
+  if (f) atomicOr(flags, f);
+}
+
+__global__ void domain_values(int64_t rows, const int64_t* __restrict__ cell, int64_t ny,
+                              const uint8_t* __restrict__ valued, Conds c, const double* __restrict__ out,
+                              int has_missing, double missing, double* __restrict__ val, uint8_t* __restrict__ valid) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t cl = cell[r];
+    bool has = cl != kNoGroup;
+    if (has) {
+      const int64_t x = cl / ny, y = cl % ny;
+      if (c.n && !c.allowed(x, y)) has = false;
+      else if (valued && !valued[x]) has = false;
+    }
+    if (has) {
+      val[r] = out[cl];
+      valid[r] = 1;
+    } else {
+      val[r] = has_missing ? missing : 0.0;
+      valid[r] = (uint8_t)(has_missing ? 1 : 0);
+    }
+  }
+}
+
+// Keys of every batch of `r` for `op`, staged as int64, with extents.
+struct StagedKeys {
+  std::vector<DeviceBuffer<int64_t>> keys;  // per key of the operand, in op.keys order
+  std::vector<int64_t> extent;              // per key
+};
+
+// Stages an operand's key columns; declines where dense::keys returns None.
+StagedKeys stage_keys(Context& ctx, const OperandD& op, const Relation& r) {
+  StagedKeys s;
+  for (auto& k : op.keys) {
+    const Field& f = r.fields[k.col];
+    if (f.dictionary || !is_integer(f.kind)) decline("a key column that isn't integers");
+    for (auto& b : r.batches)
+      if (b.columns[k.col].nulls() > 0) decline("a NULL key");
+    DeviceColumn c = stage_column(ctx, r, k.col, false);
+    KeyStats st;
+    s.keys.push_back(keys_as_i64(ctx, c, &st));
+    if (st.negative || st.too_large) decline("a negative key, or one too large for int64");
+    if (st.max == INT64_MAX) decline("a key whose extent doesn't fit");
+    s.extent.push_back(st.max + 1);
+  }
+  return s;
+}
+
+Role role_of(const std::vector<int>& dims, const OperandD& op, const StagedKeys& s, const std::vector<int64_t>& extent) {
+  Role r;
+  if (dims.size() > (size_t)kMaxDims) decline("more than 8 dimensions in one role");
+  for (int d : dims) {
+    int slot = -1;
+    for (size_t i = 0; i < op.keys.size(); i++)
+      if (op.keys[i].dim == d) slot = (int)i;
+    r.keys[r.n] = s.keys[slot].get();
+    r.extent[r.n] = extent[d];
+    r.n++;
+  }
+  return r;
+}
+
+bool worth(uint64_t cells, uint64_t rows) {
+  return cells <= sat_add(sat_mul(rows, 4), (uint64_t)kFewCells) && cells < UINT32_MAX;
+}
+
+}  // namespace
+
+FoldOutput dense_fold(Context& ctx, const FoldD& f, const Relation& a, const Relation& b, const Relation* domain,
+                      const std::vector<Field>& schema, const einfold_options& o, Budget& budget) {
+  cudaStream_t s = ctx.stream;
+  if (f.operands.size() != 2) decline("not two operands");
+  const OperandD& op_a = f.operands[0];
+  const OperandD& op_b = f.operands[1];
+  if (f.row_expr) decline("a row expression");
+  // Roles (dense.rs:196-219): W, X, Y in output order, Z in dimension order.
+  std::vector<int> ws, xs, ys, zs;
+  for (auto& out : f.outputs) {
+    bool ha = op_a.holds(out.dim), hb = op_b.holds(out.dim);
+    if (ha && hb) ws.push_back(out.dim);
+    else if (ha) xs.push_back(out.dim);
+    else if (hb) ys.push_back(out.dim);
+    else decline("an output neither operand holds");
+  }
+  xs.insert(xs.begin(), ws.begin(), ws.end());
+  for (int d = 0; d < f.n_dims(); d++)
+    if (f.is_aggregated(d)) {
+      if (!op_a.holds(d) || !op_b.holds(d)) decline("a summed dimension one operand lacks");
+      zs.push_back(d);
+    }
+  auto is_output = [&](int d) {
+    for (int x : xs) if (x == d) return true;
+    for (int y : ys) if (y == d) return true;
+    return false;
+  };
+  for (auto& c : f.conditions)
+    if (!is_output(c.left) || !is_output(c.right)) decline("a condition on a summed dimension");
+  auto integers = [&](const OperandD& op, const Relation& r) {
+    if (r.batches.empty()) return true;
+    for (auto& k : op.keys) {
+      const Field& fl = r.fields[k.col];
+      if (fl.dictionary || !is_integer(fl.kind)) return false;
+    }
+    return true;
+  };
+  if (!integers(op_a, a) || !integers(op_b, b)) decline("keys that aren't integers");
+  const uint64_t ra = (uint64_t)a.rows(), rb = (uint64_t)b.rows();
+  budget.reserve(sat_mul(sat_add(sat_mul(ra, op_a.keys.size()), sat_mul(rb, op_b.keys.size())), 8),
+                 "the dense algorithm's keys");
+  StagedKeys ka = stage_keys(ctx, op_a, a), kb = stage_keys(ctx, op_b, b);
+  std::vector<int64_t> extent(f.n_dims(), 0);
+  for (size_t i = 0; i < op_a.keys.size(); i++) extent[op_a.keys[i].dim] = std::max(extent[op_a.keys[i].dim], ka.extent[i]);
+  for (size_t i = 0; i < op_b.keys.size(); i++) extent[op_b.keys[i].dim] = std::max(extent[op_b.keys[i].dim], kb.extent[i]);
+  auto size = [&](const std::vector<int>& dims, uint64_t* out) {
+    uint64_t n = 1;
+    for (int d : dims)
+      if (!checked_mul(n, (uint64_t)extent[d], &n)) return false;
+    *out = n;
+    return true;
+  };
+  std::vector<int> wzs = ws;
+  wzs.insert(wzs.end(), zs.begin(), zs.end());
+  uint64_t nw, nx, nz, ny;
+  if (!size(ws, &nw) || !size(xs, &nx) || !size(zs, &nz) || !size(ys, &ny)) decline("sizes that overflow");
+  const uint64_t per_batch = nw ? nx / nw : 0;
+  const uint64_t out_rows = domain ? (uint64_t)domain->rows() : sat_mul(nx, ny);
+  if (!worth(sat_mul(nx, nz), ra) || !worth(sat_mul(sat_mul(nw, nz), ny), rb) || !worth(sat_mul(nx, ny), out_rows))
+    decline("too sparse for dense matrices");
+  const uint64_t na = nx * nz, nb = nw * nz * ny;
+  const uint64_t out_columns = f.outputs.size() + 1 + (domain ? 1 : 0);
+  const uint64_t working = sat_add(sat_add(sat_add(sat_mul(na, 12), sat_mul(nx, 2)), sat_add(sat_mul(nb, 12), sat_mul(ra + rb, 8))),
+                                   sat_add(sat_mul(sat_mul(nx, ny), 16), sat_mul(sat_mul(out_rows, out_columns), 8)));
+  budget.reserve(working, "the dense algorithm's matrices");
+  const bool zero_default = f.domain && f.domain->has_missing && std::signbit(f.domain->missing) == false &&
+                            f.domain->missing == 0.0;
+
+  // The operands' factors.
+  if (op_a.factor < 0 || op_b.factor < 0) decline("an operand without a factor");
+  if (a.fields[op_a.factor].kind != Kind::Float64 || a.fields[op_a.factor].dictionary) decline("factors that aren't Float64");
+  if (b.fields[op_b.factor].kind != Kind::Float64 || b.fields[op_b.factor].dictionary) decline("factors that aren't Float64");
+  DeviceColumn fa = stage_column(ctx, a, op_a.factor), fb = stage_column(ctx, b, op_b.factor);
+
+  DeviceBuffer<double> am(na, s), btm(nb, s), out(nx * ny, s);
+  DeviceBuffer<int32_t> held(na, s), present(nb, s);
+  DeviceBuffer<uint8_t> reached(nx, s), valued(nx, s);
+  DeviceBuffer<unsigned> flags(1, s);
+  am.zero(); btm.zero(); held.zero(); present.zero(); reached.zero(); valued.zero(); flags.zero();
+  Role rxs = role_of(xs, op_a, ka, extent), rzs = role_of(zs, op_a, ka, extent);
+  Role rwzs = role_of(wzs, op_b, kb, extent), rys = role_of(ys, op_b, kb, extent);
+  if (ra) {
+    scatter_a_kernel<<<blocks_for(ra, 256), 256, 0, s>>>(rxs, rzs, (int64_t)ra, (const double*)fa.data.get(),
+                                                         fa.valid.get(), (int64_t)nz, am.get(), held.get(),
+                                                         reached.get(), valued.get(), flags.get());
+    ctx.kernels++;
+  }
+  if (rb) {
+    scatter_b_kernel<<<blocks_for(rb, 256), 256, 0, s>>>(rwzs, rys, (int64_t)rb, (const double*)fb.data.get(),
+                                                         fb.valid.get(), (int64_t)nz, (int64_t)ny, btm.get(),
+                                                         present.get(), flags.get());
+    ctx.kernels++;
+  }
+  EF_LAUNCH_CHECK();
+  unsigned fl = 0;
+  EF_CUDA(cudaMemcpyAsync(&fl, flags.get(), 4, cudaMemcpyDeviceToHost, s));
+  EF_CUDA(cudaStreamSynchronize(s));
+  if (fl & F_DUP_A) decline("duplicate key tuples in a");
+  if (fl & F_DUP_B) decline("duplicate key tuples in b");
+  const bool finite = !(fl & F_NONFINITE_A);
+  // Without duplicates, every row of b holds its own cell.
+  const bool holes = fb.nulls > 0 || rb < nb;
+  if (holes && (!zero_default || !finite)) decline("holes in b without a 0.0 default over finite factors");
+  present.reset();
+
+  // The fold's conditions, on output keys.
+  std::vector<int> order = xs;
+  order.insert(order.end(), ys.begin(), ys.end());
+  auto key_at = [&](int d) {
+    KeyAt k{};
+    bool in_x = false;
+    for (int x : xs) in_x |= x == d;
+    const std::vector<int>& role = in_x ? xs : ys;
+    size_t slot = 0;
+    while (role[slot] != d) slot++;
+    int64_t stride = 1;
+    for (size_t i = slot + 1; i < role.size(); i++) stride *= extent[role[i]];
+    k.in_x = in_x;
+    k.stride = stride;
+    k.extent = extent[d] ? extent[d] : 1;
+    return k;
+  };
+  Conds conds;
+  if (f.conditions.size() > (size_t)kMaxDims) decline("more than 8 conditions");
+  for (auto& c : f.conditions) {
+    conds.left[conds.n] = key_at(c.left);
+    conds.right[conds.n] = key_at(c.right);
+    conds.cmp[conds.n] = c.cmp;
+    conds.offset[conds.n] = c.offset;
+    conds.n++;
+  }
+
+  // Each domain row's cell, before the product (dense.rs:400-434).
+  DeviceBuffer<int64_t> cells;
+  int64_t nd = 0;
+  if (f.domain && domain) {
+    nd = domain->rows();
+    cells.allocate((size_t)(nd ? nd : 1), s);
+    DomainKeys dk;
+    std::vector<DeviceColumn> dcols;
+    std::vector<DeviceBuffer<int64_t>> dkeys;
+    if (f.outputs.size() > (size_t)kMaxDims) decline("more than 8 outputs");
+    for (auto& out_d : f.outputs) {
+      dcols.push_back(stage_column(ctx, *domain, out_d.domain_col, true));
+      DeviceColumn& c = dcols.back();
+      if (!is_integer(c.kind)) fail(EINFOLD_INVALID, "a domain key column that isn't integers");
+      KeyStats st;
+      dkeys.push_back(keys_as_i64(ctx, c, &st));
+      int64_t stride = 1;
+      size_t slot = 0;
+      while (order[slot] != out_d.dim) slot++;
+      for (size_t i = slot + 1; i < order.size(); i++) stride *= extent[order[i]];
+      dk.key[dk.n] = dkeys.back().get();
+      dk.valid[dk.n] = c.valid.get();
+      dk.extent[dk.n] = extent[out_d.dim];
+      dk.stride[dk.n] = stride;
+      dk.n++;
+    }
+    if (nd) {
+      locate_kernel<<<blocks_for(nd, 256), 256, 0, s>>>(dk, nd, cells.get());
+      ctx.kernels++;
+    }
+    if (o.domain_rows == 1 && nd) {
+      DeviceBuffer<int32_t> seen(nx * ny, s);
+      seen.zero();
+      unique_cells<<<blocks_for(nd, 256), 256, 0, s>>>(nd, cells.get(), seen.get(), flags.get());
+      ctx.kernels++;
+      EF_LAUNCH_CHECK();
+      EF_CUDA(cudaMemcpyAsync(&fl, flags.get(), 4, cudaMemcpyDeviceToHost, s));
+      EF_CUDA(cudaStreamSynchronize(s));
+      if (fl & F_REPEATED) decline("two domain rows with one cell");
+    }
+  }
+
+  // The product (dense.rs:442-467 and accumulate, :706-770).
+  const bool split = o.precision == 0 && finite && !(fl & F_NONFINITE_B);
+  if (nx && ny) {
+    if (split) {
+      split_gemm(ctx, am.get(), btm.get(), out.get(), (int64_t)nw, (int64_t)per_batch, (int64_t)ny, (int64_t)nz,
+                 o.slices ? o.slices : kDefaultSlices, s);
+    } else {
+      fp64_gemm(ctx, am.get(), held.get(), btm.get(), out.get(), (int64_t)nw, (int64_t)per_batch, (int64_t)ny,
+                (int64_t)nz, 0, (int64_t)(nx * ny >= (uint64_t)kFewCells ? 0 : kZBlock), false, s);
+    }
+  }
+  am.reset();
+  btm.reset();
+  held.reset();
+
+  FoldOutput result;
+  result.algorithm = EINFOLD_ALG_DENSE;
+  if (f.domain && domain) {
+    const DomainD& spec = *f.domain;
+    DeviceBuffer<double> val((size_t)(nd ? nd : 1), s);
+    DeviceBuffer<uint8_t> valid((size_t)(nd ? nd : 1), s);
+    if (nd) {
+      domain_values<<<blocks_for(nd, 256), 256, 0, s>>>(nd, cells.get(), (int64_t)(ny ? ny : 1),
+                                                        zero_default ? nullptr : valued.get(), conds, out.get(),
+                                                        spec.has_missing, spec.missing, val.get(), valid.get());
+      ctx.kernels++;
+      EF_LAUNCH_CHECK();
+    }
+    HostBuffer hv = to_host(ctx, val.get(), (size_t)nd * 8);
+    HostBuffer hvalid = to_host(ctx, valid.get(), (size_t)nd);
+    int64_t off = 0;
+    for (auto& batch : domain->batches) {
+      OutBatch ob;
+      ob.rows = batch.rows;
+      for (size_t i = 0; i < spec.carry.size(); i++) {
+        OutColumn c = copy_column(batch.columns[spec.carry[i]], domain->fields[spec.carry[i]]);
+        c.format = schema[i].format;
+        c.name = schema[i].name;
+        ob.columns.push_back(std::move(c));
+      }
+      OutColumn v;
+      v.format = "g";
+      v.kind = Kind::Float64;
+      v.name = schema.back().name;
+      v.length = batch.rows;
+      v.values = HostBuffer((size_t)batch.rows * 8);
+      if (batch.rows) std::memcpy(v.values.ptr, hv.as<double>() + off, (size_t)batch.rows * 8);
+      int64_t nulls = 0;
+      for (int64_t i = 0; i < batch.rows; i++) nulls += !hvalid.as<uint8_t>()[off + i];
+      v.null_count = nulls;
+      if (nulls) {
+        v.validity = HostBuffer((size_t)(batch.rows + 7) / 8);
+        std::memset(v.validity.ptr, 0, v.validity.bytes);
+        for (int64_t i = 0; i < batch.rows; i++)
+          if (hvalid.as<uint8_t>()[off + i]) v.validity.as<uint8_t>()[i >> 3] |= (uint8_t)(1u << (i & 7));
+      }
+      ob.columns.push_back(std::move(v));
+      result.batches.push_back(std::move(ob));
+      off += batch.rows;
+    }
+    return result;
+  }
+  if (f.domain || domain) fail(EINFOLD_INVALID, "a fold with a domain was given no domain relation");
+
+  // Output rows (dense.rs:516-575): (x, y) for each reached x, in order, every
+  // y, minus the groups the conditions disallow.
+  const int64_t cells_n = (int64_t)(nx * ny);
+  DeviceBuffer<uint8_t> sel((size_t)(cells_n ? cells_n : 1), s);
+  DeviceBuffer<int64_t> pos((size_t)(cells_n ? cells_n : 1), s);
+  if (cells_n) {
+    select_cells<<<blocks_for(cells_n, 256), 256, 0, s>>>((int64_t)nx, (int64_t)ny, reached.get(), conds, sel.get());
+    ctx.kernels++;
+    EF_LAUNCH_CHECK();
+  }
+  const int64_t n_out = exclusive_scan_flags(ctx, sel.get(), cells_n, pos.get());
+  OutKeys ok;
+  std::vector<DeviceBuffer<uint8_t>> key_dev;
+  if (f.outputs.size() > (size_t)kMaxDims) decline("more than 8 outputs");
+  for (size_t i = 0; i < f.outputs.size(); i++) {
+    int width = width_of(schema[i].kind);
+    key_dev.emplace_back((size_t)(n_out ? n_out * width : 1), s);
+    ok.key[ok.n] = key_at(f.outputs[i].dim);
+    ok.width[ok.n] = width;
+    ok.out[ok.n] = key_dev.back().get();
+    ok.n++;
+  }
+  DeviceBuffer<double> vals((size_t)(n_out ? n_out : 1), s);
+  DeviceBuffer<uint8_t> vvalid((size_t)(n_out ? n_out : 1), s);
+  DeviceBuffer<unsigned long long> nulls(1, s);
+  nulls.zero();
+  if (cells_n) {
+    emit_cells<<<blocks_for(cells_n, 256), 256, 0, s>>>((int64_t)nx, (int64_t)ny, sel.get(), pos.get(), ok, out.get(),
+                                                        valued.get(), vals.get(), vvalid.get(), nulls.get());
+    ctx.kernels++;
+    EF_LAUNCH_CHECK();
+  }
+  unsigned long long n_nulls = 0;
+  EF_CUDA(cudaMemcpyAsync(&n_nulls, nulls.get(), 8, cudaMemcpyDeviceToHost, s));
+  EF_CUDA(cudaStreamSynchronize(s));
+  OutBatch ob;
+  ob.rows = n_out;
+  for (size_t i = 0; i < f.outputs.size(); i++) {
+    OutColumn c;
+    c.format = schema[i].format;
+    c.name = schema[i].name;
+    c.kind = schema[i].kind;
+    c.nullable = schema[i].nullable;
+    c.length = n_out;
+    c.values = to_host(ctx, key_dev[i].get(), (size_t)(n_out * width_of(schema[i].kind)));
+    ob.columns.push_back(std::move(c));
+  }
+  OutColumn v;
+  v.format = "g";
+  v.kind = Kind::Float64;
+  v.name = schema.back().name;
+  v.length = n_out;
+  v.values = to_host(ctx, vals.get(), (size_t)n_out * 8);
+  v.null_count = (int64_t)n_nulls;
+  if (n_nulls) {
+    DeviceBuffer<uint8_t> bits((size_t)((n_out + 7) / 8), s);
+    pack_bits(ctx, vvalid.get(), n_out, bits.get());
+    v.validity = to_host(ctx, bits.get(), (size_t)((n_out + 7) / 8));
+  }
+  ob.columns.push_back(std::move(v));
+  result.batches.push_back(std::move(ob));
+  return result;
+}
+
+}  // namespace ef

@@ -1,0 +1,583 @@
+// Dense products on the B200: the split product on the tensor cores
+// (tcgen05 kind::i8, operands staged by TMA, level accumulators in TMEM),
+// and the FP64 product on the CUDA cores in the reference's order.
+//
+// The split product. Each row of A (and of BT, a column of B) is scaled by a
+// power of two 2^e with |x / 2^e| < 1/4, rounded to 8S fractional bits, and
+// written as S balanced base-256 digits in [-128, 127], most significant
+// first: x ≈ 2^e Σ_s d_s 2^{-8s}. A product a·b is then 2^{e+f} Σ_{s,t}
+// d_s g_t 2^{-8(s+t)}; the terms of level l = s + t ≤ S + 1 are kept (the
+// others are below the rounding of the digits), and each level's sum over k
+// is an exact int32 accumulation on the tensor cores while S·k·2^14 < 2^31.
+// One MMA per digit s of A covers every digit t ≤ S + 1 - s of B at once: the
+// B tile holds B's digits stacked along N, and the MMA's accumulator starts
+// at TMEM column (s - 1)·64, so that the product of digits s and t lands in
+// column (s + t - 2)·64 + j: level l's accumulator. The epilogue reads the S
+// levels, combines them in FP64 from the smallest up, and scales by 2^{e+f}.
+// Integer sums are exact, so the result doesn't depend on the tiling, the
+// order of the MMAs, or the number of SMs.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "gemm.cuh"
+
+namespace ef {
+namespace {
+
+constexpr int BM = 128;  // rows of A per tile (TMEM lanes)
+constexpr int BN = 64;   // columns of C per tile (per level)
+constexpr int BK = 64;   // bytes (int8 values) of k per pipeline stage
+constexpr int kThreads = 192;
+constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s: a bounded wait's limit
+constexpr int kGroup = 8;                    // tile rows per raster group
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t now_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Waits for the phase of `parity` to complete, for at most kWaitNs. Waiters
+// that expect a long wait (the epilogue) back off between polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, bool patient = false) {
+  if (mbar_try_wait(bar, parity)) return true;
+  uint64_t start = now_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (now_ns() - start > kWaitNs) return false;
+    if (patient) __nanosleep(256);
+  }
+  return true;
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+      ::"r"(smem_u32(dst)), "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t cols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)), "r"(cols)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t cols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(cols) : "memory");
+}
+
+// D (+)= A · B^T for int8 A (128 x 32) and B (N x 32), both K-major in
+// shared memory, D int32 in TMEM.
+__device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n"
+      ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t* v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Shared-memory matrix descriptor: K-major, 64-byte swizzle, 8-row groups
+// 512 bytes apart (the layout TMA writes with CU_TENSOR_MAP_SWIZZLE_64B).
+__device__ __forceinline__ uint64_t desc_sw64(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr & 0x3FFFFu) >> 4);  // start address
+  d |= (uint64_t)1 << 16;                   // leading byte offset (unused here)
+  d |= (uint64_t)(512 >> 4) << 32;          // stride byte offset: 8 rows x 64 B
+  d |= (uint64_t)1 << 46;                   // descriptor version for sm_100
+  d |= (uint64_t)4 << 61;                   // 64-byte swizzle
+  return d;
+}
+
+// Instruction descriptor: int8 x int8 -> int32, K-major A and B, M = 128.
+__host__ __device__ constexpr uint32_t idesc_i8(int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+
+template <int S>
+struct SplitShape {
+  static constexpr int kASlab = BM * BK;
+  static constexpr int kBSlab = BN * BK;
+  static constexpr int kStage = S * (kASlab + kBSlab);
+  static constexpr int kStagesFit = (220 * 1024) / kStage;
+  static constexpr int kStages = kStagesFit > 4 ? 4 : kStagesFit;
+  static constexpr int kSmem = kStages * kStage + 1024 + 256;
+  // TMEM columns: S levels of BN int32 columns, rounded up to a power of two.
+  static constexpr uint32_t kTmemCols = S * BN <= 128 ? 128 : (S * BN <= 256 ? 256 : 512);
+  static_assert(kStages >= 2, "two pipeline stages must fit");
+};
+
+template <int S>
+__global__ void __launch_bounds__(kThreads, 1)
+    split_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constant__ CUtensorMap tma_b,
+                      const int32_t* __restrict__ ea, const int32_t* __restrict__ eb, double* __restrict__ c,
+                      int m, int n, int m_pad, int n_pad, int kb0, int k_blocks, int tiles_m, int tiles_n,
+                      int accumulate, int* status) {
+  using Sh = SplitShape<S>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t* sA = smem;
+  uint8_t* sB = smem + Sh::kStages * S * Sh::kASlab;
+  uint64_t* full = (uint64_t*)(sB + Sh::kStages * S * Sh::kBSlab);
+  uint64_t* empty = full + Sh::kStages;
+  uint64_t* done = empty + Sh::kStages;
+  uint32_t* tmem_slot = (uint32_t*)(done + 1);
+  int* failed = (int*)(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w = blockIdx.y;
+  // Grouped raster: kGroup tile rows share each tile column in turn, so the
+  // CTAs on the GPU at once read a compact block of A's and B's digits.
+  const int tile = blockIdx.x;
+  const int per_group = kGroup * tiles_n;
+  const int first_m = (tile / per_group) * kGroup;
+  const int group_rows = min(tiles_m - first_m, kGroup);
+  const int tm = first_m + (tile % per_group) % group_rows;
+  const int tn = (tile % per_group) / group_rows;
+  const int m0 = tm * BM, n0 = tn * BN;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < Sh::kStages; i++) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    mbar_init(done, 1);
+    *failed = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, Sh::kTmemCols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // Producer: one 3D TMA load per operand per stage brings all S digits.
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&tma_a) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&tma_b) : "memory");
+    for (int kb = 0; kb < k_blocks; kb++) {
+      const int st = kb % Sh::kStages;
+      const uint32_t round = (uint32_t)(kb / Sh::kStages);
+      if (!mbar_wait(&empty[st], (round & 1) ^ 1)) {
+        atomicOr(status, 2);
+        *failed = 1;
+        break;
+      }
+      mbar_expect_tx(&full[st], (uint32_t)Sh::kStage);
+      const int kc = (kb0 + kb) * BK;
+      tma_load_3d(sA + st * S * Sh::kASlab, &tma_a, &full[st], kc, m0, w * S);
+      tma_load_3d(sB + st * S * Sh::kBSlab, &tma_b, &full[st], kc, n0, w * S);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer.
+    for (int kb = 0; kb < k_blocks; kb++) {
+      const int st = kb % Sh::kStages;
+      const uint32_t round = (uint32_t)(kb / Sh::kStages);
+      if (!mbar_wait(&full[st], round & 1)) {
+        atomicOr(status, 2);
+        *failed = 1;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t a_base = smem_u32(sA + st * S * Sh::kASlab);
+      const uint32_t b_base = smem_u32(sB + st * S * Sh::kBSlab);
+#pragma unroll
+      for (int kk = 0; kk < BK / 32; kk++) {
+#pragma unroll
+        for (int s = 1; s <= S; s++) {
+          const int total = (S + 1 - s) * BN;
+#pragma unroll
+          for (int nn0 = 0; nn0 < total; nn0 += 256) {
+            const int nn = total - nn0 < 256 ? total - nn0 : 256;
+            const uint64_t ad = desc_sw64(a_base + (s - 1) * Sh::kASlab + kk * 32);
+            const uint64_t bd = desc_sw64(b_base + nn0 * BK + kk * 32);
+            const uint32_t acc = (kb > 0 || kk > 0 || s > 1) ? 1u : 0u;
+            umma_i8(tmem + (uint32_t)((s - 1) * BN + nn0), ad, bd, idesc_i8(nn), acc);
+          }
+        }
+      }
+      umma_commit(&empty[st]);
+    }
+    // Signals the epilogue once every MMA issued so far has completed.
+    umma_commit(done);
+  } else if (warp >= 2) {
+    // Epilogue: warp w reads TMEM lanes 32·(w % 4) .. +31.
+    const bool ok = mbar_wait(done, 0, true);
+    tc_fence_after();
+    if (!ok) atomicOr(status, 2);
+    const int q = warp & 3;
+    const int r = m0 + q * 32 + lane;
+    const bool run = ok && !*failed && k_blocks > 0;
+    const int er = run && r < m ? ea[(int64_t)w * m_pad + r] : 0;
+    double* crow = c + ((int64_t)w * m + r) * (int64_t)n;
+#pragma unroll 1
+    for (int chunk = 0; chunk < BN / 16; chunk++) {
+      double v[16];
+#pragma unroll
+      for (int j = 0; j < 16; j++) v[j] = 0.0;
+      if (run) {
+#pragma unroll
+        for (int l = S + 1; l >= 2; l--) {
+          int32_t acc[16];
+          tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((l - 2) * BN + chunk * 16), acc);
+          tmem_wait_ld();
+          const double scale = ldexp(1.0, -8 * l);
+#pragma unroll
+          for (int j = 0; j < 16; j++) v[j] += (double)acc[j] * scale;
+        }
+      }
+      if (run && r < m) {
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          const int col = n0 + chunk * 16 + j;
+          if (col < n) {
+            double x = ldexp(v[j], er + eb[(int64_t)w * n_pad + col]);
+            if (accumulate) x += crow[col];
+            crow[col] = x;
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, Sh::kTmemCols);
+  }
+}
+
+// Per row of x [rows][k] (leading dimension ld): the exponent e with
+// max|x| < 2^(e-2), or 0 for a row of zeros; status bit 1 if a value isn't
+// finite. One block per row, rows of `rows_pad` per batch.
+__global__ void row_exponents(const double* __restrict__ x, int64_t batches, int64_t rows, int64_t k, int64_t ld,
+                              int64_t rows_pad, int32_t* __restrict__ e, int* status) {
+  __shared__ double red[32];
+  for (int64_t g = blockIdx.x; g < batches * rows_pad; g += gridDim.x) {
+    const int64_t w = g / rows_pad, r = g % rows_pad;
+    double m = 0.0;
+    bool bad = false;
+    if (r < rows) {
+      const double* row = x + (w * rows + r) * ld;
+      for (int64_t i = threadIdx.x; i < k; i += blockDim.x) {
+        double v = fabs(row[i]);
+        bad |= !(v <= 1.7976931348623157e308);
+        m = fmax(m, v);
+      }
+    }
+    if (bad) atomicOr(status, 1);
+    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+      for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      if (threadIdx.x == 0) {
+        int ex = 0;
+        if (m > 0.0 && m <= 1.7976931348623157e308) {
+          frexp(m, &ex);
+          ex += 2;
+        }
+        e[g] = ex;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// The S digits of x / 2^e, 16 values of k per thread, written to
+// digits[(w·S + s)][r][k] for r < rows_pad and k < k_pad (zeros beyond).
+template <int S>
+__global__ void row_digits(const double* __restrict__ x, int64_t batches, int64_t rows, int64_t k, int64_t ld,
+                           int64_t rows_pad, int64_t k_pad, const int32_t* __restrict__ e,
+                           int8_t* __restrict__ digits) {
+  const int64_t chunks = k_pad / 16;
+  const int64_t total = batches * rows_pad * chunks;
+  const int64_t slab = rows_pad * k_pad;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t kc = i % chunks, g = i / chunks;
+    const int64_t w = g / rows_pad, r = g % rows_pad;
+    uint32_t word[S][4];
+#pragma unroll
+    for (int s = 0; s < S; s++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) word[s][q] = 0;
+    const int shift = 8 * S - e[g];
+    const double* row = x + (w * rows + r) * ld;
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      const int64_t kk = kc * 16 + j;
+      double v = (r < rows && kk < k) ? row[kk] : 0.0;
+      if (!(fabs(v) <= 1.7976931348623157e308)) v = 0.0;
+      long long X = llrint(ldexp(v, shift));
+#pragma unroll
+      for (int s = S - 1; s >= 0; s--) {
+        const long long d = ((X + 128) & 255) - 128;
+        word[s][j >> 2] |= ((uint32_t)(d & 255)) << (8 * (j & 3));
+        X = (X - d) >> 8;
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < S; s++) {
+      uint4* dst = (uint4*)(digits + (w * S + s) * slab + r * k_pad + kc * 16);
+      *dst = make_uint4(word[s][0], word[s][1], word[s][2], word[s][3]);
+    }
+  }
+}
+
+// FP64 product in k order. 64x64 tiles, 256 threads, 4x4 cells each.
+template <bool FMA>
+__global__ void __launch_bounds__(256) fp64_gemm_kernel(const double* __restrict__ a, const int32_t* __restrict__ held,
+                                                        const double* __restrict__ bt, double* __restrict__ c,
+                                                        int64_t m, int64_t n, int64_t k, int64_t zblock) {
+  constexpr int T = 64, KT = 16;
+  __shared__ double As[KT][T + 1];
+  __shared__ double Bs[KT][T + 1];
+  __shared__ uint8_t Hs[KT][T + 4];
+  const int64_t w = blockIdx.z;
+  const double* A = a + w * m * k;
+  const int32_t* H = held ? held + w * m * k : nullptr;
+  const double* B = bt + w * n * k;
+  double* C = c + w * m * n;
+  const int64_t r0 = (int64_t)blockIdx.y * T, c0 = (int64_t)blockIdx.x * T;
+  const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
+  double part[4][4], out[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) part[i][j] = out[i][j] = 0.0;
+  for (int64_t k0 = 0; k0 < k; k0 += KT) {
+    for (int idx = threadIdx.x; idx < T * KT; idx += 256) {
+      const int row = idx / KT, kk = idx % KT;
+      const int64_t gr = r0 + row, gk = k0 + kk;
+      const bool in = gr < m && gk < k;
+      As[kk][row] = in ? A[gr * k + gk] : 0.0;
+      Hs[kk][row] = in ? (H ? (uint8_t)(H[gr * k + gk] == 2) : (uint8_t)1) : (uint8_t)0;
+      const int64_t gc = c0 + row;
+      Bs[kk][row] = (gc < n && gk < k) ? B[gc * k + gk] : 0.0;
+    }
+    __syncthreads();
+    const int kt = (int)((k - k0) < KT ? (k - k0) : KT);
+    for (int kk = 0; kk < kt; kk++) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const double av = As[kk][tr * 4 + i];
+        const bool h = Hs[kk][tr * 4 + i] != 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const double bv = Bs[kk][tc * 4 + j];
+          if (FMA) {
+            if (h) part[i][j] = fma(av, bv, part[i][j]);
+          } else {
+            const double p = h ? __dmul_rn(av, bv) : 0.0;
+            part[i][j] = __dadd_rn(part[i][j], p);
+          }
+        }
+      }
+      if (zblock > 0 && (k0 + kk + 1) % zblock == 0) {
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            out[i][j] = __dadd_rn(out[i][j], part[i][j]);
+            part[i][j] = 0.0;
+          }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int64_t gr = r0 + tr * 4 + i;
+    if (gr >= m) continue;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int64_t gc = c0 + tc * 4 + j;
+      if (gc >= n) continue;
+      double v = part[i][j];
+      if (zblock > 0) v = (k % zblock != 0) ? __dadd_rn(out[i][j], part[i][j]) : out[i][j];
+      C[gr * n + gc] = v;
+    }
+  }
+}
+
+__global__ void transpose_kernel(const double* __restrict__ b, double* __restrict__ bt, int64_t rows, int64_t cols) {
+  __shared__ double tile[32][33];
+  const int64_t w = blockIdx.z;
+  const double* B = b + w * rows * cols;
+  double* BT = bt + w * rows * cols;
+  const int64_t x0 = (int64_t)blockIdx.x * 32, y0 = (int64_t)blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int64_t r = y0 + i, cc = x0 + threadIdx.x;
+    tile[i][threadIdx.x] = (r < rows && cc < cols) ? B[r * cols + cc] : 0.0;
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int64_t cc = x0 + i, r = y0 + threadIdx.x;
+    if (cc < cols && r < rows) BT[cc * rows + r] = tile[threadIdx.x][i];
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  });
+  if (!fn) fail(EINFOLD_DEVICE, "cuTensorMapEncodeTiled is unavailable");
+  return fn;
+}
+
+// A 3D int8 tensor map over digits [planes][rows][k_pad], boxes of
+// (64 B of k, box_rows, S planes), 64-byte swizzle.
+CUtensorMap digit_map(const int8_t* digits, int64_t k_pad, int64_t rows, int64_t planes, int box_rows, int S) {
+  CUtensorMap map;
+  cuuint64_t dims[3] = {(cuuint64_t)k_pad, (cuuint64_t)rows, (cuuint64_t)planes};
+  cuuint64_t strides[2] = {(cuuint64_t)k_pad, (cuuint64_t)(k_pad * rows)};
+  cuuint32_t box[3] = {(cuuint32_t)BK, (cuuint32_t)box_rows, (cuuint32_t)S};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, (void*)digits, dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) fail(EINFOLD_DEVICE, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return map;
+}
+
+inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+template <int S>
+void split_gemm_s(Context& ctx, const double* a, const double* bt, double* c, int64_t batches, int64_t m,
+                  int64_t n, int64_t k, cudaStream_t stream) {
+  using Sh = SplitShape<S>;
+  const int64_t m_pad = round_up(m, BM), n_pad = round_up(n, BN), k_pad = round_up(k > 0 ? k : 1, BK);
+  DeviceBuffer<int8_t> da((size_t)(batches * S * m_pad * k_pad), stream);
+  DeviceBuffer<int8_t> db((size_t)(batches * S * n_pad * k_pad), stream);
+  DeviceBuffer<int32_t> ea((size_t)(batches * m_pad), stream), eb((size_t)(batches * n_pad), stream);
+  DeviceBuffer<int> status(1, stream);
+  status.zero();
+  row_exponents<<<blocks_for((uint64_t)(batches * m_pad), 1, 148 * 16), 256, 0, stream>>>(
+      a, batches, m, k, k, m_pad, ea.get(), status.get());
+  row_exponents<<<blocks_for((uint64_t)(batches * n_pad), 1, 148 * 16), 256, 0, stream>>>(
+      bt, batches, n, k, k, n_pad, eb.get(), status.get());
+  row_digits<S><<<blocks_for((uint64_t)(batches * m_pad * (k_pad / 16)), 256), 256, 0, stream>>>(
+      a, batches, m, k, k, m_pad, k_pad, ea.get(), da.get());
+  row_digits<S><<<blocks_for((uint64_t)(batches * n_pad * (k_pad / 16)), 256), 256, 0, stream>>>(
+      bt, batches, n, k, k, n_pad, k_pad, eb.get(), db.get());
+  EF_LAUNCH_CHECK();
+  ctx.kernels += 4;
+  CUtensorMap ta = digit_map(da.get(), k_pad, m_pad, batches * S, BM, S);
+  CUtensorMap tb = digit_map(db.get(), k_pad, n_pad, batches * S, BN, S);
+  EF_CUDA(cudaFuncSetAttribute(split_gemm_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::kSmem));
+  // Each level's int32 sum is exact while S·kc·2^14 < 2^31: long k runs in
+  // chunks whose FP64 results are added.
+  const int64_t k_blocks = k_pad / BK;
+  const int64_t chunk_blocks = ((int64_t)1 << 31) / ((int64_t)S << 14) / BK;
+  const int tiles_m = (int)(m_pad / BM), tiles_n = (int)(n_pad / BN);
+  for (int64_t kb0 = 0; kb0 < k_blocks; kb0 += chunk_blocks) {
+    const int kbs = (int)std::min<int64_t>(chunk_blocks, k_blocks - kb0);
+    dim3 grid((unsigned)(tiles_m * tiles_n), (unsigned)batches);
+    split_gemm_kernel<S><<<grid, kThreads, Sh::kSmem, stream>>>(ta, tb, ea.get(), eb.get(), c, (int)m, (int)n,
+                                                                 (int)m_pad, (int)n_pad, (int)kb0, kbs, tiles_m,
+                                                                 tiles_n, kb0 > 0 ? 1 : 0, status.get());
+    EF_LAUNCH_CHECK();
+    ctx.kernels++;
+  }
+  int st = 0;
+  EF_CUDA(cudaMemcpyAsync(&st, status.get(), sizeof(int), cudaMemcpyDeviceToHost, stream));
+  EF_CUDA(cudaStreamSynchronize(stream));
+  if (st & 1) fail(EINFOLD_INVALID, "the split product was given a value that isn't finite");
+  if (st & 2) fail(EINFOLD_TIMEOUT, "a bounded wait in the split product ran out");
+}
+
+}  // namespace
+
+void split_gemm(Context& ctx, const double* a, const double* bt, double* c, int64_t batches, int64_t m, int64_t n,
+                int64_t k, int slices, cudaStream_t stream) {
+  if (batches <= 0 || m <= 0 || n <= 0) return;
+  if (m > INT32_MAX / 2 || n > INT32_MAX / 2 || batches > 65535) fail(EINFOLD_INVALID, "a product too large");
+  if (k <= 0) {
+    EF_CUDA(cudaMemsetAsync(c, 0, (size_t)(batches * m * n) * sizeof(double), stream));
+    return;
+  }
+  switch (slices) {
+    case 2: split_gemm_s<2>(ctx, a, bt, c, batches, m, n, k, stream); break;
+    case 3: split_gemm_s<3>(ctx, a, bt, c, batches, m, n, k, stream); break;
+    case 4: split_gemm_s<4>(ctx, a, bt, c, batches, m, n, k, stream); break;
+    case 5: split_gemm_s<5>(ctx, a, bt, c, batches, m, n, k, stream); break;
+    case 6: split_gemm_s<6>(ctx, a, bt, c, batches, m, n, k, stream); break;
+    case 7: split_gemm_s<7>(ctx, a, bt, c, batches, m, n, k, stream); break;
+    default: fail(EINFOLD_INVALID, "slices must be 2 to 7, not %d", slices);
+  }
+}
+
+void fp64_gemm(Context& ctx, const double* a, const int32_t* held, const double* bt, double* c, int64_t batches,
+               int64_t m, int64_t n, int64_t k, int64_t /*batch_of_row*/, int64_t zblock, bool fused_multiply_add,
+               cudaStream_t stream) {
+  if (batches <= 0 || m <= 0 || n <= 0) return;
+  dim3 grid((unsigned)((n + 63) / 64), (unsigned)((m + 63) / 64), (unsigned)batches);
+  if (fused_multiply_add)
+    fp64_gemm_kernel<true><<<grid, 256, 0, stream>>>(a, held, bt, c, m, n, k, 0);
+  else
+    fp64_gemm_kernel<false><<<grid, 256, 0, stream>>>(a, held, bt, c, m, n, k, zblock);
+  EF_LAUNCH_CHECK();
+  ctx.kernels++;
+}
+
+void transpose(const double* b, double* bt, int64_t batches, int64_t rows, int64_t cols, cudaStream_t stream) {
+  dim3 grid((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32), (unsigned)batches);
+  transpose_kernel<<<grid, dim3(32, 8), 0, stream>>>(b, bt, rows, cols);
+  EF_LAUNCH_CHECK();
+}
+
+}  // namespace ef

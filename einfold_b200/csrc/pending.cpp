@@ -1,0 +1,24 @@
+// Entry points whose device paths are not built yet fail loudly.
+#include "fold.h"
+
+namespace ef {
+
+FoldOutput discriminate_fold(Context&, const FoldD&, const Relation&, const Relation&, const Relation*,
+                             const std::vector<Field>&, const einfold_options&, Budget&) {
+  fail(EINFOLD_COMPUTE, "the discrimination algorithm is not built yet");
+}
+FoldOutput chain_fold(Context&, const FoldD&, const std::vector<const Relation*>&, const std::vector<Field>&,
+                      const einfold_options&, Budget&) {
+  fail(EINFOLD_COMPUTE, "chains are not built yet");
+}
+FoldOutput fused_pipeline(Context&, const PipelineD&, const Relation&, const Relation&, const Relation&,
+                          const std::vector<Field>&, const einfold_options&, Budget&) {
+  fail(EINFOLD_COMPUTE, "the fused pipeline is not built yet");
+}
+
+}  // namespace ef
+
+extern "C" int32_t einfold_rank_words(einfold_context*, const uint64_t*, int64_t, uint32_t*, uint32_t*, int64_t*,
+                                      void*) {
+  return EINFOLD_COMPUTE;
+}

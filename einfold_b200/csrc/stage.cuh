@@ -1,0 +1,62 @@
+// Staging Arrow columns into HBM, once per call, and small device helpers
+// shared by the folds.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "arrow.h"
+#include "common.h"
+
+namespace ef {
+
+// One column of a relation, every batch concatenated, in HBM.
+struct DeviceColumn {
+  Kind kind = Kind::Other;
+  int width = 0;
+  int64_t rows = 0;
+  int64_t nulls = 0;
+  DeviceBuffer<uint8_t> data;   // fixed-width values (rows * width)
+  DeviceBuffer<uint8_t> valid;  // one byte per row, 1 = valid; empty when nulls == 0
+  // var-length kinds
+  DeviceBuffer<int64_t> offsets;  // rows + 1
+  DeviceBuffer<uint8_t> bytes;
+};
+
+// Copies column `col` of every batch into HBM; validity as bytes.
+DeviceColumn stage_column(Context& ctx, const Relation& r, int col, bool with_validity = true);
+
+// Keys of an integer column as int64, with the largest value and whether any
+// is negative or too large for int64 (an unsigned 2^63 or more).
+struct KeyStats {
+  int64_t max = -1;
+  bool negative = false;
+  bool too_large = false;
+};
+DeviceBuffer<int64_t> keys_as_i64(Context& ctx, const DeviceColumn& c, KeyStats* stats);
+
+// Exclusive prefix sum of n flags (uint8) into int64 positions; returns the total.
+int64_t exclusive_scan_flags(Context& ctx, const uint8_t* flags, int64_t n, int64_t* out);
+
+// Packs n bytes (0/1) into an Arrow validity bitmap of (n + 7) / 8 bytes.
+void pack_bits(Context& ctx, const uint8_t* bytes, int64_t n, uint8_t* bits);
+
+// Device to host, into a fresh host buffer.
+HostBuffer to_host(Context& ctx, const void* dev, size_t bytes);
+
+// A row of small descriptors passed to kernels by value.
+constexpr int kMaxDims = 8;
+struct Role {
+  int n = 0;
+  const int64_t* keys[kMaxDims] = {};
+  int64_t extent[kMaxDims] = {};
+};
+
+__device__ __forceinline__ int64_t role_position(const Role& r, int64_t row) {
+  int64_t p = 0;
+  for (int i = 0; i < r.n; i++) p = p * r.extent[i] + r.keys[i][row];
+  return p;
+}
+
+}  // namespace ef

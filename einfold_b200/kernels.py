@@ -1,0 +1,387 @@
+"""einfold's kernel layer on a B200: the Python face of the C ABI.
+
+The functions mirror ``einfold_kernels`` (``crates/einfold-kernels/src/lib.rs:43-48``)
+name for name: :func:`fold`, :func:`fold_dense`, :func:`fold_chain`,
+:func:`pipeline`, :func:`schema`, :func:`pipeline_schema`, with :class:`Options`,
+:class:`Budget`, :class:`Host`, :class:`FloatKeys`, :class:`DomainRows`,
+:class:`Relation`, :class:`Folded`, :class:`Piped` and :class:`Algorithm`.
+Relations are pyarrow record batches; they cross into the library through the
+Arrow C Data Interface, and every computation runs on the GPU. Where the
+reference returns ``Ok(None)`` (the caller runs the host's plan) these return
+``None``; its ``ArrowError`` variants are the exceptions below.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import pyarrow as pa
+
+from . import _lib, ir
+
+
+class ArrowMemoryError(MemoryError):
+    """``ArrowError::MemoryError``: the budget refused (``options.rs:101-108``)."""
+
+
+class ArrowInvalidArgumentError(ValueError):
+    """``ArrowError::InvalidArgumentError`` (``lib.rs:54-56``)."""
+
+
+class ArrowComputeError(RuntimeError):
+    """``ArrowError::ComputeError`` (``discriminate.rs:383-387``)."""
+
+
+class DeviceError(RuntimeError):
+    """A CUDA error or a device-side wait that ran out."""
+
+
+class FloatKeys(enum.IntEnum):
+    BITWISE = 0
+    SIGNED_ZEROS_EQUAL = 1
+
+
+@dataclass(frozen=True)
+class Host:
+    float_keys: FloatKeys = FloatKeys.BITWISE
+
+
+class DomainRows(enum.IntEnum):
+    ANY = 0
+    UNIQUE_KEYS = 1
+
+
+class Budget:
+    """The memory a kernel may take beyond its inputs (``options.rs:56-65``)."""
+
+    def grow(self, nbytes: int) -> bool:  # pragma: no cover - interface
+        return True
+
+    def shrink(self, nbytes: int) -> None:
+        pass
+
+
+class Precision(enum.Enum):
+    """How dense products are computed: int8 slices on the tensor cores with
+    exact integer sums and an FP64 combine (``SPLIT``), or FP64 on the CUDA
+    cores in the reference's order of additions (``FP64``)."""
+
+    SPLIT = 0
+    FP64 = 1
+
+
+@dataclass
+class Options:
+    host: Host = field(default_factory=Host)
+    threads: int = 1
+    domain_rows: DomainRows = DomainRows.ANY
+    budget: Optional[Budget] = None
+    precision: Precision = Precision.SPLIT
+    slices: int = 0
+    device: int = 0
+
+
+class Algorithm(enum.Enum):
+    DENSE = "dense"
+    DISCRIMINATE = "discriminate"
+    FUSED = "fused"
+
+
+@dataclass
+class Relation:
+    schema: pa.Schema
+    batches: List[pa.RecordBatch]
+
+
+@dataclass
+class Folded:
+    algorithm: Algorithm
+    batches: List[pa.RecordBatch]
+
+
+@dataclass
+class Piped:
+    batches: List[pa.RecordBatch]
+    tiles_visited: int
+    tiles: int
+
+
+# ---------------------------------------------------------------------------
+# Marshalling
+# ---------------------------------------------------------------------------
+
+
+class _Keep:
+    """Holds the ctypes objects a call's pointers refer to."""
+
+    def __init__(self):
+        self.items = []
+        self.exported_arrays = []
+        self.exported_schemas = []
+
+    def add(self, x):
+        self.items.append(x)
+        return x
+
+    def release(self):
+        rel_a = ctypes.CFUNCTYPE(None, ctypes.POINTER(_lib.ArrowArray))
+        rel_s = ctypes.CFUNCTYPE(None, ctypes.POINTER(_lib.ArrowSchema))
+        for a in self.exported_arrays:
+            if a.release:
+                rel_a(a.release)(ctypes.byref(a))
+        for s in self.exported_schemas:
+            if s.release:
+                rel_s(s.release)(ctypes.byref(s))
+        self.exported_arrays.clear()
+        self.exported_schemas.clear()
+
+
+def _array(ctype, values):
+    arr = (ctype * max(len(values), 1))()
+    for i, v in enumerate(values):
+        arr[i] = v
+    return arr
+
+
+def _expression(e: Optional[ir.Expression], keep: _Keep) -> _lib.Expression:
+    if e is None:
+        return _lib.Expression(0, None)
+    nodes = [_lib.ExprNode(k, a, b, 0, v) for (k, a, b, v) in e.postfix()]
+    arr = keep.add(_array(_lib.ExprNode, nodes))
+    return _lib.Expression(len(nodes), arr)
+
+
+def _operand(op: ir.Operand, keep: _Keep) -> _lib.Operand:
+    keys = keep.add(_array(_lib.Key, [_lib.Key(k.dimension, k.column) for k in op.keys]))
+    return _lib.Operand(len(op.keys), keys, -1 if op.factor is None else op.factor)
+
+
+def _fold_desc(f: ir.Fold, keep: _Keep) -> _lib.FoldDesc:
+    eq = keep.add(_array(ctypes.c_int32, [int(d.equality) for d in f.dimensions()]))
+    ops = keep.add(_array(_lib.Operand, [_operand(o, keep) for o in f.operands()]))
+    outs = keep.add(_array(_lib.Output, [
+        _lib.Output(o.dimension, -1 if o.domain_key is None else o.domain_key.column,
+                    0 if o.domain_key is None else int(o.domain_key.equality)) for o in f.outputs()]))
+    conds = keep.add(_array(_lib.Condition, [
+        _lib.Condition(c.left, int(c.comparison), c.right, 0, c.offset) for c in f.conditions()]))
+    dom = None
+    if f.domain() is not None:
+        carry = keep.add(_array(ctypes.c_int32, list(f.domain().carry)))
+        missing = f.domain().missing
+        dom = keep.add(_lib.Domain(len(f.domain().carry), carry, 0 if missing is None else 1, 0,
+                                   0.0 if missing is None else missing))
+    row = f.row()
+    desc = _lib.FoldDesc(len(f.dimensions()), eq, len(f.operands()), ops, len(f.outputs()), outs,
+                         0 if row.is_product else 1, _expression(row.expression, keep),
+                         ctypes.pointer(dom) if dom is not None else None, len(f.conditions()), conds)
+    return keep.add(desc)
+
+
+def _pipeline_desc(p: ir.Pipeline, keep: _Keep) -> _lib.PipelineDesc:
+    prod = _fold_desc(p.producer(), keep)
+    w = p.weight()
+    eq = keep.add(_array(ctypes.c_int32, [int(d.equality) for d in p.dimensions()]))
+    outs = keep.add(_array(ctypes.c_int32, list(p.outputs())))
+    if w.is_exp:
+        desc = _lib.PipelineDesc(ctypes.pointer(prod), 0, w.scale.kind, w.scale.c, int(w.shift),
+                                 int(p.normalizer()), _lib.Expression(0, None), len(p.dimensions()), eq,
+                                 _operand(p.values(), keep), len(p.outputs()), outs)
+    else:
+        desc = _lib.PipelineDesc(ctypes.pointer(prod), 1, 0, 1.0, 0, int(p.normalizer()),
+                                 _expression(w.of, keep), len(p.dimensions()), eq, _operand(p.values(), keep),
+                                 len(p.outputs()), outs)
+    return keep.add(desc)
+
+
+def _export_schema(s: pa.Schema, keep: _Keep) -> _lib.ArrowSchema:
+    c = keep.add(_lib.ArrowSchema())
+    s._export_to_c(ctypes.addressof(c))
+    keep.exported_schemas.append(c)
+    return c
+
+
+def _relation(r, keep: _Keep) -> _lib.Relation:
+    if isinstance(r, Relation):
+        schema, batches = r.schema, list(r.batches)
+    elif isinstance(r, pa.Table):
+        schema, batches = r.schema, r.to_batches()
+    elif isinstance(r, pa.RecordBatch):
+        schema, batches = r.schema, [r]
+    else:
+        batches = list(r)
+        if not batches:
+            raise ArrowInvalidArgumentError("a relation of no batches needs its schema: pass a Relation")
+        schema = batches[0].schema
+    cs = _export_schema(schema, keep)
+    arrays = []
+    for b in batches:
+        a = keep.add(_lib.ArrowArray())
+        b._export_to_c(ctypes.addressof(a))
+        keep.exported_arrays.append(a)
+        arrays.append(ctypes.pointer(a))
+    ptrs = keep.add(_array(ctypes.POINTER(_lib.ArrowArray), arrays))
+    return keep.add(_lib.Relation(ctypes.pointer(cs), len(batches), ptrs))
+
+
+def _options(o: Options, keep: _Keep) -> _lib.Options:
+    grow = _lib.GROW(0)
+    shrink = _lib.SHRINK(0)
+    if o.budget is not None:
+        budget = o.budget
+        grow = keep.add(_lib.GROW(lambda _ctx, n: 1 if budget.grow(int(n)) else 0))
+        shrink = keep.add(_lib.SHRINK(lambda _ctx, n: budget.shrink(int(n))))
+    return keep.add(_lib.Options(int(o.host.float_keys), max(int(o.threads), 1), int(o.domain_rows),
+                                 int(o.precision.value), int(o.slices), 0, None, grow, shrink))
+
+
+def _raise(status: int, message: str):
+    if status == _lib.BUDGET:
+        raise ArrowMemoryError(message)
+    if status == _lib.INVALID:
+        raise ArrowInvalidArgumentError(message)
+    if status == _lib.COMPUTE:
+        raise ArrowComputeError(message)
+    raise DeviceError(f"{_lib.STATUS_NAMES.get(status, status)}: {message}")
+
+
+@dataclass
+class CallInfo:
+    """What the last call on this thread did on the device."""
+
+    kernels_launched: int = 0
+    device_ms: float = 0.0
+    message: str = ""
+
+
+last_call = CallInfo()
+
+
+def _collect(res: _lib.Result) -> List[pa.RecordBatch]:
+    lib = _lib.load()
+    try:
+        schema = pa.Schema._import_from_c(ctypes.addressof(res.schema.contents))
+        return [pa.RecordBatch._import_from_c(ctypes.addressof(res.batches[i]), schema)
+                for i in range(res.n_batches)]
+    finally:
+        lib.einfold_result_release(ctypes.byref(res))
+
+
+def _call(fn, *args) -> Optional[_lib.Result]:
+    res = _lib.Result()
+    status = fn(_lib.context(args[-1]), *args[:-1], ctypes.byref(res))
+    msg = res.message.decode(errors="replace")
+    last_call.kernels_launched = res.kernels_launched
+    last_call.device_ms = res.device_ms
+    last_call.message = msg
+    if status == _lib.DECLINED:
+        return None
+    if status != _lib.OK:
+        _raise(status, msg)
+    return res
+
+
+# ---------------------------------------------------------------------------
+# The kernel layer's functions (crates/einfold-kernels/src/algorithm.rs)
+# ---------------------------------------------------------------------------
+
+
+def fold(f: ir.Fold, a, b, domain=None, schema: Optional[pa.Schema] = None,
+         options: Optional[Options] = None) -> Folded:
+    """``einfold_kernels::fold`` (algorithm.rs:97-133): dense when its
+    requirements hold, else discrimination."""
+    options = options or Options()
+    keep = _Keep()
+    try:
+        res = _call(_lib.load().einfold_fold, ctypes.byref(_fold_desc(f, keep)), ctypes.byref(_relation(a, keep)),
+                    ctypes.byref(_relation(b, keep)),
+                    ctypes.byref(_relation(domain, keep)) if domain is not None else None,
+                    ctypes.byref(_options(options, keep)), options.device)
+        if res is None:
+            raise ArrowComputeError("the fold declined")
+        alg = Algorithm(_lib.ALGORITHMS[res.algorithm])
+        return Folded(alg, _collect(res))
+    finally:
+        keep.release()
+
+
+def fold_dense(f: ir.Fold, a, b, domain=None, schema: Optional[pa.Schema] = None,
+               options: Optional[Options] = None) -> Optional[List[pa.RecordBatch]]:
+    """``einfold_kernels::fold_dense`` (algorithm.rs:52-62)."""
+    options = options or Options()
+    keep = _Keep()
+    try:
+        res = _call(_lib.load().einfold_fold_dense, ctypes.byref(_fold_desc(f, keep)),
+                    ctypes.byref(_relation(a, keep)), ctypes.byref(_relation(b, keep)),
+                    ctypes.byref(_relation(domain, keep)) if domain is not None else None,
+                    ctypes.byref(_options(options, keep)), options.device)
+        return None if res is None else _collect(res)
+    finally:
+        keep.release()
+
+
+def fold_chain(f: ir.Fold, operands: Sequence, schema: Optional[pa.Schema] = None,
+               options: Optional[Options] = None) -> Optional[List[pa.RecordBatch]]:
+    """``einfold_kernels::fold_chain`` (algorithm.rs:76-83)."""
+    options = options or Options()
+    keep = _Keep()
+    try:
+        rels = keep.add(_array(_lib.Relation, [_relation(r, keep) for r in operands]))
+        res = _call(_lib.load().einfold_fold_chain, ctypes.byref(_fold_desc(f, keep)), rels,
+                    ctypes.byref(_options(options, keep)), options.device)
+        return None if res is None else _collect(res)
+    finally:
+        keep.release()
+
+
+def pipeline(p: ir.Pipeline, operands: Sequence, schema: Optional[pa.Schema] = None,
+             options: Optional[Options] = None) -> Optional[Piped]:
+    """``einfold_kernels::pipeline`` (algorithm.rs:146-160) over ``[q, k, v]``."""
+    options = options or Options()
+    keep = _Keep()
+    try:
+        rels = keep.add(_array(_lib.Relation, [_relation(r, keep) for r in operands]))
+        res = _call(_lib.load().einfold_pipeline, ctypes.byref(_pipeline_desc(p, keep)), rels,
+                    ctypes.byref(_options(options, keep)), options.device)
+        if res is None:
+            return None
+        visited, tiles = int(res.tiles_visited), int(res.tiles)
+        return Piped(_collect(res), visited, tiles)
+    finally:
+        keep.release()
+
+
+def schema(f: ir.Fold, operands: Sequence[pa.Schema], domain: Optional[pa.Schema] = None) -> pa.Schema:
+    """``einfold_kernels::schema`` (schema.rs:31-36)."""
+    keep = _Keep()
+    try:
+        ptrs = keep.add(_array(ctypes.POINTER(_lib.ArrowSchema),
+                               [ctypes.pointer(_export_schema(s, keep)) for s in operands]))
+        dom = ctypes.pointer(_export_schema(domain, keep)) if domain is not None else None
+        out = _lib.ArrowSchema()
+        msg = ctypes.create_string_buffer(480)
+        st = _lib.load().einfold_schema(ctypes.byref(_fold_desc(f, keep)), ptrs, len(operands), dom,
+                                        ctypes.byref(out), msg, 480)
+        if st != _lib.OK:
+            _raise(st, msg.value.decode())
+        return pa.Schema._import_from_c(ctypes.addressof(out))
+    finally:
+        keep.release()
+
+
+def pipeline_schema(p: ir.Pipeline, inputs: Sequence[pa.Schema]) -> pa.Schema:
+    """``einfold_kernels::pipeline_schema`` (schema.rs:155-206)."""
+    keep = _Keep()
+    try:
+        ptrs = keep.add(_array(ctypes.POINTER(_lib.ArrowSchema),
+                               [ctypes.pointer(_export_schema(s, keep)) for s in inputs]))
+        out = _lib.ArrowSchema()
+        msg = ctypes.create_string_buffer(480)
+        st = _lib.load().einfold_pipeline_schema(ctypes.byref(_pipeline_desc(p, keep)), ptrs, ctypes.byref(out),
+                                                 msg, 480)
+        if st != _lib.OK:
+            _raise(st, msg.value.decode())
+        return pa.Schema._import_from_c(ctypes.addressof(out))
+    finally:
+        keep.release()

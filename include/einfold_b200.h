@@ -1,0 +1,256 @@
+/*
+ * einfold_b200 — a C ABI for einfold's kernel layer on one NVIDIA B200.
+ *
+ * The entry points replace the four functions that einfold's physical
+ * operator calls (crates/einfold-kernels/src/algorithm.rs:52-160):
+ *
+ *   einfold_fold        <- einfold_kernels::fold        (algorithm.rs:97-133)
+ *   einfold_fold_dense  <- einfold_kernels::fold_dense  (algorithm.rs:52-62)
+ *   einfold_fold_chain  <- einfold_kernels::fold_chain  (algorithm.rs:76-83)
+ *   einfold_pipeline    <- einfold_kernels::pipeline    (algorithm.rs:146-160)
+ *   einfold_schema / einfold_pipeline_schema
+ *                       <- einfold_kernels::{schema, pipeline_schema}
+ *                          (schema.rs:31-36, 155-206)
+ *
+ * Tables cross the boundary in the Arrow C Data Interface: a relation is its
+ * batches, each exported as a struct array (what arrow-rs's
+ * `FFI_ArrowArray::new(&StructArray::from(batch).to_data())` and pyarrow's
+ * `RecordBatch._export_to_c` give), with the schema exported once. Results
+ * come back the same way and are owned by the library until
+ * einfold_result_release. Fold and pipeline descriptions are plain structs
+ * mirroring crates/einfold-ir (fold.rs:59-416, pipeline.rs:63-201,
+ * expression.rs:57-135).
+ *
+ * The lower entry points (einfold_rank_words, einfold_split_gemm,
+ * einfold_fp64_gemm, einfold_attention_*) take device pointers and a CUDA
+ * stream; they serve a caller that keeps its data in HBM, such as the
+ * torch.autograd.Function in the Python package, and the benchmarks.
+ *
+ * Every call is synchronous with respect to the host unless it takes a
+ * stream. Calls on one context are serialized by the context; contexts on
+ * the same device may be used from different threads.
+ */
+#ifndef EINFOLD_B200_H
+#define EINFOLD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- Arrow C Data Interface (https://arrow.apache.org/docs/format/CDataInterface.html) ---- */
+#ifndef ARROW_C_DATA_INTERFACE
+#define ARROW_C_DATA_INTERFACE
+#define ARROW_FLAG_DICTIONARY_ORDERED 1
+#define ARROW_FLAG_NULLABLE 2
+#define ARROW_FLAG_MAP_KEYS_SORTED 4
+struct ArrowSchema {
+  const char* format;
+  const char* name;
+  const char* metadata;
+  int64_t flags;
+  int64_t n_children;
+  struct ArrowSchema** children;
+  struct ArrowSchema* dictionary;
+  void (*release)(struct ArrowSchema*);
+  void* private_data;
+};
+struct ArrowArray {
+  int64_t length;
+  int64_t null_count;
+  int64_t offset;
+  int64_t n_buffers;
+  int64_t n_children;
+  const void** buffers;
+  struct ArrowArray** children;
+  struct ArrowArray* dictionary;
+  void (*release)(struct ArrowArray*);
+  void* private_data;
+};
+#endif
+
+/* ---- Status ---- */
+typedef enum {
+  EINFOLD_OK = 0,
+  /* The kernels' requirements don't hold: the caller runs the host's plan
+   * (Ok(None) in the reference). */
+  EINFOLD_DECLINED = 1,
+  /* The budget refused memory (ArrowError::MemoryError, options.rs:101-108). */
+  EINFOLD_BUDGET = 2,
+  /* Inputs the fold doesn't fit (ArrowError::InvalidArgumentError, lib.rs:54-56). */
+  EINFOLD_INVALID = 3,
+  /* A limit of the algorithm (ArrowError::ComputeError, discriminate.rs:383-387). */
+  EINFOLD_COMPUTE = 4,
+  /* A CUDA error: the device is unusable for this call. */
+  EINFOLD_DEVICE = 5,
+  /* A bounded device-side wait ran out; the context stays usable. */
+  EINFOLD_TIMEOUT = 6
+} einfold_status;
+
+/* Which algorithm computed a fold (algorithm.rs:23-36). */
+typedef enum { EINFOLD_ALG_NONE = 0, EINFOLD_ALG_DENSE = 1, EINFOLD_ALG_DISCRIMINATE = 2, EINFOLD_ALG_FUSED = 3 } einfold_algorithm;
+
+/* ---- Fold descriptions (crates/einfold-ir/src/fold.rs) ---- */
+typedef struct { int32_t dimension; int32_t column; } einfold_key;            /* fold.rs:Key */
+typedef struct {                                                              /* fold.rs:Operand */
+  int32_t n_keys;
+  const einfold_key* keys;
+  int32_t factor; /* column index, or -1 for none */
+} einfold_operand;
+typedef struct {                                                              /* fold.rs:Output */
+  int32_t dimension;
+  int32_t domain_column;   /* -1 when the fold has no domain */
+  int32_t domain_equality; /* 0 '=', 1 IS NOT DISTINCT FROM */
+} einfold_output;
+typedef struct {                                                              /* fold.rs:Condition */
+  int32_t left;
+  int32_t comparison; /* 0 <, 1 <=, 2 >, 3 >= */
+  int32_t right;
+  int32_t pad;
+  int64_t offset;     /* left <comparison> right + offset */
+} einfold_condition;
+typedef struct {                                                              /* fold.rs:Domain */
+  int32_t n_carry;
+  const int32_t* carry;
+  int32_t has_missing;
+  int32_t pad;
+  double missing;
+} einfold_domain;
+/* An expression in postfix order (expression.rs:117-135). kind: 0 column
+ * (a = operand, b = column), 1 literal (value), 2 unary (a = 0 negate,
+ * 1 abs, 2 exp, 3 ln), 3 binary (a = 0 +, 1 -, 2 *, 3 /, 4 power). */
+typedef struct { int32_t kind; int32_t a; int32_t b; int32_t pad; double value; } einfold_expr_node;
+typedef struct { int32_t n_nodes; const einfold_expr_node* nodes; } einfold_expression;
+
+typedef struct {
+  int32_t n_dimensions;
+  const int32_t* equality;   /* per dimension: 0 '=', 1 IS NOT DISTINCT FROM */
+  int32_t n_operands;
+  const einfold_operand* operands;
+  int32_t n_outputs;
+  const einfold_output* outputs;
+  int32_t row_is_expression; /* 0: product of factors; 1: `row` */
+  einfold_expression row;
+  const einfold_domain* domain; /* NULL: no domain */
+  int32_t n_conditions;
+  const einfold_condition* conditions;
+} einfold_fold_desc;
+
+/* ---- Pipelines (crates/einfold-ir/src/pipeline.rs) ---- */
+typedef struct {
+  const einfold_fold_desc* producer;
+  int32_t weight_is_expression; /* 0: Weight::Exp{scale, shift}; 1: Weight::Of(weight) */
+  int32_t scale_kind;           /* 0 One, 1 Times(c), 2 Over(c) */
+  double scale_c;
+  int32_t shift;                /* 0 None, 1 KeptMaximum */
+  int32_t normalizer;           /* 0 KeptGroups, 1 JoinedRows, 2 None */
+  einfold_expression weight;    /* reads operand 0, column 0: the score */
+  int32_t n_dimensions;         /* the pipeline's own dimensions */
+  const int32_t* equality;
+  einfold_operand values;
+  int32_t n_outputs;
+  const int32_t* outputs;
+} einfold_pipeline_desc;
+
+/* ---- Relations ---- */
+typedef struct {
+  const struct ArrowSchema* schema; /* a struct schema: the relation's columns */
+  int64_t n_batches;
+  struct ArrowArray* const* batches; /* each a struct array of `schema` */
+} einfold_relation;
+
+/* ---- Options (options.rs:70-84) ---- */
+typedef struct {
+  int32_t float_keys;  /* 0 Bitwise, 1 SignedZerosEqual (options.rs:14-23) */
+  int32_t threads;     /* host threads for staging; results don't depend on it */
+  int32_t domain_rows; /* 0 Any, 1 UniqueKeys (options.rs:35-44) */
+  /* Dense products: 0 split (int8 slices on the tensor cores, exact integer
+   * accumulation, FP64 combine), 1 fp64 (CUDA-core FP64 in the reference's
+   * order of additions: the reference's bits). */
+  int32_t precision;
+  int32_t slices;      /* split products: slices per operand, 0 = default (6) */
+  int32_t pad;
+  /* The budget (options.rs:56-65): grow returns nonzero if `bytes` more may be
+   * allocated; shrink gives bytes back. NULL grow = no limit. */
+  void* budget_ctx;
+  int32_t (*budget_grow)(void* ctx, uint64_t bytes);
+  void (*budget_shrink)(void* ctx, uint64_t bytes);
+} einfold_options;
+
+/* ---- Results ---- */
+typedef struct {
+  int32_t status;    /* einfold_status */
+  int32_t algorithm; /* einfold_algorithm */
+  int64_t n_batches;
+  struct ArrowArray* batches; /* n_batches struct arrays, library-owned */
+  struct ArrowSchema* schema; /* the result's schema, library-owned */
+  uint64_t tiles_visited;     /* pipelines: pairs of tiles computed (fused.rs:114-123) */
+  uint64_t tiles;             /* pipelines: pairs of tiles in the same batch */
+  /* Device kernels launched and device milliseconds spent, for metrics. */
+  uint64_t kernels_launched;
+  double device_ms;
+  char message[480];
+} einfold_result;
+
+typedef struct einfold_context einfold_context;
+
+/* A context on `device` (one stream). NULL on failure; see einfold_last_error. */
+einfold_context* einfold_context_create(int32_t device);
+void einfold_context_destroy(einfold_context* ctx);
+const char* einfold_last_error(void);
+/* The library's version string. */
+const char* einfold_version(void);
+
+/* einfold_kernels::fold: dense when its requirements hold, else
+ * discrimination. `domain` may be NULL. */
+int32_t einfold_fold(einfold_context* ctx, const einfold_fold_desc* fold, const einfold_relation* a,
+                     const einfold_relation* b, const einfold_relation* domain, const einfold_options* options,
+                     einfold_result* result);
+/* einfold_kernels::fold_dense: the dense algorithm or EINFOLD_DECLINED. */
+int32_t einfold_fold_dense(einfold_context* ctx, const einfold_fold_desc* fold, const einfold_relation* a,
+                           const einfold_relation* b, const einfold_relation* domain,
+                           const einfold_options* options, einfold_result* result);
+/* einfold_kernels::fold_chain over three operands. */
+int32_t einfold_fold_chain(einfold_context* ctx, const einfold_fold_desc* fold, const einfold_relation* operands,
+                           const einfold_options* options, einfold_result* result);
+/* einfold_kernels::pipeline over q, k and v. */
+int32_t einfold_pipeline(einfold_context* ctx, const einfold_pipeline_desc* pipeline,
+                         const einfold_relation* operands, const einfold_options* options,
+                         einfold_result* result);
+/* einfold_kernels::schema: the result schema of a fold over `operands`
+ * (2 or 3) and an optional domain. On success *out is owned by the caller. */
+int32_t einfold_schema(const einfold_fold_desc* fold, const struct ArrowSchema* const* operands,
+                       int32_t n_operands, const struct ArrowSchema* domain, struct ArrowSchema* out,
+                       char* message, int32_t message_len);
+int32_t einfold_pipeline_schema(const einfold_pipeline_desc* pipeline, const struct ArrowSchema* const* inputs,
+                                struct ArrowSchema* out, char* message, int32_t message_len);
+/* Releases what a result holds. */
+void einfold_result_release(einfold_result* result);
+
+/* ---- Device-pointer entry points ---- */
+
+/* Ranks of n 64-bit words in their order (discriminate.rs:280-292): rank[i]
+ * for each word, first[r] the smallest index holding rank r; *n_ranks gets
+ * the number of distinct words. All pointers are device memory. */
+int32_t einfold_rank_words(einfold_context* ctx, const uint64_t* words, int64_t n, uint32_t* rank,
+                           uint32_t* first, int64_t* n_ranks, void* stream);
+
+/* C[w] = A[w] · B[w] for w < batches, FP64, all row-major device arrays:
+ * A [batches][m][k], B [batches][k][n] (b_transposed = 0) or
+ * [batches][n][k] (b_transposed = 1), C [batches][m][n].
+ * einfold_split_gemm slices each row of A and column of B into `slices`
+ * int8 digits under a power-of-two scale, multiplies them on the tensor
+ * cores with exact int32 accumulation and combines the levels in FP64;
+ * every input must be finite. einfold_fp64_gemm adds in k order with
+ * unfused multiply and add. */
+int32_t einfold_split_gemm(einfold_context* ctx, const double* a, const double* b, double* c, int64_t batches,
+                           int64_t m, int64_t n, int64_t k, int32_t b_transposed, int32_t slices, void* stream);
+int32_t einfold_fp64_gemm(einfold_context* ctx, const double* a, const double* b, double* c, int64_t batches,
+                          int64_t m, int64_t n, int64_t k, int32_t b_transposed, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
