@@ -121,6 +121,11 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t* v) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// 2^e for |e| < 1022, exactly, from its bits.
+__device__ __forceinline__ double pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
+// 2^{-8l}.
+__device__ __forceinline__ double exp2_neg8(int l) { return pow2(-8 * l); }
+
 // Shared-memory matrix descriptor: K-major, 64-byte swizzle, 8-row groups
 // 512 bytes apart (the layout TMA writes with CU_TENSOR_MAP_SWIZZLE_64B).
 __device__ __forceinline__ uint64_t desc_sw64(uint32_t addr) {
@@ -248,7 +253,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     // Signals the epilogue once every MMA issued so far has completed.
     umma_commit(done);
   } else if (warp >= 2) {
-    // Epilogue: warp w reads TMEM lanes 32·(w % 4) .. +31.
+    // Epilogue: warp w reads TMEM lanes 32·(w % 4) .. +31, one row per thread.
     const bool ok = mbar_wait(done, 0, true);
     tc_fence_after();
     if (!ok) atomicOr(status, 2);
@@ -257,31 +262,37 @@ __global__ void __launch_bounds__(kThreads, 1)
     const bool run = ok && !*failed && k_blocks > 0;
     const int er = run && r < m ? ea[(int64_t)w * m_pad + r] : 0;
     double* crow = c + ((int64_t)w * m + r) * (int64_t)n;
+    const uint32_t lane_addr = tmem + ((uint32_t)(q * 32) << 16);
 #pragma unroll 1
     for (int chunk = 0; chunk < BN / 16; chunk++) {
-      double v[16];
-#pragma unroll
-      for (int j = 0; j < 16; j++) v[j] = 0.0;
+      int32_t acc[S][16];
       if (run) {
 #pragma unroll
-        for (int l = S + 1; l >= 2; l--) {
-          int32_t acc[16];
-          tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((l - 2) * BN + chunk * 16), acc);
-          tmem_wait_ld();
-          const double scale = ldexp(1.0, -8 * l);
-#pragma unroll
-          for (int j = 0; j < 16; j++) v[j] += (double)acc[j] * scale;
-        }
+        for (int l = 0; l < S; l++) tmem_ld16(lane_addr + (uint32_t)(l * BN + chunk * 16), acc[l]);
+        tmem_wait_ld();
       }
       if (run && r < m) {
 #pragma unroll
         for (int j = 0; j < 16; j++) {
           const int col = n0 + chunk * 16 + j;
-          if (col < n) {
-            double x = ldexp(v[j], er + eb[(int64_t)w * n_pad + col]);
-            if (accumulate) x += crow[col];
-            crow[col] = x;
+          if (col >= n) continue;
+          // Levels 2.. S+1 in groups of three, each summed exactly in int64
+          // (|level| < 2^31, so three of them shifted by 8 bits fit in 2^48),
+          // then converted once and added from the smallest group up.
+          double v = 0.0;
+#pragma unroll
+          for (int g = (S - 1) / 3; g >= 0; g--) {
+            long long part = 0;
+            const int l0 = 3 * g, l1 = (3 * g + 3 < S ? 3 * g + 3 : S);
+#pragma unroll
+            for (int l = l0; l < l1; l++) part = part * 256 + (long long)acc[l][j];
+            // part carries levels l0+2 .. l1+1, its last at weight 2^{-8(l1+1)}.
+            v += (double)part * exp2_neg8(l1 + 1);
           }
+          const int e = er + eb[(int64_t)w * n_pad + col];
+          double x = (e > -960 && e < 960) ? v * pow2(e) : ldexp(v, e);
+          if (accumulate) x += crow[col];
+          crow[col] = x;
         }
       }
     }
@@ -294,20 +305,28 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
-// Per row of x [rows][k] (leading dimension ld): the exponent e with
-// max|x| < 2^(e-2), or 0 for a row of zeros; status bit 1 if a value isn't
-// finite. One block per row, rows of `rows_pad` per batch.
-__global__ void row_exponents(const double* __restrict__ x, int64_t batches, int64_t rows, int64_t k, int64_t ld,
-                              int64_t rows_pad, int32_t* __restrict__ e, int* status) {
-  __shared__ double red[32];
+// Slices rows of x [batches][rows][k] (leading dimension ld): for each row,
+// the exponent e with max|x| < 2^(e-2) (0 for a row of zeros), then the S
+// digits of x / 2^e, written to digits[(w·S + s)][r][k] for r < rows_pad and
+// k < k_pad (zeros beyond). One block per row: the second pass over a row
+// reads it from L2. Status bit 1 if a value isn't finite.
+template <int S>
+__global__ void __launch_bounds__(256) slice_rows(const double* __restrict__ x, int64_t batches, int64_t rows,
+                                                  int64_t k, int64_t ld, int64_t rows_pad, int64_t k_pad,
+                                                  int32_t* __restrict__ e_out, int8_t* __restrict__ digits,
+                                                  int* status) {
+  __shared__ double red[8];
+  __shared__ int ex_s;
+  const int64_t slab = rows_pad * k_pad;
   for (int64_t g = blockIdx.x; g < batches * rows_pad; g += gridDim.x) {
     const int64_t w = g / rows_pad, r = g % rows_pad;
+    const double* row = x + (w * rows + r) * ld;
+    const bool live = r < rows;
     double m = 0.0;
     bool bad = false;
-    if (r < rows) {
-      const double* row = x + (w * rows + r) * ld;
+    if (live) {
       for (int64_t i = threadIdx.x; i < k; i += blockDim.x) {
-        double v = fabs(row[i]);
+        const double v = fabs(row[i]);
         bad |= !(v <= 1.7976931348623157e308);
         m = fmax(m, v);
       }
@@ -316,59 +335,45 @@ __global__ void row_exponents(const double* __restrict__ x, int64_t batches, int
     for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
     __syncthreads();
-    if (threadIdx.x < 32) {
-      m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
-      for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-      if (threadIdx.x == 0) {
-        int ex = 0;
-        if (m > 0.0 && m <= 1.7976931348623157e308) {
-          frexp(m, &ex);
-          ex += 2;
+    if (threadIdx.x == 0) {
+      double mm = 0.0;
+      for (int i = 0; i < (int)(blockDim.x >> 5); i++) mm = fmax(mm, red[i]);
+      int ex = 0;
+      if (mm > 0.0 && mm <= 1.7976931348623157e308) {
+        frexp(mm, &ex);
+        ex += 2;
+      }
+      ex_s = ex;
+      e_out[g] = ex;
+    }
+    __syncthreads();
+    const int shift = 8 * S - ex_s;
+    for (int64_t kc = threadIdx.x; kc < k_pad / 16; kc += blockDim.x) {
+      uint32_t word[S][4];
+#pragma unroll
+      for (int s = 0; s < S; s++)
+#pragma unroll
+        for (int qq = 0; qq < 4; qq++) word[s][qq] = 0;
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        const int64_t kk = kc * 16 + j;
+        double v = (live && kk < k) ? row[kk] : 0.0;
+        if (!(fabs(v) <= 1.7976931348623157e308)) v = 0.0;
+        long long X = llrint(ldexp(v, shift));
+#pragma unroll
+        for (int s = S - 1; s >= 0; s--) {
+          const long long d = ((X + 128) & 255) - 128;
+          word[s][j >> 2] |= ((uint32_t)(d & 255)) << (8 * (j & 3));
+          X = (X - d) >> 8;
         }
-        e[g] = ex;
+      }
+#pragma unroll
+      for (int s = 0; s < S; s++) {
+        uint4* dst = (uint4*)(digits + (w * S + s) * slab + r * k_pad + kc * 16);
+        *dst = make_uint4(word[s][0], word[s][1], word[s][2], word[s][3]);
       }
     }
     __syncthreads();
-  }
-}
-
-// The S digits of x / 2^e, 16 values of k per thread, written to
-// digits[(w·S + s)][r][k] for r < rows_pad and k < k_pad (zeros beyond).
-template <int S>
-__global__ void row_digits(const double* __restrict__ x, int64_t batches, int64_t rows, int64_t k, int64_t ld,
-                           int64_t rows_pad, int64_t k_pad, const int32_t* __restrict__ e,
-                           int8_t* __restrict__ digits) {
-  const int64_t chunks = k_pad / 16;
-  const int64_t total = batches * rows_pad * chunks;
-  const int64_t slab = rows_pad * k_pad;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t kc = i % chunks, g = i / chunks;
-    const int64_t w = g / rows_pad, r = g % rows_pad;
-    uint32_t word[S][4];
-#pragma unroll
-    for (int s = 0; s < S; s++)
-#pragma unroll
-      for (int q = 0; q < 4; q++) word[s][q] = 0;
-    const int shift = 8 * S - e[g];
-    const double* row = x + (w * rows + r) * ld;
-#pragma unroll
-    for (int j = 0; j < 16; j++) {
-      const int64_t kk = kc * 16 + j;
-      double v = (r < rows && kk < k) ? row[kk] : 0.0;
-      if (!(fabs(v) <= 1.7976931348623157e308)) v = 0.0;
-      long long X = llrint(ldexp(v, shift));
-#pragma unroll
-      for (int s = S - 1; s >= 0; s--) {
-        const long long d = ((X + 128) & 255) - 128;
-        word[s][j >> 2] |= ((uint32_t)(d & 255)) << (8 * (j & 3));
-        X = (X - d) >> 8;
-      }
-    }
-#pragma unroll
-    for (int s = 0; s < S; s++) {
-      uint4* dst = (uint4*)(digits + (w * S + s) * slab + r * k_pad + kc * 16);
-      *dst = make_uint4(word[s][0], word[s][1], word[s][2], word[s][3]);
-    }
   }
 }
 
@@ -506,16 +511,12 @@ void split_gemm_s(Context& ctx, const double* a, const double* bt, double* c, in
   DeviceBuffer<int32_t> ea((size_t)(batches * m_pad), stream), eb((size_t)(batches * n_pad), stream);
   DeviceBuffer<int> status(1, stream);
   status.zero();
-  row_exponents<<<blocks_for((uint64_t)(batches * m_pad), 1, 148 * 16), 256, 0, stream>>>(
-      a, batches, m, k, k, m_pad, ea.get(), status.get());
-  row_exponents<<<blocks_for((uint64_t)(batches * n_pad), 1, 148 * 16), 256, 0, stream>>>(
-      bt, batches, n, k, k, n_pad, eb.get(), status.get());
-  row_digits<S><<<blocks_for((uint64_t)(batches * m_pad * (k_pad / 16)), 256), 256, 0, stream>>>(
-      a, batches, m, k, k, m_pad, k_pad, ea.get(), da.get());
-  row_digits<S><<<blocks_for((uint64_t)(batches * n_pad * (k_pad / 16)), 256), 256, 0, stream>>>(
-      bt, batches, n, k, k, n_pad, k_pad, eb.get(), db.get());
+  slice_rows<S><<<blocks_for((uint64_t)(batches * m_pad), 1, 148 * 8), 256, 0, stream>>>(
+      a, batches, m, k, k, m_pad, k_pad, ea.get(), da.get(), status.get());
+  slice_rows<S><<<blocks_for((uint64_t)(batches * n_pad), 1, 148 * 8), 256, 0, stream>>>(
+      bt, batches, n, k, k, n_pad, k_pad, eb.get(), db.get(), status.get());
   EF_LAUNCH_CHECK();
-  ctx.kernels += 4;
+  ctx.kernels += 2;
   CUtensorMap ta = digit_map(da.get(), k_pad, m_pad, batches * S, BM, S);
   CUtensorMap tb = digit_map(db.get(), k_pad, n_pad, batches * S, BN, S);
   EF_CUDA(cudaFuncSetAttribute(split_gemm_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::kSmem));
