@@ -91,7 +91,8 @@ class PipelineDesc(ctypes.Structure):
 
 class Relation(ctypes.Structure):
     _fields_ = [("schema", ctypes.POINTER(ArrowSchema)), ("n_batches", ctypes.c_int64),
-                ("batches", ctypes.POINTER(ctypes.POINTER(ArrowArray)))]
+                ("batches", ctypes.POINTER(ctypes.POINTER(ArrowArray))), ("device", ctypes.c_int32),
+                ("pad", ctypes.c_int32)]
 
 
 GROW = ctypes.CFUNCTYPE(ctypes.c_int32, ctypes.c_void_p, ctypes.c_uint64)
@@ -100,7 +101,7 @@ SHRINK = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint64)
 
 class Options(ctypes.Structure):
     _fields_ = [("float_keys", ctypes.c_int32), ("threads", ctypes.c_int32), ("domain_rows", ctypes.c_int32),
-                ("precision", ctypes.c_int32), ("slices", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("precision", ctypes.c_int32), ("slices", ctypes.c_int32), ("result_on_device", ctypes.c_int32),
                 ("budget_ctx", ctypes.c_void_p), ("budget_grow", GROW), ("budget_shrink", SHRINK)]
 
 
@@ -109,6 +110,7 @@ class Result(ctypes.Structure):
                 ("batches", ctypes.POINTER(ArrowArray)), ("schema", ctypes.POINTER(ArrowSchema)),
                 ("tiles_visited", ctypes.c_uint64), ("tiles", ctypes.c_uint64),
                 ("kernels_launched", ctypes.c_uint64), ("device_ms", ctypes.c_double),
+                ("product_ms", ctypes.c_double), ("product_ops", ctypes.c_double),
                 ("message", ctypes.c_char * 480)]
 
 

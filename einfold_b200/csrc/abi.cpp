@@ -1,5 +1,6 @@
 // The extern "C" entry points of include/einfold_b200.h.
 #include <cstring>
+#include <cstdlib>
 #include <mutex>
 
 #include "fold.h"
@@ -31,6 +32,10 @@ int32_t guarded(einfold_context* ctx, einfold_result* result, F&& body) {
   try {
     ef::DeviceGuard dev(c->device);
     c->kernels = 0;
+    c->last_phase = 0;
+    c->phase("call");
+    c->product_ms = 0;
+    c->product_ops = 0;
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
@@ -45,6 +50,8 @@ int32_t guarded(einfold_context* ctx, einfold_result* result, F&& body) {
     if (result) {
       result->device_ms = ms;
       result->kernels_launched = c->kernels;
+      result->product_ms = c->product_ms;
+      result->product_ops = c->product_ops;
     }
   } catch (const ef::Declined& d) {
     status = EINFOLD_DECLINED;
@@ -111,6 +118,7 @@ einfold_context* einfold_context_create(int32_t device) {
   try {
     auto* c = new einfold_context();
     c->device = device;
+    c->tracing = std::getenv("EINFOLD_TRACE") != nullptr;
     ef::DeviceGuard dev(device);
     EF_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     EF_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
@@ -235,13 +243,7 @@ int32_t einfold_split_gemm(einfold_context* ctx, const double* a, const double* 
   einfold_result r;
   return guarded(ctx, &r, [&](ef::Context& cx) -> int32_t {
     cudaStream_t s = stream ? (cudaStream_t)stream : cx.stream;
-    if (b_transposed) {
-      ef::split_gemm(cx, a, b, c, batches, m, n, k, slices ? slices : ef::kDefaultSlices, s);
-    } else {
-      ef::DeviceBuffer<double> bt((size_t)(batches * n * k), s);
-      ef::transpose(b, bt.get(), batches, k, n, s);
-      ef::split_gemm(cx, a, bt.get(), c, batches, m, n, k, slices ? slices : ef::kDefaultSlices, s);
-    }
+    ef::split_gemm(cx, a, b, b_transposed == 0, c, batches, m, n, k, slices ? slices : ef::kDefaultSlices, s);
     return EINFOLD_OK;
   });
 }
@@ -251,12 +253,12 @@ int32_t einfold_fp64_gemm(einfold_context* ctx, const double* a, const double* b
   einfold_result r;
   return guarded(ctx, &r, [&](ef::Context& cx) -> int32_t {
     cudaStream_t s = stream ? (cudaStream_t)stream : cx.stream;
-    if (b_transposed) {
+    if (!b_transposed) {
       ef::fp64_gemm(cx, a, nullptr, b, c, batches, m, n, k, 0, 0, false, s);
     } else {
-      ef::DeviceBuffer<double> bt((size_t)(batches * n * k), s);
-      ef::transpose(b, bt.get(), batches, k, n, s);
-      ef::fp64_gemm(cx, a, nullptr, bt.get(), c, batches, m, n, k, 0, 0, false, s);
+      ef::DeviceBuffer<double> bn((size_t)(batches * n * k), s);
+      ef::transpose(b, bn.get(), batches, n, k, s);
+      ef::fp64_gemm(cx, a, nullptr, bn.get(), c, batches, m, n, k, 0, 0, false, s);
     }
     EF_CUDA(cudaStreamSynchronize(s));
     return EINFOLD_OK;

@@ -64,9 +64,26 @@ const char* format_of(Kind k) {
   }
 }
 
+void Buffer::reset() {
+  if (ptr) {
+    if (device < 0) {
+      std::free(ptr);
+    } else {
+      int old = -1;
+      cudaGetDevice(&old);
+      cudaSetDevice(device);
+      cudaFree(ptr);
+      if (old >= 0) cudaSetDevice(old);
+    }
+  }
+  ptr = nullptr;
+  bytes = 0;
+}
+
 int64_t Column::nulls() const {
   if (!validity) return 0;
   if (null_count >= 0) return null_count;
+  if (device) fail(EINFOLD_INVALID, "a device column must state its null count");
   int64_t n = 0;
   for (int64_t i = 0; i < length; i++) n += !valid(i);
   return n;
@@ -137,6 +154,7 @@ Relation import_relation(const einfold_relation* r) {
   Relation rel;
   if (!r) return rel;
   rel.fields = import_schema(r->schema);
+  rel.device = r->device;
   for (int64_t i = 0; i < r->n_batches; i++) {
     const ArrowArray* b = r->batches[i];
     if (!b || b->n_children != (int64_t)rel.fields.size())
@@ -148,6 +166,7 @@ Relation import_relation(const einfold_relation* r) {
       if (b->children[c]->length < b->offset + b->length)
         fail(EINFOLD_INVALID, "a column shorter than its batch");
       col.length = b->length;
+      col.device = r->device >= 0;
       batch.columns.push_back(col);
     }
     rel.batches.push_back(std::move(batch));
@@ -273,6 +292,7 @@ void release_result(einfold_result* r) {
 }
 
 OutColumn copy_column(const Column& c, const Field& f) {
+  if (c.device) fail(EINFOLD_INVALID, "carrying a device column is not supported");
   OutColumn o;
   o.format = f.format;
   o.nullable = f.nullable;
@@ -282,14 +302,14 @@ OutColumn copy_column(const Column& c, const Field& f) {
   int64_t nulls = c.nulls();
   o.null_count = nulls;
   if (nulls) {
-    o.validity = HostBuffer((size_t)((c.length + 7) / 8));
+    o.validity = Buffer(HostBuffer((size_t)((c.length + 7) / 8)));
     std::memset(o.validity.ptr, 0, o.validity.bytes);
     uint8_t* v = o.validity.as<uint8_t>();
     for (int64_t i = 0; i < c.length; i++)
       if (c.valid(i)) v[i >> 3] |= (uint8_t)(1u << (i & 7));
   }
   if (c.kind == Kind::Bool) {
-    o.values = HostBuffer((size_t)((c.length + 7) / 8));
+    o.values = Buffer(HostBuffer((size_t)((c.length + 7) / 8)));
     std::memset(o.values.ptr, 0, o.values.bytes);
     uint8_t* v = o.values.as<uint8_t>();
     for (int64_t i = 0; i < c.length; i++) {
@@ -300,8 +320,8 @@ OutColumn copy_column(const Column& c, const Field& f) {
     bool large = c.kind == Kind::LargeUtf8 || c.kind == Kind::LargeBinary;
     int64_t total = 0;
     for (int64_t i = 0; i < c.length; i++) { int64_t l; c.bytes(i, &l); total += l; }
-    o.values = HostBuffer((size_t)(c.length + 1) * (large ? 8 : 4));
-    o.data = HostBuffer((size_t)(total ? total : 1));
+    o.values = Buffer(HostBuffer((size_t)(c.length + 1) * (large ? 8 : 4)));
+    o.data = Buffer(HostBuffer((size_t)(total ? total : 1)));
     int64_t pos = 0;
     for (int64_t i = 0; i < c.length; i++) {
       int64_t l;
@@ -315,7 +335,7 @@ OutColumn copy_column(const Column& c, const Field& f) {
     o.null_count = c.length;
   } else {
     int w = width_of(c.kind);
-    o.values = HostBuffer((size_t)(c.length * w));
+    o.values = Buffer(HostBuffer((size_t)(c.length * w)));
     if (c.length) std::memcpy(o.values.ptr, c.values + c.offset * w, (size_t)(c.length * w));
   }
   return o;

@@ -43,6 +43,7 @@ struct Column {
   const uint8_t* data = nullptr;      // var-length bytes
   std::shared_ptr<Column> dictionary; // a dictionary column's values; `values` holds indices
   Kind index_kind = Kind::Other;
+  bool device = false;                // buffers in device memory
 
   bool valid(int64_t i) const {
     if (!validity) return true;
@@ -63,6 +64,7 @@ struct Batch {
 struct Relation {
   std::vector<Field> fields;
   std::vector<Batch> batches;
+  int device = -1;  // -1: host memory; else the CUDA device holding the buffers
   int64_t rows() const {
     int64_t n = 0;
     for (auto& b : batches) n += b.rows;
@@ -92,6 +94,26 @@ struct HostBuffer {
   template <class T> T* as() const { return (T*)ptr; }
 };
 
+// A result buffer: host memory (malloc) or device memory (cudaFree on `device`).
+struct Buffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  int device = -1;
+  Buffer() = default;
+  Buffer(HostBuffer&& h) : ptr(h.ptr), bytes(h.bytes), device(-1) { h.ptr = nullptr; h.bytes = 0; }
+  Buffer(const Buffer&) = delete;
+  Buffer(Buffer&& o) noexcept : ptr(o.ptr), bytes(o.bytes), device(o.device) { o.ptr = nullptr; o.bytes = 0; }
+  Buffer& operator=(Buffer&& o) noexcept {
+    reset();
+    ptr = o.ptr; bytes = o.bytes; device = o.device;
+    o.ptr = nullptr; o.bytes = 0;
+    return *this;
+  }
+  void reset();
+  ~Buffer() { reset(); }
+  template <class T> T* as() const { return (T*)ptr; }
+};
+
 // One column of a result: values, optional validity bitmap, and var-length data.
 struct OutColumn {
   std::string format;
@@ -99,9 +121,9 @@ struct OutColumn {
   bool nullable = true;
   int64_t length = 0;
   int64_t null_count = 0;
-  HostBuffer validity;  // empty when there are no NULLs
-  HostBuffer values;
-  HostBuffer data;      // var-length kinds only
+  Buffer validity;  // empty when there are no NULLs
+  Buffer values;
+  Buffer data;      // var-length kinds only
   Kind kind = Kind::Other;
 };
 

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
@@ -143,11 +144,17 @@ struct PinnedArena {
 };
 
 struct Context {
+  // With EINFOLD_TRACE set, phase() synchronizes the stream and prints the
+  // milliseconds since the previous phase to stderr.
+  bool tracing = false;
+  double last_phase = 0;
+  void phase(const char* name);
   int device = 0;
   cudaStream_t stream = nullptr;
   std::mutex lock;
   int sm_count = 148;
   uint64_t kernels = 0;  // kernels launched by the current call
+  double product_ms = 0, product_ops = 0;  // the split products' kernels in the current call
   PinnedArena pinned;
   // Device-resident scratch kept across calls.
   void* status_word = nullptr;  // int32 status set by bounded device waits
@@ -164,6 +171,17 @@ struct DeviceGuard {
     if (old >= 0) cudaSetDevice(old);
   }
 };
+
+inline double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+inline void Context::phase(const char* name) {
+  if (!tracing) return;
+  cudaStreamSynchronize(stream);
+  double t = now_ms();
+  std::fprintf(stderr, "[einfold] %-28s %9.3f ms\n", name, last_phase ? t - last_phase : 0.0);
+  last_phase = t;
+}
 
 inline unsigned blocks_for(uint64_t n, unsigned threads, unsigned cap = 148u * 32u) {
   uint64_t b = (n + threads - 1) / threads;

@@ -24,16 +24,20 @@ constexpr int64_t kFewCells = 4096;
 constexpr int64_t kZBlock = 4096;
 constexpr int64_t kNoGroup = -1;
 
+// Scatters a's rows into a[x][z]; `held` packs a 2-bit code per cell (0
+// absent, 1 NULL factor, 2 valued), 16 cells a word, so that a repeated
+// position shows in the bits an atomic OR returns.
 __global__ void scatter_a_kernel(Role xs, Role zs, int64_t rows, const double* __restrict__ vals,
                                  const uint8_t* __restrict__ valid, int64_t nz, double* __restrict__ a,
-                                 int32_t* __restrict__ held, uint8_t* __restrict__ reached,
+                                 uint32_t* __restrict__ held, uint8_t* __restrict__ reached,
                                  uint8_t* __restrict__ valued, unsigned* flags) {
   unsigned f = 0;
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
     const int64_t x = role_position(xs, r), z = role_position(zs, r);
     const int64_t p = x * nz + z;
     const bool v = valid ? valid[r] != 0 : true;
-    if (atomicExch(&held[p], v ? 2 : 1) != 0) f |= F_DUP_A;
+    const unsigned sh = (unsigned)(p & 15) * 2;
+    if ((atomicOr(&held[p >> 4], (v ? 2u : 1u) << sh) >> sh) & 3u) f |= F_DUP_A;
     reached[x] = 1;
     if (v) {
       const double val = vals[r];
@@ -45,18 +49,18 @@ __global__ void scatter_a_kernel(Role xs, Role zs, int64_t rows, const double* _
   if (f) atomicOr(flags, f);
 }
 
+// Scatters b's rows into b[w][z][y] (its natural layout: each row of b's
+// matrix contiguous); `present` packs a bit per cell.
 __global__ void scatter_b_kernel(Role wzs, Role ys, int64_t rows, const double* __restrict__ vals,
-                                 const uint8_t* __restrict__ valid, int64_t nz, int64_t ny, double* __restrict__ bt,
-                                 int32_t* __restrict__ present, unsigned* flags) {
+                                 const uint8_t* __restrict__ valid, int64_t ny, double* __restrict__ bm,
+                                 uint32_t* __restrict__ present, unsigned* flags) {
   unsigned f = 0;
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t wz = role_position(wzs, r), y = role_position(ys, r);
-    const int64_t w = wz / nz, z = wz % nz;
-    const int64_t p = (w * ny + y) * nz + z;
-    if (atomicExch(&present[p], 1) != 0) f |= F_DUP_B;
+    const int64_t p = role_position(wzs, r) * ny + role_position(ys, r);
+    if (atomicOr(&present[p >> 5], 1u << (p & 31)) & (1u << (p & 31))) f |= F_DUP_B;
     if (!valid || valid[r]) {
       const double val = vals[r];
-      bt[p] = val;
+      bm[p] = val;
       if (!isfinite(val)) f |= F_NONFINITE_B;
     }
   }
@@ -98,11 +102,21 @@ struct OutKeys {
   void* out[kMaxDims];
 };
 
+// The keys of output dimensions along x (or y), one table per key:
+// table[k][p] = (p / stride) % extent, so that emitting needs no division.
+__global__ void key_tables(int64_t n, OutKeys keys, int in_x, int64_t* __restrict__ tables) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
+    for (int k = 0; k < keys.n; k++)
+      if (keys.key[k].in_x == in_x) tables[(int64_t)k * n + p] = keys.key[k].at(p, p);
+}
+
+// Which cells are output rows: reached x and, with conditions, allowed (x, y).
 __global__ void select_cells(int64_t nx, int64_t ny, const uint8_t* __restrict__ reached, Conds c,
                              uint8_t* __restrict__ sel) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nx * ny; i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t x = i / ny, y = i % ny;
-    sel[i] = reached[x] && (c.n == 0 || c.allowed(x, y));
+  for (int64_t x = blockIdx.y; x < nx; x += gridDim.y) {
+    const bool r = reached[x] != 0;
+    for (int64_t y = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; y < ny; y += (int64_t)gridDim.x * blockDim.x)
+      sel[x * ny + y] = r && c.allowed(x, y);
   }
 }
 
@@ -115,19 +129,29 @@ __device__ __forceinline__ void store_key(void* base, int width, int64_t i, int6
   }
 }
 
-__global__ void emit_cells(int64_t nx, int64_t ny, const uint8_t* __restrict__ sel, const int64_t* __restrict__ pos,
-                           OutKeys keys, const double* __restrict__ out, const uint8_t* __restrict__ valued,
-                           double* __restrict__ val_out, uint8_t* __restrict__ valid_out,
-                           unsigned long long* nulls) {
+// Writes the output rows: cell (x, y) goes to pos[x*ny + y] when `sel` is
+// given (conditions), else to row_index[x]·ny + y for reached x.
+__global__ void emit_cells(int64_t nx, int64_t ny, const uint8_t* __restrict__ reached,
+                           const int64_t* __restrict__ row_index, const uint8_t* __restrict__ sel,
+                           const int64_t* __restrict__ pos, OutKeys keys, const int64_t* __restrict__ xtab,
+                           const int64_t* __restrict__ ytab, const double* __restrict__ out,
+                           const uint8_t* __restrict__ valued, double* __restrict__ val_out,
+                           uint8_t* __restrict__ valid_out, unsigned long long* nulls) {
   unsigned long long local = 0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nx * ny; i += (int64_t)gridDim.x * blockDim.x) {
-    if (!sel[i]) continue;
-    const int64_t x = i / ny, y = i % ny, o = pos[i];
-    for (int k = 0; k < keys.n; k++) store_key(keys.out[k], keys.width[k], o, keys.key[k].at(x, y));
-    val_out[o] = out[i];
+  for (int64_t x = blockIdx.y; x < nx; x += gridDim.y) {
+    if (!reached[x]) continue;
     const uint8_t v = valued[x];
-    valid_out[o] = v;
-    local += !v;
+    const int64_t base = sel ? 0 : row_index[x] * ny;
+    for (int64_t y = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; y < ny; y += (int64_t)gridDim.x * blockDim.x) {
+      const int64_t i = x * ny + y;
+      if (sel && !sel[i]) continue;
+      const int64_t o = sel ? pos[i] : base + y;
+      for (int k = 0; k < keys.n; k++)
+        store_key(keys.out[k], keys.width[k], o, keys.key[k].in_x ? xtab[(int64_t)k * nx + x] : ytab[(int64_t)k * ny + y]);
+      val_out[o] = out[i];
+      valid_out[o] = v;
+      local += !v;
+    }
   }
   if (local) atomicAdd(nulls, local);
 }
@@ -184,7 +208,9 @@ __global__ void domain_values(int64_t rows, const int64_t* __restrict__ cell, in
 
 // Keys of every batch of `r` for `op`, staged as int64, with extents.
 struct StagedKeys {
-  std::vector<DeviceBuffer<int64_t>> keys;  // per key of the operand, in op.keys order
+  std::vector<DeviceColumn> cols;           // staged columns (int64 ones read in place)
+  std::vector<DeviceBuffer<int64_t>> wide;  // other integer columns widened to int64
+  std::vector<const int64_t*> keys;         // per key of the operand, in op.keys order
   std::vector<int64_t> extent;              // per key
 };
 
@@ -196,9 +222,16 @@ StagedKeys stage_keys(Context& ctx, const OperandD& op, const Relation& r) {
     if (f.dictionary || !is_integer(f.kind)) decline("a key column that isn't integers");
     for (auto& b : r.batches)
       if (b.columns[k.col].nulls() > 0) decline("a NULL key");
-    DeviceColumn c = stage_column(ctx, r, k.col, false);
+    s.cols.push_back(stage_column(ctx, r, k.col, false));
+    DeviceColumn& c = s.cols.back();
     KeyStats st;
-    s.keys.push_back(keys_as_i64(ctx, c, &st));
+    if (c.kind == Kind::Int64) {
+      key_stats_i64(ctx, (const int64_t*)c.ptr(), c.rows, &st);
+      s.keys.push_back((const int64_t*)c.ptr());
+    } else {
+      s.wide.push_back(keys_as_i64(ctx, c, &st));
+      s.keys.push_back(s.wide.back().get());
+    }
     if (st.negative || st.too_large) decline("a negative key, or one too large for int64");
     if (st.max == INT64_MAX) decline("a key whose extent doesn't fit");
     s.extent.push_back(st.max + 1);
@@ -213,7 +246,7 @@ Role role_of(const std::vector<int>& dims, const OperandD& op, const StagedKeys&
     int slot = -1;
     for (size_t i = 0; i < op.keys.size(); i++)
       if (op.keys[i].dim == d) slot = (int)i;
-    r.keys[r.n] = s.keys[slot].get();
+    r.keys[r.n] = s.keys[slot];
     r.extent[r.n] = extent[d];
     r.n++;
   }
@@ -267,7 +300,9 @@ FoldOutput dense_fold(Context& ctx, const FoldD& f, const Relation& a, const Rel
   const uint64_t ra = (uint64_t)a.rows(), rb = (uint64_t)b.rows();
   budget.reserve(sat_mul(sat_add(sat_mul(ra, op_a.keys.size()), sat_mul(rb, op_b.keys.size())), 8),
                  "the dense algorithm's keys");
+  ctx.phase("dense: checks");
   StagedKeys ka = stage_keys(ctx, op_a, a), kb = stage_keys(ctx, op_b, b);
+  ctx.phase("dense: keys");
   std::vector<int64_t> extent(f.n_dims(), 0);
   for (size_t i = 0; i < op_a.keys.size(); i++) extent[op_a.keys[i].dim] = std::max(extent[op_a.keys[i].dim], ka.extent[i]);
   for (size_t i = 0; i < op_b.keys.size(); i++) extent[op_b.keys[i].dim] = std::max(extent[op_b.keys[i].dim], kb.extent[i]);
@@ -299,27 +334,34 @@ FoldOutput dense_fold(Context& ctx, const FoldD& f, const Relation& a, const Rel
   if (a.fields[op_a.factor].kind != Kind::Float64 || a.fields[op_a.factor].dictionary) decline("factors that aren't Float64");
   if (b.fields[op_b.factor].kind != Kind::Float64 || b.fields[op_b.factor].dictionary) decline("factors that aren't Float64");
   DeviceColumn fa = stage_column(ctx, a, op_a.factor), fb = stage_column(ctx, b, op_b.factor);
+  ctx.phase("dense: factors staged");
 
-  DeviceBuffer<double> am(na, s), btm(nb, s), out(nx * ny, s);
-  DeviceBuffer<int32_t> held(na, s), present(nb, s);
+  DeviceBuffer<double> am(na, s), bm(nb, s), out(nx * ny, s);
+  DeviceBuffer<uint32_t> held((na + 15) / 16, s), present((nb + 31) / 32, s);
   DeviceBuffer<uint8_t> reached(nx, s), valued(nx, s);
   DeviceBuffer<unsigned> flags(1, s);
-  am.zero(); btm.zero(); held.zero(); present.zero(); reached.zero(); valued.zero(); flags.zero();
+  // Cells no row writes must read as 0: only incomplete operands or NULL
+  // factors leave any (a repeated row declines below).
+  if (ra < na || fa.nulls > 0) am.zero();
+  if (rb < nb || fb.nulls > 0) bm.zero();
+  held.zero(); present.zero(); reached.zero(); valued.zero(); flags.zero();
+  ctx.phase("dense: matrices allocated");
   Role rxs = role_of(xs, op_a, ka, extent), rzs = role_of(zs, op_a, ka, extent);
   Role rwzs = role_of(wzs, op_b, kb, extent), rys = role_of(ys, op_b, kb, extent);
   if (ra) {
-    scatter_a_kernel<<<blocks_for(ra, 256), 256, 0, s>>>(rxs, rzs, (int64_t)ra, (const double*)fa.data.get(),
+    scatter_a_kernel<<<blocks_for(ra, 256), 256, 0, s>>>(rxs, rzs, (int64_t)ra, (const double*)fa.ptr(),
                                                          fa.valid.get(), (int64_t)nz, am.get(), held.get(),
                                                          reached.get(), valued.get(), flags.get());
     ctx.kernels++;
   }
   if (rb) {
-    scatter_b_kernel<<<blocks_for(rb, 256), 256, 0, s>>>(rwzs, rys, (int64_t)rb, (const double*)fb.data.get(),
-                                                         fb.valid.get(), (int64_t)nz, (int64_t)ny, btm.get(),
-                                                         present.get(), flags.get());
+    scatter_b_kernel<<<blocks_for(rb, 256), 256, 0, s>>>(rwzs, rys, (int64_t)rb, (const double*)fb.ptr(),
+                                                         fb.valid.get(), (int64_t)ny, bm.get(), present.get(),
+                                                         flags.get());
     ctx.kernels++;
   }
   EF_LAUNCH_CHECK();
+  ctx.phase("dense: scatter");
   unsigned fl = 0;
   EF_CUDA(cudaMemcpyAsync(&fl, flags.get(), 4, cudaMemcpyDeviceToHost, s));
   EF_CUDA(cudaStreamSynchronize(s));
@@ -404,20 +446,22 @@ FoldOutput dense_fold(Context& ctx, const FoldD& f, const Relation& a, const Rel
   const bool split = o.precision == 0 && finite && !(fl & F_NONFINITE_B);
   if (nx && ny) {
     if (split) {
-      split_gemm(ctx, am.get(), btm.get(), out.get(), (int64_t)nw, (int64_t)per_batch, (int64_t)ny, (int64_t)nz,
-                 o.slices ? o.slices : kDefaultSlices, s);
+      split_gemm(ctx, am.get(), bm.get(), true, out.get(), (int64_t)nw, (int64_t)per_batch, (int64_t)ny,
+                 (int64_t)nz, o.slices ? o.slices : kDefaultSlices, s);
     } else {
-      fp64_gemm(ctx, am.get(), held.get(), btm.get(), out.get(), (int64_t)nw, (int64_t)per_batch, (int64_t)ny,
+      fp64_gemm(ctx, am.get(), held.get(), bm.get(), out.get(), (int64_t)nw, (int64_t)per_batch, (int64_t)ny,
                 (int64_t)nz, 0, (int64_t)(nx * ny >= (uint64_t)kFewCells ? 0 : kZBlock), false, s);
     }
   }
+  ctx.phase("dense: product");
   am.reset();
-  btm.reset();
+  bm.reset();
   held.reset();
 
   FoldOutput result;
   result.algorithm = EINFOLD_ALG_DENSE;
   if (f.domain && domain) {
+    if (o.result_on_device) fail(EINFOLD_INVALID, "results in device memory are not supported with a domain");
     const DomainD& spec = *f.domain;
     DeviceBuffer<double> val((size_t)(nd ? nd : 1), s);
     DeviceBuffer<uint8_t> valid((size_t)(nd ? nd : 1), s);
@@ -445,13 +489,13 @@ FoldOutput dense_fold(Context& ctx, const FoldD& f, const Relation& a, const Rel
       v.kind = Kind::Float64;
       v.name = schema.back().name;
       v.length = batch.rows;
-      v.values = HostBuffer((size_t)batch.rows * 8);
+      v.values = Buffer(HostBuffer((size_t)batch.rows * 8));
       if (batch.rows) std::memcpy(v.values.ptr, hv.as<double>() + off, (size_t)batch.rows * 8);
       int64_t nulls = 0;
       for (int64_t i = 0; i < batch.rows; i++) nulls += !hvalid.as<uint8_t>()[off + i];
       v.null_count = nulls;
       if (nulls) {
-        v.validity = HostBuffer((size_t)(batch.rows + 7) / 8);
+        v.validity = Buffer(HostBuffer((size_t)(batch.rows + 7) / 8));
         std::memset(v.validity.ptr, 0, v.validity.bytes);
         for (int64_t i = 0; i < batch.rows; i++)
           if (hvalid.as<uint8_t>()[off + i]) v.validity.as<uint8_t>()[i >> 3] |= (uint8_t)(1u << (i & 7));
@@ -467,32 +511,49 @@ FoldOutput dense_fold(Context& ctx, const FoldD& f, const Relation& a, const Rel
   // Output rows (dense.rs:516-575): (x, y) for each reached x, in order, every
   // y, minus the groups the conditions disallow.
   const int64_t cells_n = (int64_t)(nx * ny);
-  DeviceBuffer<uint8_t> sel((size_t)(cells_n ? cells_n : 1), s);
-  DeviceBuffer<int64_t> pos((size_t)(cells_n ? cells_n : 1), s);
-  if (cells_n) {
-    select_cells<<<blocks_for(cells_n, 256), 256, 0, s>>>((int64_t)nx, (int64_t)ny, reached.get(), conds, sel.get());
-    ctx.kernels++;
-    EF_LAUNCH_CHECK();
-  }
-  const int64_t n_out = exclusive_scan_flags(ctx, sel.get(), cells_n, pos.get());
   OutKeys ok;
-  std::vector<DeviceBuffer<uint8_t>> key_dev;
   if (f.outputs.size() > (size_t)kMaxDims) decline("more than 8 outputs");
   for (size_t i = 0; i < f.outputs.size(); i++) {
-    int width = width_of(schema[i].kind);
-    key_dev.emplace_back((size_t)(n_out ? n_out * width : 1), s);
     ok.key[ok.n] = key_at(f.outputs[i].dim);
-    ok.width[ok.n] = width;
-    ok.out[ok.n] = key_dev.back().get();
+    ok.width[ok.n] = width_of(schema[i].kind);
     ok.n++;
+  }
+  DeviceBuffer<int64_t> xtab((size_t)(ok.n * nx ? ok.n * nx : 1), s), ytab((size_t)(ok.n * ny ? ok.n * ny : 1), s);
+  if (nx) key_tables<<<blocks_for(nx, 256), 256, 0, s>>>((int64_t)nx, ok, 1, xtab.get());
+  if (ny) key_tables<<<blocks_for(ny, 256), 256, 0, s>>>((int64_t)ny, ok, 0, ytab.get());
+  ctx.kernels += 2;
+  DeviceBuffer<uint8_t> sel;
+  DeviceBuffer<int64_t> pos, row_index;
+  const dim3 grid2((unsigned)std::max<uint64_t>(1, std::min<uint64_t>((ny + 255) / 256, 64)),
+                   (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(nx, 65535)));
+  int64_t n_out;
+  if (conds.n) {
+    sel.allocate((size_t)(cells_n ? cells_n : 1), s);
+    pos.allocate((size_t)(cells_n ? cells_n : 1), s);
+    if (cells_n) {
+      select_cells<<<grid2, 256, 0, s>>>((int64_t)nx, (int64_t)ny, reached.get(), conds, sel.get());
+      ctx.kernels++;
+      EF_LAUNCH_CHECK();
+    }
+    n_out = exclusive_scan_flags(ctx, sel.get(), cells_n, pos.get());
+  } else {
+    row_index.allocate((size_t)(nx ? nx : 1), s);
+    n_out = exclusive_scan_flags(ctx, reached.get(), (int64_t)nx, row_index.get()) * (int64_t)ny;
+  }
+  ctx.phase("dense: select");
+  std::vector<DeviceBuffer<uint8_t>> key_dev;
+  for (int i = 0; i < ok.n; i++) {
+    key_dev.emplace_back((size_t)(n_out ? n_out * ok.width[i] : 1), s);
+    ok.out[i] = key_dev.back().get();
   }
   DeviceBuffer<double> vals((size_t)(n_out ? n_out : 1), s);
   DeviceBuffer<uint8_t> vvalid((size_t)(n_out ? n_out : 1), s);
   DeviceBuffer<unsigned long long> nulls(1, s);
   nulls.zero();
-  if (cells_n) {
-    emit_cells<<<blocks_for(cells_n, 256), 256, 0, s>>>((int64_t)nx, (int64_t)ny, sel.get(), pos.get(), ok, out.get(),
-                                                        valued.get(), vals.get(), vvalid.get(), nulls.get());
+  if (cells_n && n_out) {
+    emit_cells<<<grid2, 256, 0, s>>>((int64_t)nx, (int64_t)ny, reached.get(), row_index.get(), sel.get(), pos.get(), ok,
+                                     xtab.get(), ytab.get(), out.get(), valued.get(), vals.get(), vvalid.get(),
+                                     nulls.get());
     ctx.kernels++;
     EF_LAUNCH_CHECK();
   }
@@ -508,7 +569,7 @@ FoldOutput dense_fold(Context& ctx, const FoldD& f, const Relation& a, const Rel
     c.kind = schema[i].kind;
     c.nullable = schema[i].nullable;
     c.length = n_out;
-    c.values = to_host(ctx, key_dev[i].get(), (size_t)(n_out * width_of(schema[i].kind)));
+    c.values = result_buffer(ctx, key_dev[i], (size_t)(n_out * ok.width[i]), o.result_on_device);
     ob.columns.push_back(std::move(c));
   }
   OutColumn v;
@@ -516,15 +577,17 @@ FoldOutput dense_fold(Context& ctx, const FoldD& f, const Relation& a, const Rel
   v.kind = Kind::Float64;
   v.name = schema.back().name;
   v.length = n_out;
-  v.values = to_host(ctx, vals.get(), (size_t)n_out * 8);
+  v.values = result_buffer(ctx, vals, (size_t)n_out * 8, o.result_on_device);
   v.null_count = (int64_t)n_nulls;
   if (n_nulls) {
     DeviceBuffer<uint8_t> bits((size_t)((n_out + 7) / 8), s);
     pack_bits(ctx, vvalid.get(), n_out, bits.get());
-    v.validity = to_host(ctx, bits.get(), (size_t)((n_out + 7) / 8));
+    v.validity = result_buffer(ctx, bits, (size_t)((n_out + 7) / 8), o.result_on_device);
   }
+  EF_CUDA(cudaStreamSynchronize(s));
   ob.columns.push_back(std::move(v));
   result.batches.push_back(std::move(ob));
+  ctx.phase("dense: result");
   return result;
 }
 

@@ -20,6 +20,7 @@
 #include <cudaTypedefs.h>
 
 #include <mutex>
+#include <type_traits>
 
 #include "gemm.cuh"
 
@@ -348,39 +349,116 @@ __global__ void __launch_bounds__(256) slice_rows(const double* __restrict__ x, 
     }
     __syncthreads();
     const int shift = 8 * S - ex_s;
-    for (int64_t kc = threadIdx.x; kc < k_pad / 16; kc += blockDim.x) {
-      uint32_t word[S][4];
+    // Four consecutive values per thread: a warp reads 1 KB of the row and
+    // writes 128 contiguous bytes of each digit plane.
+    for (int64_t q4 = threadIdx.x; q4 < k_pad / 4; q4 += blockDim.x) {
+      uint32_t word[S];
 #pragma unroll
-      for (int s = 0; s < S; s++)
+      for (int s = 0; s < S; s++) word[s] = 0;
 #pragma unroll
-        for (int qq = 0; qq < 4; qq++) word[s][qq] = 0;
-#pragma unroll
-      for (int j = 0; j < 16; j++) {
-        const int64_t kk = kc * 16 + j;
+      for (int j = 0; j < 4; j++) {
+        const int64_t kk = q4 * 4 + j;
         double v = (live && kk < k) ? row[kk] : 0.0;
         if (!(fabs(v) <= 1.7976931348623157e308)) v = 0.0;
         long long X = llrint(ldexp(v, shift));
 #pragma unroll
         for (int s = S - 1; s >= 0; s--) {
           const long long d = ((X + 128) & 255) - 128;
-          word[s][j >> 2] |= ((uint32_t)(d & 255)) << (8 * (j & 3));
+          word[s] |= ((uint32_t)(d & 255)) << (8 * j);
           X = (X - d) >> 8;
         }
       }
 #pragma unroll
-      for (int s = 0; s < S; s++) {
-        uint4* dst = (uint4*)(digits + (w * S + s) * slab + r * k_pad + kc * 16);
-        *dst = make_uint4(word[s][0], word[s][1], word[s][2], word[s][3]);
-      }
+      for (int s = 0; s < S; s++)
+        *(uint32_t*)(digits + (w * S + s) * slab + r * k_pad + q4 * 4) = word[s];
     }
     __syncthreads();
   }
 }
 
+// The largest magnitude of each column of x [batches][k][n] (row-major):
+// blocks of rows reduce apart and combine with an atomic max on the bits
+// (non-negative doubles order as their bits). Status bit 1 if a value isn't
+// finite. `colmax` must start at zero.
+__global__ void col_max(const double* __restrict__ x, int64_t batches, int64_t k, int64_t n,
+                        unsigned long long* __restrict__ colmax, int* status) {
+  const int64_t col = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t w = blockIdx.z;
+  const int64_t rows_per = (k + gridDim.y - 1) / gridDim.y;
+  const int64_t r0 = (int64_t)blockIdx.y * rows_per, r1 = min(k, r0 + rows_per);
+  if (col >= n) return;
+  double m = 0.0;
+  bool bad = false;
+  const double* p = x + w * k * n + col;
+  for (int64_t r = r0; r < r1; r++) {
+    const double v = fabs(p[r * n]);
+    bad |= !(v <= 1.7976931348623157e308);
+    m = fmax(m, v);
+  }
+  if (bad) atomicOr(status, 1);
+  if (m > 0.0) atomicMax(&colmax[w * n + col], (unsigned long long)__double_as_longlong(m));
+}
+
+// The S digits of each column of x [batches][k][n] under its column's
+// exponent, written K-major: digits[(w·S + s)][col][kk] for col < n_pad and
+// kk < k_pad. A 64 x 64 tile is staged in shared memory, read along n and
+// cut along k; each thread cuts 16 values of k of one column.
+template <int S>
+__global__ void __launch_bounds__(256) col_digits(const double* __restrict__ x, int64_t k, int64_t n, int64_t n_pad,
+                                                  int64_t k_pad, const unsigned long long* __restrict__ colmax,
+                                                  int32_t* __restrict__ e_out, int8_t* __restrict__ digits) {
+  __shared__ double tile[64][65];
+  const int64_t w = blockIdx.z;
+  const int64_t k0 = (int64_t)blockIdx.y * 64, n0 = (int64_t)blockIdx.x * 64;
+  const double* X = x + w * k * n;
+  for (int i = threadIdx.x; i < 64 * 64; i += 256) {
+    const int kr = i / 64, nc = i % 64;
+    const int64_t gk = k0 + kr, gn = n0 + nc;
+    double v = (gk < k && gn < n) ? X[gk * n + gn] : 0.0;
+    if (!(fabs(v) <= 1.7976931348623157e308)) v = 0.0;
+    tile[kr][nc] = v;
+  }
+  __syncthreads();
+  const int nl = threadIdx.x / 4, kc = threadIdx.x % 4;
+  const int64_t col = n0 + nl;
+  if (col >= n_pad) return;
+  int ex = 0;
+  if (col < n) {
+    const double mm = __longlong_as_double((long long)colmax[w * n + col]);
+    if (mm > 0.0) {
+      frexp(mm, &ex);
+      ex += 2;
+    }
+  }
+  if (blockIdx.y == 0 && kc == 0) e_out[w * n_pad + col] = ex;
+  const int shift = 8 * S - ex;
+  uint32_t word[S][4];
+#pragma unroll
+  for (int s = 0; s < S; s++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) word[s][q] = 0;
+#pragma unroll
+  for (int j = 0; j < 16; j++) {
+    long long X2 = llrint(ldexp(tile[kc * 16 + j][nl], shift));
+#pragma unroll
+    for (int s = S - 1; s >= 0; s--) {
+      const long long d = ((X2 + 128) & 255) - 128;
+      word[s][j >> 2] |= ((uint32_t)(d & 255)) << (8 * (j & 3));
+      X2 = (X2 - d) >> 8;
+    }
+  }
+  const int64_t slab = n_pad * k_pad;
+#pragma unroll
+  for (int s = 0; s < S; s++) {
+    uint4* dst = (uint4*)(digits + (w * S + s) * slab + col * k_pad + k0 + kc * 16);
+    *dst = make_uint4(word[s][0], word[s][1], word[s][2], word[s][3]);
+  }
+}
+
 // FP64 product in k order. 64x64 tiles, 256 threads, 4x4 cells each.
 template <bool FMA>
-__global__ void __launch_bounds__(256) fp64_gemm_kernel(const double* __restrict__ a, const int32_t* __restrict__ held,
-                                                        const double* __restrict__ bt, double* __restrict__ c,
+__global__ void __launch_bounds__(256) fp64_gemm_kernel(const double* __restrict__ a, const uint32_t* __restrict__ held,
+                                                        const double* __restrict__ b, double* __restrict__ c,
                                                         int64_t m, int64_t n, int64_t k, int64_t zblock) {
   constexpr int T = 64, KT = 16;
   __shared__ double As[KT][T + 1];
@@ -388,8 +466,7 @@ __global__ void __launch_bounds__(256) fp64_gemm_kernel(const double* __restrict
   __shared__ uint8_t Hs[KT][T + 4];
   const int64_t w = blockIdx.z;
   const double* A = a + w * m * k;
-  const int32_t* H = held ? held + w * m * k : nullptr;
-  const double* B = bt + w * n * k;
+  const double* B = b + w * k * n;
   double* C = c + w * m * n;
   const int64_t r0 = (int64_t)blockIdx.y * T, c0 = (int64_t)blockIdx.x * T;
   const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
@@ -404,9 +481,14 @@ __global__ void __launch_bounds__(256) fp64_gemm_kernel(const double* __restrict
       const int64_t gr = r0 + row, gk = k0 + kk;
       const bool in = gr < m && gk < k;
       As[kk][row] = in ? A[gr * k + gk] : 0.0;
-      Hs[kk][row] = in ? (H ? (uint8_t)(H[gr * k + gk] == 2) : (uint8_t)1) : (uint8_t)0;
-      const int64_t gc = c0 + row;
-      Bs[kk][row] = (gc < n && gk < k) ? B[gc * k + gk] : 0.0;
+      const int64_t cell = (w * m + gr) * k + gk;
+      Hs[kk][row] = in ? (held ? (uint8_t)(((held[cell >> 4] >> ((cell & 15) * 2)) & 3) == 2) : (uint8_t)1)
+                       : (uint8_t)0;
+    }
+    for (int idx = threadIdx.x; idx < T * KT; idx += 256) {
+      const int kk = idx / T, col = idx % T;
+      const int64_t gc = c0 + col, gk = k0 + kk;
+      Bs[kk][col] = (gc < n && gk < k) ? B[gk * n + gc] : 0.0;
     }
     __syncthreads();
     const int kt = (int)((k - k0) < KT ? (k - k0) : KT);
@@ -501,76 +583,163 @@ CUtensorMap digit_map(const int8_t* digits, int64_t k_pad, int64_t rows, int64_t
 
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
+// Scratch the split product needs beyond its inputs and output.
+struct SplitScratch {
+  int8_t* da;                   // A's digits [batches·S][m_pad][k_pad]
+  int8_t* db;                   // B's digits [batches·S][n_pad][k_pad]
+  int32_t* ea;                  // A's row exponents [batches][m_pad]
+  int32_t* eb;                  // B's column exponents [batches][n_pad]
+  unsigned long long* colmax;   // B's column maxima [batches][n] (natural B only)
+  int* status;
+};
+
+struct SplitDims {
+  int64_t m_pad, n_pad, k_pad;
+};
+
+SplitDims split_dims(int64_t m, int64_t n, int64_t k) {
+  return {round_up(m, BM), round_up(n, BN), round_up(k > 0 ? k : 1, BK)};
+}
+
+// Bytes of each scratch array, 256-byte aligned, in SplitScratch order.
+void split_scratch_sizes(int S, int64_t batches, int64_t m, int64_t n, int64_t k, size_t sz[6]) {
+  SplitDims d = split_dims(m, n, k);
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  sz[0] = al((size_t)(batches * S * d.m_pad * d.k_pad));
+  sz[1] = al((size_t)(batches * S * d.n_pad * d.k_pad));
+  sz[2] = al((size_t)(batches * d.m_pad) * 4);
+  sz[3] = al((size_t)(batches * d.n_pad) * 4);
+  sz[4] = al((size_t)(batches * n) * 8);
+  sz[5] = 256;
+}
+
+// The product with scratch already in place: slices both operands, runs the
+// tensor-core kernel over k in chunks, and returns the status word. Allocates
+// nothing. `timed` records CUDA events around the product kernels.
 template <int S>
-void split_gemm_s(Context& ctx, const double* a, const double* bt, double* c, int64_t batches, int64_t m,
-                  int64_t n, int64_t k, cudaStream_t stream) {
+int split_run(Context& ctx, const double* a, const double* b, bool b_natural, double* c, int64_t batches, int64_t m,
+              int64_t n, int64_t k, const SplitScratch& sc, cudaStream_t stream, bool timed) {
   using Sh = SplitShape<S>;
-  const int64_t m_pad = round_up(m, BM), n_pad = round_up(n, BN), k_pad = round_up(k > 0 ? k : 1, BK);
-  DeviceBuffer<int8_t> da((size_t)(batches * S * m_pad * k_pad), stream);
-  DeviceBuffer<int8_t> db((size_t)(batches * S * n_pad * k_pad), stream);
-  DeviceBuffer<int32_t> ea((size_t)(batches * m_pad), stream), eb((size_t)(batches * n_pad), stream);
-  DeviceBuffer<int> status(1, stream);
-  status.zero();
+  const SplitDims d = split_dims(m, n, k);
+  const int64_t m_pad = d.m_pad, n_pad = d.n_pad, k_pad = d.k_pad;
+  EF_CUDA(cudaMemsetAsync(sc.status, 0, sizeof(int), stream));
   slice_rows<S><<<blocks_for((uint64_t)(batches * m_pad), 1, 148 * 8), 256, 0, stream>>>(
-      a, batches, m, k, k, m_pad, k_pad, ea.get(), da.get(), status.get());
-  slice_rows<S><<<blocks_for((uint64_t)(batches * n_pad), 1, 148 * 8), 256, 0, stream>>>(
-      bt, batches, n, k, k, n_pad, k_pad, eb.get(), db.get(), status.get());
+      a, batches, m, k, k, m_pad, k_pad, sc.ea, sc.da, sc.status);
+  if (b_natural) {
+    EF_CUDA(cudaMemsetAsync(sc.colmax, 0, (size_t)(batches * n) * 8, stream));
+    const unsigned splits = (unsigned)std::min<int64_t>(64, (k + 127) / 128);
+    col_max<<<dim3((unsigned)((n + 255) / 256), splits, (unsigned)batches), 256, 0, stream>>>(b, batches, k, n,
+                                                                                             sc.colmax, sc.status);
+    col_digits<S><<<dim3((unsigned)(n_pad / 64), (unsigned)(k_pad / 64), (unsigned)batches), 256, 0, stream>>>(
+        b, k, n, n_pad, k_pad, sc.colmax, sc.eb, sc.db);
+    ctx.kernels += 2;
+  } else {
+    slice_rows<S><<<blocks_for((uint64_t)(batches * n_pad), 1, 148 * 8), 256, 0, stream>>>(
+        b, batches, n, k, k, n_pad, k_pad, sc.eb, sc.db, sc.status);
+    ctx.kernels++;
+  }
   EF_LAUNCH_CHECK();
-  ctx.kernels += 2;
-  CUtensorMap ta = digit_map(da.get(), k_pad, m_pad, batches * S, BM, S);
-  CUtensorMap tb = digit_map(db.get(), k_pad, n_pad, batches * S, BN, S);
+  ctx.kernels++;
+  ctx.phase("split: sliced");
+  CUtensorMap ta = digit_map(sc.da, k_pad, m_pad, batches * S, BM, S);
+  CUtensorMap tb = digit_map(sc.db, k_pad, n_pad, batches * S, BN, S);
   EF_CUDA(cudaFuncSetAttribute(split_gemm_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::kSmem));
   // Each level's int32 sum is exact while S·kc·2^14 < 2^31: long k runs in
   // chunks whose FP64 results are added.
   const int64_t k_blocks = k_pad / BK;
   const int64_t chunk_blocks = ((int64_t)1 << 31) / ((int64_t)S << 14) / BK;
   const int tiles_m = (int)(m_pad / BM), tiles_n = (int)(n_pad / BN);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (timed) {
+    EF_CUDA(cudaEventCreate(&e0));
+    EF_CUDA(cudaEventCreate(&e1));
+    EF_CUDA(cudaEventRecord(e0, stream));
+  }
   for (int64_t kb0 = 0; kb0 < k_blocks; kb0 += chunk_blocks) {
     const int kbs = (int)std::min<int64_t>(chunk_blocks, k_blocks - kb0);
     dim3 grid((unsigned)(tiles_m * tiles_n), (unsigned)batches);
-    split_gemm_kernel<S><<<grid, kThreads, Sh::kSmem, stream>>>(ta, tb, ea.get(), eb.get(), c, (int)m, (int)n,
-                                                                 (int)m_pad, (int)n_pad, (int)kb0, kbs, tiles_m,
-                                                                 tiles_n, kb0 > 0 ? 1 : 0, status.get());
+    split_gemm_kernel<S><<<grid, kThreads, Sh::kSmem, stream>>>(ta, tb, sc.ea, sc.eb, c, (int)m, (int)n, (int)m_pad,
+                                                                 (int)n_pad, (int)kb0, kbs, tiles_m, tiles_n,
+                                                                 kb0 > 0 ? 1 : 0, sc.status);
     EF_LAUNCH_CHECK();
     ctx.kernels++;
   }
+  if (timed) EF_CUDA(cudaEventRecord(e1, stream));
   int st = 0;
-  EF_CUDA(cudaMemcpyAsync(&st, status.get(), sizeof(int), cudaMemcpyDeviceToHost, stream));
+  EF_CUDA(cudaMemcpyAsync(&st, sc.status, sizeof(int), cudaMemcpyDeviceToHost, stream));
   EF_CUDA(cudaStreamSynchronize(stream));
+  if (timed) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // Digit products executed: S(S+1)/2 pairs of an (m_pad x k_pad) by
+    // (k_pad x n_pad) int8 product, 2 ops per multiply-add.
+    ctx.product_ms += ms;
+    ctx.product_ops += 2.0 * (double)batches * (double)m_pad * (double)n_pad * (double)k_pad * (S * (S + 1) / 2);
+  }
+  return st;
+}
+
+void check_status(int st) {
   if (st & 1) fail(EINFOLD_INVALID, "the split product was given a value that isn't finite");
   if (st & 2) fail(EINFOLD_TIMEOUT, "a bounded wait in the split product ran out");
 }
 
+template <int S>
+void split_gemm_s(Context& ctx, const double* a, const double* b, bool b_natural, double* c, int64_t batches,
+                  int64_t m, int64_t n, int64_t k, cudaStream_t stream) {
+  size_t sz[6];
+  split_scratch_sizes(S, batches, m, n, k, sz);
+  size_t total = 0;
+  for (size_t x : sz) total += x;
+  DeviceBuffer<uint8_t> scratch(total, stream);
+  uint8_t* p = scratch.get();
+  SplitScratch sc;
+  sc.da = (int8_t*)p; p += sz[0];
+  sc.db = (int8_t*)p; p += sz[1];
+  sc.ea = (int32_t*)p; p += sz[2];
+  sc.eb = (int32_t*)p; p += sz[3];
+  sc.colmax = (unsigned long long*)p; p += sz[4];
+  sc.status = (int*)p;
+  check_status(split_run<S>(ctx, a, b, b_natural, c, batches, m, n, k, sc, stream, true));
+}
+
+template <class F>
+void dispatch_slices(int slices, F&& f) {
+  switch (slices) {
+    case 2: f(std::integral_constant<int, 2>()); break;
+    case 3: f(std::integral_constant<int, 3>()); break;
+    case 4: f(std::integral_constant<int, 4>()); break;
+    case 5: f(std::integral_constant<int, 5>()); break;
+    case 6: f(std::integral_constant<int, 6>()); break;
+    case 7: f(std::integral_constant<int, 7>()); break;
+    default: fail(EINFOLD_INVALID, "slices must be 2 to 7, not %d", slices);
+  }
+}
+
 }  // namespace
 
-void split_gemm(Context& ctx, const double* a, const double* bt, double* c, int64_t batches, int64_t m, int64_t n,
-                int64_t k, int slices, cudaStream_t stream) {
+void split_gemm(Context& ctx, const double* a, const double* b, bool b_natural, double* c, int64_t batches,
+                int64_t m, int64_t n, int64_t k, int slices, cudaStream_t stream) {
   if (batches <= 0 || m <= 0 || n <= 0) return;
   if (m > INT32_MAX / 2 || n > INT32_MAX / 2 || batches > 65535) fail(EINFOLD_INVALID, "a product too large");
   if (k <= 0) {
     EF_CUDA(cudaMemsetAsync(c, 0, (size_t)(batches * m * n) * sizeof(double), stream));
     return;
   }
-  switch (slices) {
-    case 2: split_gemm_s<2>(ctx, a, bt, c, batches, m, n, k, stream); break;
-    case 3: split_gemm_s<3>(ctx, a, bt, c, batches, m, n, k, stream); break;
-    case 4: split_gemm_s<4>(ctx, a, bt, c, batches, m, n, k, stream); break;
-    case 5: split_gemm_s<5>(ctx, a, bt, c, batches, m, n, k, stream); break;
-    case 6: split_gemm_s<6>(ctx, a, bt, c, batches, m, n, k, stream); break;
-    case 7: split_gemm_s<7>(ctx, a, bt, c, batches, m, n, k, stream); break;
-    default: fail(EINFOLD_INVALID, "slices must be 2 to 7, not %d", slices);
-  }
+  dispatch_slices(slices, [&](auto S) { split_gemm_s<decltype(S)::value>(ctx, a, b, b_natural, c, batches, m, n, k, stream); });
 }
 
-void fp64_gemm(Context& ctx, const double* a, const int32_t* held, const double* bt, double* c, int64_t batches,
+void fp64_gemm(Context& ctx, const double* a, const uint32_t* held, const double* b, double* c, int64_t batches,
                int64_t m, int64_t n, int64_t k, int64_t /*batch_of_row*/, int64_t zblock, bool fused_multiply_add,
                cudaStream_t stream) {
   if (batches <= 0 || m <= 0 || n <= 0) return;
   dim3 grid((unsigned)((n + 63) / 64), (unsigned)((m + 63) / 64), (unsigned)batches);
   if (fused_multiply_add)
-    fp64_gemm_kernel<true><<<grid, 256, 0, stream>>>(a, held, bt, c, m, n, k, 0);
+    fp64_gemm_kernel<true><<<grid, 256, 0, stream>>>(a, held, b, c, m, n, k, 0);
   else
-    fp64_gemm_kernel<false><<<grid, 256, 0, stream>>>(a, held, bt, c, m, n, k, zblock);
+    fp64_gemm_kernel<false><<<grid, 256, 0, stream>>>(a, held, b, c, m, n, k, zblock);
   EF_LAUNCH_CHECK();
   ctx.kernels++;
 }

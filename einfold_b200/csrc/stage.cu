@@ -42,7 +42,7 @@ __global__ void widen(const T* __restrict__ in, int64_t n, int64_t* __restrict__
       w = (int64_t)v;
     }
     if (w < 0) f |= 1;
-    out[i] = w;
+    if (out) out[i] = w;
     if (w > local) local = w;
   }
   for (int o = 16; o; o >>= 1) {
@@ -76,12 +76,16 @@ DeviceColumn stage_column(Context& ctx, const Relation& r, int col, bool with_va
   if (col < 0 || col >= (int)r.fields.size()) fail(EINFOLD_INVALID, "column %d of a relation with %zu", col, r.fields.size());
   d.kind = r.fields[col].kind;
   d.rows = r.rows();
+  const cudaMemcpyKind from = r.device >= 0 ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (r.device >= 0 && r.device != ctx.device)
+    fail(EINFOLD_INVALID, "a relation on device %d given to a context on device %d", r.device, ctx.device);
   for (auto& b : r.batches) {
     const Column& c = b.columns[col];
     if (c.dictionary) fail(EINFOLD_INVALID, "dictionary columns are not staged here");
     d.nulls += c.nulls();
   }
   if (is_var(d.kind)) {
+    if (r.device >= 0) fail(EINFOLD_INVALID, "variable-length columns must be in host memory");
     bool large = d.kind == Kind::LargeUtf8 || d.kind == Kind::LargeBinary;
     // Offsets rebased per batch on the host (one pass over the offsets), bytes copied as they are.
     std::vector<int64_t> off((size_t)d.rows + 1);
@@ -129,7 +133,7 @@ DeviceColumn stage_column(Context& ctx, const Relation& r, int col, bool with_va
     for (auto& b : r.batches) {
       const Column& c = b.columns[col];
       int64_t first = c.offset / 8, last = (c.offset + c.length + 7) / 8;
-      if (last > first) EF_CUDA(cudaMemcpyAsync(bits.get() + pos, c.values + first, (size_t)(last - first), cudaMemcpyHostToDevice, s));
+      if (last > first) EF_CUDA(cudaMemcpyAsync(bits.get() + pos, c.values + first, (size_t)(last - first), from, s));
       pos += last - first;
     }
     if (seg.empty()) seg.push_back({0, -1, 0, 0});
@@ -140,14 +144,20 @@ DeviceColumn stage_column(Context& ctx, const Relation& r, int col, bool with_va
   } else if (d.kind != Kind::Null) {
     d.width = width_of(d.kind);
     if (!d.width) fail(EINFOLD_INVALID, "a column of an unsupported type");
-    d.data.allocate((size_t)(d.rows * d.width ? d.rows * d.width : 1), s);
-    int64_t row = 0;
-    for (auto& b : r.batches) {
-      const Column& c = b.columns[col];
-      if (c.length)
-        EF_CUDA(cudaMemcpyAsync(d.data.get() + row * d.width, c.values + c.offset * d.width, (size_t)(c.length * d.width),
-                                cudaMemcpyHostToDevice, s));
-      row += c.length;
+    if (r.device >= 0 && r.batches.size() == 1) {
+      // One batch already in HBM: read in place.
+      const Column& c = r.batches[0].columns[col];
+      d.alias = c.values + c.offset * d.width;
+    } else {
+      d.data.allocate((size_t)(d.rows * d.width ? d.rows * d.width : 1), s);
+      int64_t row = 0;
+      for (auto& b : r.batches) {
+        const Column& c = b.columns[col];
+        if (c.length)
+          EF_CUDA(cudaMemcpyAsync(d.data.get() + row * d.width, c.values + c.offset * d.width,
+                                  (size_t)(c.length * d.width), from, s));
+        row += c.length;
+      }
     }
   }
   if (with_validity && d.nulls > 0) {
@@ -171,7 +181,7 @@ DeviceColumn stage_column(Context& ctx, const Relation& r, int col, bool with_va
       const Column& c = b.columns[col];
       if (c.validity && c.nulls() > 0) {
         int64_t first = c.offset / 8, last = (c.offset + c.length + 7) / 8;
-        EF_CUDA(cudaMemcpyAsync(bits.get() + pos, c.validity + first, (size_t)(last - first), cudaMemcpyHostToDevice, s));
+        EF_CUDA(cudaMemcpyAsync(bits.get() + pos, c.validity + first, (size_t)(last - first), from, s));
         pos += last - first;
       }
     }
@@ -194,14 +204,14 @@ DeviceBuffer<int64_t> keys_as_i64(Context& ctx, const DeviceColumn& c, KeyStats*
   flags.zero();
   unsigned g = blocks_for(c.rows, 256);
   switch (c.kind) {
-    case Kind::Int8: widen<int8_t><<<g, 256, 0, s>>>((const int8_t*)c.data.get(), c.rows, out.get(), mx.get(), flags.get()); break;
-    case Kind::UInt8: widen<uint8_t><<<g, 256, 0, s>>>((const uint8_t*)c.data.get(), c.rows, out.get(), mx.get(), flags.get()); break;
-    case Kind::Int16: widen<int16_t><<<g, 256, 0, s>>>((const int16_t*)c.data.get(), c.rows, out.get(), mx.get(), flags.get()); break;
-    case Kind::UInt16: widen<uint16_t><<<g, 256, 0, s>>>((const uint16_t*)c.data.get(), c.rows, out.get(), mx.get(), flags.get()); break;
-    case Kind::Int32: widen<int32_t><<<g, 256, 0, s>>>((const int32_t*)c.data.get(), c.rows, out.get(), mx.get(), flags.get()); break;
-    case Kind::UInt32: widen<uint32_t><<<g, 256, 0, s>>>((const uint32_t*)c.data.get(), c.rows, out.get(), mx.get(), flags.get()); break;
-    case Kind::Int64: widen<int64_t><<<g, 256, 0, s>>>((const int64_t*)c.data.get(), c.rows, out.get(), mx.get(), flags.get()); break;
-    case Kind::UInt64: widen<uint64_t><<<g, 256, 0, s>>>((const uint64_t*)c.data.get(), c.rows, out.get(), mx.get(), flags.get()); break;
+    case Kind::Int8: widen<int8_t><<<g, 256, 0, s>>>((const int8_t*)c.ptr(), c.rows, out.get(), mx.get(), flags.get()); break;
+    case Kind::UInt8: widen<uint8_t><<<g, 256, 0, s>>>((const uint8_t*)c.ptr(), c.rows, out.get(), mx.get(), flags.get()); break;
+    case Kind::Int16: widen<int16_t><<<g, 256, 0, s>>>((const int16_t*)c.ptr(), c.rows, out.get(), mx.get(), flags.get()); break;
+    case Kind::UInt16: widen<uint16_t><<<g, 256, 0, s>>>((const uint16_t*)c.ptr(), c.rows, out.get(), mx.get(), flags.get()); break;
+    case Kind::Int32: widen<int32_t><<<g, 256, 0, s>>>((const int32_t*)c.ptr(), c.rows, out.get(), mx.get(), flags.get()); break;
+    case Kind::UInt32: widen<uint32_t><<<g, 256, 0, s>>>((const uint32_t*)c.ptr(), c.rows, out.get(), mx.get(), flags.get()); break;
+    case Kind::Int64: widen<int64_t><<<g, 256, 0, s>>>((const int64_t*)c.ptr(), c.rows, out.get(), mx.get(), flags.get()); break;
+    case Kind::UInt64: widen<uint64_t><<<g, 256, 0, s>>>((const uint64_t*)c.ptr(), c.rows, out.get(), mx.get(), flags.get()); break;
     default: fail(EINFOLD_INVALID, "keys_as_i64 of a non-integer column");
   }
   EF_LAUNCH_CHECK();
@@ -215,6 +225,25 @@ DeviceBuffer<int64_t> keys_as_i64(Context& ctx, const DeviceColumn& c, KeyStats*
   stats->negative = f & 1;
   stats->too_large = (f & 2) != 0;
   return out;
+}
+
+void key_stats_i64(Context& ctx, const int64_t* keys, int64_t n, KeyStats* stats) {
+  cudaStream_t s = ctx.stream;
+  DeviceBuffer<unsigned long long> mx(1, s);
+  DeviceBuffer<int> flags(1, s);
+  mx.zero();
+  flags.zero();
+  widen<int64_t><<<blocks_for(n, 256), 256, 0, s>>>(keys, n, nullptr, mx.get(), flags.get());
+  EF_LAUNCH_CHECK();
+  ctx.kernels++;
+  unsigned long long m = 0;
+  int f = 0;
+  EF_CUDA(cudaMemcpyAsync(&m, mx.get(), 8, cudaMemcpyDeviceToHost, s));
+  EF_CUDA(cudaMemcpyAsync(&f, flags.get(), 4, cudaMemcpyDeviceToHost, s));
+  EF_CUDA(cudaStreamSynchronize(s));
+  stats->max = n ? (int64_t)m : -1;
+  stats->negative = f & 1;
+  stats->too_large = (f & 2) != 0;
 }
 
 int64_t exclusive_scan_flags(Context& ctx, const uint8_t* flags, int64_t n, int64_t* out) {

@@ -18,6 +18,8 @@ struct DeviceColumn {
   int64_t rows = 0;
   int64_t nulls = 0;
   DeviceBuffer<uint8_t> data;   // fixed-width values (rows * width)
+  const uint8_t* alias = nullptr;  // the caller's device buffer, used in place of `data`
+  const uint8_t* ptr() const { return alias ? alias : data.get(); }
   DeviceBuffer<uint8_t> valid;  // one byte per row, 1 = valid; empty when nulls == 0
   // var-length kinds
   DeviceBuffer<int64_t> offsets;  // rows + 1
@@ -35,6 +37,8 @@ struct KeyStats {
   bool too_large = false;
 };
 DeviceBuffer<int64_t> keys_as_i64(Context& ctx, const DeviceColumn& c, KeyStats* stats);
+// The same statistics of int64 keys already in HBM, read in place.
+void key_stats_i64(Context& ctx, const int64_t* keys, int64_t n, KeyStats* stats);
 
 // Exclusive prefix sum of n flags (uint8) into int64 positions; returns the total.
 int64_t exclusive_scan_flags(Context& ctx, const uint8_t* flags, int64_t n, int64_t* out);
@@ -44,6 +48,20 @@ void pack_bits(Context& ctx, const uint8_t* bytes, int64_t n, uint8_t* bits);
 
 // Device to host, into a fresh host buffer.
 HostBuffer to_host(Context& ctx, const void* dev, size_t bytes);
+
+// A result buffer from a device buffer: moved into the result as it is when
+// the result stays in device memory, else copied to host memory.
+template <class T>
+Buffer result_buffer(Context& ctx, DeviceBuffer<T>& dev, size_t bytes, bool on_device) {
+  if (!on_device) return Buffer(to_host(ctx, dev.get(), bytes));
+  Buffer b;
+  b.ptr = dev.ptr;
+  b.bytes = bytes;
+  b.device = ctx.device;
+  dev.ptr = nullptr;
+  dev.count = 0;
+  return b;
+}
 
 // A row of small descriptors passed to kernels by value.
 constexpr int kMaxDims = 8;

@@ -81,6 +81,9 @@ class Options:
     precision: Precision = Precision.SPLIT
     slices: int = 0
     device: int = 0
+    # Leave the result's buffers in HBM: the functions then return DeviceBatch
+    # objects instead of pyarrow record batches.
+    result_on_device: bool = False
 
 
 class Algorithm(enum.Enum):
@@ -93,6 +96,74 @@ class Algorithm(enum.Enum):
 class Relation:
     schema: pa.Schema
     batches: List[pa.RecordBatch]
+
+
+_FORMATS = {pa.int8(): b"c", pa.uint8(): b"C", pa.int16(): b"s", pa.uint16(): b"S", pa.int32(): b"i",
+            pa.uint32(): b"I", pa.int64(): b"l", pa.uint64(): b"L", pa.float32(): b"f", pa.float64(): b"g"}
+
+
+class DeviceRelation:
+    """One batch whose columns are CUDA tensors already in HBM (the Arrow C
+    Device Data Interface's CUDA placement): fixed-width columns, each with an
+    optional validity bitmap tensor (uint8, bit i = row i) and its null count."""
+
+    def __init__(self, schema: pa.Schema, columns: Sequence, validity: Optional[Sequence] = None,
+                 null_counts: Optional[Sequence[int]] = None, device: int = 0):
+        self.schema = schema
+        self.columns = list(columns)
+        self.validity = list(validity) if validity is not None else [None] * len(self.columns)
+        self.null_counts = list(null_counts) if null_counts is not None else [0] * len(self.columns)
+        self.device = device
+        self.rows = int(self.columns[0].numel()) if self.columns else 0
+        for f in schema:
+            if f.type not in _FORMATS:
+                raise ArrowInvalidArgumentError(f"a device column of type {f.type}")
+
+
+class _CudaArray:
+    """A device buffer seen through __cuda_array_interface__ (for torch.as_tensor)."""
+
+    def __init__(self, ptr: int, n: int, typestr: str, owner):
+        self.owner = owner
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False), "version": 3,
+                                         "strides": None}
+
+
+class DeviceBatch:
+    """A result whose buffers are in HBM, owned until :meth:`release`."""
+
+    _TYPESTR = {b"c": "|i1", b"C": "|u1", b"s": "<i2", b"S": "<u2", b"i": "<i4", b"I": "<u4", b"l": "<i8",
+                b"L": "<u8", b"f": "<f4", b"g": "<f8"}
+
+    def __init__(self, res):
+        self._res = res
+        self.rows = int(res.batches[0].length) if res.n_batches else 0
+        self.formats = []
+        s = res.schema.contents
+        for i in range(s.n_children):
+            self.formats.append(s.children[i].contents.format)
+
+    def column(self, i: int):
+        """Column i's values as a CUDA tensor sharing the result's memory."""
+        import torch
+
+        arr = self._res.batches[0].children[i].contents
+        ptr = arr.buffers[1]
+        return torch.as_tensor(_CudaArray(ptr or 0, self.rows, self._TYPESTR[self.formats[i]], self), device="cuda")
+
+    def null_count(self, i: int) -> int:
+        return int(self._res.batches[0].children[i].contents.null_count)
+
+    def release(self):
+        if self._res is not None:
+            _lib.load().einfold_result_release(ctypes.byref(self._res))
+            self._res = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
 
 
 @dataclass
@@ -202,7 +273,23 @@ def _export_schema(s: pa.Schema, keep: _Keep) -> _lib.ArrowSchema:
     return c
 
 
+def _device_relation(r: "DeviceRelation", keep: _Keep) -> _lib.Relation:
+    cs = _export_schema(r.schema, keep)
+    children = []
+    for col, valid, nulls in zip(r.columns, r.validity, r.null_counts):
+        bufs = keep.add(_array(ctypes.c_void_p, [valid.data_ptr() if valid is not None else None, col.data_ptr()]))
+        child = keep.add(_lib.ArrowArray(int(col.numel()), int(nulls), 0, 2, 0, bufs, None, None, None, None))
+        children.append(ctypes.pointer(child))
+    kids = keep.add(_array(ctypes.POINTER(_lib.ArrowArray), children))
+    top_bufs = keep.add(_array(ctypes.c_void_p, [None]))
+    top = keep.add(_lib.ArrowArray(r.rows, 0, 0, 1, len(children), top_bufs, kids, None, None, None))
+    ptrs = keep.add(_array(ctypes.POINTER(_lib.ArrowArray), [ctypes.pointer(top)]))
+    return keep.add(_lib.Relation(ctypes.pointer(cs), 1, ptrs, r.device, 0))
+
+
 def _relation(r, keep: _Keep) -> _lib.Relation:
+    if isinstance(r, DeviceRelation):
+        return _device_relation(r, keep)
     if isinstance(r, Relation):
         schema, batches = r.schema, list(r.batches)
     elif isinstance(r, pa.Table):
@@ -222,7 +309,7 @@ def _relation(r, keep: _Keep) -> _lib.Relation:
         keep.exported_arrays.append(a)
         arrays.append(ctypes.pointer(a))
     ptrs = keep.add(_array(ctypes.POINTER(_lib.ArrowArray), arrays))
-    return keep.add(_lib.Relation(ctypes.pointer(cs), len(batches), ptrs))
+    return keep.add(_lib.Relation(ctypes.pointer(cs), len(batches), ptrs, -1, 0))
 
 
 def _options(o: Options, keep: _Keep) -> _lib.Options:
@@ -233,7 +320,8 @@ def _options(o: Options, keep: _Keep) -> _lib.Options:
         grow = keep.add(_lib.GROW(lambda _ctx, n: 1 if budget.grow(int(n)) else 0))
         shrink = keep.add(_lib.SHRINK(lambda _ctx, n: budget.shrink(int(n))))
     return keep.add(_lib.Options(int(o.host.float_keys), max(int(o.threads), 1), int(o.domain_rows),
-                                 int(o.precision.value), int(o.slices), 0, None, grow, shrink))
+                                 int(o.precision.value), int(o.slices), int(bool(o.result_on_device)), None, grow,
+                                 shrink))
 
 
 def _raise(status: int, message: str):
@@ -252,6 +340,8 @@ class CallInfo:
 
     kernels_launched: int = 0
     device_ms: float = 0.0
+    product_ms: float = 0.0
+    product_ops: float = 0.0
     message: str = ""
 
 
@@ -274,6 +364,8 @@ def _call(fn, *args) -> Optional[_lib.Result]:
     msg = res.message.decode(errors="replace")
     last_call.kernels_launched = res.kernels_launched
     last_call.device_ms = res.device_ms
+    last_call.product_ms = res.product_ms
+    last_call.product_ops = res.product_ops
     last_call.message = msg
     if status == _lib.DECLINED:
         return None
@@ -301,6 +393,8 @@ def fold(f: ir.Fold, a, b, domain=None, schema: Optional[pa.Schema] = None,
         if res is None:
             raise ArrowComputeError("the fold declined")
         alg = Algorithm(_lib.ALGORITHMS[res.algorithm])
+        if options.result_on_device:
+            return Folded(alg, [DeviceBatch(res)])
         return Folded(alg, _collect(res))
     finally:
         keep.release()

@@ -159,6 +159,11 @@ typedef struct {
   const struct ArrowSchema* schema; /* a struct schema: the relation's columns */
   int64_t n_batches;
   struct ArrowArray* const* batches; /* each a struct array of `schema` */
+  /* Where the batches' buffers live: -1 host memory; d >= 0 the memory of
+   * CUDA device d (the Arrow C Device Data Interface's ARROW_DEVICE_CUDA).
+   * Device columns must state their null counts. */
+  int32_t device;
+  int32_t pad;
 } einfold_relation;
 
 /* ---- Options (options.rs:70-84) ---- */
@@ -171,7 +176,9 @@ typedef struct {
    * order of additions: the reference's bits). */
   int32_t precision;
   int32_t slices;      /* split products: slices per operand, 0 = default (6) */
-  int32_t pad;
+  /* 0: result buffers in host memory; 1: in the context's device memory
+   * (released with cudaFree by the arrays' release callbacks). */
+  int32_t result_on_device;
   /* The budget (options.rs:56-65): grow returns nonzero if `bytes` more may be
    * allocated; shrink gives bytes back. NULL grow = no limit. */
   void* budget_ctx;
@@ -191,6 +198,10 @@ typedef struct {
   /* Device kernels launched and device milliseconds spent, for metrics. */
   uint64_t kernels_launched;
   double device_ms;
+  /* The dense products' tensor-core kernels: milliseconds (CUDA events around
+   * their launches on the call's stream) and int8 multiply-adds x 2 done. */
+  double product_ms;
+  double product_ops;
   char message[480];
 } einfold_result;
 

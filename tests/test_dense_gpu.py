@@ -139,3 +139,25 @@ def test_masked_groups_are_dropped():
     got = K.fold_dense(f, K.Relation(sa, a), K.Relation(sb, b))
     assert rows_of(got).num_rows == n * (n + 1) // 2
     assert_same_rows(rows_of(got), rows_of(want), np.full(n * (n + 1) // 2, split_bound(d, [1.0], [1.0])[0, 0]))
+
+
+def test_device_relations_and_device_results_match_host_ones():
+    import torch
+
+    rng = oracle.Rng.seeded(11, 0)
+    ni, nj, nk = 100, 64, 70
+    sa, a = complete(["i", "j"], [ni, nj], rng.units(ni * nj) * 2 - 1, rng, batches=1, shuffle=False)
+    sb, b = complete(["j", "k"], [nj, nk], rng.units(nj * nk) * 2 - 1, rng, batches=1, shuffle=False)
+    f = matmul_fold()
+    host = rows_of(K.fold(f, K.Relation(sa, a), K.Relation(sb, b)).batches)
+    cols = lambda t: [torch.as_tensor(np.asarray(c.to_numpy())).cuda() for c in pa.Table.from_batches(t).columns]
+    da = K.DeviceRelation(sa, cols(a))
+    db = K.DeviceRelation(sb, cols(b))
+    dev = K.fold(f, da, db, options=K.Options(result_on_device=True)).batches[0]
+    assert dev.rows == host.num_rows
+    for c in range(3):
+        got = dev.column(c).cpu().numpy()
+        want = np.asarray(host.column(c).to_numpy())
+        assert np.array_equal(got.view(np.uint64) if got.dtype == np.float64 else got,
+                              want.view(np.uint64) if want.dtype == np.float64 else want)
+    dev.release()
