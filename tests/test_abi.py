@@ -1,0 +1,78 @@
+"""The C ABI library loads, exports what the header declares, and computes
+schemas on the host (no GPU needed)."""
+import os
+
+import pyarrow as pa
+import pytest
+
+from einfold_b200 import _lib, ir, kernels as K
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "einfold_b200.h")
+
+
+def test_every_declared_symbol_is_exported():
+    lib = _lib.load()
+    declared = _lib.declared_symbols(HEADER)
+    assert len(declared) >= 14
+    for name in declared:
+        assert hasattr(lib, name), name
+        assert name in _lib.SIGNATURES, f"{name} has no ctypes signature"
+    assert lib.einfold_version().startswith(b"einfold_b200")
+
+
+def _matmul():
+    e = ir.EQ
+    return ir.Fold([e, e, e], [ir.Operand([(0, 0), (1, 1)], 2), ir.Operand([(1, 0), (2, 1)], 2)],
+                   [ir.Output(0), ir.Output(2)])
+
+
+def test_schema_follows_the_key_types():
+    sa = pa.schema([("i", pa.int32()), ("j", pa.int64()), ("v", pa.float64())])
+    sb = pa.schema([("j", pa.int64()), ("k", pa.uint16()), ("v", pa.float64())])
+    s = K.schema(_matmul(), [sa, sb])
+    assert [f.type for f in s] == [pa.int32(), pa.uint16(), pa.float64()]
+    assert [f.name for f in s] == ["0", "1", "2"]
+
+
+def test_schema_rejects_mismatched_keys_and_non_float_values():
+    sa = pa.schema([("i", pa.int64()), ("j", pa.int64()), ("v", pa.float64())])
+    sb = pa.schema([("j", pa.int32()), ("k", pa.int64()), ("v", pa.float64())])
+    with pytest.raises(K.ArrowInvalidArgumentError):
+        K.schema(_matmul(), [sa, sb])
+    sb = pa.schema([("j", pa.int64()), ("k", pa.int64()), ("v", pa.float32())])
+    with pytest.raises(K.ArrowInvalidArgumentError):
+        K.schema(_matmul(), [sa, sb])
+
+
+def test_domain_schema_carries_columns_and_a_non_null_default():
+    e = ir.EQ
+    f = ir.Fold([e, e, e], [ir.Operand([(0, 0), (1, 1)], 2), ir.Operand([(1, 0), (2, 1)], 2)],
+                [ir.Output(0, ir.DomainKey(1)), ir.Output(2, ir.DomainKey(2))], domain=ir.Domain((0, 1, 2), 0.0))
+    sa = pa.schema([("i", pa.int64()), ("j", pa.int64()), ("v", pa.float64())])
+    sb = pa.schema([("j", pa.int64()), ("k", pa.int64()), ("v", pa.float64())])
+    sd = pa.schema([("tag", pa.string()), ("i", pa.int64()), ("k", pa.int64())])
+    s = K.schema(f, [sa, sb], sd)
+    assert [f.type for f in s] == [pa.string(), pa.int64(), pa.int64(), pa.float64()]
+    assert not s.field(3).nullable
+
+
+def test_invalid_folds_are_rejected_by_the_ir():
+    e = ir.EQ
+    with pytest.raises(ir.InvalidFold):
+        ir.Fold([e, e], [ir.Operand([(0, 0)], 1)], [ir.Output(0)])  # dimension 1 held by no operand
+    with pytest.raises(ir.InvalidFold):
+        ir.Fold([e], [ir.Operand([(0, 0), (0, 1)], 2)], [ir.Output(0)])
+    with pytest.raises(ir.InvalidFold):
+        _matmul().with_conditions([ir.Condition(0, ir.Comparison.LESS, 0, 0)])
+
+
+def test_pipeline_schema():
+    e = ir.EQ
+    scores = ir.Fold([e, e, e], [ir.Operand([(0, 0), (1, 1)], 2), ir.Operand([(2, 0), (1, 1)], 2)],
+                     [ir.Output(0), ir.Output(2)])
+    p = ir.Pipeline(scores, ir.Weight.exp(), [e], ir.Operand([(2, 0), (3, 1)], 2), [0, 3], ir.Normalizer.KEPT_GROUPS)
+    q = pa.schema([("t", pa.int64()), ("d", pa.int64()), ("x", pa.float64())])
+    v = pa.schema([("t", pa.int64()), ("c", pa.int32()), ("x", pa.float64())])
+    s = K.pipeline_schema(p, [q, q, v])
+    assert [f.type for f in s] == [pa.int64(), pa.int32(), pa.float64()]
