@@ -142,6 +142,9 @@ SIGNATURES = {
     "einfold_split_gemm": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                             ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                             ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
+    "einfold_split_gemm_static": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                                   ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32,
+                                                   ctypes.c_int32, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int32]),
     "einfold_fp64_gemm": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                            ctypes.c_int32, ctypes.c_void_p]),

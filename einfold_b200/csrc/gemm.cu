@@ -750,4 +750,82 @@ void transpose(const double* b, double* bt, int64_t batches, int64_t rows, int64
   EF_LAUNCH_CHECK();
 }
 
+// ---- The split product for callers that can't allocate ----------------
+
+namespace {
+
+// Scratch for einfold_split_gemm_static: every device that loads the library
+// holds these 64 MiB until the process exits.
+constexpr size_t kStaticScratchBytes = (size_t)64 << 20;
+__device__ __align__(256) uint8_t g_split_scratch[kStaticScratchBytes];
+
+std::mutex g_static_lock;
+void* g_static_base[64] = {};
+
+// The array's device address on the current device. The first call on a
+// device looks it up (and sets the product kernels' shared-memory limit);
+// host code can't use the array's name as an address.
+uint8_t* static_scratch(int device) {
+  std::lock_guard<std::mutex> lock(g_static_lock);
+  if (device < 0 || device >= 64) fail(EINFOLD_INVALID, "device %d out of range", device);
+  if (!g_static_base[device]) {
+    void* p = nullptr;
+    EF_CUDA(cudaGetSymbolAddress(&p, g_split_scratch));
+    g_static_base[device] = p;
+  }
+  return (uint8_t*)g_static_base[device];
+}
+
+}  // namespace
+
 }  // namespace ef
+
+extern "C" int32_t einfold_split_gemm_static(const double* a, const double* b, double* c, int64_t batches, int64_t m,
+                                             int64_t n, int64_t k, int32_t b_transposed, int32_t slices,
+                                             void* stream, char* message, int32_t message_len) {
+  using namespace ef;
+  try {
+    int device = 0;
+    EF_CUDA(cudaGetDevice(&device));
+    uint8_t* base = static_scratch(device);
+    const int S = slices ? slices : kDefaultSlices;
+    if (S < kMinSlices || S > kMaxSlices) fail(EINFOLD_INVALID, "slices must be 2 to 7, not %d", S);
+    if (batches < 0 || m < 0 || n < 0 || k < 0) fail(EINFOLD_INVALID, "negative sizes");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (batches == 0 || m == 0 || n == 0) return EINFOLD_OK;
+    if (m > INT32_MAX / 2 || n > INT32_MAX / 2 || batches > 65535) fail(EINFOLD_INVALID, "a product too large");
+    if (k == 0) {
+      EF_CUDA(cudaMemsetAsync(c, 0, (size_t)(batches * m * n) * sizeof(double), s));
+      EF_CUDA(cudaStreamSynchronize(s));
+      return EINFOLD_OK;
+    }
+    size_t sz[6];
+    split_scratch_sizes(S, batches, m, n, k, sz);
+    size_t total = 0;
+    for (size_t x : sz) total += x;
+    if (total > kStaticScratchBytes)
+      fail(EINFOLD_INVALID,
+           "this product needs %zu bytes of scratch, more than the %zu einfold_split_gemm_static holds; "
+           "use einfold_split_gemm", total, kStaticScratchBytes);
+    SplitScratch sc;
+    uint8_t* p = base;
+    sc.da = (int8_t*)p; p += sz[0];
+    sc.db = (int8_t*)p; p += sz[1];
+    sc.ea = (int32_t*)p; p += sz[2];
+    sc.eb = (int32_t*)p; p += sz[3];
+    sc.colmax = (unsigned long long*)p; p += sz[4];
+    sc.status = (int*)p;
+    Context local;  // no stream or pool of its own: the caller's stream, nothing allocated
+    local.device = device;
+    local.stream = s;
+    int st = 0;
+    dispatch_slices(S, [&](auto SS) {
+      st = split_run<decltype(SS)::value>(local, a, b, b_transposed == 0, c, batches, m, n, k, sc, s, false);
+    });
+    check_status(st);
+    return EINFOLD_OK;
+  } catch (const Failure& f) {
+    if (message && message_len > 0) std::snprintf(message, (size_t)message_len, "%s", f.what());
+    return f.status;
+  }
+}

@@ -261,6 +261,24 @@ int32_t einfold_split_gemm(einfold_context* ctx, const double* a, const double* 
 int32_t einfold_fp64_gemm(einfold_context* ctx, const double* a, const double* b, double* c, int64_t batches,
                           int64_t m, int64_t n, int64_t k, int32_t b_transposed, void* stream);
 
+/* einfold_split_gemm for callers that can't allocate device memory: an
+ * engine that hands every byte of HBM to its own pool, or code running
+ * inside an allocator callback or under a memory budget that forbids any
+ * allocation outside its pool. It has no counterpart in the reference.
+ * Its scratch (the operands' digits and scales) lives in one 64 MiB array in
+ * the library's device memory, which every GPU that loads the library holds
+ * until the process exits; a product needing more returns EINFOLD_INVALID
+ * with the sizes in `message`, and einfold_split_gemm is the one to call.
+ * No context: it runs on the calling thread's current device and `stream`
+ * (NULL: the legacy default stream) and returns once the product is done.
+ * It calls no cudaMalloc or cudaFree. Its first call on a device looks up
+ * the array's address, so make that call before any stream capture. Every
+ * call shares the array: calls that overlap on the GPU, from two threads or
+ * two streams, race and give wrong results; serialize them. */
+int32_t einfold_split_gemm_static(const double* a, const double* b, double* c, int64_t batches, int64_t m,
+                                  int64_t n, int64_t k, int32_t b_transposed, int32_t slices, void* stream,
+                                  char* message, int32_t message_len);
+
 #ifdef __cplusplus
 }
 #endif
