@@ -5,6 +5,7 @@
 
 #include "fold.h"
 #include "gemm.cuh"
+#include "rank.cuh"
 
 struct einfold_context : ef::Context {};
 
@@ -244,6 +245,17 @@ int32_t einfold_split_gemm(einfold_context* ctx, const double* a, const double* 
   return guarded(ctx, &r, [&](ef::Context& cx) -> int32_t {
     cudaStream_t s = stream ? (cudaStream_t)stream : cx.stream;
     ef::split_gemm(cx, a, b, b_transposed == 0, c, batches, m, n, k, slices ? slices : ef::kDefaultSlices, s);
+    return EINFOLD_OK;
+  });
+}
+
+int32_t einfold_rank_words(einfold_context* ctx, const uint64_t* words, int64_t n, uint32_t* rank, uint32_t* first,
+                           int64_t* n_ranks, void* stream) {
+  einfold_result r;
+  return guarded(ctx, &r, [&](ef::Context& cx) -> int32_t {
+    cudaStream_t s = stream ? (cudaStream_t)stream : cx.stream;
+    int64_t k = ef::rank_keys(cx, words, 1, n, n, rank, first, s);
+    if (n_ranks) *n_ranks = k;
     return EINFOLD_OK;
   });
 }

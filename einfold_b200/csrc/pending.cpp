@@ -18,7 +18,3 @@ FoldOutput fused_pipeline(Context&, const PipelineD&, const Relation&, const Rel
 
 }  // namespace ef
 
-extern "C" int32_t einfold_rank_words(einfold_context*, const uint64_t*, int64_t, uint32_t*, uint32_t*, int64_t*,
-                                      void*) {
-  return EINFOLD_COMPUTE;
-}

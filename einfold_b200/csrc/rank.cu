@@ -1,0 +1,361 @@
+// Ranking keys by their bytes on the device: the discrimination algorithm's
+// first step (crates/einfold-kernels/src/discriminate.rs:103-156 `radix`,
+// :212-235 `ranks`, :280-292 `ranks_of_words`).
+//
+// Keys are W 64-bit words each, most significant word first, ordered as
+// unsigned integers. A stable LSD radix sort of (key, row) pairs runs one
+// 8-bit pass per byte that varies between keys (constant bytes are skipped,
+// as the reference skips them), then each row's rank is the number of
+// distinct keys before its own, and first[r] the smallest row holding rank r
+// (the first of its run, as the sort is stable).
+//
+// One pass: the keys are cut into as many chunks as blocks fit on the GPU at
+// once. An upsweep counts each chunk's digits; one exclusive scan of the
+// digit-major table gives each (digit, chunk) its first output position; a
+// downsweep block then sorts its chunk tile by tile: each key ranked among
+// equal digits of its warp with __match_any_sync in row order, warps combined
+// in shared memory, the tile reordered by digit in shared memory and written
+// out run by run, contiguously. No block waits on another. Every pass is
+// stable, so the result is the reference's bit for bit.
+#include <cub/cub.cuh>
+
+#include "ptx.cuh"
+#include "rank.cuh"
+#include "stage.cuh"
+
+namespace ef {
+
+void thrust_iota(Context& ctx, uint32_t* out, int64_t n, cudaStream_t s);
+
+namespace {
+
+constexpr int kThreads = 256;
+
+template <int W>
+__global__ void or_and_words(const uint64_t* __restrict__ keys, int64_t n, int64_t ld, unsigned long long* __restrict__ acc) {
+  unsigned long long o[W], a[W];
+#pragma unroll
+  for (int w = 0; w < W; w++) { o[w] = 0; a[w] = ~0ull; }
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+#pragma unroll
+    for (int w = 0; w < W; w++) {
+      const unsigned long long k = keys[(int64_t)w * ld + i];
+      o[w] |= k;
+      a[w] &= k;
+    }
+#pragma unroll
+  for (int w = 0; w < W; w++) {
+    for (int s = 16; s; s >>= 1) {
+      o[w] |= __shfl_xor_sync(0xffffffffu, o[w], s);
+      a[w] &= __shfl_xor_sync(0xffffffffu, a[w], s);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicOr(&acc[2 * w], o[w]);
+      atomicAnd(&acc[2 * w + 1], a[w]);
+    }
+  }
+}
+
+// Upsweep of one pass: the digit counts of each chunk of consecutive keys,
+// written digit-major (table[d·chunks + c]) so that one exclusive scan gives
+// every (digit, chunk)'s first output position, stably.
+__global__ void __launch_bounds__(kThreads) chunk_counts(const uint64_t* __restrict__ kw, int64_t n, int shift,
+                                                         int64_t chunk, int chunks,
+                                                         unsigned long long* __restrict__ table) {
+  __shared__ unsigned int h[8][256];
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int i = tid; i < 8 * 256; i += kThreads) (&h[0][0])[i] = 0;
+  __syncthreads();
+  const int64_t c = blockIdx.x;
+  const int64_t lo = c * chunk, hi = min(n, lo + chunk);
+  for (int64_t i = lo + tid; i < hi; i += kThreads) atomicAdd(&h[warp][(kw[i] >> shift) & 255], 1u);
+  __syncthreads();
+  unsigned int t = 0;
+#pragma unroll
+  for (int w = 0; w < 8; w++) t += h[w][tid];
+  table[(int64_t)tid * chunks + c] = t;
+}
+
+// Downsweep of one pass: block c sorts its chunk tile by tile, each key
+// ranked among equal digits in row order (warp __match_any_sync, warps
+// combined in shared memory), its destination its digit's running offset plus
+// that rank. Tiles arrive by TMA bulk copies into two shared-memory stages, the
+// next one in flight while the current one is ranked; each stage is then
+// reused to reorder its tile by digit, and the tile is written out run by
+// run, contiguously.
+template <int W, int ITEMS>
+__global__ void __launch_bounds__(kThreads) chunk_scatter(const uint64_t* __restrict__ kin,
+                                                          const uint32_t* __restrict__ vin,
+                                                          uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                          int64_t n, int64_t ldi, int64_t ldo, int word, int shift,
+                                                          int64_t chunk, int chunks,
+                                                          const long long* __restrict__ offsets, int* err) {
+  constexpr int TILE = kThreads * ITEMS;
+  constexpr int WARPS = kThreads / 32;
+  constexpr int STAGE = TILE * (8 * W + 4);
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ unsigned int warp_hist[WARPS][256];
+  __shared__ unsigned int tile_start[256];
+  __shared__ long long running[256];
+  __shared__ __align__(8) uint64_t bar[2];
+  typedef cub::BlockScan<unsigned int, kThreads> Scan;
+  __shared__ typename Scan::TempStorage tmp;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int64_t c = blockIdx.x;
+  const int64_t lo = c * chunk, hi = min(n, lo + chunk);
+  const int64_t tiles = (hi - lo + TILE - 1) / TILE;
+  running[tid] = offsets[(int64_t)tid * chunks + c];
+  const unsigned lt_mask = (1u << lane) - 1u;
+  auto skeys = [&](int s) { return (uint64_t*)(smem + s * STAGE); };
+  auto svals = [&](int s) { return (uint32_t*)(smem + s * STAGE + TILE * 8 * W); };
+  // Issues tile t's copies into stage t & 1: whole 16-byte multiples by TMA,
+  // a ragged tail of the array's last tile by the waiting threads.
+  auto issue = [&](int64_t t) {
+    const int s = (int)(t & 1);
+    const int64_t base = lo + t * TILE;
+    const int64_t count = min((int64_t)TILE, hi - base);
+    const int64_t bulk = count & ~(int64_t)3;
+    const uint32_t bytes = (uint32_t)(bulk * 8 * W + (vin ? bulk * 4 : 0));
+    ptx::mbar_expect_tx(&bar[s], bytes);
+    if (bulk) {
+      for (int w = 0; w < W; w++)
+        ptx::bulk_load(skeys(s) + w * TILE, kin + (int64_t)w * ldi + base, (uint32_t)(bulk * 8), &bar[s]);
+      if (vin) ptx::bulk_load(svals(s), vin + base, (uint32_t)(bulk * 4), &bar[s]);
+    }
+  };
+  if (tid == 0) {
+    ptx::mbar_init(&bar[0], 1);
+    ptx::mbar_init(&bar[1], 1);
+    ptx::mbar_fence_init();
+    if (tiles > 0) issue(0);
+    if (tiles > 1) issue(1);
+  }
+  __syncthreads();
+  for (int64_t t = 0; t < tiles; t++) {
+    const int s = (int)(t & 1);
+    const int64_t base = lo + t * TILE;
+    const int64_t count = min((int64_t)TILE, hi - base);
+    const int64_t bulk = count & ~(int64_t)3;
+    if (!ptx::mbar_wait(&bar[s], (uint32_t)((t >> 1) & 1), true)) atomicOr(err, 1);
+    for (int i = tid; i < WARPS * 256; i += kThreads) (&warp_hist[0][0])[i] = 0;
+    __syncthreads();
+    uint64_t key[ITEMS][W];
+    uint32_t val[ITEMS];
+    int digit[ITEMS];
+    unsigned int local[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+      const int off = warp * 32 * ITEMS + i * 32 + lane;
+      if (off < count) {
+        const bool in_smem = off < bulk;
+#pragma unroll
+        for (int w = 0; w < W; w++) key[i][w] = in_smem ? skeys(s)[w * TILE + off] : kin[(int64_t)w * ldi + base + off];
+        val[i] = vin ? (in_smem ? svals(s)[off] : vin[base + off]) : (uint32_t)(base + off);
+        uint64_t wd = key[i][0];
+#pragma unroll
+        for (int w = 1; w < W; w++)
+          if (word == w) wd = key[i][w];
+        digit[i] = (int)((wd >> shift) & 255);
+      } else {
+        digit[i] = 256;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+      const int d = digit[i];
+      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      const unsigned below = __popc(peers & lt_mask);
+      const unsigned old = d < 256 ? warp_hist[warp][d] : 0u;
+      __syncwarp();
+      if (d < 256 && below == 0) warp_hist[warp][d] = old + __popc(peers);
+      __syncwarp();
+      local[i] = old + below;
+    }
+    __syncthreads();  // every item read out of the stage; warp counts complete
+    unsigned int total = 0;
+#pragma unroll
+    for (int w = 0; w < WARPS; w++) {
+      const unsigned cnt = warp_hist[w][tid];
+      warp_hist[w][tid] = total;
+      total += cnt;
+    }
+    unsigned int ex;
+    Scan(tmp).ExclusiveSum(total, ex);
+    tile_start[tid] = ex;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+      const int d = digit[i];
+      if (d < 256) {
+        const unsigned pos = tile_start[d] + warp_hist[warp][d] + local[i];
+#pragma unroll
+        for (int w = 0; w < W; w++) skeys(s)[w * TILE + pos] = key[i][w];
+        svals(s)[pos] = val[i];
+      }
+    }
+    __syncthreads();
+    for (int j = tid; j < count; j += kThreads) {
+      const uint64_t wd = skeys(s)[word * TILE + j];
+      const int d = (int)((wd >> shift) & 255);
+      const long long dst = running[d] + (j - (long long)tile_start[d]);
+#pragma unroll
+      for (int w = 0; w < W; w++) kout[(int64_t)w * ldo + dst] = skeys(s)[w * TILE + j];
+      vout[dst] = svals(s)[j];
+    }
+    __syncthreads();  // the stage is free again
+    running[tid] += total;
+    if (tid == 0 && t + 2 < tiles) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(t + 2);
+    }
+  }
+}
+
+template <int W>
+__global__ void head_flags(const uint64_t* __restrict__ keys, int64_t n, int64_t ld, uint8_t* __restrict__ head) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    bool h = i == 0;
+    if (!h)
+#pragma unroll
+      for (int w = 0; w < W; w++) h |= keys[(int64_t)w * ld + i] != keys[(int64_t)w * ld + i - 1];
+    head[i] = h;
+  }
+}
+
+__global__ void finish_ranks(const uint8_t* __restrict__ head, const int64_t* __restrict__ before,
+                             const uint32_t* __restrict__ rows, int64_t n, uint32_t* __restrict__ rank,
+                             uint32_t* __restrict__ first) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = before[i] + head[i] - 1;
+    rank[rows[i]] = (uint32_t)r;
+    if (head[i]) first[r] = rows[i];
+  }
+}
+
+template <int W>
+int64_t rank_keys_w(Context& ctx, const uint64_t* keys, int64_t n, int64_t ld, uint32_t* rank, uint32_t* first,
+                    cudaStream_t s, uint32_t* sorted_rows) {
+  if (n <= 0) return 0;
+  // TMA bulk copies read 16-byte aligned words: copy keys that aren't.
+  DeviceBuffer<uint64_t> aligned;
+  if (((uintptr_t)keys & 15) || (W > 1 && (ld & 1))) {
+    const int64_t lda = (n + 1) & ~(int64_t)1;
+    aligned.allocate((size_t)(W * lda), s);
+    EF_CUDA(cudaMemcpy2DAsync(aligned.get(), (size_t)lda * 8, keys, (size_t)ld * 8, (size_t)n * 8, W,
+                              cudaMemcpyDeviceToDevice, s));
+    keys = aligned.get();
+    ld = lda;
+  }
+  if (n >= (int64_t)UINT32_MAX) fail(EINFOLD_COMPUTE, "ranking at most 2^32 - 1 rows together");
+  constexpr int ITEMS = W == 1 ? 8 : (W == 2 ? 6 : 4);
+  constexpr int TILE = kThreads * ITEMS;
+  DeviceBuffer<unsigned long long> acc(2 * W, s);
+  {
+    std::vector<unsigned long long> init(2 * W);
+    for (int w = 0; w < W; w++) { init[2 * w] = 0; init[2 * w + 1] = ~0ull; }
+    EF_CUDA(cudaMemcpyAsync(acc.get(), init.data(), init.size() * 8, cudaMemcpyHostToDevice, s));
+    or_and_words<W><<<blocks_for(n, 256), 256, 0, s>>>(keys, n, ld, acc.get());
+    ctx.kernels++;
+    std::vector<unsigned long long> got(2 * W);
+    EF_CUDA(cudaMemcpyAsync(got.data(), acc.get(), got.size() * 8, cudaMemcpyDeviceToHost, s));
+    EF_CUDA(cudaStreamSynchronize(s));
+    init = got;
+    // Passes: least significant byte of the last word first; bytes no key varies in are skipped.
+    std::vector<int> pw, ps;
+    for (int w = W - 1; w >= 0; w--)
+      for (int sh = 0; sh < 64; sh += 8)
+        if (((init[2 * w] ^ init[2 * w + 1]) >> sh) & 0xff) {
+          pw.push_back(w);
+          ps.push_back(sh);
+        }
+    const int passes = (int)pw.size();
+    DeviceBuffer<uint64_t> kb[2];
+    DeviceBuffer<uint32_t> vb[2];
+    const uint64_t* cur_k = keys;
+    int64_t cur_ld = ld;
+    const uint32_t* cur_v = nullptr;
+    if (passes) {
+      const int64_t ldb = (n + 1) & ~(int64_t)1;
+      for (int b = 0; b < 2; b++) {
+        kb[b].allocate((size_t)(W * ldb), s);
+        vb[b].allocate((size_t)n, s);
+      }
+      // Chunks: as many as blocks resident at once, each a whole number of tiles.
+      int per_sm = 0;
+      const size_t smem = 2 * (size_t)TILE * (8 * W + 4);
+      EF_CUDA(cudaFuncSetAttribute(chunk_scatter<W, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      EF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chunk_scatter<W, ITEMS>, kThreads, smem));
+      int64_t chunks = (int64_t)std::max(1, per_sm) * ctx.sm_count;
+      int64_t chunk = ((n + chunks - 1) / chunks + TILE - 1) / TILE * TILE;
+      chunks = (n + chunk - 1) / chunk;
+      DeviceBuffer<unsigned long long> table((size_t)(256 * chunks), s);
+      DeviceBuffer<long long> offsets((size_t)(256 * chunks), s);
+      size_t temp = 0;
+      EF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, table.get(), offsets.get(), (int)(256 * chunks), s));
+      DeviceBuffer<uint8_t> scan_tmp(temp ? temp : 1, s);
+      DeviceBuffer<int> err(1, s);
+      err.zero();
+      for (int p = 0; p < passes; p++) {
+        chunk_counts<<<(unsigned)chunks, kThreads, 0, s>>>(cur_k + (int64_t)pw[p] * cur_ld, n, ps[p], chunk,
+                                                            (int)chunks, table.get());
+        EF_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp.get(), temp, table.get(), offsets.get(), (int)(256 * chunks), s));
+        chunk_scatter<W, ITEMS><<<(unsigned)chunks, kThreads, smem, s>>>(cur_k, cur_v, kb[p & 1].get(), vb[p & 1].get(),
+                                                                         n, cur_ld, ldb, pw[p], ps[p], chunk, (int)chunks,
+                                                                         offsets.get(), err.get());
+        EF_LAUNCH_CHECK();
+        ctx.kernels += 3;
+        cur_k = kb[p & 1].get();
+        cur_ld = ldb;
+        cur_v = vb[p & 1].get();
+      }
+      int e = 0;
+      EF_CUDA(cudaMemcpyAsync(&e, err.get(), 4, cudaMemcpyDeviceToHost, s));
+      EF_CUDA(cudaStreamSynchronize(s));
+      if (e) fail(EINFOLD_TIMEOUT, "a bounded wait in the radix sort ran out");
+    }
+    DeviceBuffer<uint32_t> identity;
+    if (!cur_v) {
+      // No byte varies: every key is the same; rows stay in order.
+      identity.allocate((size_t)n, s);
+      thrust_iota(ctx, identity.get(), n, s);
+      cur_v = identity.get();
+    }
+    DeviceBuffer<uint8_t> head((size_t)n, s);
+    DeviceBuffer<int64_t> before((size_t)n, s);
+    head_flags<W><<<blocks_for(n, 256), 256, 0, s>>>(cur_k, n, cur_ld, head.get());
+    ctx.kernels++;
+    const int64_t distinct = exclusive_scan_flags(ctx, head.get(), n, before.get());
+    finish_ranks<<<blocks_for(n, 256), 256, 0, s>>>(head.get(), before.get(), cur_v, n, rank, first);
+    ctx.kernels++;
+    if (sorted_rows) EF_CUDA(cudaMemcpyAsync(sorted_rows, cur_v, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+    EF_LAUNCH_CHECK();
+    EF_CUDA(cudaStreamSynchronize(s));
+    return distinct;
+  }
+}
+
+}  // namespace
+
+__global__ void iota_kernel(uint32_t* out, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (uint32_t)i;
+}
+
+void thrust_iota(Context& ctx, uint32_t* out, int64_t n, cudaStream_t s) {
+  iota_kernel<<<blocks_for(n, 256), 256, 0, s>>>(out, n);
+  ctx.kernels++;
+}
+
+int64_t rank_keys(Context& ctx, const uint64_t* keys, int words, int64_t n, int64_t ld, uint32_t* rank,
+                  uint32_t* first, cudaStream_t s, uint32_t* sorted_rows) {
+  switch (words) {
+    case 1: return rank_keys_w<1>(ctx, keys, n, ld, rank, first, s, sorted_rows);
+    case 2: return rank_keys_w<2>(ctx, keys, n, ld, rank, first, s, sorted_rows);
+    case 3: return rank_keys_w<3>(ctx, keys, n, ld, rank, first, s, sorted_rows);
+    case 4: return rank_keys_w<4>(ctx, keys, n, ld, rank, first, s, sorted_rows);
+    default: fail(EINFOLD_INVALID, "keys of %d words", words);
+  }
+}
+
+}  // namespace ef

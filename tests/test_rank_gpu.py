@@ -1,0 +1,79 @@
+"""Radix ranking on the GPU against the oracle's restatement of `radix` and
+`ranks_of_words` (discriminate.rs:103-156, 280-292): bit-exact ranks and
+first rows."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from einfold_b200 import _lib
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _rank(words: np.ndarray):
+    import torch
+
+    lib = _lib.load()
+    n = len(words)
+    w = torch.from_numpy(words.view(np.int64)).cuda() if n else torch.zeros(1, dtype=torch.int64, device="cuda")
+    rank = torch.zeros(max(n, 1), dtype=torch.int32, device="cuda")
+    first = torch.zeros(max(n, 1), dtype=torch.int32, device="cuda")
+    k = ctypes.c_int64(-1)
+    torch.cuda.synchronize()
+    st = lib.einfold_rank_words(_lib.context(0), w.data_ptr(), n, rank.data_ptr(), first.data_ptr(), ctypes.byref(k),
+                                None)
+    assert st == _lib.OK, lib.einfold_last_error()
+    return rank.cpu().numpy()[:n].view(np.uint32), first.cpu().numpy()[: k.value].view(np.uint32), k.value
+
+
+def _check(words):
+    got_rank, got_first, k = _rank(words)
+    want = oracle.ranks_of_words(words)
+    assert k == len(want.first)
+    assert np.array_equal(got_rank, want.rank)
+    assert np.array_equal(got_first, want.first)
+    # And what the ranks mean, independently of both implementations.
+    u, first_idx, inv = np.unique(words, return_index=True, return_inverse=True)
+    assert np.array_equal(got_rank, inv.astype(np.uint32))
+    assert np.array_equal(got_first, first_idx.astype(np.uint32))
+
+
+@pytest.mark.parametrize("n", [1, 2, 31, 4095, 4096, 4097, 100_003])
+def test_random_words_with_duplicates(n):
+    rng = oracle.Rng.seeded(n, 1)
+    pool = rng.u64s(max(n // 3, 1))
+    words = pool[(rng.u64s(n) % np.uint64(len(pool))).astype(np.int64)]
+    _check(words)
+
+
+def test_signed_keys_order_by_their_value():
+    rng = oracle.Rng.seeded(5, 2)
+    keys = (rng.u64s(50_000) % np.uint64(2001)).astype(np.int64) - 1000
+    words = keys.view(np.uint64) ^ np.uint64(1 << 63)
+    _check(words)
+    got_rank, got_first, k = _rank(words)
+    assert k == len(np.unique(keys))
+    order = np.argsort(got_rank, kind="stable")
+    assert np.all(np.diff(keys[order]) >= 0)
+
+
+def test_all_equal_and_few_varying_bytes():
+    _check(np.full(10_000, 0xDEADBEEF00000000, dtype=np.uint64))
+    rng = oracle.Rng.seeded(6, 3)
+    low = rng.u64s(70_000) & np.uint64(0xFF)
+    _check((low << np.uint64(40)) | np.uint64(0x1234))
+
+
+def test_zipf_hashes_at_the_sorting_paths_size():
+    # 4M keys over a 200k pool of 63-bit hashes with Zipf(1.1) frequencies.
+    rng = oracle.Rng.seeded(0, 7)
+    pool = rng.u64s(200_000) >> np.uint64(1)
+    ranks = np.arange(1, len(pool) + 1, dtype=np.float64)
+    p = ranks ** -1.1
+    cdf = np.cumsum(p / p.sum())
+    pick = np.searchsorted(cdf, rng.units(4_000_000), side="right").clip(0, len(pool) - 1)
+    keys = pool[pick].view(np.int64)
+    words = keys.view(np.uint64) ^ np.uint64(1 << 63)
+    _check(words)
