@@ -1,0 +1,845 @@
+// The discrimination fold on the device (crates/einfold-kernels/src/discriminate.rs:369-650).
+//
+// 1. Keys as words. Each row's key columns are encoded into fixed-width
+//    bytes that compare (as unsigned words, most significant first) in
+//    Arrow's default order and are equal exactly when the host calls the keys
+//    equal: per column a byte for NULL (0) or valid (1), then integers
+//    sign-flipped big-endian, floats by their total-order bits (-0.0 made 0.0
+//    first under SignedZerosEqual, keys.rs:61-76), strings as their bytes with
+//    0x00 escaped as 0x00 0xFF and two 0x00 after, zero-padded to the longest.
+//    A single non-NULL integer column is its sign-flipped value alone
+//    (discriminate.rs:244-272).
+// 2. Ranks (rank.cu): the join's keys over a‖b, the outputs' over each
+//    operand with the domain's.
+// 3. a's joining rows sorted by (x, z, NULL-first factor bits), b's by (z, y,
+//    factor bits): one stable radix sort each (the reference's two counting
+//    sorts and break_ties, :497-506).
+// 4. Gustavson's product, one block per output key x: its rows of a in order,
+//    each adding p·q into a dense accumulator over y for the rows of b with
+//    its z, in order; rows of b sharing a y are one thread's run, so every
+//    group's terms are added in the reference's order, bit for bit. A first
+//    traversal counts each x's groups, a second fills them, in (x, y) order.
+#include <cub/cub.cuh>
+
+#include <cmath>
+#include <cstring>
+
+#include "fold.h"
+#include "rank.cuh"
+#include "stage.cuh"
+
+namespace ef {
+namespace {
+
+constexpr int kMaxWords = 4;
+
+struct KeyCol {
+  int kind;            // Kind
+  int width;           // bytes of a fixed-width value
+  const uint8_t* data; // fixed-width values, or var-length bytes
+  const int64_t* off;  // var-length offsets
+  const uint8_t* valid;
+  int pad_len;         // var-length: encoded bytes incl. the two terminators, padded
+  int start;           // first byte of this column in the key
+  int canon_zero;      // SignedZerosEqual on a float column
+};
+
+struct KeyCols {
+  int n = 0;
+  KeyCol c[8];
+  int words = 1;
+  int fast_int = 0;    // one non-NULL integer column: sign-flipped value
+};
+
+__device__ __forceinline__ void put_byte(uint64_t* w, int pos, uint8_t b) {
+  w[pos >> 3] |= (uint64_t)b << (8 * (7 - (pos & 7)));
+}
+
+__device__ uint64_t ordered_bits(const KeyCol& c, int64_t r) {
+  switch ((Kind)c.kind) {
+    case Kind::Int8: return (uint64_t)(int64_t)((const int8_t*)c.data)[r] ^ (1ull << 63);
+    case Kind::Int16: return (uint64_t)(int64_t)((const int16_t*)c.data)[r] ^ (1ull << 63);
+    case Kind::Int32: return (uint64_t)(int64_t)((const int32_t*)c.data)[r] ^ (1ull << 63);
+    case Kind::Int64: return (uint64_t)((const int64_t*)c.data)[r] ^ (1ull << 63);
+    case Kind::UInt8: return ((const uint8_t*)c.data)[r];
+    case Kind::UInt16: return ((const uint16_t*)c.data)[r];
+    case Kind::UInt32: return ((const uint32_t*)c.data)[r];
+    case Kind::UInt64: return ((const uint64_t*)c.data)[r];
+    case Kind::Bool: return c.data[r];
+    case Kind::Float16: {
+      uint64_t u = ((const uint16_t*)c.data)[r];
+      if (c.canon_zero && u == 0x8000) u = 0;
+      return ((u & 0x8000) ? (~u & 0xFFFF) : (u | 0x8000)) << 48;
+    }
+    case Kind::Float32: {
+      uint64_t u = ((const uint32_t*)c.data)[r];
+      if (c.canon_zero && u == 0x80000000u) u = 0;
+      return ((u & 0x80000000u) ? (~u & 0xFFFFFFFFu) : (u | 0x80000000u)) << 32;
+    }
+    case Kind::Float64: {
+      uint64_t u = ((const uint64_t*)c.data)[r];
+      if (c.canon_zero && u == 0x8000000000000000ull) u = 0;
+      return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+    }
+    default: return 0;
+  }
+}
+
+__global__ void encode_keys(KeyCols k, int64_t rows, int64_t row0, uint64_t* __restrict__ out, int64_t ld) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t w[kMaxWords] = {0, 0, 0, 0};
+    if (k.fast_int) {
+      w[0] = ordered_bits(k.c[0], r);
+    } else {
+      for (int i = 0; i < k.n; i++) {
+        const KeyCol& c = k.c[i];
+        const bool v = !c.valid || c.valid[r];
+        put_byte(w, c.start, v ? 1 : 0);
+        if (!v) continue;
+        if (c.off) {
+          const int64_t b0 = c.off[r], b1 = c.off[r + 1];
+          int pos = c.start + 1;
+          for (int64_t b = b0; b < b1; b++) {
+            const uint8_t ch = c.data[b];
+            put_byte(w, pos++, ch);
+            if (ch == 0) put_byte(w, pos++, 0xFF);
+          }
+          // two zero terminators and zero padding are already zero
+        } else {
+          const uint64_t bits = ordered_bits(c, r);
+          for (int b = 0; b < 8; b++) put_byte(w, c.start + 1 + b, (uint8_t)(bits >> (8 * (7 - b))));
+        }
+      }
+    }
+    for (int i = 0; i < k.words; i++) out[(int64_t)i * ld + row0 + r] = w[i];
+  }
+}
+
+// The longest escaped string of a column (bytes + one per 0x00).
+__global__ void escaped_max(const uint8_t* __restrict__ data, const int64_t* __restrict__ off,
+                            const uint8_t* __restrict__ valid, int64_t rows, unsigned long long* mx) {
+  unsigned long long local = 0;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    if (valid && !valid[r]) continue;
+    unsigned long long len = 0;
+    for (int64_t b = off[r]; b < off[r + 1]; b++) len += data[b] == 0 ? 2 : 1;
+    local = len > local ? len : local;
+  }
+  for (int o = 16; o; o >>= 1) {
+    unsigned long long x = __shfl_xor_sync(0xffffffffu, local, o);
+    local = x > local ? x : local;
+  }
+  if ((threadIdx.x & 31) == 0 && local) atomicMax(mx, local);
+}
+
+// Rows with no NULL in a key compared with '=' (discriminate.rs:346-356).
+__global__ void joinable_rows(int n_cols, const uint8_t* const* __restrict__ valid, const int* __restrict__ strict,
+                              int64_t rows, uint8_t* __restrict__ ok) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    bool j = true;
+    for (int i = 0; i < n_cols; i++)
+      if (strict[i] && valid[i] && !valid[i][r]) j = false;
+    ok[r] = j;
+  }
+}
+
+// Sort keys of an operand's joining rows: word 0 = (major rank << 32) | minor
+// rank, word 1 = factor valid (NULL first), word 2 = factor bits.
+__global__ void sort_words(const int64_t* __restrict__ pick, int64_t m, const uint32_t* __restrict__ major,
+                           const uint32_t* __restrict__ minor, const double* __restrict__ f,
+                           const uint8_t* __restrict__ fvalid, uint64_t* __restrict__ out, int64_t ld) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = pick[i];
+    const bool v = !fvalid || fvalid[r];
+    out[i] = ((uint64_t)major[r] << 32) | minor[r];
+    out[ld + i] = v ? 1 : 0;
+    out[2 * ld + i] = v ? (uint64_t)__double_as_longlong(f[r]) : 0;
+  }
+}
+
+__global__ void compact_rows(const uint8_t* __restrict__ ok, const int64_t* __restrict__ pos, int64_t rows,
+                             int64_t* __restrict__ pick) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x)
+    if (ok[r]) pick[pos[r]] = r;
+}
+
+// The sorted rows' arrays: rank along `key`, factor value and validity.
+__global__ void lay_out(const uint32_t* __restrict__ order, const int64_t* __restrict__ pick, int64_t m,
+                        const uint32_t* __restrict__ k1, const uint32_t* __restrict__ k2, const double* __restrict__ f,
+                        const uint8_t* __restrict__ fvalid, uint32_t* __restrict__ o1, uint32_t* __restrict__ o2,
+                        double* __restrict__ of, uint8_t* __restrict__ ov, unsigned long long* __restrict__ count1) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = pick[order[i]];
+    o1[i] = k1[r];
+    o2[i] = k2[r];
+    const bool v = !fvalid || fvalid[r];
+    of[i] = v ? f[r] : 0.0;
+    ov[i] = v;
+    atomicAdd(&count1[k1[r]], 1ull);
+  }
+}
+
+// Gustavson's product over x, count (fill == false) or fill (fill == true).
+// acc/flags: per block, a dense accumulator over y (flags: bit 0 reached, bit 1 valued).
+template <bool FILL>
+__global__ void __launch_bounds__(256) gustavson(int64_t nx, int64_t ny, const int64_t* __restrict__ a_start,
+                                                 const uint32_t* __restrict__ a_z, const double* __restrict__ a_f,
+                                                 const uint8_t* __restrict__ a_v, const int64_t* __restrict__ b_start,
+                                                 const uint32_t* __restrict__ b_y, const double* __restrict__ b_f,
+                                                 const uint8_t* __restrict__ b_v, double* __restrict__ acc_all,
+                                                 uint32_t* __restrict__ reached_all, uint32_t* __restrict__ valued_all,
+                                                 int64_t* __restrict__ group_count, const int64_t* __restrict__ group_off,
+                                                 uint32_t* __restrict__ gy, double* __restrict__ gsum,
+                                                 uint8_t* __restrict__ gvalued) {
+  const int64_t words = (ny + 31) / 32;
+  double* acc = acc_all + (FILL ? (int64_t)blockIdx.x * ny : 0);
+  uint32_t* reached = reached_all + (int64_t)blockIdx.x * words;
+  uint32_t* valued = valued_all + (int64_t)blockIdx.x * words;
+  __shared__ unsigned long long s_count;
+  for (int64_t x = blockIdx.x; x < nx; x += gridDim.x) {
+    for (int64_t i = a_start[x]; i < a_start[x + 1]; i++) {
+      const uint32_t z = a_z[i];
+      const double p = a_f[i];
+      const bool pv = a_v[i] != 0;
+      const int64_t j0 = b_start[z], j1 = b_start[z + 1];
+      for (int64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+        const uint32_t y = b_y[j];
+        if (j > j0 && b_y[j - 1] == y) continue;  // not the first of its run
+        // This thread's run: every row of b with this z and y, in order.
+        bool any = false;
+        double s = FILL ? acc[y] : 0.0;
+        for (int64_t q = j; q < j1 && b_y[q] == y; q++) {
+          if (pv && b_v[q]) {
+            if (FILL) s = __dadd_rn(s, __dmul_rn(p, b_f[q]));
+            any = true;
+          }
+        }
+        const uint32_t bit = 1u << (y & 31);
+        if (!(reached[y >> 5] & bit)) atomicOr(&reached[y >> 5], bit);
+        if (any) {
+          if (FILL) acc[y] = s;
+          if (!(valued[y >> 5] & bit)) atomicOr(&valued[y >> 5], bit);
+        }
+      }
+      __syncthreads();
+    }
+    // The groups of x, in y order: count, or write and clear.
+    if (threadIdx.x == 0) s_count = 0;
+    __syncthreads();
+    if (!FILL) {
+      unsigned long long c = 0;
+      for (int64_t w = threadIdx.x; w < words; w += blockDim.x) {
+        c += __popc(reached[w]);
+        reached[w] = 0;
+        valued[w] = 0;
+      }
+      atomicAdd(&s_count, c);
+      __syncthreads();
+      if (threadIdx.x == 0) group_count[x] = (int64_t)s_count;
+    } else {
+      // Ordered emission: one warp walks the words in order, lanes spread
+      // over the set bits of each word by prefix counts.
+      if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        int64_t out = group_off[x];
+        for (int64_t w0 = 0; w0 < words; w0 += 32) {
+          const int64_t w = w0 + lane;
+          const uint32_t bits = w < words ? reached[w] : 0u;
+          const uint32_t vb = w < words ? valued[w] : 0u;
+          const int cnt = __popc(bits);
+          int pre = cnt;
+          for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, pre, o);
+            if (lane >= o) pre += t;
+          }
+          const int total = __shfl_sync(0xffffffffu, pre, 31);
+          int64_t pos = out + pre - cnt;
+          uint32_t b = bits;
+          while (b) {
+            const int k = __ffs(b) - 1;
+            b &= b - 1;
+            const uint32_t y = (uint32_t)(w * 32 + k);
+            gy[pos] = y;
+            const bool v = (vb >> k) & 1u;
+            gsum[pos] = v ? acc[y] : 0.0;
+            gvalued[pos] = v;
+            acc[y] = 0.0;
+            pos++;
+          }
+          if (w < words) {
+            reached[w] = 0;
+            valued[w] = 0;
+          }
+          out += total;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void fill_x(const int64_t* __restrict__ off, int64_t nx, uint32_t* __restrict__ gx) {
+  for (int64_t x = blockIdx.x; x < nx; x += gridDim.x)
+    for (int64_t g = off[x] + threadIdx.x; g < off[x + 1]; g += blockDim.x) gx[g] = (uint32_t)x;
+}
+
+// Fixed-width gather of a key column by row (take), with validity bytes.
+__global__ void gather_fixed(const uint8_t* __restrict__ data, const uint8_t* __restrict__ valid, int width,
+                             int canon_zero, const uint32_t* __restrict__ first, const uint32_t* __restrict__ g,
+                             int64_t n, uint8_t* __restrict__ out, uint8_t* __restrict__ ovalid,
+                             unsigned long long* __restrict__ nulls) {
+  unsigned long long local = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = first[g[i]];
+    const bool v = !valid || valid[r];
+    ovalid[i] = v;
+    local += !v;
+    switch (width) {
+      case 1: out[i] = data[r]; break;
+      case 2: ((uint16_t*)out)[i] = ((const uint16_t*)data)[r]; break;
+      case 4: {
+        uint32_t u = ((const uint32_t*)data)[r];
+        if (canon_zero && u == 0x80000000u) u = 0;
+        ((uint32_t*)out)[i] = u;
+        break;
+      }
+      default: {
+        uint64_t u = ((const uint64_t*)data)[r];
+        if (canon_zero && u == 0x8000000000000000ull) u = 0;
+        ((uint64_t*)out)[i] = u;
+      }
+    }
+  }
+  if (local) atomicAdd(nulls, local);
+}
+
+__global__ void gather_valid(const uint8_t* __restrict__ valid, const uint32_t* __restrict__ first,
+                             const uint32_t* __restrict__ g, int64_t n, uint8_t* __restrict__ ovalid,
+                             unsigned long long* __restrict__ nulls) {
+  unsigned long long local = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const bool v = !valid || valid[first[g[i]]];
+    ovalid[i] = v;
+    local += !v;
+  }
+  if (local) atomicAdd(nulls, local);
+}
+
+__global__ void gather_lengths(const int64_t* __restrict__ off, const uint32_t* __restrict__ first,
+                               const uint32_t* __restrict__ g, int64_t n, int64_t* __restrict__ len) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = first[g[i]];
+    len[i] = off[r + 1] - off[r];
+  }
+}
+
+__global__ void gather_bytes(const uint8_t* __restrict__ data, const int64_t* __restrict__ off,
+                             const uint32_t* __restrict__ first, const uint32_t* __restrict__ g,
+                             const int64_t* __restrict__ out_off, int64_t n, uint8_t* __restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = first[g[i]];
+    const int64_t b0 = off[r], len = off[r + 1] - b0, o = out_off[i];
+    for (int64_t b = 0; b < len; b++) out[o + b] = data[b0 + b];
+  }
+}
+
+// A domain row's value: its (x, y) group's sum when the group exists with a
+// value, else the default (discriminate.rs:613-649).
+__global__ void domain_lookup(int64_t rows, const uint32_t* __restrict__ xr, const uint32_t* __restrict__ yr,
+                              const uint8_t* __restrict__ matches, int64_t nx, const int64_t* __restrict__ goff,
+                              const uint32_t* __restrict__ gy, const double* __restrict__ gsum,
+                              const uint8_t* __restrict__ gval, int has_missing, double missing,
+                              double* __restrict__ val, uint8_t* __restrict__ valid) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    bool found = false;
+    double v = 0.0;
+    const uint32_t x = xr ? xr[r] : 0u, y = yr ? yr[r] : 0u;
+    if (matches[r] && (int64_t)x < nx) {
+      int64_t lo = goff[x], hi = goff[x + 1];
+      while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (gy[mid] < y) lo = mid + 1; else hi = mid;
+      }
+      if (lo < goff[x + 1] && gy[lo] == y && gval[lo]) {
+        found = true;
+        v = gsum[lo];
+      }
+    }
+    val[r] = found ? v : (has_missing ? missing : 0.0);
+    valid[r] = found || has_missing;
+  }
+}
+
+// One set of key columns from a relation (rows of every batch), staged.
+struct StagedKeySet {
+  std::vector<DeviceColumn> cols;
+  std::vector<Kind> kinds;
+};
+
+StagedKeySet stage_set(Context& ctx, const Relation& r, const std::vector<int>& cols) {
+  StagedKeySet s;
+  for (int c : cols) {
+    const Field& f = r.fields[c];
+    if (f.dictionary) fail(EINFOLD_COMPUTE, "dictionary-encoded keys are not supported by the device fold");
+    s.cols.push_back(stage_column(ctx, r, c, true));
+    s.kinds.push_back(f.kind);
+  }
+  return s;
+}
+
+// Encodes the rows of `sets` (same columns' types each, concatenated in order)
+// into words; returns the word count and the layout stride.
+int encode_sets(Context& ctx, const std::vector<const StagedKeySet*>& sets, int float_keys, int64_t total,
+                DeviceBuffer<uint64_t>& words, int64_t* ld_out) {
+  cudaStream_t s = ctx.stream;
+  const int n_cols = sets.empty() ? 0 : (int)sets[0]->cols.size();
+  if (n_cols > 8) fail(EINFOLD_COMPUTE, "more than 8 key columns");
+  const int64_t ld = (total + 1) & ~(int64_t)1;
+  *ld_out = ld;
+  // Fast path: one integer column with no NULLs anywhere.
+  bool fast = n_cols == 1 && is_integer(sets[0]->kinds[0]);
+  if (fast)
+    for (auto* st : sets) fast = fast && st->cols[0].nulls == 0;
+  int bytes = 0;
+  std::vector<int> start(n_cols), pad(n_cols, 0);
+  for (int i = 0; i < n_cols; i++) {
+    start[i] = bytes;
+    const Kind k = sets[0]->kinds[i];
+    if (is_var(k)) {
+      unsigned long long mx = 0;
+      DeviceBuffer<unsigned long long> dmx(1, s);
+      dmx.zero();
+      for (auto* st : sets) {
+        const DeviceColumn& c = st->cols[i];
+        if (c.rows)
+          escaped_max<<<blocks_for(c.rows, 256), 256, 0, s>>>(c.bytes.get(), c.offsets.get(), c.valid.get(), c.rows,
+                                                              dmx.get());
+      }
+      EF_CUDA(cudaMemcpyAsync(&mx, dmx.get(), 8, cudaMemcpyDeviceToHost, s));
+      EF_CUDA(cudaStreamSynchronize(s));
+      pad[i] = (int)mx + 2;
+      bytes += 1 + pad[i];
+    } else {
+      bytes += 1 + 8;
+    }
+  }
+  const int nwords = fast ? 1 : std::max(1, (bytes + 7) / 8);
+  if (nwords > kMaxWords) fail(EINFOLD_COMPUTE, "keys longer than %d bytes are not supported by the device fold", 8 * kMaxWords);
+  words.allocate((size_t)(nwords * ld ? nwords * ld : 1), s);
+  if (nwords * ld) words.zero();
+  int64_t row0 = 0;
+  for (auto* st : sets) {
+    KeyCols kc;
+    kc.n = n_cols;
+    kc.words = nwords;
+    kc.fast_int = fast;
+    int64_t rows = n_cols ? st->cols[0].rows : 0;
+    for (int i = 0; i < n_cols; i++) {
+      const DeviceColumn& c = st->cols[i];
+      KeyCol& k = kc.c[i];
+      k.kind = (int)c.kind;
+      k.width = c.width;
+      k.data = is_var(c.kind) ? c.bytes.get() : c.ptr();
+      k.off = is_var(c.kind) ? c.offsets.get() : nullptr;
+      k.valid = c.valid.get();
+      k.pad_len = pad[i];
+      k.start = start[i];
+      k.canon_zero = float_keys == 1 && is_float(c.kind);
+    }
+    if (rows) {
+      encode_keys<<<blocks_for(rows, 256), 256, 0, s>>>(kc, rows, row0, words.get(), ld);
+      ctx.kernels++;
+    }
+    row0 += rows;
+  }
+  (void)total;
+  EF_LAUNCH_CHECK();
+  return nwords;
+}
+
+struct RankSet {
+  DeviceBuffer<uint32_t> rank;
+  DeviceBuffer<uint32_t> first;
+  int64_t count = 0;
+};
+
+RankSet rank_sets(Context& ctx, const std::vector<const StagedKeySet*>& sets, int64_t total, int float_keys) {
+  RankSet r;
+  cudaStream_t s = ctx.stream;
+  r.rank.allocate((size_t)(total ? total : 1), s);
+  r.first.allocate((size_t)(total ? total : 1), s);
+  if (total == 0) return r;
+  const int n_cols = sets.empty() ? 0 : (int)sets[0]->cols.size();
+  if (n_cols == 0) {
+    // No columns: every key is empty, one rank, first row 0.
+    EF_CUDA(cudaMemsetAsync(r.rank.get(), 0, (size_t)total * 4, s));
+    EF_CUDA(cudaMemsetAsync(r.first.get(), 0, 4, s));
+    r.count = 1;
+    return r;
+  }
+  DeviceBuffer<uint64_t> words;
+  int64_t ld = 0;
+  const int nw = encode_sets(ctx, sets, float_keys, total, words, &ld);
+  r.count = rank_keys(ctx, words.get(), nw, total, ld, r.rank.get(), r.first.get(), s);
+  return r;
+}
+
+}  // namespace
+
+FoldOutput discriminate_fold(Context& ctx, const FoldD& f, const Relation& a, const Relation& b,
+                             const Relation* domain, const std::vector<Field>& schema, const einfold_options& o,
+                             Budget& budget) {
+  cudaStream_t s = ctx.stream;
+  if (f.operands.size() != 2) fail(EINFOLD_INVALID, "the discrimination algorithm folds two operands");
+  if (f.row_expr) fail(EINFOLD_COMPUTE, "row expressions are folded by the fused pipeline only");
+  const int64_t na = a.rows(), nb = b.rows();
+  const int64_t nd = domain ? domain->rows() : 0;
+  if (std::max(na + nb, std::max(na, nb) + nd) >= (int64_t)UINT32_MAX)
+    fail(EINFOLD_COMPUTE, "EinFold's discrimination algorithm ranks at most 2^32 - 1 rows together");
+  const OperandD& oa = f.operands[0];
+  const OperandD& ob = f.operands[1];
+  std::vector<int> shared;
+  for (int d = 0; d < f.n_dims(); d++)
+    if (oa.holds(d) && ob.holds(d)) shared.push_back(d);
+  std::vector<int> a_out, b_out;
+  for (size_t i = 0; i < f.outputs.size(); i++) (oa.holds(f.outputs[i].dim) ? a_out : b_out).push_back((int)i);
+  auto factor_ok = [&](const OperandD& op, const Relation& r) {
+    return op.factor >= 0 && r.fields[op.factor].kind == Kind::Float64 && !r.fields[op.factor].dictionary;
+  };
+  if (!factor_ok(oa, a) || !factor_ok(ob, b)) fail(EINFOLD_INVALID, "factors must be Float64");
+  // The reference's estimate of what ranking and ordering allocate (:414-437).
+  const uint64_t ranked = sat_add(sat_mul((uint64_t)(na + nb), 2), sat_mul((uint64_t)nd, 2));
+  budget.reserve(sat_add(sat_mul(ranked, 28), sat_mul((uint64_t)(na + nb), 40)), "the discrimination algorithm's ranks");
+
+  auto cols_of = [&](const OperandD& op, const std::vector<int>& dims) {
+    std::vector<int> c;
+    for (int d : dims) c.push_back(op.column_of(d));
+    return c;
+  };
+  std::vector<int> a_out_dims, b_out_dims;
+  for (int i : a_out) a_out_dims.push_back(f.outputs[i].dim);
+  for (int i : b_out) b_out_dims.push_back(f.outputs[i].dim);
+  StagedKeySet a_sh = stage_set(ctx, a, cols_of(oa, shared)), b_sh = stage_set(ctx, b, cols_of(ob, shared));
+  StagedKeySet a_o = stage_set(ctx, a, cols_of(oa, a_out_dims)), b_o = stage_set(ctx, b, cols_of(ob, b_out_dims));
+  StagedKeySet d_a, d_b;
+  if (domain) {
+    std::vector<int> da, db;
+    for (int i : a_out) da.push_back(f.outputs[i].domain_col);
+    for (int i : b_out) db.push_back(f.outputs[i].domain_col);
+    d_a = stage_set(ctx, *domain, da);
+    d_b = stage_set(ctx, *domain, db);
+  }
+  ctx.phase("discriminate: staged");
+  // Joinable rows: no NULL in a key compared with '='.
+  auto joinable = [&](const StagedKeySet& ks, int64_t rows, DeviceBuffer<uint8_t>& ok) {
+    ok.allocate((size_t)(rows ? rows : 1), s);
+    std::vector<const uint8_t*> valid;
+    std::vector<int> strict;
+    for (size_t i = 0; i < ks.cols.size(); i++) {
+      valid.push_back(ks.cols[i].valid.get());
+      strict.push_back(f.equality[shared[i]] == 0);
+    }
+    DeviceBuffer<const uint8_t*> dv(std::max<size_t>(1, valid.size()), s);
+    DeviceBuffer<int> ds(std::max<size_t>(1, strict.size()), s);
+    if (!valid.empty()) {
+      EF_CUDA(cudaMemcpyAsync(dv.get(), valid.data(), valid.size() * sizeof(void*), cudaMemcpyHostToDevice, s));
+      EF_CUDA(cudaMemcpyAsync(ds.get(), strict.data(), strict.size() * 4, cudaMemcpyHostToDevice, s));
+    }
+    if (rows) joinable_rows<<<blocks_for(rows, 256), 256, 0, s>>>((int)valid.size(), dv.get(), ds.get(), rows, ok.get());
+    EF_CUDA(cudaStreamSynchronize(s));
+  };
+  DeviceBuffer<uint8_t> a_ok, b_ok;
+  joinable(a_sh, na, a_ok);
+  joinable(b_sh, nb, b_ok);
+  // Ranks.
+  RankSet z = rank_sets(ctx, {&a_sh, &b_sh}, na + nb, o.float_keys);
+  RankSet x = domain && !a_out.empty() ? rank_sets(ctx, {&a_o, &d_a}, na + nd, o.float_keys)
+                                       : rank_sets(ctx, {&a_o}, na, o.float_keys);
+  RankSet y = domain && !b_out.empty() ? rank_sets(ctx, {&b_o, &d_b}, nb + nd, o.float_keys)
+                                       : rank_sets(ctx, {&b_o}, nb, o.float_keys);
+  if (domain && a_out.empty()) {  // no a outputs: every domain row has the one rank 0
+    RankSet xx;
+    xx.rank.allocate((size_t)(na + nd + 1), s);
+    EF_CUDA(cudaMemsetAsync(xx.rank.get(), 0, (size_t)(na + nd + 1) * 4, s));
+    xx.first = std::move(x.first);
+    xx.count = x.count;
+    x = std::move(xx);
+  }
+  if (domain && b_out.empty()) {
+    RankSet yy;
+    yy.rank.allocate((size_t)(nb + nd + 1), s);
+    EF_CUDA(cudaMemsetAsync(yy.rank.get(), 0, (size_t)(nb + nd + 1) * 4, s));
+    yy.first = std::move(y.first);
+    yy.count = y.count;
+    y = std::move(yy);
+  }
+  const int64_t nx = std::max<int64_t>(x.count, 1), nz = std::max<int64_t>(z.count, 1),
+                ny = std::max<int64_t>(y.count, 1);
+  ctx.phase("discriminate: ranked");
+
+  // a's joining rows by (x, z, factor bits), b's by (z, y, factor bits).
+  DeviceColumn af = stage_column(ctx, a, oa.factor), bf = stage_column(ctx, b, ob.factor);
+  auto order_rows = [&](int64_t rows, const DeviceBuffer<uint8_t>& ok, const uint32_t* major, const uint32_t* minor,
+                        const DeviceColumn& fc, int64_t n_major, DeviceBuffer<uint32_t>& o_major,
+                        DeviceBuffer<uint32_t>& o_minor, DeviceBuffer<double>& o_f, DeviceBuffer<uint8_t>& o_v,
+                        DeviceBuffer<int64_t>& start) -> int64_t {
+    DeviceBuffer<int64_t> pos((size_t)(rows ? rows : 1), s);
+    const int64_t m = exclusive_scan_flags(ctx, ok.get(), rows, pos.get());
+    DeviceBuffer<int64_t> pick((size_t)(m ? m : 1), s);
+    if (rows) compact_rows<<<blocks_for(rows, 256), 256, 0, s>>>(ok.get(), pos.get(), rows, pick.get());
+    const int64_t ld = (m + 1) & ~(int64_t)1;
+    DeviceBuffer<uint64_t> w((size_t)(3 * ld ? 3 * ld : 1), s);
+    DeviceBuffer<uint32_t> order((size_t)(m ? m : 1), s), rk((size_t)(m ? m : 1), s), fi((size_t)(m ? m : 1), s);
+    o_major.allocate((size_t)(m ? m : 1), s);
+    o_minor.allocate((size_t)(m ? m : 1), s);
+    o_f.allocate((size_t)(m ? m : 1), s);
+    o_v.allocate((size_t)(m ? m : 1), s);
+    DeviceBuffer<unsigned long long> counts((size_t)n_major + 1, s);
+    counts.zero();
+    if (m) {
+      sort_words<<<blocks_for(m, 256), 256, 0, s>>>(pick.get(), m, major, minor, (const double*)fc.ptr(),
+                                                    fc.valid.get(), w.get(), ld);
+      rank_keys(ctx, w.get(), 3, m, ld, rk.get(), fi.get(), s, order.get());
+      lay_out<<<blocks_for(m, 256), 256, 0, s>>>(order.get(), pick.get(), m, major, minor, (const double*)fc.ptr(),
+                                                 fc.valid.get(), o_major.get(), o_minor.get(), o_f.get(), o_v.get(),
+                                                 counts.get());
+      ctx.kernels += 3;
+    }
+    start.allocate((size_t)n_major + 1, s);
+    EF_CUDA(cudaMemsetAsync(start.get(), 0, 8, s));
+    size_t temp = 0;
+    EF_CUDA(cub::DeviceScan::InclusiveSum(nullptr, temp, counts.get(), (unsigned long long*)start.get() + 1, (int)n_major, s));
+    DeviceBuffer<uint8_t> t(temp ? temp : 1, s);
+    EF_CUDA(cub::DeviceScan::InclusiveSum(t.get(), temp, counts.get(), (unsigned long long*)start.get() + 1, (int)n_major, s));
+    EF_LAUNCH_CHECK();
+    return m;
+  };
+  DeviceBuffer<uint32_t> a_x, a_z, b_z, b_y;
+  DeviceBuffer<double> a_f, b_f;
+  DeviceBuffer<uint8_t> a_v, b_v;
+  DeviceBuffer<int64_t> a_start, b_start;
+  const int64_t ma = order_rows(na, a_ok, x.rank.get(), z.rank.get(), af, nx, a_x, a_z, a_f, a_v, a_start);
+  const int64_t mb = order_rows(nb, b_ok, z.rank.get() + na, y.rank.get(), bf, nz, b_z, b_y, b_f, b_v, b_start);
+  (void)ma;
+  (void)mb;
+  ctx.phase("discriminate: ordered");
+
+  // Gustavson's product: count, offsets, fill.
+  const int64_t words = (ny + 31) / 32;
+  int blocks = std::min<int64_t>(nx, (int64_t)ctx.sm_count * 4);
+  while (blocks > 1 && (uint64_t)blocks * (uint64_t)(ny * 8 + words * 8) > (4ull << 30)) blocks /= 2;
+  budget.reserve(sat_mul((uint64_t)blocks, (uint64_t)(ny * 8 + words * 8)), "the discrimination algorithm's accumulators");
+  DeviceBuffer<uint32_t> reached((size_t)(blocks * words), s), valued((size_t)(blocks * words), s);
+  reached.zero();
+  valued.zero();
+  DeviceBuffer<int64_t> gcount((size_t)nx, s), goff((size_t)nx + 1, s);
+  gustavson<false><<<blocks, 256, 0, s>>>(nx, ny, a_start.get(), a_z.get(), a_f.get(), a_v.get(), b_start.get(),
+                                          b_y.get(), b_f.get(), b_v.get(), nullptr, reached.get(), valued.get(),
+                                          gcount.get(), nullptr, nullptr, nullptr, nullptr);
+  ctx.kernels++;
+  EF_LAUNCH_CHECK();
+  EF_CUDA(cudaMemsetAsync(goff.get(), 0, 8, s));
+  {
+    size_t temp = 0;
+    EF_CUDA(cub::DeviceScan::InclusiveSum(nullptr, temp, gcount.get(), goff.get() + 1, (int)nx, s));
+    DeviceBuffer<uint8_t> t(temp ? temp : 1, s);
+    EF_CUDA(cub::DeviceScan::InclusiveSum(t.get(), temp, gcount.get(), goff.get() + 1, (int)nx, s));
+  }
+  int64_t groups = 0;
+  EF_CUDA(cudaMemcpyAsync(&groups, goff.get() + nx, 8, cudaMemcpyDeviceToHost, s));
+  EF_CUDA(cudaStreamSynchronize(s));
+  const uint64_t out_bytes = f.domain ? (uint64_t)nd * 8 : sat_mul((uint64_t)groups, 8 * (f.outputs.size() + 1));
+  budget.reserve(sat_add(sat_mul((uint64_t)groups, 24), out_bytes), "the discrimination algorithm's groups");
+  DeviceBuffer<double> acc((size_t)blocks * ny, s);
+  acc.zero();
+  DeviceBuffer<uint32_t> gy((size_t)(groups ? groups : 1), s), gx((size_t)(groups ? groups : 1), s);
+  DeviceBuffer<double> gsum((size_t)(groups ? groups : 1), s);
+  DeviceBuffer<uint8_t> gval((size_t)(groups ? groups : 1), s);
+  gustavson<true><<<blocks, 256, 0, s>>>(nx, ny, a_start.get(), a_z.get(), a_f.get(), a_v.get(), b_start.get(),
+                                         b_y.get(), b_f.get(), b_v.get(), acc.get(), reached.get(), valued.get(),
+                                         nullptr, goff.get(), gy.get(), gsum.get(), gval.get());
+  ctx.kernels++;
+  EF_LAUNCH_CHECK();
+  ctx.phase("discriminate: product");
+
+  FoldOutput result;
+  result.algorithm = EINFOLD_ALG_DISCRIMINATE;
+  if (f.domain) {
+    if (!domain) fail(EINFOLD_INVALID, "a fold with a domain was given no domain relation");
+    if (o.result_on_device) fail(EINFOLD_INVALID, "results in device memory are not supported with a domain");
+    const DomainD& spec = *f.domain;
+    // Domain rows joinable under each output's domain equality.
+    std::vector<int> all_cols;
+    for (auto& out : f.outputs) all_cols.push_back(out.domain_col);
+    StagedKeySet dk = stage_set(ctx, *domain, all_cols);
+    DeviceBuffer<uint8_t> matches((size_t)(nd ? nd : 1), s);
+    {
+      std::vector<const uint8_t*> valid;
+      std::vector<int> strict;
+      for (size_t i = 0; i < f.outputs.size(); i++) {
+        valid.push_back(dk.cols[i].valid.get());
+        strict.push_back(f.outputs[i].domain_eq == 0);
+      }
+      DeviceBuffer<const uint8_t*> dv(std::max<size_t>(1, valid.size()), s);
+      DeviceBuffer<int> ds(std::max<size_t>(1, strict.size()), s);
+      if (!valid.empty()) {
+        EF_CUDA(cudaMemcpyAsync(dv.get(), valid.data(), valid.size() * sizeof(void*), cudaMemcpyHostToDevice, s));
+        EF_CUDA(cudaMemcpyAsync(ds.get(), strict.data(), strict.size() * 4, cudaMemcpyHostToDevice, s));
+      }
+      if (nd) joinable_rows<<<blocks_for(nd, 256), 256, 0, s>>>((int)valid.size(), dv.get(), ds.get(), nd, matches.get());
+    }
+    DeviceBuffer<double> val((size_t)(nd ? nd : 1), s);
+    DeviceBuffer<uint8_t> valid((size_t)(nd ? nd : 1), s);
+    if (nd)
+      domain_lookup<<<blocks_for(nd, 256), 256, 0, s>>>(nd, x.rank.get() + na, y.rank.get() + nb, matches.get(), nx,
+                                                        goff.get(), gy.get(), gsum.get(), gval.get(), spec.has_missing,
+                                                        spec.missing, val.get(), valid.get());
+    EF_LAUNCH_CHECK();
+    HostBuffer hv = to_host(ctx, val.get(), (size_t)nd * 8);
+    HostBuffer hvalid = to_host(ctx, valid.get(), (size_t)nd);
+    int64_t off = 0;
+    for (auto& batch : domain->batches) {
+      OutBatch ob2;
+      ob2.rows = batch.rows;
+      for (size_t i = 0; i < spec.carry.size(); i++) {
+        OutColumn c = copy_column(batch.columns[spec.carry[i]], domain->fields[spec.carry[i]]);
+        c.format = schema[i].format;
+        c.name = schema[i].name;
+        ob2.columns.push_back(std::move(c));
+      }
+      OutColumn v;
+      v.format = "g";
+      v.kind = Kind::Float64;
+      v.name = schema.back().name;
+      v.length = batch.rows;
+      v.values = Buffer(HostBuffer((size_t)batch.rows * 8));
+      if (batch.rows) std::memcpy(v.values.ptr, hv.as<double>() + off, (size_t)batch.rows * 8);
+      int64_t nulls = 0;
+      for (int64_t i = 0; i < batch.rows; i++) nulls += !hvalid.as<uint8_t>()[off + i];
+      v.null_count = nulls;
+      if (nulls) {
+        v.validity = Buffer(HostBuffer((size_t)(batch.rows + 7) / 8));
+        std::memset(v.validity.ptr, 0, v.validity.bytes);
+        for (int64_t i = 0; i < batch.rows; i++)
+          if (hvalid.as<uint8_t>()[off + i]) v.validity.as<uint8_t>()[i >> 3] |= (uint8_t)(1u << (i & 7));
+      }
+      ob2.columns.push_back(std::move(v));
+      result.batches.push_back(std::move(ob2));
+      off += batch.rows;
+    }
+    return result;
+  }
+
+  // Groups' keys from a row of a or b that has them (take of first rows).
+  if (groups) {
+    fill_x<<<std::min<int64_t>(nx, 65535), 256, 0, s>>>(goff.get(), nx, gx.get());
+    ctx.kernels++;
+  }
+  OutBatch out_batch;
+  out_batch.rows = groups;
+  for (size_t i = 0; i < f.outputs.size(); i++) {
+    const bool from_a = oa.holds(f.outputs[i].dim);
+    const std::vector<int>& outs = from_a ? a_out : b_out;
+    size_t j = 0;
+    while (outs[j] != (int)i) j++;
+    const DeviceColumn& src = (from_a ? a_o : b_o).cols[j];
+    const uint32_t* first = from_a ? x.first.get() : y.first.get();
+    const uint32_t* g = from_a ? gx.get() : gy.get();
+    OutColumn c;
+    c.format = schema[i].format;
+    c.name = schema[i].name;
+    c.kind = schema[i].kind;
+    c.nullable = schema[i].nullable;
+    c.length = groups;
+    DeviceBuffer<uint8_t> cvalid((size_t)(groups ? groups : 1), s);
+    DeviceBuffer<unsigned long long> cn(1, s);
+    cn.zero();
+    if (is_var(src.kind)) {
+      DeviceBuffer<int64_t> len((size_t)(groups ? groups : 1), s), offs((size_t)groups + 1, s);
+      if (groups) {
+        gather_lengths<<<blocks_for(groups, 256), 256, 0, s>>>(src.offsets.get(), first, g, groups, len.get());
+        EF_CUDA(cudaMemsetAsync(offs.get(), 0, 8, s));
+        size_t temp = 0;
+        EF_CUDA(cub::DeviceScan::InclusiveSum(nullptr, temp, len.get(), offs.get() + 1, (int)groups, s));
+        DeviceBuffer<uint8_t> t(temp ? temp : 1, s);
+        EF_CUDA(cub::DeviceScan::InclusiveSum(t.get(), temp, len.get(), offs.get() + 1, (int)groups, s));
+      } else {
+        EF_CUDA(cudaMemsetAsync(offs.get(), 0, 8, s));
+      }
+      int64_t total = 0;
+      EF_CUDA(cudaMemcpyAsync(&total, offs.get() + groups, 8, cudaMemcpyDeviceToHost, s));
+      EF_CUDA(cudaStreamSynchronize(s));
+      DeviceBuffer<uint8_t> bytes((size_t)(total ? total : 1), s);
+      if (groups) {
+        gather_bytes<<<blocks_for(groups, 256), 256, 0, s>>>(src.bytes.get(), src.offsets.get(), first, g, offs.get(),
+                                                             groups, bytes.get());
+        gather_valid<<<blocks_for(groups, 256), 256, 0, s>>>(src.valid.get(), first, g, groups, cvalid.get(), cn.get());
+      }
+      const bool large = src.kind == Kind::LargeUtf8 || src.kind == Kind::LargeBinary;
+      HostBuffer ho = to_host(ctx, offs.get(), (size_t)(groups + 1) * 8);
+      if (large) {
+        c.values = Buffer(std::move(ho));
+      } else {
+        if (total > INT32_MAX) fail(EINFOLD_COMPUTE, "string output over 2 GiB");
+        HostBuffer h32((size_t)(groups + 1) * 4);
+        for (int64_t q = 0; q <= groups; q++) h32.as<int32_t>()[q] = (int32_t)ho.as<int64_t>()[q];
+        c.values = Buffer(std::move(h32));
+      }
+      c.data = Buffer(to_host(ctx, bytes.get(), (size_t)total));
+    } else {
+      const int width = width_of(src.kind) ? width_of(src.kind) : 1;
+      DeviceBuffer<uint8_t> vals((size_t)(groups ? groups * width : 1), s);
+      if (groups)
+        gather_fixed<<<blocks_for(groups, 256), 256, 0, s>>>(src.ptr(), src.valid.get(), width,
+                                                             o.float_keys == 1 && is_float(src.kind), first, g, groups,
+                                                             vals.get(), cvalid.get(), cn.get());
+      c.values = result_buffer(ctx, vals, (size_t)(groups * width), o.result_on_device);
+    }
+    unsigned long long cnulls = 0;
+    EF_CUDA(cudaMemcpyAsync(&cnulls, cn.get(), 8, cudaMemcpyDeviceToHost, s));
+    EF_CUDA(cudaStreamSynchronize(s));
+    c.null_count = (int64_t)cnulls;
+    if (cnulls) {
+      DeviceBuffer<uint8_t> bits((size_t)((groups + 7) / 8), s);
+      pack_bits(ctx, cvalid.get(), groups, bits.get());
+      c.validity = result_buffer(ctx, bits, (size_t)((groups + 7) / 8), o.result_on_device);
+    }
+    out_batch.columns.push_back(std::move(c));
+  }
+  OutColumn v;
+  v.format = "g";
+  v.kind = Kind::Float64;
+  v.name = schema.back().name;
+  v.length = groups;
+  DeviceBuffer<uint8_t> vbits((size_t)((groups + 7) / 8 ? (groups + 7) / 8 : 1), s);
+  unsigned long long vnulls = 0;
+  {
+    DeviceBuffer<unsigned long long> cnt(1, s);
+    cnt.zero();
+    // NULL where no product had a value.
+    DeviceBuffer<uint8_t> inv((size_t)(groups ? groups : 1), s);
+    if (groups) {
+      pack_bits(ctx, gval.get(), groups, vbits.get());
+      size_t temp = 0;
+      cub::TransformInputIterator<unsigned long long, cub::CastOp<unsigned long long>, const uint8_t*> it(
+          gval.get(), cub::CastOp<unsigned long long>());
+      EF_CUDA(cub::DeviceReduce::Sum(nullptr, temp, it, cnt.get(), (int)groups, s));
+      DeviceBuffer<uint8_t> t(temp ? temp : 1, s);
+      EF_CUDA(cub::DeviceReduce::Sum(t.get(), temp, it, cnt.get(), (int)groups, s));
+      unsigned long long valued_n = 0;
+      EF_CUDA(cudaMemcpyAsync(&valued_n, cnt.get(), 8, cudaMemcpyDeviceToHost, s));
+      EF_CUDA(cudaStreamSynchronize(s));
+      vnulls = (unsigned long long)groups - valued_n;
+    }
+  }
+  v.values = result_buffer(ctx, gsum, (size_t)groups * 8, o.result_on_device);
+  v.null_count = (int64_t)vnulls;
+  if (vnulls) v.validity = result_buffer(ctx, vbits, (size_t)((groups + 7) / 8), o.result_on_device);
+  out_batch.columns.push_back(std::move(v));
+  EF_CUDA(cudaStreamSynchronize(s));
+  result.batches.push_back(std::move(out_batch));
+  ctx.phase("discriminate: result");
+  return result;
+}
+
+}  // namespace ef

@@ -3,10 +3,6 @@
 
 namespace ef {
 
-FoldOutput discriminate_fold(Context&, const FoldD&, const Relation&, const Relation&, const Relation*,
-                             const std::vector<Field>&, const einfold_options&, Budget&) {
-  fail(EINFOLD_COMPUTE, "the discrimination algorithm is not built yet");
-}
 FoldOutput chain_fold(Context&, const FoldD&, const std::vector<const Relation*>&, const std::vector<Field>&,
                       const einfold_options&, Budget&) {
   fail(EINFOLD_COMPUTE, "chains are not built yet");

@@ -71,7 +71,16 @@ def assert_same_rows(got: pa.Table, want: pa.Table, tol: Optional[np.ndarray] = 
     assert got.num_columns == want.num_columns
     for c in range(got.num_columns - 1):
         assert got.column(c).type == want.column(c).type, (got.column(c).type, want.column(c).type)
-        assert got.column(c).equals(want.column(c)), f"key column {c} differs"
+        gc, wc = got.column(c).combine_chunks(), want.column(c).combine_chunks()
+        if pa.types.is_floating(gc.type):
+            # By their bits, NaNs and signed zeros included.
+            assert gc.null_count == wc.null_count and gc.is_null().equals(wc.is_null()), f"key column {c} NULLs differ"
+            width = {16: np.uint16, 32: np.uint32, 64: np.uint64}[gc.type.bit_width]
+            gb = np.asarray(gc.fill_null(0).to_numpy(zero_copy_only=False)).view(width)
+            wb = np.asarray(wc.fill_null(0).to_numpy(zero_copy_only=False)).view(width)
+            assert np.array_equal(gb, wb), f"key column {c} differs"
+        else:
+            assert gc.equals(wc), f"key column {c} differs"
     gv, wv = got.column(got.num_columns - 1), want.column(want.num_columns - 1)
     gnull = np.asarray(gv.is_null().to_numpy(zero_copy_only=False), bool)
     wnull = np.asarray(wv.is_null().to_numpy(zero_copy_only=False), bool)
