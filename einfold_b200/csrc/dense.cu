@@ -67,13 +67,6 @@ __global__ void scatter_b_kernel(Role wzs, Role ys, int64_t rows, const double* 
   if (f) atomicOr(flags, f);
 }
 
-// Where output keys come from: position x (in_x) or y, their stride and extent.
-struct KeyAt {
-  int in_x;
-  int64_t stride, extent;
-  __device__ __forceinline__ int64_t at(int64_t x, int64_t y) const { return ((in_x ? x : y) / stride) % extent; }
-};
-
 struct Conds {
   int n = 0;
   KeyAt left[kMaxDims], right[kMaxDims];
@@ -95,21 +88,6 @@ struct Conds {
   }
 };
 
-struct OutKeys {
-  int n = 0;
-  KeyAt key[kMaxDims];
-  int width[kMaxDims];
-  void* out[kMaxDims];
-};
-
-// The keys of output dimensions along x (or y), one table per key:
-// table[k][p] = (p / stride) % extent, so that emitting needs no division.
-__global__ void key_tables(int64_t n, OutKeys keys, int in_x, int64_t* __restrict__ tables) {
-  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
-    for (int k = 0; k < keys.n; k++)
-      if (keys.key[k].in_x == in_x) tables[(int64_t)k * n + p] = keys.key[k].at(p, p);
-}
-
 // Which cells are output rows: reached x and, with conditions, allowed (x, y).
 __global__ void select_cells(int64_t nx, int64_t ny, const uint8_t* __restrict__ reached, Conds c,
                              uint8_t* __restrict__ sel) {
@@ -117,15 +95,6 @@ __global__ void select_cells(int64_t nx, int64_t ny, const uint8_t* __restrict__
     const bool r = reached[x] != 0;
     for (int64_t y = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; y < ny; y += (int64_t)gridDim.x * blockDim.x)
       sel[x * ny + y] = r && c.allowed(x, y);
-  }
-}
-
-__device__ __forceinline__ void store_key(void* base, int width, int64_t i, int64_t v) {
-  switch (width) {
-    case 1: ((uint8_t*)base)[i] = (uint8_t)v; break;
-    case 2: ((uint16_t*)base)[i] = (uint16_t)v; break;
-    case 4: ((uint32_t*)base)[i] = (uint32_t)v; break;
-    default: ((int64_t*)base)[i] = v; break;
   }
 }
 
@@ -204,53 +173,6 @@ __global__ void domain_values(int64_t rows, const int64_t* __restrict__ cell, in
       valid[r] = (uint8_t)(has_missing ? 1 : 0);
     }
   }
-}
-
-// Keys of every batch of `r` for `op`, staged as int64, with extents.
-struct StagedKeys {
-  std::vector<DeviceColumn> cols;           // staged columns (int64 ones read in place)
-  std::vector<DeviceBuffer<int64_t>> wide;  // other integer columns widened to int64
-  std::vector<const int64_t*> keys;         // per key of the operand, in op.keys order
-  std::vector<int64_t> extent;              // per key
-};
-
-// Stages an operand's key columns; declines where dense::keys returns None.
-StagedKeys stage_keys(Context& ctx, const OperandD& op, const Relation& r) {
-  StagedKeys s;
-  for (auto& k : op.keys) {
-    const Field& f = r.fields[k.col];
-    if (f.dictionary || !is_integer(f.kind)) decline("a key column that isn't integers");
-    for (auto& b : r.batches)
-      if (b.columns[k.col].nulls() > 0) decline("a NULL key");
-    s.cols.push_back(stage_column(ctx, r, k.col, false));
-    DeviceColumn& c = s.cols.back();
-    KeyStats st;
-    if (c.kind == Kind::Int64) {
-      key_stats_i64(ctx, (const int64_t*)c.ptr(), c.rows, &st);
-      s.keys.push_back((const int64_t*)c.ptr());
-    } else {
-      s.wide.push_back(keys_as_i64(ctx, c, &st));
-      s.keys.push_back(s.wide.back().get());
-    }
-    if (st.negative || st.too_large) decline("a negative key, or one too large for int64");
-    if (st.max == INT64_MAX) decline("a key whose extent doesn't fit");
-    s.extent.push_back(st.max + 1);
-  }
-  return s;
-}
-
-Role role_of(const std::vector<int>& dims, const OperandD& op, const StagedKeys& s, const std::vector<int64_t>& extent) {
-  Role r;
-  if (dims.size() > (size_t)kMaxDims) decline("more than 8 dimensions in one role");
-  for (int d : dims) {
-    int slot = -1;
-    for (size_t i = 0; i < op.keys.size(); i++)
-      if (op.keys[i].dim == d) slot = (int)i;
-    r.keys[r.n] = s.keys[slot];
-    r.extent[r.n] = extent[d];
-    r.n++;
-  }
-  return r;
 }
 
 bool worth(uint64_t cells, uint64_t rows) {

@@ -1,0 +1,821 @@
+// The fused pipeline on the device (crates/einfold-kernels/src/fused.rs:151-1086).
+//
+// Host side: the reference's control logic, roles W/X/E/J/Y, the mask of
+// conditions between the one X and the one J dimension, which columns the
+// producer reads, the decline rules. Device side: keys and extents, the
+// placement of each read column as a dense matrix with duplicate detection,
+// each J position's value statistics, the tiles, and the output columns.
+//
+// Layout in HBM: each column q reads as q[x][e]; each column k reads as
+// k[j][e] (e contiguous: the scores' K-major operands), the values v[j][y];
+// the result out[x][y]. Batch keys W lead both X and J, so that a batch's
+// positions are a contiguous range of each.
+//
+// The tile kernel computes, per 64-row X tile and 64-wide chunk of Y, what
+// fused.rs:694-1019 computes per X tile: the J tiles of 64 between the
+// first and last allowed J position of its rows, scores by a product or a
+// row expression summed over E, weights by an online softmax shifted by
+// the running maximum or by an expression of the score, the weighted sums,
+// the normalisation, and every guard that sends the pipeline back to the
+// host plan (overflows :1024-1028, Bounds::hold :1058-1086). A chunk of Y
+// recomputes its tile's scores; each guard is a conjunction over outputs,
+// so the chunks' flags OR to the whole row's.
+#include <algorithm>
+#include <cmath>
+#include <optional>
+
+#include "fold.h"
+#include "stage.cuh"
+
+namespace ef {
+namespace {
+
+constexpr int XT = 64, JT = 64;  // fused.rs XT, JT: tiles visited count in these
+constexpr int YC = 64;           // outputs per CTA along y
+constexpr int kMaxMask = 8;
+constexpr int kMaxSlots = 8;
+constexpr int kThreads = 256;
+
+struct Mask {
+  int n = 0;
+  int cmp[kMaxMask] = {};
+  int64_t off[kMaxMask] = {};
+  int64_t lnx = 1, lnj = 0;  // positions per batch along X and J
+};
+
+// allowed(x) (fused.rs:350-368): the half-open J interval that X position
+// x may join, the intersection of each condition's, in 128-bit integers,
+// clamped to x's batch.
+__host__ __device__ inline void allowed(const Mask& m, int64_t x, int64_t& lo_out, int64_t& hi_out) {
+  const int64_t group_start = (x / m.lnx) * m.lnj;
+  const __int128 xx = x % m.lnx, n = m.lnj;
+  __int128 lo = 0, hi = n;
+  for (int i = 0; i < m.n; i++) {
+    const __int128 bound = xx - (__int128)m.off[i];
+    switch (m.cmp[i]) {
+      case 3: if (bound + 1 < hi) hi = bound + 1; break;  // x >= j + c
+      case 2: if (bound < hi) hi = bound; break;          // x >  j + c
+      case 1: if (bound > lo) lo = bound; break;          // x <= j + c
+      default: if (bound + 1 > lo) lo = bound + 1; break; // x <  j + c
+    }
+  }
+  const __int128 l = lo < 0 ? 0 : (lo > n ? n : lo);
+  __int128 h = hi > lo ? hi : lo;
+  h = h < 0 ? 0 : (h > n ? n : h);
+  lo_out = group_start + (int64_t)l;
+  hi_out = group_start + (int64_t)h;
+}
+
+// A postfix expression (expression.rs:61-120) over slots; column nodes
+// carry their slot in `a`. Every operation rounds once, as Rust's f64 does.
+__device__ double eval(const ExprNode* __restrict__ nodes, int n, const double* slots) {
+  double st[64];
+  int sp = 0;
+  for (int i = 0; i < n; i++) {
+    const ExprNode e = nodes[i];
+    if (e.kind == 0) {
+      st[sp++] = slots[e.a];
+    } else if (e.kind == 1) {
+      st[sp++] = e.value;
+    } else if (e.kind == 2) {
+      const double x = st[sp - 1];
+      st[sp - 1] = e.a == 0 ? -x : e.a == 1 ? fabs(x) : e.a == 2 ? exp(x) : log(x);
+    } else {
+      const double b = st[--sp], a = st[sp - 1];
+      double r;
+      switch (e.a) {
+        case 0: r = __dadd_rn(a, b); break;
+        case 1: r = __dsub_rn(a, b); break;
+        case 2: r = __dmul_rn(a, b); break;
+        case 3: r = __ddiv_rn(a, b); break;
+        default: r = pow(a, b); break;
+      }
+      st[sp - 1] = r;
+    }
+  }
+  return st[0];
+}
+
+enum : uint8_t { J_FINITE = 1, J_INFINITE = 2 };
+
+struct TileArgs {
+  int64_t nx, ne, nj, ny;
+  Mask mask;
+  int weight_expr, scale_kind, shifted, normalizer;
+  double scale_c;
+  const ExprNode* wnodes;
+  int wn;
+  int score_expr;
+  const double* q;  // [x][e]
+  const double* k;  // [j][e]
+  const ExprNode* snodes;
+  int sn, n_slots;
+  const double* mats[kMaxSlots];
+  int side[kMaxSlots];  // 0: [x][e], 1: [j][e]
+  const double* v;      // [j][y]
+  const uint8_t* jflag;
+  const double* largest;
+  const double* smallest;
+  double* out;  // [x][y]
+  unsigned long long* visited;
+  unsigned* overflowed;
+};
+
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_min(double v) {
+  for (int o = 16; o; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+struct RowState {
+  double m[XT], z[XT], high[XT], light[XT], low[XT], rl[XT], rs[XT], resc[XT], lost[XT];
+  long long terms[XT];
+  int lo[XT], hi[XT];
+  uint8_t sw[XT], sw_before[XT], pend[XT], spv[XT], check[XT];
+};
+
+constexpr int kStage = 32 * 65;  // doubles in one staged operand chunk (e rows of 64 + 1)
+constexpr size_t kTileSmem = sizeof(double) * (XT * (JT + 1) + 2 * kStage) + sizeof(RowState);
+
+__global__ void __launch_bounds__(kThreads) fused_tiles(const TileArgs p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double(*blk)[JT + 1] = reinterpret_cast<double(*)[JT + 1]>(smem);
+  double* stg = reinterpret_cast<double*>(smem + sizeof(double) * XT * (JT + 1));
+  RowState& S = *reinterpret_cast<RowState*>(smem + sizeof(double) * (XT * (JT + 1) + 2 * kStage));
+  __shared__ long long s_first, s_last;
+
+  const int t = threadIdx.x, tx = t & 15, ty = t >> 4, warp = t >> 5, lane = t & 31;
+  const int64_t x0 = (int64_t)blockIdx.x * XT;
+  const int rows = (int)std::min<int64_t>(XT, p.nx - x0);
+  const int64_t y0 = (int64_t)blockIdx.y * YC;
+  const int ycount = p.ny > y0 ? (int)std::min<int64_t>(YC, p.ny - y0) : 0;
+  const bool map = p.weight_expr != 0;
+  const bool shifted = !map && p.shifted != 0;
+  const bool unnormalized = p.normalizer == 2;
+  const double NEG_INF = -INFINITY, POS_INF = INFINITY;
+
+  if (t == 0) { s_first = p.nj; s_last = 0; }
+  if (t < XT) {
+    S.m[t] = shifted ? NEG_INF : 0.0;
+    S.z[t] = 0.0;
+    S.high[t] = NEG_INF;
+    S.light[t] = POS_INF;
+    S.low[t] = POS_INF;
+    S.rl[t] = 0.0;
+    S.rs[t] = POS_INF;
+    S.terms[t] = 0;
+    S.sw[t] = 0;
+  }
+  __syncthreads();
+  if (t < rows) {
+    int64_t lo, hi;
+    allowed(p.mask, x0 + t, lo, hi);
+    if (lo < hi) {
+      atomicMin(&s_first, (long long)lo);
+      atomicMax(&s_last, (long long)hi);
+    }
+  }
+  __syncthreads();
+  const int64_t first = s_first, last = s_last;
+
+  double acc[4][4];
+  for (int i = 0; i < 4; i++)
+    for (int jj = 0; jj < 4; jj++) acc[i][jj] = 0.0;
+  unsigned sv = 0;  // special_value bits of this thread's 16 outputs
+  bool over = false;
+  unsigned long long visited = 0;
+
+  for (int64_t j0 = first - first % JT; j0 < last; j0 += JT) {
+    const int width = (int)std::min<int64_t>(JT, p.nj - j0);
+    // Each row's allowed positions within this tile, relative to j0.
+    bool has = false;
+    if (t < XT) {
+      int lo = 0, hi = 0;
+      if (t < rows) {
+        int64_t l, h;
+        allowed(p.mask, x0 + t, l, h);
+        l = l < j0 ? j0 : (l > j0 + width ? j0 + width : l);
+        h = h < j0 ? j0 : (h > j0 + width ? j0 + width : h);
+        lo = (int)(l - j0);
+        hi = (int)(h - j0);
+      }
+      S.lo[t] = lo;
+      S.hi[t] = hi;
+      S.pend[t] = 0;
+      S.spv[t] = 0;
+      has = lo < hi;
+    }
+    if (!__syncthreads_or(has)) continue;
+    visited++;
+
+    // Scores of the pair of tiles.
+    double s[4][4];
+    if (!p.score_expr) {
+      for (int i = 0; i < 4; i++)
+        for (int jj = 0; jj < 4; jj++) s[i][jj] = 0.0;
+      double* qs = stg;            // [e][r], rows of 65
+      double* ks = stg + kStage;   // [e][j]
+      for (int64_t e0 = 0; e0 < p.ne; e0 += 32) {
+        const int ec = (int)std::min<int64_t>(32, p.ne - e0);
+        for (int idx = t; idx < XT * 32; idx += kThreads) {
+          const int r = idx >> 5, e = idx & 31;
+          qs[e * 65 + r] = (r < rows && e < ec) ? p.q[(x0 + r) * p.ne + e0 + e] : 0.0;
+          ks[e * 65 + r] = (r < width && e < ec) ? p.k[(j0 + r) * p.ne + e0 + e] : 0.0;
+        }
+        __syncthreads();
+        for (int e = 0; e < ec; e++) {
+          double qv[4], kv[4];
+          for (int i = 0; i < 4; i++) qv[i] = qs[e * 65 + ty + 16 * i];
+          for (int jj = 0; jj < 4; jj++) kv[jj] = ks[e * 65 + tx + 16 * jj];
+          for (int i = 0; i < 4; i++)
+            for (int jj = 0; jj < 4; jj++) s[i][jj] = fma(qv[i], kv[jj], s[i][jj]);
+        }
+        __syncthreads();
+      }
+    } else {
+      double slots[kMaxSlots];
+      for (int i = 0; i < 4; i++)
+        for (int jj = 0; jj < 4; jj++) {
+          const int r = ty + 16 * i, j = tx + 16 * jj;
+          double acc_s = 0.0;
+          if (r < rows && j < width) {
+            for (int64_t e = 0; e < p.ne; e++) {
+              for (int sl = 0; sl < p.n_slots; sl++)
+                slots[sl] = p.side[sl] == 0 ? p.mats[sl][(x0 + r) * p.ne + e] : p.mats[sl][(j0 + j) * p.ne + e];
+              const double val = eval(p.snodes, p.sn, slots);
+              acc_s = e == 0 ? val : __dadd_rn(acc_s, val);
+            }
+          }
+          s[i][jj] = acc_s;
+        }
+    }
+    for (int i = 0; i < 4; i++)
+      for (int jj = 0; jj < 4; jj++) blk[ty + 16 * i][tx + 16 * jj] = s[i][jj];
+    __syncthreads();
+
+    // Weights and the row state (fused.rs:811-909), a warp per row.
+    for (int rr = 0; rr < XT / 8; rr++) {
+      const int r = warp * (XT / 8) + rr;
+      if (r >= rows) continue;
+      const int lo = S.lo[r], hi = S.hi[r];
+      if (lo >= hi) continue;
+      const int ja = lane, jb = lane + 32;
+      const bool ina = ja >= lo && ja < hi, inb = jb >= lo && jb < hi;
+      const uint8_t fa = ina ? p.jflag[j0 + ja] : J_FINITE, fb = inb ? p.jflag[j0 + jb] : J_FINITE;
+      {
+        const double lg = fmax(ina ? p.largest[j0 + ja] : 0.0, inb ? p.largest[j0 + jb] : 0.0);
+        const double sm = fmin(ina ? p.smallest[j0 + ja] : POS_INF, inb ? p.smallest[j0 + jb] : POS_INF);
+        const double wlg = warp_max(lg), wsm = warp_min(sm);
+        if (lane == 0) {
+          S.terms[r] += hi - lo;
+          S.rl[r] = fmax(S.rl[r], wlg);
+          S.rs[r] = fmin(S.rs[r], wsm);
+        }
+      }
+      double sa = ina ? blk[r][ja] : 0.0, sb = inb ? blk[r][jb] : 0.0;
+      if (map) {
+        if (ina) sa = eval(p.wnodes, p.wn, &sa);
+        if (inb) sb = eval(p.wnodes, p.wn, &sb);
+        const bool bad = (ina && (!isfinite(sa) || !(fa & J_FINITE))) || (inb && (!isfinite(sb) || !(fb & J_FINITE)));
+        if (__any_sync(0xffffffffu, bad)) over = true;
+        const double aa = fabs(sa), ab = fabs(sb);
+        const double hw = warp_max(fmax(ina ? aa : NEG_INF, inb ? ab : NEG_INF));
+        const double lw = warp_min(fmin(ina && aa != 0.0 ? aa : POS_INF, inb && ab != 0.0 ? ab : POS_INF));
+        const double sum = warp_sum((ina ? sa : 0.0) + (inb ? sb : 0.0));
+        if (ina) blk[r][ja] = sa;
+        if (inb) blk[r][jb] = sb;
+        if (lane == 0) {
+          S.high[r] = fmax(S.high[r], hw);
+          S.light[r] = fmin(S.light[r], lw);
+          S.z[r] += sum;
+        }
+        continue;
+      }
+      if (p.scale_kind == 1) { sa = sa * p.scale_c; sb = sb * p.scale_c; }
+      else if (p.scale_kind == 2) { sa = __ddiv_rn(sa, p.scale_c); sb = __ddiv_rn(sb, p.scale_c); }
+      const bool fina = ina && isfinite(sa), finb = inb && isfinite(sb);
+      const double hs = warp_max(fmax(fina ? sa : NEG_INF, finb ? sb : NEG_INF));
+      const double ls = warp_min(fmin(fina ? sa : POS_INF, finb ? sb : POS_INF));
+      const double lows = warp_min(fmin(fina && (fa & J_INFINITE) ? sa : POS_INF, finb && (fb & J_INFINITE) ? sb : POS_INF));
+      const bool any_nan = __any_sync(0xffffffffu, (ina && isnan(sa)) || (inb && isnan(sb)));
+      const double mx = warp_max(fmax(ina && !isnan(sa) ? sa : NEG_INF, inb && !isnan(sb) ? sb : NEG_INF));
+      const bool special_values = __any_sync(0xffffffffu, (ina && !(fa & J_FINITE)) || (inb && !(fb & J_FINITE)));
+      const double m_old = S.m[r];
+      // The largest score so far, or NaN once any score is NaN.
+      const double shift = shifted ? ((isnan(m_old) || any_nan) ? NAN : fmax(m_old, mx)) : 0.0;
+      if (lane == 0) {
+        S.high[r] = fmax(S.high[r], hs);
+        S.light[r] = fmin(S.light[r], ls);
+        S.low[r] = fmin(S.low[r], lows);
+      }
+      if (shift == NEG_INF) {
+        // Every score so far is -inf: weights 0 here.
+        if (ina) blk[r][ja] = 0.0;
+        if (inb) blk[r][jb] = 0.0;
+        continue;
+      }
+      const double rescale = exp(m_old - shift);
+      const double wa = ina ? exp(sa - shift) : 0.0, wb = inb ? exp(sb - shift) : 0.0;
+      const double sum = warp_sum(wa + wb);
+      const bool special_weights = __any_sync(0xffffffffu, (ina && !isfinite(wa)) || (inb && !isfinite(wb)));
+      if (ina) blk[r][ja] = wa;
+      if (inb) blk[r][jb] = wb;
+      if (lane == 0) {
+        S.sw_before[r] = S.sw[r];
+        if (shifted && rescale != 1.0) {
+          // overflows(z, a, ...) before the rescale: z's part here, a's by
+          // the threads that hold a.
+          if (!S.sw[r] && !isfinite(S.z[r])) over = true;
+          S.z[r] *= rescale;
+          S.pend[r] = 1;
+          S.resc[r] = rescale;
+        }
+        S.sw[r] |= special_weights;
+        S.spv[r] = special_values;
+        if (unnormalized && (special_weights || special_values)) over = true;
+        S.z[r] += sum;
+        S.m[r] = shift;
+      }
+    }
+    __syncthreads();
+
+    // The weighted values: a += w · v over each row's allowed span.
+    double* vs = stg;  // [j][y], rows of 65
+    for (int idx = t; idx < JT * YC; idx += kThreads) {
+      const int j = idx >> 6, y = idx & 63;
+      vs[j * 65 + y] = (j < width && y < ycount) ? p.v[(j0 + j) * p.ny + y0 + y] : 0.0;
+    }
+    __syncthreads();
+    for (int i = 0; i < 4; i++) {
+      const int r = ty + 16 * i;
+      if (r >= rows) continue;
+      const int lo = S.lo[r], hi = S.hi[r];
+      if (lo >= hi) continue;
+      if (S.pend[r]) {
+        const double rescale = S.resc[r];
+        for (int jj = 0; jj < 4; jj++) {
+          const int y = tx + 16 * jj;
+          if (y < ycount && !S.sw_before[r] && !((sv >> (i * 4 + jj)) & 1) && !isfinite(acc[i][jj])) over = true;
+          acc[i][jj] *= rescale;
+        }
+      }
+      for (int j = lo; j < hi; j++) {
+        const double w = blk[r][j];
+        for (int jj = 0; jj < 4; jj++) acc[i][jj] = fma(w, vs[j * 65 + tx + 16 * jj], acc[i][jj]);
+      }
+      if (S.spv[r])
+        for (int j = lo; j < hi; j++)
+          if (!(p.jflag[j0 + j] & J_FINITE))
+            for (int jj = 0; jj < 4; jj++)
+              if (!isfinite(vs[j * 65 + tx + 16 * jj])) sv |= 1u << (i * 4 + jj);
+    }
+    __syncthreads();
+  }
+
+  // Normalisation and the row guards (fused.rs:941-1013).
+  const double normal = 2.0 * 2.2250738585072014e-308;
+  if (t < rows) {
+    const int r = t;
+    const bool zp = !unnormalized;
+    const double z = S.z[r], m = S.m[r];
+    if (zp && !S.sw[r] && !isfinite(z)) over = true;
+    S.check[r] = 0;
+    auto weight = [&](double bound) { return map ? bound : shifted ? exp(bound - m) : exp(bound); };
+    const double heaviest = weight(S.high[r]);
+    if (!(S.sw[r] || S.high[r] == NEG_INF || heaviest == 0.0)) {
+      const double lightest = weight(S.light[r]);
+      const double largest = S.rl[r], smallest = S.rs[r];
+      const double terms = 2.0 * (double)S.terms[r];
+      bool finite = isfinite(__dmul_rn(__dmul_rn(heaviest, largest), terms));
+      if (finite && zp) {
+        const double quotient = __ddiv_rn(heaviest, fabs(z));
+        finite = isfinite(quotient) && isfinite(__dmul_rn(__dmul_rn(quotient, largest), terms));
+      }
+      const double inverse = zp ? __ddiv_rn(1.0, fabs(z)) : 1.0;
+      const double tiniest = 4.9406564584124654e-324;
+      S.lost[r] = __dmul_rn(__dmul_rn(terms, tiniest), __dadd_rn(__dadd_rn(inverse, largest), 1.0));
+      bool no_underflow = smallest == POS_INF;
+      if (!no_underflow) {
+        no_underflow = __dmul_rn(lightest, smallest) >= normal;
+        if (no_underflow && zp) {
+          const double quotient = __ddiv_rn(lightest, fabs(z));
+          no_underflow = quotient >= normal && __dmul_rn(quotient, smallest) >= normal;
+        }
+      }
+      if (!finite) over = true;
+      else if (!no_underflow) S.check[r] = 1;
+      if (S.low[r] != POS_INF) {
+        const double lw = shifted ? exp(S.low[r] - m) : exp(S.low[r]);
+        const bool ok = lw >= normal && (!zp || __ddiv_rn(lw, fabs(z)) >= normal);
+        if (!ok) over = true;
+      }
+    }
+  }
+  __syncthreads();
+  const double rounding = 2.220446049250313e-16 / 4.0;
+  for (int i = 0; i < 4; i++) {
+    const int r = ty + 16 * i;
+    if (r >= rows) continue;
+    const double z = S.z[r];
+    const bool swr = S.sw[r] != 0;
+    for (int jj = 0; jj < 4; jj++) {
+      const int y = tx + 16 * jj;
+      if (y >= ycount) continue;
+      const bool spec = (sv >> (i * 4 + jj)) & 1;
+      double a = acc[i][jj];
+      if (unnormalized) {
+        if (shifted && S.m[r] == NEG_INF) a = NAN;
+      } else {
+        if (!swr && !spec && !isfinite(a)) over = true;
+        a = __ddiv_rn(a, z);
+        if (z != 0.0 && !swr && !spec && !isfinite(a)) over = true;
+      }
+      if (S.check[r] && !spec && !(S.lost[r] <= rounding * fabs(a))) over = true;
+      p.out[(x0 + r) * p.ny + y0 + y] = a;
+    }
+  }
+  if (__syncthreads_or(over) && t == 0) atomicOr(p.overflowed, 1u);
+  if (t == 0 && blockIdx.y == 0 && visited) atomicAdd(p.visited, visited);
+}
+
+// Each J position's values: whether all are finite, whether any is
+// infinite, the largest finite magnitude (0 if none) and the smallest
+// nonzero finite one (+inf if none) (fused.rs:371-385). A warp per J.
+__global__ void value_stats(int64_t nj, int64_t ny, const double* __restrict__ v, uint8_t* __restrict__ flag,
+                            double* __restrict__ largest, double* __restrict__ smallest) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t j = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < nj;
+       j += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    bool fin = true, inf = false;
+    double lg = 0.0, sm = INFINITY;
+    for (int64_t y = lane; y < ny; y += 32) {
+      const double x = v[j * ny + y];
+      if (!isfinite(x)) {
+        fin = false;
+        inf |= isinf(x);
+      } else {
+        const double a = fabs(x);
+        lg = fmax(lg, a);
+        if (a != 0.0) sm = fmin(sm, a);
+      }
+    }
+    fin = __all_sync(0xffffffffu, fin);
+    inf = __any_sync(0xffffffffu, inf);
+    lg = warp_max(lg);
+    sm = warp_min(sm);
+    if (lane == 0) {
+      flag[j] = (fin ? J_FINITE : 0) | (inf ? J_INFINITE : 0);
+      largest[j] = lg;
+      smallest[j] = sm;
+    }
+  }
+}
+
+// Scatters a column's rows into matrix[row][col]; a repeated cell sets *dup.
+__global__ void place_kernel(Role rows_r, Role cols_r, int64_t n, int64_t ncols, const double* __restrict__ vals,
+                             double* __restrict__ mat, unsigned* __restrict__ held, unsigned* dup) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t cell = role_position(rows_r, i) * ncols + role_position(cols_r, i);
+    const unsigned bit = 1u << (cell & 31);
+    if (atomicOr(&held[cell >> 5], bit) & bit) atomicOr(dup, 1u);
+    mat[cell] = vals[i];
+  }
+}
+
+// Output rows: x has one if it is allowed some J position.
+__global__ void row_flags(int64_t nx, int64_t nj, Mask m, uint8_t* __restrict__ flags) {
+  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < nx; x += (int64_t)gridDim.x * blockDim.x) {
+    int64_t lo, hi;
+    allowed(m, x, lo, hi);
+    flags[x] = nj > 0 && lo < hi;
+  }
+}
+
+__global__ void emit_rows(int64_t nx, int64_t ny, const uint8_t* __restrict__ flags,
+                          const int64_t* __restrict__ row_index, OutKeys keys, const int64_t* __restrict__ xtab,
+                          const int64_t* __restrict__ ytab, const double* __restrict__ out,
+                          double* __restrict__ val_out) {
+  for (int64_t x = blockIdx.y; x < nx; x += gridDim.y) {
+    if (!flags[x]) continue;
+    const int64_t base = row_index[x] * ny;
+    for (int64_t y = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; y < ny; y += (int64_t)gridDim.x * blockDim.x) {
+      const int64_t o = base + y;
+      for (int k = 0; k < keys.n; k++)
+        store_key(keys.out[k], keys.width[k], o, keys.key[k].in_x ? xtab[(int64_t)k * nx + x] : ytab[(int64_t)k * ny + y]);
+      val_out[o] = out[x * ny + y];
+    }
+  }
+}
+
+struct Placement {
+  int operand;                 // 0 q, 1 k, 2 v
+  const std::vector<int>* rows;
+  const std::vector<int>* cols;
+  int column;
+};
+
+std::optional<uint64_t> size_of(const std::vector<int>& dims, const std::vector<int64_t>& extent) {
+  uint64_t n = 1;
+  for (int d : dims)
+    if (!checked_mul(n, (uint64_t)extent[d], &n)) return std::nullopt;
+  return n;
+}
+
+}  // namespace
+
+FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, const Relation& k, const Relation& v,
+                          const std::vector<Field>& schema, const einfold_options& o, Budget& budget) {
+  (void)budget;  // the tile path asks no budget (fused.rs:151-489)
+  cudaStream_t s = ctx.stream;
+  const FoldD& pr = p.producer;
+  if (pr.operands.size() != 2) decline("a pipeline's producer of other than two operands");
+  const OperandD &op_q = pr.operands[0], &op_k = pr.operands[1], &values = p.values;
+  const int own = pr.n_dims(), n = own + (int)p.equality.size();
+  auto output = [&](int d) { return std::find(p.outputs.begin(), p.outputs.end(), d) != p.outputs.end(); };
+  std::vector<int> ws, xs, es, js;
+  for (int d = 0; d < own; d++) {
+    const bool hq = op_q.holds(d), hk = op_k.holds(d), produced = pr.output_of(d) >= 0, out = output(d),
+               hv = values.holds(d);
+    if (hq && hk && produced && out && hv) ws.push_back(d);
+    else if (hq && !hk && produced && out && !hv) xs.push_back(d);
+    else if (hq && hk && !produced && !out && !hv) es.push_back(d);
+    else if (!hq && hk && produced && !out && hv) js.push_back(d);
+    else decline("a dimension of no pipeline role");
+  }
+  std::vector<int> ys;
+  for (int d = own; d < n; d++) {
+    if (!output(d)) decline("a pipeline that sums its own dimension away");
+    ys.push_back(d);
+  }
+  Mask mask;
+  for (auto& c : pr.conditions) {
+    if (xs.size() != 1 || js.size() != 1) decline("a condition without one X and one J dimension");
+    ConditionD m;
+    if (c.left == xs[0] && c.right == js[0]) m = c;
+    else if (c.left == js[0] && c.right == xs[0]) {
+      auto mm = c.mirrored();
+      if (!mm) decline("a condition whose mirror overflows");
+      m = *mm;
+    } else {
+      decline("a condition on other dimensions");
+    }
+    if (mask.n == kMaxMask) decline("more than 8 conditions");
+    mask.cmp[mask.n] = m.cmp;
+    mask.off[mask.n] = m.offset;
+    mask.n++;
+  }
+  const std::vector<int> local_xs = xs, local_js = js;
+  xs.insert(xs.begin(), ws.begin(), ws.end());
+  js.insert(js.begin(), ws.begin(), ws.end());
+
+  // The producer's columns: each operand's factor, or what its expression reads.
+  std::vector<std::pair<int, int>> read;
+  if (!pr.row_expr) {
+    if (op_q.factor < 0 || op_k.factor < 0) decline("a product's operand without a factor");
+    read = {{0, op_q.factor}, {1, op_k.factor}};
+  } else {
+    read = pr.row_columns();
+    std::sort(read.begin(), read.end());
+    read.erase(std::unique(read.begin(), read.end()), read.end());
+    bool reads0 = false, reads1 = false;
+    for (auto& rc : read) {
+      reads0 |= rc.first == 0;
+      reads1 |= rc.first == 1;
+      if (rc.first > 1) decline("an expression reading a third operand");
+    }
+    if (!reads0 || !reads1) decline("an expression that doesn't read both operands");
+    if ((int)read.size() > kMaxSlots) decline("an expression reading more than 8 columns");
+  }
+  std::vector<Placement> placements;
+  for (auto& rc : read) placements.push_back(rc.first == 0 ? Placement{0, &xs, &es, rc.second} : Placement{1, &js, &es, rc.second});
+  placements.push_back(Placement{2, &js, &ys, values.factor});
+  const OperandD* ops[3] = {&op_q, &op_k, &values};
+  const Relation* rels[3] = {&q, &k, &v};
+
+  // Keys and extents, each operand's staged once.
+  std::vector<int64_t> extent((size_t)n, 0);
+  std::optional<StagedKeys> staged[3];
+  for (auto& pl : placements) {
+    if (staged[pl.operand]) continue;
+    staged[pl.operand] = stage_keys(ctx, *ops[pl.operand], *rels[pl.operand]);
+    const OperandD& op = *ops[pl.operand];
+    for (size_t i = 0; i < op.keys.size(); i++)
+      extent[op.keys[i].dim] = std::max(extent[op.keys[i].dim], staged[pl.operand]->extent[i]);
+  }
+  auto nx_ = size_of(xs, extent), ne_ = size_of(es, extent), nj_ = size_of(js, extent), ny_ = size_of(ys, extent);
+  auto lnx_ = size_of(local_xs, extent), lnj_ = size_of(local_js, extent);
+  if (!nx_ || !ne_ || !nj_ || !ny_ || !lnx_ || !lnj_) decline("an extent product that overflows");
+  const uint64_t nx = *nx_, ne = *ne_, nj = *nj_, ny = *ny_;
+  mask.lnx = (int64_t)std::max<uint64_t>(*lnx_, 1);
+  mask.lnj = (int64_t)*lnj_;
+  ctx.phase("fused: keys");
+
+  // Placement (fused.rs:624-664): exactly one non-NULL row per cell.
+  std::vector<DeviceBuffer<double>> matrices;
+  for (auto& pl : placements) {
+    const Relation& r = *rels[pl.operand];
+    const OperandD& op = *ops[pl.operand];
+    auto rows_n = size_of(*pl.rows, extent), cols_n = size_of(*pl.cols, extent);
+    if (!rows_n || !cols_n) decline("an extent product that overflows");
+    uint64_t cells = 0;
+    if (!checked_mul(*rows_n, *cols_n, &cells)) decline("an extent product that overflows");
+    uint64_t total = 0;
+    for (auto& b : r.batches) total += (uint64_t)b.rows;
+    if (total != cells || cells >= UINT32_MAX) decline("an operand without one row per cell");
+    const Field& f = r.fields[pl.column];
+    if (f.dictionary || f.kind != Kind::Float64) decline("a column that isn't DOUBLE");
+    for (auto& b : r.batches)
+      if (b.columns[pl.column].nulls() > 0) decline("a NULL factor");
+    DeviceColumn col = stage_column(ctx, r, pl.column, false);
+    DeviceBuffer<double> mat((size_t)std::max<uint64_t>(cells, 1), s);
+    DeviceBuffer<unsigned> held((size_t)std::max<uint64_t>((cells + 31) / 32, 1), s);
+    DeviceBuffer<unsigned> dup(1, s);
+    held.zero();
+    dup.zero();
+    if (cells) {
+      const Role rr = role_of(*pl.rows, op, *staged[pl.operand], extent);
+      const Role cr = role_of(*pl.cols, op, *staged[pl.operand], extent);
+      place_kernel<<<blocks_for((int64_t)cells, 256), 256, 0, s>>>(rr, cr, (int64_t)cells, (int64_t)*cols_n,
+                                                                   (const double*)col.ptr(), mat.get(), held.get(),
+                                                                   dup.get());
+      ctx.kernels++;
+      EF_LAUNCH_CHECK();
+    }
+    unsigned d = 0;
+    EF_CUDA(cudaMemcpyAsync(&d, dup.get(), 4, cudaMemcpyDeviceToHost, s));
+    EF_CUDA(cudaStreamSynchronize(s));
+    if (d) decline("an operand with a repeated cell");
+    matrices.push_back(std::move(mat));
+  }
+  uint64_t out_cells = 0;
+  if (!checked_mul(nx, ny, &out_cells) || out_cells >= UINT32_MAX) decline("an output of 2^32 cells or more");
+  ctx.phase("fused: place");
+
+  DeviceBuffer<uint8_t> jflag((size_t)std::max<uint64_t>(nj, 1), s);
+  DeviceBuffer<double> largest((size_t)std::max<uint64_t>(nj, 1), s), smallest((size_t)std::max<uint64_t>(nj, 1), s);
+  if (nj) {
+    value_stats<<<blocks_for((int64_t)nj * 32, 256), 256, 0, s>>>((int64_t)nj, (int64_t)ny, matrices.back().get(),
+                                                                  jflag.get(), largest.get(), smallest.get());
+    ctx.kernels++;
+    EF_LAUNCH_CHECK();
+  }
+
+  // Expressions, with column nodes pointing at their slots.
+  std::vector<ExprNode> snodes = pr.row, wnodes = p.weight;
+  for (auto& e : snodes)
+    if (e.kind == 0) {
+      const auto it = std::find(read.begin(), read.end(), std::make_pair(e.a, e.b));
+      e.a = (int)(it - read.begin());
+    }
+  for (auto& e : wnodes)
+    if (e.kind == 0) e.a = 0;
+  DeviceBuffer<ExprNode> dnodes(std::max<size_t>(snodes.size() + wnodes.size(), 1), s);
+  if (!snodes.empty())
+    EF_CUDA(cudaMemcpyAsync(dnodes.get(), snodes.data(), snodes.size() * sizeof(ExprNode), cudaMemcpyHostToDevice, s));
+  if (!wnodes.empty())
+    EF_CUDA(cudaMemcpyAsync(dnodes.get() + snodes.size(), wnodes.data(), wnodes.size() * sizeof(ExprNode),
+                            cudaMemcpyHostToDevice, s));
+
+  TileArgs a{};
+  a.nx = (int64_t)nx;
+  a.ne = (int64_t)ne;
+  a.nj = (int64_t)nj;
+  a.ny = (int64_t)ny;
+  a.mask = mask;
+  a.weight_expr = p.weight_expr;
+  a.scale_kind = p.scale_kind;
+  a.scale_c = p.scale_c;
+  a.shifted = p.shift == 1;
+  a.normalizer = p.normalizer;
+  a.wnodes = dnodes.get() + snodes.size();
+  a.wn = (int)wnodes.size();
+  a.score_expr = pr.row_expr;
+  if (!pr.row_expr) {
+    a.q = matrices[0].get();
+    a.k = matrices[1].get();
+  } else {
+    a.snodes = dnodes.get();
+    a.sn = (int)snodes.size();
+    a.n_slots = (int)read.size();
+    for (size_t i = 0; i < read.size(); i++) {
+      a.mats[i] = matrices[i].get();
+      a.side[i] = read[i].first;
+    }
+  }
+  a.v = matrices.back().get();
+  a.jflag = jflag.get();
+  a.largest = largest.get();
+  a.smallest = smallest.get();
+  DeviceBuffer<double> out((size_t)std::max<uint64_t>(out_cells, 1), s);
+  DeviceBuffer<unsigned long long> visited(1, s);
+  DeviceBuffer<unsigned> overflowed(1, s);
+  visited.zero();
+  overflowed.zero();
+  a.out = out.get();
+  a.visited = visited.get();
+  a.overflowed = overflowed.get();
+  const uint64_t x_tiles = (nx + XT - 1) / XT;
+  if (x_tiles) {
+    EF_CUDA(cudaFuncSetAttribute(fused_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
+    const dim3 grid((unsigned)x_tiles, (unsigned)std::max<uint64_t>((ny + YC - 1) / YC, 1));
+    fused_tiles<<<grid, kThreads, kTileSmem, s>>>(a);
+    ctx.kernels++;
+    EF_LAUNCH_CHECK();
+  }
+  unsigned long long n_visited = 0;
+  unsigned of = 0;
+  EF_CUDA(cudaMemcpyAsync(&n_visited, visited.get(), 8, cudaMemcpyDeviceToHost, s));
+  EF_CUDA(cudaMemcpyAsync(&of, overflowed.get(), 4, cudaMemcpyDeviceToHost, s));
+  EF_CUDA(cudaStreamSynchronize(s));
+  ctx.phase("fused: tiles");
+  if (of) decline("a sum that overflowed or may have underflowed");
+
+  // The pairs of tiles that share a batch (fused.rs:386-397).
+  uint64_t tile_pairs = 0;
+  const uint64_t lnx = (uint64_t)mask.lnx, lnj = (uint64_t)mask.lnj;
+  for (uint64_t t = 0; t < x_tiles; t++) {
+    const uint64_t x0 = t * XT, x1 = std::min<uint64_t>((t + 1) * XT, nx);
+    const uint64_t start = x0 / lnx * lnj, end = (x1 - 1) / lnx * lnj + lnj;
+    tile_pairs += (end + JT - 1) / JT - start / JT;
+  }
+
+  // The rows: every y for each x with an allowed J position, in order.
+  DeviceBuffer<uint8_t> flags((size_t)std::max<uint64_t>(nx, 1), s);
+  DeviceBuffer<int64_t> row_index((size_t)std::max<uint64_t>(nx, 1), s);
+  if (nx) {
+    row_flags<<<blocks_for((int64_t)nx, 256), 256, 0, s>>>((int64_t)nx, (int64_t)nj, mask, flags.get());
+    ctx.kernels++;
+    EF_LAUNCH_CHECK();
+  }
+  const int64_t n_rows = exclusive_scan_flags(ctx, flags.get(), (int64_t)nx, row_index.get());
+  const int64_t n_out = n_rows * (int64_t)ny;
+  OutKeys okeys;
+  if (p.outputs.size() > (size_t)kMaxDims) decline("more than 8 outputs");
+  for (size_t i = 0; i < p.outputs.size(); i++) {
+    const int d = p.outputs[i];
+    const bool in_x = std::find(xs.begin(), xs.end(), d) != xs.end();
+    const std::vector<int>& role = in_x ? xs : ys;
+    const size_t slot = (size_t)(std::find(role.begin(), role.end(), d) - role.begin());
+    int64_t stride = 1;
+    for (size_t e = slot + 1; e < role.size(); e++) stride *= extent[role[e]];
+    okeys.key[okeys.n] = KeyAt{in_x ? 1 : 0, stride, std::max<int64_t>(extent[d], 1)};
+    okeys.width[okeys.n] = width_of(schema[i].kind);
+    okeys.n++;
+  }
+  DeviceBuffer<int64_t> xtab((size_t)std::max<uint64_t>(okeys.n * nx, 1), s),
+      ytab((size_t)std::max<uint64_t>(okeys.n * ny, 1), s);
+  if (nx) key_tables<<<blocks_for((int64_t)nx, 256), 256, 0, s>>>((int64_t)nx, okeys, 1, xtab.get());
+  if (ny) key_tables<<<blocks_for((int64_t)ny, 256), 256, 0, s>>>((int64_t)ny, okeys, 0, ytab.get());
+  ctx.kernels += 2;
+  std::vector<DeviceBuffer<uint8_t>> key_dev;
+  for (int i = 0; i < okeys.n; i++) {
+    key_dev.emplace_back((size_t)(n_out ? n_out * okeys.width[i] : 1), s);
+    okeys.out[i] = key_dev.back().get();
+  }
+  DeviceBuffer<double> vals((size_t)(n_out ? n_out : 1), s);
+  if (n_out) {
+    const dim3 grid2((unsigned)std::max<uint64_t>(1, std::min<uint64_t>((ny + 255) / 256, 64)),
+                     (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(nx, 65535)));
+    emit_rows<<<grid2, 256, 0, s>>>((int64_t)nx, (int64_t)ny, flags.get(), row_index.get(), okeys, xtab.get(),
+                                    ytab.get(), out.get(), vals.get());
+    ctx.kernels++;
+    EF_LAUNCH_CHECK();
+  }
+  OutBatch ob;
+  ob.rows = n_out;
+  for (size_t i = 0; i < p.outputs.size(); i++) {
+    OutColumn c;
+    c.format = schema[i].format;
+    c.name = schema[i].name;
+    c.kind = schema[i].kind;
+    c.nullable = schema[i].nullable;
+    c.length = n_out;
+    c.values = result_buffer(ctx, key_dev[i], (size_t)(n_out * okeys.width[i]), o.result_on_device);
+    ob.columns.push_back(std::move(c));
+  }
+  OutColumn val;
+  val.format = "g";
+  val.kind = Kind::Float64;
+  val.name = schema.back().name;
+  val.nullable = schema.back().nullable;
+  val.length = n_out;
+  val.values = result_buffer(ctx, vals, (size_t)n_out * 8, o.result_on_device);
+  ob.columns.push_back(std::move(val));
+  EF_CUDA(cudaStreamSynchronize(s));
+  FoldOutput result;
+  result.algorithm = EINFOLD_ALG_FUSED;
+  result.batches.push_back(std::move(ob));
+  result.tiles_visited = n_visited;
+  result.tiles = tile_pairs;
+  ctx.phase("fused: result");
+  return result;
+}
+
+}  // namespace ef

@@ -7,10 +7,6 @@ FoldOutput chain_fold(Context&, const FoldD&, const std::vector<const Relation*>
                       const einfold_options&, Budget&) {
   fail(EINFOLD_COMPUTE, "chains are not built yet");
 }
-FoldOutput fused_pipeline(Context&, const PipelineD&, const Relation&, const Relation&, const Relation&,
-                          const std::vector<Field>&, const einfold_options&, Budget&) {
-  fail(EINFOLD_COMPUTE, "the fused pipeline is not built yet");
-}
 
 }  // namespace ef
 

@@ -280,4 +280,48 @@ HostBuffer to_host(Context& ctx, const void* dev, size_t bytes) {
   return h;
 }
 
+__global__ void key_tables(int64_t n, OutKeys keys, int in_x, int64_t* __restrict__ tables) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
+    for (int k = 0; k < keys.n; k++)
+      if (keys.key[k].in_x == in_x) tables[(int64_t)k * n + p] = keys.key[k].at(p, p);
+}
+
+StagedKeys stage_keys(Context& ctx, const OperandD& op, const Relation& r) {
+  StagedKeys s;
+  for (auto& k : op.keys) {
+    const Field& f = r.fields[k.col];
+    if (f.dictionary || !is_integer(f.kind)) decline("a key column that isn't integers");
+    for (auto& b : r.batches)
+      if (b.columns[k.col].nulls() > 0) decline("a NULL key");
+    s.cols.push_back(stage_column(ctx, r, k.col, false));
+    DeviceColumn& c = s.cols.back();
+    KeyStats st;
+    if (c.kind == Kind::Int64) {
+      key_stats_i64(ctx, (const int64_t*)c.ptr(), c.rows, &st);
+      s.keys.push_back((const int64_t*)c.ptr());
+    } else {
+      s.wide.push_back(keys_as_i64(ctx, c, &st));
+      s.keys.push_back(s.wide.back().get());
+    }
+    if (st.negative || st.too_large) decline("a negative key, or one too large for int64");
+    if (st.max == INT64_MAX) decline("a key whose extent doesn't fit");
+    s.extent.push_back(st.max + 1);
+  }
+  return s;
+}
+
+Role role_of(const std::vector<int>& dims, const OperandD& op, const StagedKeys& s, const std::vector<int64_t>& extent) {
+  Role r;
+  if (dims.size() > (size_t)kMaxDims) decline("more than 8 dimensions in one role");
+  for (int d : dims) {
+    int slot = -1;
+    for (size_t i = 0; i < op.keys.size(); i++)
+      if (op.keys[i].dim == d) slot = (int)i;
+    r.keys[r.n] = s.keys[slot];
+    r.extent[r.n] = extent[d];
+    r.n++;
+  }
+  return r;
+}
+
 }  // namespace ef

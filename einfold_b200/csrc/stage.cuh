@@ -8,6 +8,7 @@
 
 #include "arrow.h"
 #include "common.h"
+#include "fold.h"
 
 namespace ef {
 
@@ -76,5 +77,53 @@ __device__ __forceinline__ int64_t role_position(const Role& r, int64_t row) {
   for (int i = 0; i < r.n; i++) p = p * r.extent[i] + r.keys[i][row];
   return p;
 }
+
+// Where output keys come from: position x (in_x) or y, their stride and extent.
+struct KeyAt {
+  int in_x;
+  int64_t stride, extent;
+  __device__ __forceinline__ int64_t at(int64_t x, int64_t y) const { return ((in_x ? x : y) / stride) % extent; }
+};
+
+// The output's key columns: where each key comes from, its width in bytes
+// and its device buffer.
+struct OutKeys {
+  int n = 0;
+  KeyAt key[kMaxDims];
+  int width[kMaxDims];
+  void* out[kMaxDims];
+};
+
+// The keys of output dimensions along x (or y), one table per key:
+// table[k][p] = (p / stride) % extent, so that emitting needs no division.
+__global__ void key_tables(int64_t n, OutKeys keys, int in_x, int64_t* __restrict__ tables);
+
+// An int64 key narrowed to an output column of `width` bytes (Arrow's cast
+// of an in-range value).
+__device__ __forceinline__ void store_key(void* base, int width, int64_t i, int64_t v) {
+  switch (width) {
+    case 1: ((uint8_t*)base)[i] = (uint8_t)v; break;
+    case 2: ((uint16_t*)base)[i] = (uint16_t)v; break;
+    case 4: ((uint32_t*)base)[i] = (uint32_t)v; break;
+    default: ((int64_t*)base)[i] = v; break;
+  }
+}
+
+// Keys of every batch of a relation for one operand, staged as int64, with
+// extents.
+struct StagedKeys {
+  std::vector<DeviceColumn> cols;           // staged columns (int64 ones read in place)
+  std::vector<DeviceBuffer<int64_t>> wide;  // other integer columns widened to int64
+  std::vector<const int64_t*> keys;         // per key of the operand, in op.keys order
+  std::vector<int64_t> extent;              // per key
+};
+
+// Stages an operand's key columns; declines where dense::keys
+// (crates/einfold-kernels/src/dense.rs:97-111) returns None: a key column
+// that isn't integers, a NULL key, a negative one.
+StagedKeys stage_keys(Context& ctx, const OperandD& op, const Relation& r);
+
+// The keys and extents of `dims`, in order, as `op` holds them.
+Role role_of(const std::vector<int>& dims, const OperandD& op, const StagedKeys& s, const std::vector<int64_t>& extent);
 
 }  // namespace ef

@@ -1,0 +1,136 @@
+"""The oracle pinned to the reference's own known answers, on the CPU: the
+SplitMix64 outputs of crates/einfold-testkit/src/rng.rs:66-78, the tile
+counts of crates/einfold-kernels/tests/pipeline_vs_sql.rs:731-760, the
+Bounds cases of crates/einfold-kernels/src/fused.rs:1116-1177, the signed
+zero keys of keys.rs:83-93, the long shared prefixes of
+discriminate.rs:663-683, and the rounding bound and repeatability of the
+dense product (kernels_vs_sql.rs:21-23, gemm.rs:52-89)."""
+import math
+
+import numpy as np
+import pyarrow as pa
+import pytest
+
+from einfold_b200 import ir
+from oracle import oracle
+from tests import pipelines as P
+from tests.tables import complete, matmul_fold, rows_of
+
+GE, GT, LE, LT = (ir.Comparison.GREATER_OR_EQUAL, ir.Comparison.GREATER, ir.Comparison.LESS_OR_EQUAL,
+                  ir.Comparison.LESS)
+
+
+def test_splitmix64_seed_zero_gives_the_reference_outputs():
+    rng = oracle.Rng.seeded(0, 0)
+    assert [rng.next_u64() for _ in range(4)] == [0xE220A8397B1DCDAF, 0x6E789E6AA1B965F4, 0x06C45D188009454F,
+                                                  0xF88BB8A8724C81EC]
+    # The vectorised stream is the same stream.
+    assert list(oracle.Rng.seeded(0, 0).u64s(4)) == [0xE220A8397B1DCDAF, 0x6E789E6AA1B965F4, 0x06C45D188009454F,
+                                                     0xF88BB8A8724C81EC]
+    a, b = oracle.Rng.seeded(5, 1), oracle.Rng.seeded(5, 2)
+    assert a.next_u64() != b.next_u64()
+
+
+def _tiles(l, nb=None, conditions=()):
+    r = P.run_oracle(P.attention(l, nb=nb, conditions=conditions))
+    vals = rows_of(r.batches).column(rows_of(r.batches).num_columns - 1).to_numpy()
+    assert len(vals) == l * (nb or 1)
+    assert np.all(np.abs(vals - 1.0) < 1e-12)  # every average of v = 1 is 1
+    return r.tiles_visited, r.tiles
+
+
+def test_causal_masks_skip_half_the_tiles():
+    assert _tiles(64 * 16, conditions=[(GE, 0)]) == (16 * 17 // 2, 256)
+
+
+def test_sliding_windows_visit_a_band_of_tiles():
+    assert _tiles(64 * 16, conditions=[(GE, 0), (LT, 64)]) == (16 + 15, 256)
+
+
+def test_batches_visit_only_their_own_tiles():
+    assert _tiles(64 * 4, nb=8, conditions=[(GE, 0)]) == (8 * 10, 8 * 16)
+    visited, tiles = _tiles(100, nb=8, conditions=[(GE, 0)])
+    assert tiles <= 13 * 4 and visited <= tiles
+
+
+def _bounds(heaviest, largest):
+    return dict(heaviest=heaviest, lightest=5e-324, largest=largest, smallest=largest, terms=3)
+
+
+def _normal(heaviest, lightest, largest, smallest):
+    return dict(heaviest=heaviest, lightest=lightest, largest=largest, smallest=smallest, terms=3)
+
+
+def _hold(b, z, results, special):
+    return oracle.bounds_hold(b["heaviest"], b["lightest"], b["largest"], b["smallest"], b["terms"], z, results,
+                              special)
+
+
+def test_bounds_cases():
+    assert _hold(_normal(1.0, 0.25, 2.0, 0.5), 1.5, [0.0, 1.0], [False, False])
+    assert _hold(_normal(1.0, 0.25, 2.0, 0.5), None, [0.0], [False])
+    assert _hold(_normal(1.0, 0.25, 0.0, math.inf), 1.5, [0.0], [False])
+    assert not _hold(_normal(1.0, 1.0, 1.0, 1e-300), 1e10, [0.0], [False])
+    assert not _hold(_normal(1.0, 1e-300, 1.0, 1e-10), None, [0.0], [False])
+    assert _hold(_bounds(1.0, 1e5), 1.5, [0.3, -2.0], [False, False])
+    assert _hold(_bounds(1.0, 1e5), None, [0.3, -2.0], [False, False])
+    assert _hold(_bounds(1.1e188, 1.0), 1.1e188, [0.4], [False])
+    assert not _hold(_bounds(1e-323, 0.125), 2e-323, [0.0], [False])
+    assert not _hold(_bounds(2.0, 1e300), 2.0, [2.5e-24], [False])
+    assert not _hold(_bounds(1.0, 1e100), 1e-309, [1e100], [False])
+    assert _hold(_bounds(1.0, 1e100), None, [1e100], [False])
+    assert not _hold(_bounds(1.0, 1e308), None, [1e308], [False])
+    assert _hold(_bounds(1.0, 1.0), 1.0, [0.0, math.inf], [True, True])
+    assert not _hold(_bounds(1.0, 1.0), 1.0, [0.0], [False])
+
+
+def test_signed_zeros_are_one_key_only_when_the_host_says_so():
+    col = pa.array([0.0, -0.0, float("nan")])
+
+    def same(float_keys):
+        enc = oracle._encode_column(oracle.host_keys([col], float_keys)[0])
+        return enc[0] == enc[1]
+
+    assert same(oracle.SIGNED_ZEROS_EQUAL)
+    assert not same(oracle.BITWISE)
+
+
+def test_keys_with_long_shared_prefixes_sort_as_their_bytes():
+    prefix = "p" * 100_000
+    strings = [f"{prefix}{i:03}" for i in reversed(range(200))]
+    r = oracle.ranks_of_bytes(oracle._encode_column(pa.array(strings)))
+    order = sorted(range(200), key=lambda i: strings[i])
+    assert [strings[r.first[k]] for k in range(len(r.first))] == [strings[i] for i in order]
+    assert np.array_equal(r.rank, np.argsort(np.argsort(strings, kind="stable"), kind="stable").astype(np.uint32))
+
+
+def test_dense_product_within_the_rounding_bound_and_repeatable():
+    rng = oracle.Rng.seeded(11, 0)
+    ni, nj, nk = 24, 300, 17
+    a_vals = rng.units(ni * nj) * 2 - 1
+    b_vals = rng.units(nj * nk) * 2 - 1
+    sa, a = complete(["i", "j"], [ni, nj], a_vals, rng)
+    sb, b = complete(["j", "k"], [nj, nk], b_vals, rng)
+    f = matmul_fold()
+    s = oracle.schema(f, [sa, sb])
+    got = rows_of(oracle.dense_fold(f, a, b, None, s, oracle.Options(threads=1)))
+    A, Bm = a_vals.reshape(ni, nj), b_vals.reshape(nj, nk)
+    exact = np.array([[math.fsum(A[i] * Bm[:, k]) for k in range(nk)] for i in range(ni)]).reshape(-1)
+    mag = (np.abs(A) @ np.abs(Bm)).reshape(-1)
+    g = got.column(2).to_numpy()
+    assert np.all(np.abs(g - exact) <= 2 * (nj - 1) * 2.0 ** -53 * mag)
+    # Other batches, another order, another number of threads: the same bits.
+    sa2, a2 = complete(["i", "j"], [ni, nj], a_vals, oracle.Rng.seeded(12, 0), batches=7)
+    again = rows_of(oracle.dense_fold(f, a2, b, None, s, oracle.Options(threads=5)))
+    assert np.array_equal(again.column(2).to_numpy().view(np.uint64), g.view(np.uint64))
+
+
+@pytest.mark.parametrize("threads", [1, 3])
+def test_fused_results_do_not_depend_on_threads_or_batches(threads):
+    def run(seed, threads):
+        case = P.attention(200, d=5, nb=2, conditions=[(GE, 0)], q_value=lambda n: oracle.Rng.seeded(1, 1).units(n),
+                           v_value=lambda n: oracle.Rng.seeded(2, 1).units(n) * 2 - 1, seed=seed)
+        return rows_of(P.run_oracle(case, threads=threads).batches)
+
+    a, b = run(1, threads), run(2, 4)
+    assert a.equals(b)
