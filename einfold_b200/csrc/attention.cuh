@@ -1,0 +1,77 @@
+// Attention-shaped pipelines on the tensor cores: the mask of a pipeline's
+// conditions, and the split forward pass over placed matrices.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "common.h"
+
+namespace ef {
+
+constexpr int kMaxMask = 8;
+
+// The conditions between the one X and the one J dimension of a pipeline,
+// each as `x <cmp> j + off`, and the positions per batch along X and J.
+struct Mask {
+  int n = 0;
+  int cmp[kMaxMask] = {};
+  int64_t off[kMaxMask] = {};
+  int64_t lnx = 1, lnj = 0;
+};
+
+// allowed(x) (fused.rs:350-368): the half-open J interval that X position
+// x may join, the intersection of each condition's, in 128-bit integers,
+// clamped to x's batch.
+__host__ __device__ inline void allowed(const Mask& m, int64_t x, int64_t& lo_out, int64_t& hi_out) {
+  const int64_t group_start = (x / m.lnx) * m.lnj;
+  const __int128 xx = x % m.lnx, n = m.lnj;
+  __int128 lo = 0, hi = n;
+  for (int i = 0; i < m.n; i++) {
+    const __int128 bound = xx - (__int128)m.off[i];
+    switch (m.cmp[i]) {
+      case 3: if (bound + 1 < hi) hi = bound + 1; break;  // x >= j + c
+      case 2: if (bound < hi) hi = bound; break;          // x >  j + c
+      case 1: if (bound > lo) lo = bound; break;          // x <= j + c
+      default: if (bound + 1 > lo) lo = bound + 1; break; // x <  j + c
+    }
+  }
+  const __int128 l = lo < 0 ? 0 : (lo > n ? n : lo);
+  __int128 h = hi > lo ? hi : lo;
+  h = h < 0 ? 0 : (h > n ? n : h);
+  lo_out = group_start + (int64_t)l;
+  hi_out = group_start + (int64_t)h;
+}
+
+// A softmax-weighted average over placed matrices, batch by batch:
+// q [w][x][e], k [w][j][e], v [w][j][y] for w < batches, x < lnx, j < lnj,
+// e < ne, y < ny; out [w·lnx + x][y] = Σ_j exp(s_xj − m_x) v_jy / z_x over the
+// allowed j, with s_xj = scale(q_x · k_j), m_x the row's largest score and
+// z_x its sum of weights; lse (if given) = m_x + ln z_x. `largest` and
+// `smallest` hold each J position's largest and smallest nonzero magnitude
+// of v (for the reference's underflow guard).
+struct AttentionProblem {
+  const double* q = nullptr;
+  const double* k = nullptr;
+  const double* v = nullptr;
+  int64_t batches = 0, lnx = 0, lnj = 0, ne = 0, ny = 0;
+  Mask mask;
+  int scale_kind = 0;  // 0 one, 1 times c, 2 over c
+  double scale_c = 1.0;
+  const double* largest = nullptr;
+  const double* smallest = nullptr;
+  double* out = nullptr;
+  double* lse = nullptr;
+};
+
+enum AttentionOutcome { ATTENTION_DONE = 0, ATTENTION_INELIGIBLE = 1, ATTENTION_GUARDED = 2 };
+
+// The split forward pass: q·k and w·v as int8 digit products on the tensor
+// cores (S slices each, level sums exact in TMEM), the online softmax in
+// FP64. INELIGIBLE when an operand isn't finite or the scores could
+// overflow (nothing written); GUARDED when the reference's overflow or
+// underflow guard fires on a row (the pipeline declines).
+AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int slices, cudaStream_t stream);
+
+}  // namespace ef

@@ -24,6 +24,7 @@
 #include <cmath>
 #include <optional>
 
+#include "attention.cuh"
 #include "fold.h"
 #include "stage.cuh"
 
@@ -32,39 +33,8 @@ namespace {
 
 constexpr int XT = 64, JT = 64;  // fused.rs XT, JT: tiles visited count in these
 constexpr int YC = 64;           // outputs per CTA along y
-constexpr int kMaxMask = 8;
 constexpr int kMaxSlots = 8;
 constexpr int kThreads = 256;
-
-struct Mask {
-  int n = 0;
-  int cmp[kMaxMask] = {};
-  int64_t off[kMaxMask] = {};
-  int64_t lnx = 1, lnj = 0;  // positions per batch along X and J
-};
-
-// allowed(x) (fused.rs:350-368): the half-open J interval that X position
-// x may join, the intersection of each condition's, in 128-bit integers,
-// clamped to x's batch.
-__host__ __device__ inline void allowed(const Mask& m, int64_t x, int64_t& lo_out, int64_t& hi_out) {
-  const int64_t group_start = (x / m.lnx) * m.lnj;
-  const __int128 xx = x % m.lnx, n = m.lnj;
-  __int128 lo = 0, hi = n;
-  for (int i = 0; i < m.n; i++) {
-    const __int128 bound = xx - (__int128)m.off[i];
-    switch (m.cmp[i]) {
-      case 3: if (bound + 1 < hi) hi = bound + 1; break;  // x >= j + c
-      case 2: if (bound < hi) hi = bound; break;          // x >  j + c
-      case 1: if (bound > lo) lo = bound; break;          // x <= j + c
-      default: if (bound + 1 > lo) lo = bound + 1; break; // x <  j + c
-    }
-  }
-  const __int128 l = lo < 0 ? 0 : (lo > n ? n : lo);
-  __int128 h = hi > lo ? hi : lo;
-  h = h < 0 ? 0 : (h > n ? n : h);
-  lo_out = group_start + (int64_t)l;
-  hi_out = group_start + (int64_t)h;
-}
 
 // A postfix expression (expression.rs:61-120) over slots; column nodes
 // carry their slot in `a`. Every operation rounds once, as Rust's f64 does.
@@ -449,7 +419,7 @@ __global__ void __launch_bounds__(kThreads) fused_tiles(const TileArgs p) {
 // infinite, the largest finite magnitude (0 if none) and the smallest
 // nonzero finite one (+inf if none) (fused.rs:371-385). A warp per J.
 __global__ void value_stats(int64_t nj, int64_t ny, const double* __restrict__ v, uint8_t* __restrict__ flag,
-                            double* __restrict__ largest, double* __restrict__ smallest) {
+                            double* __restrict__ largest, double* __restrict__ smallest, unsigned* nonfinite) {
   const int lane = threadIdx.x & 31;
   for (int64_t j = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < nj;
        j += ((int64_t)gridDim.x * blockDim.x) >> 5) {
@@ -471,11 +441,44 @@ __global__ void value_stats(int64_t nj, int64_t ny, const double* __restrict__ v
     lg = warp_max(lg);
     sm = warp_min(sm);
     if (lane == 0) {
+      if (!fin) atomicOr(nonfinite, 1u);
       flag[j] = (fin ? J_FINITE : 0) | (inf ? J_INFINITE : 0);
       largest[j] = lg;
       smallest[j] = sm;
     }
   }
+}
+
+// The pairs of 64 x 64 tiles that fused.rs:749-758 visits: for each X
+// tile, the J tiles between its rows' first and last allowed position that
+// some row's interval meets. A warp per X tile, a row per lane (two rows).
+__global__ void count_tiles(int64_t nx, int64_t nj, Mask m, unsigned long long* visited) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long local = 0;
+  for (int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t * XT < nx;
+       t += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    int64_t lo[2], hi[2];
+    long long first = nj, last = 0;
+    for (int i = 0; i < 2; i++) {
+      const int64_t x = t * XT + lane + 32 * i;
+      lo[i] = hi[i] = 0;
+      if (x < nx) allowed(m, x, lo[i], hi[i]);
+      if (lo[i] < hi[i]) {
+        first = min(first, (long long)lo[i]);
+        last = max(last, (long long)hi[i]);
+      }
+    }
+    for (int o = 16; o; o >>= 1) {
+      first = min(first, __shfl_xor_sync(0xffffffffu, first, o));
+      last = max(last, __shfl_xor_sync(0xffffffffu, last, o));
+    }
+    for (long long j0 = first - first % JT; j0 < last; j0 += JT) {
+      const long long j1 = min(j0 + JT, (long long)nj);
+      const bool meets = (lo[0] < hi[0] && lo[0] < j1 && hi[0] > j0) || (lo[1] < hi[1] && lo[1] < j1 && hi[1] > j0);
+      if (__any_sync(0xffffffffu, meets)) local++;
+    }
+  }
+  if (lane == 0 && local) atomicAdd(visited, local);
 }
 
 // Scatters a column's rows into matrix[row][col]; a repeated cell sets *dup.
@@ -660,12 +663,18 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
 
   DeviceBuffer<uint8_t> jflag((size_t)std::max<uint64_t>(nj, 1), s);
   DeviceBuffer<double> largest((size_t)std::max<uint64_t>(nj, 1), s), smallest((size_t)std::max<uint64_t>(nj, 1), s);
+  DeviceBuffer<unsigned> nonfinite(1, s);
+  nonfinite.zero();
   if (nj) {
     value_stats<<<blocks_for((int64_t)nj * 32, 256), 256, 0, s>>>((int64_t)nj, (int64_t)ny, matrices.back().get(),
-                                                                  jflag.get(), largest.get(), smallest.get());
+                                                                  jflag.get(), largest.get(), smallest.get(),
+                                                                  nonfinite.get());
     ctx.kernels++;
     EF_LAUNCH_CHECK();
   }
+  unsigned v_nonfinite = 0;
+  EF_CUDA(cudaMemcpyAsync(&v_nonfinite, nonfinite.get(), 4, cudaMemcpyDeviceToHost, s));
+  EF_CUDA(cudaStreamSynchronize(s));
 
   // Expressions, with column nodes pointing at their slots.
   std::vector<ExprNode> snodes = pr.row, wnodes = p.weight;
@@ -722,7 +731,38 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
   a.visited = visited.get();
   a.overflowed = overflowed.get();
   const uint64_t x_tiles = (nx + XT - 1) / XT;
-  if (x_tiles) {
+  // The split form on the tensor cores, where it applies: product scores, a
+  // softmax shifted by the kept maximum, an average, finite operands.
+  bool split_done = false;
+  const int64_t batches_w = mask.lnx > 0 ? (int64_t)nx / mask.lnx : 0;
+  if (o.precision == 0 && !pr.row_expr && !p.weight_expr && p.shift == 1 && p.normalizer != 2 && !v_nonfinite &&
+      nx > 0 && nj > 0 && ny > 0 && batches_w * mask.lnx == (int64_t)nx && batches_w * mask.lnj == (int64_t)nj) {
+    AttentionProblem ap;
+    ap.q = matrices[0].get();
+    ap.k = matrices[1].get();
+    ap.v = matrices.back().get();
+    ap.batches = batches_w;
+    ap.lnx = mask.lnx;
+    ap.lnj = mask.lnj;
+    ap.ne = (int64_t)ne;
+    ap.ny = (int64_t)ny;
+    ap.mask = mask;
+    ap.scale_kind = p.scale_kind;
+    ap.scale_c = p.scale_c;
+    ap.largest = largest.get();
+    ap.smallest = smallest.get();
+    ap.out = out.get();
+    const int slices = o.slices > 0 ? o.slices : 6;
+    const AttentionOutcome r = attention_split(ctx, ap, slices, s);
+    if (r == ATTENTION_GUARDED) decline("a sum that overflowed or may have underflowed");
+    if (r == ATTENTION_DONE) {
+      split_done = true;
+      count_tiles<<<blocks_for(x_tiles * 32, 256), 256, 0, s>>>((int64_t)nx, (int64_t)nj, mask, visited.get());
+      ctx.kernels++;
+      EF_LAUNCH_CHECK();
+    }
+  }
+  if (x_tiles && !split_done) {
     EF_CUDA(cudaFuncSetAttribute(fused_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
     const dim3 grid((unsigned)x_tiles, (unsigned)std::max<uint64_t>((ny + YC - 1) / YC, 1));
     fused_tiles<<<grid, kThreads, kTileSmem, s>>>(a);

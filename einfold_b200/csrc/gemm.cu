@@ -23,126 +23,24 @@
 #include <type_traits>
 
 #include "gemm.cuh"
+#include "ptx.cuh"
 
 namespace ef {
 namespace {
+
+using namespace ptx;
 
 constexpr int BM = 128;  // rows of A per tile (TMEM lanes)
 constexpr int BN = 64;   // columns of C per tile (per level)
 constexpr int BK = 64;   // bytes (int8 values) of k per pipeline stage
 constexpr int kThreads = 192;
-constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s: a bounded wait's limit
 constexpr int kGroup = 8;                    // tile rows per raster group
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ uint64_t now_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Waits for the phase of `parity` to complete, for at most kWaitNs. Waiters
-// that expect a long wait (the epilogue) back off between polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, bool patient = false) {
-  if (mbar_try_wait(bar, parity)) return true;
-  uint64_t start = now_ns();
-  while (!mbar_try_wait(bar, parity)) {
-    if (now_ns() - start > kWaitNs) return false;
-    if (patient) __nanosleep(256);
-  }
-  return true;
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
-      ::"r"(smem_u32(dst)), "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
-      : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t cols) {
-  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)), "r"(cols)
-               : "memory");
-}
-__device__ __forceinline__ void tmem_relinquish() {
-  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t cols) {
-  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(cols) : "memory");
-}
-
-// D (+)= A · B^T for int8 A (128 x 32) and B (N x 32), both K-major in
-// shared memory, D int32 in TMEM.
-__device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
-                                        uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n"
-      ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
-      : "memory");
-}
-
-__device__ __forceinline__ void umma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t* v) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-      : "r"(taddr));
-}
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-
-// 2^e for |e| < 1022, exactly, from its bits.
-__device__ __forceinline__ double pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
 // 2^{-8l}.
 __device__ __forceinline__ double exp2_neg8(int l) { return pow2(-8 * l); }
 
-// Shared-memory matrix descriptor: K-major, 64-byte swizzle, 8-row groups
-// 512 bytes apart (the layout TMA writes with CU_TENSOR_MAP_SWIZZLE_64B).
-__device__ __forceinline__ uint64_t desc_sw64(uint32_t addr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((addr & 0x3FFFFu) >> 4);  // start address
-  d |= (uint64_t)1 << 16;                   // leading byte offset (unused here)
-  d |= (uint64_t)(512 >> 4) << 32;          // stride byte offset: 8 rows x 64 B
-  d |= (uint64_t)1 << 46;                   // descriptor version for sm_100
-  d |= (uint64_t)4 << 61;                   // 64-byte swizzle
-  return d;
-}
-
-// Instruction descriptor: int8 x int8 -> int32, K-major A and B, M = 128.
-__host__ __device__ constexpr uint32_t idesc_i8(int n) {
-  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
-}
+// Instruction descriptor of the split product: M = BM.
+__host__ __device__ constexpr uint32_t idesc_i8(int n) { return ptx::idesc_i8(BM, n); }
 
 template <int S>
 struct SplitShape {
@@ -729,6 +627,38 @@ void split_gemm(Context& ctx, const double* a, const double* b, bool b_natural, 
     return;
   }
   dispatch_slices(slices, [&](auto S) { split_gemm_s<decltype(S)::value>(ctx, a, b, b_natural, c, batches, m, n, k, stream); });
+}
+
+void slice_rows_into(int S, const double* x, int64_t batches, int64_t rows, int64_t k, int64_t ld, int64_t rows_pad,
+                     int64_t k_pad, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream) {
+  if (batches <= 0 || rows_pad <= 0) return;
+  dispatch_slices(S, [&](auto SS) {
+    slice_rows<decltype(SS)::value><<<blocks_for((uint64_t)(batches * rows_pad), 1, 148 * 8), 256, 0, stream>>>(
+        x, batches, rows, k, ld, rows_pad, k_pad, e_out, digits, status);
+  });
+  EF_LAUNCH_CHECK();
+}
+
+void slice_cols_into(int S, const double* x, int64_t batches, int64_t k, int64_t n, int64_t n_pad, int64_t k_pad,
+                     unsigned long long* colmax, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream) {
+  if (batches <= 0 || n_pad <= 0 || k_pad <= 0) return;
+  if (n_pad % 64 || k_pad % 64) fail(EINFOLD_INVALID, "column digits need multiples of 64");
+  EF_CUDA(cudaMemsetAsync(colmax, 0, (size_t)(batches * n) * 8, stream));
+  if (n > 0 && k > 0) {
+    const unsigned splits = (unsigned)std::min<int64_t>(64, (k + 127) / 128);
+    col_max<<<dim3((unsigned)((n + 255) / 256), splits, (unsigned)batches), 256, 0, stream>>>(x, batches, k, n, colmax,
+                                                                                             status);
+  }
+  dispatch_slices(S, [&](auto SS) {
+    col_digits<decltype(SS)::value><<<dim3((unsigned)(n_pad / 64), (unsigned)(k_pad / 64), (unsigned)batches), 256, 0,
+                                      stream>>>(x, k, n, n_pad, k_pad, colmax, e_out, digits);
+  });
+  EF_LAUNCH_CHECK();
+}
+
+CUtensorMap digit_planes_map(const int8_t* digits, int64_t k_pad, int64_t rows, int64_t planes, int box_rows,
+                             int box_planes) {
+  return digit_map(digits, k_pad, rows, planes, box_rows, box_planes);
 }
 
 void fp64_gemm(Context& ctx, const double* a, const uint32_t* held, const double* b, double* c, int64_t batches,

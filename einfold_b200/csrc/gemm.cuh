@@ -1,6 +1,7 @@
 // Dense products for the dense fold and the device entry points.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -31,6 +32,24 @@ void split_gemm(Context& ctx, const double* a, const double* b, bool b_natural, 
 void fp64_gemm(Context& ctx, const double* a, const uint32_t* held, const double* b, double* c, int64_t batches,
                int64_t m, int64_t n, int64_t k, int64_t batch_of_row, int64_t zblock, bool fused_multiply_add,
                cudaStream_t stream);
+
+// The split product's operand slicing, for kernels that stage digits
+// themselves. Rows of x [batches][rows][k] (leading dimension ld) become S
+// int8 digit planes digits[(w·S + s)][r][kk] for r < rows_pad, kk < k_pad
+// (zeros beyond), each row under a power-of-two scale 2^e with e in
+// e_out[w·rows_pad + r]; status bit 1 if a value isn't finite.
+void slice_rows_into(int S, const double* x, int64_t batches, int64_t rows, int64_t k, int64_t ld, int64_t rows_pad,
+                     int64_t k_pad, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream);
+// Columns of x [batches][k][n] become K-major digit planes
+// digits[(w·S + s)][col][kk] for col < n_pad and kk < k_pad (both multiples
+// of 64), each column under its own power of two, e_out[w·n_pad + col];
+// colmax is scratch of batches·n words.
+void slice_cols_into(int S, const double* x, int64_t batches, int64_t k, int64_t n, int64_t n_pad, int64_t k_pad,
+                     unsigned long long* colmax, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream);
+// A TMA map over digit planes [planes][rows][k_pad] (uint8), boxes of 64
+// bytes of k by box_rows rows by box_planes planes, 64-byte swizzle.
+CUtensorMap digit_planes_map(const int8_t* digits, int64_t k_pad, int64_t rows, int64_t planes, int box_rows,
+                             int box_planes);
 
 // BT[w][j][i] = B[w][i][j] for a [batches][rows][cols] array.
 void transpose(const double* b, double* bt, int64_t batches, int64_t rows, int64_t cols, cudaStream_t stream);
