@@ -1,8 +1,10 @@
 // The extern "C" entry points of include/einfold_b200.h.
+#include <cmath>
 #include <cstring>
 #include <cstdlib>
 #include <mutex>
 
+#include "attention.cuh"
 #include "fold.h"
 #include "gemm.cuh"
 #include "rank.cuh"
@@ -272,6 +274,78 @@ int32_t einfold_fp64_gemm(einfold_context* ctx, const double* a, const double* b
       ef::transpose(b, bn.get(), batches, n, k, s);
       ef::fp64_gemm(cx, a, nullptr, bn.get(), c, batches, m, n, k, 0, 0, false, s);
     }
+    EF_CUDA(cudaStreamSynchronize(s));
+    return EINFOLD_OK;
+  });
+}
+
+static ef::AttentionProblem attention_problem(const double* q, const double* k, const double* v, double* out,
+                                              double* lse, int64_t batches, int64_t lq, int64_t lk, int64_t d,
+                                              int64_t dv, int32_t n_conditions, const int32_t* comparisons,
+                                              const int64_t* offsets, double scale) {
+  if (batches < 0 || lq < 0 || lk < 0 || d < 0 || dv < 0) ef::fail(EINFOLD_INVALID, "a negative extent");
+  if (n_conditions < 0 || n_conditions > ef::kMaxMask)
+    ef::fail(EINFOLD_INVALID, "0 to 8 conditions, not %d", n_conditions);
+  if (n_conditions && (!comparisons || !offsets)) ef::fail(EINFOLD_INVALID, "conditions without comparisons or offsets");
+  if (!std::isfinite(scale)) ef::fail(EINFOLD_INVALID, "a scale that isn't finite");
+  ef::AttentionProblem p;
+  p.q = q;
+  p.k = k;
+  p.v = v;
+  p.out = out;
+  p.lse = lse;
+  p.batches = batches;
+  p.lnx = lq;
+  p.lnj = lk;
+  p.ne = d;
+  p.ny = dv;
+  p.mask.n = n_conditions;
+  for (int i = 0; i < n_conditions; i++) {
+    if (comparisons[i] < 0 || comparisons[i] > 3) ef::fail(EINFOLD_INVALID, "a comparison of kind %d", comparisons[i]);
+    p.mask.cmp[i] = comparisons[i];
+    p.mask.off[i] = offsets[i];
+  }
+  p.mask.lnx = lq > 0 ? lq : 1;
+  p.mask.lnj = lk;
+  p.scale_kind = scale == 1.0 ? 0 : 1;
+  p.scale_c = scale;
+  return p;
+}
+
+int32_t einfold_attention_forward(einfold_context* ctx, const double* q, const double* k, const double* v,
+                                  double* out, double* lse, int64_t batches, int64_t lq, int64_t lk, int64_t d,
+                                  int64_t dv, int32_t n_conditions, const int32_t* comparisons,
+                                  const int64_t* offsets, double scale, int32_t precision, int32_t slices,
+                                  void* stream, einfold_result* info) {
+  return guarded(ctx, info, [&](ef::Context& cx) -> int32_t {
+    cudaStream_t s = stream ? (cudaStream_t)stream : cx.stream;
+    ef::AttentionProblem p =
+        attention_problem(q, k, v, out, lse, batches, lq, lk, d, dv, n_conditions, comparisons, offsets, scale);
+    const ef::AttentionOutcome r = ef::attention_forward(cx, p, precision, slices, s);
+    EF_CUDA(cudaStreamSynchronize(s));
+    if (r == ef::ATTENTION_GUARDED) ef::decline("a sum that overflowed or may have underflowed");
+    return EINFOLD_OK;
+  });
+}
+
+int32_t einfold_attention_backward(einfold_context* ctx, const double* q, const double* k, const double* v,
+                                   const double* out, const double* lse, const double* d_out, double* d_q,
+                                   double* d_k, double* d_v, int64_t batches, int64_t lq, int64_t lk, int64_t d,
+                                   int64_t dv, int32_t n_conditions, const int32_t* comparisons,
+                                   const int64_t* offsets, double scale, int32_t precision, void* stream,
+                                   einfold_result* info) {
+  return guarded(ctx, info, [&](ef::Context& cx) -> int32_t {
+    cudaStream_t s = stream ? (cudaStream_t)stream : cx.stream;
+    ef::AttentionGradients g;
+    g.f = attention_problem(q, k, v, nullptr, nullptr, batches, lq, lk, d, dv, n_conditions, comparisons, offsets,
+                            scale);
+    g.out = out;
+    g.lse = lse;
+    g.d_out = d_out;
+    g.d_q = d_q;
+    g.d_k = d_k;
+    g.d_v = d_v;
+    ef::attention_backward(cx, g, precision, s);
     EF_CUDA(cudaStreamSynchronize(s));
     return EINFOLD_OK;
   });

@@ -9,15 +9,18 @@
 //      TMA) multiply on tcgen05 kind::i8, each digit s of q against digits
 //      1..S+1-s of k stacked along N, so that digit pair (s, t) accumulates
 //      in TMEM columns (s + t - 2)·64: level l's exact int32 sum.
-//   2. Eight epilogue warps read the levels (a row per TMEM lane, half the
-//      columns per warp group), combine them in FP64 under the row's and
-//      key's powers of two, apply the mask, update the running maximum
-//      (shared between the two halves), rescale the running sums, and turn
-//      the weights exp(s - m) in [0, 1] into S digit planes of a fixed scale
-//      2^2, written to shared memory in the MMA's 64-byte swizzle.
+//   2. Sixteen epilogue warps read the levels (a row per TMEM lane, a
+//      quarter of the columns per warp group), combine them in FP64 under
+//      the row's and key's powers of two, apply the mask, update the running
+//      maximum (shared between the quarters), and turn the weights
+//      exp(s - m) in [0, 1] into S digit planes of a fixed scale 2^2,
+//      written to shared memory in the MMA's 64-byte swizzle.
 //   3. w·v: the weights' digits against v's column-scaled digits, the same
 //      level scheme, into the same TMEM columns (q·k's levels were read).
-//   4. The epilogue adds the levels to its FP64 sums.
+//   4. The epilogue rescales the row's FP64 running sums and adds the
+//      levels to them. The sums live in the 128 TMEM columns the six
+//      slices' 384 level columns leave free, two 32-bit columns a value, so
+//      that a thread's registers hold only its 16 scores.
 // A TMA producer warp double-buffers k and v tiles; an MMA warp issues both
 // products. Every wait is bounded (2 s); on a timeout the kernel sets a
 // status bit, waits for its copies and MMAs in flight, frees TMEM and
@@ -32,7 +35,9 @@
 #include <cmath>
 
 #include "attention.cuh"
+#include "fastexp.cuh"
 #include "gemm.cuh"
+#include "levels.cuh"
 #include "ptx.cuh"
 
 namespace ef {
@@ -43,8 +48,9 @@ using namespace ptx;
 constexpr int AM = 128;  // query rows per CTA (TMEM lanes)
 constexpr int AJ = 64;   // key positions per tile
 constexpr int AY = 64;   // value columns per CTA
-constexpr int kEpi = 256;
+constexpr int kEpi = 512;     // 16 epilogue warps: a row per TMEM lane, a quarter of the columns each
 constexpr int kAttnThreads = 64 + kEpi;
+constexpr int kSumCol = 384;  // TMEM columns of the rows' FP64 running sums, two per value
 constexpr int kMaxSmem = 232448;
 
 template <int S, int KB>
@@ -53,12 +59,12 @@ struct AttnShape {
   static constexpr int kK = KB * S * AJ * 64;  // k digits per stage [kb][t][64][64 B]
   static constexpr int kV = S * AY * 64;       // v digits per stage [t][64 y][64 B of j]
   static constexpr int kP = S * AM * 64;       // weight digits [s][128][64 B of j]
-  static constexpr int kAux = 4096;            // barriers, row spans, exchanges, exponents
+  static constexpr int kAux = 8192;            // barriers, row spans, exponents, exchanges
   static constexpr int kFixed = kQ + kP + kAux + 1024;
   static constexpr int kStages = kFixed + 2 * (kK + kV) <= kMaxSmem ? 2 : 1;
   static constexpr int kSmem = kFixed + kStages * (kK + kV);
   static_assert(kSmem <= kMaxSmem, "the tiles must fit in shared memory");
-  static_assert(S * 64 <= 512, "the levels must fit in TMEM");
+  static_assert(S * 64 <= kSumCol, "the levels and the running sums must fit in TMEM");
 };
 
 struct AttnArgs {
@@ -70,28 +76,28 @@ struct AttnArgs {
   const int32_t* eq;  // [w][lnx_pad]
   const int32_t* ek;  // [w][lnj_pad]
   const int32_t* ev;  // [w][ny_pad]
-  const double* largest;
-  const double* smallest;
+  const double* rl;   // [w·lnx + x]: the largest magnitude of the values the row weighs
+  const double* rs;   // and the smallest nonzero one (+inf if none)
+  const double* exp_table;
   double* out;  // [w·lnx + x][ny]
   double* lse;  // [w·lnx + x] or null
   int* status;  // bit 0: a guard fired; bit 1: a wait ran out
   unsigned long long* tiles;  // (row tile, key tile) pairs computed
 };
 
-// The S levels of one TMEM column, combined: Σ_l L_l 2^{-8(l+2)}, in groups
-// of three summed exactly in int64 and added from the smallest group up.
+// The S levels of this thread's 4 TMEM columns at `col`.
 template <int S>
-__device__ __forceinline__ double combine(const int32_t (&L)[S][8], int i) {
-  double v = 0.0;
+__device__ __forceinline__ void load_levels(uint32_t lane_addr, int col, int32_t (&L)[S][4]) {
 #pragma unroll
-  for (int g = (S - 1) / 3; g >= 0; g--) {
-    long long part = 0;
-    const int l0 = 3 * g, l1 = (3 * g + 3 < S ? 3 * g + 3 : S);
-#pragma unroll
-    for (int l = l0; l < l1; l++) part = part * 256 + (long long)L[l][i];
-    v += (double)part * pow2(-8 * (l1 + 1));
-  }
-  return v;
+  for (int l = 0; l < S; l++) tmem_ld4(lane_addr + (uint32_t)(l * 64 + col), L[l]);
+  tmem_wait_ld();
+}
+
+template <int S, int KB>
+__device__ __forceinline__ double level_sum(const int32_t (&L)[S][4], int i) {
+  // Level sums of products over 64 values of k fit the int32 pairs.
+  if constexpr (KB == 1) return combine_levels_small<S, 4>(L, i);
+  else return combine_levels<S, 4>(L, i);
 }
 
 template <int S, int KB>
@@ -120,7 +126,9 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
   int* row_lo = (int*)(aux + 256);                // [128]
   int* row_hi = row_lo + AM;                      // [128]
   int* ev_s = row_hi + AM;                        // [64]
-  double* red = (double*)(aux + 2048);            // [2][128]
+  int* ek_s = (int*)(aux + 1536);                 // [2][64], a stage's key exponents
+  double* texp = (double*)(aux + 2048);           // [64]
+  double* red = (double*)(aux + 4096);            // [4][128]
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int xt = (int)(gridDim.x - 1 - blockIdx.x);  // the longest rows of a causal mask first
@@ -168,6 +176,8 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
   } else if (threadIdx.x < AM + AY) {
     const int c = threadIdx.x - AM;
     ev_s[c] = a.y0 + c < a.ny_pad ? a.ev[(int64_t)w * a.ny_pad + a.y0 + c] : 0;
+  } else if (threadIdx.x < AM + AY + 64) {
+    texp[threadIdx.x - AM - AY] = a.exp_table[threadIdx.x - AM - AY];
   }
   __syncthreads();
   const uint32_t tmem = *tmem_slot;
@@ -178,7 +188,8 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
 
   if (warp == 0) {
     if (lane == 0 && n_tiles > 0) {
-      // Producer: q's digits once, then k's and v's per tile.
+      // Producer: q's digits once, then k's and v's per tile, with the
+      // keys' exponents.
       prefetch_map(&tq);
       prefetch_map(&tk);
       prefetch_map(&tv);
@@ -194,11 +205,12 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
           *(volatile int*)failed = 1;
           break;
         }
-        mbar_expect_tx(&kv_full[st], (uint32_t)(Sh::kK + Sh::kV));
+        mbar_expect_tx(&kv_full[st], (uint32_t)(Sh::kK + Sh::kV + AJ * 4));
         const int jl0 = (jt0 + it) * AJ;
         for (int kb = 0; kb < KB; kb++)
           tma_load_3d(sK + st * Sh::kK + kb * S * AJ * 64, &tk, &kv_full[st], kb * 64, jl0, w * S);
         tma_load_3d(sV + st * Sh::kV, &tv, &kv_full[st], jl0, a.y0, w * S);
+        bulk_load(ek_s + st * AJ, a.ek + (int64_t)w * a.lnj_pad + jl0, AJ * 4, &kv_full[st]);
         issued = it + 1;
       }
       // Copies still in flight complete before the CTA may exit.
@@ -269,7 +281,9 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
     }
   } else {
     // Epilogue: warp w reads TMEM lanes 32·(w % 4) .. +31; warps 2..5 take
-    // columns 0..31 of each tile, warps 6..9 columns 32..63.
+    // columns 0..15 of each tile and of the sums, 6..9 columns 16..31, and
+    // so on.
+    constexpr int CW = 16;  // columns per thread
     const int h = (warp - 2) >> 2;
     const int r = (warp & 3) * 32 + lane;
     const int64_t xl = (int64_t)xt * AM + r;
@@ -277,88 +291,67 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
     const int lo = row_lo[r], hi = row_hi[r];
     const int eqr = valid ? a.eq[(int64_t)w * a.lnx_pad + xl] : 0;
     const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    const uint32_t sum_addr = lane_addr + (uint32_t)(kSumCol + h * 2 * CW);
     const double NEG_INF = -INFINITY;
-    double m = NEG_INF, z = 0.0, light = INFINITY, rl = 0.0, rs = INFINITY;
-    long long terms = 0;
-    double o[32];
-#pragma unroll
-    for (int c = 0; c < 32; c++) o[c] = 0.0;
+    const double to_int = pow2(8 * S - 2);
+    double m = NEG_INF, z = 0.0, light = INFINITY;
     bool ok = true;
     for (int it = 0; it < n_tiles; it++) {
-      const int jl0 = (jt0 + it) * AJ;
+      const int jl0 = (jt0 + it) * AJ + h * CW;
+      const int* eks = ek_s + (it % Sh::kStages) * AJ + h * CW;
       ok = named_bar_and(1, kEpi, mbar_wait(qk_full, (uint32_t)(it & 1)));
       if (!ok) break;
       tc_fence_after();
-      double sc[32];
+      double sc[CW];
 #pragma unroll
-      for (int c8 = 0; c8 < 4; c8++) {
-        int32_t L[S][8];
+      for (int c4 = 0; c4 < CW / 4; c4++) {
+        int32_t L[S][4];
+        load_levels<S>(lane_addr, h * CW + c4 * 4, L);
 #pragma unroll
-        for (int l = 0; l < S; l++) tmem_ld8(lane_addr + (uint32_t)(l * AJ + h * 32 + c8 * 8), L[l]);
-        tmem_wait_ld();
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-          const int jl = jl0 + h * 32 + c8 * 8 + i;
-          double s = scale2(combine<S>(L, i), eqr + a.ek[(int64_t)w * a.lnj_pad + jl]);
+        for (int i = 0; i < 4; i++) {
+          const int c = c4 * 4 + i;
+          double s = scale2(level_sum<S, KB>(L, i), eqr + eks[c]);
           if (a.scale_kind == 1) s = s * a.scale_c;
           else if (a.scale_kind == 2) s = __ddiv_rn(s, a.scale_c);
-          sc[c8 * 8 + i] = s;
+          const bool in = valid && jl0 + c >= lo && jl0 + c < hi;
+          sc[c] = in ? s : NEG_INF;
         }
       }
-      // The row's allowed keys in this half tile, their largest score, and
-      // the guard's statistics.
+      // The row's largest score in this tile, over the four quarters.
       double mx = NEG_INF;
 #pragma unroll
-      for (int c = 0; c < 32; c++) {
-        const int jl = jl0 + h * 32 + c;
-        if (valid && jl >= lo && jl < hi) {
-          mx = fmax(mx, sc[c]);
-          light = fmin(light, sc[c]);
-          terms++;
-          rl = fmax(rl, a.largest[(int64_t)w * a.lnj + jl]);
-          rs = fmin(rs, a.smallest[(int64_t)w * a.lnj + jl]);
-        } else {
-          sc[c] = NEG_INF;
-        }
+      for (int c = 0; c < CW; c++) {
+        mx = fmax(mx, sc[c]);
+        if (sc[c] != NEG_INF) light = fmin(light, sc[c]);
       }
       red[h * AM + r] = mx;
       named_bar(1, kEpi);
-      mx = fmax(mx, red[(1 - h) * AM + r]);
+      mx = fmax(fmax(red[r], red[AM + r]), fmax(red[2 * AM + r], red[3 * AM + r]));
       const double m_new = fmax(m, mx);
+      double rescale = 1.0;
       if (m_new != m) {
-        const double rescale = m == NEG_INF ? 0.0 : exp(m - m_new);
+        rescale = m == NEG_INF ? 0.0 : exp_tang(m - m_new, texp);
         z *= rescale;
-#pragma unroll
-        for (int c = 0; c < 32; c++) o[c] *= rescale;
         m = m_new;
       }
       // Weights and their digits: W = w · 2^(8S-2) < 2^(8S-2), balanced
-      // base-256 digits, most significant first.
-      const double to_int = pow2(8 * S - 2);
+      // base-256 digits, most significant first, four columns a word.
+      uint8_t* prow = sP + r * 64;
 #pragma unroll
-      for (int c16 = 0; c16 < 2; c16++) {
-        uint32_t wd[S][4];
+      for (int c4 = 0; c4 < CW / 4; c4++) {
+        uint32_t wd[S][1];
 #pragma unroll
-        for (int s = 0; s < S; s++)
+        for (int s = 0; s < S; s++) wd[s][0] = 0;
 #pragma unroll
-          for (int q = 0; q < 4; q++) wd[s][q] = 0;
-#pragma unroll
-        for (int i = 0; i < 16; i++) {
-          const double s0 = sc[c16 * 16 + i];
-          const double wt = s0 == NEG_INF ? 0.0 : exp(s0 - m);
+        for (int i = 0; i < 4; i++) {
+          const double sv = sc[c4 * 4 + i];
+          const double wt = sv == NEG_INF ? 0.0 : exp_tang(sv - m, texp);
           z += wt;
-          long long W = llrint(wt * to_int);
-#pragma unroll
-          for (int s = S - 1; s >= 0; s--) {
-            const long long d = ((W + 128) & 255) - 128;
-            wd[s][i >> 2] |= ((uint32_t)(d & 255)) << (8 * (i & 3));
-            W = (W - d) >> 8;
-          }
+          cut_digits32<S, 1>(llrint(wt * to_int), i, wd);
         }
+        const uint32_t off = sw64_offset((uint32_t)r, (uint32_t)(h * CW + c4 * 4)) - (uint32_t)r * 64;
 #pragma unroll
-        for (int s = 0; s < S; s++)
-          *(uint4*)(sP + s * AM * 64 + sw64_offset((uint32_t)r, (uint32_t)((2 * h + c16) * 16))) =
-              make_uint4(wd[s][0], wd[s][1], wd[s][2], wd[s][3]);
+        for (int s = 0; s < S; s++) *(uint32_t*)(prow + s * AM * 64 + off) = wd[s][0];
       }
       fence_proxy_async();
       tc_fence_before();
@@ -367,15 +360,26 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
       ok = named_bar_and(1, kEpi, mbar_wait(pv_full, (uint32_t)(it & 1)));
       if (!ok) break;
       tc_fence_after();
+      // sums = sums · rescale + this tile's weighted values, four at a time.
 #pragma unroll
-      for (int c8 = 0; c8 < 4; c8++) {
-        int32_t L[S][8];
+      for (int c4 = 0; c4 < CW / 4; c4++) {
+        int32_t L[S][4];
+        load_levels<S>(lane_addr, h * CW + c4 * 4, L);
+        uint32_t sum[8];
+        if (it > 0) {
+          tmem_ld8(sum_addr + c4 * 8, (int32_t*)sum);
+          tmem_wait_ld();
+        }
 #pragma unroll
-        for (int l = 0; l < S; l++) tmem_ld8(lane_addr + (uint32_t)(l * AY + h * 32 + c8 * 8), L[l]);
-        tmem_wait_ld();
-#pragma unroll
-        for (int i = 0; i < 8; i++) o[c8 * 8 + i] += scale2(combine<S>(L, i), 2 + ev_s[h * 32 + c8 * 8 + i]);
+        for (int i = 0; i < 4; i++) {
+          const double prev = it > 0 ? __hiloint2double((int)sum[2 * i + 1], (int)sum[2 * i]) * rescale : 0.0;
+          const double v = prev + scale2(combine_levels_small<S, 4>(L, i), 2 + ev_s[h * CW + c4 * 4 + i]);
+          sum[2 * i] = (uint32_t)__double2loint(v);
+          sum[2 * i + 1] = (uint32_t)__double2hiint(v);
+        }
+        tmem_st8(sum_addr + c4 * 8, sum);
       }
+      tmem_wait_st();
       tc_fence_before();
       named_bar(1, kEpi);
       if (warp == 2 && lane == 0) mbar_arrive(tmem_free);
@@ -386,34 +390,36 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
         *(volatile int*)failed = 1;
       }
     } else if (n_tiles > 0) {
-      // The two halves' sums and statistics (P's digits are no longer read).
+      // The four quarters' sums of weights and lightest scores (P's digits
+      // are no longer read).
       double* xz = (double*)sP;
-      double* xl_ = xz + 2 * AM;
-      double* xrl = xl_ + 2 * AM;
-      double* xrs = xrl + 2 * AM;
-      long long* xt_ = (long long*)(xrs + 2 * AM);
+      double* xlg = xz + 4 * AM;
       xz[h * AM + r] = z;
-      xl_[h * AM + r] = light;
-      xrl[h * AM + r] = rl;
-      xrs[h * AM + r] = rs;
-      xt_[h * AM + r] = terms;
+      xlg[h * AM + r] = light;
       named_bar(1, kEpi);
-      const int o2 = (1 - h) * AM + r;
-      z += xz[o2];
-      light = fmin(light, xl_[o2]);
-      rl = fmax(rl, xrl[o2]);
-      rs = fmin(rs, xrs[o2]);
-      terms += xt_[o2];
+      z = (xz[r] + xz[AM + r]) + (xz[2 * AM + r] + xz[3 * AM + r]);
+      light = fmin(fmin(xlg[r], xlg[AM + r]), fmin(xlg[2 * AM + r], xlg[3 * AM + r]));
+      tc_fence_after();
+      double o[CW];
+#pragma unroll
+      for (int c4 = 0; c4 < CW / 4; c4++) {
+        uint32_t sum[8];
+        tmem_ld8(sum_addr + c4 * 8, (int32_t*)sum);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 4; i++) o[c4 * 4 + i] = __hiloint2double((int)sum[2 * i + 1], (int)sum[2 * i]);
+      }
       if (valid && lo < hi) {
         // Bounds::hold (fused.rs:1058-1086): the heaviest weight is
         // exp(high - m) = 1, the row's largest score being m.
+        const double rl = a.rl[x_base + xl], rs = a.rs[x_base + xl];
         bool over = !(z <= 1.7976931348623157e308);
         const double normal = 2.0 * 2.2250738585072014e-308;
-        const double heaviest = 1.0, lightest = exp(light - m);
-        const double t2 = 2.0 * (double)terms;
-        bool finite = isfinite(heaviest * rl * t2);
+        const double lightest = exp(light - m);
+        const double t2 = 2.0 * (double)(hi - lo);
+        bool finite = isfinite(rl * t2);
         if (finite) {
-          const double quotient = heaviest / fabs(z);
+          const double quotient = 1.0 / fabs(z);
           finite = isfinite(quotient) && isfinite(quotient * rl * t2);
         }
         const double lost = (t2 * 4.9406564584124654e-324) * ((1.0 / fabs(z) + rl) + 1.0);
@@ -429,8 +435,8 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
         const double rounding = 2.220446049250313e-16 / 4.0;
         double* orow = a.out + (x_base + xl) * a.ny;
 #pragma unroll
-        for (int c = 0; c < 32; c++) {
-          const int64_t y = (int64_t)a.y0 + h * 32 + c;
+        for (int c = 0; c < CW; c++) {
+          const int64_t y = (int64_t)a.y0 + h * CW + c;
           if (y >= a.ny) continue;
           if (!isfinite(o[c])) over = true;
           const double v = __ddiv_rn(o[c], z);
@@ -448,6 +454,54 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
   if (warp == 1) {
     tc_fence_after();
     tmem_dealloc(tmem, 512);
+  }
+}
+
+// Each row's largest and smallest nonzero value magnitude over its allowed
+// keys (the bounds of Bounds::hold), from blocks of 64 keys' extrema.
+__global__ void block_extrema(int64_t nj, const double* __restrict__ largest, const double* __restrict__ smallest,
+                              double* __restrict__ bmax, double* __restrict__ bmin) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t b = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b * 64 < nj;
+       b += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    double mx = 0.0, mn = INFINITY;
+    for (int64_t j = b * 64 + lane; j < min(nj, b * 64 + 64); j += 32) {
+      mx = fmax(mx, largest[j]);
+      mn = fmin(mn, smallest[j]);
+    }
+    for (int o = 16; o; o >>= 1) {
+      mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    }
+    if (lane == 0) {
+      bmax[b] = mx;
+      bmin[b] = mn;
+    }
+  }
+}
+
+__global__ void row_value_bounds(int64_t nx, Mask m, const double* __restrict__ largest,
+                                 const double* __restrict__ smallest, const double* __restrict__ bmax,
+                                 const double* __restrict__ bmin, double* __restrict__ rl, double* __restrict__ rs) {
+  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < nx; x += (int64_t)gridDim.x * blockDim.x) {
+    int64_t lo, hi;
+    allowed(m, x, lo, hi);
+    double mx = 0.0, mn = INFINITY;
+    int64_t j = lo;
+    for (; j < hi && (j & 63); j++) {
+      mx = fmax(mx, largest[j]);
+      mn = fmin(mn, smallest[j]);
+    }
+    for (; j + 64 <= hi; j += 64) {
+      mx = fmax(mx, bmax[j >> 6]);
+      mn = fmin(mn, bmin[j >> 6]);
+    }
+    for (; j < hi; j++) {
+      mx = fmax(mx, largest[j]);
+      mn = fmin(mn, smallest[j]);
+    }
+    rl[x] = mx;
+    rs[x] = mn;
   }
 }
 
@@ -473,10 +527,12 @@ void launch(const CUtensorMap& tq, const CUtensorMap& tk, const CUtensorMap& tv,
 }  // namespace
 
 AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int slices, cudaStream_t stream) {
+  // Six slices: their levels (384 TMEM columns) and the rows' FP64 sums
+  // (128) fill TMEM.
   const int S = slices;
-  if (S != 6 && S != 7) return ATTENTION_INELIGIBLE;
+  if (S != 6) return ATTENTION_INELIGIBLE;
   const int KB = p.ne <= 64 ? 1 : (p.ne <= 128 ? 2 : 0);
-  if (KB == 0 || (S == 7 && KB == 2)) return ATTENTION_INELIGIBLE;
+  if (KB == 0) return ATTENTION_INELIGIBLE;
   if (p.batches <= 0 || p.lnx <= 0 || p.lnj <= 0 || p.ny <= 0) return ATTENTION_INELIGIBLE;
   if (p.lnx > (1 << 30) || p.lnj > (1 << 30) || p.batches > 65535 || p.batches * S > INT32_MAX) return ATTENTION_INELIGIBLE;
   const int64_t W = p.batches;
@@ -531,8 +587,22 @@ AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int sl
   args.eq = eq;
   args.ek = ek;
   args.ev = ev;
-  args.largest = p.largest;
-  args.smallest = p.smallest;
+  // The rows' value bounds for the guard, from blocks of 64 keys.
+  const int64_t nx = W * p.lnx, nj = W * p.lnj;
+  DeviceBuffer<double> bounds((size_t)(2 * nx + 2 * ((nj + 63) / 64)), stream);
+  double* rl = bounds.get();
+  double* rs = rl + nx;
+  double* bmax = rs + nx;
+  double* bmin = bmax + (nj + 63) / 64;
+  block_extrema<<<blocks_for((uint64_t)((nj + 63) / 64) * 32, 256), 256, 0, stream>>>(nj, p.largest, p.smallest, bmax,
+                                                                                     bmin);
+  row_value_bounds<<<blocks_for((uint64_t)nx, 256), 256, 0, stream>>>(nx, p.mask, p.largest, p.smallest, bmax, bmin,
+                                                                      rl, rs);
+  EF_LAUNCH_CHECK();
+  ctx.kernels += 2;
+  args.rl = rl;
+  args.rs = rs;
+  args.exp_table = exp_table(ctx.device);
   args.out = p.out;
   args.lse = p.lse;
   args.status = status + 1;
@@ -544,9 +614,8 @@ AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int sl
   EF_CUDA(cudaEventRecord(e0, stream));
   for (int64_t y0 = 0; y0 < p.ny; y0 += AY) {
     args.y0 = (int)y0;
-    if (S == 6 && KB == 1) launch<6, 1>(tq, tk, tv, args, grid, stream);
-    else if (S == 6) launch<6, 2>(tq, tk, tv, args, grid, stream);
-    else launch<7, 1>(tq, tk, tv, args, grid, stream);
+    if (KB == 1) launch<6, 1>(tq, tk, tv, args, grid, stream);
+    else launch<6, 2>(tq, tk, tv, args, grid, stream);
     ctx.kernels++;
   }
   EF_CUDA(cudaEventRecord(e1, stream));

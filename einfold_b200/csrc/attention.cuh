@@ -74,4 +74,24 @@ enum AttentionOutcome { ATTENTION_DONE = 0, ATTENTION_INELIGIBLE = 1, ATTENTION_
 // underflow guard fires on a row (the pipeline declines).
 AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int slices, cudaStream_t stream);
 
+// The forward pass over placed matrices: the split form when `precision`
+// is 0 and it applies, else the FP64 tile kernel (fused.rs's tile, in FP64
+// on the CUDA cores). Computes each J position's value statistics itself.
+AttentionOutcome attention_forward(Context& ctx, AttentionProblem p, int precision, int slices, cudaStream_t stream);
+
+// The gradients of the forward pass's out, from its saved lse:
+// d_v = Pᵀ·d_out, d_k = scale·dSᵀ·q, d_q = scale·dS·k, with
+// P = exp(s - lse) over the allowed pairs, dS = P∘(d_out·vᵀ - D),
+// D = rowsum(d_out∘out).
+struct AttentionGradients {
+  AttentionProblem f;  // q, k, v, shapes, mask, scale
+  const double* out = nullptr;
+  const double* lse = nullptr;
+  const double* d_out = nullptr;
+  double* d_q = nullptr;
+  double* d_k = nullptr;
+  double* d_v = nullptr;
+};
+void attention_backward(Context& ctx, const AttentionGradients& g, int precision, cudaStream_t stream);
+
 }  // namespace ef

@@ -1,0 +1,760 @@
+// The backward pass of an attention-shaped pipeline: the gradients of the
+// forward pass's average with respect to q, k and v, with the scores
+// recomputed tile by tile from the saved log-sum-exp rather than stored.
+//
+// One kernel shape serves the three gradients. A CTA owns 128 rows of one
+// batch and walks the column tiles of 64 its rows may pair with; per tile
+//   s  = scale · (A1_r · B1_c)                  (product 1)
+//   p  = exp(s - lse_x) on allowed pairs, else 0
+//   dp = A2_r · B2_c, ds = p · (dp - D_x)       (product 2; not for d_v)
+//   out_r += Σ_c w_rc · B3_c,  w = p (d_v) or ds (d_k, d_q)
+// with x the query of the pair and D_x = Σ_y d_out_xy · out_xy:
+//   d_v: rows keys,    A1 = k, B1 = q,                         B3 = d_out
+//   d_k: rows keys,    A1 = k, B1 = q, A2 = v,     B2 = d_out, B3 = q
+//   d_q: rows queries, A1 = q, B1 = k, A2 = d_out, B2 = v,     B3 = k
+// (d_k and d_q then times scale). Each output row is summed by one CTA in
+// column order: no atomics, the same bits on every run.
+//
+// The split form runs every product on tcgen05 kind::i8 over six int8
+// digit planes, as the forward pass does, into TMEM columns 0..383; the
+// weights w are cut into digits under a power of two per row and tile, and
+// the rows' FP64 sums live in TMEM columns 384..511. Sixteen epilogue warps
+// take a quarter of the columns each. The FP64 form runs the same tiles on
+// the CUDA cores.
+#include <algorithm>
+#include <cmath>
+
+#include "attention.cuh"
+#include "fastexp.cuh"
+#include "gemm.cuh"
+#include "levels.cuh"
+#include "ptx.cuh"
+
+namespace ef {
+namespace {
+
+using namespace ptx;
+
+enum GradMode { GRAD_V = 0, GRAD_K = 1, GRAD_Q = 2 };
+
+constexpr int GM = 128, GJ = 64, GY = 64;
+constexpr int kEpi = 512;
+constexpr int kGradThreads = 64 + kEpi;
+constexpr int kSumCol = 384;
+constexpr int kMaxSmem = 232448;
+constexpr int S = 6;
+
+template <int MODE>
+struct GradShape {
+  static constexpr bool kTwo = MODE != GRAD_V;
+  static constexpr int kA1 = S * GM * 64;            // rows' digits, product 1 (64 B of features)
+  static constexpr int kA2 = kTwo ? S * GM * 64 : 0;  // rows' digits, product 2
+  static constexpr int kB1 = S * GJ * 64;            // per stage
+  static constexpr int kB2 = kTwo ? S * GJ * 64 : 0;
+  static constexpr int kB3 = S * GY * 64;
+  static constexpr int kE = 2 * GJ * 4;              // the columns' exponents of products 1 and 2
+  static constexpr int kP = S * GM * 64;
+  static constexpr int kAux = 8192;
+  static constexpr int kFixed = kA1 + kA2 + kP + kAux + 1024;
+  static constexpr int kStage = kB1 + kB2 + kB3 + kE;
+  static constexpr int kStages = kFixed + 2 * kStage <= kMaxSmem ? 2 : 1;
+  static constexpr int kSmem = kFixed + kStages * kStage;
+  static_assert(kSmem <= kMaxSmem, "the tiles must fit in shared memory");
+};
+
+struct GradArgs {
+  Mask mask;  // the columns each row may pair with
+  int64_t lr, lc, lr_pad, lc_pad, dy, dy_pad;
+  int y0;
+  double scale, out_factor;
+  const int32_t* e_a1;  // [w][lr_pad]
+  const int32_t* e_b1;  // [w][lc_pad]
+  const int32_t* e_a2;
+  const int32_t* e_b2;
+  const int32_t* e_b3;  // [w][dy_pad]
+  const double* lse;    // per query: [w·lq + x]
+  const double* dd;     // D per query
+  const double* exp_table;
+  double* out;  // [w·lr + r][dy]
+  int* status;
+  unsigned long long* tiles;
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(kGradThreads, 1)
+    grad_split(const __grid_constant__ CUtensorMap ta1, const __grid_constant__ CUtensorMap tb1,
+               const __grid_constant__ CUtensorMap ta2, const __grid_constant__ CUtensorMap tb2,
+               const __grid_constant__ CUtensorMap tb3, const GradArgs a) {
+  using Sh = GradShape<MODE>;
+  constexpr bool kTwo = Sh::kTwo;
+  constexpr int CW = 16;  // columns per epilogue thread
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t* sA1 = smem;
+  uint8_t* sA2 = sA1 + Sh::kA1;
+  uint8_t* sP = sA2 + Sh::kA2;
+  uint8_t* sB = sP + Sh::kP;  // stages of [B1 | B2 | B3 | exponents]
+  uint8_t* aux = sB + Sh::kStages * Sh::kStage;
+  uint64_t* bars = (uint64_t*)aux;
+  uint64_t* a_full = bars + 0;
+  uint64_t* kv_full = bars + 1;   // [2]
+  uint64_t* kv_empty = bars + 3;  // [2]
+  uint64_t* s1_full = bars + 5;
+  uint64_t* t1_free = bars + 6;
+  uint64_t* s2_full = bars + 7;
+  uint64_t* p_full = bars + 8;
+  uint64_t* o_full = bars + 9;
+  uint64_t* tmem_free = bars + 10;
+  uint32_t* tmem_slot = (uint32_t*)(bars + 16);
+  int* failed = (int*)(tmem_slot + 1);
+  long long* span = (long long*)(tmem_slot + 4);
+  int* row_lo = (int*)(aux + 256);
+  int* row_hi = row_lo + GM;
+  int* e3_s = row_hi + GM;               // [64]
+  double* texp = (double*)(aux + 2048);  // [64]
+  double* red = (double*)(aux + 4096);   // [4][128]
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int rt = (int)(gridDim.x - 1 - blockIdx.x);
+  const int w = blockIdx.y;
+  const int64_t r_base = (int64_t)w * a.lr, c_base = (int64_t)w * a.lc;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 11; i++) mbar_init(&bars[i], 1);
+    *failed = 0;
+    span[0] = LLONG_MAX;
+    span[1] = LLONG_MIN;
+    mbar_fence_init();
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (threadIdx.x < GM) {
+    const int64_t rl = (int64_t)rt * GM + threadIdx.x;
+    int lo = 0, hi = 0;
+    if (rl < a.lr) {
+      int64_t l, h;
+      allowed(a.mask, r_base + rl, l, h);
+      lo = (int)(l - c_base);
+      hi = (int)(h - c_base);
+      if (lo < hi) {
+        atomicMin(&span[0], (long long)lo);
+        atomicMax(&span[1], (long long)hi);
+      }
+    }
+    row_lo[threadIdx.x] = lo;
+    row_hi[threadIdx.x] = hi;
+  } else if (threadIdx.x < GM + GY) {
+    const int c = threadIdx.x - GM;
+    e3_s[c] = a.y0 + c < a.dy_pad ? a.e_b3[(int64_t)w * a.dy_pad + a.y0 + c] : 0;
+  } else if (threadIdx.x < GM + GY + 64) {
+    texp[threadIdx.x - GM - GY] = a.exp_table[threadIdx.x - GM - GY];
+  }
+  __syncthreads();
+  const uint32_t tmem = *tmem_slot;
+  const long long first = span[0], last = span[1];
+  const int ct0 = first < last ? (int)(first / GJ) : 0;
+  const int n_tiles = first < last ? (int)((last + GJ - 1) / GJ) - ct0 : 0;
+  if (threadIdx.x == 0 && n_tiles > 0) atomicAdd(a.tiles, (unsigned long long)n_tiles);
+
+  if (warp == 0) {
+    if (lane == 0 && n_tiles > 0) {
+      prefetch_map(&ta1);
+      prefetch_map(&tb1);
+      prefetch_map(&tb3);
+      mbar_expect_tx(a_full, (uint32_t)(Sh::kA1 + Sh::kA2));
+      tma_load_3d(sA1, &ta1, a_full, 0, rt * GM, w * S);
+      if (kTwo) tma_load_3d(sA2, &ta2, a_full, 0, rt * GM, w * S);
+      int issued = 0;
+      for (int it = 0; it < n_tiles; it++) {
+        const int st = it % Sh::kStages;
+        const uint32_t round = (uint32_t)(it / Sh::kStages);
+        if (*(volatile int*)failed) break;
+        if (!mbar_wait(&kv_empty[st], (round & 1) ^ 1)) {
+          atomicOr(a.status, 2);
+          *(volatile int*)failed = 1;
+          break;
+        }
+        mbar_expect_tx(&kv_full[st], (uint32_t)(Sh::kB1 + Sh::kB2 + Sh::kB3 + (kTwo ? 2 : 1) * GJ * 4));
+        const int cl0 = (ct0 + it) * GJ;
+        uint8_t* stage = sB + st * Sh::kStage;
+        int* es = (int*)(stage + Sh::kB1 + Sh::kB2 + Sh::kB3);
+        tma_load_3d(stage, &tb1, &kv_full[st], 0, cl0, w * S);
+        if (kTwo) tma_load_3d(stage + Sh::kB1, &tb2, &kv_full[st], 0, cl0, w * S);
+        tma_load_3d(stage + Sh::kB1 + Sh::kB2, &tb3, &kv_full[st], cl0, a.y0, w * S);
+        bulk_load(es, a.e_b1 + (int64_t)w * a.lc_pad + cl0, GJ * 4, &kv_full[st]);
+        if (kTwo) bulk_load(es + GJ, a.e_b2 + (int64_t)w * a.lc_pad + cl0, GJ * 4, &kv_full[st]);
+        issued = it + 1;
+      }
+      mbar_wait(a_full, 0);
+      for (int it = std::max(0, issued - Sh::kStages); it < issued; it++)
+        mbar_wait(&kv_full[it % Sh::kStages], (uint32_t)((it / Sh::kStages) & 1));
+    }
+  } else if (warp == 1) {
+    if (lane == 0 && n_tiles > 0) {
+      uint64_t* last_bar = nullptr;
+      uint32_t last_parity = 0;
+      bool ok = mbar_wait(a_full, 0);
+      // D (+)= A · B over S digit planes, the level scheme of the forward pass.
+      auto product = [&](uint32_t a_base, uint32_t b_base, int n) {
+#pragma unroll
+        for (int kk = 0; kk < 2; kk++)
+#pragma unroll
+          for (int s = 1; s <= S; s++) {
+            const int total = (S + 1 - s) * n;
+#pragma unroll
+            for (int nn0 = 0; nn0 < total; nn0 += 256) {
+              const int nn = total - nn0 < 256 ? total - nn0 : 256;
+              umma_i8(tmem + (uint32_t)((s - 1) * n + nn0), desc_sw64(a_base + (s - 1) * GM * 64 + kk * 32),
+                      desc_sw64(b_base + nn0 * 64 + kk * 32), idesc_i8(GM, nn), (kk > 0 || s > 1) ? 1u : 0u);
+            }
+          }
+      };
+      for (int it = 0; ok && it < n_tiles; it++) {
+        const int st = it % Sh::kStages;
+        const uint32_t round = (uint32_t)(it / Sh::kStages);
+        const uint32_t par = (uint32_t)(it & 1);
+        ok = mbar_wait(&kv_full[st], round & 1) && (it == 0 || mbar_wait(tmem_free, par ^ 1));
+        if (!ok || *(volatile int*)failed) break;
+        tc_fence_after();
+        const uint32_t stage = smem_u32(sB + st * Sh::kStage);
+        product(smem_u32(sA1), stage, GJ);
+        umma_commit(s1_full);
+        last_bar = s1_full;
+        last_parity = par;
+        if (kTwo) {
+          ok = mbar_wait(t1_free, par);
+          if (!ok || *(volatile int*)failed) break;
+          tc_fence_after();
+          product(smem_u32(sA2), stage + Sh::kB1, GJ);
+          umma_commit(s2_full);
+          last_bar = s2_full;
+        }
+        ok = mbar_wait(p_full, par);
+        if (!ok || *(volatile int*)failed) break;
+        tc_fence_after();
+        product(smem_u32(sP), stage + Sh::kB1 + Sh::kB2, GY);
+        umma_commit(o_full);
+        umma_commit(&kv_empty[st]);
+        last_bar = o_full;
+      }
+      if (!ok) {
+        atomicOr(a.status, 2);
+        *(volatile int*)failed = 1;
+      }
+      if (last_bar) mbar_wait(last_bar, last_parity);
+    }
+  } else {
+    const int h = (warp - 2) >> 2;
+    const int r = (warp & 3) * 32 + lane;
+    const int64_t rl = (int64_t)rt * GM + r;
+    const bool valid = rl < a.lr;
+    const int lo = row_lo[r], hi = row_hi[r];
+    const int e1r = valid ? a.e_a1[(int64_t)w * a.lr_pad + rl] : 0;
+    const int e2r = (kTwo && valid) ? a.e_a2[(int64_t)w * a.lr_pad + rl] : 0;
+    // A row of queries reads its own lse and D; a row of keys its columns'.
+    const double lse_r = (MODE == GRAD_Q && valid) ? a.lse[r_base + rl] : 0.0;
+    const double dd_r = (MODE == GRAD_Q && valid) ? a.dd[r_base + rl] : 0.0;
+    const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    const uint32_t sum_addr = lane_addr + (uint32_t)(kSumCol + h * 2 * CW);
+    bool ok = true;
+    for (int it = 0; it < n_tiles; it++) {
+      const int st = it % Sh::kStages;
+      const int cl0 = (ct0 + it) * GJ + h * CW;
+      const int* es = (const int*)(sB + st * Sh::kStage + Sh::kB1 + Sh::kB2 + Sh::kB3) + h * CW;
+      const uint32_t par = (uint32_t)(it & 1);
+      ok = named_bar_and(1, kEpi, mbar_wait(s1_full, par));
+      if (!ok) break;
+      tc_fence_after();
+      double wv[CW];
+#pragma unroll
+      for (int c4 = 0; c4 < CW / 4; c4++) {
+        int32_t L[S][4];
+#pragma unroll
+        for (int l = 0; l < S; l++) tmem_ld4(lane_addr + (uint32_t)(l * GJ + h * CW + c4 * 4), L[l]);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          const int c = c4 * 4 + i;
+          const int cl = cl0 + c;
+          double p = 0.0;
+          if (valid && cl >= lo && cl < hi) {
+            const double s = a.scale * scale2(combine_levels_small<S, 4>(L, i), e1r + es[c]);
+            p = exp_tang(s - (MODE == GRAD_Q ? lse_r : a.lse[c_base + cl]), texp);
+          }
+          wv[c] = p;
+        }
+      }
+      if (kTwo) {
+        tc_fence_before();
+        named_bar(1, kEpi);
+        if (warp == 2 && lane == 0) mbar_arrive(t1_free);
+        ok = named_bar_and(1, kEpi, mbar_wait(s2_full, par));
+        if (!ok) break;
+        tc_fence_after();
+#pragma unroll
+        for (int c4 = 0; c4 < CW / 4; c4++) {
+          int32_t L[S][4];
+#pragma unroll
+          for (int l = 0; l < S; l++) tmem_ld4(lane_addr + (uint32_t)(l * GJ + h * CW + c4 * 4), L[l]);
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            const int c = c4 * 4 + i;
+            const int cl = cl0 + c;
+            if (wv[c] != 0.0) {
+              const double dp = scale2(combine_levels_small<S, 4>(L, i), e2r + es[GJ + c]);
+              wv[c] = wv[c] * (dp - (MODE == GRAD_Q ? dd_r : a.dd[c_base + cl]));
+            }
+          }
+        }
+      }
+      // The row's power of two for this tile, over the four quarters.
+      double mx = 0.0;
+#pragma unroll
+      for (int c = 0; c < CW; c++) mx = fmax(mx, fabs(wv[c]));
+      red[h * GM + r] = mx;
+      named_bar(1, kEpi);
+      const int ew = slice_exponent(fmax(fmax(red[r], red[GM + r]), fmax(red[2 * GM + r], red[3 * GM + r])));
+      // The weights' digits: W = w · 2^(8S - ew), |W| < 2^(8S-2).
+      const int shift = 8 * S - ew;
+      uint8_t* prow = sP + r * 64;
+#pragma unroll
+      for (int c4 = 0; c4 < CW / 4; c4++) {
+        uint32_t wd[S][1];
+#pragma unroll
+        for (int s = 0; s < S; s++) wd[s][0] = 0;
+#pragma unroll
+        for (int i = 0; i < 4; i++) cut_digits32<S, 1>(llrint(scale2(wv[c4 * 4 + i], shift)), i, wd);
+        const uint32_t off = sw64_offset((uint32_t)r, (uint32_t)(h * CW + c4 * 4)) - (uint32_t)r * 64;
+#pragma unroll
+        for (int s = 0; s < S; s++) *(uint32_t*)(prow + s * GM * 64 + off) = wd[s][0];
+      }
+      fence_proxy_async();
+      tc_fence_before();
+      named_bar(1, kEpi);
+      if (warp == 2 && lane == 0) mbar_arrive(p_full);
+      ok = named_bar_and(1, kEpi, mbar_wait(o_full, par));
+      if (!ok) break;
+      tc_fence_after();
+#pragma unroll
+      for (int c4 = 0; c4 < CW / 4; c4++) {
+        int32_t L[S][4];
+#pragma unroll
+        for (int l = 0; l < S; l++) tmem_ld4(lane_addr + (uint32_t)(l * GY + h * CW + c4 * 4), L[l]);
+        uint32_t sum[8];
+        if (it > 0) tmem_ld8(sum_addr + c4 * 8, (int32_t*)sum);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          const double prev = it > 0 ? __hiloint2double((int)sum[2 * i + 1], (int)sum[2 * i]) : 0.0;
+          const double v = prev + scale2(combine_levels_small<S, 4>(L, i), ew + e3_s[h * CW + c4 * 4 + i]);
+          sum[2 * i] = (uint32_t)__double2loint(v);
+          sum[2 * i + 1] = (uint32_t)__double2hiint(v);
+        }
+        tmem_st8(sum_addr + c4 * 8, sum);
+      }
+      tmem_wait_st();
+      tc_fence_before();
+      named_bar(1, kEpi);
+      if (warp == 2 && lane == 0) mbar_arrive(tmem_free);
+    }
+    if (!ok) {
+      if (warp == 2 && lane == 0) {
+        atomicOr(a.status, 2);
+        *(volatile int*)failed = 1;
+      }
+    } else {
+      // Every lane of the warp reads TMEM (the loads are warp-wide); the
+      // rows past the batch's end write nothing.
+      tc_fence_after();
+      double* orow = a.out + (r_base + rl) * a.dy;
+#pragma unroll
+      for (int c4 = 0; c4 < CW / 4; c4++) {
+        uint32_t sum[8];
+        if (n_tiles > 0) {
+          tmem_ld8(sum_addr + c4 * 8, (int32_t*)sum);
+          tmem_wait_ld();
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          const int64_t y = (int64_t)a.y0 + h * CW + c4 * 4 + i;
+          const double v = n_tiles > 0 ? __hiloint2double((int)sum[2 * i + 1], (int)sum[2 * i]) : 0.0;
+          if (valid && y < a.dy) orow[y] = a.out_factor * v;
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+// The same tiles in FP64 on the CUDA cores: 64 rows by 64 outputs per CTA,
+// a 4 x 4 block of (row, output) per thread.
+constexpr int FT = 64;
+struct GradFp64Args {
+  Mask mask;
+  int64_t lr, lc, d1, d2, dy;  // rows, columns per batch; widths of products 1, 2 and the values
+  double scale, out_factor;
+  const double* a1;  // [w·lr + r][d1]
+  const double* b1;  // [w·lc + c][d1]
+  const double* a2;  // [w·lr + r][d2]
+  const double* b2;  // [w·lc + c][d2]
+  const double* b3;  // [w·lc + c][dy]
+  const double* lse;
+  const double* dd;
+  double* out;  // [w·lr + r][dy]
+};
+
+constexpr size_t kFp64Smem = sizeof(double) * (FT * (FT + 1) + 2 * 32 * (FT + 1));
+
+template <int MODE>
+__global__ void __launch_bounds__(256) grad_fp64(const GradFp64Args a) {
+  extern __shared__ __align__(16) unsigned char smem_fp64[];
+  double(*blk)[FT + 1] = reinterpret_cast<double(*)[FT + 1]>(smem_fp64);
+  double(*sa)[FT + 1] = reinterpret_cast<double(*)[FT + 1]>(smem_fp64 + sizeof(double) * FT * (FT + 1));
+  double(*sb)[FT + 1] = sa + 32;
+  __shared__ int s_lo[FT], s_hi[FT];
+  __shared__ long long s_first, s_last;
+  const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+  const int w = blockIdx.z;
+  const int64_t r0 = (int64_t)blockIdx.x * FT, y0 = (int64_t)blockIdx.y * FT;
+  const int64_t r_base = (int64_t)w * a.lr, c_base = (int64_t)w * a.lc;
+  const int rows = (int)std::min<int64_t>(FT, a.lr - r0);
+  if (t == 0) {
+    s_first = LLONG_MAX;
+    s_last = LLONG_MIN;
+  }
+  __syncthreads();
+  if (t < FT) {
+    int lo = 0, hi = 0;
+    if (t < rows) {
+      int64_t l, h;
+      allowed(a.mask, r_base + r0 + t, l, h);
+      lo = (int)(l - c_base);
+      hi = (int)(h - c_base);
+      if (lo < hi) {
+        atomicMin(&s_first, (long long)lo);
+        atomicMax(&s_last, (long long)hi);
+      }
+    }
+    s_lo[t] = lo;
+    s_hi[t] = hi;
+  }
+  __syncthreads();
+  const long long first = s_first, last = s_last;
+  double acc[4][4] = {};
+  // Σ_e A[r][e] B[c][e] for this thread's 4 x 4 (row, column) pairs.
+  auto product = [&](const double* A, const double* B, int64_t dk, int64_t c0, int width, double (&o)[4][4]) {
+    for (int i = 0; i < 4; i++)
+      for (int j = 0; j < 4; j++) o[i][j] = 0.0;
+    for (int64_t e0 = 0; e0 < dk; e0 += 32) {
+      const int ec = (int)std::min<int64_t>(32, dk - e0);
+      for (int idx = t; idx < FT * 32; idx += 256) {
+        const int rr = idx >> 5, e = idx & 31;
+        sa[e][rr] = (rr < rows && e < ec) ? A[(r_base + r0 + rr) * dk + e0 + e] : 0.0;
+        sb[e][rr] = (rr < width && e < ec) ? B[(c_base + c0 + rr) * dk + e0 + e] : 0.0;
+      }
+      __syncthreads();
+      for (int e = 0; e < ec; e++)
+        for (int i = 0; i < 4; i++)
+          for (int j = 0; j < 4; j++) o[i][j] = fma(sa[e][ty + 16 * i], sb[e][tx + 16 * j], o[i][j]);
+      __syncthreads();
+    }
+  };
+  for (long long c0 = first < last ? first - first % FT : 0; c0 < last; c0 += FT) {
+    const int width = (int)std::min<long long>(FT, a.lc - c0);
+    double s[4][4];
+    product(a.a1, a.b1, a.d1, c0, width, s);
+    double dp[4][4];
+    if (MODE != GRAD_V) product(a.a2, a.b2, a.d2, c0, width, dp);
+    for (int i = 0; i < 4; i++)
+      for (int j = 0; j < 4; j++) {
+        const int rr = ty + 16 * i, cc = tx + 16 * j;
+        const int64_t cl = c0 + cc;
+        double wgt = 0.0;
+        if (rr < rows && cc < width && cl >= s_lo[rr] && cl < s_hi[rr]) {
+          const int64_t xq = MODE == GRAD_Q ? r_base + r0 + rr : c_base + cl;
+          wgt = exp(a.scale * s[i][j] - a.lse[xq]);
+          if (MODE != GRAD_V) wgt = wgt * (dp[i][j] - a.dd[xq]);
+        }
+        blk[rr][cc] = wgt;
+      }
+    __syncthreads();
+    for (int cc = 0; cc < width; cc++) {
+      double bv[4];
+      for (int j = 0; j < 4; j++) {
+        const int64_t y = y0 + tx + 16 * j;
+        bv[j] = y < a.dy ? a.b3[(c_base + c0 + cc) * a.dy + y] : 0.0;
+      }
+      for (int i = 0; i < 4; i++) {
+        const double wgt = blk[ty + 16 * i][cc];
+        for (int j = 0; j < 4; j++) acc[i][j] = fma(wgt, bv[j], acc[i][j]);
+      }
+    }
+    __syncthreads();
+  }
+  for (int i = 0; i < 4; i++) {
+    const int rr = ty + 16 * i;
+    if (rr >= rows) continue;
+    for (int j = 0; j < 4; j++) {
+      const int64_t y = y0 + tx + 16 * j;
+      if (y < a.dy) a.out[(r_base + r0 + rr) * a.dy + y] = a.out_factor * acc[i][j];
+    }
+  }
+}
+
+// D_x = Σ_y d_out[x][y] · out[x][y], a warp per row.
+__global__ void row_dots(int64_t n, int64_t dv, const double* __restrict__ d_out, const double* __restrict__ out,
+                         double* __restrict__ dd) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t x = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; x < n;
+       x += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    double s = 0.0;
+    for (int64_t y = lane; y < dv; y += 32) s = fma(d_out[x * dv + y], out[x * dv + y], s);
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) dd[x] = s;
+  }
+}
+
+inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+// The mask of keys as rows: each condition x <cmp> j + off as j <cmp'> x - off.
+Mask transposed(const Mask& m) {
+  static const int mirror[4] = {2, 3, 0, 1};
+  Mask t;
+  t.n = m.n;
+  for (int i = 0; i < m.n; i++) {
+    if (m.off[i] == INT64_MIN) fail(EINFOLD_INVALID, "a condition offset of -2^63 has no mirror");
+    t.cmp[i] = mirror[m.cmp[i]];
+    t.off[i] = -m.off[i];
+  }
+  t.lnx = m.lnj > 0 ? m.lnj : 1;
+  t.lnj = m.lnx;
+  return t;
+}
+
+// One operand's digits: rows (or columns) sliced, with exponents.
+struct Digits {
+  int8_t* d = nullptr;
+  int32_t* e = nullptr;
+};
+
+template <int MODE>
+void launch_split(const CUtensorMap* maps, const GradArgs& args, dim3 grid, cudaStream_t stream) {
+  using Sh = GradShape<MODE>;
+  EF_CUDA(cudaFuncSetAttribute(grad_split<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::kSmem));
+  grad_split<MODE><<<grid, kGradThreads, Sh::kSmem, stream>>>(maps[0], maps[1], maps[2], maps[3], maps[4], args);
+  EF_LAUNCH_CHECK();
+}
+
+// The split backward; false if it doesn't apply or an operand isn't finite
+// (nothing written).
+bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd, cudaStream_t s) {
+  const AttentionProblem& f = g.f;
+  const int64_t W = f.batches, lq = f.lnx, lk = f.lnj, d = f.ne, dv = f.ny;
+  if (d > 64 || dv > 64 || d <= 0 || dv <= 0 || lq <= 0 || lk <= 0) return false;
+  if (lq > (1 << 30) || lk > (1 << 30) || W > 65535) return false;
+  const int64_t lq_pad = round_up(lq, GM), lk_pad = round_up(lk, GM);
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  // Row digits of q, k, v, d_out (64 B of features each) and column digits
+  // of d_out, q, k (K-major along the batch's positions).
+  const size_t rq = al((size_t)(W * S * lq_pad * 64)), rk = al((size_t)(W * S * lk_pad * 64));
+  const size_t cq = al((size_t)(W * S * 64 * lq_pad)), ck = al((size_t)(W * S * 64 * lk_pad));
+  const size_t eqs = al((size_t)(W * lq_pad) * 4), eks = al((size_t)(W * lk_pad) * 4), ecs = al((size_t)(W * 64) * 4);
+  const size_t cm = al((size_t)(W * 64) * 8);
+  const size_t total = 2 * rq + 2 * rk + 2 * cq + ck + 2 * eqs + 2 * eks + 3 * ecs + cm + 256;
+  DeviceBuffer<uint8_t> scratch(total, s);
+  uint8_t* p = scratch.get();
+  auto take = [&](size_t n) {
+    uint8_t* q = p;
+    p += n;
+    return q;
+  };
+  Digits Qr{(int8_t*)take(rq), nullptr}, dOr{(int8_t*)take(rq), nullptr}, Kr{(int8_t*)take(rk), nullptr},
+      Vr{(int8_t*)take(rk), nullptr}, dOc{(int8_t*)take(cq), nullptr}, Qc{(int8_t*)take(cq), nullptr},
+      Kc{(int8_t*)take(ck), nullptr};
+  Qr.e = (int32_t*)take(eqs);
+  dOr.e = (int32_t*)take(eqs);
+  Kr.e = (int32_t*)take(eks);
+  Vr.e = (int32_t*)take(eks);
+  dOc.e = (int32_t*)take(ecs);
+  Qc.e = (int32_t*)take(ecs);
+  Kc.e = (int32_t*)take(ecs);
+  unsigned long long* colmax = (unsigned long long*)take(cm);
+  int* status = (int*)take(256);  // [0] slicing, [1] kernels, [2..7] tile pairs of the three kernels
+  unsigned long long* tiles = (unsigned long long*)(status + 2);
+  EF_CUDA(cudaMemsetAsync(status, 0, 32, s));
+  slice_rows_into(S, f.q, W, lq, d, d, lq_pad, 64, Qr.e, Qr.d, status, s);
+  slice_rows_into(S, g.d_out, W, lq, dv, dv, lq_pad, 64, dOr.e, dOr.d, status, s);
+  slice_rows_into(S, f.k, W, lk, d, d, lk_pad, 64, Kr.e, Kr.d, status, s);
+  slice_rows_into(S, f.v, W, lk, dv, dv, lk_pad, 64, Vr.e, Vr.d, status, s);
+  slice_cols_into(S, g.d_out, W, lq, dv, 64, lq_pad, colmax, dOc.e, dOc.d, status, s);
+  slice_cols_into(S, f.q, W, lq, d, 64, lq_pad, colmax, Qc.e, Qc.d, status, s);
+  slice_cols_into(S, f.k, W, lk, d, 64, lk_pad, colmax, Kc.e, Kc.d, status, s);
+  ctx.kernels += 10;
+  int st = 0;
+  EF_CUDA(cudaMemcpyAsync(&st, status, 4, cudaMemcpyDeviceToHost, s));
+  EF_CUDA(cudaStreamSynchronize(s));
+  if (st & 1) return false;
+  ctx.phase("attention backward: sliced");
+  auto rows_map = [&](const Digits& x, int64_t rows_pad, int box) {
+    return digit_planes_map(x.d, 64, rows_pad, W * S, box, S);
+  };
+  auto cols_map = [&](const Digits& x, int64_t k_pad) { return digit_planes_map(x.d, k_pad, 64, W * S, GY, S); };
+  cudaEvent_t e0, e1;
+  EF_CUDA(cudaEventCreate(&e0));
+  EF_CUDA(cudaEventCreate(&e1));
+  EF_CUDA(cudaEventRecord(e0, s));
+  const Mask keys_mask = transposed(f.mask);
+  const double* table = exp_table(ctx.device);
+  for (int mode = 0; mode < 3; mode++) {
+    GradArgs a{};
+    CUtensorMap maps[5];
+    const bool keys = mode != GRAD_Q;
+    a.mask = keys ? keys_mask : f.mask;
+    a.lr = keys ? lk : lq;
+    a.lc = keys ? lq : lk;
+    a.lr_pad = keys ? lk_pad : lq_pad;
+    a.lc_pad = keys ? lq_pad : lk_pad;
+    a.scale = f.scale_kind == 1 ? f.scale_c : 1.0;
+    a.lse = g.lse;
+    a.dd = dd;
+    a.exp_table = table;
+    a.status = status + 1;
+    a.tiles = tiles + mode;
+    if (mode == GRAD_V) {
+      maps[0] = rows_map(Kr, lk_pad, GM);
+      maps[1] = rows_map(Qr, lq_pad, GJ);
+      maps[2] = maps[0];
+      maps[3] = maps[1];
+      maps[4] = cols_map(dOc, lq_pad);
+      a.e_a1 = Kr.e;
+      a.e_b1 = Qr.e;
+      a.e_b3 = dOc.e;
+      a.dy = dv;
+      a.out = g.d_v;
+      a.out_factor = 1.0;
+    } else if (mode == GRAD_K) {
+      maps[0] = rows_map(Kr, lk_pad, GM);
+      maps[1] = rows_map(Qr, lq_pad, GJ);
+      maps[2] = rows_map(Vr, lk_pad, GM);
+      maps[3] = rows_map(dOr, lq_pad, GJ);
+      maps[4] = cols_map(Qc, lq_pad);
+      a.e_a1 = Kr.e;
+      a.e_b1 = Qr.e;
+      a.e_a2 = Vr.e;
+      a.e_b2 = dOr.e;
+      a.e_b3 = Qc.e;
+      a.dy = d;
+      a.out = g.d_k;
+      a.out_factor = a.scale;
+    } else {
+      maps[0] = rows_map(Qr, lq_pad, GM);
+      maps[1] = rows_map(Kr, lk_pad, GJ);
+      maps[2] = rows_map(dOr, lq_pad, GM);
+      maps[3] = rows_map(Vr, lk_pad, GJ);
+      maps[4] = cols_map(Kc, lk_pad);
+      a.e_a1 = Qr.e;
+      a.e_b1 = Kr.e;
+      a.e_a2 = dOr.e;
+      a.e_b2 = Vr.e;
+      a.e_b3 = Kc.e;
+      a.dy = d;
+      a.out = g.d_q;
+      a.out_factor = a.scale;
+    }
+    a.dy_pad = 64;
+    a.y0 = 0;
+    const dim3 grid((unsigned)(a.lr_pad / GM), (unsigned)W);
+    if (mode == GRAD_V) launch_split<GRAD_V>(maps, a, grid, s);
+    else if (mode == GRAD_K) launch_split<GRAD_K>(maps, a, grid, s);
+    else launch_split<GRAD_Q>(maps, a, grid, s);
+    ctx.kernels++;
+  }
+  EF_CUDA(cudaEventRecord(e1, s));
+  unsigned long long pairs[3] = {};
+  EF_CUDA(cudaMemcpyAsync(&st, status + 1, 4, cudaMemcpyDeviceToHost, s));
+  EF_CUDA(cudaMemcpyAsync(pairs, tiles, 24, cudaMemcpyDeviceToHost, s));
+  EF_CUDA(cudaStreamSynchronize(s));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st & 2) fail(EINFOLD_TIMEOUT, "a bounded wait in the attention backward ran out");
+  // Digit products executed: per pair of tiles, S(S+1)/2 digit pairs of a
+  // 128 x 64 x 64 product, two of them for d_v and three for d_k and d_q.
+  ctx.product_ms += ms;
+  const double per = (S * (S + 1) / 2) * 2.0 * GM * GJ * 64;
+  ctx.product_ops += per * (2.0 * (double)pairs[0] + 3.0 * (double)(pairs[1] + pairs[2]));
+  ctx.phase("attention backward: tiles");
+  return true;
+}
+
+void backward_fp64(Context& ctx, const AttentionGradients& g, const double* dd, cudaStream_t s) {
+  const AttentionProblem& f = g.f;
+  const int64_t W = f.batches, lq = f.lnx, lk = f.lnj, d = f.ne, dv = f.ny;
+  const Mask keys_mask = transposed(f.mask);
+  for (int mode = 0; mode < 3; mode++) {
+    GradFp64Args a{};
+    const bool keys = mode != GRAD_Q;
+    a.mask = keys ? keys_mask : f.mask;
+    a.lr = keys ? lk : lq;
+    a.lc = keys ? lq : lk;
+    a.scale = f.scale_kind == 1 ? f.scale_c : 1.0;
+    a.lse = g.lse;
+    a.dd = dd;
+    if (mode == GRAD_V) {
+      a.a1 = f.k; a.b1 = f.q; a.d1 = d; a.b3 = g.d_out; a.dy = dv; a.out = g.d_v; a.out_factor = 1.0;
+    } else if (mode == GRAD_K) {
+      a.a1 = f.k; a.b1 = f.q; a.d1 = d; a.a2 = f.v; a.b2 = g.d_out; a.d2 = dv; a.b3 = f.q; a.dy = d;
+      a.out = g.d_k; a.out_factor = a.scale;
+    } else {
+      a.a1 = f.q; a.b1 = f.k; a.d1 = d; a.a2 = g.d_out; a.b2 = f.v; a.d2 = dv; a.b3 = f.k; a.dy = d;
+      a.out = g.d_q; a.out_factor = a.scale;
+    }
+    if (a.lr == 0 || a.dy == 0 || W == 0) continue;
+    const dim3 grid((unsigned)((a.lr + FT - 1) / FT), (unsigned)((a.dy + FT - 1) / FT), (unsigned)W);
+    if (mode == GRAD_V) {
+      EF_CUDA(cudaFuncSetAttribute(grad_fp64<GRAD_V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFp64Smem));
+      grad_fp64<GRAD_V><<<grid, 256, kFp64Smem, s>>>(a);
+    } else if (mode == GRAD_K) {
+      EF_CUDA(cudaFuncSetAttribute(grad_fp64<GRAD_K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFp64Smem));
+      grad_fp64<GRAD_K><<<grid, 256, kFp64Smem, s>>>(a);
+    } else {
+      EF_CUDA(cudaFuncSetAttribute(grad_fp64<GRAD_Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFp64Smem));
+      grad_fp64<GRAD_Q><<<grid, 256, kFp64Smem, s>>>(a);
+    }
+    EF_LAUNCH_CHECK();
+    ctx.kernels++;
+  }
+  EF_CUDA(cudaStreamSynchronize(s));
+  ctx.phase("attention backward: fp64 tiles");
+}
+
+}  // namespace
+
+void attention_backward(Context& ctx, const AttentionGradients& g, int precision, cudaStream_t s) {
+  const AttentionProblem& f = g.f;
+  const int64_t W = f.batches, lq = f.lnx;
+  if (W <= 0) return;
+  if (W > 65535) fail(EINFOLD_INVALID, "more than 65535 batches");
+  DeviceBuffer<double> dd((size_t)std::max<int64_t>(W * lq, 1), s);
+  if (W * lq > 0) {
+    row_dots<<<blocks_for((uint64_t)(W * lq) * 32, 256), 256, 0, s>>>(W * lq, f.ny, g.d_out, g.out, dd.get());
+    EF_LAUNCH_CHECK();
+    ctx.kernels++;
+  }
+  if (precision == 0 && backward_split(ctx, g, dd.get(), s)) return;
+  backward_fp64(ctx, g, dd.get(), s);
+}
+
+}  // namespace ef

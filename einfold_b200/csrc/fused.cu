@@ -87,6 +87,7 @@ struct TileArgs {
   const double* largest;
   const double* smallest;
   double* out;  // [x][y]
+  double* lse;  // [x]: m + ln z of a normalised softmax row, or null
   unsigned long long* visited;
   unsigned* overflowed;
 };
@@ -410,6 +411,7 @@ __global__ void __launch_bounds__(kThreads) fused_tiles(const TileArgs p) {
       if (S.check[r] && !spec && !(S.lost[r] <= rounding * fabs(a))) over = true;
       p.out[(x0 + r) * p.ny + y0 + y] = a;
     }
+    if (p.lse && tx == 0 && blockIdx.y == 0 && !unnormalized && !map) p.lse[x0 + r] = S.m[r] + log(S.z[r]);
   }
   if (__syncthreads_or(over) && t == 0) atomicOr(p.overflowed, 1u);
   if (t == 0 && blockIdx.y == 0 && visited) atomicAdd(p.visited, visited);
@@ -856,6 +858,64 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
   result.tiles = tile_pairs;
   ctx.phase("fused: result");
   return result;
+}
+
+AttentionOutcome attention_forward(Context& ctx, AttentionProblem p, int precision, int slices, cudaStream_t s) {
+  const int64_t nx = p.batches * p.lnx, nj = p.batches * p.lnj;
+  if (nx == 0 || p.ny == 0) return ATTENTION_DONE;
+  DeviceBuffer<uint8_t> jflag((size_t)std::max<int64_t>(nj, 1), s);
+  DeviceBuffer<double> largest((size_t)std::max<int64_t>(nj, 1), s), smallest((size_t)std::max<int64_t>(nj, 1), s);
+  DeviceBuffer<unsigned> nonfinite(1, s);
+  nonfinite.zero();
+  if (nj) {
+    value_stats<<<blocks_for(nj * 32, 256), 256, 0, s>>>(nj, p.ny, p.v, jflag.get(), largest.get(), smallest.get(),
+                                                         nonfinite.get());
+    ctx.kernels++;
+    EF_LAUNCH_CHECK();
+  }
+  unsigned v_nonfinite = 0;
+  EF_CUDA(cudaMemcpyAsync(&v_nonfinite, nonfinite.get(), 4, cudaMemcpyDeviceToHost, s));
+  EF_CUDA(cudaStreamSynchronize(s));
+  p.largest = largest.get();
+  p.smallest = smallest.get();
+  if (precision == 0 && !v_nonfinite && nj > 0) {
+    const AttentionOutcome r = attention_split(ctx, p, slices > 0 ? slices : 6, s);
+    if (r != ATTENTION_INELIGIBLE) return r;
+  }
+  TileArgs a{};
+  a.nx = nx;
+  a.ne = p.ne;
+  a.nj = nj;
+  a.ny = p.ny;
+  a.mask = p.mask;
+  a.scale_kind = p.scale_kind;
+  a.scale_c = p.scale_c;
+  a.shifted = 1;
+  a.normalizer = 0;
+  a.q = p.q;
+  a.k = p.k;
+  a.v = p.v;
+  a.jflag = jflag.get();
+  a.largest = largest.get();
+  a.smallest = smallest.get();
+  a.out = p.out;
+  a.lse = p.lse;
+  DeviceBuffer<unsigned long long> visited(1, s);
+  DeviceBuffer<unsigned> overflowed(1, s);
+  visited.zero();
+  overflowed.zero();
+  a.visited = visited.get();
+  a.overflowed = overflowed.get();
+  EF_CUDA(cudaFuncSetAttribute(fused_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
+  const dim3 grid((unsigned)((nx + XT - 1) / XT), (unsigned)((p.ny + YC - 1) / YC));
+  fused_tiles<<<grid, kThreads, kTileSmem, s>>>(a);
+  ctx.kernels++;
+  EF_LAUNCH_CHECK();
+  unsigned of = 0;
+  EF_CUDA(cudaMemcpyAsync(&of, overflowed.get(), 4, cudaMemcpyDeviceToHost, s));
+  EF_CUDA(cudaStreamSynchronize(s));
+  ctx.phase("attention: fp64 tiles");
+  return of ? ATTENTION_GUARDED : ATTENTION_DONE;
 }
 
 }  // namespace ef

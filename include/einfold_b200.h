@@ -279,6 +279,49 @@ int32_t einfold_split_gemm_static(const double* a, const double* b, double* c, i
                                   int64_t n, int64_t k, int32_t b_transposed, int32_t slices, void* stream,
                                   char* message, int32_t message_len);
 
+/* ---- Attention over device arrays ----
+ * The pipeline einfold_pipeline runs for product scores, weights
+ * exp(s - MAX(s)) over the kept groups and an average normalised by their
+ * sum (fused.rs:694-1019), over placed FP64 device arrays rather than Arrow
+ * relations: for w < batches and x < lq,
+ *   out[w][x][y] = Σ_j exp(s_xj - m_x) v[w][j][y] / Σ_j exp(s_xj - m_x),
+ *   s_xj = scale · (q[w][x] · k[w][j]),  m_x = max_j s_xj,
+ * over the j < lk that every condition allows, x <cmp_i> j + off_i (cmp 0 <,
+ * 1 <=, 2 >, 3 >=; at most 8; none: every j). q [batches][lq][d], k
+ * [batches][lk][d], v [batches][lk][dv], out [batches][lq][dv], lse
+ * [batches][lq] (may be NULL) = m_x + ln Σ_j exp(s_xj - m_x); a row with no
+ * allowed j is left unwritten. precision 0 runs the split form (int8 digit
+ * products on the tensor cores, six slices; `slices` 0 or 6) when every
+ * value is finite and d <= 128, else (and for precision 1, or other slice
+ * counts) the FP64 tile kernel. Returns EINFOLD_DECLINED where the
+ * reference's overflow or underflow guards (fused.rs:1024-1086) would send
+ * the pipeline back to the host plan. `info` (may be NULL) receives the
+ * message, kernels launched and device times. The reference's pipeline
+ * has no device-array entry; these stand where a caller holds the operands
+ * as tensors, and for training. */
+int32_t einfold_attention_forward(einfold_context* ctx, const double* q, const double* k, const double* v,
+                                  double* out, double* lse, int64_t batches, int64_t lq, int64_t lk, int64_t d,
+                                  int64_t dv, int32_t n_conditions, const int32_t* comparisons,
+                                  const int64_t* offsets, double scale, int32_t precision, int32_t slices,
+                                  void* stream, einfold_result* info);
+
+/* The gradients of einfold_attention_forward's out: given its q, k, v, out
+ * and lse and the upstream gradient d_out [batches][lq][dv], writes d_q,
+ * d_k, d_v (shaped as q, k, v). Scores are recomputed tile by tile from the
+ * saved lse: P = exp(s - lse), dV = Pᵀ·dO, dP = dO·Vᵀ, D = rowsum(dO∘O),
+ * dS = P∘(dP - D), dQ = scale·dS·K, dK = scale·dSᵀ·Q; each output row is
+ * summed by one CTA in a fixed order (no atomics: the same bits on every
+ * run). precision 0: the split form (six slices) where every value is
+ * finite and d, dv <= 64; otherwise, and for precision 1, FP64. The
+ * reference has no backward pass for its fused pipeline: its gradients are
+ * gradient SQL that the host plan runs. */
+int32_t einfold_attention_backward(einfold_context* ctx, const double* q, const double* k, const double* v,
+                                   const double* out, const double* lse, const double* d_out, double* d_q,
+                                   double* d_k, double* d_v, int64_t batches, int64_t lq, int64_t lk, int64_t d,
+                                   int64_t dv, int32_t n_conditions, const int32_t* comparisons,
+                                   const int64_t* offsets, double scale, int32_t precision, void* stream,
+                                   einfold_result* info);
+
 #ifdef __cplusplus
 }
 #endif
