@@ -1,19 +1,28 @@
 """Benchmark of einfold's kernel layer on B200s.
 
-One step is one dense matrix-product fold of 8192x8192 by 8192x8192 FP64
-tables through the C ABI (``SUM(a.v * b.v) ... GROUP BY a.i, b.k`` over
-a(i, j, v) and b(j, k, v), 67.1M rows each), computed in the split form:
-int8 slices on the tensor cores with exact integer sums and an FP64 combine.
-The metric is its FP64-equivalent throughput (2·n³ per step), next to the
-plain FP64 GPU form (cuBLAS DGEMM on the same matrices) and the error against
-it.
+One step is the metric's workload, in the split form (int8 digit products
+on the tensor cores with exact integer sums and an FP64 combine):
+
+* a dense matrix-product fold of 8192x8192 by 8192x8192 FP64 tables through
+  the C ABI (``SUM(a.v * b.v) ... GROUP BY a.i, b.k`` over a(i, j, v) and
+  b(j, k, v), 67.1M rows each): 2·n³ FLOP;
+* causal attention over q, k, v (b 0..3, h 0..15, t 0..4095, d 0..63),
+  values normal(0, 1/8): the forward pass (scores, online softmax, weighted
+  values over the T(T+1)/2 allowed pairs of each of the 64 groups, 4·d FLOP
+  a pair) and the backward pass from the saved log-sum-exp for an upstream
+  gradient normal(0, 1) (five products, 10·d FLOP a pair).
+
+The metric is the step's FP64-equivalent throughput, next to the plain FP64
+GPU form of the same step (cuBLAS DGEMM for the fold, the faster of torch's
+float64 attention and this library's FP64 tile kernels for attention) and
+the errors against it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-With N > 1 (under torchrun, one process per GPU) every rank folds its own
-tables: replicas, no collective on the data path. ``--impl reference`` times
-the reference's CPU algorithm (its C restatement in ``oracle/``, as the
-reference's Rust can't be built here) on a bounded sample of the same fold.
+With N > 1 (under torchrun, one process per GPU) every rank runs its own
+step: replicas, no collective on the data path. ``--impl reference`` times
+the reference's CPU algorithms (their C restatements in ``oracle/``, as the
+reference's Rust can't be built here) on a bounded sample of the same step.
 """
 from __future__ import annotations
 
@@ -31,7 +40,12 @@ sys.path.insert(0, ROOT)
 
 METRIC = "attn fwd+bwd & matmul fold TFLOP/s: split-BF16 vs FP64 GPU at equal error"
 N = 8192
+B, H, T, D = 4, 16, 4096, 64
 SEED = 0
+PAIRS = B * H * T * (T + 1) // 2
+ATT_FWD = 4.0 * D * PAIRS
+ATT_BWD = 10.0 * D * PAIRS
+FOLD = 2.0 * N ** 3
 
 
 def _peaks():
@@ -108,8 +122,8 @@ def _matmul_fold():
 
 
 def _tables(device):
-    """a(i, j, v) and b(j, k, v) on the device, keys in row-major order, v
-    uniform[-1, 1] from SplitMix64 (seed 0; salts 1 and 2)."""
+    """a(i, j, v) and b(j, k, v), keys in row-major order, v uniform[-1, 1]
+    from SplitMix64 (seed 0; salts 1 and 2)."""
     import torch
 
     from einfold_b200 import synthetic as S
@@ -122,10 +136,20 @@ def _tables(device):
     return (i, j, av), (i.clone(), j.clone(), bv)
 
 
-def _cpu_sample(a_cols, b_cols, rows=1024, cols=2048):
+def _attention_inputs(device, groups=B * H):
+    """q, k, v [groups][T][D] normal(0, 1/8) and d_out normal(0, 1) from
+    SplitMix64 (seed 0; salts 3 to 6)."""
+    from einfold_b200 import synthetic as S
+
+    n = groups * T * D
+    q, k, v = (S.normal(SEED, salt, n, 1.0 / 8, device=device).view(groups, T, D) for salt in (3, 4, 5))
+    d_out = S.normal(SEED, 6, n, 1.0, device=device).view(groups, T, D)
+    return q, k, v, d_out
+
+
+def _cpu_fold_sample(a_cols, b_cols, rows=1024, cols=2048):
     """A bounded sample of the fold for the CPU: a's first `rows` values of i
     against b's first `cols` values of k, every j: 2·rows·n·cols FLOP."""
-    import numpy as np
     import pyarrow as pa
 
     ai, aj, av = (t[: rows * N].cpu().numpy() for t in a_cols)
@@ -135,7 +159,29 @@ def _cpu_sample(a_cols, b_cols, rows=1024, cols=2048):
     return a, b, 2.0 * rows * N * cols
 
 
-def _time_cpu(a, b, flops, threads, steps=1):
+def _cpu_attention_sample(q, k, v):
+    """One (b, h) group of the attention as Arrow tables q(t, d, x), k(t, d, x),
+    v(t, c, x) and the causal pipeline over them: 4·d·T(T+1)/2 FLOP."""
+    import numpy as np
+    import pyarrow as pa
+
+    from einfold_b200 import ir
+
+    t, d = np.indices((T, D)).reshape(2, -1)
+
+    def table(x, names):
+        return [pa.record_batch([pa.array(t), pa.array(d), pa.array(x.reshape(-1).cpu().numpy())], names=names)]
+
+    e = ir.EQ
+    producer = ir.Fold([e, e, e], [ir.Operand([(0, 0), (1, 1)], 2), ir.Operand([(2, 0), (1, 1)], 2)],
+                       [ir.Output(0), ir.Output(2)]).with_conditions(
+        [ir.Condition(0, ir.Comparison.GREATER_OR_EQUAL, 2, 0)])
+    p = ir.Pipeline(producer, ir.Weight.exp(), [e], ir.Operand([(2, 0), (3, 1)], 2), [0, 3], ir.Normalizer.KEPT_GROUPS)
+    return p, table(q[0], ["t", "d", "x"]), table(k[0], ["t", "d", "x"]), table(v[0], ["t", "c", "x"]), \
+        4.0 * D * T * (T + 1) / 2
+
+
+def _time_cpu_fold(a, b, threads, steps=1):
     from oracle import oracle
 
     f = _matmul_fold()
@@ -150,46 +196,76 @@ def _time_cpu(a, b, flops, threads, steps=1):
     return times
 
 
+def _time_cpu_attention(sample, threads, steps=1):
+    from oracle import oracle
+
+    p, q, k, v, _ = sample
+    s = oracle.pipeline_schema(p, [q[0].schema, k[0].schema, v[0].schema])
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        out = oracle.pipeline(p, q, k, v, s, oracle.Options(threads=threads))
+        times.append(time.perf_counter() - t0)
+        assert out is not None
+    return times
+
+
+def _cpu_baseline(cols_a, cols_b, qkv, threads, steps):
+    """The oracle's C restatements of dense::fold and fused::pipeline on a
+    bounded sample of the step; FLOP per second over both."""
+    a, b, fold_flops = _cpu_fold_sample(cols_a, cols_b)
+    att = _cpu_attention_sample(*qkv)
+    _time_cpu_fold(a, b, threads, 1)
+    tf = _time_cpu_fold(a, b, threads, steps)
+    ta = _time_cpu_attention(att, threads, steps)
+    flops = (fold_flops + att[4]) * steps
+    return flops / (sum(tf) + sum(ta)) / 1e12, 1e3 * (sum(tf) + sum(ta)) / steps
+
+
+CPU_SAMPLE = ("dense fold 1024x8192 . 8192x2048 and the causal attention forward of one (b, h) group, "
+              "T=4096, d=64 (oracle/ C restatements of dense::fold and fused::pipeline; the reference has "
+              "no backward pass for its fused pipeline)")
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import torch
-
     from oracle import oracle
 
     oracle.build()
     a_cols, b_cols = _tables("cpu")
-    a, b, flops = _cpu_sample(a_cols, b_cols)
+    q, k, v, _ = _attention_inputs("cpu", groups=1)
     threads = os.cpu_count() or 1
-    _time_cpu(a, b, flops, threads, steps=args.warmup)
-    times = _time_cpu(a, b, flops, threads, steps=args.steps)
-    t = sum(times)
-    value = flops * len(times) / t / 1e12
+    value, ms = _cpu_baseline(a_cols, b_cols, (q, k, v), threads, max(args.steps, 1))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / len(times), "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"dense matrix-product fold {N}x{N} . {N}x{N}, FP64 uniform[-1,1] (seed 0); "
-                               f"each step a bounded sample: 1024 values of i x 2048 of k, every j",
+        "config": {"workload": f"dense matrix-product fold {N}x{N} . {N}x{N} and causal attention "
+                               f"B={B} H={H} T={T} d={D}; each step a bounded sample: " + CPU_SAMPLE,
                    "global_batch": 1, "parallelism": "host threads"},
-        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": threads, "kind": "port",
-                         "sample": "dense fold 1024x8192 . 8192x2048 (oracle/ C restatement of dense::fold)"},
+        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": threads, "kind": "port", "sample": CPU_SAMPLE},
         "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
+def _rel(a, b):
+    return ((a - b).norm() / b.norm()).item()
+
+
 def run_ours(args):
-    import numpy as np
     import pyarrow as pa
     import torch
 
+    from einfold_b200 import autograd as A
     from einfold_b200 import kernels as K
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    dev = f"cuda:{local}"
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -204,60 +280,110 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    def event():
+        return torch.cuda.Event(enable_timing=True)
+
     f = _matmul_fold()
-    (ai, aj, av), (bj, bk, bv) = _tables(f"cuda:{local}")
+    (ai, aj, av), (bj, bk, bv) = _tables(dev)
     sa = pa.schema([("i", pa.int64()), ("j", pa.int64()), ("v", pa.float64())])
     sb = pa.schema([("j", pa.int64()), ("k", pa.int64()), ("v", pa.float64())])
     ra = K.DeviceRelation(sa, [ai, aj, av], device=local)
     rb = K.DeviceRelation(sb, [bj, bk, bv], device=local)
     opts = K.Options(slices=args.slices, device=local, result_on_device=True)
-    flops = 2.0 * N ** 3
+    q, k, v, d_out = _attention_inputs(dev)
+    causal = A.causal()
+    split, fp64 = K.Precision.SPLIT, K.Precision.FP64
 
-    # The plain FP64 GPU form: cuBLAS DGEMM on the same matrices, and the error.
-    A = av.view(N, N)
-    B = bv.view(N, N)
-    ref = torch.matmul(A, B)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record()
-    for _ in range(3):
-        torch.matmul(A, B, out=ref)
-    e1.record()
-    torch.cuda.synchronize()
-    fp64_ms = e0.elapsed_time(e1) / 3
-    out = K.fold(f, ra, rb, options=opts)
-    got = out.batches[0].column(2).view(N, N)
-    err = ((got - ref).abs().max() / ref.abs().max()).item()
-    keys_ok = bool((out.batches[0].column(0).view(N, N)[:, 0] == torch.arange(N, device=got.device)).all()) and \
-        bool((out.batches[0].column(1).view(N, N)[0] == torch.arange(N, device=got.device)).all())
-    out.batches[0].release()
+    # One step; per component: the product kernels' time and digit ops, and
+    # the kernels launched.
+    stats = {"fold": [], "attn_fwd": [], "attn_bwd": []}
+    launches = [0]
+
+    def note(name):
+        stats[name].append((K.last_call.product_ms, K.last_call.product_ops))
+        launches[0] += K.last_call.kernels_launched
+
+    def step(record=False):
+        K.fold(f, ra, rb, options=opts).batches[0].release()
+        if record:
+            note("fold")
+        out, lse = A.attention_forward(q, k, v, causal, 1.0, split)
+        if record:
+            note("attn_fwd")
+        grads = A.attention_backward(q, k, v, out, lse, d_out, causal, 1.0, split)
+        if record:
+            note("attn_bwd")
+        return out, grads
+
+    # The plain FP64 GPU form of the same step, and the errors against it.
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = event(), event()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    A_, B_ = av.view(N, N), bv.view(N, N)
+    ref = torch.matmul(A_, B_)
+    dgemm_ms = timed(lambda: torch.matmul(A_, B_, out=ref), 3)
+    folded = K.fold(f, ra, rb, options=opts)
+    got = folded.batches[0].column(2).view(N, N)
+    fold_err = ((got - ref).abs().max() / ref.abs().max()).item()
+    keys_ok = bool((folded.batches[0].column(0).view(N, N)[:, 0] == torch.arange(N, device=dev)).all()) and \
+        bool((folded.batches[0].column(1).view(N, N)[0] == torch.arange(N, device=dev)).all())
+    folded.batches[0].release()
     del ref, got
 
+    mask = torch.ones(T, T, dtype=torch.bool, device=dev).tril()
+
+    def torch_attention():
+        qr, kr, vr = (t.detach().requires_grad_(True) for t in (q, k, v))
+        s = (qr @ kr.transpose(-1, -2)).masked_fill(~mask, float("-inf"))
+        out = torch.softmax(s, -1) @ vr
+        grads = torch.autograd.grad(out, (qr, kr, vr), d_out)
+        return out.detach(), grads
+
+    torch_ms = timed(torch_attention, 1)
+    out_t, grads_t = torch_attention()
+    out_s, grads_s = step()
+    attn_err = {"out": _rel(out_s, out_t), "d_q": _rel(grads_s[0], grads_t[0]), "d_k": _rel(grads_s[1], grads_t[1]),
+                "d_v": _rel(grads_s[2], grads_t[2])}
+    del out_t, grads_t, out_s, grads_s
+    torch.cuda.empty_cache()
+
+    def tiles_fp64():
+        out, lse = A.attention_forward(q, k, v, causal, 1.0, fp64)
+        A.attention_backward(q, k, v, out, lse, d_out, causal, 1.0, fp64)
+
+    tiles_ms = timed(tiles_fp64, 1)
+    fp64_attention_ms = min(torch_ms, tiles_ms)
+    fp64_step_ms = dgemm_ms + fp64_attention_ms
+
     for _ in range(args.warmup):
-        K.fold(f, ra, rb, options=opts).batches[0].release()
+        step()
     barrier()
-    product_ms, product_ops, launches = [], [], 0
     with Clocks(local) as clocks:
-        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0, t1 = event(), event()
         barrier()
         t0.record()
         for _ in range(args.steps):
-            r = K.fold(f, ra, rb, options=opts)
-            product_ms.append(K.last_call.product_ms)
-            product_ops.append(K.last_call.product_ops)
-            launches += K.last_call.kernels_launched
-            r.batches[0].release()
+            step(record=True)
         t1.record()
         barrier()
     ms = t0.elapsed_time(t1)
     if dist is not None:
-        tt = torch.tensor([ms], device=f"cuda:{local}")
+        tt = torch.tensor([ms], device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
     ms_per_step = ms / args.steps
+    flops = FOLD + ATT_FWD + ATT_BWD
     value = world * flops * args.steps / (ms / 1e3) / 1e12
 
-    # End to end: the public API with host Arrow buffers in pinned memory.
+    # End to end: the public API from pinned host memory, results read back.
     e2e = None
     if not args.no_e2e:
         pinned = []
@@ -271,67 +397,94 @@ def run_ours(args):
 
         ha = pa.record_batch([host_col(ai), host_col(aj), host_col(av)], schema=sa)
         hb = pa.record_batch([host_col(bj), host_col(bk), host_col(bv)], schema=sb)
+        hq, hk, hv, hd = (t.cpu().pin_memory() for t in (q, k, v, d_out))
+        back = [torch.empty(q.shape, dtype=torch.float64, pin_memory=True) for _ in range(4)]
         hopts = K.Options(slices=args.slices, device=local)
-        res = K.fold(f, K.Relation(sa, [ha]), K.Relation(sb, [hb]), options=hopts)
+
+        def e2e_step():
+            res = K.fold(f, K.Relation(sa, [ha]), K.Relation(sb, [hb]), options=hopts)
+            dq, dk, dv_, dd = (t.to(dev, non_blocking=True) for t in (hq, hk, hv, hd))
+            out, lse = A.attention_forward(dq, dk, dv_, causal, 1.0, split)
+            grads = A.attention_backward(dq, dk, dv_, out, lse, dd, causal, 1.0, split)
+            for dst, src in zip(back, (out,) + tuple(grads)):
+                dst.copy_(src, non_blocking=True)
+            torch.cuda.synchronize()
+            return res
+
+        res = e2e_step()
         d2h = sum(buf.size for batch in res.batches for col in batch.columns for buf in col.buffers() if buf)
+        d2h += sum(t.numel() * 8 for t in back)
         h2d = sum(buf.size for batch in (ha, hb) for col in batch.columns for buf in col.buffers() if buf)
+        h2d += sum(t.numel() * 8 for t in (hq, hk, hv, hd))
         del res
         e2e_steps = max(1, min(args.steps, 3))
         barrier()
         t0.record()
         for _ in range(e2e_steps):
-            res = K.fold(f, K.Relation(sa, [ha]), K.Relation(sb, [hb]), options=hopts)
-            del res
+            del_res = e2e_step()
+            del del_res
         t1.record()
         barrier()
         ems = t0.elapsed_time(t1)
         if dist is not None:
-            tt = torch.tensor([ems], device=f"cuda:{local}")
+            tt = torch.tensor([ems], device=dev)
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             ems = float(tt.item())
         e2e = {"value": world * flops * e2e_steps / (ems / 1e3) / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
                "ms_per_step": ems / e2e_steps}
-        del ha, hb, pinned
+        del ha, hb, pinned, hq, hk, hv, hd, back
 
+    # Rooflines of the three product kernels: digit ops executed on the
+    # tensor cores per second against the int8 dense peak.
     bf16, hbm, basis = _peaks()
     int8_peak = 2.0 * bf16
-    p_ms = statistics.mean(product_ms) if product_ms else None
-    p_ops = statistics.mean(product_ops) if product_ops else None
-    achieved = p_ops / (p_ms / 1e3) / 1e12 if p_ms else None
-    traffic = _profiled_traffic()
-    roofline = {"bound": "tensor", "kernel": "split_gemm_kernel<6>", "achieved": achieved, "peak": int8_peak,
-                "unit": "TFLOP/s", "frac": achieved / int8_peak if achieved else None, "traffic": traffic,
-                "peak_basis": f"int8 dense = 2 x {basis} bf16 burst ({bf16} TFLOP/s)",
-                "kernel_ms": p_ms, "ops_per_launch": p_ops}
+    names = {"fold": "split_gemm_kernel<6>", "attn_fwd": "attn_fwd_split<6,1>", "attn_bwd": "grad_split (3 kernels)"}
+    kernels = {}
+    for key, recs in stats.items():
+        p_ms = statistics.mean(r[0] for r in recs)
+        p_ops = statistics.mean(r[1] for r in recs)
+        achieved = p_ops / (p_ms / 1e3) / 1e12 if p_ms else None
+        kernels[key] = {"kernel": names[key], "ms": p_ms, "ops_per_step": p_ops, "achieved": achieved,
+                        "frac": achieved / int8_peak if achieved else None, "share": p_ms / ms_per_step}
+    top = max(kernels, key=lambda k_: kernels[k_]["ms"])
+    roofline = {"bound": "tensor", "kernel": kernels[top]["kernel"], "achieved": kernels[top]["achieved"],
+                "peak": int8_peak, "unit": "TFLOP/s", "frac": kernels[top]["frac"],
+                "traffic": _profiled_traffic(top), "peak_basis": f"int8 dense = 2 x {basis} bf16 burst ({bf16} TFLOP/s)",
+                "kernel_ms": kernels[top]["ms"], "ops_per_launch": kernels[top]["ops_per_step"], "kernels": kernels}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         from oracle import oracle
 
         oracle.build()
-        a, b, sflops = _cpu_sample((ai, aj, av), (bj, bk, bv))
         threads = os.cpu_count() or 1
-        times = _time_cpu(a, b, sflops, threads, steps=1)
-        cpu = {"value": sflops / times[0] / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": "port",
-               "sample": "dense fold 1024x8192 . 8192x2048 (oracle/ C restatement of dense::fold)"}
+        cval, _ = _cpu_baseline((ai, aj, av), (bj, bk, bv), (q[:1].cpu(), k[:1].cpu(), v[:1].cpu()), threads, 1)
+        cpu = {"value": cval, "unit": "TFLOP/s", "cores": threads, "kind": "port", "sample": CPU_SAMPLE}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int8 slices (exact int32 sums) -> f64", "data": "synthetic",
-            "config": {"workload": f"dense matrix-product fold {N}x{N} . {N}x{N} through einfold_fold, "
-                                   f"a(i,j,v) and b(j,k,v) with {N * N} rows each, FP64 uniform[-1,1] (seed 0)",
-                       "slices": args.slices, "l2": "inputs larger than L2 (3.2 GB of tables per step)",
+            "config": {"workload": f"dense matrix-product fold {N}x{N} . {N}x{N} through einfold_fold (a(i,j,v), "
+                                   f"b(j,k,v), {N * N} rows each, FP64 uniform[-1,1]) + causal attention "
+                                   f"B={B} H={H} T={T} d={D} forward and backward (values normal(0,1/8), "
+                                   f"d_out normal(0,1)), SplitMix64 seed 0",
+                       "flop_per_step": {"fold": FOLD, "attention_forward": ATT_FWD, "attention_backward": ATT_BWD},
+                       "slices": args.slices, "l2": "inputs larger than L2 (3.2 GB of tables, 0.5 GB of q,k,v,d_out)",
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                       "max_rel_error_vs_fp64": err, "keys_exact": keys_ok},
-            "fp64_gpu": {"value": flops / (fp64_ms / 1e3) / 1e12, "unit": "TFLOP/s", "form": "cuBLAS DGEMM (torch)",
-                         "ms": fp64_ms, "ratio_split_over_fp64": (flops / (ms_per_step / 1e3)) / (flops / (fp64_ms / 1e3))},
+                       "errors_vs_fp64": {"fold_max_rel": fold_err, "attention_norm_rel": attn_err},
+                       "keys_exact": keys_ok},
+            "fp64_gpu": {"value": flops / (fp64_step_ms / 1e3) / 1e12, "unit": "TFLOP/s", "ms": fp64_step_ms,
+                         "form": "cuBLAS DGEMM (fold) + the faster of torch float64 attention and the FP64 tiles",
+                         "fold_dgemm_ms": dgemm_ms, "attention_torch_f64_ms": torch_ms,
+                         "attention_fp64_tiles_ms": tiles_ms,
+                         "ratio_split_over_fp64": fp64_step_ms / ms_per_step},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": launches,
+            "gpu_launches": launches[0],
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -340,9 +493,12 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def _profiled_traffic():
-    """DRAM bytes per launch of the product kernel, from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "split_gemm_kernel_matmul8192.txt")
+def _profiled_traffic(component):
+    """DRAM bytes per step of a component's product kernel, from the committed
+    ncu summary (`traffic_bytes_per_launch:` line), or None."""
+    files = {"fold": "split_gemm_kernel_matmul8192.txt", "attn_fwd": "attn_fwd_split_causal_T4096.txt",
+             "attn_bwd": "grad_split_causal_T4096.txt"}
+    path = os.path.join(ROOT, "profiles", files[component])
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -355,7 +511,7 @@ def _profiled_traffic():
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--slices", type=int, default=6)

@@ -65,6 +65,13 @@ def _call(fn, device: int, *args) -> _lib.Result:
     st = fn(_lib.context(device), *args, ctypes.c_void_p(stream), ctypes.byref(info))
     if st == _lib.DECLINED:
         raise Declined(info.message.decode(errors="replace"))
+    from .kernels import last_call
+
+    last_call.kernels_launched = info.kernels_launched
+    last_call.device_ms = info.device_ms
+    last_call.product_ms = info.product_ms
+    last_call.product_ops = info.product_ops
+    last_call.message = info.message.decode(errors="replace")
     if st != _lib.OK:
         _raise(st, info.message.decode(errors="replace"))
     return info
