@@ -274,6 +274,73 @@ __global__ void __launch_bounds__(256) slice_rows(const double* __restrict__ x, 
   }
 }
 
+// The same cut for rows of at most 128 values (attention's features): a
+// warp per row, four consecutive values per lane, the same digits.
+template <int S>
+__global__ void __launch_bounds__(256) slice_short_rows(const double* __restrict__ x, int64_t batches, int64_t rows,
+                                                        int64_t k, int64_t ld, int64_t rows_pad, int64_t k_pad,
+                                                        int32_t* __restrict__ e_out, int8_t* __restrict__ digits,
+                                                        int* status) {
+  const int lane = threadIdx.x & 31;
+  const int64_t slab = rows_pad * k_pad;
+  for (int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < batches * rows_pad;
+       g += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    const int64_t w = g / rows_pad, r = g % rows_pad;
+    const double* row = x + (w * rows + r) * ld;
+    const bool live = r < rows;
+    double v[4];
+    double m = 0.0;
+    bool bad = false;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int64_t kk = lane * 4 + j;
+      v[j] = (live && kk < k) ? row[kk] : 0.0;
+      const double a = fabs(v[j]);
+      bad |= !(a <= 1.7976931348623157e308);
+      m = fmax(m, a);
+    }
+    if (bad) atomicOr(status, 1);
+    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    int ex = 0;
+    if (m > 0.0 && m <= 1.7976931348623157e308) {
+      frexp(m, &ex);
+      ex += 2;
+    }
+    if (lane == 0) e_out[g] = ex;
+    if (lane * 4 < k_pad) {
+      const int shift = 8 * S - ex;
+      uint32_t word[S];
+#pragma unroll
+      for (int s = 0; s < S; s++) word[s] = 0;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const double vv = fabs(v[j]) <= 1.7976931348623157e308 ? v[j] : 0.0;
+        long long X = llrint(ldexp(vv, shift));
+#pragma unroll
+        for (int s = S - 1; s >= 0; s--) {
+          const long long d = ((X + 128) & 255) - 128;
+          word[s] |= ((uint32_t)(d & 255)) << (8 * j);
+          X = (X - d) >> 8;
+        }
+      }
+#pragma unroll
+      for (int s = 0; s < S; s++) *(uint32_t*)(digits + (w * S + s) * slab + r * k_pad + lane * 4) = word[s];
+    }
+  }
+}
+
+// Launches the row slicer that suits the row length.
+template <int S>
+void launch_slice_rows(const double* x, int64_t batches, int64_t rows, int64_t k, int64_t ld, int64_t rows_pad,
+                       int64_t k_pad, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream) {
+  if (k_pad <= 128)
+    slice_short_rows<S><<<blocks_for((uint64_t)(batches * rows_pad) * 32, 256), 256, 0, stream>>>(
+        x, batches, rows, k, ld, rows_pad, k_pad, e_out, digits, status);
+  else
+    slice_rows<S><<<blocks_for((uint64_t)(batches * rows_pad), 1, 148 * 8), 256, 0, stream>>>(
+        x, batches, rows, k, ld, rows_pad, k_pad, e_out, digits, status);
+}
+
 // The largest magnitude of each column of x [batches][k][n] (row-major):
 // blocks of rows reduce apart and combine with an atomic max on the bits
 // (non-negative doubles order as their bits). Status bit 1 if a value isn't
@@ -521,8 +588,7 @@ int split_run(Context& ctx, const double* a, const double* b, bool b_natural, do
   const SplitDims d = split_dims(m, n, k);
   const int64_t m_pad = d.m_pad, n_pad = d.n_pad, k_pad = d.k_pad;
   EF_CUDA(cudaMemsetAsync(sc.status, 0, sizeof(int), stream));
-  slice_rows<S><<<blocks_for((uint64_t)(batches * m_pad), 1, 148 * 8), 256, 0, stream>>>(
-      a, batches, m, k, k, m_pad, k_pad, sc.ea, sc.da, sc.status);
+  launch_slice_rows<S>(a, batches, m, k, k, m_pad, k_pad, sc.ea, sc.da, sc.status, stream);
   if (b_natural) {
     EF_CUDA(cudaMemsetAsync(sc.colmax, 0, (size_t)(batches * n) * 8, stream));
     const unsigned splits = (unsigned)std::min<int64_t>(64, (k + 127) / 128);
@@ -532,8 +598,7 @@ int split_run(Context& ctx, const double* a, const double* b, bool b_natural, do
         b, k, n, n_pad, k_pad, sc.colmax, sc.eb, sc.db);
     ctx.kernels += 2;
   } else {
-    slice_rows<S><<<blocks_for((uint64_t)(batches * n_pad), 1, 148 * 8), 256, 0, stream>>>(
-        b, batches, n, k, k, n_pad, k_pad, sc.eb, sc.db, sc.status);
+    launch_slice_rows<S>(b, batches, n, k, k, n_pad, k_pad, sc.eb, sc.db, sc.status, stream);
     ctx.kernels++;
   }
   EF_LAUNCH_CHECK();
@@ -633,8 +698,7 @@ void slice_rows_into(int S, const double* x, int64_t batches, int64_t rows, int6
                      int64_t k_pad, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream) {
   if (batches <= 0 || rows_pad <= 0) return;
   dispatch_slices(S, [&](auto SS) {
-    slice_rows<decltype(SS)::value><<<blocks_for((uint64_t)(batches * rows_pad), 1, 148 * 8), 256, 0, stream>>>(
-        x, batches, rows, k, ld, rows_pad, k_pad, e_out, digits, status);
+    launch_slice_rows<decltype(SS)::value>(x, batches, rows, k, ld, rows_pad, k_pad, e_out, digits, status, stream);
   });
   EF_LAUNCH_CHECK();
 }
