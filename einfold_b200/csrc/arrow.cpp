@@ -1,7 +1,11 @@
 // Arrow C Data Interface import and export for the einfold_b200 library.
 #include "arrow.h"
 
+#include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <unordered_map>
 
 namespace ef {
 
@@ -64,9 +68,71 @@ const char* format_of(Kind k) {
   }
 }
 
+namespace {
+
+// The cache behind pinned_acquire: free blocks by capacity (2 MiB granules),
+// the capacities of blocks in use, and at most kMaxCached bytes kept free.
+struct PinnedPool {
+  static constexpr size_t kGranule = 2u << 20;
+  static constexpr size_t kMaxCached = 16ull << 30;
+  std::mutex m;
+  std::multimap<size_t, void*> free_blocks;
+  std::unordered_map<void*, size_t> live;
+  size_t cached = 0;
+};
+
+PinnedPool& pinned_pool() {
+  static PinnedPool* pool = new PinnedPool;  // outlives every result released at exit
+  return *pool;
+}
+
+}  // namespace
+
+void* pinned_acquire(size_t bytes) {
+  PinnedPool& pool = pinned_pool();
+  const size_t cap = (std::max<size_t>(bytes, 1) + PinnedPool::kGranule - 1) / PinnedPool::kGranule * PinnedPool::kGranule;
+  {
+    std::lock_guard<std::mutex> lock(pool.m);
+    auto it = pool.free_blocks.lower_bound(cap);
+    if (it != pool.free_blocks.end() && it->first <= 2 * cap) {
+      void* p = it->second;
+      pool.live[p] = it->first;
+      pool.cached -= it->first;
+      pool.free_blocks.erase(it);
+      return p;
+    }
+  }
+  void* p = nullptr;
+  if (cudaHostAlloc(&p, cap, cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(pool.m);
+  pool.live[p] = cap;
+  return p;
+}
+
+void pinned_release(void* p) {
+  if (!p) return;
+  PinnedPool& pool = pinned_pool();
+  std::lock_guard<std::mutex> lock(pool.m);
+  auto it = pool.live.find(p);
+  if (it == pool.live.end()) return;
+  const size_t cap = it->second;
+  pool.live.erase(it);
+  if (pool.cached + cap > PinnedPool::kMaxCached) {
+    cudaFreeHost(p);
+    return;
+  }
+  pool.free_blocks.emplace(cap, p);
+  pool.cached += cap;
+}
+
 void Buffer::reset() {
   if (ptr) {
-    if (device < 0) {
+    if (device == -2) {
+      pinned_release(ptr);
+    } else if (device < 0) {
       std::free(ptr);
     } else {
       int old = -1;

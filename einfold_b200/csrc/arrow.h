@@ -76,21 +76,49 @@ std::vector<Field> import_schema(const ArrowSchema* s);
 Relation import_relation(const einfold_relation* r);
 
 // malloc'd host memory handed to an exported array.
+// Page-locked host blocks for results copied from the device, from a
+// process-wide cache: a released result's block serves the next result of
+// a similar size, so steady-state calls neither page-lock nor touch fresh
+// pages, and device-to-host copies run at the link's speed. Null when
+// page-locked memory can't be had.
+void* pinned_acquire(size_t bytes);
+void pinned_release(void* p);
+
 struct HostBuffer {
   void* ptr = nullptr;
   size_t bytes = 0;
+  bool pinned = false;  // from pinned_acquire
   HostBuffer() = default;
   explicit HostBuffer(size_t n) : ptr(n ? std::malloc(n) : nullptr), bytes(n) {
     if (n && !ptr) fail(EINFOLD_BUDGET, "out of host memory for %zu bytes", n);
   }
+  // A page-locked buffer where one can be had, else an ordinary one.
+  static HostBuffer page_locked(size_t n) {
+    HostBuffer h;
+    h.ptr = pinned_acquire(n);
+    if (h.ptr) {
+      h.bytes = n;
+      h.pinned = true;
+      return h;
+    }
+    return HostBuffer(n);
+  }
   HostBuffer(const HostBuffer&) = delete;
-  HostBuffer(HostBuffer&& o) noexcept : ptr(o.ptr), bytes(o.bytes) { o.ptr = nullptr; o.bytes = 0; }
+  HostBuffer(HostBuffer&& o) noexcept : ptr(o.ptr), bytes(o.bytes), pinned(o.pinned) {
+    o.ptr = nullptr;
+    o.bytes = 0;
+  }
   HostBuffer& operator=(HostBuffer&& o) noexcept {
-    std::free(ptr);
-    ptr = o.ptr; bytes = o.bytes; o.ptr = nullptr; o.bytes = 0;
+    release();
+    ptr = o.ptr; bytes = o.bytes; pinned = o.pinned; o.ptr = nullptr; o.bytes = 0;
     return *this;
   }
-  ~HostBuffer() { std::free(ptr); }
+  ~HostBuffer() { release(); }
+  void release() {
+    if (pinned) pinned_release(ptr);
+    else std::free(ptr);
+    ptr = nullptr;
+  }
   template <class T> T* as() const { return (T*)ptr; }
 };
 
@@ -100,7 +128,8 @@ struct Buffer {
   size_t bytes = 0;
   int device = -1;
   Buffer() = default;
-  Buffer(HostBuffer&& h) : ptr(h.ptr), bytes(h.bytes), device(-1) { h.ptr = nullptr; h.bytes = 0; }
+  // device -1: host memory (malloc); -2: a page-locked block (pinned_acquire).
+  Buffer(HostBuffer&& h) : ptr(h.ptr), bytes(h.bytes), device(h.pinned ? -2 : -1) { h.ptr = nullptr; h.bytes = 0; }
   Buffer(const Buffer&) = delete;
   Buffer(Buffer&& o) noexcept : ptr(o.ptr), bytes(o.bytes), device(o.device) { o.ptr = nullptr; o.bytes = 0; }
   Buffer& operator=(Buffer&& o) noexcept {

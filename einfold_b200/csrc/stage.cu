@@ -271,7 +271,7 @@ void pack_bits(Context& ctx, const uint8_t* bytes, int64_t n, uint8_t* bits) {
 }
 
 HostBuffer to_host(Context& ctx, const void* dev, size_t bytes) {
-  HostBuffer h(bytes ? bytes : 1);
+  HostBuffer h = HostBuffer::page_locked(bytes ? bytes : 1);
   if (bytes) {
     EF_CUDA(cudaMemcpyAsync(h.ptr, dev, bytes, cudaMemcpyDeviceToHost, ctx.stream));
     EF_CUDA(cudaStreamSynchronize(ctx.stream));
