@@ -453,6 +453,8 @@ def run_ours(args):
                 "traffic": _profiled_traffic(top), "peak_basis": f"int8 dense = 2 x {basis} bf16 burst ({bf16} TFLOP/s)",
                 "kernel_ms": kernels[top]["ms"], "ops_per_launch": kernels[top]["ops_per_step"], "kernels": kernels}
 
+    ranking = _ranking(hbm, basis) if not args.no_ranking else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         from oracle import oracle
@@ -482,6 +484,7 @@ def run_ours(args):
                          "attention_fp64_tiles_ms": tiles_ms,
                          "ratio_split_over_fp64": fp64_step_ms / ms_per_step},
             "roofline": roofline,
+            "ranking": ranking,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches[0],
@@ -491,6 +494,50 @@ def run_ours(args):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def _ranking(hbm, basis):
+    """einfold_rank_words on random 64-bit keys (each drawn from a pool of
+    n/2), timed with CUDA events: 2^28 keys (8 GB-scale passes, beyond L2)
+    and 4M keys (the sorting path's join column). Bytes moved, per key: 8
+    read by the varying-byte scan; per 8-bit pass 8 (digit counts) + 12 read
+    + 12 written; then 9 (run heads) + 17 (ranks and first rows)."""
+    import ctypes
+
+    import torch
+
+    from einfold_b200 import _lib
+    from einfold_b200 import synthetic as S
+
+    lib = _lib.load()
+    out = {}
+    for n in (1 << 28, 1 << 22):
+        pool = S.u64(SEED, 7, n // 2)
+        words = pool[(S.u64(SEED, 8, n) % (n // 2)).to(torch.int64)].contiguous()
+        del pool
+        rank_ = torch.empty(n, dtype=torch.int32, device="cuda")
+        first = torch.empty(n, dtype=torch.int32, device="cuda")
+        k = ctypes.c_int64(0)
+        times = []
+        for _ in range(4):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            st = lib.einfold_rank_words(_lib.context(torch.cuda.current_device()), words.data_ptr(), n,
+                                        rank_.data_ptr(), first.data_ptr(), ctypes.byref(k), None)
+            e1.record()
+            torch.cuda.synchronize()
+            assert st == _lib.OK
+            times.append(e0.elapsed_time(e1))
+        ms = statistics.median(times[1:])
+        passes = 8
+        moved = n * (8 + passes * 32 + 26)
+        out[f"n{n}"] = {"keys": n, "distinct": k.value, "ms": ms, "gkeys_per_s": n / ms / 1e6, "passes": passes,
+                        "moved_gb_per_s": moved / ms / 1e6, "frac_of_hbm": moved / ms / 1e6 / hbm}
+        del words, rank_, first
+        torch.cuda.empty_cache()
+    out["peak"] = {"hbm_gb_per_s": hbm, "basis": basis}
+    return out
 
 
 def _profiled_traffic(component):
@@ -517,6 +564,7 @@ def main():
     p.add_argument("--slices", type=int, default=6)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-ranking", action="store_true")
     args = p.parse_args()
     if args.impl == "reference":
         run_reference(args)

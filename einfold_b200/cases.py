@@ -2,11 +2,15 @@
 
     python -m einfold_b200.cases attention --groups 8 --t 2048 --d 64 [--backward]
     python -m einfold_b200.cases product --n 4096
+    python -m einfold_b200.cases rank --n 67108864 [--repeat 3]
 
 ``attention`` runs the split causal attention forward (and backward) over
 q, k, v normal(0, 1/8) and d_out normal(0, 1) (SplitMix64, seed 0);
 ``product`` runs einfold_split_gemm on two n x n uniform[-1, 1] FP64
-matrices. Each prints one line and exits 0 when the kernels ran.
+matrices; ``rank`` ranks n uniform random 64-bit keys (each drawn from a
+pool of n/2, so keys repeat) with einfold_rank_words and prints the keys
+per second of the last of `repeat` runs, timed with CUDA events. Each
+prints one line and exits 0 when the kernels ran.
 """
 from __future__ import annotations
 
@@ -38,6 +42,33 @@ def product(n: int) -> None:
     print(f"product n={n}: max|C| {c.abs().max().item():.6f}")
 
 
+def rank(n: int, repeat: int) -> None:
+    import ctypes
+
+    from . import _lib
+
+    pool = S.u64(0, 7, max(n // 2, 1))
+    pick = (S.u64(0, 8, n) % max(n // 2, 1)).to(torch.int64)
+    words = pool[pick].contiguous()
+    rank_ = torch.empty(n, dtype=torch.int32, device="cuda")
+    first = torch.empty(n, dtype=torch.int32, device="cuda")
+    k = ctypes.c_int64(0)
+    lib = _lib.load()
+    ms = 0.0
+    for _ in range(max(repeat, 1)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        st = lib.einfold_rank_words(_lib.context(0), words.data_ptr(), n, rank_.data_ptr(), first.data_ptr(),
+                                    ctypes.byref(k), None)
+        e1.record()
+        torch.cuda.synchronize()
+        if st != _lib.OK:
+            raise RuntimeError(lib.einfold_last_error().decode())
+        ms = e0.elapsed_time(e1)
+    print(f"rank n={n}: {k.value} distinct, {ms:.3f} ms, {n / ms / 1e6:.3f} Gkeys/s")
+
+
 def main() -> None:
     p = argparse.ArgumentParser()
     sub = p.add_subparsers(dest="case", required=True)
@@ -48,9 +79,14 @@ def main() -> None:
     pa.add_argument("--backward", action="store_true")
     pp = sub.add_parser("product")
     pp.add_argument("--n", type=int, default=4096)
+    pr = sub.add_parser("rank")
+    pr.add_argument("--n", type=int, default=1 << 26)
+    pr.add_argument("--repeat", type=int, default=3)
     args = p.parse_args()
     if args.case == "attention":
         attention(args.groups, args.t, args.d, args.backward)
+    elif args.case == "rank":
+        rank(args.n, args.repeat)
     else:
         product(args.n)
 

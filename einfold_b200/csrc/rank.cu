@@ -59,6 +59,8 @@ __global__ void or_and_words(const uint64_t* __restrict__ keys, int64_t n, int64
 // Upsweep of one pass: the digit counts of each chunk of consecutive keys,
 // written digit-major (table[d·chunks + c]) so that one exclusive scan gives
 // every (digit, chunk)'s first output position, stably.
+// gridDim.y blocks share a chunk, each counting a slice of it and adding
+// into the table, which starts at zero.
 __global__ void __launch_bounds__(kThreads) chunk_counts(const uint64_t* __restrict__ kw, int64_t n, int shift,
                                                          int64_t chunk, int chunks,
                                                          unsigned long long* __restrict__ table) {
@@ -67,14 +69,17 @@ __global__ void __launch_bounds__(kThreads) chunk_counts(const uint64_t* __restr
   for (int i = tid; i < 8 * 256; i += kThreads) (&h[0][0])[i] = 0;
   __syncthreads();
   const int64_t c = blockIdx.x;
-  const int64_t lo = c * chunk, hi = min(n, lo + chunk);
+  const int64_t slice = (chunk + gridDim.y - 1) / gridDim.y;
+  const int64_t lo = c * chunk + blockIdx.y * slice, hi = min(min(n, c * chunk + chunk), lo + slice);
   for (int64_t i = lo + tid; i < hi; i += kThreads) atomicAdd(&h[warp][(kw[i] >> shift) & 255], 1u);
   __syncthreads();
   unsigned int t = 0;
 #pragma unroll
   for (int w = 0; w < 8; w++) t += h[w][tid];
-  table[(int64_t)tid * chunks + c] = t;
+  if (t) atomicAdd(&table[(int64_t)tid * chunks + c], (unsigned long long)t);
 }
+
+constexpr int kCountSplit = 4;  // blocks counting each chunk
 
 // Downsweep of one pass: block c sorts its chunk tile by tile, each key
 // ranked among equal digits in row order (warp __match_any_sync, warps
@@ -297,8 +302,9 @@ int64_t rank_keys_w(Context& ctx, const uint64_t* keys, int64_t n, int64_t ld, u
       DeviceBuffer<int> err(1, s);
       err.zero();
       for (int p = 0; p < passes; p++) {
-        chunk_counts<<<(unsigned)chunks, kThreads, 0, s>>>(cur_k + (int64_t)pw[p] * cur_ld, n, ps[p], chunk,
-                                                            (int)chunks, table.get());
+        EF_CUDA(cudaMemsetAsync(table.get(), 0, (size_t)(256 * chunks) * 8, s));
+        chunk_counts<<<dim3((unsigned)chunks, kCountSplit), kThreads, 0, s>>>(cur_k + (int64_t)pw[p] * cur_ld, n,
+                                                                              ps[p], chunk, (int)chunks, table.get());
         EF_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp.get(), temp, table.get(), offsets.get(), (int)(256 * chunks), s));
         chunk_scatter<W, ITEMS><<<(unsigned)chunks, kThreads, smem, s>>>(cur_k, cur_v, kb[p & 1].get(), vb[p & 1].get(),
                                                                          n, cur_ld, ldb, pw[p], ps[p], chunk, (int)chunks,
