@@ -339,19 +339,19 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
       uint8_t* prow = sP + r * 64;
 #pragma unroll
       for (int c4 = 0; c4 < CW / 4; c4++) {
-        uint32_t wd[S][1];
-#pragma unroll
-        for (int s = 0; s < S; s++) wd[s][0] = 0;
+        double x[4];
 #pragma unroll
         for (int i = 0; i < 4; i++) {
           const double sv = sc[c4 * 4 + i];
           const double wt = sv == NEG_INF ? 0.0 : exp_tang(sv - m, texp);
           z += wt;
-          cut_digits32<S, 1>(llrint(wt * to_int), i, wd);
+          x[i] = wt * to_int;
         }
+        uint32_t planes[S];
+        digit_planes4<S>(x, planes);
         const uint32_t off = sw64_offset((uint32_t)r, (uint32_t)(h * CW + c4 * 4)) - (uint32_t)r * 64;
 #pragma unroll
-        for (int s = 0; s < S; s++) *(uint32_t*)(prow + s * AM * 64 + off) = wd[s][0];
+        for (int s = 0; s < S; s++) *(uint32_t*)(prow + s * AM * 64 + off) = planes[s];
       }
       fence_proxy_async();
       tc_fence_before();

@@ -325,14 +325,14 @@ __global__ void __launch_bounds__(kGradThreads, 1)
       uint8_t* prow = sP + r * 64;
 #pragma unroll
       for (int c4 = 0; c4 < CW / 4; c4++) {
-        uint32_t wd[S][1];
+        double x[4];
 #pragma unroll
-        for (int s = 0; s < S; s++) wd[s][0] = 0;
-#pragma unroll
-        for (int i = 0; i < 4; i++) cut_digits32<S, 1>(llrint(scale2(wv[c4 * 4 + i], shift)), i, wd);
+        for (int i = 0; i < 4; i++) x[i] = scale2(wv[c4 * 4 + i], shift);
+        uint32_t planes[S];
+        digit_planes4<S>(x, planes);
         const uint32_t off = sw64_offset((uint32_t)r, (uint32_t)(h * CW + c4 * 4)) - (uint32_t)r * 64;
 #pragma unroll
-        for (int s = 0; s < S; s++) *(uint32_t*)(prow + s * GM * 64 + off) = wd[s][0];
+        for (int s = 0; s < S; s++) *(uint32_t*)(prow + s * GM * 64 + off) = planes[s];
       }
       fence_proxy_async();
       tc_fence_before();

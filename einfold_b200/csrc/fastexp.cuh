@@ -27,8 +27,11 @@ const double* exp_table(int device);
 
 __device__ __forceinline__ double exp_tang(double x, const double* __restrict__ table) {
   if (!(x >= -708.0 && x <= 709.0)) return exp(x);
-  const double kf = rint(x * k64OverLn2);
-  const int k = (int)kf;
+  // k = x·64/ln2 rounded to the nearest integer by adding 1.5·2^52 (one
+  // rounding of the exact product), read from the sum's low word.
+  const double t = fma(x, k64OverLn2, 6755399441055744.0);
+  const double kf = t - 6755399441055744.0;
+  const int k = __double2loint(t);
   double r = fma(-kf, kLn2Over64Hi, x);
   r = fma(-kf, kLn2Over64Lo, r);
   double p = fma(r, 1.0 / 120.0, 1.0 / 24.0);

@@ -23,15 +23,49 @@ __device__ __forceinline__ double combine_levels(const int32_t (&L)[S][N], int i
   return v;
 }
 
+// x as a double, exactly, with an add on the FP64 pipe rather than a
+// conversion: the double whose high word is 0x43300000 and low word
+// x + 2^31 is 2^52 + 2^31 + x.
+__device__ __forceinline__ double i2d(int x) {
+  return __hiloint2double(0x43300000, x ^ (int)0x80000000) - 4503601774854144.0;
+}
+
 // The same for levels small enough that two of them, one shifted by 8 bits,
 // fit in int32 (|L_l| < 2^23): pairs combined in int32, then converted.
 template <int S, int N>
 __device__ __forceinline__ double combine_levels_small(const int32_t (&L)[S][N], int i) {
-  double v = (S & 1) ? (double)L[S - 1][i] * ptx::pow2(-8 * (S + 1)) : 0.0;
+  double v = (S & 1) ? i2d(L[S - 1][i]) * ptx::pow2(-8 * (S + 1)) : 0.0;
 #pragma unroll
-  for (int p = S / 2 - 1; p >= 0; p--)
-    v = fma((double)(L[2 * p][i] * 256 + L[2 * p + 1][i]), ptx::pow2(-8 * (2 * p + 3)), v);
+  for (int p = S / 2 - 1; p >= 0; p--) v = fma(i2d(L[2 * p][i] * 256 + L[2 * p + 1][i]), ptx::pow2(-8 * (2 * p + 3)), v);
   return v;
+}
+
+// The S digit planes of four values already scaled to integers-to-be
+// (|x| < 2^(8S-2), S <= 6), four columns a word: x rounds to the nearest
+// integer W (ties to even, as llrint) by adding 1.5·2^52, and W's balanced
+// base-256 digits d_s in [-128, 127] are the bytes of W + 0x80…80 with
+// their top bits flipped (byte s of W + Σ 128·256^s is d_s + 128). planes[s]
+// holds digit s (most significant first) of the four values, byte c for
+// value c: the bytes the split product's digit planes hold.
+template <int S>
+__device__ __forceinline__ void digit_planes4(const double (&x)[4], uint32_t (&planes)[S]) {
+  static_assert(S <= 6, "six digits or fewer fit the 48-bit window");
+  constexpr long long kBias = 0x4338000000000000ll - 0x808080808080ll;
+  uint32_t lo[4], hi[4];
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    const long long u = __double_as_longlong(x[c] + 6755399441055744.0) - kBias;  // 1.5·2^52
+    lo[c] = (uint32_t)u;
+    hi[c] = (uint32_t)(u >> 32);
+  }
+#pragma unroll
+  for (int s = 0; s < S; s++) {
+    const int b = S - 1 - s;  // byte of W holding digit s
+    const uint32_t* h = b < 4 ? lo : hi;
+    const uint32_t sel = (uint32_t)((b & 3) | (((b & 3) + 4) << 4));
+    const uint32_t t01 = __byte_perm(h[0], h[1], sel), t23 = __byte_perm(h[2], h[3], sel);
+    planes[s] = __byte_perm(t01, t23, 0x5410) ^ 0x80808080u;
+  }
 }
 
 // The exponent e with |x| < 2^(e-2) for the largest magnitude x of a row
@@ -43,29 +77,6 @@ __device__ __forceinline__ int slice_exponent(double largest) {
     e += 2;
   }
   return e;
-}
-
-// Cuts X (|X| < 2^(8S-2), S <= 7) into S balanced base-256 digits, most
-// significant first, packing digit s of value i into byte (i & 3) of
-// word[s][i >> 2], in 32-bit arithmetic: the low 24 bits give the last three
-// digits, and their carry joins the high part.
-template <int S, int W>
-__device__ __forceinline__ void cut_digits32(long long X, int i, uint32_t (&word)[S][W]) {
-  int lo = (int)(X & 0xFFFFFF);
-  int hi = (int)(X >> 24);
-#pragma unroll
-  for (int s = S - 1; s >= S - 3; s--) {
-    const int d = ((lo + 128) & 255) - 128;
-    word[s][i >> 2] |= ((uint32_t)(d & 255)) << (8 * (i & 3));
-    lo = (lo - d) >> 8;
-  }
-  hi += lo;
-#pragma unroll
-  for (int s = S - 4; s >= 0; s--) {
-    const int d = ((hi + 128) & 255) - 128;
-    word[s][i >> 2] |= ((uint32_t)(d & 255)) << (8 * (i & 3));
-    hi = (hi - d) >> 8;
-  }
 }
 
 }  // namespace ef
