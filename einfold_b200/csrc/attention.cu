@@ -18,9 +18,12 @@
 //   3. w·v: the weights' digits against v's column-scaled digits, the same
 //      level scheme, into the same TMEM columns (q·k's levels were read).
 //   4. The epilogue rescales the row's FP64 running sums and adds the
-//      levels to them. The sums live in the 128 TMEM columns the six
+//      levels to them, in units of each value column's power of two (applied
+//      once, at the end). The sums live in the 128 TMEM columns the six
 //      slices' 384 level columns leave free, two 32-bit columns a value, so
 //      that a thread's registers hold only its 16 scores.
+// The four warps sharing a row exchange its maximum over a named barrier of
+// their own; every other hand-off is an mbarrier each warp arrives on.
 // A TMA producer warp double-buffers k and v tiles; an MMA warp issues both
 // products. Every wait is bounded (2 s); on a timeout the kernel sets a
 // status bit, waits for its copies and MMAs in flight, frees TMEM and
@@ -100,7 +103,9 @@ __device__ __forceinline__ double level_sum(const int32_t (&L)[S][4], int i) {
   else return combine_levels<S, 4>(L, i);
 }
 
-template <int S, int KB>
+// FAST: every q row's and k row's exponents sum to at most 1023 and at
+// least -1022, so a score's power of two is a normal double.
+template <int S, int KB, bool FAST>
 __global__ void __launch_bounds__(kAttnThreads, 1)
     attn_fwd_split(const __grid_constant__ CUtensorMap tq, const __grid_constant__ CUtensorMap tk,
                    const __grid_constant__ CUtensorMap tv, const AttnArgs a) {
@@ -143,8 +148,8 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
     }
     mbar_init(qk_full, 1);
     mbar_init(pv_full, 1);
-    mbar_init(p_full, 1);
-    mbar_init(tmem_free, 1);
+    mbar_init(p_full, kEpi / 32);  // each epilogue warp arrives
+    mbar_init(tmem_free, kEpi / 32);
     *failed = 0;
     span[0] = LLONG_MAX;
     span[1] = LLONG_MIN;
@@ -282,25 +287,36 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
   } else {
     // Epilogue: warp w reads TMEM lanes 32·(w % 4) .. +31; warps 2..5 take
     // columns 0..15 of each tile and of the sums, 6..9 columns 16..31, and
-    // so on.
+    // so on. The four warps of a lane quarter exchange row maxima over their
+    // own named barrier; each warp signals the MMA warp by itself.
     constexpr int CW = 16;  // columns per thread
+    constexpr int kShift = 8 * S - 2;
     const int h = (warp - 2) >> 2;
-    const int r = (warp & 3) * 32 + lane;
+    const int quarter = warp & 3;
+    const int r = quarter * 32 + lane;
     const int64_t xl = (int64_t)xt * AM + r;
     const bool valid = xl < a.lnx;
     const int lo = row_lo[r], hi = row_hi[r];
+    // Column c of a tile starting at jl0 is allowed iff (unsigned)(jl0 + c - lo) < span.
+    const unsigned span = (valid && lo < hi) ? (unsigned)(hi - lo) : 0u;
     const int eqr = valid ? a.eq[(int64_t)w * a.lnx_pad + xl] : 0;
-    const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
     const uint32_t sum_addr = lane_addr + (uint32_t)(kSumCol + h * 2 * CW);
     const double NEG_INF = -INFINITY;
-    const double to_int = pow2(8 * S - 2);
+    // z sums the weights times 2^(8S-2); the running sums are in units of
+    // their columns' powers of two 2^(2 + ev).
     double m = NEG_INF, z = 0.0, light = INFINITY;
-    bool ok = true;
+    auto wait = [&](uint64_t* bar, uint32_t parity) {
+      if (*(volatile int*)failed) return;
+      if (!mbar_wait(bar, parity)) {
+        *(volatile int*)failed = 1;
+        atomicOr(a.status, 2);
+      }
+    };
     for (int it = 0; it < n_tiles; it++) {
       const int jl0 = (jt0 + it) * AJ + h * CW;
       const int* eks = ek_s + (it % Sh::kStages) * AJ + h * CW;
-      ok = named_bar_and(1, kEpi, mbar_wait(qk_full, (uint32_t)(it & 1)));
-      if (!ok) break;
+      wait(qk_full, (uint32_t)(it & 1));
       tc_fence_after();
       double sc[CW];
 #pragma unroll
@@ -310,22 +326,37 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
 #pragma unroll
         for (int i = 0; i < 4; i++) {
           const int c = c4 * 4 + i;
-          double s = scale2(level_sum<S, KB>(L, i), eqr + eks[c]);
-          if (a.scale_kind == 1) s = s * a.scale_c;
-          else if (a.scale_kind == 2) s = __ddiv_rn(s, a.scale_c);
-          const bool in = valid && jl0 + c >= lo && jl0 + c < hi;
-          sc[c] = in ? s : NEG_INF;
+          const double l = level_sum<S, KB>(L, i);
+          sc[c] = FAST ? l * pow2(eqr + eks[c]) : scale2(l, eqr + eks[c]);
         }
       }
-      // The row's largest score in this tile, over the four quarters.
-      double mx = NEG_INF;
+      if (a.scale_kind == 1) {
 #pragma unroll
-      for (int c = 0; c < CW; c++) {
-        mx = fmax(mx, sc[c]);
-        if (sc[c] != NEG_INF) light = fmin(light, sc[c]);
+        for (int c = 0; c < CW; c++) sc[c] *= a.scale_c;
+      } else if (a.scale_kind == 2) {
+#pragma unroll
+        for (int c = 0; c < CW; c++) sc[c] = __ddiv_rn(sc[c], a.scale_c);
+      }
+      // The mask, and the row's largest and smallest allowed scores.
+      const int off = jl0 - lo;
+      double mx = NEG_INF;
+      if (__all_sync(0xffffffffu, off >= 0 && (unsigned)off + CW <= span)) {
+#pragma unroll
+        for (int c = 0; c < CW; c++) {
+          mx = fmax(mx, sc[c]);
+          light = fmin(light, sc[c]);
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < CW; c++) {
+          const bool in = (unsigned)(off + c) < span;
+          light = fmin(light, in ? sc[c] : INFINITY);
+          sc[c] = in ? sc[c] : NEG_INF;
+          mx = fmax(mx, sc[c]);
+        }
       }
       red[h * AM + r] = mx;
-      named_bar(1, kEpi);
+      named_bar(2 + quarter, 128);
       mx = fmax(fmax(red[r], red[AM + r]), fmax(red[2 * AM + r], red[3 * AM + r]));
       const double m_new = fmax(m, mx);
       double rescale = 1.0;
@@ -334,8 +365,9 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
         z *= rescale;
         m = m_new;
       }
-      // Weights and their digits: W = w · 2^(8S-2) < 2^(8S-2), balanced
-      // base-256 digits, most significant first, four columns a word.
+      // Weights and their digits: W = exp(s - m) · 2^(8S-2) < 2^(8S-2),
+      // balanced base-256 digits, most significant first, four columns a
+      // word.
       uint8_t* prow = sP + r * 64;
 #pragma unroll
       for (int c4 = 0; c4 < CW / 4; c4++) {
@@ -343,22 +375,21 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
 #pragma unroll
         for (int i = 0; i < 4; i++) {
           const double sv = sc[c4 * 4 + i];
-          const double wt = sv == NEG_INF ? 0.0 : exp_tang(sv - m, texp);
-          z += wt;
-          x[i] = wt * to_int;
+          const double wt = exp_weight(sv - m, texp, kShift);
+          x[i] = sv == NEG_INF ? 0.0 : wt;
+          z += x[i];
         }
         uint32_t planes[S];
         digit_planes4<S>(x, planes);
-        const uint32_t off = sw64_offset((uint32_t)r, (uint32_t)(h * CW + c4 * 4)) - (uint32_t)r * 64;
+        const uint32_t off4 = sw64_offset((uint32_t)r, (uint32_t)(h * CW + c4 * 4)) - (uint32_t)r * 64;
 #pragma unroll
-        for (int s = 0; s < S; s++) *(uint32_t*)(prow + s * AM * 64 + off) = planes[s];
+        for (int s = 0; s < S; s++) *(uint32_t*)(prow + s * AM * 64 + off4) = planes[s];
       }
       fence_proxy_async();
       tc_fence_before();
-      named_bar(1, kEpi);
-      if (warp == 2 && lane == 0) mbar_arrive(p_full);
-      ok = named_bar_and(1, kEpi, mbar_wait(pv_full, (uint32_t)(it & 1)));
-      if (!ok) break;
+      __syncwarp();
+      if (lane == 0) mbar_arrive(p_full);
+      wait(pv_full, (uint32_t)(it & 1));
       tc_fence_after();
       // sums = sums · rescale + this tile's weighted values, four at a time.
 #pragma unroll
@@ -372,8 +403,8 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
         }
 #pragma unroll
         for (int i = 0; i < 4; i++) {
-          const double prev = it > 0 ? __hiloint2double((int)sum[2 * i + 1], (int)sum[2 * i]) * rescale : 0.0;
-          const double v = prev + scale2(combine_levels_small<S, 4>(L, i), 2 + ev_s[h * CW + c4 * 4 + i]);
+          const double l = combine_levels_small<S, 4>(L, i);
+          const double v = it > 0 ? fma(__hiloint2double((int)sum[2 * i + 1], (int)sum[2 * i]), rescale, l) : l;
           sum[2 * i] = (uint32_t)__double2loint(v);
           sum[2 * i + 1] = (uint32_t)__double2hiint(v);
         }
@@ -381,23 +412,18 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
       }
       tmem_wait_st();
       tc_fence_before();
-      named_bar(1, kEpi);
-      if (warp == 2 && lane == 0) mbar_arrive(tmem_free);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tmem_free);
     }
-    if (!ok) {
-      if (warp == 2 && lane == 0) {
-        atomicOr(a.status, 2);
-        *(volatile int*)failed = 1;
-      }
-    } else if (n_tiles > 0) {
+    if (n_tiles > 0) {
       // The four quarters' sums of weights and lightest scores (P's digits
       // are no longer read).
       double* xz = (double*)sP;
       double* xlg = xz + 4 * AM;
       xz[h * AM + r] = z;
       xlg[h * AM + r] = light;
-      named_bar(1, kEpi);
-      z = (xz[r] + xz[AM + r]) + (xz[2 * AM + r] + xz[3 * AM + r]);
+      named_bar(2 + quarter, 128);
+      z = ((xz[r] + xz[AM + r]) + (xz[2 * AM + r] + xz[3 * AM + r])) * pow2(-kShift);
       light = fmin(fmin(xlg[r], xlg[AM + r]), fmin(xlg[2 * AM + r], xlg[3 * AM + r]));
       tc_fence_after();
       double o[CW];
@@ -407,9 +433,10 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
         tmem_ld8(sum_addr + c4 * 8, (int32_t*)sum);
         tmem_wait_ld();
 #pragma unroll
-        for (int i = 0; i < 4; i++) o[c4 * 4 + i] = __hiloint2double((int)sum[2 * i + 1], (int)sum[2 * i]);
+        for (int i = 0; i < 4; i++)
+          o[c4 * 4 + i] = scale2(__hiloint2double((int)sum[2 * i + 1], (int)sum[2 * i]), 2 + ev_s[h * CW + c4 * 4 + i]);
       }
-      if (valid && lo < hi) {
+      if (valid && lo < hi && !*(volatile int*)failed) {
         // Bounds::hold (fused.rs:1058-1086): the heaviest weight is
         // exp(high - m) = 1, the row's largest score being m.
         const double rl = a.rl[x_base + xl], rs = a.rs[x_base + xl];
@@ -505,22 +532,14 @@ __global__ void row_value_bounds(int64_t nx, Mask m, const double* __restrict__ 
   }
 }
 
-__global__ void exp_max(const int32_t* __restrict__ e, int64_t n, int* __restrict__ out) {
-  int m = INT_MIN;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    m = max(m, e[i]);
-  for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
-}
-
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
-template <int S, int KB>
+template <int S, int KB, bool FAST>
 void launch(const CUtensorMap& tq, const CUtensorMap& tk, const CUtensorMap& tv, const AttnArgs& args, dim3 grid,
             cudaStream_t stream) {
   using Sh = AttnShape<S, KB>;
-  EF_CUDA(cudaFuncSetAttribute(attn_fwd_split<S, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::kSmem));
-  attn_fwd_split<S, KB><<<grid, kAttnThreads, Sh::kSmem, stream>>>(tq, tk, tv, args);
+  EF_CUDA(cudaFuncSetAttribute(attn_fwd_split<S, KB, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::kSmem));
+  attn_fwd_split<S, KB, FAST><<<grid, kAttnThreads, Sh::kSmem, stream>>>(tq, tk, tv, args);
   EF_LAUNCH_CHECK();
 }
 
@@ -551,25 +570,29 @@ AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int sl
   int32_t* ek = eq + W * lnx_pad;
   int32_t* ev = ek + W * lnj_pad;
   unsigned long long* colmax = (unsigned long long*)(b + szq + szk + szv + sze);
-  // [0] slicing, [1] kernel, [2] max eq, [3] max ek, [4..5] tile pairs
+  // [0] slicing, [1] kernel, [2..3] max eq, max -eq, [4..5] max ek, max -ek,
+  // [6..7] tile pairs
   int* status = (int*)(b + szq + szk + szv + sze + szc);
-  unsigned long long* tiles = (unsigned long long*)(status + 4);
-  EF_CUDA(cudaMemsetAsync(status, 0, 24, stream));
-  const int init[2] = {INT_MIN, INT_MIN};
-  EF_CUDA(cudaMemcpyAsync(status + 2, init, 8, cudaMemcpyHostToDevice, stream));
+  unsigned long long* tiles = (unsigned long long*)(status + 6);
+  EF_CUDA(cudaMemsetAsync(status, 0, 32, stream));
+  const int init[4] = {INT_MIN, INT_MIN, INT_MIN, INT_MIN};
+  EF_CUDA(cudaMemcpyAsync(status + 2, init, 16, cudaMemcpyHostToDevice, stream));
   slice_rows_into(S, p.q, W, p.lnx, p.ne, p.ne, lnx_pad, d_pad, eq, qd, status, stream);
   slice_rows_into(S, p.k, W, p.lnj, p.ne, p.ne, lnj_pad, d_pad, ek, kd, status, stream);
   slice_cols_into(S, p.v, W, p.lnj, p.ny, ny_pad, lnj_pad, colmax, ev, vd, status, stream);
-  exp_max<<<blocks_for((uint64_t)(W * lnx_pad), 256), 256, 0, stream>>>(eq, W * lnx_pad, status + 2);
-  exp_max<<<blocks_for((uint64_t)(W * lnj_pad), 256), 256, 0, stream>>>(ek, W * lnj_pad, status + 3);
+  exponent_range(eq, W * lnx_pad, status + 2, stream);
+  exponent_range(ek, W * lnj_pad, status + 4, stream);
   ctx.kernels += 6;
-  int st[4];
-  EF_CUDA(cudaMemcpyAsync(st, status, 16, cudaMemcpyDeviceToHost, stream));
+  int st[6];
+  EF_CUDA(cudaMemcpyAsync(st, status, 24, cudaMemcpyDeviceToHost, stream));
   EF_CUDA(cudaStreamSynchronize(stream));
   ctx.phase("attention: sliced");
   // Every operand finite, and no score near overflow: |s| < ne · 2^(eq+ek-4).
   if (st[0] & 1) return ATTENTION_INELIGIBLE;
-  if ((int64_t)st[2] + st[3] + 8 + (int64_t)std::ceil(std::log2((double)p.ne + 1)) > 1000) return ATTENTION_INELIGIBLE;
+  if ((int64_t)st[2] + st[4] + 8 + (int64_t)std::ceil(std::log2((double)p.ne + 1)) > 1000) return ATTENTION_INELIGIBLE;
+  // Scores' powers of two 2^(eq + ek) all normal doubles (the bound above
+  // keeps eq + ek below 1000).
+  const bool fast = (int64_t)st[3] + st[5] <= 1022;
 
   const CUtensorMap tq = digit_planes_map(qd, d_pad, lnx_pad, W * S, AM, S);
   const CUtensorMap tk = digit_planes_map(kd, d_pad, lnj_pad, W * S, AJ, S);
@@ -614,8 +637,13 @@ AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int sl
   EF_CUDA(cudaEventRecord(e0, stream));
   for (int64_t y0 = 0; y0 < p.ny; y0 += AY) {
     args.y0 = (int)y0;
-    if (KB == 1) launch<6, 1>(tq, tk, tv, args, grid, stream);
-    else launch<6, 2>(tq, tk, tv, args, grid, stream);
+    if (KB == 1) {
+      if (fast) launch<6, 1, true>(tq, tk, tv, args, grid, stream);
+      else launch<6, 1, false>(tq, tk, tv, args, grid, stream);
+    } else {
+      if (fast) launch<6, 2, true>(tq, tk, tv, args, grid, stream);
+      else launch<6, 2, false>(tq, tk, tv, args, grid, stream);
+    }
     ctx.kernels++;
   }
   EF_CUDA(cudaEventRecord(e1, stream));

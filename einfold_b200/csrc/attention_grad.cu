@@ -22,7 +22,9 @@
 // take a quarter of the columns each. The FP64 form runs the same tiles on
 // the CUDA cores.
 #include <algorithm>
+#include <climits>
 #include <cmath>
+#include <type_traits>
 
 #include "attention.cuh"
 #include "fastexp.cuh"
@@ -53,10 +55,12 @@ struct GradShape {
   static constexpr int kB2 = kTwo ? S * GJ * 64 : 0;
   static constexpr int kB3 = S * GY * 64;
   static constexpr int kE = 2 * GJ * 4;              // the columns' exponents of products 1 and 2
+  // Rows of keys: the columns' (queries') lse, and for d_k their D.
+  static constexpr int kL = (MODE == GRAD_V ? 1 : (MODE == GRAD_K ? 2 : 0)) * GJ * 8;
   static constexpr int kP = S * GM * 64;
   static constexpr int kAux = 8192;
   static constexpr int kFixed = kA1 + kA2 + kP + kAux + 1024;
-  static constexpr int kStage = kB1 + kB2 + kB3 + kE;
+  static constexpr int kStage = (kB1 + kB2 + kB3 + kE + kL + 1023) / 1024 * 1024;
   static constexpr int kStages = kFixed + 2 * kStage <= kMaxSmem ? 2 : 1;
   static constexpr int kSmem = kFixed + kStages * kStage;
   static_assert(kSmem <= kMaxSmem, "the tiles must fit in shared memory");
@@ -74,13 +78,17 @@ struct GradArgs {
   const int32_t* e_b3;  // [w][dy_pad]
   const double* lse;    // per query: [w·lq + x]
   const double* dd;     // D per query
+  const double* lse_pad;  // the same, [w][lq_pad] (zeros past lq), for stages of keys' rows
+  const double* dd_pad;
   const double* exp_table;
   double* out;  // [w·lr + r][dy]
   int* status;
   unsigned long long* tiles;
 };
 
-template <int MODE>
+// FAST: every pair of row and column exponents of products 1 and 2 sums to
+// a normal double's power of two.
+template <int MODE, bool FAST>
 __global__ void __launch_bounds__(kGradThreads, 1)
     grad_split(const __grid_constant__ CUtensorMap ta1, const __grid_constant__ CUtensorMap tb1,
                const __grid_constant__ CUtensorMap ta2, const __grid_constant__ CUtensorMap tb2,
@@ -121,6 +129,10 @@ __global__ void __launch_bounds__(kGradThreads, 1)
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < 11; i++) mbar_init(&bars[i], 1);
+    // Each epilogue warp arrives on the barriers that free TMEM or shared memory.
+    mbar_init(t1_free, kEpi / 32);
+    mbar_init(p_full, kEpi / 32);
+    mbar_init(tmem_free, kEpi / 32);
     *failed = 0;
     span[0] = LLONG_MAX;
     span[1] = LLONG_MIN;
@@ -179,7 +191,7 @@ __global__ void __launch_bounds__(kGradThreads, 1)
           *(volatile int*)failed = 1;
           break;
         }
-        mbar_expect_tx(&kv_full[st], (uint32_t)(Sh::kB1 + Sh::kB2 + Sh::kB3 + (kTwo ? 2 : 1) * GJ * 4));
+        mbar_expect_tx(&kv_full[st], (uint32_t)(Sh::kB1 + Sh::kB2 + Sh::kB3 + (kTwo ? 2 : 1) * GJ * 4 + Sh::kL));
         const int cl0 = (ct0 + it) * GJ;
         uint8_t* stage = sB + st * Sh::kStage;
         int* es = (int*)(stage + Sh::kB1 + Sh::kB2 + Sh::kB3);
@@ -188,6 +200,11 @@ __global__ void __launch_bounds__(kGradThreads, 1)
         tma_load_3d(stage + Sh::kB1 + Sh::kB2, &tb3, &kv_full[st], cl0, a.y0, w * S);
         bulk_load(es, a.e_b1 + (int64_t)w * a.lc_pad + cl0, GJ * 4, &kv_full[st]);
         if (kTwo) bulk_load(es + GJ, a.e_b2 + (int64_t)w * a.lc_pad + cl0, GJ * 4, &kv_full[st]);
+        if (MODE != GRAD_Q) {
+          double* ls = (double*)(stage + Sh::kB1 + Sh::kB2 + Sh::kB3 + Sh::kE);
+          bulk_load(ls, a.lse_pad + (int64_t)w * a.lc_pad + cl0, GJ * 8, &kv_full[st]);
+          if (MODE == GRAD_K) bulk_load(ls + GJ, a.dd_pad + (int64_t)w * a.lc_pad + cl0, GJ * 8, &kv_full[st]);
+        }
         issued = it + 1;
       }
       mbar_wait(a_full, 0);
@@ -249,26 +266,45 @@ __global__ void __launch_bounds__(kGradThreads, 1)
       if (last_bar) mbar_wait(last_bar, last_parity);
     }
   } else {
+    // Epilogue: warp w reads TMEM lanes 32·(w % 4) .. +31 and a quarter of
+    // the columns; the four warps of a lane quarter exchange row maxima over
+    // their own named barrier, and each warp signals the MMA warp by itself.
     const int h = (warp - 2) >> 2;
-    const int r = (warp & 3) * 32 + lane;
+    const int quarter = warp & 3;
+    const int r = quarter * 32 + lane;
     const int64_t rl = (int64_t)rt * GM + r;
     const bool valid = rl < a.lr;
     const int lo = row_lo[r], hi = row_hi[r];
+    // Column c of a tile starting at cl0 is allowed iff (unsigned)(cl0 + c - lo) < span.
+    const unsigned span = (valid && lo < hi) ? (unsigned)(hi - lo) : 0u;
     const int e1r = valid ? a.e_a1[(int64_t)w * a.lr_pad + rl] : 0;
     const int e2r = (kTwo && valid) ? a.e_a2[(int64_t)w * a.lr_pad + rl] : 0;
     // A row of queries reads its own lse and D; a row of keys its columns'.
     const double lse_r = (MODE == GRAD_Q && valid) ? a.lse[r_base + rl] : 0.0;
     const double dd_r = (MODE == GRAD_Q && valid) ? a.dd[r_base + rl] : 0.0;
-    const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
     const uint32_t sum_addr = lane_addr + (uint32_t)(kSumCol + h * 2 * CW);
-    bool ok = true;
+    int e3lo = INT_MAX, e3hi = INT_MIN;
+    for (int c = 0; c < GY; c++) {
+      e3lo = min(e3lo, e3_s[c]);
+      e3hi = max(e3hi, e3_s[c]);
+    }
+    auto wait = [&](uint64_t* bar, uint32_t parity) {
+      if (*(volatile int*)failed) return;
+      if (!mbar_wait(bar, parity)) {
+        *(volatile int*)failed = 1;
+        atomicOr(a.status, 2);
+      }
+    };
     for (int it = 0; it < n_tiles; it++) {
       const int st = it % Sh::kStages;
       const int cl0 = (ct0 + it) * GJ + h * CW;
-      const int* es = (const int*)(sB + st * Sh::kStage + Sh::kB1 + Sh::kB2 + Sh::kB3) + h * CW;
+      const uint8_t* stage = sB + st * Sh::kStage;
+      const int* es = (const int*)(stage + Sh::kB1 + Sh::kB2 + Sh::kB3) + h * CW;
+      const double* ls = (const double*)(stage + Sh::kB1 + Sh::kB2 + Sh::kB3 + Sh::kE) + h * CW;
       const uint32_t par = (uint32_t)(it & 1);
-      ok = named_bar_and(1, kEpi, mbar_wait(s1_full, par));
-      if (!ok) break;
+      const int off = cl0 - lo;
+      wait(s1_full, par);
       tc_fence_after();
       double wv[CW];
 #pragma unroll
@@ -280,21 +316,17 @@ __global__ void __launch_bounds__(kGradThreads, 1)
 #pragma unroll
         for (int i = 0; i < 4; i++) {
           const int c = c4 * 4 + i;
-          const int cl = cl0 + c;
-          double p = 0.0;
-          if (valid && cl >= lo && cl < hi) {
-            const double s = a.scale * scale2(combine_levels_small<S, 4>(L, i), e1r + es[c]);
-            p = exp_tang(s - (MODE == GRAD_Q ? lse_r : a.lse[c_base + cl]), texp);
-          }
-          wv[c] = p;
+          const double l = combine_levels_small<S, 4>(L, i);
+          const double s = a.scale * (FAST ? l * pow2(e1r + es[c]) : scale2(l, e1r + es[c]));
+          const double p = exp_weight(s - (MODE == GRAD_Q ? lse_r : ls[c]), texp, 0);
+          wv[c] = (unsigned)(off + c) < span ? p : 0.0;
         }
       }
       if (kTwo) {
         tc_fence_before();
-        named_bar(1, kEpi);
-        if (warp == 2 && lane == 0) mbar_arrive(t1_free);
-        ok = named_bar_and(1, kEpi, mbar_wait(s2_full, par));
-        if (!ok) break;
+        __syncwarp();
+        if (lane == 0) mbar_arrive(t1_free);
+        wait(s2_full, par);
         tc_fence_after();
 #pragma unroll
         for (int c4 = 0; c4 < CW / 4; c4++) {
@@ -305,11 +337,10 @@ __global__ void __launch_bounds__(kGradThreads, 1)
 #pragma unroll
           for (int i = 0; i < 4; i++) {
             const int c = c4 * 4 + i;
-            const int cl = cl0 + c;
-            if (wv[c] != 0.0) {
-              const double dp = scale2(combine_levels_small<S, 4>(L, i), e2r + es[GJ + c]);
-              wv[c] = wv[c] * (dp - (MODE == GRAD_Q ? dd_r : a.dd[c_base + cl]));
-            }
+            const double l = combine_levels_small<S, 4>(L, i);
+            const double dp = FAST ? l * pow2(e2r + es[GJ + c]) : scale2(l, e2r + es[GJ + c]);
+            const double t = wv[c] * (dp - (MODE == GRAD_Q ? dd_r : ls[GJ + c]));
+            wv[c] = wv[c] != 0.0 ? t : 0.0;
           }
         }
       }
@@ -318,74 +349,77 @@ __global__ void __launch_bounds__(kGradThreads, 1)
 #pragma unroll
       for (int c = 0; c < CW; c++) mx = fmax(mx, fabs(wv[c]));
       red[h * GM + r] = mx;
-      named_bar(1, kEpi);
+      named_bar(2 + quarter, 128);
       const int ew = slice_exponent(fmax(fmax(red[r], red[GM + r]), fmax(red[2 * GM + r], red[3 * GM + r])));
-      // The weights' digits: W = w · 2^(8S - ew), |W| < 2^(8S-2).
+      // The weights' digits: W = w · 2^(8S - ew), |W| < 2^(8S-2), the power
+      // of two applied in two exact halves (8S - ew lies in [-978, 1119]).
       const int shift = 8 * S - ew;
+      const double f1 = pow2(shift >> 1), f2 = pow2(shift - (shift >> 1));
       uint8_t* prow = sP + r * 64;
 #pragma unroll
       for (int c4 = 0; c4 < CW / 4; c4++) {
         double x[4];
 #pragma unroll
-        for (int i = 0; i < 4; i++) x[i] = scale2(wv[c4 * 4 + i], shift);
+        for (int i = 0; i < 4; i++) x[i] = wv[c4 * 4 + i] * f1 * f2;
         uint32_t planes[S];
         digit_planes4<S>(x, planes);
-        const uint32_t off = sw64_offset((uint32_t)r, (uint32_t)(h * CW + c4 * 4)) - (uint32_t)r * 64;
+        const uint32_t off4 = sw64_offset((uint32_t)r, (uint32_t)(h * CW + c4 * 4)) - (uint32_t)r * 64;
 #pragma unroll
-        for (int s = 0; s < S; s++) *(uint32_t*)(prow + s * GM * 64 + off) = planes[s];
+        for (int s = 0; s < S; s++) *(uint32_t*)(prow + s * GM * 64 + off4) = planes[s];
       }
       fence_proxy_async();
       tc_fence_before();
-      named_bar(1, kEpi);
-      if (warp == 2 && lane == 0) mbar_arrive(p_full);
-      ok = named_bar_and(1, kEpi, mbar_wait(o_full, par));
-      if (!ok) break;
+      __syncwarp();
+      if (lane == 0) mbar_arrive(p_full);
+      wait(o_full, par);
       tc_fence_after();
+      // sums += this tile's levels · 2^(ew + e3): one rounding either way,
+      // the power of two a normal double on the first path.
+      auto add_levels = [&](auto normal) {
 #pragma unroll
-      for (int c4 = 0; c4 < CW / 4; c4++) {
-        int32_t L[S][4];
+        for (int c4 = 0; c4 < CW / 4; c4++) {
+          int32_t L[S][4];
 #pragma unroll
-        for (int l = 0; l < S; l++) tmem_ld4(lane_addr + (uint32_t)(l * GY + h * CW + c4 * 4), L[l]);
-        uint32_t sum[8];
-        if (it > 0) tmem_ld8(sum_addr + c4 * 8, (int32_t*)sum);
-        tmem_wait_ld();
+          for (int l = 0; l < S; l++) tmem_ld4(lane_addr + (uint32_t)(l * GY + h * CW + c4 * 4), L[l]);
+          uint32_t sum[8];
+          if (it > 0) tmem_ld8(sum_addr + c4 * 8, (int32_t*)sum);
+          tmem_wait_ld();
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-          const double prev = it > 0 ? __hiloint2double((int)sum[2 * i + 1], (int)sum[2 * i]) : 0.0;
-          const double v = prev + scale2(combine_levels_small<S, 4>(L, i), ew + e3_s[h * CW + c4 * 4 + i]);
-          sum[2 * i] = (uint32_t)__double2loint(v);
-          sum[2 * i + 1] = (uint32_t)__double2hiint(v);
+          for (int i = 0; i < 4; i++) {
+            const int e = ew + e3_s[h * CW + c4 * 4 + i];
+            const double prev = it > 0 ? __hiloint2double((int)sum[2 * i + 1], (int)sum[2 * i]) : 0.0;
+            const double l = combine_levels_small<S, 4>(L, i);
+            const double v = decltype(normal)::value ? fma(l, pow2(e), prev) : prev + scale2(l, e);
+            sum[2 * i] = (uint32_t)__double2loint(v);
+            sum[2 * i + 1] = (uint32_t)__double2hiint(v);
+          }
+          tmem_st8(sum_addr + c4 * 8, sum);
         }
-        tmem_st8(sum_addr + c4 * 8, sum);
-      }
+      };
+      if (__all_sync(0xffffffffu, ew + e3lo >= -1022 && ew + e3hi <= 1023)) add_levels(std::true_type{});
+      else add_levels(std::false_type{});
       tmem_wait_st();
       tc_fence_before();
-      named_bar(1, kEpi);
-      if (warp == 2 && lane == 0) mbar_arrive(tmem_free);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tmem_free);
     }
-    if (!ok) {
-      if (warp == 2 && lane == 0) {
-        atomicOr(a.status, 2);
-        *(volatile int*)failed = 1;
+    // Every lane of the warp reads TMEM (the loads are warp-wide); the rows
+    // past the batch's end write nothing.
+    tc_fence_after();
+    const bool store = valid && !*(volatile int*)failed;
+    double* orow = a.out + (r_base + rl) * a.dy;
+#pragma unroll
+    for (int c4 = 0; c4 < CW / 4; c4++) {
+      uint32_t sum[8];
+      if (n_tiles > 0) {
+        tmem_ld8(sum_addr + c4 * 8, (int32_t*)sum);
+        tmem_wait_ld();
       }
-    } else {
-      // Every lane of the warp reads TMEM (the loads are warp-wide); the
-      // rows past the batch's end write nothing.
-      tc_fence_after();
-      double* orow = a.out + (r_base + rl) * a.dy;
 #pragma unroll
-      for (int c4 = 0; c4 < CW / 4; c4++) {
-        uint32_t sum[8];
-        if (n_tiles > 0) {
-          tmem_ld8(sum_addr + c4 * 8, (int32_t*)sum);
-          tmem_wait_ld();
-        }
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-          const int64_t y = (int64_t)a.y0 + h * CW + c4 * 4 + i;
-          const double v = n_tiles > 0 ? __hiloint2double((int)sum[2 * i + 1], (int)sum[2 * i]) : 0.0;
-          if (valid && y < a.dy) orow[y] = a.out_factor * v;
-        }
+      for (int i = 0; i < 4; i++) {
+        const int64_t y = (int64_t)a.y0 + h * CW + c4 * 4 + i;
+        const double v = n_tiles > 0 ? __hiloint2double((int)sum[2 * i + 1], (int)sum[2 * i]) : 0.0;
+        if (store && y < a.dy) orow[y] = a.out_factor * v;
       }
     }
   }
@@ -549,11 +583,28 @@ struct Digits {
 };
 
 template <int MODE>
-void launch_split(const CUtensorMap* maps, const GradArgs& args, dim3 grid, cudaStream_t stream) {
+void launch_split(const CUtensorMap* maps, const GradArgs& args, dim3 grid, bool fast, cudaStream_t stream) {
   using Sh = GradShape<MODE>;
-  EF_CUDA(cudaFuncSetAttribute(grad_split<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::kSmem));
-  grad_split<MODE><<<grid, kGradThreads, Sh::kSmem, stream>>>(maps[0], maps[1], maps[2], maps[3], maps[4], args);
+  if (fast) {
+    EF_CUDA(cudaFuncSetAttribute(grad_split<MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::kSmem));
+    grad_split<MODE, true><<<grid, kGradThreads, Sh::kSmem, stream>>>(maps[0], maps[1], maps[2], maps[3], maps[4],
+                                                                       args);
+  } else {
+    EF_CUDA(cudaFuncSetAttribute(grad_split<MODE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::kSmem));
+    grad_split<MODE, false><<<grid, kGradThreads, Sh::kSmem, stream>>>(maps[0], maps[1], maps[2], maps[3], maps[4],
+                                                                        args);
+  }
   EF_LAUNCH_CHECK();
+}
+
+// dst[w][x] = src[w·l + x] for x < l, 0 up to l_pad.
+__global__ void pad_rows(const double* __restrict__ src, int64_t batches, int64_t l, int64_t l_pad,
+                         double* __restrict__ dst) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < batches * l_pad;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t w = i / l_pad, x = i - w * l_pad;
+    dst[i] = x < l ? src[w * l + x] : 0.0;
+  }
 }
 
 // The split backward; false if it doesn't apply or an operand isn't finite
@@ -570,8 +621,8 @@ bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd,
   const size_t rq = al((size_t)(W * S * lq_pad * 64)), rk = al((size_t)(W * S * lk_pad * 64));
   const size_t cq = al((size_t)(W * S * 64 * lq_pad)), ck = al((size_t)(W * S * 64 * lk_pad));
   const size_t eqs = al((size_t)(W * lq_pad) * 4), eks = al((size_t)(W * lk_pad) * 4), ecs = al((size_t)(W * 64) * 4);
-  const size_t cm = al((size_t)(W * 64) * 8);
-  const size_t total = 2 * rq + 2 * rk + 2 * cq + ck + 2 * eqs + 2 * eks + 3 * ecs + cm + 256;
+  const size_t cm = al((size_t)(W * 64) * 8), lp = al((size_t)(W * lq_pad) * 8);
+  const size_t total = 2 * rq + 2 * rk + 2 * cq + ck + 2 * eqs + 2 * eks + 3 * ecs + cm + 2 * lp + 256;
   DeviceBuffer<uint8_t> scratch(total, s);
   uint8_t* p = scratch.get();
   auto take = [&](size_t n) {
@@ -590,9 +641,15 @@ bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd,
   Qc.e = (int32_t*)take(ecs);
   Kc.e = (int32_t*)take(ecs);
   unsigned long long* colmax = (unsigned long long*)take(cm);
-  int* status = (int*)take(256);  // [0] slicing, [1] kernels, [2..7] tile pairs of the three kernels
+  double* lse_pad = (double*)take(lp);
+  double* dd_pad = (double*)take(lp);
+  // [0] slicing, [1] kernels, [2..7] tile pairs of the three kernels,
+  // [8..15] (max e, max -e) of q's, k's, v's and d_out's rows
+  int* status = (int*)take(256);
   unsigned long long* tiles = (unsigned long long*)(status + 2);
   EF_CUDA(cudaMemsetAsync(status, 0, 32, s));
+  const int init[8] = {INT_MIN, INT_MIN, INT_MIN, INT_MIN, INT_MIN, INT_MIN, INT_MIN, INT_MIN};
+  EF_CUDA(cudaMemcpyAsync(status + 8, init, 32, cudaMemcpyHostToDevice, s));
   slice_rows_into(S, f.q, W, lq, d, d, lq_pad, 64, Qr.e, Qr.d, status, s);
   slice_rows_into(S, g.d_out, W, lq, dv, dv, lq_pad, 64, dOr.e, dOr.d, status, s);
   slice_rows_into(S, f.k, W, lk, d, d, lk_pad, 64, Kr.e, Kr.d, status, s);
@@ -600,11 +657,22 @@ bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd,
   slice_cols_into(S, g.d_out, W, lq, dv, 64, lq_pad, colmax, dOc.e, dOc.d, status, s);
   slice_cols_into(S, f.q, W, lq, d, 64, lq_pad, colmax, Qc.e, Qc.d, status, s);
   slice_cols_into(S, f.k, W, lk, d, 64, lk_pad, colmax, Kc.e, Kc.d, status, s);
-  ctx.kernels += 10;
-  int st = 0;
-  EF_CUDA(cudaMemcpyAsync(&st, status, 4, cudaMemcpyDeviceToHost, s));
+  exponent_range(Qr.e, W * lq_pad, status + 8, s);
+  exponent_range(Kr.e, W * lk_pad, status + 10, s);
+  exponent_range(Vr.e, W * lk_pad, status + 12, s);
+  exponent_range(dOr.e, W * lq_pad, status + 14, s);
+  pad_rows<<<blocks_for((uint64_t)(W * lq_pad), 256), 256, 0, s>>>(g.lse, W, lq, lq_pad, lse_pad);
+  pad_rows<<<blocks_for((uint64_t)(W * lq_pad), 256), 256, 0, s>>>(dd, W, lq, lq_pad, dd_pad);
+  EF_LAUNCH_CHECK();
+  ctx.kernels += 16;
+  int sts[16];
+  EF_CUDA(cudaMemcpyAsync(sts, status, 64, cudaMemcpyDeviceToHost, s));
   EF_CUDA(cudaStreamSynchronize(s));
+  int st = sts[0];
   if (st & 1) return false;
+  // Products 1 (q·k) and 2 (d_out·v) have normal powers of two 2^(e_r + e_c).
+  const bool fast = (int64_t)sts[8] + sts[10] <= 1023 && (int64_t)sts[9] + sts[11] <= 1022 &&
+                    (int64_t)sts[12] + sts[14] <= 1023 && (int64_t)sts[13] + sts[15] <= 1022;
   ctx.phase("attention backward: sliced");
   auto rows_map = [&](const Digits& x, int64_t rows_pad, int box) {
     return digit_planes_map(x.d, 64, rows_pad, W * S, box, S);
@@ -628,6 +696,8 @@ bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd,
     a.scale = f.scale_kind == 1 ? f.scale_c : 1.0;
     a.lse = g.lse;
     a.dd = dd;
+    a.lse_pad = lse_pad;
+    a.dd_pad = dd_pad;
     a.exp_table = table;
     a.status = status + 1;
     a.tiles = tiles + mode;
@@ -675,9 +745,9 @@ bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd,
     a.dy_pad = 64;
     a.y0 = 0;
     const dim3 grid((unsigned)(a.lr_pad / GM), (unsigned)W);
-    if (mode == GRAD_V) launch_split<GRAD_V>(maps, a, grid, s);
-    else if (mode == GRAD_K) launch_split<GRAD_K>(maps, a, grid, s);
-    else launch_split<GRAD_Q>(maps, a, grid, s);
+    if (mode == GRAD_V) launch_split<GRAD_V>(maps, a, grid, fast, s);
+    else if (mode == GRAD_K) launch_split<GRAD_K>(maps, a, grid, fast, s);
+    else launch_split<GRAD_Q>(maps, a, grid, fast, s);
     ctx.kernels++;
   }
   EF_CUDA(cudaEventRecord(e1, s));

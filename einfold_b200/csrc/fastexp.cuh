@@ -42,4 +42,25 @@ __device__ __forceinline__ double exp_tang(double x, const double* __restrict__ 
   return p * table[k & 63] * ptx::pow2(k >> 6);
 }
 
+// 2^shift · exp(x) for softmax weights (x <= 0 and 0 <= shift <= 64, or
+// shift = 0), without the range test: x is clamped to [-708, 709], so the
+// scaling stays a normal power of two. Below -708 the result (under 2^(shift-1021)) stands in for a weight
+// that no digit of W = 2^shift · w keeps and that a sum of weights holding
+// the row's heaviest one (2^shift) absorbs. A NaN argument gives a finite
+// value, for callers that select another one for it.
+__device__ __forceinline__ double exp_weight(double x, const double* __restrict__ table, int shift) {
+  x = fmin(fmax(x, -708.0), 709.0);
+  const double t = fma(x, k64OverLn2, 6755399441055744.0);
+  const double kf = t - 6755399441055744.0;
+  const int k = __double2loint(t);
+  double r = fma(-kf, kLn2Over64Hi, x);
+  r = fma(-kf, kLn2Over64Lo, r);
+  double p = fma(r, 1.0 / 120.0, 1.0 / 24.0);
+  p = fma(p, r, 1.0 / 6.0);
+  p = fma(p, r, 0.5);
+  p = fma(p, r, 1.0);
+  p = fma(p, r, 1.0);
+  return p * table[k & 63] * ptx::pow2((k >> 6) + shift);
+}
+
 }  // namespace ef

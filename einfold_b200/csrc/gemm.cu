@@ -19,6 +19,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <climits>
 #include <mutex>
 #include <type_traits>
 
@@ -692,6 +693,28 @@ void split_gemm(Context& ctx, const double* a, const double* b, bool b_natural, 
     return;
   }
   dispatch_slices(slices, [&](auto S) { split_gemm_s<decltype(S)::value>(ctx, a, b, b_natural, c, batches, m, n, k, stream); });
+}
+
+__global__ void exponent_range_kernel(const int32_t* __restrict__ e, int64_t n, int* __restrict__ out) {
+  int hi = INT_MIN, lo = INT_MIN;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    hi = max(hi, e[i]);
+    lo = max(lo, -e[i]);
+  }
+  for (int o = 16; o; o >>= 1) {
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    lo = max(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(out, hi);
+    atomicMax(out + 1, lo);
+  }
+}
+
+void exponent_range(const int32_t* e, int64_t n, int* out, cudaStream_t stream) {
+  if (n <= 0) return;
+  exponent_range_kernel<<<blocks_for((uint64_t)n, 256), 256, 0, stream>>>(e, n, out);
+  EF_LAUNCH_CHECK();
 }
 
 void slice_rows_into(int S, const double* x, int64_t batches, int64_t rows, int64_t k, int64_t ld, int64_t rows_pad,

@@ -46,6 +46,9 @@ void slice_rows_into(int S, const double* x, int64_t batches, int64_t rows, int6
 // colmax is scratch of batches·n words.
 void slice_cols_into(int S, const double* x, int64_t batches, int64_t k, int64_t n, int64_t n_pad, int64_t k_pad,
                      unsigned long long* colmax, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream);
+// out[0] = max e[i] and out[1] = max -e[i] over n exponents, folded into
+// what out already holds (INT_MIN for a fresh pair).
+void exponent_range(const int32_t* e, int64_t n, int* out, cudaStream_t stream);
 // A TMA map over digit planes [planes][rows][k_pad] (uint8), boxes of 64
 // bytes of k by box_rows rows by box_planes planes, 64-byte swizzle.
 CUtensorMap digit_planes_map(const int8_t* digits, int64_t k_pad, int64_t rows, int64_t planes, int box_rows,
