@@ -26,23 +26,39 @@ constexpr int64_t kNoGroup = -1;
 
 // Scatters a's rows into a[x][z]; `held` packs a 2-bit code per cell (0
 // absent, 1 NULL factor, 2 valued), 16 cells a word, so that a repeated
-// position shows in the bits an atomic OR returns.
+// position shows in the bits an atomic OR returns. The lanes of a warp that
+// share a word OR their codes together first and one of them issues the
+// atomic (rows in key order share words). Every thread of a block runs the same iterations,
+// so the warp-wide matches see all the warp's rows.
 __global__ void scatter_a_kernel(Role xs, Role zs, int64_t rows, const double* __restrict__ vals,
                                  const uint8_t* __restrict__ valid, int64_t nz, double* __restrict__ a,
                                  uint32_t* __restrict__ held, uint8_t* __restrict__ reached,
                                  uint8_t* __restrict__ valued, unsigned* flags) {
   unsigned f = 0;
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < rows; base += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = base + threadIdx.x;
+    const unsigned active = __ballot_sync(0xffffffffu, r < rows);
+    if (r >= rows) continue;
     const int64_t x = role_position(xs, r), z = role_position(zs, r);
     const int64_t p = x * nz + z;
     const bool v = valid ? valid[r] != 0 : true;
     const unsigned sh = (unsigned)(p & 15) * 2;
-    if ((atomicOr(&held[p >> 4], (v ? 2u : 1u) << sh) >> sh) & 3u) f |= F_DUP_A;
-    reached[x] = 1;
+    const unsigned long long word = (unsigned long long)(p >> 4);
+    const unsigned same_word = __match_any_sync(active, word);
+    const unsigned bits = __reduce_or_sync(same_word, (v ? 2u : 1u) << sh);
+    // A cell twice in the warp leaves fewer distinct cells than lanes.
+    if (__popc(__reduce_or_sync(same_word, 1u << (p & 15))) != __popc(same_word)) f |= F_DUP_A;
+    const int leader = __ffs(same_word) - 1;
+    unsigned old = 0;
+    if (lane == leader) old = atomicOr(&held[word], bits);
+    old = __shfl_sync(same_word, old, leader);
+    if ((old >> sh) & 3u) f |= F_DUP_A;
+    if (!reached[x]) reached[x] = 1;
     if (v) {
       const double val = vals[r];
       a[p] = val;
-      valued[x] = 1;
+      if (!valued[x]) valued[x] = 1;
       if (!isfinite(val)) f |= F_NONFINITE_A;
     }
   }
@@ -50,14 +66,29 @@ __global__ void scatter_a_kernel(Role xs, Role zs, int64_t rows, const double* _
 }
 
 // Scatters b's rows into b[w][z][y] (its natural layout: each row of b's
-// matrix contiguous); `present` packs a bit per cell.
+// matrix contiguous); `present` packs a bit per cell, ORed per word across
+// the warp's lanes first as in scatter_a_kernel.
 __global__ void scatter_b_kernel(Role wzs, Role ys, int64_t rows, const double* __restrict__ vals,
                                  const uint8_t* __restrict__ valid, int64_t ny, double* __restrict__ bm,
                                  uint32_t* __restrict__ present, unsigned* flags) {
   unsigned f = 0;
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < rows; base += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = base + threadIdx.x;
+    const unsigned active = __ballot_sync(0xffffffffu, r < rows);
+    if (r >= rows) continue;
     const int64_t p = role_position(wzs, r) * ny + role_position(ys, r);
-    if (atomicOr(&present[p >> 5], 1u << (p & 31)) & (1u << (p & 31))) f |= F_DUP_B;
+    const unsigned bit = 1u << (p & 31);
+    const unsigned long long word = (unsigned long long)(p >> 5);
+    const unsigned same_word = __match_any_sync(active, word);
+    const unsigned bits = __reduce_or_sync(same_word, bit);
+    // A cell twice in the warp leaves fewer distinct bits than lanes.
+    if (__popc(bits) != __popc(same_word)) f |= F_DUP_B;
+    const int leader = __ffs(same_word) - 1;
+    unsigned old = 0;
+    if (lane == leader) old = atomicOr(&present[word], bits);
+    old = __shfl_sync(same_word, old, leader);
+    if (old & bit) f |= F_DUP_B;
     if (!valid || valid[r]) {
       const double val = vals[r];
       bm[p] = val;
@@ -446,8 +477,10 @@ FoldOutput dense_fold(Context& ctx, const FoldD& f, const Relation& a, const Rel
   ctx.kernels += 2;
   DeviceBuffer<uint8_t> sel;
   DeviceBuffer<int64_t> pos, row_index;
-  const dim3 grid2((unsigned)std::max<uint64_t>(1, std::min<uint64_t>((ny + 255) / 256, 64)),
-                   (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(nx, 65535)));
+  // Blocks of 256 cells of a row, each block walking rows x, x + gridDim.y,
+  // ... (about 16 blocks an SM).
+  const uint64_t gx = std::min<uint64_t>(std::max<uint64_t>((ny + 255) / 256, 1), 64);
+  const dim3 grid2((unsigned)gx, (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(nx, 148 * 16 / gx)));
   int64_t n_out;
   if (conds.n) {
     sel.allocate((size_t)(cells_n ? cells_n : 1), s);
