@@ -143,7 +143,9 @@ void einfold_context_destroy(einfold_context* ctx) {
   {
     ef::DeviceGuard dev(ctx->device);
     if (ctx->stream) {
+      ctx->kept.release(ctx->stream);
       cudaStreamSynchronize(ctx->stream);
+      ef::device_cache_forget(ctx->stream);
       cudaStreamDestroy(ctx->stream);
     }
   }

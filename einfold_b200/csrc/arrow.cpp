@@ -138,12 +138,19 @@ void Buffer::reset() {
       int old = -1;
       cudaGetDevice(&old);
       cudaSetDevice(device);
-      cudaFree(ptr);
+      if (capacity) {
+        // As cudaFree would: the block is free once every stream is done.
+        cudaDeviceSynchronize();
+        device_free_synchronized(ptr, capacity, device);
+      } else {
+        cudaFree(ptr);
+      }
       if (old >= 0) cudaSetDevice(old);
     }
   }
   ptr = nullptr;
   bytes = 0;
+  capacity = 0;
 }
 
 int64_t Column::nulls() const {

@@ -122,20 +122,25 @@ struct HostBuffer {
   template <class T> T* as() const { return (T*)ptr; }
 };
 
-// A result buffer: host memory (malloc) or device memory (cudaFree on `device`).
+// A result buffer: host memory (malloc) or device memory on `device`
+// (a device_alloc block of `capacity` bytes, returned to the block cache
+// after a device synchronization; cudaFree when capacity is 0).
 struct Buffer {
   void* ptr = nullptr;
   size_t bytes = 0;
   int device = -1;
+  size_t capacity = 0;
   Buffer() = default;
   // device -1: host memory (malloc); -2: a page-locked block (pinned_acquire).
   Buffer(HostBuffer&& h) : ptr(h.ptr), bytes(h.bytes), device(h.pinned ? -2 : -1) { h.ptr = nullptr; h.bytes = 0; }
   Buffer(const Buffer&) = delete;
-  Buffer(Buffer&& o) noexcept : ptr(o.ptr), bytes(o.bytes), device(o.device) { o.ptr = nullptr; o.bytes = 0; }
+  Buffer(Buffer&& o) noexcept : ptr(o.ptr), bytes(o.bytes), device(o.device), capacity(o.capacity) {
+    o.ptr = nullptr; o.bytes = 0; o.capacity = 0;
+  }
   Buffer& operator=(Buffer&& o) noexcept {
     reset();
-    ptr = o.ptr; bytes = o.bytes; device = o.device;
-    o.ptr = nullptr; o.bytes = 0;
+    ptr = o.ptr; bytes = o.bytes; device = o.device; capacity = o.capacity;
+    o.ptr = nullptr; o.bytes = 0; o.capacity = 0;
     return *this;
   }
   void reset();

@@ -84,7 +84,19 @@ struct GradArgs {
   double* out;  // [w·lr + r][dy]
   int* status;
   unsigned long long* tiles;
+  int w0;  // the first batch of this launch (blockIdx.y counts from it)
+  // The d_k kernel's exports for the tile kernels (null: none), indexed by
+  // the launch's own batches: P's digit tiles as the d_v kernel cuts them,
+  // [batch][row block][column tile][S][128 rows][64 B] in the MMA's 64-byte
+  // swizzle, with their rows' powers of two [tile][128]; and dS, query-major,
+  // [batch][lq_pad][lk_pad].
+  uint8_t* p_tiles;
+  int32_t* p_exp;
+  double* ds_out;
+  int64_t n_rb, n_ct;  // row blocks and column tiles of a batch
 };
+
+constexpr int kPTile = S * GM * 64;  // bytes of one tile of weight digits
 
 // FAST: every pair of row and column exponents of products 1 and 2 sums to
 // a normal double's power of two.
@@ -120,11 +132,12 @@ __global__ void __launch_bounds__(kGradThreads, 1)
   int* row_hi = row_lo + GM;
   int* e3_s = row_hi + GM;               // [64]
   double* texp = (double*)(aux + 2048);  // [64]
-  double* red = (double*)(aux + 4096);   // [4][128]
+  int* red = (int*)(aux + 4096);         // [4][128] the quarters' exponents
+  int* redp = (int*)(aux + 6144);        // [4][128] the same for P (d_k's export)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int rt = (int)(gridDim.x - 1 - blockIdx.x);
-  const int w = blockIdx.y;
+  const int w = a.w0 + (int)blockIdx.y;
   const int64_t r_base = (int64_t)w * a.lr, c_base = (int64_t)w * a.lc;
 
   if (threadIdx.x == 0) {
@@ -323,9 +336,44 @@ __global__ void __launch_bounds__(kGradThreads, 1)
         }
       }
       if (kTwo) {
+        // d_k's export of dS: column c (a query) of this tile, the rows' keys contiguous.
+        double* ds_col = (MODE == GRAD_K && a.ds_out)
+                             ? a.ds_out + ((int64_t)blockIdx.y * a.lc_pad + cl0) * a.lr_pad + (int64_t)rt * GM + r
+                             : nullptr;
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(t1_free);
+        if (MODE == GRAD_K && a.p_tiles) {
+          // While d_out·v runs: P's digits for the d_v tile kernel, cut as
+          // that kernel's own epilogue would (W = p · 2^(8S - ep), ep the
+          // row's exponent over these 64 columns), stored as swizzled rows.
+          double mp = 0.0;
+#pragma unroll
+          for (int c = 0; c < CW; c++) mp = fmax(mp, wv[c]);
+          redp[h * GM + r] = mp > 0.0 ? slice_exponent(mp) : INT_MIN;
+          named_bar(2 + quarter, 128);
+          int ep = max(max(redp[r], redp[GM + r]), max(redp[2 * GM + r], redp[3 * GM + r]));
+          ep = ep == INT_MIN ? 0 : ep;
+          const int shift = 8 * S - ep;
+          const double f1 = pow2(shift >> 1), f2 = pow2(shift - (shift >> 1));
+          const int64_t tile = ((int64_t)blockIdx.y * a.n_rb + rt) * a.n_ct + (ct0 + it);
+          uint8_t* dst = a.p_tiles + tile * kPTile + sw64_offset((uint32_t)r, (uint32_t)(h * CW));
+          uint32_t chunk[S][4];
+#pragma unroll
+          for (int c4 = 0; c4 < CW / 4; c4++) {
+            double x[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) x[i] = wv[c4 * 4 + i] * f1 * f2;
+            uint32_t planes[S];
+            digit_planes4<S>(x, planes);
+#pragma unroll
+            for (int s = 0; s < S; s++) chunk[s][c4] = planes[s];
+          }
+#pragma unroll
+          for (int s = 0; s < S; s++)
+            *(uint4*)(dst + s * GM * 64) = make_uint4(chunk[s][0], chunk[s][1], chunk[s][2], chunk[s][3]);
+          if (h == 0) a.p_exp[tile * GM + r] = ep;
+        }
         wait(s2_full, par);
         tc_fence_after();
 #pragma unroll
@@ -341,6 +389,7 @@ __global__ void __launch_bounds__(kGradThreads, 1)
             const double dp = FAST ? l * pow2(e2r + es[GJ + c]) : scale2(l, e2r + es[GJ + c]);
             const double t = wv[c] * (dp - (MODE == GRAD_Q ? dd_r : ls[GJ + c]));
             wv[c] = wv[c] != 0.0 ? t : 0.0;
+            if (ds_col) ds_col[(int64_t)c * a.lr_pad] = wv[c];
           }
         }
       }
@@ -348,9 +397,10 @@ __global__ void __launch_bounds__(kGradThreads, 1)
       double mx = 0.0;
 #pragma unroll
       for (int c = 0; c < CW; c++) mx = fmax(mx, fabs(wv[c]));
-      red[h * GM + r] = mx;
+      red[h * GM + r] = mx > 0.0 ? slice_exponent(mx) : INT_MIN;
       named_bar(2 + quarter, 128);
-      const int ew = slice_exponent(fmax(fmax(red[r], red[GM + r]), fmax(red[2 * GM + r], red[3 * GM + r])));
+      int ew = max(max(red[r], red[GM + r]), max(red[2 * GM + r], red[3 * GM + r]));
+      ew = ew == INT_MIN ? 0 : ew;
       // The weights' digits: W = w · 2^(8S - ew), |W| < 2^(8S-2), the power
       // of two applied in two exact halves (8S - ew lies in [-978, 1119]).
       const int shift = 8 * S - ew;
@@ -405,6 +455,299 @@ __global__ void __launch_bounds__(kGradThreads, 1)
     }
     // Every lane of the warp reads TMEM (the loads are warp-wide); the rows
     // past the batch's end write nothing.
+    tc_fence_after();
+    const bool store = valid && !*(volatile int*)failed;
+    double* orow = a.out + (r_base + rl) * a.dy;
+#pragma unroll
+    for (int c4 = 0; c4 < CW / 4; c4++) {
+      uint32_t sum[8];
+      if (n_tiles > 0) {
+        tmem_ld8(sum_addr + c4 * 8, (int32_t*)sum);
+        tmem_wait_ld();
+      }
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int64_t y = (int64_t)a.y0 + h * CW + c4 * 4 + i;
+        const double v = n_tiles > 0 ? __hiloint2double((int)sum[2 * i + 1], (int)sum[2 * i]) : 0.0;
+        if (store && y < a.dy) orow[y] = a.out_factor * v;
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+// The d_v and d_q tiles from the weights the d_k kernel exported: one
+// product a tile (the weights' digits against the columns' B3 digits) and
+// the rows' sums, with no scores, exponentials or d_out·v recomputed. d_v
+// reads P's digit tiles and their rows' powers of two as they are; d_q reads
+// dS (query-major, four 128-byte-swizzled boxes of 16 keys a tile), applies
+// the mask and cuts its digits under the row's power of two over the tile,
+// as grad_split's epilogue does, so that both gradients come out with the
+// same bits as there.
+template <int MODE>
+struct TileShape {
+  static constexpr bool kQ = MODE == GRAD_Q;
+  static constexpr int kDs = kQ ? GM * GJ * 8 : 0;  // one dS tile
+  static constexpr int kBufs = kQ ? 1 : 2;          // weight digit tiles (d_v: one a stage)
+  static constexpr int kB3 = S * GY * 64;
+  static constexpr int kStage = kB3 + (kQ ? 0 : 1024);  // B3, and for d_v the rows' exponents
+  static constexpr int kAux = 8192;
+  static constexpr int kSmem = kDs + kBufs * kPTile + 2 * kStage + kAux + 1024;
+  static_assert(kSmem <= kMaxSmem, "the tiles must fit in shared memory");
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(kGradThreads, 1)
+    grad_tiles(const __grid_constant__ CUtensorMap tds, const __grid_constant__ CUtensorMap tb3, const GradArgs a) {
+  using Sh = TileShape<MODE>;
+  constexpr bool kQ = Sh::kQ;
+  constexpr int CW = 16;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t* sDs = smem;
+  uint8_t* sP = sDs + Sh::kDs;
+  uint8_t* sB = sP + Sh::kBufs * kPTile;  // 2 stages of [B3 | rows' exponents]
+  uint8_t* aux = sB + 2 * Sh::kStage;
+  uint64_t* bars = (uint64_t*)aux;
+  uint64_t* kv_full = bars + 0;   // [2]
+  uint64_t* kv_empty = bars + 2;  // [2]
+  uint64_t* ds_empty = bars + 4;
+  uint64_t* p_full = bars + 5;
+  uint64_t* o_full = bars + 6;
+  uint64_t* tmem_free = bars + 7;
+  uint32_t* tmem_slot = (uint32_t*)(bars + 16);
+  int* failed = (int*)(tmem_slot + 1);
+  long long* span = (long long*)(tmem_slot + 4);
+  int* row_lo = (int*)(aux + 256);
+  int* row_hi = row_lo + GM;
+  int* e3_s = row_hi + GM;        // [64]
+  int* red = (int*)(aux + 4096);  // [4][128]
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int rt = (int)(gridDim.x - 1 - blockIdx.x);
+  const int w = a.w0 + (int)blockIdx.y;
+  const int64_t r_base = (int64_t)w * a.lr, c_base = (int64_t)w * a.lc;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 2; i++) {
+      mbar_init(&kv_full[i], 1);
+      // d_v: the MMAs' commit and every epilogue warp (which reads the
+      // stage's exponents) free a stage.
+      mbar_init(&kv_empty[i], kQ ? 1 : 1 + kEpi / 32);
+    }
+    mbar_init(ds_empty, kEpi / 32);
+    mbar_init(p_full, kEpi / 32);
+    mbar_init(o_full, 1);
+    mbar_init(tmem_free, kEpi / 32);
+    *failed = 0;
+    span[0] = LLONG_MAX;
+    span[1] = LLONG_MIN;
+    mbar_fence_init();
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (threadIdx.x < GM) {
+    const int64_t rl = (int64_t)rt * GM + threadIdx.x;
+    int lo = 0, hi = 0;
+    if (rl < a.lr) {
+      int64_t l, h;
+      allowed(a.mask, r_base + rl, l, h);
+      lo = (int)(l - c_base);
+      hi = (int)(h - c_base);
+      if (lo < hi) {
+        atomicMin(&span[0], (long long)lo);
+        atomicMax(&span[1], (long long)hi);
+      }
+    }
+    row_lo[threadIdx.x] = lo;
+    row_hi[threadIdx.x] = hi;
+  } else if (threadIdx.x < GM + GY) {
+    const int c = threadIdx.x - GM;
+    e3_s[c] = a.y0 + c < a.dy_pad ? a.e_b3[(int64_t)w * a.dy_pad + a.y0 + c] : 0;
+  }
+  __syncthreads();
+  const uint32_t tmem = *tmem_slot;
+  const long long first = span[0], last = span[1];
+  const int ct0 = first < last ? (int)(first / GJ) : 0;
+  const int n_tiles = first < last ? (int)((last + GJ - 1) / GJ) - ct0 : 0;
+  if (threadIdx.x == 0 && n_tiles > 0) atomicAdd(a.tiles, (unsigned long long)n_tiles);
+  auto tile_of = [&](int it) { return ((int64_t)blockIdx.y * a.n_rb + rt) * a.n_ct + (ct0 + it); };
+
+  if (warp == 0) {
+    if (lane == 0 && n_tiles > 0) {
+      prefetch_map(&tb3);
+      if (kQ) prefetch_map(&tds);
+      int issued = 0;
+      for (int it = 0; it < n_tiles; it++) {
+        const int st = it & 1;
+        const uint32_t round = (uint32_t)(it >> 1);
+        if (*(volatile int*)failed) break;
+        if (!mbar_wait(&kv_empty[st], (round & 1) ^ 1) || (kQ && it > 0 && !mbar_wait(ds_empty, (uint32_t)((it - 1) & 1)))) {
+          atomicOr(a.status, 2);
+          *(volatile int*)failed = 1;
+          break;
+        }
+        const int cl0 = (ct0 + it) * GJ;
+        uint8_t* stage = sB + st * Sh::kStage;
+        mbar_expect_tx(&kv_full[st], (uint32_t)(Sh::kB3 + (kQ ? Sh::kDs : kPTile + GM * 4)));
+        tma_load_3d(stage, &tb3, &kv_full[st], cl0, a.y0, w * S);
+        if (kQ) {
+          for (int j = 0; j < 4; j++)
+            tma_load_3d(sDs + j * GM * 128, &tds, &kv_full[st], cl0 + 16 * j, rt * GM, (int)blockIdx.y);
+        } else {
+          bulk_load(sP + st * kPTile, a.p_tiles + tile_of(it) * kPTile, kPTile, &kv_full[st]);
+          bulk_load(stage + Sh::kB3, a.p_exp + tile_of(it) * GM, GM * 4, &kv_full[st]);
+        }
+        issued = it + 1;
+      }
+      for (int it = std::max(0, issued - 2); it < issued; it++) mbar_wait(&kv_full[it & 1], (uint32_t)((it >> 1) & 1));
+    }
+  } else if (warp == 1) {
+    if (lane == 0 && n_tiles > 0) {
+      int last = -1;  // the last tile whose MMAs were committed
+      bool ok = true;
+      for (int it = 0; ok && it < n_tiles; it++) {
+        const int st = it & 1;
+        const uint32_t par = (uint32_t)(it & 1);
+        ok = mbar_wait(&kv_full[st], (uint32_t)((it >> 1) & 1)) && (it == 0 || mbar_wait(tmem_free, par ^ 1)) &&
+             (!kQ || mbar_wait(p_full, par));
+        if (!ok || *(volatile int*)failed) break;
+        tc_fence_after();
+        const uint32_t a_base = smem_u32(sP + (kQ ? 0 : st * kPTile)), b_base = smem_u32(sB + st * Sh::kStage);
+#pragma unroll
+        for (int kk = 0; kk < 2; kk++)
+#pragma unroll
+          for (int s = 1; s <= S; s++) {
+            const int total = (S + 1 - s) * GY;
+#pragma unroll
+            for (int nn0 = 0; nn0 < total; nn0 += 256) {
+              const int nn = total - nn0 < 256 ? total - nn0 : 256;
+              umma_i8(tmem + (uint32_t)((s - 1) * GY + nn0), desc_sw64(a_base + (s - 1) * GM * 64 + kk * 32),
+                      desc_sw64(b_base + nn0 * 64 + kk * 32), idesc_i8(GM, nn), (kk > 0 || s > 1) ? 1u : 0u);
+            }
+          }
+        umma_commit(o_full);
+        umma_commit(&kv_empty[st]);
+        last = it;
+      }
+      if (!ok) {
+        atomicOr(a.status, 2);
+        *(volatile int*)failed = 1;
+      }
+      // MMAs still running complete before TMEM is freed.
+      if (last >= 0) mbar_wait(o_full, (uint32_t)(last & 1));
+    }
+  } else {
+    const int h = (warp - 2) >> 2;
+    const int quarter = warp & 3;
+    const int r = quarter * 32 + lane;
+    const int64_t rl = (int64_t)rt * GM + r;
+    const bool valid = rl < a.lr;
+    const int lo = row_lo[r], hi = row_hi[r];
+    const unsigned span_r = (valid && lo < hi) ? (unsigned)(hi - lo) : 0u;
+    const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
+    const uint32_t sum_addr = lane_addr + (uint32_t)(kSumCol + h * 2 * CW);
+    int e3lo = INT_MAX, e3hi = INT_MIN;
+    for (int c = 0; c < GY; c++) {
+      e3lo = min(e3lo, e3_s[c]);
+      e3hi = max(e3hi, e3_s[c]);
+    }
+    auto wait = [&](uint64_t* bar, uint32_t parity) {
+      if (*(volatile int*)failed) return;
+      if (!mbar_wait(bar, parity)) {
+        *(volatile int*)failed = 1;
+        atomicOr(a.status, 2);
+      }
+    };
+    for (int it = 0; it < n_tiles; it++) {
+      const int st = it & 1;
+      const uint32_t par = (uint32_t)(it & 1);
+      wait(&kv_full[st], (uint32_t)((it >> 1) & 1));
+      int ew;
+      if (kQ) {
+        // This row's 16 keys of the tile: box h, 128-byte row r, its 16-byte
+        // chunks permuted by r mod 8.
+        const uint8_t* row = sDs + h * GM * 128 + r * 128;
+        const int off = (ct0 + it) * GJ + h * CW - lo;
+        double wv[CW];
+#pragma unroll
+        for (int j = 0; j < CW / 2; j++) {
+          const double2 v = *(const double2*)(row + ((j ^ (r & 7)) << 4));
+          wv[2 * j] = (unsigned)(off + 2 * j) < span_r ? v.x : 0.0;
+          wv[2 * j + 1] = (unsigned)(off + 2 * j + 1) < span_r ? v.y : 0.0;
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(ds_empty);
+        double mx = 0.0;
+#pragma unroll
+        for (int c = 0; c < CW; c++) mx = fmax(mx, fabs(wv[c]));
+        red[h * GM + r] = mx > 0.0 ? slice_exponent(mx) : INT_MIN;
+        named_bar(2 + quarter, 128);
+        ew = max(max(red[r], red[GM + r]), max(red[2 * GM + r], red[3 * GM + r]));
+        ew = ew == INT_MIN ? 0 : ew;
+        const int shift = 8 * S - ew;
+        const double f1 = pow2(shift >> 1), f2 = pow2(shift - (shift >> 1));
+        uint8_t* prow = sP + r * 64;
+#pragma unroll
+        for (int c4 = 0; c4 < CW / 4; c4++) {
+          double x[4];
+#pragma unroll
+          for (int i = 0; i < 4; i++) x[i] = wv[c4 * 4 + i] * f1 * f2;
+          uint32_t planes[S];
+          digit_planes4<S>(x, planes);
+          const uint32_t off4 = sw64_offset((uint32_t)r, (uint32_t)(h * CW + c4 * 4)) - (uint32_t)r * 64;
+#pragma unroll
+          for (int s = 0; s < S; s++) *(uint32_t*)(prow + s * GM * 64 + off4) = planes[s];
+        }
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(p_full);
+      } else {
+        ew = ((const int*)(sB + st * Sh::kStage + Sh::kB3))[r];
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&kv_empty[st]);
+      }
+      wait(o_full, par);
+      tc_fence_after();
+      // sums += this tile's levels · 2^(ew + e3), as in grad_split.
+      auto add_levels = [&](auto normal) {
+#pragma unroll
+        for (int c4 = 0; c4 < CW / 4; c4++) {
+          int32_t L[S][4];
+#pragma unroll
+          for (int l = 0; l < S; l++) tmem_ld4(lane_addr + (uint32_t)(l * GY + h * CW + c4 * 4), L[l]);
+          uint32_t sum[8];
+          if (it > 0) tmem_ld8(sum_addr + c4 * 8, (int32_t*)sum);
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            const int e = ew + e3_s[h * CW + c4 * 4 + i];
+            const double prev = it > 0 ? __hiloint2double((int)sum[2 * i + 1], (int)sum[2 * i]) : 0.0;
+            const double l = combine_levels_small<S, 4>(L, i);
+            const double v = decltype(normal)::value ? fma(l, pow2(e), prev) : prev + scale2(l, e);
+            sum[2 * i] = (uint32_t)__double2loint(v);
+            sum[2 * i + 1] = (uint32_t)__double2hiint(v);
+          }
+          tmem_st8(sum_addr + c4 * 8, sum);
+        }
+      };
+      if (__all_sync(0xffffffffu, ew + e3lo >= -1022 && ew + e3hi <= 1023)) add_levels(std::true_type{});
+      else add_levels(std::false_type{});
+      tmem_wait_st();
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tmem_free);
+    }
     tc_fence_after();
     const bool store = valid && !*(volatile int*)failed;
     double* orow = a.out + (r_base + rl) * a.dy;
@@ -597,6 +940,15 @@ void launch_split(const CUtensorMap* maps, const GradArgs& args, dim3 grid, bool
   EF_LAUNCH_CHECK();
 }
 
+template <int MODE>
+void launch_tiles(const CUtensorMap& tds, const CUtensorMap& tb3, const GradArgs& args, dim3 grid,
+                  cudaStream_t stream) {
+  using Sh = TileShape<MODE>;
+  EF_CUDA(cudaFuncSetAttribute(grad_tiles<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::kSmem));
+  grad_tiles<MODE><<<grid, kGradThreads, Sh::kSmem, stream>>>(tds, tb3, args);
+  EF_LAUNCH_CHECK();
+}
+
 // dst[w][x] = src[w·l + x] for x < l, 0 up to l_pad.
 __global__ void pad_rows(const double* __restrict__ src, int64_t batches, int64_t l, int64_t l_pad,
                          double* __restrict__ dst) {
@@ -678,15 +1030,14 @@ bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd,
     return digit_planes_map(x.d, 64, rows_pad, W * S, box, S);
   };
   auto cols_map = [&](const Digits& x, int64_t k_pad) { return digit_planes_map(x.d, k_pad, 64, W * S, GY, S); };
-  cudaEvent_t e0, e1;
-  EF_CUDA(cudaEventCreate(&e0));
-  EF_CUDA(cudaEventCreate(&e1));
-  EF_CUDA(cudaEventRecord(e0, s));
   const Mask keys_mask = transposed(f.mask);
   const double* table = exp_table(ctx.device);
+  GradArgs args[3];
+  CUtensorMap mode_maps[3][5];
   for (int mode = 0; mode < 3; mode++) {
-    GradArgs a{};
-    CUtensorMap maps[5];
+    GradArgs& a = args[mode];
+    a = GradArgs{};
+    CUtensorMap* maps = mode_maps[mode];
     const bool keys = mode != GRAD_Q;
     a.mask = keys ? keys_mask : f.mask;
     a.lr = keys ? lk : lq;
@@ -744,11 +1095,53 @@ bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd,
     }
     a.dy_pad = 64;
     a.y0 = 0;
-    const dim3 grid((unsigned)(a.lr_pad / GM), (unsigned)W);
-    if (mode == GRAD_V) launch_split<GRAD_V>(maps, a, grid, fast, s);
-    else if (mode == GRAD_K) launch_split<GRAD_K>(maps, a, grid, fast, s);
-    else launch_split<GRAD_Q>(maps, a, grid, fast, s);
-    ctx.kernels++;
+    a.n_rb = a.lr_pad / GM;
+    a.n_ct = a.lc_pad / GJ;
+  }
+  // The tile path, while its exports fit in half the free memory (in chunks
+  // of batches): d_k first, exporting P's digits and dS; then d_v and d_q
+  // from them, one product a tile each. Otherwise the three kernels each
+  // recompute the scores.
+  const int64_t n_kb = lk_pad / GM, n_qt = lq_pad / GJ;
+  const size_t p_bytes = al((size_t)(lk_pad * lq_pad * S)), ds_bytes = al((size_t)(lk_pad * lq_pad) * 8),
+               pe_bytes = al((size_t)(n_kb * n_qt * GM) * 4);
+  const size_t per_batch = p_bytes + ds_bytes + pe_bytes;
+  // Free memory is asked only when the kept exports are too small.
+  int64_t chunk = W;
+  if (ctx.kept.bytes < (size_t)W * per_batch) {
+    size_t free_b = 0, total_b = 0;
+    EF_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    chunk = std::min<int64_t>(W, (int64_t)((free_b / 2 + ctx.kept.bytes) / per_batch));
+  }
+  uint8_t* p_tiles = chunk >= 1 ? (uint8_t*)ctx.kept.get((size_t)chunk * per_batch, s) : nullptr;
+  cudaEvent_t e0, e1;
+  EF_CUDA(cudaEventCreate(&e0));
+  EF_CUDA(cudaEventCreate(&e1));
+  EF_CUDA(cudaEventRecord(e0, s));
+  if (chunk >= 1) {
+    double* ds = (double*)(p_tiles + (size_t)chunk * p_bytes);
+    int32_t* p_exp = (int32_t*)((uint8_t*)ds + (size_t)chunk * ds_bytes);
+    const CUtensorMap tds = f64_boxes_map(ds, lk_pad, lq_pad, chunk, 16, GM);
+    for (int64_t w0 = 0; w0 < W; w0 += chunk) {
+      const unsigned wc = (unsigned)std::min<int64_t>(chunk, W - w0);
+      GradArgs k = args[GRAD_K], v = args[GRAD_V], q = args[GRAD_Q];
+      k.w0 = v.w0 = q.w0 = (int)w0;
+      k.p_tiles = v.p_tiles = p_tiles;
+      k.p_exp = v.p_exp = p_exp;
+      k.ds_out = ds;
+      launch_split<GRAD_K>(mode_maps[GRAD_K], k, dim3((unsigned)n_kb, wc), fast, s);
+      launch_tiles<GRAD_V>(tds, mode_maps[GRAD_V][4], v, dim3((unsigned)n_kb, wc), s);
+      launch_tiles<GRAD_Q>(tds, mode_maps[GRAD_Q][4], q, dim3((unsigned)(lq_pad / GM), wc), s);
+      ctx.kernels += 3;
+    }
+  } else {
+    for (int mode = 0; mode < 3; mode++) {
+      const dim3 grid((unsigned)(args[mode].lr_pad / GM), (unsigned)W);
+      if (mode == GRAD_V) launch_split<GRAD_V>(mode_maps[mode], args[mode], grid, fast, s);
+      else if (mode == GRAD_K) launch_split<GRAD_K>(mode_maps[mode], args[mode], grid, fast, s);
+      else launch_split<GRAD_Q>(mode_maps[mode], args[mode], grid, fast, s);
+      ctx.kernels++;
+    }
   }
   EF_CUDA(cudaEventRecord(e1, s));
   unsigned long long pairs[3] = {};
@@ -761,10 +1154,12 @@ bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd,
   cudaEventDestroy(e1);
   if (st & 2) fail(EINFOLD_TIMEOUT, "a bounded wait in the attention backward ran out");
   // Digit products executed: per pair of tiles, S(S+1)/2 digit pairs of a
-  // 128 x 64 x 64 product, two of them for d_v and three for d_k and d_q.
+  // 128 x 64 x 64 product, three for d_k, and for d_v and d_q one on the
+  // tile path (else two and three).
   ctx.product_ms += ms;
   const double per = (S * (S + 1) / 2) * 2.0 * GM * GJ * 64;
-  ctx.product_ops += per * (2.0 * (double)pairs[0] + 3.0 * (double)(pairs[1] + pairs[2]));
+  const double pv = chunk >= 1 ? 1.0 : 2.0, pq = chunk >= 1 ? 1.0 : 3.0;
+  ctx.product_ops += per * (pv * (double)pairs[0] + 3.0 * (double)pairs[1] + pq * (double)pairs[2]);
   ctx.phase("attention backward: tiles");
   return true;
 }

@@ -87,8 +87,19 @@ inline bool checked_mul(uint64_t a, uint64_t b, uint64_t* out) {
 
 struct Context;
 
-// A device allocation from the context's stream-ordered pool, freed on the
-// same stream when it goes out of scope.
+// Device scratch through a process-wide cache of freed blocks keyed by
+// stream, device and size class: a block freed on a stream is reused in
+// stream order on it; one freed after a device synchronization on any
+// stream of its device. Misses go to the stream-ordered pool.
+void* device_alloc(size_t bytes, cudaStream_t s);
+void device_free(void* p, size_t bytes, cudaStream_t s);
+void device_free_synchronized(void* p, size_t bytes, int device);
+// Hands a stream's cached blocks over to any stream (the stream is about
+// to be destroyed, its work done).
+void device_cache_forget(cudaStream_t s);
+
+// A device allocation (device_alloc), freed on the same stream when it goes
+// out of scope.
 template <class T>
 struct DeviceBuffer {
   T* ptr = nullptr;
@@ -109,13 +120,13 @@ struct DeviceBuffer {
     reset();
     stream = s;
     count = n;
-    if (n) EF_CUDA(cudaMallocAsync((void**)&ptr, n * sizeof(T), s));
+    if (n) ptr = (T*)device_alloc(n * sizeof(T), s);
   }
   void zero() {
     if (count) EF_CUDA(cudaMemsetAsync(ptr, 0, count * sizeof(T), stream));
   }
   void reset() {
-    if (ptr) cudaFreeAsync(ptr, stream);
+    if (ptr) device_free(ptr, count * sizeof(T), stream);
     ptr = nullptr;
     count = 0;
   }
@@ -143,6 +154,27 @@ struct PinnedArena {
   }
 };
 
+// Device scratch kept across calls: grown on demand (stream-ordered),
+// freed with the context. Calls that use it end synchronized, so the next
+// call may reuse it on any stream.
+struct KeptScratch {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  void* get(size_t n, cudaStream_t s) {
+    if (n > bytes) {
+      release(s);
+      EF_CUDA(cudaMallocAsync(&ptr, n, s));
+      bytes = n;
+    }
+    return ptr;
+  }
+  void release(cudaStream_t s) {
+    if (ptr) cudaFreeAsync(ptr, s);
+    ptr = nullptr;
+    bytes = 0;
+  }
+};
+
 struct Context {
   // With EINFOLD_TRACE set, phase() synchronizes the stream and prints the
   // milliseconds since the previous phase to stderr.
@@ -156,6 +188,7 @@ struct Context {
   uint64_t kernels = 0;  // kernels launched by the current call
   double product_ms = 0, product_ops = 0;  // the split products' kernels in the current call
   PinnedArena pinned;
+  KeptScratch kept;  // the attention backward's exports
   // Device-resident scratch kept across calls.
   void* status_word = nullptr;  // int32 status set by bounded device waits
 };

@@ -293,6 +293,7 @@ FoldOutput dense_fold(Context& ctx, const FoldD& f, const Relation& a, const Rel
   DeviceBuffer<uint32_t> held((na + 15) / 16, s), present((nb + 31) / 32, s);
   DeviceBuffer<uint8_t> reached(nx, s), valued(nx, s);
   DeviceBuffer<unsigned> flags(1, s);
+  ctx.phase("dense: matrices reserved");
   // Cells no row writes must read as 0: only incomplete operands or NULL
   // factors leave any (a repeated row declines below).
   if (ra < na || fa.nulls > 0) am.zero();
@@ -505,6 +506,7 @@ FoldOutput dense_fold(Context& ctx, const FoldD& f, const Relation& a, const Rel
   DeviceBuffer<uint8_t> vvalid((size_t)(n_out ? n_out : 1), s);
   DeviceBuffer<unsigned long long> nulls(1, s);
   nulls.zero();
+  ctx.phase("dense: result reserved");
   if (cells_n && n_out) {
     emit_cells<<<grid2, 256, 0, s>>>((int64_t)nx, (int64_t)ny, reached.get(), row_index.get(), sel.get(), pos.get(), ok,
                                      xtab.get(), ytab.get(), out.get(), valued.get(), vals.get(), vvalid.get(),
@@ -515,6 +517,7 @@ FoldOutput dense_fold(Context& ctx, const FoldD& f, const Relation& a, const Rel
   unsigned long long n_nulls = 0;
   EF_CUDA(cudaMemcpyAsync(&n_nulls, nulls.get(), 8, cudaMemcpyDeviceToHost, s));
   EF_CUDA(cudaStreamSynchronize(s));
+  ctx.phase("dense: cells emitted");
   OutBatch ob;
   ob.rows = n_out;
   for (size_t i = 0; i < f.outputs.size(); i++) {

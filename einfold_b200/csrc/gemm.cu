@@ -748,6 +748,20 @@ CUtensorMap digit_planes_map(const int8_t* digits, int64_t k_pad, int64_t rows, 
   return digit_map(digits, k_pad, rows, planes, box_rows, box_planes);
 }
 
+CUtensorMap f64_boxes_map(const double* x, int64_t cols, int64_t rows, int64_t batches, int box_cols, int box_rows) {
+  if (box_cols * 8 > 128) fail(EINFOLD_INVALID, "a 128-byte-swizzled box holds at most 16 doubles a row");
+  CUtensorMap map;
+  cuuint64_t dims[3] = {(cuuint64_t)cols, (cuuint64_t)rows, (cuuint64_t)batches};
+  cuuint64_t strides[2] = {(cuuint64_t)(cols * 8), (cuuint64_t)(cols * rows * 8)};
+  cuuint32_t box[3] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)x, dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) fail(EINFOLD_DEVICE, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return map;
+}
+
 void fp64_gemm(Context& ctx, const double* a, const uint32_t* held, const double* b, double* c, int64_t batches,
                int64_t m, int64_t n, int64_t k, int64_t /*batch_of_row*/, int64_t zblock, bool fused_multiply_add,
                cudaStream_t stream) {

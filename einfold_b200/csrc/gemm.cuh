@@ -54,6 +54,10 @@ void exponent_range(const int32_t* e, int64_t n, int* out, cudaStream_t stream);
 CUtensorMap digit_planes_map(const int8_t* digits, int64_t k_pad, int64_t rows, int64_t planes, int box_rows,
                              int box_planes);
 
+// A TMA map over doubles [batches][rows][cols] (cols a multiple of 2),
+// boxes of box_cols (at most 16) by box_rows in the 128-byte swizzle.
+CUtensorMap f64_boxes_map(const double* x, int64_t cols, int64_t rows, int64_t batches, int box_cols, int box_rows);
+
 // BT[w][j][i] = B[w][i][j] for a [batches][rows][cols] array.
 void transpose(const double* b, double* bt, int64_t batches, int64_t rows, int64_t cols, cudaStream_t stream);
 

@@ -59,6 +59,7 @@ Buffer result_buffer(Context& ctx, DeviceBuffer<T>& dev, size_t bytes, bool on_d
   b.ptr = dev.ptr;
   b.bytes = bytes;
   b.device = ctx.device;
+  b.capacity = dev.count * sizeof(T);
   dev.ptr = nullptr;
   dev.count = 0;
   return b;
