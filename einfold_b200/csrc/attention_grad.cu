@@ -493,11 +493,13 @@ template <int MODE>
 struct TileShape {
   static constexpr bool kQ = MODE == GRAD_Q;
   static constexpr int kDs = kQ ? GM * GJ * 8 : 0;  // one dS tile
+  static constexpr int kDsBufs = kQ ? 2 : 0;        // d_q: dS tiles double-buffered
   static constexpr int kBufs = kQ ? 1 : 2;          // weight digit tiles (d_v: one a stage)
   static constexpr int kB3 = S * GY * 64;
   static constexpr int kStage = kB3 + (kQ ? 0 : 1024);  // B3, and for d_v the rows' exponents
+  static constexpr int kStages = kQ ? 1 : 2;
   static constexpr int kAux = 8192;
-  static constexpr int kSmem = kDs + kBufs * kPTile + 2 * kStage + kAux + 1024;
+  static constexpr int kSmem = kDsBufs * kDs + kBufs * kPTile + kStages * kStage + kAux + 1024;
   static_assert(kSmem <= kMaxSmem, "the tiles must fit in shared memory");
 };
 
@@ -509,17 +511,18 @@ __global__ void __launch_bounds__(kGradThreads, 1)
   constexpr int CW = 16;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint8_t* sDs = smem;
-  uint8_t* sP = sDs + Sh::kDs;
-  uint8_t* sB = sP + Sh::kBufs * kPTile;  // 2 stages of [B3 | rows' exponents]
-  uint8_t* aux = sB + 2 * Sh::kStage;
+  uint8_t* sDs = smem;  // d_q: [2] dS tiles
+  uint8_t* sP = sDs + Sh::kDsBufs * Sh::kDs;
+  uint8_t* sB = sP + Sh::kBufs * kPTile;  // stages of [B3 | rows' exponents]
+  uint8_t* aux = sB + Sh::kStages * Sh::kStage;
   uint64_t* bars = (uint64_t*)aux;
-  uint64_t* kv_full = bars + 0;   // [2]
+  uint64_t* kv_full = bars + 0;   // [2] B3 stages (d_v: with the weights' tile)
   uint64_t* kv_empty = bars + 2;  // [2]
-  uint64_t* ds_empty = bars + 4;
-  uint64_t* p_full = bars + 5;
-  uint64_t* o_full = bars + 6;
-  uint64_t* tmem_free = bars + 7;
+  uint64_t* ds_full = bars + 4;   // [2] d_q: dS tiles
+  uint64_t* ds_empty = bars + 6;  // [2]
+  uint64_t* p_full = bars + 8;
+  uint64_t* o_full = bars + 9;
+  uint64_t* tmem_free = bars + 10;
   uint32_t* tmem_slot = (uint32_t*)(bars + 16);
   int* failed = (int*)(tmem_slot + 1);
   long long* span = (long long*)(tmem_slot + 4);
@@ -540,7 +543,10 @@ __global__ void __launch_bounds__(kGradThreads, 1)
       // stage's exponents) free a stage.
       mbar_init(&kv_empty[i], kQ ? 1 : 1 + kEpi / 32);
     }
-    mbar_init(ds_empty, kEpi / 32);
+    for (int i = 0; i < 2; i++) {
+      mbar_init(&ds_full[i], 1);
+      mbar_init(&ds_empty[i], kEpi / 32);
+    }
     mbar_init(p_full, kEpi / 32);
     mbar_init(o_full, 1);
     mbar_init(tmem_free, kEpi / 32);
@@ -591,36 +597,59 @@ __global__ void __launch_bounds__(kGradThreads, 1)
       for (int it = 0; it < n_tiles; it++) {
         const int st = it & 1;
         const uint32_t round = (uint32_t)(it >> 1);
+        const int cl0 = (ct0 + it) * GJ;
         if (*(volatile int*)failed) break;
-        if (!mbar_wait(&kv_empty[st], (round & 1) ^ 1) || (kQ && it > 0 && !mbar_wait(ds_empty, (uint32_t)((it - 1) & 1)))) {
+        bool ok;
+        if (kQ) {
+          // dS two tiles ahead; B3 (one stage) once the previous tile's MMAs are done.
+          ok = mbar_wait(&ds_empty[st], (round & 1) ^ 1);
+          if (ok) {
+            mbar_expect_tx(&ds_full[st], (uint32_t)Sh::kDs);
+            for (int j = 0; j < 4; j++)
+              tma_load_3d(sDs + st * Sh::kDs + j * GM * 128, &tds, &ds_full[st], cl0 + 16 * j, rt * GM,
+                          (int)blockIdx.y);
+          }
+          ok = ok && (it == 0 || mbar_wait(&kv_empty[0], (uint32_t)((it - 1) & 1)));
+          if (ok) {
+            mbar_expect_tx(&kv_full[0], (uint32_t)Sh::kB3);
+            tma_load_3d(sB, &tb3, &kv_full[0], cl0, a.y0, w * S);
+          }
+        } else {
+          ok = mbar_wait(&kv_empty[st], (round & 1) ^ 1);
+          if (ok) {
+            uint8_t* stage = sB + st * Sh::kStage;
+            mbar_expect_tx(&kv_full[st], (uint32_t)(Sh::kB3 + kPTile + GM * 4));
+            tma_load_3d(stage, &tb3, &kv_full[st], cl0, a.y0, w * S);
+            bulk_load(sP + st * kPTile, a.p_tiles + tile_of(it) * kPTile, kPTile, &kv_full[st]);
+            bulk_load(stage + Sh::kB3, a.p_exp + tile_of(it) * GM, GM * 4, &kv_full[st]);
+          }
+        }
+        if (!ok) {
           atomicOr(a.status, 2);
           *(volatile int*)failed = 1;
           break;
         }
-        const int cl0 = (ct0 + it) * GJ;
-        uint8_t* stage = sB + st * Sh::kStage;
-        mbar_expect_tx(&kv_full[st], (uint32_t)(Sh::kB3 + (kQ ? Sh::kDs : kPTile + GM * 4)));
-        tma_load_3d(stage, &tb3, &kv_full[st], cl0, a.y0, w * S);
-        if (kQ) {
-          for (int j = 0; j < 4; j++)
-            tma_load_3d(sDs + j * GM * 128, &tds, &kv_full[st], cl0 + 16 * j, rt * GM, (int)blockIdx.y);
-        } else {
-          bulk_load(sP + st * kPTile, a.p_tiles + tile_of(it) * kPTile, kPTile, &kv_full[st]);
-          bulk_load(stage + Sh::kB3, a.p_exp + tile_of(it) * GM, GM * 4, &kv_full[st]);
-        }
         issued = it + 1;
       }
-      for (int it = std::max(0, issued - 2); it < issued; it++) mbar_wait(&kv_full[it & 1], (uint32_t)((it >> 1) & 1));
+      // Copies still in flight complete before the CTA may exit.
+      for (int it = std::max(0, issued - 2); it < issued; it++) {
+        if (kQ) {
+          mbar_wait(&ds_full[it & 1], (uint32_t)((it >> 1) & 1));
+          if (it == issued - 1) mbar_wait(&kv_full[0], (uint32_t)(it & 1));
+        } else {
+          mbar_wait(&kv_full[it & 1], (uint32_t)((it >> 1) & 1));
+        }
+      }
     }
   } else if (warp == 1) {
     if (lane == 0 && n_tiles > 0) {
       int last = -1;  // the last tile whose MMAs were committed
       bool ok = true;
       for (int it = 0; ok && it < n_tiles; it++) {
-        const int st = it & 1;
+        const int st = kQ ? 0 : (it & 1);
         const uint32_t par = (uint32_t)(it & 1);
-        ok = mbar_wait(&kv_full[st], (uint32_t)((it >> 1) & 1)) && (it == 0 || mbar_wait(tmem_free, par ^ 1)) &&
-             (!kQ || mbar_wait(p_full, par));
+        ok = mbar_wait(&kv_full[st], kQ ? par : (uint32_t)((it >> 1) & 1)) &&
+             (it == 0 || mbar_wait(tmem_free, par ^ 1)) && (!kQ || mbar_wait(p_full, par));
         if (!ok || *(volatile int*)failed) break;
         tc_fence_after();
         const uint32_t a_base = smem_u32(sP + (kQ ? 0 : st * kPTile)), b_base = smem_u32(sB + st * Sh::kStage);
@@ -672,12 +701,12 @@ __global__ void __launch_bounds__(kGradThreads, 1)
     for (int it = 0; it < n_tiles; it++) {
       const int st = it & 1;
       const uint32_t par = (uint32_t)(it & 1);
-      wait(&kv_full[st], (uint32_t)((it >> 1) & 1));
+      wait(kQ ? &ds_full[st] : &kv_full[st], (uint32_t)((it >> 1) & 1));
       int ew;
       if (kQ) {
         // This row's 16 keys of the tile: box h, 128-byte row r, its 16-byte
         // chunks permuted by r mod 8.
-        const uint8_t* row = sDs + h * GM * 128 + r * 128;
+        const uint8_t* row = sDs + st * Sh::kDs + h * GM * 128 + r * 128;
         const int off = (ct0 + it) * GJ + h * CW - lo;
         double wv[CW];
 #pragma unroll
@@ -687,7 +716,7 @@ __global__ void __launch_bounds__(kGradThreads, 1)
           wv[2 * j + 1] = (unsigned)(off + 2 * j + 1) < span_r ? v.y : 0.0;
         }
         __syncwarp();
-        if (lane == 0) mbar_arrive(ds_empty);
+        if (lane == 0) mbar_arrive(&ds_empty[st]);
         double mx = 0.0;
 #pragma unroll
         for (int c = 0; c < CW; c++) mx = fmax(mx, fabs(wv[c]));
