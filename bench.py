@@ -439,7 +439,8 @@ def run_ours(args):
     # tensor cores per second against the int8 dense peak.
     bf16, hbm, basis = _peaks()
     int8_peak = 2.0 * bf16
-    names = {"fold": "split_gemm_kernel<6>", "attn_fwd": "attn_fwd_split<6,1>", "attn_bwd": "grad_split (3 kernels)"}
+    names = {"fold": "split_gemm_kernel<6>", "attn_fwd": "attn_fwd_split<6,1>",
+             "attn_bwd": "grad_split<d_k> + grad_tiles<d_v> + grad_tiles<d_q>"}
     kernels = {}
     for key, recs in stats.items():
         p_ms = statistics.mean(r[0] for r in recs)
@@ -544,7 +545,7 @@ def _profiled_traffic(component):
     """DRAM bytes per step of a component's product kernel, from the committed
     ncu summary (`traffic_bytes_per_launch:` line), or None."""
     files = {"fold": "split_gemm_kernel_matmul8192.txt", "attn_fwd": "attn_fwd_split_causal_T4096.txt",
-             "attn_bwd": "grad_split_causal_T4096.txt"}
+             "attn_bwd": "attention_backward_kernels_causal_T4096.txt"}
     path = os.path.join(ROOT, "profiles", files[component])
     try:
         for line in open(path):
