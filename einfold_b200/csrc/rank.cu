@@ -82,9 +82,13 @@ __global__ void __launch_bounds__(kThreads) chunk_counts(const uint64_t* __restr
 constexpr int kCountSplit = 4;  // blocks counting each chunk
 
 // Downsweep of one pass: block c sorts its chunk tile by tile, each key
-// ranked among equal digits in row order (warp __match_any_sync, warps
-// combined in shared memory), its destination its digit's running offset plus
-// that rank. Tiles arrive by TMA bulk copies into two shared-memory stages, the
+// ranked among equal digits in row order, its destination its digit's
+// running offset plus that rank. Within a warp, item i of every lane is
+// matched with __match_any_sync; each group's first lane stores the group's
+// size as a byte in counts[warp][digit][i], and a lane's rank among its warp's
+// equal digits is the sum of the bytes of items before its own (at most
+// 7·32, one 64-bit load and two dp4a) plus its place in its group: no item
+// waits on another's result. Tiles arrive by TMA bulk copies into two shared-memory stages, the
 // next one in flight while the current one is ranked; each stage is then
 // reused to reorder its tile by digit, and the tile is written out run by
 // run, contiguously.
@@ -99,7 +103,10 @@ __global__ void __launch_bounds__(kThreads) chunk_scatter(const uint64_t* __rest
   constexpr int WARPS = kThreads / 32;
   constexpr int STAGE = TILE * (8 * W + 4);
   extern __shared__ __align__(128) uint8_t smem[];
-  __shared__ unsigned int warp_hist[WARPS][256];
+  static_assert(ITEMS <= 8, "a digit's counts of the warp's items fill one 64-bit word");
+  // Byte i: item i's group size; then (low word) the warp's first place
+  // among the tile's keys of the digit.
+  __shared__ __align__(16) uint64_t counts[WARPS][256];
   __shared__ unsigned int tile_start[256];
   __shared__ long long running[256];
   __shared__ __align__(8) uint64_t bar[2];
@@ -143,8 +150,10 @@ __global__ void __launch_bounds__(kThreads) chunk_scatter(const uint64_t* __rest
     const int64_t count = min((int64_t)TILE, hi - base);
     const int64_t bulk = count & ~(int64_t)3;
     if (!ptx::mbar_wait(&bar[s], (uint32_t)((t >> 1) & 1), true)) atomicOr(err, 1);
-    for (int i = tid; i < WARPS * 256; i += kThreads) (&warp_hist[0][0])[i] = 0;
-    __syncthreads();
+    // This warp's byte counts start at zero (its own 2 KB; no other warp reads them yet).
+#pragma unroll
+    for (int i = 0; i < 256 / 32; i++) counts[warp][i * 32 + lane] = 0;
+    __syncwarp();
     uint64_t key[ITEMS][W];
     uint32_t val[ITEMS];
     int digit[ITEMS];
@@ -171,18 +180,26 @@ __global__ void __launch_bounds__(kThreads) chunk_scatter(const uint64_t* __rest
       const int d = digit[i];
       const unsigned peers = __match_any_sync(0xffffffffu, d);
       const unsigned below = __popc(peers & lt_mask);
-      const unsigned old = d < 256 ? warp_hist[warp][d] : 0u;
-      __syncwarp();
-      if (d < 256 && below == 0) warp_hist[warp][d] = old + __popc(peers);
-      __syncwarp();
-      local[i] = old + below;
+      if (d < 256 && below == 0) ((uint8_t*)&counts[warp][d])[i] = (uint8_t)__popc(peers);
+      local[i] = below;
     }
-    __syncthreads();  // every item read out of the stage; warp counts complete
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+      const int d = digit[i];
+      if (i > 0 && d < 256) {
+        const uint64_t c = counts[warp][d] & ((1ull << (8 * i)) - 1);  // items before i
+        local[i] += (unsigned)__dp4a((int)(uint32_t)c, 0x01010101, __dp4a((int)(uint32_t)(c >> 32), 0x01010101, 0));
+      }
+    }
+    __syncthreads();  // every item read out of the stage; every warp's counts complete
     unsigned int total = 0;
 #pragma unroll
     for (int w = 0; w < WARPS; w++) {
-      const unsigned cnt = warp_hist[w][tid];
-      warp_hist[w][tid] = total;
+      const uint64_t c = counts[w][tid];
+      // The warp's count of this digit, up to 256: the bytes summed in 32 bits.
+      const unsigned cnt = (unsigned)__dp4a((int)(uint32_t)c, 0x01010101, __dp4a((int)(uint32_t)(c >> 32), 0x01010101, 0));
+      counts[w][tid] = total;
       total += cnt;
     }
     unsigned int ex;
@@ -193,7 +210,7 @@ __global__ void __launch_bounds__(kThreads) chunk_scatter(const uint64_t* __rest
     for (int i = 0; i < ITEMS; i++) {
       const int d = digit[i];
       if (d < 256) {
-        const unsigned pos = tile_start[d] + warp_hist[warp][d] + local[i];
+        const unsigned pos = tile_start[d] + (unsigned)counts[warp][d] + local[i];
 #pragma unroll
         for (int w = 0; w < W; w++) skeys(s)[w * TILE + pos] = key[i][w];
         svals(s)[pos] = val[i];
@@ -206,7 +223,7 @@ __global__ void __launch_bounds__(kThreads) chunk_scatter(const uint64_t* __rest
       const long long dst = running[d] + (j - (long long)tile_start[d]);
 #pragma unroll
       for (int w = 0; w < W; w++) kout[(int64_t)w * ldo + dst] = skeys(s)[w * TILE + j];
-      vout[dst] = svals(s)[j];
+      if (vout) vout[dst] = svals(s)[j];
     }
     __syncthreads();  // the stage is free again
     running[tid] += total;
@@ -238,6 +255,37 @@ __global__ void finish_ranks(const uint8_t* __restrict__ head, const int64_t* __
   }
 }
 
+// One stable pass of the LSD sort over n (key, row) pairs on byte `shift`
+// of key word `word`: digit counts per chunk, one scan, the downsweep. With
+// vin null the rows are the positions; with vout null they aren't written.
+template <int W>
+void radix_pass(Context& ctx, const uint64_t* kin, int64_t ldi, const uint32_t* vin, uint64_t* kout, int64_t ldo,
+                uint32_t* vout, int64_t n, int word, int shift, int* err, cudaStream_t s) {
+  constexpr int ITEMS = W == 1 ? 8 : (W == 2 ? 6 : 4);
+  constexpr int TILE = kThreads * ITEMS;
+  // Chunks: as many as blocks resident at once, each a whole number of tiles.
+  int per_sm = 0;
+  const size_t smem = 2 * (size_t)TILE * (8 * W + 4);
+  EF_CUDA(cudaFuncSetAttribute(chunk_scatter<W, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  EF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chunk_scatter<W, ITEMS>, kThreads, smem));
+  int64_t chunks = (int64_t)std::max(1, per_sm) * ctx.sm_count;
+  const int64_t chunk = ((n + chunks - 1) / chunks + TILE - 1) / TILE * TILE;
+  chunks = (n + chunk - 1) / chunk;
+  DeviceBuffer<unsigned long long> table((size_t)(256 * chunks), s);
+  DeviceBuffer<long long> offsets((size_t)(256 * chunks), s);
+  size_t temp = 0;
+  EF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, table.get(), offsets.get(), (int)(256 * chunks), s));
+  DeviceBuffer<uint8_t> scan_tmp(temp ? temp : 1, s);
+  EF_CUDA(cudaMemsetAsync(table.get(), 0, (size_t)(256 * chunks) * 8, s));
+  chunk_counts<<<dim3((unsigned)chunks, kCountSplit), kThreads, 0, s>>>(kin + (int64_t)word * ldi, n, shift, chunk,
+                                                                        (int)chunks, table.get());
+  EF_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp.get(), temp, table.get(), offsets.get(), (int)(256 * chunks), s));
+  chunk_scatter<W, ITEMS><<<(unsigned)chunks, kThreads, smem, s>>>(kin, vin, kout, vout, n, ldi, ldo, word, shift,
+                                                                   chunk, (int)chunks, offsets.get(), err);
+  EF_LAUNCH_CHECK();
+  ctx.kernels += 3;
+}
+
 template <int W>
 int64_t rank_keys_w(Context& ctx, const uint64_t* keys, int64_t n, int64_t ld, uint32_t* rank, uint32_t* first,
                     cudaStream_t s, uint32_t* sorted_rows) {
@@ -253,8 +301,6 @@ int64_t rank_keys_w(Context& ctx, const uint64_t* keys, int64_t n, int64_t ld, u
     ld = lda;
   }
   if (n >= (int64_t)UINT32_MAX) fail(EINFOLD_COMPUTE, "ranking at most 2^32 - 1 rows together");
-  constexpr int ITEMS = W == 1 ? 8 : (W == 2 ? 6 : 4);
-  constexpr int TILE = kThreads * ITEMS;
   DeviceBuffer<unsigned long long> acc(2 * W, s);
   {
     std::vector<unsigned long long> init(2 * W);
@@ -280,45 +326,20 @@ int64_t rank_keys_w(Context& ctx, const uint64_t* keys, int64_t n, int64_t ld, u
     const uint64_t* cur_k = keys;
     int64_t cur_ld = ld;
     const uint32_t* cur_v = nullptr;
+    DeviceBuffer<int> err(1, s);
+    err.zero();
     if (passes) {
       const int64_t ldb = (n + 1) & ~(int64_t)1;
       for (int b = 0; b < 2; b++) {
         kb[b].allocate((size_t)(W * ldb), s);
         vb[b].allocate((size_t)n, s);
       }
-      // Chunks: as many as blocks resident at once, each a whole number of tiles.
-      int per_sm = 0;
-      const size_t smem = 2 * (size_t)TILE * (8 * W + 4);
-      EF_CUDA(cudaFuncSetAttribute(chunk_scatter<W, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      EF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chunk_scatter<W, ITEMS>, kThreads, smem));
-      int64_t chunks = (int64_t)std::max(1, per_sm) * ctx.sm_count;
-      int64_t chunk = ((n + chunks - 1) / chunks + TILE - 1) / TILE * TILE;
-      chunks = (n + chunk - 1) / chunk;
-      DeviceBuffer<unsigned long long> table((size_t)(256 * chunks), s);
-      DeviceBuffer<long long> offsets((size_t)(256 * chunks), s);
-      size_t temp = 0;
-      EF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, table.get(), offsets.get(), (int)(256 * chunks), s));
-      DeviceBuffer<uint8_t> scan_tmp(temp ? temp : 1, s);
-      DeviceBuffer<int> err(1, s);
-      err.zero();
       for (int p = 0; p < passes; p++) {
-        EF_CUDA(cudaMemsetAsync(table.get(), 0, (size_t)(256 * chunks) * 8, s));
-        chunk_counts<<<dim3((unsigned)chunks, kCountSplit), kThreads, 0, s>>>(cur_k + (int64_t)pw[p] * cur_ld, n,
-                                                                              ps[p], chunk, (int)chunks, table.get());
-        EF_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp.get(), temp, table.get(), offsets.get(), (int)(256 * chunks), s));
-        chunk_scatter<W, ITEMS><<<(unsigned)chunks, kThreads, smem, s>>>(cur_k, cur_v, kb[p & 1].get(), vb[p & 1].get(),
-                                                                         n, cur_ld, ldb, pw[p], ps[p], chunk, (int)chunks,
-                                                                         offsets.get(), err.get());
-        EF_LAUNCH_CHECK();
-        ctx.kernels += 3;
+        radix_pass<W>(ctx, cur_k, cur_ld, cur_v, kb[p & 1].get(), ldb, vb[p & 1].get(), n, pw[p], ps[p], err.get(), s);
         cur_k = kb[p & 1].get();
         cur_ld = ldb;
         cur_v = vb[p & 1].get();
       }
-      int e = 0;
-      EF_CUDA(cudaMemcpyAsync(&e, err.get(), 4, cudaMemcpyDeviceToHost, s));
-      EF_CUDA(cudaStreamSynchronize(s));
-      if (e) fail(EINFOLD_TIMEOUT, "a bounded wait in the radix sort ran out");
     }
     DeviceBuffer<uint32_t> identity;
     if (!cur_v) {
@@ -336,7 +357,10 @@ int64_t rank_keys_w(Context& ctx, const uint64_t* keys, int64_t n, int64_t ld, u
     ctx.kernels++;
     if (sorted_rows) EF_CUDA(cudaMemcpyAsync(sorted_rows, cur_v, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
     EF_LAUNCH_CHECK();
+    int e = 0;
+    EF_CUDA(cudaMemcpyAsync(&e, err.get(), 4, cudaMemcpyDeviceToHost, s));
     EF_CUDA(cudaStreamSynchronize(s));
+    if (e) fail(EINFOLD_TIMEOUT, "a bounded wait in the radix sort ran out");
     return distinct;
   }
 }

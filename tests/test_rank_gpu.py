@@ -77,3 +77,12 @@ def test_zipf_hashes_at_the_sorting_paths_size():
     keys = pool[pick].view(np.int64)
     words = keys.view(np.uint64) ^ np.uint64(1 << 63)
     _check(words)
+
+
+def test_more_than_4m_rows():
+    # Rank and first arrays beyond L2, chunks of many tiles.
+    n = (1 << 22) + 12_345
+    rng = oracle.Rng.seeded(9, 4)
+    pool = rng.u64s(n // 2)
+    words = pool[(rng.u64s(n) % np.uint64(len(pool))).astype(np.int64)]
+    _check(words)
