@@ -151,6 +151,14 @@ SIGNATURES = {
     "einfold_attention_backward": (ctypes.c_int32, [ctypes.c_void_p] + [ctypes.c_void_p] * 9 + [ctypes.c_int64] * 5 +
                                    [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_int32,
                                     ctypes.c_void_p, ctypes.POINTER(Result)]),
+    "einfold_attention_forward_ragged": (ctypes.c_int32, [ctypes.c_void_p] + [ctypes.c_void_p] * 5 +
+                                         [ctypes.c_int64] * 5 + [ctypes.c_void_p] * 2 +
+                                         [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                          ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.POINTER(Result)]),
+    "einfold_attention_backward_ragged": (ctypes.c_int32, [ctypes.c_void_p] + [ctypes.c_void_p] * 9 +
+                                          [ctypes.c_int64] * 5 + [ctypes.c_void_p] * 2 +
+                                          [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                           ctypes.c_int32, ctypes.c_void_p, ctypes.POINTER(Result)]),
     "einfold_fp64_gemm": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                            ctypes.c_int32, ctypes.c_void_p]),

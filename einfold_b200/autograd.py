@@ -84,13 +84,33 @@ def _batches(lead) -> int:
     return n
 
 
+def _lengths(x, lead, name, device):
+    """A ragged batch's lengths as a contiguous int64 tensor, one value per
+    batch, on the operands' device; or None."""
+    if x is None:
+        return None
+    x = torch.as_tensor(x, dtype=torch.int64)
+    if x.numel() != _batches(lead):
+        raise ValueError(f"{name} needs one length per batch ({_batches(lead)}), not {x.numel()}")
+    return x.reshape(-1).to(device).contiguous()
+
+
+def _ptr(x):
+    return x.data_ptr() if x is not None else None
+
+
 def attention_forward(q: torch.Tensor, k: torch.Tensor, v: torch.Tensor, conditions: Conditions = (),
-                      scale: float = 1.0, precision: Precision = Precision.SPLIT,
-                      slices: int = 0) -> Tuple[torch.Tensor, torch.Tensor]:
+                      scale: float = 1.0, precision: Precision = Precision.SPLIT, slices: int = 0,
+                      q_lengths=None, k_lengths=None) -> Tuple[torch.Tensor, torch.Tensor]:
     """out [..., lq, dv] and lse [..., lq] of softmax(scale·q·kᵀ) · v over the
     allowed pairs (q.t <cmp> k.t + off for every condition). Rows with no
     allowed key are NaN. Raises ``Declined`` where the reference's overflow
-    or underflow guards send the pipeline back to the host plan."""
+    or underflow guards send the pipeline back to the host plan.
+
+    Ragged batches: ``q_lengths`` / ``k_lengths`` (one per batch) say how
+    many of the padded rows of q, and of k and v, each batch uses; queries
+    past their length are NaN rows, keys past it are never joined. The
+    padding rows must hold finite values (zeros, say)."""
     q, k, v = _check(q, "q"), _check(k, "k"), _check(v, "v")
     *lead, lq, d = q.shape
     lk, dv = k.shape[-2], v.shape[-1]
@@ -100,46 +120,75 @@ def attention_forward(q: torch.Tensor, k: torch.Tensor, v: torch.Tensor, conditi
     out = torch.full((*lead, lq, dv), float("nan"), dtype=torch.float64, device=q.device)
     lse = torch.full((*lead, lq), float("nan"), dtype=torch.float64, device=q.device)
     n, cmp, off = _conditions(conditions)
-    _call(_lib.load().einfold_attention_forward, q.device.index or 0, q.data_ptr(), k.data_ptr(), v.data_ptr(),
-          out.data_ptr(), lse.data_ptr(), _batches(lead), lq, lk, d, dv, n, cmp, off, float(scale),
-          Precision(precision).value, int(slices))
+    ql = _lengths(q_lengths, lead, "q_lengths", q.device)
+    kl = _lengths(k_lengths, lead, "k_lengths", q.device)
+    lib = _lib.load()
+    if ql is None and kl is None:
+        _call(lib.einfold_attention_forward, q.device.index or 0, q.data_ptr(), k.data_ptr(), v.data_ptr(),
+              out.data_ptr(), lse.data_ptr(), _batches(lead), lq, lk, d, dv, n, cmp, off, float(scale),
+              Precision(precision).value, int(slices))
+    else:
+        _call(lib.einfold_attention_forward_ragged, q.device.index or 0, q.data_ptr(), k.data_ptr(), v.data_ptr(),
+              out.data_ptr(), lse.data_ptr(), _batches(lead), lq, lk, d, dv, _ptr(ql), _ptr(kl), n, cmp, off,
+              float(scale), Precision(precision).value, int(slices))
     return out, lse
 
 
 def attention_backward(q, k, v, out, lse, d_out, conditions: Conditions = (), scale: float = 1.0,
-                       precision: Precision = Precision.SPLIT) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
-    """d_q, d_k, d_v of ``attention_forward``'s out for the upstream d_out."""
+                       precision: Precision = Precision.SPLIT, q_lengths=None,
+                       k_lengths=None) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
+    """d_q, d_k, d_v of ``attention_forward``'s out for the upstream d_out
+    (ragged batches as there: the padding rows' gradients are zero, and
+    d_out's padding rows must be finite)."""
     q, k, v = _check(q, "q"), _check(k, "k"), _check(v, "v")
     out, lse, d_out = _check(out, "out"), _check(lse, "lse"), _check(d_out, "d_out")
     *lead, lq, d = q.shape
     lk, dv = k.shape[-2], v.shape[-1]
     d_q, d_k, d_v = torch.empty_like(q), torch.empty_like(k), torch.empty_like(v)
     n, cmp, off = _conditions(conditions)
-    _call(_lib.load().einfold_attention_backward, q.device.index or 0, q.data_ptr(), k.data_ptr(), v.data_ptr(),
-          out.data_ptr(), lse.data_ptr(), d_out.data_ptr(), d_q.data_ptr(), d_k.data_ptr(), d_v.data_ptr(),
-          _batches(lead), lq, lk, d, dv, n, cmp, off, float(scale), Precision(precision).value)
+    ql = _lengths(q_lengths, lead, "q_lengths", q.device)
+    kl = _lengths(k_lengths, lead, "k_lengths", q.device)
+    lib = _lib.load()
+    if ql is None and kl is None:
+        _call(lib.einfold_attention_backward, q.device.index or 0, q.data_ptr(), k.data_ptr(), v.data_ptr(),
+              out.data_ptr(), lse.data_ptr(), d_out.data_ptr(), d_q.data_ptr(), d_k.data_ptr(), d_v.data_ptr(),
+              _batches(lead), lq, lk, d, dv, n, cmp, off, float(scale), Precision(precision).value)
+    else:
+        _call(lib.einfold_attention_backward_ragged, q.device.index or 0, q.data_ptr(), k.data_ptr(), v.data_ptr(),
+              out.data_ptr(), lse.data_ptr(), d_out.data_ptr(), d_q.data_ptr(), d_k.data_ptr(), d_v.data_ptr(),
+              _batches(lead), lq, lk, d, dv, _ptr(ql), _ptr(kl), n, cmp, off, float(scale),
+              Precision(precision).value)
     return d_q, d_k, d_v
 
 
 class _Attention(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, q, k, v, conditions, scale, precision, slices):
-        out, lse = attention_forward(q, k, v, conditions, scale, precision, slices)
+    def forward(ctx, q, k, v, conditions, scale, precision, slices, q_lengths, k_lengths):
+        out, lse = attention_forward(q, k, v, conditions, scale, precision, slices, q_lengths, k_lengths)
         ctx.save_for_backward(q, k, v, out, lse)
         ctx.conditions, ctx.scale, ctx.precision = conditions, scale, precision
+        ctx.lengths = (q_lengths, k_lengths)
         return out
 
     @staticmethod
     def backward(ctx, d_out):
         q, k, v, out, lse = ctx.saved_tensors
-        d_q, d_k, d_v = attention_backward(q, k, v, out, lse, d_out, ctx.conditions, ctx.scale, ctx.precision)
-        return d_q, d_k, d_v, None, None, None, None
+        d_out = d_out.contiguous()
+        if ctx.lengths != (None, None):
+            # The padding rows carry no gradient (and must be finite).
+            d_out = torch.nan_to_num(d_out, nan=0.0)
+        d_q, d_k, d_v = attention_backward(q, k, v, out, lse, d_out, ctx.conditions, ctx.scale, ctx.precision,
+                                           *ctx.lengths)
+        return d_q, d_k, d_v, None, None, None, None, None, None
 
 
 def attention(q: torch.Tensor, k: torch.Tensor, v: torch.Tensor, conditions: Conditions = (), scale: float = 1.0,
-              precision: Precision = Precision.SPLIT, slices: int = 0) -> torch.Tensor:
-    """Differentiable softmax attention (see ``attention_forward``)."""
-    return _Attention.apply(q, k, v, list(conditions), float(scale), Precision(precision), int(slices))
+              precision: Precision = Precision.SPLIT, slices: int = 0, q_lengths=None,
+              k_lengths=None) -> torch.Tensor:
+    """Differentiable softmax attention (see ``attention_forward``; ragged
+    batches by ``q_lengths`` / ``k_lengths``)."""
+    return _Attention.apply(q, k, v, list(conditions), float(scale), Precision(precision), int(slices), q_lengths,
+                            k_lengths)
 
 
 def _gemm(a: torch.Tensor, b: torch.Tensor, b_transposed: bool, precision: Precision, slices: int) -> torch.Tensor:

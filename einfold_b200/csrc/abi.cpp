@@ -353,4 +353,65 @@ int32_t einfold_attention_backward(einfold_context* ctx, const double* q, const 
   });
 }
 
+// Ragged lengths: read back, checked against the padded extents, and
+// attached to the problem's mask.
+static void attach_lengths(ef::AttentionProblem& p, const int64_t* q_lengths, const int64_t* k_lengths,
+                           cudaStream_t s) {
+  auto fetch = [&](const int64_t* dev, int64_t limit, const char* what, std::vector<int64_t>& host) {
+    if (!dev || p.batches == 0) return;
+    host.resize((size_t)p.batches);
+    EF_CUDA(cudaMemcpyAsync(host.data(), dev, (size_t)p.batches * 8, cudaMemcpyDeviceToHost, s));
+    EF_CUDA(cudaStreamSynchronize(s));
+    for (int64_t x : host)
+      if (x < 0 || x > limit)
+        ef::fail(EINFOLD_INVALID, "a %s length of %lld outside [0, %lld]", what, (long long)x, (long long)limit);
+  };
+  fetch(q_lengths, p.lnx, "query", p.xlen_host);
+  fetch(k_lengths, p.lnj, "key", p.jlen_host);
+  p.mask.xlen = p.batches ? q_lengths : nullptr;
+  p.mask.jlen = p.batches ? k_lengths : nullptr;
+}
+
+int32_t einfold_attention_forward_ragged(einfold_context* ctx, const double* q, const double* k, const double* v,
+                                         double* out, double* lse, int64_t batches, int64_t lq, int64_t lk,
+                                         int64_t d, int64_t dv, const int64_t* q_lengths, const int64_t* k_lengths,
+                                         int32_t n_conditions, const int32_t* comparisons, const int64_t* offsets,
+                                         double scale, int32_t precision, int32_t slices, void* stream,
+                                         einfold_result* info) {
+  return guarded(ctx, info, [&](ef::Context& cx) -> int32_t {
+    cudaStream_t s = stream ? (cudaStream_t)stream : cx.stream;
+    ef::AttentionProblem p =
+        attention_problem(q, k, v, out, lse, batches, lq, lk, d, dv, n_conditions, comparisons, offsets, scale);
+    attach_lengths(p, q_lengths, k_lengths, s);
+    const ef::AttentionOutcome r = ef::attention_forward(cx, p, precision, slices, s);
+    EF_CUDA(cudaStreamSynchronize(s));
+    if (r == ef::ATTENTION_GUARDED) ef::decline("a sum that overflowed or may have underflowed");
+    return EINFOLD_OK;
+  });
+}
+
+int32_t einfold_attention_backward_ragged(einfold_context* ctx, const double* q, const double* k, const double* v,
+                                          const double* out, const double* lse, const double* d_out, double* d_q,
+                                          double* d_k, double* d_v, int64_t batches, int64_t lq, int64_t lk,
+                                          int64_t d, int64_t dv, const int64_t* q_lengths, const int64_t* k_lengths,
+                                          int32_t n_conditions, const int32_t* comparisons, const int64_t* offsets,
+                                          double scale, int32_t precision, void* stream, einfold_result* info) {
+  return guarded(ctx, info, [&](ef::Context& cx) -> int32_t {
+    cudaStream_t s = stream ? (cudaStream_t)stream : cx.stream;
+    ef::AttentionGradients g;
+    g.f = attention_problem(q, k, v, nullptr, nullptr, batches, lq, lk, d, dv, n_conditions, comparisons, offsets,
+                            scale);
+    attach_lengths(g.f, q_lengths, k_lengths, s);
+    g.out = out;
+    g.lse = lse;
+    g.d_out = d_out;
+    g.d_q = d_q;
+    g.d_k = d_k;
+    g.d_v = d_v;
+    ef::attention_backward(cx, g, precision, s);
+    EF_CUDA(cudaStreamSynchronize(s));
+    return EINFOLD_OK;
+  });
+}
+
 }  // extern "C"

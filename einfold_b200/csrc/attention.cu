@@ -86,6 +86,7 @@ struct AttnArgs {
   double* lse;  // [w·lnx + x] or null
   int* status;  // bit 0: a guard fired; bit 1: a wait ran out
   unsigned long long* tiles;  // (row tile, key tile) pairs computed
+  const int2* items;  // ragged batches: block i runs (query tile, batch) items[i]; null: the grid's
 };
 
 // The S levels of this thread's 4 TMEM columns at `col`.
@@ -136,8 +137,9 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
   double* red = (double*)(aux + 4096);            // [4][128]
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int xt = (int)(gridDim.x - 1 - blockIdx.x);  // the longest rows of a causal mask first
-  const int w = blockIdx.y;
+  // The longest rows of a causal mask first; ragged batches by their work list.
+  const int xt = a.items ? a.items[blockIdx.x].x : (int)(gridDim.x - 1 - blockIdx.x);
+  const int w = a.items ? a.items[blockIdx.x].y : (int)blockIdx.y;
   const int64_t x_base = (int64_t)w * a.lnx;
 
   if (threadIdx.x == 0) {
@@ -630,7 +632,39 @@ AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int sl
   args.lse = p.lse;
   args.status = status + 1;
   args.tiles = tiles;
-  const dim3 grid((unsigned)(lnx_pad / AM), (unsigned)W);
+  dim3 grid((unsigned)(lnx_pad / AM), (unsigned)W);
+  // Ragged batches: one block per query tile that joins some key, the tiles
+  // with the most key tiles first.
+  DeviceBuffer<int2> items;
+  if (!p.xlen_host.empty() || !p.jlen_host.empty()) {
+    Mask hm = p.mask;
+    hm.xlen = p.xlen_host.empty() ? nullptr : p.xlen_host.data();
+    hm.jlen = p.jlen_host.empty() ? nullptr : p.jlen_host.data();
+    std::vector<std::pair<int64_t, int2>> work;
+    for (int64_t w = 0; w < W; w++) {
+      const int64_t rows = hm.xlen ? hm.xlen[w] : p.lnx;
+      for (int64_t xt = 0; xt * AM < rows; xt++) {
+        int64_t first = INT64_MAX, last = INT64_MIN;
+        for (int64_t r = xt * AM; r < std::min(rows, xt * AM + AM); r++) {
+          int64_t lo, hi;
+          allowed(hm, w * p.lnx + r, lo, hi);
+          if (lo < hi) {
+            first = std::min(first, lo - w * p.lnj);
+            last = std::max(last, hi - w * p.lnj);
+          }
+        }
+        if (first < last) work.push_back({(last + AJ - 1) / AJ - first / AJ, make_int2((int)xt, (int)w)});
+      }
+    }
+    std::stable_sort(work.begin(), work.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    std::vector<int2> list;
+    for (auto& x : work) list.push_back(x.second);
+    if (list.empty()) return ATTENTION_DONE;
+    items.allocate(list.size(), stream);
+    EF_CUDA(cudaMemcpyAsync(items.get(), list.data(), list.size() * sizeof(int2), cudaMemcpyHostToDevice, stream));
+    args.items = items.get();
+    grid = dim3((unsigned)list.size(), 1);
+  }
   cudaEvent_t e0, e1;
   EF_CUDA(cudaEventCreate(&e0));
   EF_CUDA(cudaEventCreate(&e1));

@@ -2,6 +2,8 @@
 // conditions, and the split forward pass over placed matrices.
 #pragma once
 
+#include <vector>
+
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -19,14 +21,24 @@ struct Mask {
   int cmp[kMaxMask] = {};
   int64_t off[kMaxMask] = {};
   int64_t lnx = 1, lnj = 0;
+  // Ragged batches (arrays of one length per batch, null: every batch
+  // full; device memory in kernels, host memory on the host): batch w's X
+  // positions at or past xlen[w] join nothing, and its J positions at or
+  // past jlen[w] are joined by none.
+  const int64_t* xlen = nullptr;
+  const int64_t* jlen = nullptr;
 };
 
 // allowed(x) (fused.rs:350-368): the half-open J interval that X position
 // x may join, the intersection of each condition's, in 128-bit integers,
-// clamped to x's batch.
+// clamped to x's batch (and to its lengths when ragged).
 __host__ __device__ inline void allowed(const Mask& m, int64_t x, int64_t& lo_out, int64_t& hi_out) {
-  const int64_t group_start = (x / m.lnx) * m.lnj;
-  const __int128 xx = x % m.lnx, n = m.lnj;
+  const int64_t w = x / m.lnx;
+  const int64_t group_start = w * m.lnj;
+  const __int128 xx = x % m.lnx;
+  __int128 n = m.lnj;
+  if (m.jlen) n = m.jlen[w] < m.lnj ? m.jlen[w] : m.lnj;
+  if (m.xlen && xx >= m.xlen[w]) n = 0;
   __int128 lo = 0, hi = n;
   for (int i = 0; i < m.n; i++) {
     const __int128 bound = xx - (__int128)m.off[i];
@@ -63,6 +75,8 @@ struct AttentionProblem {
   const double* smallest = nullptr;
   double* out = nullptr;
   double* lse = nullptr;
+  // Ragged batches: host copies of the mask's lengths (empty: full).
+  std::vector<int64_t> xlen_host, jlen_host;
 };
 
 enum AttentionOutcome { ATTENTION_DONE = 0, ATTENTION_INELIGIBLE = 1, ATTENTION_GUARDED = 2 };

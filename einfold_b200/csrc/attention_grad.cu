@@ -945,6 +945,8 @@ Mask transposed(const Mask& m) {
   }
   t.lnx = m.lnj > 0 ? m.lnj : 1;
   t.lnj = m.lnx;
+  t.xlen = m.jlen;
+  t.jlen = m.xlen;
   return t;
 }
 

@@ -322,6 +322,30 @@ int32_t einfold_attention_backward(einfold_context* ctx, const double* q, const 
                                    const int64_t* offsets, double scale, int32_t precision, void* stream,
                                    einfold_result* info);
 
+/* Ragged batches (groups of different lengths, which the reference's
+ * placement declines, fused.rs:624-664): the same operands padded to lq and
+ * lk rows, batch w using q_lengths[w] queries and k_lengths[w] keys (device
+ * arrays of `batches` int64 values, each in [0, lq] and [0, lk]; NULL:
+ * full). A query at or past its batch's length joins nothing (its out and
+ * lse rows are left unwritten, its d_q row is zero), a key at or past it is
+ * joined by none (its d_k and d_v rows are zero); the padding rows must
+ * hold finite values. The forward pass runs all batches in one launch over
+ * the query tiles that join some key, the tiles with the most key tiles
+ * first. Otherwise as einfold_attention_forward and
+ * einfold_attention_backward. */
+int32_t einfold_attention_forward_ragged(einfold_context* ctx, const double* q, const double* k, const double* v,
+                                         double* out, double* lse, int64_t batches, int64_t lq, int64_t lk,
+                                         int64_t d, int64_t dv, const int64_t* q_lengths, const int64_t* k_lengths,
+                                         int32_t n_conditions, const int32_t* comparisons, const int64_t* offsets,
+                                         double scale, int32_t precision, int32_t slices, void* stream,
+                                         einfold_result* info);
+int32_t einfold_attention_backward_ragged(einfold_context* ctx, const double* q, const double* k, const double* v,
+                                          const double* out, const double* lse, const double* d_out, double* d_q,
+                                          double* d_k, double* d_v, int64_t batches, int64_t lq, int64_t lk,
+                                          int64_t d, int64_t dv, const int64_t* q_lengths, const int64_t* k_lengths,
+                                          int32_t n_conditions, const int32_t* comparisons, const int64_t* offsets,
+                                          double scale, int32_t precision, void* stream, einfold_result* info);
+
 #ifdef __cplusplus
 }
 #endif
