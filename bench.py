@@ -455,6 +455,7 @@ def run_ours(args):
                 "kernel_ms": kernels[top]["ms"], "ops_per_launch": kernels[top]["ops_per_step"], "kernels": kernels}
 
     ranking = _ranking(hbm, basis) if not args.no_ranking else None
+    ragged = _ragged() if not args.no_ragged else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -486,6 +487,7 @@ def run_ours(args):
                          "ratio_split_over_fp64": fp64_step_ms / ms_per_step},
             "roofline": roofline,
             "ranking": ranking,
+            "ragged": ragged,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches[0],
@@ -541,6 +543,48 @@ def _ranking(hbm, basis):
     return out
 
 
+def _ragged():
+    """Ragged batches (64 groups, d=128, lengths log-uniform in [128, 8192],
+    window |tq - tk| <= 512, values normal(0, 1/sqrt(128)), padded to the
+    longest): the attention forward in the split form (one launch over the
+    query tiles that join some key) and in the FP64 form, timed with CUDA
+    events, FLOP = 4·d per allowed pair; the split result's error against
+    the FP64 one (max |diff| / max |out|)."""
+    import torch
+
+    from einfold_b200 import autograd as A
+    from einfold_b200 import cases as C
+    from einfold_b200.kernels import Precision
+
+    groups, d, radius = 64, 128, 512
+    q, k, v, lengths = C.ragged_inputs(groups, d, seed=SEED)
+    flop = 4.0 * d * C.allowed_pairs(lengths, radius)
+    out = {"groups": groups, "d": d, "window": radius, "rows": int(lengths.sum()), "padded_to": int(lengths.max()),
+           "flop": flop}
+    results = {}
+    for name, prec in (("split", Precision.SPLIT), ("fp64", Precision.FP64)):
+        times = []
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            o, _ = A.attention_forward(q, k, v, A.window(radius), d ** -0.5, prec, q_lengths=lengths,
+                                       k_lengths=lengths)
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        results[name] = o
+        ms = statistics.median(times)
+        out[name] = {"ms": ms, "tflop_per_s": flop / ms / 1e9}
+    seen = ~torch.isnan(results["fp64"])
+    out["split_max_rel_err"] = ((results["split"][seen] - results["fp64"][seen]).abs().max() /
+                                results["fp64"][seen].abs().max()).item()
+    out["ratio_split_over_fp64"] = out["fp64"]["ms"] / out["split"]["ms"]
+    del q, k, v, results
+    torch.cuda.empty_cache()
+    return out
+
+
 def _profiled_traffic(component):
     """DRAM bytes per step of a component's product kernel, from the committed
     ncu summary (`traffic_bytes_per_launch:` line), or None."""
@@ -566,6 +610,7 @@ def main():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-ranking", action="store_true")
+    p.add_argument("--no-ragged", action="store_true")
     args = p.parse_args()
     if args.impl == "reference":
         run_reference(args)
