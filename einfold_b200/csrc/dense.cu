@@ -29,7 +29,8 @@ constexpr int64_t kNoGroup = -1;
 // position shows in the bits an atomic OR returns. The lanes of a warp that
 // share a word OR their codes together first and one of them issues the
 // atomic (rows in key order share words). Every thread of a block runs the same iterations,
-// so the warp-wide matches see all the warp's rows.
+// so the warp-wide matches see all the warp's rows. NARROW: word indices fit 32 bits.
+template <bool NARROW>
 __global__ void scatter_a_kernel(Role xs, Role zs, int64_t rows, const double* __restrict__ vals,
                                  const uint8_t* __restrict__ valid, int64_t nz, double* __restrict__ a,
                                  uint32_t* __restrict__ held, uint8_t* __restrict__ reached,
@@ -45,7 +46,7 @@ __global__ void scatter_a_kernel(Role xs, Role zs, int64_t rows, const double* _
     const bool v = valid ? valid[r] != 0 : true;
     const unsigned sh = (unsigned)(p & 15) * 2;
     const unsigned long long word = (unsigned long long)(p >> 4);
-    const unsigned same_word = __match_any_sync(active, word);
+    const unsigned same_word = NARROW ? __match_any_sync(active, (unsigned)word) : __match_any_sync(active, word);
     const unsigned bits = __reduce_or_sync(same_word, (v ? 2u : 1u) << sh);
     // A cell twice in the warp leaves fewer distinct cells than lanes.
     if (__popc(__reduce_or_sync(same_word, 1u << (p & 15))) != __popc(same_word)) f |= F_DUP_A;
@@ -54,11 +55,11 @@ __global__ void scatter_a_kernel(Role xs, Role zs, int64_t rows, const double* _
     if (lane == leader) old = atomicOr(&held[word], bits);
     old = __shfl_sync(same_word, old, leader);
     if ((old >> sh) & 3u) f |= F_DUP_A;
-    if (!reached[x]) reached[x] = 1;
+    reached[x] = 1;
     if (v) {
       const double val = vals[r];
       a[p] = val;
-      if (!valued[x]) valued[x] = 1;
+      valued[x] = 1;
       if (!isfinite(val)) f |= F_NONFINITE_A;
     }
   }
@@ -68,6 +69,7 @@ __global__ void scatter_a_kernel(Role xs, Role zs, int64_t rows, const double* _
 // Scatters b's rows into b[w][z][y] (its natural layout: each row of b's
 // matrix contiguous); `present` packs a bit per cell, ORed per word across
 // the warp's lanes first as in scatter_a_kernel.
+template <bool NARROW>
 __global__ void scatter_b_kernel(Role wzs, Role ys, int64_t rows, const double* __restrict__ vals,
                                  const uint8_t* __restrict__ valid, int64_t ny, double* __restrict__ bm,
                                  uint32_t* __restrict__ present, unsigned* flags) {
@@ -80,7 +82,7 @@ __global__ void scatter_b_kernel(Role wzs, Role ys, int64_t rows, const double* 
     const int64_t p = role_position(wzs, r) * ny + role_position(ys, r);
     const unsigned bit = 1u << (p & 31);
     const unsigned long long word = (unsigned long long)(p >> 5);
-    const unsigned same_word = __match_any_sync(active, word);
+    const unsigned same_word = NARROW ? __match_any_sync(active, (unsigned)word) : __match_any_sync(active, word);
     const unsigned bits = __reduce_or_sync(same_word, bit);
     // A cell twice in the warp leaves fewer distinct bits than lanes.
     if (__popc(bits) != __popc(same_word)) f |= F_DUP_B;
@@ -151,6 +153,39 @@ __global__ void emit_cells(int64_t nx, int64_t ny, const uint8_t* __restrict__ r
       val_out[o] = out[i];
       valid_out[o] = v;
       local += !v;
+    }
+  }
+  if (local) atomicAdd(nulls, local);
+}
+
+// emit_cells for the common case, no conditions, keys of 8 bytes and an
+// even ny: two cells a thread, each column written 16 bytes at a time.
+__global__ void emit_cell_pairs(int64_t nx, int64_t ny, const uint8_t* __restrict__ reached,
+                                const int64_t* __restrict__ row_index, OutKeys keys,
+                                const int64_t* __restrict__ xtab, const int64_t* __restrict__ ytab,
+                                const double* __restrict__ out, const uint8_t* __restrict__ valued,
+                                double* __restrict__ val_out, uint8_t* __restrict__ valid_out,
+                                unsigned long long* nulls) {
+  unsigned long long local = 0;
+  for (int64_t x = blockIdx.y; x < nx; x += gridDim.y) {
+    if (!reached[x]) continue;
+    const uint8_t v = valued[x];
+    const int64_t base = row_index[x] * ny;
+    for (int64_t y = 2 * ((int64_t)blockIdx.x * blockDim.x + threadIdx.x); y < ny;
+         y += 2 * (int64_t)gridDim.x * blockDim.x) {
+      const int64_t o = base + y, i = x * ny + y;
+      for (int k = 0; k < keys.n; k++) {
+        longlong2 kv;
+        if (keys.key[k].in_x) {
+          kv.x = kv.y = xtab[(int64_t)k * nx + x];
+        } else {
+          kv = *(const longlong2*)(ytab + (int64_t)k * ny + y);
+        }
+        *(longlong2*)((int64_t*)keys.out[k] + o) = kv;
+      }
+      *(double2*)(val_out + o) = *(const double2*)(out + i);
+      *(uchar2*)(valid_out + o) = make_uchar2(v, v);
+      local += v ? 0 : 2;
     }
   }
   if (local) atomicAdd(nulls, local);
@@ -303,15 +338,16 @@ FoldOutput dense_fold(Context& ctx, const FoldD& f, const Relation& a, const Rel
   Role rxs = role_of(xs, op_a, ka, extent), rzs = role_of(zs, op_a, ka, extent);
   Role rwzs = role_of(wzs, op_b, kb, extent), rys = role_of(ys, op_b, kb, extent);
   if (ra) {
-    scatter_a_kernel<<<blocks_for(ra, 256), 256, 0, s>>>(rxs, rzs, (int64_t)ra, (const double*)fa.ptr(),
-                                                         fa.valid.get(), (int64_t)nz, am.get(), held.get(),
-                                                         reached.get(), valued.get(), flags.get());
+    auto scatter_a = na / 16 < (1ull << 32) ? scatter_a_kernel<true> : scatter_a_kernel<false>;
+    scatter_a<<<blocks_for(ra, 256), 256, 0, s>>>(rxs, rzs, (int64_t)ra, (const double*)fa.ptr(), fa.valid.get(),
+                                                  (int64_t)nz, am.get(), held.get(), reached.get(), valued.get(),
+                                                  flags.get());
     ctx.kernels++;
   }
   if (rb) {
-    scatter_b_kernel<<<blocks_for(rb, 256), 256, 0, s>>>(rwzs, rys, (int64_t)rb, (const double*)fb.ptr(),
-                                                         fb.valid.get(), (int64_t)ny, bm.get(), present.get(),
-                                                         flags.get());
+    auto scatter_b = nb / 32 < (1ull << 32) ? scatter_b_kernel<true> : scatter_b_kernel<false>;
+    scatter_b<<<blocks_for(rb, 256), 256, 0, s>>>(rwzs, rys, (int64_t)rb, (const double*)fb.ptr(), fb.valid.get(),
+                                                  (int64_t)ny, bm.get(), present.get(), flags.get());
     ctx.kernels++;
   }
   EF_LAUNCH_CHECK();
@@ -507,7 +543,17 @@ FoldOutput dense_fold(Context& ctx, const FoldD& f, const Relation& a, const Rel
   DeviceBuffer<unsigned long long> nulls(1, s);
   nulls.zero();
   ctx.phase("dense: result reserved");
-  if (cells_n && n_out) {
+  bool pairs = !sel.get() && ny % 2 == 0;
+  for (int k = 0; k < ok.n; k++) pairs = pairs && ok.width[k] == 8;
+  if (cells_n && n_out && pairs) {
+    const uint64_t gx = std::min<uint64_t>(std::max<uint64_t>((ny / 2 + 255) / 256, 1), 64);
+    const dim3 grid_pairs((unsigned)gx, (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(nx, 148 * 16 / gx)));
+    emit_cell_pairs<<<grid_pairs, 256, 0, s>>>((int64_t)nx, (int64_t)ny, reached.get(), row_index.get(), ok,
+                                               xtab.get(), ytab.get(), out.get(), valued.get(), vals.get(),
+                                               vvalid.get(), nulls.get());
+    ctx.kernels++;
+    EF_LAUNCH_CHECK();
+  } else if (cells_n && n_out) {
     emit_cells<<<grid2, 256, 0, s>>>((int64_t)nx, (int64_t)ny, reached.get(), row_index.get(), sel.get(), pos.get(), ok,
                                      xtab.get(), ytab.get(), out.get(), valued.get(), vals.get(), vvalid.get(),
                                      nulls.get());

@@ -24,6 +24,7 @@
 #include <type_traits>
 
 #include "gemm.cuh"
+#include "levels.cuh"
 #include "ptx.cuh"
 
 namespace ef {
@@ -330,10 +331,77 @@ __global__ void __launch_bounds__(256) slice_short_rows(const double* __restrict
   }
 }
 
+// Rows of at most 64 values (k_pad == 64), for S <= 6: half a warp per row,
+// four values a lane loaded 16 bytes at a time, the digits cut from the
+// bytes of the rounded values (digit_planes4: round to nearest, ties to
+// even, as llrint, so the same digits as slice_short_rows).
+template <int S>
+__global__ void __launch_bounds__(256) slice_half_warp_rows(const double* __restrict__ x, int64_t batches,
+                                                            int64_t rows, int64_t k, int64_t ld, int64_t rows_pad,
+                                                            int32_t* __restrict__ e_out, int8_t* __restrict__ digits,
+                                                            int* status) {
+  constexpr int64_t kPad = 64;
+  const int lane = threadIdx.x & 31, l16 = lane & 15, half = lane >> 4;
+  const int64_t slab = rows_pad * kPad, total = batches * rows_pad;
+  // Both halves of a warp take their loop steps together (the shuffles are warp-wide).
+  for (int64_t gp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; gp * 2 < total;
+       gp += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    const int64_t g = gp * 2 + half;
+    const int64_t w = g / rows_pad, r = g % rows_pad;
+    const bool live = g < total && r < rows;
+    const double* row = x + (w * rows + r) * ld;
+    const int64_t c0 = (int64_t)l16 * 4;
+    double v[4];
+    if (live && c0 + 3 < k && ((((uintptr_t)(row + c0)) & 15) == 0)) {
+      const double2 a = *(const double2*)(row + c0), b = *(const double2*)(row + c0 + 2);
+      v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; j++) v[j] = (live && c0 + j < k) ? row[c0 + j] : 0.0;
+    }
+    double m = 0.0;
+    bool bad = false;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const double a = fabs(v[j]);
+      bad |= !(a <= 1.7976931348623157e308);
+      m = fmax(m, a);
+      if (!(a <= 1.7976931348623157e308)) v[j] = 0.0;
+    }
+    if (bad) atomicOr(status, 1);
+    for (int o = 8; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    int ex = 0;
+    if (m > 0.0 && m <= 1.7976931348623157e308) {
+      frexp(m, &ex);
+      ex += 2;
+    }
+    if (g < total) {
+      if (l16 == 0) e_out[g] = ex;
+      // x · 2^(8S - ex) in two exact factors (8S - ex may leave the normal range).
+      const int shift = 8 * S - ex;
+      const double f1 = ptx::pow2(shift >> 1), f2 = ptx::pow2(shift - (shift >> 1));
+      double xs[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) xs[j] = v[j] * f1 * f2;
+      uint32_t planes[S];
+      digit_planes4<S>(xs, planes);
+#pragma unroll
+      for (int s2 = 0; s2 < S; s2++) *(uint32_t*)(digits + (w * S + s2) * slab + r * kPad + c0) = planes[s2];
+    }
+  }
+}
+
 // Launches the row slicer that suits the row length.
 template <int S>
 void launch_slice_rows(const double* x, int64_t batches, int64_t rows, int64_t k, int64_t ld, int64_t rows_pad,
                        int64_t k_pad, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream) {
+  if constexpr (S <= 6) {
+    if (k_pad == 64) {
+      slice_half_warp_rows<S><<<blocks_for((uint64_t)(batches * rows_pad) * 16, 256), 256, 0, stream>>>(
+          x, batches, rows, k, ld, rows_pad, e_out, digits, status);
+      return;
+    }
+  }
   if (k_pad <= 128)
     slice_short_rows<S><<<blocks_for((uint64_t)(batches * rows_pad) * 32, 256), 256, 0, stream>>>(
         x, batches, rows, k, ld, rows_pad, k_pad, e_out, digits, status);
@@ -399,18 +467,34 @@ __global__ void __launch_bounds__(256) col_digits(const double* __restrict__ x, 
   if (blockIdx.y == 0 && kc == 0) e_out[w * n_pad + col] = ex;
   const int shift = 8 * S - ex;
   uint32_t word[S][4];
+  if constexpr (S <= 6) {
+    // The bytes of the rounded values (round to nearest, ties to even, as
+    // llrint), the power of two in two exact factors.
+    const double f1 = ptx::pow2(shift >> 1), f2 = ptx::pow2(shift - (shift >> 1));
 #pragma unroll
-  for (int s = 0; s < S; s++)
+    for (int q = 0; q < 4; q++) {
+      double xs[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) word[s][q] = 0;
+      for (int i = 0; i < 4; i++) xs[i] = tile[kc * 16 + q * 4 + i][nl] * f1 * f2;
+      uint32_t planes[S];
+      digit_planes4<S>(xs, planes);
 #pragma unroll
-  for (int j = 0; j < 16; j++) {
-    long long X2 = llrint(ldexp(tile[kc * 16 + j][nl], shift));
+      for (int s = 0; s < S; s++) word[s][q] = planes[s];
+    }
+  } else {
 #pragma unroll
-    for (int s = S - 1; s >= 0; s--) {
-      const long long d = ((X2 + 128) & 255) - 128;
-      word[s][j >> 2] |= ((uint32_t)(d & 255)) << (8 * (j & 3));
-      X2 = (X2 - d) >> 8;
+    for (int s = 0; s < S; s++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) word[s][q] = 0;
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      long long X2 = llrint(ldexp(tile[kc * 16 + j][nl], shift));
+#pragma unroll
+      for (int s = S - 1; s >= 0; s--) {
+        const long long d = ((X2 + 128) & 255) - 128;
+        word[s][j >> 2] |= ((uint32_t)(d & 255)) << (8 * (j & 3));
+        X2 = (X2 - d) >> 8;
+      }
     }
   }
   const int64_t slab = n_pad * k_pad;
