@@ -36,6 +36,7 @@
 // and averages to ~1e-14 of max|v|.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "attention.cuh"
 #include "fastexp.cuh"
@@ -545,6 +546,59 @@ void launch(const CUtensorMap& tq, const CUtensorMap& tk, const CUtensorMap& tv,
   EF_LAUNCH_CHECK();
 }
 
+// The work list of a ragged problem: its (query tile, batch) items that
+// join some key, by their key-tile counts, largest first. The lists of the
+// last few shapes (lengths, extents and conditions) are kept: a training
+// loop asks for the same one at every step.
+std::vector<int2> ragged_work(const AttentionProblem& p) {
+  std::vector<int64_t> key = {p.batches, p.lnx, p.lnj, p.mask.n, (int64_t)p.xlen_host.size(),
+                              (int64_t)p.jlen_host.size()};
+  for (int i = 0; i < p.mask.n; i++) {
+    key.push_back(p.mask.cmp[i]);
+    key.push_back(p.mask.off[i]);
+  }
+  key.insert(key.end(), p.xlen_host.begin(), p.xlen_host.end());
+  key.insert(key.end(), p.jlen_host.begin(), p.jlen_host.end());
+  static std::mutex lock;
+  static std::vector<std::pair<std::vector<int64_t>, std::vector<int2>>> kept;  // most recent last
+  {
+    std::lock_guard<std::mutex> g(lock);
+    for (size_t i = 0; i < kept.size(); i++)
+      if (kept[i].first == key) {
+        auto hit = kept[i];
+        kept.erase(kept.begin() + (int64_t)i);
+        kept.push_back(hit);
+        return hit.second;
+      }
+  }
+  Mask hm = p.mask;
+  hm.xlen = p.xlen_host.empty() ? nullptr : p.xlen_host.data();
+  hm.jlen = p.jlen_host.empty() ? nullptr : p.jlen_host.data();
+  std::vector<std::pair<int64_t, int2>> work;
+  for (int64_t w = 0; w < p.batches; w++) {
+    const int64_t rows = hm.xlen ? hm.xlen[w] : p.lnx;
+    for (int64_t xt = 0; xt * AM < rows; xt++) {
+      int64_t first = INT64_MAX, last = INT64_MIN;
+      for (int64_t r = xt * AM; r < std::min(rows, xt * AM + AM); r++) {
+        int64_t lo, hi;
+        allowed(hm, w * p.lnx + r, lo, hi);
+        if (lo < hi) {
+          first = std::min(first, lo - w * p.lnj);
+          last = std::max(last, hi - w * p.lnj);
+        }
+      }
+      if (first < last) work.push_back({(last + AJ - 1) / AJ - first / AJ, make_int2((int)xt, (int)w)});
+    }
+  }
+  std::stable_sort(work.begin(), work.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+  std::vector<int2> list;
+  for (auto& x : work) list.push_back(x.second);
+  std::lock_guard<std::mutex> g(lock);
+  kept.emplace_back(std::move(key), list);
+  if (kept.size() > 8) kept.erase(kept.begin());
+  return list;
+}
+
 }  // namespace
 
 AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int slices, cudaStream_t stream) {
@@ -579,9 +633,10 @@ AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int sl
   EF_CUDA(cudaMemsetAsync(status, 0, 32, stream));
   const int init[4] = {INT_MIN, INT_MIN, INT_MIN, INT_MIN};
   EF_CUDA(cudaMemcpyAsync(status + 2, init, 16, cudaMemcpyHostToDevice, stream));
-  slice_rows_into(S, p.q, W, p.lnx, p.ne, p.ne, lnx_pad, d_pad, eq, qd, status, stream);
-  slice_rows_into(S, p.k, W, p.lnj, p.ne, p.ne, lnj_pad, d_pad, ek, kd, status, stream);
-  slice_cols_into(S, p.v, W, p.lnj, p.ny, ny_pad, lnj_pad, colmax, ev, vd, status, stream);
+  // Ragged batches: the padding rows are not read (their digits are zeros).
+  slice_rows_into(S, p.q, W, p.lnx, p.ne, p.ne, lnx_pad, d_pad, eq, qd, status, stream, p.mask.xlen);
+  slice_rows_into(S, p.k, W, p.lnj, p.ne, p.ne, lnj_pad, d_pad, ek, kd, status, stream, p.mask.jlen);
+  slice_cols_into(S, p.v, W, p.lnj, p.ny, ny_pad, lnj_pad, colmax, ev, vd, status, stream, p.mask.jlen);
   exponent_range(eq, W * lnx_pad, status + 2, stream);
   exponent_range(ek, W * lnj_pad, status + 4, stream);
   ctx.kernels += 6;
@@ -637,28 +692,7 @@ AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int sl
   // with the most key tiles first.
   DeviceBuffer<int2> items;
   if (!p.xlen_host.empty() || !p.jlen_host.empty()) {
-    Mask hm = p.mask;
-    hm.xlen = p.xlen_host.empty() ? nullptr : p.xlen_host.data();
-    hm.jlen = p.jlen_host.empty() ? nullptr : p.jlen_host.data();
-    std::vector<std::pair<int64_t, int2>> work;
-    for (int64_t w = 0; w < W; w++) {
-      const int64_t rows = hm.xlen ? hm.xlen[w] : p.lnx;
-      for (int64_t xt = 0; xt * AM < rows; xt++) {
-        int64_t first = INT64_MAX, last = INT64_MIN;
-        for (int64_t r = xt * AM; r < std::min(rows, xt * AM + AM); r++) {
-          int64_t lo, hi;
-          allowed(hm, w * p.lnx + r, lo, hi);
-          if (lo < hi) {
-            first = std::min(first, lo - w * p.lnj);
-            last = std::max(last, hi - w * p.lnj);
-          }
-        }
-        if (first < last) work.push_back({(last + AJ - 1) / AJ - first / AJ, make_int2((int)xt, (int)w)});
-      }
-    }
-    std::stable_sort(work.begin(), work.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-    std::vector<int2> list;
-    for (auto& x : work) list.push_back(x.second);
+    const std::vector<int2> list = ragged_work(p);
     if (list.empty()) return ATTENTION_DONE;
     items.allocate(list.size(), stream);
     EF_CUDA(cudaMemcpyAsync(items.get(), list.data(), list.size() * sizeof(int2), cudaMemcpyHostToDevice, stream));

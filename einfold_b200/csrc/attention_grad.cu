@@ -1033,13 +1033,15 @@ bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd,
   EF_CUDA(cudaMemsetAsync(status, 0, 32, s));
   const int init[8] = {INT_MIN, INT_MIN, INT_MIN, INT_MIN, INT_MIN, INT_MIN, INT_MIN, INT_MIN};
   EF_CUDA(cudaMemcpyAsync(status + 8, init, 32, cudaMemcpyHostToDevice, s));
-  slice_rows_into(S, f.q, W, lq, d, d, lq_pad, 64, Qr.e, Qr.d, status, s);
-  slice_rows_into(S, g.d_out, W, lq, dv, dv, lq_pad, 64, dOr.e, dOr.d, status, s);
-  slice_rows_into(S, f.k, W, lk, d, d, lk_pad, 64, Kr.e, Kr.d, status, s);
-  slice_rows_into(S, f.v, W, lk, dv, dv, lk_pad, 64, Vr.e, Vr.d, status, s);
-  slice_cols_into(S, g.d_out, W, lq, dv, 64, lq_pad, colmax, dOc.e, dOc.d, status, s);
-  slice_cols_into(S, f.q, W, lq, d, 64, lq_pad, colmax, Qc.e, Qc.d, status, s);
-  slice_cols_into(S, f.k, W, lk, d, 64, lk_pad, colmax, Kc.e, Kc.d, status, s);
+  // Ragged batches: the padding rows are not read (their digits are zeros).
+  const int64_t *xl = f.mask.xlen, *jl = f.mask.jlen;
+  slice_rows_into(S, f.q, W, lq, d, d, lq_pad, 64, Qr.e, Qr.d, status, s, xl);
+  slice_rows_into(S, g.d_out, W, lq, dv, dv, lq_pad, 64, dOr.e, dOr.d, status, s, xl);
+  slice_rows_into(S, f.k, W, lk, d, d, lk_pad, 64, Kr.e, Kr.d, status, s, jl);
+  slice_rows_into(S, f.v, W, lk, dv, dv, lk_pad, 64, Vr.e, Vr.d, status, s, jl);
+  slice_cols_into(S, g.d_out, W, lq, dv, 64, lq_pad, colmax, dOc.e, dOc.d, status, s, xl);
+  slice_cols_into(S, f.q, W, lq, d, 64, lq_pad, colmax, Qc.e, Qc.d, status, s, xl);
+  slice_cols_into(S, f.k, W, lk, d, 64, lk_pad, colmax, Kc.e, Kc.d, status, s, jl);
   exponent_range(Qr.e, W * lq_pad, status + 8, s);
   exponent_range(Kr.e, W * lk_pad, status + 10, s);
   exponent_range(Vr.e, W * lk_pad, status + 12, s);

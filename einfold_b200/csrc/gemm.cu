@@ -215,14 +215,14 @@ template <int S>
 __global__ void __launch_bounds__(256) slice_rows(const double* __restrict__ x, int64_t batches, int64_t rows,
                                                   int64_t k, int64_t ld, int64_t rows_pad, int64_t k_pad,
                                                   int32_t* __restrict__ e_out, int8_t* __restrict__ digits,
-                                                  int* status) {
+                                                  int* status, const int64_t* __restrict__ lens) {
   __shared__ double red[8];
   __shared__ int ex_s;
   const int64_t slab = rows_pad * k_pad;
   for (int64_t g = blockIdx.x; g < batches * rows_pad; g += gridDim.x) {
     const int64_t w = g / rows_pad, r = g % rows_pad;
     const double* row = x + (w * rows + r) * ld;
-    const bool live = r < rows;
+    const bool live = r < rows && (!lens || r < lens[w]);
     double m = 0.0;
     bool bad = false;
     if (live) {
@@ -282,14 +282,14 @@ template <int S>
 __global__ void __launch_bounds__(256) slice_short_rows(const double* __restrict__ x, int64_t batches, int64_t rows,
                                                         int64_t k, int64_t ld, int64_t rows_pad, int64_t k_pad,
                                                         int32_t* __restrict__ e_out, int8_t* __restrict__ digits,
-                                                        int* status) {
+                                                        int* status, const int64_t* __restrict__ lens) {
   const int lane = threadIdx.x & 31;
   const int64_t slab = rows_pad * k_pad;
   for (int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < batches * rows_pad;
        g += ((int64_t)gridDim.x * blockDim.x) >> 5) {
     const int64_t w = g / rows_pad, r = g % rows_pad;
     const double* row = x + (w * rows + r) * ld;
-    const bool live = r < rows;
+    const bool live = r < rows && (!lens || r < lens[w]);
     double v[4];
     double m = 0.0;
     bool bad = false;
@@ -339,7 +339,7 @@ template <int S>
 __global__ void __launch_bounds__(256) slice_half_warp_rows(const double* __restrict__ x, int64_t batches,
                                                             int64_t rows, int64_t k, int64_t ld, int64_t rows_pad,
                                                             int32_t* __restrict__ e_out, int8_t* __restrict__ digits,
-                                                            int* status) {
+                                                            int* status, const int64_t* __restrict__ lens) {
   constexpr int64_t kPad = 64;
   const int lane = threadIdx.x & 31, l16 = lane & 15, half = lane >> 4;
   const int64_t slab = rows_pad * kPad, total = batches * rows_pad;
@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(256) slice_half_warp_rows(const double* __rest
        gp += ((int64_t)gridDim.x * blockDim.x) >> 5) {
     const int64_t g = gp * 2 + half;
     const int64_t w = g / rows_pad, r = g % rows_pad;
-    const bool live = g < total && r < rows;
+    const bool live = g < total && r < rows && (!lens || r < lens[w]);
     const double* row = x + (w * rows + r) * ld;
     const int64_t c0 = (int64_t)l16 * 4;
     double v[4];
@@ -394,20 +394,21 @@ __global__ void __launch_bounds__(256) slice_half_warp_rows(const double* __rest
 // Launches the row slicer that suits the row length.
 template <int S>
 void launch_slice_rows(const double* x, int64_t batches, int64_t rows, int64_t k, int64_t ld, int64_t rows_pad,
-                       int64_t k_pad, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream) {
+                       int64_t k_pad, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream,
+                       const int64_t* lens = nullptr) {
   if constexpr (S <= 6) {
     if (k_pad == 64) {
       slice_half_warp_rows<S><<<blocks_for((uint64_t)(batches * rows_pad) * 16, 256), 256, 0, stream>>>(
-          x, batches, rows, k, ld, rows_pad, e_out, digits, status);
+          x, batches, rows, k, ld, rows_pad, e_out, digits, status, lens);
       return;
     }
   }
   if (k_pad <= 128)
     slice_short_rows<S><<<blocks_for((uint64_t)(batches * rows_pad) * 32, 256), 256, 0, stream>>>(
-        x, batches, rows, k, ld, rows_pad, k_pad, e_out, digits, status);
+        x, batches, rows, k, ld, rows_pad, k_pad, e_out, digits, status, lens);
   else
     slice_rows<S><<<blocks_for((uint64_t)(batches * rows_pad), 1, 148 * 8), 256, 0, stream>>>(
-        x, batches, rows, k, ld, rows_pad, k_pad, e_out, digits, status);
+        x, batches, rows, k, ld, rows_pad, k_pad, e_out, digits, status, lens);
 }
 
 // The largest magnitude of each column of x [batches][k][n] (row-major):
@@ -415,11 +416,11 @@ void launch_slice_rows(const double* x, int64_t batches, int64_t rows, int64_t k
 // (non-negative doubles order as their bits). Status bit 1 if a value isn't
 // finite. `colmax` must start at zero.
 __global__ void col_max(const double* __restrict__ x, int64_t batches, int64_t k, int64_t n,
-                        unsigned long long* __restrict__ colmax, int* status) {
+                        unsigned long long* __restrict__ colmax, int* status, const int64_t* __restrict__ lens) {
   const int64_t col = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t w = blockIdx.z;
   const int64_t rows_per = (k + gridDim.y - 1) / gridDim.y;
-  const int64_t r0 = (int64_t)blockIdx.y * rows_per, r1 = min(k, r0 + rows_per);
+  const int64_t r0 = (int64_t)blockIdx.y * rows_per, r1 = min(lens ? min(k, lens[w]) : k, r0 + rows_per);
   if (col >= n) return;
   double m = 0.0;
   bool bad = false;
@@ -440,15 +441,17 @@ __global__ void col_max(const double* __restrict__ x, int64_t batches, int64_t k
 template <int S>
 __global__ void __launch_bounds__(256) col_digits(const double* __restrict__ x, int64_t k, int64_t n, int64_t n_pad,
                                                   int64_t k_pad, const unsigned long long* __restrict__ colmax,
-                                                  int32_t* __restrict__ e_out, int8_t* __restrict__ digits) {
+                                                  int32_t* __restrict__ e_out, int8_t* __restrict__ digits,
+                                                  const int64_t* __restrict__ lens) {
   __shared__ double tile[64][65];
   const int64_t w = blockIdx.z;
   const int64_t k0 = (int64_t)blockIdx.y * 64, n0 = (int64_t)blockIdx.x * 64;
   const double* X = x + w * k * n;
+  const int64_t kl = lens ? min(k, lens[w]) : k;
   for (int i = threadIdx.x; i < 64 * 64; i += 256) {
     const int kr = i / 64, nc = i % 64;
     const int64_t gk = k0 + kr, gn = n0 + nc;
-    double v = (gk < k && gn < n) ? X[gk * n + gn] : 0.0;
+    double v = (gk < kl && gn < n) ? X[gk * n + gn] : 0.0;
     if (!(fabs(v) <= 1.7976931348623157e308)) v = 0.0;
     tile[kr][nc] = v;
   }
@@ -678,9 +681,10 @@ int split_run(Context& ctx, const double* a, const double* b, bool b_natural, do
     EF_CUDA(cudaMemsetAsync(sc.colmax, 0, (size_t)(batches * n) * 8, stream));
     const unsigned splits = (unsigned)std::min<int64_t>(64, (k + 127) / 128);
     col_max<<<dim3((unsigned)((n + 255) / 256), splits, (unsigned)batches), 256, 0, stream>>>(b, batches, k, n,
-                                                                                             sc.colmax, sc.status);
+                                                                                             sc.colmax, sc.status,
+                                                                                             nullptr);
     col_digits<S><<<dim3((unsigned)(n_pad / 64), (unsigned)(k_pad / 64), (unsigned)batches), 256, 0, stream>>>(
-        b, k, n, n_pad, k_pad, sc.colmax, sc.eb, sc.db);
+        b, k, n, n_pad, k_pad, sc.colmax, sc.eb, sc.db, nullptr);
     ctx.kernels += 2;
   } else {
     launch_slice_rows<S>(b, batches, n, k, k, n_pad, k_pad, sc.eb, sc.db, sc.status, stream);
@@ -802,27 +806,30 @@ void exponent_range(const int32_t* e, int64_t n, int* out, cudaStream_t stream) 
 }
 
 void slice_rows_into(int S, const double* x, int64_t batches, int64_t rows, int64_t k, int64_t ld, int64_t rows_pad,
-                     int64_t k_pad, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream) {
+                     int64_t k_pad, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream,
+                     const int64_t* lens) {
   if (batches <= 0 || rows_pad <= 0) return;
   dispatch_slices(S, [&](auto SS) {
-    launch_slice_rows<decltype(SS)::value>(x, batches, rows, k, ld, rows_pad, k_pad, e_out, digits, status, stream);
+    launch_slice_rows<decltype(SS)::value>(x, batches, rows, k, ld, rows_pad, k_pad, e_out, digits, status, stream,
+                                           lens);
   });
   EF_LAUNCH_CHECK();
 }
 
 void slice_cols_into(int S, const double* x, int64_t batches, int64_t k, int64_t n, int64_t n_pad, int64_t k_pad,
-                     unsigned long long* colmax, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream) {
+                     unsigned long long* colmax, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream,
+                     const int64_t* lens) {
   if (batches <= 0 || n_pad <= 0 || k_pad <= 0) return;
   if (n_pad % 64 || k_pad % 64) fail(EINFOLD_INVALID, "column digits need multiples of 64");
   EF_CUDA(cudaMemsetAsync(colmax, 0, (size_t)(batches * n) * 8, stream));
   if (n > 0 && k > 0) {
     const unsigned splits = (unsigned)std::min<int64_t>(64, (k + 127) / 128);
     col_max<<<dim3((unsigned)((n + 255) / 256), splits, (unsigned)batches), 256, 0, stream>>>(x, batches, k, n, colmax,
-                                                                                             status);
+                                                                                             status, lens);
   }
   dispatch_slices(S, [&](auto SS) {
     col_digits<decltype(SS)::value><<<dim3((unsigned)(n_pad / 64), (unsigned)(k_pad / 64), (unsigned)batches), 256, 0,
-                                      stream>>>(x, k, n, n_pad, k_pad, colmax, e_out, digits);
+                                      stream>>>(x, k, n, n_pad, k_pad, colmax, e_out, digits, lens);
   });
   EF_LAUNCH_CHECK();
 }

@@ -37,15 +37,20 @@ void fp64_gemm(Context& ctx, const double* a, const uint32_t* held, const double
 // themselves. Rows of x [batches][rows][k] (leading dimension ld) become S
 // int8 digit planes digits[(w·S + s)][r][kk] for r < rows_pad, kk < k_pad
 // (zeros beyond), each row under a power-of-two scale 2^e with e in
-// e_out[w·rows_pad + r]; status bit 1 if a value isn't finite.
+// e_out[w·rows_pad + r]; status bit 1 if a value isn't finite. With
+// `lens` (device, one per batch), rows at or past lens[w] are not read and
+// slice to zeros.
 void slice_rows_into(int S, const double* x, int64_t batches, int64_t rows, int64_t k, int64_t ld, int64_t rows_pad,
-                     int64_t k_pad, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream);
+                     int64_t k_pad, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream,
+                     const int64_t* lens = nullptr);
 // Columns of x [batches][k][n] become K-major digit planes
 // digits[(w·S + s)][col][kk] for col < n_pad and kk < k_pad (both multiples
 // of 64), each column under its own power of two, e_out[w·n_pad + col];
-// colmax is scratch of batches·n words.
+// colmax is scratch of batches·n words; with `lens`, rows of x (positions
+// along k) at or past lens[w] count as zeros and are not read.
 void slice_cols_into(int S, const double* x, int64_t batches, int64_t k, int64_t n, int64_t n_pad, int64_t k_pad,
-                     unsigned long long* colmax, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream);
+                     unsigned long long* colmax, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream,
+                     const int64_t* lens = nullptr);
 // out[0] = max e[i] and out[1] = max -e[i] over n exponents, folded into
 // what out already holds (INT_MIN for a fresh pair).
 void exponent_range(const int32_t* e, int64_t n, int* out, cudaStream_t stream);
