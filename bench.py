@@ -456,6 +456,7 @@ def run_ours(args):
 
     ranking = _ranking(hbm, basis) if not args.no_ranking else None
     ragged = _ragged() if not args.no_ragged else None
+    sparse = _sparse(cpu=rank == 0 and world == 1 and not args.no_cpu) if not args.no_sparse else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -488,6 +489,7 @@ def run_ours(args):
             "roofline": roofline,
             "ranking": ranking,
             "ragged": ragged,
+            "sparse": sparse,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches[0],
@@ -585,6 +587,92 @@ def _ragged():
     return out
 
 
+def _sparse_tables():
+    """The sorting path's tables at 1/40 of their size: a(i, j, v) and b(j,
+    k, v), 50,000 rows each; i and k 16-hex-digit strings from 50,000
+    distinct, j 63-bit hashes from a pool of 200,000 drawn with Zipf(1.1)
+    frequencies, v normal(0, 1); SplitMix64 (seed 0, salts 11-17)."""
+    import numpy as np
+    import pyarrow as pa
+
+    from einfold_b200 import synthetic as S
+
+    n, pool, names = 50_000, 200_000, 50_000
+
+    def units(salt, m):
+        return S.units(SEED, salt, m, device="cpu").to(dtype=__import__("torch").float64).numpy()
+
+    def hexes(salt):
+        words = S.u64(SEED, salt, names, device="cpu").numpy().view(np.uint64)
+        return np.array([f"{int(x):016x}" for x in words], dtype=object)
+
+    hashes = S.u64(SEED, 13, pool, device="cpu").numpy().view(np.uint64) >> np.uint64(1)
+    cdf = np.cumsum(np.arange(1, pool + 1, dtype=np.float64) ** -1.1)
+    cdf /= cdf[-1]
+
+    def joins(salt):
+        return hashes[np.searchsorted(cdf, units(salt, n), side="right").clip(0, pool - 1)].astype(np.int64)
+
+    def normal(salt):
+        u1, u2 = units(salt, n), units(salt + 100, n)
+        return np.sqrt(-2.0 * np.log1p(-u1)) * np.cos(2 * np.pi * u2)
+
+    ia, kb = hexes(11), hexes(12)
+    pick_a = (units(14, n) * names).astype(np.int64).clip(0, names - 1)
+    pick_b = (units(15, n) * names).astype(np.int64).clip(0, names - 1)
+    ja, jb = joins(16), joins(17)
+    a = pa.record_batch([pa.array(ia[pick_a], pa.string()), pa.array(ja), pa.array(normal(18))], names=["i", "j", "v"])
+    b = pa.record_batch([pa.array(jb), pa.array(kb[pick_b], pa.string()), pa.array(normal(19))], names=["j", "k", "v"])
+    ua, ca = np.unique(ja, return_counts=True)
+    ub, cb = np.unique(jb, return_counts=True)
+    common, xa, xb = np.intersect1d(ua, ub, return_indices=True)
+    pairs = int((ca[xa].astype(np.int64) * cb[xb].astype(np.int64)).sum())
+    return a, b, pairs
+
+
+def _sparse(cpu=False):
+    """The discrimination fold (ranking, counting sorts, the Gustavson
+    product, grouped output) on the sorting path's tables scaled to 50,000
+    rows an operand, result left in HBM, timed with CUDA events: pair
+    products (one per pair of rows joining on j) per second."""
+    import torch
+
+    from einfold_b200 import kernels as K
+
+    a, b, pairs = _sparse_tables()
+    f = _matmul_fold()
+    opts = K.Options(result_on_device=True)
+    ra, rb = K.Relation(a.schema, [a]), K.Relation(b.schema, [b])
+    times, groups, alg = [], 0, None
+    for _ in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        got = K.fold(f, ra, rb, options=opts)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+        alg = got.algorithm.name.lower()
+        groups = sum(batch.rows for batch in got.batches)
+        for batch in got.batches:
+            batch.release()
+    ms = statistics.median(times[1:])
+    out = {"rows_per_operand": a.num_rows, "pairs": pairs, "groups": groups, "algorithm": alg, "ms": ms,
+           "gpairs_per_s": pairs / ms / 1e6, "host_to_device": "the Arrow tables are copied in each call"}
+    if cpu:
+        # The CPU baseline leg: the oracle's restatement of discriminate::fold
+        # (one host thread), on the same tables.
+        from oracle import oracle
+
+        oracle.build()
+        t0 = time.perf_counter()
+        want = oracle.fold(f, a.schema, [a], b.schema, [b], None, oracle.schema(f, [a.schema, b.schema]))
+        sec = time.perf_counter() - t0
+        out["cpu_oracle"] = {"seconds": sec, "gpairs_per_s": pairs / sec / 1e9, "cores": 1,
+                             "groups": sum(x.num_rows for x in want.batches)}
+    return out
+
+
 def _profiled_traffic(component):
     """DRAM bytes per step of a component's product kernel, from the committed
     ncu summary (`traffic_bytes_per_launch:` line), or None."""
@@ -611,6 +699,7 @@ def main():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-ranking", action="store_true")
     p.add_argument("--no-ragged", action="store_true")
+    p.add_argument("--no-sparse", action="store_true")
     args = p.parse_args()
     if args.impl == "reference":
         run_reference(args)

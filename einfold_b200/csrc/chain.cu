@@ -147,6 +147,7 @@ Relation as_relation(const std::vector<OutBatch>& batches, const std::vector<Fie
       c.null_count = oc.null_count;
       c.validity = oc.null_count ? (const uint8_t*)oc.validity.ptr : nullptr;
       c.values = (const uint8_t*)oc.values.ptr;
+      c.data = (const uint8_t*)oc.data.ptr;
       c.device = true;
       b.columns.push_back(c);
     }

@@ -343,6 +343,13 @@ __global__ void gather_bytes(const uint8_t* __restrict__ data, const int64_t* __
   }
 }
 
+// Arrow Utf8/Binary offsets: the int64 offsets narrowed to int32 (the
+// caller checked that the total fits).
+__global__ void narrow_offsets(const int64_t* __restrict__ in, int64_t n, int32_t* __restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (int32_t)in[i];
+}
+
 // A domain row's value: its (x, y) group's sum when the group exists with a
 // value, else the default (discriminate.rs:613-649).
 __global__ void domain_lookup(int64_t rows, const uint32_t* __restrict__ xr, const uint32_t* __restrict__ yr,
@@ -776,16 +783,16 @@ FoldOutput discriminate_fold(Context& ctx, const FoldD& f, const Relation& a, co
         gather_valid<<<blocks_for(groups, 256), 256, 0, s>>>(src.valid.get(), first, g, groups, cvalid.get(), cn.get());
       }
       const bool large = src.kind == Kind::LargeUtf8 || src.kind == Kind::LargeBinary;
-      HostBuffer ho = to_host(ctx, offs.get(), (size_t)(groups + 1) * 8);
       if (large) {
-        c.values = Buffer(std::move(ho));
+        c.values = result_buffer(ctx, offs, (size_t)(groups + 1) * 8, o.result_on_device);
       } else {
         if (total > INT32_MAX) fail(EINFOLD_COMPUTE, "string output over 2 GiB");
-        HostBuffer h32((size_t)(groups + 1) * 4);
-        for (int64_t q = 0; q <= groups; q++) h32.as<int32_t>()[q] = (int32_t)ho.as<int64_t>()[q];
-        c.values = Buffer(std::move(h32));
+        DeviceBuffer<int32_t> o32((size_t)groups + 1, s);
+        narrow_offsets<<<blocks_for((uint64_t)groups + 1, 256), 256, 0, s>>>(offs.get(), groups + 1, o32.get());
+        ctx.kernels++;
+        c.values = result_buffer(ctx, o32, (size_t)(groups + 1) * 4, o.result_on_device);
       }
-      c.data = Buffer(to_host(ctx, bytes.get(), (size_t)total));
+      c.data = result_buffer(ctx, bytes, (size_t)total, o.result_on_device);
     } else {
       const int width = width_of(src.kind) ? width_of(src.kind) : 1;
       DeviceBuffer<uint8_t> vals((size_t)(groups ? groups * width : 1), s);
