@@ -107,8 +107,8 @@ __global__ void __launch_bounds__(kThreads) chunk_scatter(const uint64_t* __rest
   // Byte i: item i's group size; then (low word) the warp's first place
   // among the tile's keys of the digit.
   __shared__ __align__(16) uint64_t counts[WARPS][256];
-  __shared__ unsigned int tile_start[256];
   __shared__ long long running[256];
+  __shared__ long long dbase[256];  // a digit's destination minus its first place in the tile
   __shared__ __align__(8) uint64_t bar[2];
   typedef cub::BlockScan<unsigned int, kThreads> Scan;
   __shared__ typename Scan::TempStorage tmp;
@@ -204,13 +204,17 @@ __global__ void __launch_bounds__(kThreads) chunk_scatter(const uint64_t* __rest
     }
     unsigned int ex;
     Scan(tmp).ExclusiveSum(total, ex);
-    tile_start[tid] = ex;
+    // Each warp's first place among the tile's keys of this digit, and the
+    // digit's destination base, so that each key needs one lookup.
+#pragma unroll
+    for (int w = 0; w < WARPS; w++) counts[w][tid] += ex;
+    dbase[tid] = running[tid] - (long long)ex;
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < ITEMS; i++) {
       const int d = digit[i];
       if (d < 256) {
-        const unsigned pos = tile_start[d] + (unsigned)counts[warp][d] + local[i];
+        const unsigned pos = (unsigned)counts[warp][d] + local[i];
 #pragma unroll
         for (int w = 0; w < W; w++) skeys(s)[w * TILE + pos] = key[i][w];
         svals(s)[pos] = val[i];
@@ -220,7 +224,7 @@ __global__ void __launch_bounds__(kThreads) chunk_scatter(const uint64_t* __rest
     for (int j = tid; j < count; j += kThreads) {
       const uint64_t wd = skeys(s)[word * TILE + j];
       const int d = (int)((wd >> shift) & 255);
-      const long long dst = running[d] + (j - (long long)tile_start[d]);
+      const long long dst = dbase[d] + j;
 #pragma unroll
       for (int w = 0; w < W; w++) kout[(int64_t)w * ldo + dst] = skeys(s)[w * TILE + j];
       if (vout) vout[dst] = svals(s)[j];
