@@ -4,6 +4,7 @@
     python -m einfold_b200.cases product --n 4096
     python -m einfold_b200.cases rank --n 67108864 [--repeat 3]
     python -m einfold_b200.cases ragged [--groups 64 --d 128 --window 512 --repeat 3]
+    python -m einfold_b200.cases sparse
 
 ``attention`` runs the split causal attention forward (and backward) over
 q, k, v normal(0, 1/8) and d_out normal(0, 1) (SplitMix64, seed 0);
@@ -13,8 +14,9 @@ pool of n/2, so keys repeat) with einfold_rank_words and prints the keys
 per second of the last of `repeat` runs, timed with CUDA events;
 ``ragged`` runs the split attention forward over ragged batches (lengths
 log-uniform in [128, 8192], a window of |tq - tk| <= radius) and prints
-the FLOP rate on the allowed pairs. Each prints one line and exits 0 when
-the kernels ran.
+the FLOP rate on the allowed pairs; ``sparse`` runs the discrimination
+fold once on the sorting path's tables at 1/40 size (the bench's). Each
+prints one line and exits 0 when the kernels ran.
 """
 from __future__ import annotations
 
@@ -121,6 +123,24 @@ def ragged(groups: int, d: int, radius: int, repeat: int) -> None:
           f"{flop / ms / 1e9:.2f} TFLOP/s (attention kernel {last_call.product_ms:.3f} ms)")
 
 
+def sparse() -> None:
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+
+    from . import kernels as K
+
+    a, b, pairs = bench._sparse_tables()
+    got = K.fold(bench._matmul_fold(), K.Relation(a.schema, [a]), K.Relation(b.schema, [b]),
+                 options=K.Options(result_on_device=True))
+    rows = sum(batch.rows for batch in got.batches)
+    for batch in got.batches:
+        batch.release()
+    print(f"sparse: {pairs} pair products, {rows} groups ({got.algorithm.name.lower()})")
+
+
 def main() -> None:
     p = argparse.ArgumentParser()
     sub = p.add_subparsers(dest="case", required=True)
@@ -136,6 +156,7 @@ def main() -> None:
     pg.add_argument("--d", type=int, default=128)
     pg.add_argument("--window", type=int, default=512)
     pg.add_argument("--repeat", type=int, default=3)
+    sub.add_parser("sparse")
     pr = sub.add_parser("rank")
     pr.add_argument("--n", type=int, default=1 << 26)
     pr.add_argument("--repeat", type=int, default=3)
@@ -146,6 +167,8 @@ def main() -> None:
         rank(args.n, args.repeat)
     elif args.case == "ragged":
         ragged(args.groups, args.d, args.window, args.repeat)
+    elif args.case == "sparse":
+        sparse()
     else:
         product(args.n)
 

@@ -196,6 +196,8 @@ __global__ void __launch_bounds__(256) gustavson(int64_t nx, int64_t ny, const i
   uint32_t* reached = reached_all + (int64_t)blockIdx.x * words;
   uint32_t* valued = valued_all + (int64_t)blockIdx.x * words;
   __shared__ unsigned long long s_count;
+  typedef cub::BlockScan<int, 256> BlockScanInt;
+  __shared__ typename BlockScanInt::TempStorage scan_tmp;
   for (int64_t x = blockIdx.x; x < nx; x += gridDim.x) {
     for (int64_t i = a_start[x]; i < a_start[x + 1]; i++) {
       const uint32_t z = a_z[i];
@@ -237,41 +239,33 @@ __global__ void __launch_bounds__(256) gustavson(int64_t nx, int64_t ny, const i
       __syncthreads();
       if (threadIdx.x == 0) group_count[x] = (int64_t)s_count;
     } else {
-      // Ordered emission: one warp walks the words in order, lanes spread
-      // over the set bits of each word by prefix counts.
-      if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        int64_t out = group_off[x];
-        for (int64_t w0 = 0; w0 < words; w0 += 32) {
-          const int64_t w = w0 + lane;
-          const uint32_t bits = w < words ? reached[w] : 0u;
-          const uint32_t vb = w < words ? valued[w] : 0u;
-          const int cnt = __popc(bits);
-          int pre = cnt;
-          for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, pre, o);
-            if (lane >= o) pre += t;
-          }
-          const int total = __shfl_sync(0xffffffffu, pre, 31);
-          int64_t pos = out + pre - cnt;
-          uint32_t b = bits;
-          while (b) {
-            const int k = __ffs(b) - 1;
-            b &= b - 1;
-            const uint32_t y = (uint32_t)(w * 32 + k);
-            gy[pos] = y;
-            const bool v = (vb >> k) & 1u;
-            gsum[pos] = v ? acc[y] : 0.0;
-            gvalued[pos] = v;
-            acc[y] = 0.0;
-            pos++;
-          }
-          if (w < words) {
-            reached[w] = 0;
-            valued[w] = 0;
-          }
-          out += total;
+      // Ordered emission by the whole block: each thread takes a run of
+      // consecutive words, a block scan of their set bits gives each run its
+      // first output position, so groups come out in y order as one walk
+      // would write them.
+      const int64_t per = (words + blockDim.x - 1) / blockDim.x;
+      const int64_t w0 = (int64_t)threadIdx.x * per, w1 = min(words, w0 + per);
+      int cnt = 0;
+      for (int64_t w = w0; w < w1; w++) cnt += __popc(reached[w]);
+      int before;
+      BlockScanInt(scan_tmp).ExclusiveSum(cnt, before);
+      int64_t pos = group_off[x] + before;
+      for (int64_t w = w0; w < w1; w++) {
+        uint32_t bits = reached[w];
+        const uint32_t vb = valued[w];
+        while (bits) {
+          const int k = __ffs(bits) - 1;
+          bits &= bits - 1;
+          const uint32_t y = (uint32_t)(w * 32 + k);
+          gy[pos] = y;
+          const bool v = (vb >> k) & 1u;
+          gsum[pos] = v ? acc[y] : 0.0;
+          gvalued[pos] = v;
+          acc[y] = 0.0;
+          pos++;
         }
+        reached[w] = 0;
+        valued[w] = 0;
       }
     }
     __syncthreads();
@@ -339,7 +333,12 @@ __global__ void gather_bytes(const uint8_t* __restrict__ data, const int64_t* __
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t r = first[g[i]];
     const int64_t b0 = off[r], len = off[r + 1] - b0, o = out_off[i];
-    for (int64_t b = 0; b < len; b++) out[o + b] = data[b0 + b];
+    if ((((uintptr_t)(data + b0) | (uintptr_t)(out + o) | (uint64_t)len) & 7) == 0) {
+      // Whole 8-byte words where the source, the destination and the length allow.
+      for (int64_t b = 0; b < len; b += 8) *(uint64_t*)(out + o + b) = *(const uint64_t*)(data + b0 + b);
+    } else {
+      for (int64_t b = 0; b < len; b++) out[o + b] = data[b0 + b];
+    }
   }
 }
 
@@ -633,7 +632,13 @@ FoldOutput discriminate_fold(Context& ctx, const FoldD& f, const Relation& a, co
 
   // Gustavson's product: count, offsets, fill.
   const int64_t words = (ny + 31) / 32;
-  int blocks = std::min<int64_t>(nx, (int64_t)ctx.sm_count * 4);
+  // Up to four blocks an SM, but their dense accumulators and bitmaps within
+  // 64 MB (at least a block an SM), so that the scattered updates stay in L2.
+  const uint64_t per_block = (uint64_t)(ny * 8 + words * 8);
+  int blocks = (int)std::min<int64_t>(
+      nx, std::max<int64_t>(ctx.sm_count, std::min<int64_t>((int64_t)ctx.sm_count * 4,
+                                                             (int64_t)((64ull << 20) / std::max<uint64_t>(per_block, 1)))));
+  blocks = std::max(blocks, 1);
   while (blocks > 1 && (uint64_t)blocks * (uint64_t)(ny * 8 + words * 8) > (4ull << 30)) blocks /= 2;
   budget.reserve(sat_mul((uint64_t)blocks, (uint64_t)(ny * 8 + words * 8)), "the discrimination algorithm's accumulators");
   DeviceBuffer<uint32_t> reached((size_t)(blocks * words), s), valued((size_t)(blocks * words), s);
