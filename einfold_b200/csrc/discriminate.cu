@@ -632,20 +632,23 @@ FoldOutput discriminate_fold(Context& ctx, const FoldD& f, const Relation& a, co
 
   // Gustavson's product: count, offsets, fill.
   const int64_t words = (ny + 31) / 32;
-  // Up to four blocks an SM, but their dense accumulators and bitmaps within
-  // 64 MB (at least a block an SM), so that the scattered updates stay in L2.
+  // The counting pass: up to four blocks an SM, each with two bitmaps of y.
+  // The filling pass: as many, but their dense accumulators and bitmaps
+  // within 64 MB (at least a block an SM), so the scattered updates stay in L2.
   const uint64_t per_block = (uint64_t)(ny * 8 + words * 8);
+  int count_blocks = (int)std::max<int64_t>(1, std::min<int64_t>(nx, (int64_t)ctx.sm_count * 4));
+  while (count_blocks > 1 && (uint64_t)count_blocks * (uint64_t)(words * 8) > (4ull << 30)) count_blocks /= 2;
   int blocks = (int)std::min<int64_t>(
-      nx, std::max<int64_t>(ctx.sm_count, std::min<int64_t>((int64_t)ctx.sm_count * 4,
-                                                             (int64_t)((64ull << 20) / std::max<uint64_t>(per_block, 1)))));
+      count_blocks, std::max<int64_t>(ctx.sm_count, (int64_t)((64ull << 20) / std::max<uint64_t>(per_block, 1))));
   blocks = std::max(blocks, 1);
-  while (blocks > 1 && (uint64_t)blocks * (uint64_t)(ny * 8 + words * 8) > (4ull << 30)) blocks /= 2;
-  budget.reserve(sat_mul((uint64_t)blocks, (uint64_t)(ny * 8 + words * 8)), "the discrimination algorithm's accumulators");
-  DeviceBuffer<uint32_t> reached((size_t)(blocks * words), s), valued((size_t)(blocks * words), s);
+  while (blocks > 1 && (uint64_t)blocks * per_block > (4ull << 30)) blocks /= 2;
+  budget.reserve(sat_add(sat_mul((uint64_t)blocks, (uint64_t)(ny * 8)), sat_mul((uint64_t)count_blocks, (uint64_t)(words * 8))),
+                 "the discrimination algorithm's accumulators");
+  DeviceBuffer<uint32_t> reached((size_t)(count_blocks * words), s), valued((size_t)(count_blocks * words), s);
   reached.zero();
   valued.zero();
   DeviceBuffer<int64_t> gcount((size_t)nx, s), goff((size_t)nx + 1, s);
-  gustavson<false><<<blocks, 256, 0, s>>>(nx, ny, a_start.get(), a_z.get(), a_f.get(), a_v.get(), b_start.get(),
+  gustavson<false><<<count_blocks, 256, 0, s>>>(nx, ny, a_start.get(), a_z.get(), a_f.get(), a_v.get(), b_start.get(),
                                           b_y.get(), b_f.get(), b_v.get(), nullptr, reached.get(), valued.get(),
                                           gcount.get(), nullptr, nullptr, nullptr, nullptr);
   ctx.kernels++;
