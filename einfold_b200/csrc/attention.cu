@@ -88,6 +88,7 @@ struct AttnArgs {
   int* status;  // bit 0: a guard fired; bit 1: a wait ran out
   unsigned long long* tiles;  // (row tile, key tile) pairs computed
   const int2* items;  // ragged batches: block i runs (query tile, batch) items[i]; null: the grid's
+  int reverse;        // the grid's query tiles from the last one (whose rows join the most keys) down
 };
 
 // The S levels of this thread's 4 TMEM columns at `col`.
@@ -139,7 +140,7 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // The longest rows of a causal mask first; ragged batches by their work list.
-  const int xt = a.items ? a.items[blockIdx.x].x : (int)(gridDim.x - 1 - blockIdx.x);
+  const int xt = a.items ? a.items[blockIdx.x].x : a.reverse ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
   const int w = a.items ? a.items[blockIdx.x].y : (int)blockIdx.y;
   const int64_t x_base = (int64_t)w * a.lnx;
 
@@ -688,6 +689,16 @@ AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int sl
   args.status = status + 1;
   args.tiles = tiles;
   dim3 grid((unsigned)(lnx_pad / AM), (unsigned)W);
+  {
+    // The query tiles whose rows join the most keys first: the last ones
+    // under a causal mask, the first ones when the mask runs the other way.
+    Mask m = p.mask;
+    m.xlen = m.jlen = nullptr;
+    int64_t lo0, hi0, lo1, hi1;
+    allowed(m, 0, lo0, hi0);
+    allowed(m, p.lnx - 1, lo1, hi1);
+    args.reverse = hi1 - lo1 >= hi0 - lo0;
+  }
   // Ragged batches: one block per query tile that joins some key, the tiles
   // with the most key tiles first.
   DeviceBuffer<int2> items;

@@ -85,6 +85,7 @@ struct GradArgs {
   int* status;
   unsigned long long* tiles;
   int w0;  // the first batch of this launch (blockIdx.y counts from it)
+  int reverse;  // row blocks from the last one (whose rows join the most columns) down
   // The d_k kernel's exports for the tile kernels (null: none), indexed by
   // the launch's own batches: P's digit tiles as the d_v kernel cuts them,
   // [batch][row block][column tile][S][128 rows][64 B] in the MMA's 64-byte
@@ -136,7 +137,7 @@ __global__ void __launch_bounds__(kGradThreads, 1)
   int* redp = (int*)(aux + 6144);        // [4][128] the same for P (d_k's export)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int rt = (int)(gridDim.x - 1 - blockIdx.x);
+  const int rt = a.reverse ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
   const int w = a.w0 + (int)blockIdx.y;
   const int64_t r_base = (int64_t)w * a.lr, c_base = (int64_t)w * a.lc;
 
@@ -532,7 +533,7 @@ __global__ void __launch_bounds__(kGradThreads, 1)
   int* red = (int*)(aux + 4096);  // [4][128]
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int rt = (int)(gridDim.x - 1 - blockIdx.x);
+  const int rt = a.reverse ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
   const int w = a.w0 + (int)blockIdx.y;
   const int64_t r_base = (int64_t)w * a.lr, c_base = (int64_t)w * a.lc;
 
@@ -933,6 +934,18 @@ __global__ void row_dots(int64_t n, int64_t dv, const double* __restrict__ d_out
 
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
+// Whether a batch's last rows join more columns than its first (causal
+// queries do; causal keys as rows the other way round): the blocks with the
+// most work then go first.
+bool last_rows_longest(Mask m, int64_t rows) {
+  if (rows <= 0) return true;
+  m.xlen = m.jlen = nullptr;
+  int64_t lo0, hi0, lo1, hi1;
+  allowed(m, 0, lo0, hi0);
+  allowed(m, rows - 1, lo1, hi1);
+  return hi1 - lo1 >= hi0 - lo0;
+}
+
 // The mask of keys as rows: each condition x <cmp> j + off as j <cmp'> x - off.
 Mask transposed(const Mask& m) {
   static const int mirror[4] = {2, 3, 0, 1};
@@ -1130,6 +1143,7 @@ bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd,
     a.y0 = 0;
     a.n_rb = a.lr_pad / GM;
     a.n_ct = a.lc_pad / GJ;
+    a.reverse = last_rows_longest(a.mask, a.lr);
   }
   // The tile path, while its exports fit in half the free memory (in chunks
   // of batches): d_k first, exporting P's digits and dS; then d_v and d_q
