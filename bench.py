@@ -113,6 +113,25 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def max_over_ranks(ms, dist, device):
+    """The slowest rank's time: every rank contributes its own and receives
+    the largest (an all-reduce of one value; the only collective of the
+    replicas besides the barriers)."""
+    if dist is None:
+        return ms
+    import torch
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_value(world, flop_per_step, steps, ms):
+    """TFLOP/s of the whole job: every rank runs `steps` steps of the same
+    work (weak scaling), in `ms` milliseconds on the slowest rank."""
+    return world * flop_per_step * steps / (ms / 1e3) / 1e12
+
+
 def _matmul_fold():
     from einfold_b200 import ir
 
@@ -374,14 +393,10 @@ def run_ours(args):
             step(record=True)
         t1.record()
         barrier()
-    ms = t0.elapsed_time(t1)
-    if dist is not None:
-        tt = torch.tensor([ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(t0.elapsed_time(t1), dist, dev)
     ms_per_step = ms / args.steps
     flops = FOLD + ATT_FWD + ATT_BWD
-    value = world * flops * args.steps / (ms / 1e3) / 1e12
+    value = replicas_value(world, flops, args.steps, ms)
 
     # End to end: the public API from pinned host memory, results read back.
     e2e = None
@@ -425,12 +440,8 @@ def run_ours(args):
             del del_res
         t1.record()
         barrier()
-        ems = t0.elapsed_time(t1)
-        if dist is not None:
-            tt = torch.tensor([ems], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ems = float(tt.item())
-        e2e = {"value": world * flops * e2e_steps / (ems / 1e3) / 1e12, "unit": "TFLOP/s",
+        ems = max_over_ranks(t0.elapsed_time(t1), dist, dev)
+        e2e = {"value": replicas_value(world, flops, e2e_steps, ems), "unit": "TFLOP/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
                "ms_per_step": ems / e2e_steps}
         del ha, hb, pinned, hq, hk, hv, hd, back
