@@ -144,12 +144,32 @@ class DeviceBatch:
             self.formats.append(s.children[i].contents.format)
 
     def column(self, i: int):
-        """Column i's values as a CUDA tensor sharing the result's memory."""
+        """Column i's values as a CUDA tensor sharing the result's memory
+        (fixed-width columns; see :meth:`strings` for string and binary)."""
         import torch
 
+        if self.formats[i] not in self._TYPESTR:
+            raise TypeError(f"column {i} has Arrow format {self.formats[i]!r}: use strings({i})")
         arr = self._res.batches[0].children[i].contents
         ptr = arr.buffers[1]
         return torch.as_tensor(_CudaArray(ptr or 0, self.rows, self._TYPESTR[self.formats[i]], self), device="cuda")
+
+    def strings(self, i: int):
+        """A string or binary column's Arrow offsets (rows + 1, int32, or int64
+        for the large kinds) and bytes (uint8) as CUDA tensors sharing the
+        result's memory."""
+        import torch
+
+        fmt = self.formats[i]
+        if fmt not in (b"u", b"z", b"U", b"Z"):
+            raise TypeError(f"column {i} has Arrow format {fmt!r}, not a string or binary one")
+        arr = self._res.batches[0].children[i].contents
+        wide = fmt in (b"U", b"Z")
+        offsets = torch.as_tensor(_CudaArray(arr.buffers[1] or 0, self.rows + 1, "<i8" if wide else "<i4", self),
+                                  device="cuda")
+        total = int(offsets[-1].item()) if self.rows else 0
+        data = torch.as_tensor(_CudaArray(arr.buffers[2] or 0, total, "|u1", self), device="cuda")
+        return offsets, data
 
     def null_count(self, i: int) -> int:
         return int(self._res.batches[0].children[i].contents.null_count)

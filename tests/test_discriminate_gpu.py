@@ -77,6 +77,35 @@ def test_string_keys_sort_as_bytes_and_null_groups():
     assert_same_rows(rows_of(got.batches), rows_of(want.batches), exact=True)
 
 
+def test_string_keys_kept_in_hbm_match_the_host_result():
+    # Results left in device memory keep string keys there too: the offsets
+    # and bytes read back through DeviceBatch.strings equal the host result.
+    rng = oracle.Rng.seeded(7, 0)
+    words = ["", "a", "ab", "0123456789abcdef", "fedcba9876543210", "é", "abc", "zz"]
+    n = 300
+    ia = [words[rng.below(len(words))] for _ in range(n)]
+    ja = [rng.below(15) for _ in range(n)]
+    jb = [rng.below(15) for _ in range(n)]
+    kb = [words[rng.below(len(words))] for _ in range(n)]
+    a, b = _keyed(ia, ja, list(rng.units(n)), jb, kb, list(rng.units(n)))
+    f = matmul_fold()
+    ra, rb = K.Relation(a[0].schema, a), K.Relation(b[0].schema, b)
+    host = rows_of(K.fold(f, ra, rb).batches)
+    dev = K.fold(f, ra, rb, options=K.Options(result_on_device=True)).batches[0]
+    try:
+        assert dev.rows == host.num_rows
+        for i in (0, 1):
+            offsets, data = dev.strings(i)
+            o, d = offsets.cpu().numpy(), bytes(data.cpu().numpy())
+            got = [d[o[r]:o[r + 1]].decode() for r in range(dev.rows)]
+            assert got == host.column(i).to_pylist()
+        assert np.array_equal(dev.column(2).cpu().numpy(), host.column(2).to_numpy())
+        with pytest.raises(TypeError):
+            dev.column(0)
+    finally:
+        dev.release()
+
+
 @pytest.mark.parametrize("equality", [E, ND])
 def test_null_join_keys_under_either_equality(equality):
     rng = oracle.Rng.seeded(4, 0)
