@@ -59,9 +59,17 @@ def _conditions(conditions: Conditions):
     return n, cmp, off
 
 
+def _stream(device: int) -> int:
+    """torch's current stream on `device` as the library's stream argument.
+    The legacy default stream (handle 0) goes as cudaStreamLegacy (1): a
+    null stream would mean the context's own stream, which does not wait
+    for work queued on the default one (the operands' copies, say)."""
+    return torch.cuda.current_stream(device).cuda_stream or 1
+
+
 def _call(fn, device: int, *args) -> _lib.Result:
     info = _lib.Result()
-    stream = torch.cuda.current_stream(device).cuda_stream
+    stream = _stream(device)
     st = fn(_lib.context(device), *args, ctypes.c_void_p(stream), ctypes.byref(info))
     if st == _lib.DECLINED:
         raise Declined(info.message.decode(errors="replace"))
@@ -199,7 +207,7 @@ def _gemm(a: torch.Tensor, b: torch.Tensor, b_transposed: bool, precision: Preci
     c = torch.empty((*lead, m, n), dtype=torch.float64, device=a.device)
     lib = _lib.load()
     device = a.device.index or 0
-    stream = ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+    stream = ctypes.c_void_p(_stream(device))
     if Precision(precision) == Precision.SPLIT:
         st = lib.einfold_split_gemm(_lib.context(device), a.data_ptr(), b.data_ptr(), c.data_ptr(), _batches(lead), m,
                                     n, kk, int(b_transposed), int(slices), stream)

@@ -378,6 +378,17 @@ def _collect(res: _lib.Result) -> List[pa.RecordBatch]:
         lib.einfold_result_release(ctypes.byref(res))
 
 
+def _after_torch(*relations) -> None:
+    """The Arrow entry points run on the context's own stream, which does not
+    wait for torch's: operands in HBM are first finished on torch's current
+    stream."""
+    for r in relations:
+        if isinstance(r, DeviceRelation):
+            import torch
+
+            torch.cuda.current_stream(r.device).synchronize()
+
+
 def _call(fn, *args) -> Optional[_lib.Result]:
     res = _lib.Result()
     status = fn(_lib.context(args[-1]), *args[:-1], ctypes.byref(res))
@@ -404,6 +415,7 @@ def fold(f: ir.Fold, a, b, domain=None, schema: Optional[pa.Schema] = None,
     """``einfold_kernels::fold`` (algorithm.rs:97-133): dense when its
     requirements hold, else discrimination."""
     options = options or Options()
+    _after_torch(a, b, domain)
     keep = _Keep()
     try:
         res = _call(_lib.load().einfold_fold, ctypes.byref(_fold_desc(f, keep)), ctypes.byref(_relation(a, keep)),
@@ -424,6 +436,7 @@ def fold_dense(f: ir.Fold, a, b, domain=None, schema: Optional[pa.Schema] = None
                options: Optional[Options] = None) -> Optional[List[pa.RecordBatch]]:
     """``einfold_kernels::fold_dense`` (algorithm.rs:52-62)."""
     options = options or Options()
+    _after_torch(a, b, domain)
     keep = _Keep()
     try:
         res = _call(_lib.load().einfold_fold_dense, ctypes.byref(_fold_desc(f, keep)),
@@ -439,6 +452,7 @@ def fold_chain(f: ir.Fold, operands: Sequence, schema: Optional[pa.Schema] = Non
                options: Optional[Options] = None) -> Optional[List[pa.RecordBatch]]:
     """``einfold_kernels::fold_chain`` (algorithm.rs:76-83)."""
     options = options or Options()
+    _after_torch(*operands)
     keep = _Keep()
     try:
         rels = keep.add(_array(_lib.Relation, [_relation(r, keep) for r in operands]))
@@ -453,6 +467,7 @@ def pipeline(p: ir.Pipeline, operands: Sequence, schema: Optional[pa.Schema] = N
              options: Optional[Options] = None) -> Optional[Piped]:
     """``einfold_kernels::pipeline`` (algorithm.rs:146-160) over ``[q, k, v]``."""
     options = options or Options()
+    _after_torch(*operands)
     keep = _Keep()
     try:
         rels = keep.add(_array(_lib.Relation, [_relation(r, keep) for r in operands]))

@@ -24,7 +24,13 @@
  * The lower entry points (einfold_rank_words, einfold_split_gemm,
  * einfold_fp64_gemm, einfold_attention_*) take device pointers and a CUDA
  * stream; they serve a caller that keeps its data in HBM, such as the
- * torch.autograd.Function in the Python package, and the benchmarks.
+ * torch.autograd.Function in the Python package, and the benchmarks. A
+ * NULL stream there means the context's own stream, which is created
+ * non-blocking: it does not wait for work queued on the legacy default
+ * stream. A caller whose operands are written on the default stream passes
+ * cudaStreamLegacy; one that writes them on another stream passes that
+ * stream. The Arrow entry points run on the context's stream: operands in
+ * HBM must be complete before the call.
  *
  * Every call is synchronous with respect to the host unless it takes a
  * stream. Calls on one context are serialized by the context; contexts on
