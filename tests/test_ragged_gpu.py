@@ -84,8 +84,10 @@ def test_ragged_gradients(precision, shape):
         qs, ks, vs = (x[w:w + 1, :t].clone().requires_grad_(True) for x in (q, k, v))
         alone = A.attention(qs, ks, vs, cond, scale, precision)
         (alone.nan_to_num() * up[w:w + 1, :t]).sum().backward()
+        # The split backward (d <= 64) gives the same bits as alone; the FP64 one within rounding.
+        form = precision if d <= 64 else Precision.FP64
         for name, a, b in (("q", qa.grad, qs.grad), ("k", ka.grad, ks.grad), ("v", va.grad, vs.grad)):
-            assert _same(a[w, :t], b[0], precision, tol=1e-12), f"d{name} of group {w}"
+            assert _same(a[w, :t], b[0], form, tol=1e-12), f"d{name} of group {w}"
             assert (a[w, t:] == 0).all(), f"d{name} past the length of group {w}"
 
 
