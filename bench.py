@@ -42,6 +42,10 @@ METRIC = "attn fwd+bwd & matmul fold TFLOP/s: split-BF16 vs FP64 GPU at equal er
 N = 8192
 B, H, T, D = 4, 16, 4096, 64
 SEED = 0
+# The split attention forward's launch schedules and graph launches, by the
+# codes the library reports.
+SCHEDULE_NAMES = {0: "grid", 1: "tiles", 2: "batches"}
+GRAPH_NAMES = {0: "direct", 1: "replayed", 2: "updated", 3: "instantiated"}
 PAIRS = B * H * T * (T + 1) // 2
 ATT_FWD = 4.0 * D * PAIRS
 ATT_BWD = 10.0 * D * PAIRS
@@ -317,10 +321,14 @@ def run_ours(args):
     # the kernels launched.
     stats = {"fold": [], "attn_fwd": [], "attn_bwd": []}
     launches = [0]
+    fwd_launch = {}
 
     def note(name):
         stats[name].append((K.last_call.product_ms, K.last_call.product_ops))
         launches[0] += K.last_call.kernels_launched
+        if name == "attn_fwd":
+            fwd_launch.update(schedule=SCHEDULE_NAMES.get(K.last_call.schedule),
+                              graph=GRAPH_NAMES.get(K.last_call.graph))
 
     def step(record=False):
         K.fold(f, ra, rb, options=opts).batches[0].release()
@@ -503,6 +511,7 @@ def run_ours(args):
             "sparse": sparse,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "attention_forward_launch": fwd_launch,
             "gpu_launches": launches[0],
             "clocks": clocks.summary(),
         }
@@ -559,14 +568,17 @@ def _ranking(hbm, basis):
 def _ragged():
     """Ragged batches (64 groups, d=128, lengths log-uniform in [128, 8192],
     window |tq - tk| <= 512, values normal(0, 1/sqrt(128)), padded to the
-    longest): the attention forward in the split form (one launch over the
-    query tiles that join some key) and in the FP64 form, timed with CUDA
+    longest): the attention forward in the split form (the query tiles that
+    join some key, under the launch schedule its first call timed fastest,
+    replayed from a CUDA graph) and in the FP64 form, timed with CUDA
     events, FLOP = 4·d per allowed pair; the split result's error against
-    the FP64 one (max |diff| / max |out|)."""
+    the FP64 one (max |diff| / max |out|); the split forward under each
+    schedule."""
     import torch
 
     from einfold_b200 import autograd as A
     from einfold_b200 import cases as C
+    from einfold_b200 import kernels as K
     from einfold_b200.kernels import Precision
 
     groups, d, radius = 64, 128, 512
@@ -576,6 +588,9 @@ def _ragged():
            "flop": flop}
     results = {}
     for name, prec in (("split", Precision.SPLIT), ("fp64", Precision.FP64)):
+        # An untimed first call: the split form times its launch schedules on
+        # a shape's first call.
+        A.attention_forward(q, k, v, A.window(radius), d ** -0.5, prec, q_lengths=lengths, k_lengths=lengths)
         times = []
         for _ in range(3):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -593,6 +608,27 @@ def _ragged():
     out["split_max_rel_err"] = ((results["split"][seen] - results["fp64"][seen]).abs().max() /
                                 results["fp64"][seen].abs().max()).item()
     out["ratio_split_over_fp64"] = out["fp64"]["ms"] / out["split"]["ms"]
+    # The split forward under each launch schedule (forced), against the one
+    # its first call timed fastest.
+    A.attention_forward(q, k, v, A.window(radius), d ** -0.5, Precision.SPLIT, q_lengths=lengths, k_lengths=lengths)
+    out["tuned_schedule"] = SCHEDULE_NAMES.get(K.last_call.schedule)
+    out["graph"] = GRAPH_NAMES.get(K.last_call.graph)
+    out["schedules_ms"] = {}
+    try:
+        for name in ("grid", "tiles", "batches"):
+            os.environ["EINFOLD_ATTENTION_SCHEDULE"] = name
+            times = []
+            for _ in range(4):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                A.attention_forward(q, k, v, A.window(radius), d ** -0.5, Precision.SPLIT, q_lengths=lengths,
+                                    k_lengths=lengths)
+                e1.record()
+                torch.cuda.synchronize()
+                times.append(e0.elapsed_time(e1))
+            out["schedules_ms"][name] = statistics.median(times[1:])
+    finally:
+        os.environ.pop("EINFOLD_ATTENTION_SCHEDULE", None)
     del q, k, v, results
     torch.cuda.empty_cache()
     return out

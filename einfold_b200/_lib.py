@@ -111,6 +111,7 @@ class Result(ctypes.Structure):
                 ("tiles_visited", ctypes.c_uint64), ("tiles", ctypes.c_uint64),
                 ("kernels_launched", ctypes.c_uint64), ("device_ms", ctypes.c_double),
                 ("product_ms", ctypes.c_double), ("product_ops", ctypes.c_double),
+                ("schedule", ctypes.c_int32), ("graph", ctypes.c_int32),
                 ("message", ctypes.c_char * 480)]
 
 

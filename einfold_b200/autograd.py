@@ -79,6 +79,8 @@ def _call(fn, device: int, *args) -> _lib.Result:
     last_call.device_ms = info.device_ms
     last_call.product_ms = info.product_ms
     last_call.product_ops = info.product_ops
+    last_call.schedule = info.schedule
+    last_call.graph = info.graph
     last_call.message = info.message.decode(errors="replace")
     if st != _lib.OK:
         _raise(st, info.message.decode(errors="replace"))

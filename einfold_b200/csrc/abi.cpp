@@ -39,6 +39,8 @@ int32_t guarded(einfold_context* ctx, einfold_result* result, F&& body) {
     c->phase("call");
     c->product_ms = 0;
     c->product_ops = 0;
+    c->schedule = -1;
+    c->graph = 0;
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
@@ -55,6 +57,8 @@ int32_t guarded(einfold_context* ctx, einfold_result* result, F&& body) {
       result->kernels_launched = c->kernels;
       result->product_ms = c->product_ms;
       result->product_ops = c->product_ops;
+      result->schedule = c->schedule;
+      result->graph = c->graph;
     }
   } catch (const ef::Declined& d) {
     status = EINFOLD_DECLINED;
@@ -145,6 +149,7 @@ void einfold_context_destroy(einfold_context* ctx) {
     if (ctx->stream) {
       ctx->kept.release(ctx->stream);
       cudaStreamSynchronize(ctx->stream);
+      ctx->graphs.clear();
       ef::device_cache_forget(ctx->stream);
       cudaStreamDestroy(ctx->stream);
     }

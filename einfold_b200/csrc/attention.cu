@@ -29,6 +29,11 @@
 // status bit, waits for its copies and MMAs in flight, frees TMEM and
 // returns.
 //
+// Launch forms: a block per (query tile, batch) item, or persistent blocks
+// (one an SM) that claim the items of a work list in its order from a
+// counter, keeping their barriers and TMEM across items: the barriers'
+// phases count the block's key tiles and q loads since the launch.
+//
 // Accuracy: each operand value carries 8S - 2 bits under its row's (or
 // column's) power of two, levels above S + 1 are dropped, and every level
 // sum is exact, so a score's error is about ne · 2^(3-8S) · max|q| · max|k|
@@ -36,6 +41,9 @@
 // and averages to ~1e-14 of max|v|.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
 #include <mutex>
 
 #include "attention.cuh"
@@ -87,7 +95,11 @@ struct AttnArgs {
   double* lse;  // [w·lnx + x] or null
   int* status;  // bit 0: a guard fired; bit 1: a wait ran out
   unsigned long long* tiles;  // (row tile, key tile) pairs computed
-  const int2* items;  // ragged batches: block i runs (query tile, batch) items[i]; null: the grid's
+  const int2* items;  // a work list of (query tile, batch) items; null: the grid's (x: tile, y: batch)
+  int n_items;
+  // Persistent blocks: the next item of the list no block has claimed (zero
+  // at the launch). Null: block i runs items[i].
+  unsigned* next;
   int reverse;        // the grid's query tiles from the last one (whose rows join the most keys) down
 };
 
@@ -130,6 +142,7 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
   uint64_t* tmem_free = bars + 8;
   uint32_t* tmem_slot = (uint32_t*)(bars + 16);
   int* failed = (int*)(tmem_slot + 1);
+  int* item_slot = (int*)(tmem_slot + 2);         // the item the block runs next
   long long* span = (long long*)(tmem_slot + 4);  // first, last
   int* row_lo = (int*)(aux + 256);                // [128]
   int* row_hi = row_lo + AM;                      // [128]
@@ -139,10 +152,6 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
   double* red = (double*)(aux + 4096);            // [4][128]
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // The longest rows of a causal mask first; ragged batches by their work list.
-  const int xt = a.items ? a.items[blockIdx.x].x : a.reverse ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
-  const int w = a.items ? a.items[blockIdx.x].y : (int)blockIdx.y;
-  const int64_t x_base = (int64_t)w * a.lnx;
 
   if (threadIdx.x == 0) {
     mbar_init(q_full, 1);
@@ -155,330 +164,365 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
     mbar_init(p_full, kEpi / 32);  // each epilogue warp arrives
     mbar_init(tmem_free, kEpi / 32);
     *failed = 0;
-    span[0] = LLONG_MAX;
-    span[1] = LLONG_MIN;
     mbar_fence_init();
   }
   if (warp == 1) {
     tmem_alloc(tmem_slot, 512);
     tmem_relinquish();
   }
+  if (threadIdx.x < 64) texp[threadIdx.x] = a.exp_table[threadIdx.x];
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  // Each row's allowed keys, local to the batch.
-  if (threadIdx.x < AM) {
-    const int64_t xl = (int64_t)xt * AM + threadIdx.x;
-    int lo = 0, hi = 0;
-    if (xl < a.lnx) {
-      int64_t l, h;
-      allowed(a.mask, x_base + xl, l, h);
-      lo = (int)(l - (int64_t)w * a.lnj);
-      hi = (int)(h - (int64_t)w * a.lnj);
-      if (lo < hi) {
-        atomicMin(&span[0], (long long)lo);
-        atomicMax(&span[1], (long long)hi);
-      }
-    }
-    row_lo[threadIdx.x] = lo;
-    row_hi[threadIdx.x] = hi;
-  } else if (threadIdx.x < AM + AY) {
-    const int c = threadIdx.x - AM;
-    ev_s[c] = a.y0 + c < a.ny_pad ? a.ev[(int64_t)w * a.ny_pad + a.y0 + c] : 0;
-  } else if (threadIdx.x < AM + AY + 64) {
-    texp[threadIdx.x - AM - AY] = a.exp_table[threadIdx.x - AM - AY];
-  }
-  __syncthreads();
   const uint32_t tmem = *tmem_slot;
-  const long long first = span[0], last = span[1];
-  const int jt0 = first < last ? (int)(first / AJ) : 0;
-  const int n_tiles = first < last ? (int)((last + AJ - 1) / AJ) - jt0 : 0;
-  if (threadIdx.x == 0 && n_tiles > 0) atomicAdd(a.tiles, (unsigned long long)n_tiles);
-
-  if (warp == 0) {
-    if (lane == 0 && n_tiles > 0) {
-      // Producer: q's digits once, then k's and v's per tile, with the
-      // keys' exponents.
-      prefetch_map(&tq);
-      prefetch_map(&tk);
-      prefetch_map(&tv);
-      mbar_expect_tx(q_full, (uint32_t)Sh::kQ);
-      for (int kb = 0; kb < KB; kb++) tma_load_3d(sQ + kb * S * AM * 64, &tq, q_full, kb * 64, xt * AM, w * S);
-      int issued = 0;
-      for (int it = 0; it < n_tiles; it++) {
-        const int st = it % Sh::kStages;
-        const uint32_t round = (uint32_t)(it / Sh::kStages);
-        if (*(volatile int*)failed) break;
-        if (!mbar_wait(&kv_empty[st], (round & 1) ^ 1)) {
-          atomicOr(a.status, 2);
-          *(volatile int*)failed = 1;
-          break;
-        }
-        mbar_expect_tx(&kv_full[st], (uint32_t)(Sh::kK + Sh::kV + AJ * 4));
-        const int jl0 = (jt0 + it) * AJ;
-        for (int kb = 0; kb < KB; kb++)
-          tma_load_3d(sK + st * Sh::kK + kb * S * AJ * 64, &tk, &kv_full[st], kb * 64, jl0, w * S);
-        tma_load_3d(sV + st * Sh::kV, &tv, &kv_full[st], jl0, a.y0, w * S);
-        bulk_load(ek_s + st * AJ, a.ek + (int64_t)w * a.lnj_pad + jl0, AJ * 4, &kv_full[st]);
-        issued = it + 1;
-      }
-      // Copies still in flight complete before the CTA may exit.
-      mbar_wait(q_full, 0);
-      for (int it = std::max(0, issued - Sh::kStages); it < issued; it++)
-        mbar_wait(&kv_full[it % Sh::kStages], (uint32_t)((it / Sh::kStages) & 1));
+  // The barriers' completed phases before the current item: one per key
+  // tile (kv_full and kv_empty by stage) and one per q load.
+  int tiles_before = 0, q_loads = 0;
+  for (int round_ = 0;; round_++) {
+    if (threadIdx.x == 0) {
+      *item_slot = a.next ? (int)atomicAdd(a.next, 1u) : round_ == 0 ? 0 : INT_MAX;
+      span[0] = LLONG_MAX;
+      span[1] = LLONG_MIN;
     }
-  } else if (warp == 1) {
-    if (lane == 0 && n_tiles > 0) {
-      // MMA issuer.
-      uint64_t* last_bar = nullptr;
-      uint32_t last_parity = 0;
-      bool ok = mbar_wait(q_full, 0);
-      for (int it = 0; ok && it < n_tiles; it++) {
-        const int st = it % Sh::kStages;
-        const uint32_t round = (uint32_t)(it / Sh::kStages);
-        ok = mbar_wait(&kv_full[st], round & 1) && (it == 0 || mbar_wait(tmem_free, (uint32_t)((it - 1) & 1)));
-        if (!ok || *(volatile int*)failed) break;
-        tc_fence_after();
-        const uint32_t q_base = smem_u32(sQ), k_base = smem_u32(sK + st * Sh::kK);
-#pragma unroll
-        for (int kb = 0; kb < KB; kb++)
-#pragma unroll
+    __syncthreads();
+    // Every thread reads the same item and failure flag: all leave together.
+    const int item = *item_slot;
+    if (*(volatile int*)failed || item >= (a.next ? a.n_items : 1)) break;
+    // The longest rows of a causal mask first; work lists in their order.
+    int xt, w;
+    if (a.items) {
+      const int2 wk = a.items[a.next ? item : (int)blockIdx.x];
+      xt = wk.x;
+      w = wk.y;
+    } else {
+      xt = a.reverse ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
+      w = (int)blockIdx.y;
+    }
+    const int64_t x_base = (int64_t)w * a.lnx;
+    // Each row's allowed keys, local to the batch.
+    if (threadIdx.x < AM) {
+      const int64_t xl = (int64_t)xt * AM + threadIdx.x;
+      int lo = 0, hi = 0;
+      if (xl < a.lnx) {
+        int64_t l, h;
+        allowed(a.mask, x_base + xl, l, h);
+        lo = (int)(l - (int64_t)w * a.lnj);
+        hi = (int)(h - (int64_t)w * a.lnj);
+        if (lo < hi) {
+          atomicMin(&span[0], (long long)lo);
+          atomicMax(&span[1], (long long)hi);
+        }
+      }
+      row_lo[threadIdx.x] = lo;
+      row_hi[threadIdx.x] = hi;
+    } else if (threadIdx.x < AM + AY) {
+      const int c = threadIdx.x - AM;
+      ev_s[c] = a.y0 + c < a.ny_pad ? a.ev[(int64_t)w * a.ny_pad + a.y0 + c] : 0;
+    }
+    __syncthreads();
+    const long long first = span[0], last = span[1];
+    const int jt0 = first < last ? (int)(first / AJ) : 0;
+    const int n_tiles = first < last ? (int)((last + AJ - 1) / AJ) - jt0 : 0;
+    if (threadIdx.x == 0 && n_tiles > 0) atomicAdd(a.tiles, (unsigned long long)n_tiles);
+
+    if (warp == 0) {
+      if (lane == 0 && n_tiles > 0) {
+        // Producer: q's digits once, then k's and v's per tile, with the
+        // keys' exponents.
+        prefetch_map(&tq);
+        prefetch_map(&tk);
+        prefetch_map(&tv);
+        mbar_expect_tx(q_full, (uint32_t)Sh::kQ);
+        for (int kb = 0; kb < KB; kb++) tma_load_3d(sQ + kb * S * AM * 64, &tq, q_full, kb * 64, xt * AM, w * S);
+        int issued = 0;
+        for (int it = 0; it < n_tiles; it++) {
+          const int g = tiles_before + it;
+          const int st = g % Sh::kStages;
+          const uint32_t round = (uint32_t)(g / Sh::kStages);
+          if (*(volatile int*)failed) break;
+          if (!mbar_wait(&kv_empty[st], (round & 1) ^ 1)) {
+            atomicOr(a.status, 2);
+            *(volatile int*)failed = 1;
+            break;
+          }
+          mbar_expect_tx(&kv_full[st], (uint32_t)(Sh::kK + Sh::kV + AJ * 4));
+          const int jl0 = (jt0 + it) * AJ;
+          for (int kb = 0; kb < KB; kb++)
+            tma_load_3d(sK + st * Sh::kK + kb * S * AJ * 64, &tk, &kv_full[st], kb * 64, jl0, w * S);
+          tma_load_3d(sV + st * Sh::kV, &tv, &kv_full[st], jl0, a.y0, w * S);
+          bulk_load(ek_s + st * AJ, a.ek + (int64_t)w * a.lnj_pad + jl0, AJ * 4, &kv_full[st]);
+          issued = it + 1;
+        }
+        // Copies still in flight complete before the item ends.
+        mbar_wait(q_full, (uint32_t)(q_loads & 1));
+        for (int it = std::max(0, issued - Sh::kStages); it < issued; it++) {
+          const int g = tiles_before + it;
+          mbar_wait(&kv_full[g % Sh::kStages], (uint32_t)((g / Sh::kStages) & 1));
+        }
+      }
+    } else if (warp == 1) {
+      if (lane == 0 && n_tiles > 0) {
+        // MMA issuer. The item's first tile needs no tmem_free: the block's
+        // barrier between items follows the epilogue's last TMEM read.
+        uint64_t* last_bar = nullptr;
+        uint32_t last_parity = 0;
+        bool ok = mbar_wait(q_full, (uint32_t)(q_loads & 1));
+        for (int it = 0; ok && it < n_tiles; it++) {
+          const int g = tiles_before + it;
+          const int st = g % Sh::kStages;
+          const uint32_t round = (uint32_t)(g / Sh::kStages);
+          ok = mbar_wait(&kv_full[st], round & 1) && (it == 0 || mbar_wait(tmem_free, (uint32_t)((g - 1) & 1)));
+          if (!ok || *(volatile int*)failed) break;
+          tc_fence_after();
+          const uint32_t q_base = smem_u32(sQ), k_base = smem_u32(sK + st * Sh::kK);
+  #pragma unroll
+          for (int kb = 0; kb < KB; kb++)
+  #pragma unroll
+            for (int kk = 0; kk < 2; kk++)
+  #pragma unroll
+              for (int s = 1; s <= S; s++) {
+                const int total = (S + 1 - s) * AJ;
+  #pragma unroll
+                for (int nn0 = 0; nn0 < total; nn0 += 256) {
+                  const int nn = total - nn0 < 256 ? total - nn0 : 256;
+                  const uint64_t ad = desc_sw64(q_base + (kb * S + s - 1) * AM * 64 + kk * 32);
+                  const uint64_t bd = desc_sw64(k_base + kb * S * AJ * 64 + nn0 * 64 + kk * 32);
+                  umma_i8(tmem + (uint32_t)((s - 1) * AJ + nn0), ad, bd, idesc_i8(AM, nn),
+                          (kb > 0 || kk > 0 || s > 1) ? 1u : 0u);
+                }
+              }
+          umma_commit(qk_full);
+          last_bar = qk_full;
+          last_parity = (uint32_t)(g & 1);
+          ok = mbar_wait(p_full, (uint32_t)(g & 1));
+          if (!ok || *(volatile int*)failed) break;
+          tc_fence_after();
+          const uint32_t p_base = smem_u32(sP), v_base = smem_u32(sV + st * Sh::kV);
+  #pragma unroll
           for (int kk = 0; kk < 2; kk++)
-#pragma unroll
+  #pragma unroll
             for (int s = 1; s <= S; s++) {
-              const int total = (S + 1 - s) * AJ;
-#pragma unroll
+              const int total = (S + 1 - s) * AY;
+  #pragma unroll
               for (int nn0 = 0; nn0 < total; nn0 += 256) {
                 const int nn = total - nn0 < 256 ? total - nn0 : 256;
-                const uint64_t ad = desc_sw64(q_base + (kb * S + s - 1) * AM * 64 + kk * 32);
-                const uint64_t bd = desc_sw64(k_base + kb * S * AJ * 64 + nn0 * 64 + kk * 32);
-                umma_i8(tmem + (uint32_t)((s - 1) * AJ + nn0), ad, bd, idesc_i8(AM, nn),
-                        (kb > 0 || kk > 0 || s > 1) ? 1u : 0u);
+                const uint64_t ad = desc_sw64(p_base + (s - 1) * AM * 64 + kk * 32);
+                const uint64_t bd = desc_sw64(v_base + nn0 * 64 + kk * 32);
+                umma_i8(tmem + (uint32_t)((s - 1) * AY + nn0), ad, bd, idesc_i8(AM, nn), (kk > 0 || s > 1) ? 1u : 0u);
               }
             }
-        umma_commit(qk_full);
-        last_bar = qk_full;
-        last_parity = (uint32_t)(it & 1);
-        ok = mbar_wait(p_full, (uint32_t)(it & 1));
-        if (!ok || *(volatile int*)failed) break;
+          umma_commit(pv_full);
+          umma_commit(&kv_empty[st]);
+          last_bar = pv_full;
+          last_parity = (uint32_t)(g & 1);
+        }
+        if (!ok) {
+          atomicOr(a.status, 2);
+          *(volatile int*)failed = 1;
+        }
+        // MMAs still running complete before TMEM is freed.
+        if (last_bar) mbar_wait(last_bar, last_parity);
+      }
+    } else {
+      // Epilogue: warp w reads TMEM lanes 32·(w % 4) .. +31; warps 2..5 take
+      // columns 0..15 of each tile and of the sums, 6..9 columns 16..31, and
+      // so on. The four warps of a lane quarter exchange row maxima over their
+      // own named barrier; each warp signals the MMA warp by itself.
+      constexpr int CW = 16;  // columns per thread
+      constexpr int kShift = 8 * S - 2;
+      const int h = (warp - 2) >> 2;
+      const int quarter = warp & 3;
+      const int r = quarter * 32 + lane;
+      const int64_t xl = (int64_t)xt * AM + r;
+      const bool valid = xl < a.lnx;
+      const int lo = row_lo[r], hi = row_hi[r];
+      // Column c of a tile starting at jl0 is allowed iff (unsigned)(jl0 + c - lo) < span.
+      const unsigned span = (valid && lo < hi) ? (unsigned)(hi - lo) : 0u;
+      const int eqr = valid ? a.eq[(int64_t)w * a.lnx_pad + xl] : 0;
+      const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
+      const uint32_t sum_addr = lane_addr + (uint32_t)(kSumCol + h * 2 * CW);
+      const double NEG_INF = -INFINITY;
+      // z sums the weights times 2^(8S-2); the running sums are in units of
+      // their columns' powers of two 2^(2 + ev).
+      double m = NEG_INF, z = 0.0, light = INFINITY;
+      auto wait = [&](uint64_t* bar, uint32_t parity) {
+        if (*(volatile int*)failed) return;
+        if (!mbar_wait(bar, parity)) {
+          *(volatile int*)failed = 1;
+          atomicOr(a.status, 2);
+        }
+      };
+      for (int it = 0; it < n_tiles; it++) {
+        const int g = tiles_before + it;
+        const int jl0 = (jt0 + it) * AJ + h * CW;
+        const int* eks = ek_s + (g % Sh::kStages) * AJ + h * CW;
+        wait(qk_full, (uint32_t)(g & 1));
         tc_fence_after();
-        const uint32_t p_base = smem_u32(sP), v_base = smem_u32(sV + st * Sh::kV);
-#pragma unroll
-        for (int kk = 0; kk < 2; kk++)
-#pragma unroll
-          for (int s = 1; s <= S; s++) {
-            const int total = (S + 1 - s) * AY;
-#pragma unroll
-            for (int nn0 = 0; nn0 < total; nn0 += 256) {
-              const int nn = total - nn0 < 256 ? total - nn0 : 256;
-              const uint64_t ad = desc_sw64(p_base + (s - 1) * AM * 64 + kk * 32);
-              const uint64_t bd = desc_sw64(v_base + nn0 * 64 + kk * 32);
-              umma_i8(tmem + (uint32_t)((s - 1) * AY + nn0), ad, bd, idesc_i8(AM, nn), (kk > 0 || s > 1) ? 1u : 0u);
-            }
+        double sc[CW];
+  #pragma unroll
+        for (int c4 = 0; c4 < CW / 4; c4++) {
+          int32_t L[S][4];
+          load_levels<S>(lane_addr, h * CW + c4 * 4, L);
+  #pragma unroll
+          for (int i = 0; i < 4; i++) {
+            const int c = c4 * 4 + i;
+            const double l = level_sum<S, KB>(L, i);
+            sc[c] = FAST ? l * pow2(eqr + eks[c]) : scale2(l, eqr + eks[c]);
           }
-        umma_commit(pv_full);
-        umma_commit(&kv_empty[st]);
-        last_bar = pv_full;
-        last_parity = (uint32_t)(it & 1);
-      }
-      if (!ok) {
-        atomicOr(a.status, 2);
-        *(volatile int*)failed = 1;
-      }
-      // MMAs still running complete before TMEM is freed.
-      if (last_bar) mbar_wait(last_bar, last_parity);
-    }
-  } else {
-    // Epilogue: warp w reads TMEM lanes 32·(w % 4) .. +31; warps 2..5 take
-    // columns 0..15 of each tile and of the sums, 6..9 columns 16..31, and
-    // so on. The four warps of a lane quarter exchange row maxima over their
-    // own named barrier; each warp signals the MMA warp by itself.
-    constexpr int CW = 16;  // columns per thread
-    constexpr int kShift = 8 * S - 2;
-    const int h = (warp - 2) >> 2;
-    const int quarter = warp & 3;
-    const int r = quarter * 32 + lane;
-    const int64_t xl = (int64_t)xt * AM + r;
-    const bool valid = xl < a.lnx;
-    const int lo = row_lo[r], hi = row_hi[r];
-    // Column c of a tile starting at jl0 is allowed iff (unsigned)(jl0 + c - lo) < span.
-    const unsigned span = (valid && lo < hi) ? (unsigned)(hi - lo) : 0u;
-    const int eqr = valid ? a.eq[(int64_t)w * a.lnx_pad + xl] : 0;
-    const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
-    const uint32_t sum_addr = lane_addr + (uint32_t)(kSumCol + h * 2 * CW);
-    const double NEG_INF = -INFINITY;
-    // z sums the weights times 2^(8S-2); the running sums are in units of
-    // their columns' powers of two 2^(2 + ev).
-    double m = NEG_INF, z = 0.0, light = INFINITY;
-    auto wait = [&](uint64_t* bar, uint32_t parity) {
-      if (*(volatile int*)failed) return;
-      if (!mbar_wait(bar, parity)) {
-        *(volatile int*)failed = 1;
-        atomicOr(a.status, 2);
-      }
-    };
-    for (int it = 0; it < n_tiles; it++) {
-      const int jl0 = (jt0 + it) * AJ + h * CW;
-      const int* eks = ek_s + (it % Sh::kStages) * AJ + h * CW;
-      wait(qk_full, (uint32_t)(it & 1));
-      tc_fence_after();
-      double sc[CW];
-#pragma unroll
-      for (int c4 = 0; c4 < CW / 4; c4++) {
-        int32_t L[S][4];
-        load_levels<S>(lane_addr, h * CW + c4 * 4, L);
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-          const int c = c4 * 4 + i;
-          const double l = level_sum<S, KB>(L, i);
-          sc[c] = FAST ? l * pow2(eqr + eks[c]) : scale2(l, eqr + eks[c]);
         }
-      }
-      if (a.scale_kind == 1) {
-#pragma unroll
-        for (int c = 0; c < CW; c++) sc[c] *= a.scale_c;
-      } else if (a.scale_kind == 2) {
-#pragma unroll
-        for (int c = 0; c < CW; c++) sc[c] = __ddiv_rn(sc[c], a.scale_c);
-      }
-      // The mask, and the row's largest and smallest allowed scores.
-      const int off = jl0 - lo;
-      double mx = NEG_INF;
-      if (__all_sync(0xffffffffu, off >= 0 && (unsigned)off + CW <= span)) {
-#pragma unroll
-        for (int c = 0; c < CW; c++) {
-          mx = fmax(mx, sc[c]);
-          light = fmin(light, sc[c]);
+        if (a.scale_kind == 1) {
+  #pragma unroll
+          for (int c = 0; c < CW; c++) sc[c] *= a.scale_c;
+        } else if (a.scale_kind == 2) {
+  #pragma unroll
+          for (int c = 0; c < CW; c++) sc[c] = __ddiv_rn(sc[c], a.scale_c);
         }
-      } else {
-#pragma unroll
-        for (int c = 0; c < CW; c++) {
-          const bool in = (unsigned)(off + c) < span;
-          light = fmin(light, in ? sc[c] : INFINITY);
-          sc[c] = in ? sc[c] : NEG_INF;
-          mx = fmax(mx, sc[c]);
+        // The mask, and the row's largest and smallest allowed scores.
+        const int off = jl0 - lo;
+        double mx = NEG_INF;
+        if (__all_sync(0xffffffffu, off >= 0 && (unsigned)off + CW <= span)) {
+  #pragma unroll
+          for (int c = 0; c < CW; c++) {
+            mx = fmax(mx, sc[c]);
+            light = fmin(light, sc[c]);
+          }
+        } else {
+  #pragma unroll
+          for (int c = 0; c < CW; c++) {
+            const bool in = (unsigned)(off + c) < span;
+            light = fmin(light, in ? sc[c] : INFINITY);
+            sc[c] = in ? sc[c] : NEG_INF;
+            mx = fmax(mx, sc[c]);
+          }
         }
-      }
-      red[h * AM + r] = mx;
-      named_bar(2 + quarter, 128);
-      mx = fmax(fmax(red[r], red[AM + r]), fmax(red[2 * AM + r], red[3 * AM + r]));
-      const double m_new = fmax(m, mx);
-      double rescale = 1.0;
-      if (m_new != m) {
-        rescale = m == NEG_INF ? 0.0 : exp_tang(m - m_new, texp);
-        z *= rescale;
-        m = m_new;
-      }
-      // Weights and their digits: W = exp(s - m) · 2^(8S-2) < 2^(8S-2),
-      // balanced base-256 digits, most significant first, four columns a
-      // word.
-      uint8_t* prow = sP + r * 64;
-#pragma unroll
-      for (int c4 = 0; c4 < CW / 4; c4++) {
-        double x[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-          const double sv = sc[c4 * 4 + i];
-          const double wt = exp_weight(sv - m, texp, kShift);
-          x[i] = sv == NEG_INF ? 0.0 : wt;
-          z += x[i];
+        red[h * AM + r] = mx;
+        named_bar(2 + quarter, 128);
+        mx = fmax(fmax(red[r], red[AM + r]), fmax(red[2 * AM + r], red[3 * AM + r]));
+        const double m_new = fmax(m, mx);
+        double rescale = 1.0;
+        if (m_new != m) {
+          rescale = m == NEG_INF ? 0.0 : exp_tang(m - m_new, texp);
+          z *= rescale;
+          m = m_new;
         }
-        uint32_t planes[S];
-        digit_planes4<S>(x, planes);
-        const uint32_t off4 = sw64_offset((uint32_t)r, (uint32_t)(h * CW + c4 * 4)) - (uint32_t)r * 64;
-#pragma unroll
-        for (int s = 0; s < S; s++) *(uint32_t*)(prow + s * AM * 64 + off4) = planes[s];
+        // Weights and their digits: W = exp(s - m) · 2^(8S-2) < 2^(8S-2),
+        // balanced base-256 digits, most significant first, four columns a
+        // word.
+        uint8_t* prow = sP + r * 64;
+  #pragma unroll
+        for (int c4 = 0; c4 < CW / 4; c4++) {
+          double x[4];
+  #pragma unroll
+          for (int i = 0; i < 4; i++) {
+            const double sv = sc[c4 * 4 + i];
+            const double wt = exp_weight(sv - m, texp, kShift);
+            x[i] = sv == NEG_INF ? 0.0 : wt;
+            z += x[i];
+          }
+          uint32_t planes[S];
+          digit_planes4<S>(x, planes);
+          const uint32_t off4 = sw64_offset((uint32_t)r, (uint32_t)(h * CW + c4 * 4)) - (uint32_t)r * 64;
+  #pragma unroll
+          for (int s = 0; s < S; s++) *(uint32_t*)(prow + s * AM * 64 + off4) = planes[s];
+        }
+        fence_proxy_async();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(p_full);
+        wait(pv_full, (uint32_t)(g & 1));
+        tc_fence_after();
+        // sums = sums · rescale + this tile's weighted values, four at a time.
+  #pragma unroll
+        for (int c4 = 0; c4 < CW / 4; c4++) {
+          int32_t L[S][4];
+          load_levels<S>(lane_addr, h * CW + c4 * 4, L);
+          uint32_t sum[8];
+          if (it > 0) {
+            tmem_ld8(sum_addr + c4 * 8, (int32_t*)sum);
+            tmem_wait_ld();
+          }
+  #pragma unroll
+          for (int i = 0; i < 4; i++) {
+            const double l = combine_levels_small<S, 4>(L, i);
+            const double v = it > 0 ? fma(__hiloint2double((int)sum[2 * i + 1], (int)sum[2 * i]), rescale, l) : l;
+            sum[2 * i] = (uint32_t)__double2loint(v);
+            sum[2 * i + 1] = (uint32_t)__double2hiint(v);
+          }
+          tmem_st8(sum_addr + c4 * 8, sum);
+        }
+        tmem_wait_st();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(tmem_free);
       }
-      fence_proxy_async();
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(p_full);
-      wait(pv_full, (uint32_t)(it & 1));
-      tc_fence_after();
-      // sums = sums · rescale + this tile's weighted values, four at a time.
-#pragma unroll
-      for (int c4 = 0; c4 < CW / 4; c4++) {
-        int32_t L[S][4];
-        load_levels<S>(lane_addr, h * CW + c4 * 4, L);
-        uint32_t sum[8];
-        if (it > 0) {
+      if (n_tiles > 0) {
+        // The four quarters' sums of weights and lightest scores (P's digits
+        // are no longer read).
+        double* xz = (double*)sP;
+        double* xlg = xz + 4 * AM;
+        xz[h * AM + r] = z;
+        xlg[h * AM + r] = light;
+        named_bar(2 + quarter, 128);
+        z = ((xz[r] + xz[AM + r]) + (xz[2 * AM + r] + xz[3 * AM + r])) * pow2(-kShift);
+        light = fmin(fmin(xlg[r], xlg[AM + r]), fmin(xlg[2 * AM + r], xlg[3 * AM + r]));
+        tc_fence_after();
+        double o[CW];
+  #pragma unroll
+        for (int c4 = 0; c4 < CW / 4; c4++) {
+          uint32_t sum[8];
           tmem_ld8(sum_addr + c4 * 8, (int32_t*)sum);
           tmem_wait_ld();
+  #pragma unroll
+          for (int i = 0; i < 4; i++)
+            o[c4 * 4 + i] = scale2(__hiloint2double((int)sum[2 * i + 1], (int)sum[2 * i]), 2 + ev_s[h * CW + c4 * 4 + i]);
         }
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-          const double l = combine_levels_small<S, 4>(L, i);
-          const double v = it > 0 ? fma(__hiloint2double((int)sum[2 * i + 1], (int)sum[2 * i]), rescale, l) : l;
-          sum[2 * i] = (uint32_t)__double2loint(v);
-          sum[2 * i + 1] = (uint32_t)__double2hiint(v);
-        }
-        tmem_st8(sum_addr + c4 * 8, sum);
-      }
-      tmem_wait_st();
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(tmem_free);
-    }
-    if (n_tiles > 0) {
-      // The four quarters' sums of weights and lightest scores (P's digits
-      // are no longer read).
-      double* xz = (double*)sP;
-      double* xlg = xz + 4 * AM;
-      xz[h * AM + r] = z;
-      xlg[h * AM + r] = light;
-      named_bar(2 + quarter, 128);
-      z = ((xz[r] + xz[AM + r]) + (xz[2 * AM + r] + xz[3 * AM + r])) * pow2(-kShift);
-      light = fmin(fmin(xlg[r], xlg[AM + r]), fmin(xlg[2 * AM + r], xlg[3 * AM + r]));
-      tc_fence_after();
-      double o[CW];
-#pragma unroll
-      for (int c4 = 0; c4 < CW / 4; c4++) {
-        uint32_t sum[8];
-        tmem_ld8(sum_addr + c4 * 8, (int32_t*)sum);
-        tmem_wait_ld();
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-          o[c4 * 4 + i] = scale2(__hiloint2double((int)sum[2 * i + 1], (int)sum[2 * i]), 2 + ev_s[h * CW + c4 * 4 + i]);
-      }
-      if (valid && lo < hi && !*(volatile int*)failed) {
-        // Bounds::hold (fused.rs:1058-1086): the heaviest weight is
-        // exp(high - m) = 1, the row's largest score being m.
-        const double rl = a.rl[x_base + xl], rs = a.rs[x_base + xl];
-        bool over = !(z <= 1.7976931348623157e308);
-        const double normal = 2.0 * 2.2250738585072014e-308;
-        const double lightest = exp(light - m);
-        const double t2 = 2.0 * (double)(hi - lo);
-        bool finite = isfinite(rl * t2);
-        if (finite) {
-          const double quotient = 1.0 / fabs(z);
-          finite = isfinite(quotient) && isfinite(quotient * rl * t2);
-        }
-        const double lost = (t2 * 4.9406564584124654e-324) * ((1.0 / fabs(z) + rl) + 1.0);
-        bool no_underflow = rs == INFINITY;
-        if (!no_underflow) {
-          no_underflow = lightest * rs >= normal;
-          if (no_underflow) {
-            const double quotient = lightest / fabs(z);
-            no_underflow = quotient >= normal && quotient * rs >= normal;
+        if (valid && lo < hi && !*(volatile int*)failed) {
+          // Bounds::hold (fused.rs:1058-1086): the heaviest weight is
+          // exp(high - m) = 1, the row's largest score being m.
+          const double rl = a.rl[x_base + xl], rs = a.rs[x_base + xl];
+          bool over = !(z <= 1.7976931348623157e308);
+          const double normal = 2.0 * 2.2250738585072014e-308;
+          const double lightest = exp(light - m);
+          const double t2 = 2.0 * (double)(hi - lo);
+          bool finite = isfinite(rl * t2);
+          if (finite) {
+            const double quotient = 1.0 / fabs(z);
+            finite = isfinite(quotient) && isfinite(quotient * rl * t2);
           }
+          const double lost = (t2 * 4.9406564584124654e-324) * ((1.0 / fabs(z) + rl) + 1.0);
+          bool no_underflow = rs == INFINITY;
+          if (!no_underflow) {
+            no_underflow = lightest * rs >= normal;
+            if (no_underflow) {
+              const double quotient = lightest / fabs(z);
+              no_underflow = quotient >= normal && quotient * rs >= normal;
+            }
+          }
+          if (!finite) over = true;
+          const double rounding = 2.220446049250313e-16 / 4.0;
+          double* orow = a.out + (x_base + xl) * a.ny;
+  #pragma unroll
+          for (int c = 0; c < CW; c++) {
+            const int64_t y = (int64_t)a.y0 + h * CW + c;
+            if (y >= a.ny) continue;
+            if (!isfinite(o[c])) over = true;
+            const double v = __ddiv_rn(o[c], z);
+            if (!isfinite(v)) over = true;
+            if (!no_underflow && !(lost <= rounding * fabs(v))) over = true;
+            orow[y] = v;
+          }
+          if (h == 0 && a.lse && a.y0 == 0) a.lse[x_base + xl] = m + log(z);
+          if (over) atomicOr(a.status, 1);
         }
-        if (!finite) over = true;
-        const double rounding = 2.220446049250313e-16 / 4.0;
-        double* orow = a.out + (x_base + xl) * a.ny;
-#pragma unroll
-        for (int c = 0; c < CW; c++) {
-          const int64_t y = (int64_t)a.y0 + h * CW + c;
-          if (y >= a.ny) continue;
-          if (!isfinite(o[c])) over = true;
-          const double v = __ddiv_rn(o[c], z);
-          if (!isfinite(v)) over = true;
-          if (!no_underflow && !(lost <= rounding * fabs(v))) over = true;
-          orow[y] = v;
-        }
-        if (h == 0 && a.lse && a.y0 == 0) a.lse[x_base + xl] = m + log(z);
-        if (over) atomicOr(a.status, 1);
       }
     }
+    tiles_before += n_tiles;
+    q_loads += n_tiles > 0 ? 1 : 0;
+    // The item's TMEM reads and shared-memory uses end before the next
+    // item's setup and MMAs.
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
   }
   tc_fence_before();
   __syncthreads();
@@ -538,21 +582,38 @@ __global__ void row_value_bounds(int64_t nx, Mask m, const double* __restrict__ 
 
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
-template <int S, int KB, bool FAST>
-void launch(const CUtensorMap& tq, const CUtensorMap& tk, const CUtensorMap& tv, const AttnArgs& args, dim3 grid,
-            cudaStream_t stream) {
-  using Sh = AttnShape<S, KB>;
-  EF_CUDA(cudaFuncSetAttribute(attn_fwd_split<S, KB, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::kSmem));
-  attn_fwd_split<S, KB, FAST><<<grid, kAttnThreads, Sh::kSmem, stream>>>(tq, tk, tv, args);
-  EF_LAUNCH_CHECK();
+// The kernel variant for d <= 64 (KB 1) or <= 128 (KB 2), with or without
+// the fast powers of two.
+using AttnKernel = void (*)(CUtensorMap, CUtensorMap, CUtensorMap, AttnArgs);
+
+AttnKernel attn_kernel(int kb, bool fast, int* smem) {
+  *smem = kb == 1 ? AttnShape<6, 1>::kSmem : AttnShape<6, 2>::kSmem;
+  if (kb == 1) return fast ? attn_fwd_split<6, 1, true> : attn_fwd_split<6, 1, false>;
+  return fast ? attn_fwd_split<6, 2, true> : attn_fwd_split<6, 2, false>;
 }
 
-// The work list of a ragged problem: its (query tile, batch) items that
-// join some key, by their key-tile counts, largest first. The lists of the
-// last few shapes (lengths, extents and conditions) are kept: a training
-// loop asks for the same one at every step.
-std::vector<int2> ragged_work(const AttentionProblem& p) {
-  std::vector<int64_t> key = {p.batches, p.lnx, p.lnj, p.mask.n, (int64_t)p.xlen_host.size(),
+// How the (query tile, batch) items of a forward pass reach the SMs.
+enum Schedule : int {
+  kGridSchedule = 0,   // a block per item: the grid's order, or the work list's by key tiles
+  kTilesSchedule = 1,  // persistent blocks claiming the items by key tiles, most first
+  kBatchSchedule = 2,  // persistent, batch by batch (the most key tiles first), in a batch by key tiles
+  kSchedules = 3,
+};
+
+// A problem's work lists (the items that join some key) and the schedule
+// timed fastest for it (-1 until timed).
+struct WorkLists {
+  std::vector<int2> by_tiles, by_batch;
+  int schedule = -1;
+};
+
+std::mutex g_work_lock;
+
+// The work lists of a problem. Those of the last few shapes (lengths,
+// extents, conditions) are kept, with their timed schedule: a training
+// loop asks for the same ones at every step.
+std::shared_ptr<WorkLists> work_lists(const AttentionProblem& p) {
+  std::vector<int64_t> key = {p.batches, p.lnx, p.lnj, p.ne, p.ny, p.mask.n, (int64_t)p.xlen_host.size(),
                               (int64_t)p.jlen_host.size()};
   for (int i = 0; i < p.mask.n; i++) {
     key.push_back(p.mask.cmp[i]);
@@ -560,10 +621,9 @@ std::vector<int2> ragged_work(const AttentionProblem& p) {
   }
   key.insert(key.end(), p.xlen_host.begin(), p.xlen_host.end());
   key.insert(key.end(), p.jlen_host.begin(), p.jlen_host.end());
-  static std::mutex lock;
-  static std::vector<std::pair<std::vector<int64_t>, std::vector<int2>>> kept;  // most recent last
+  static std::vector<std::pair<std::vector<int64_t>, std::shared_ptr<WorkLists>>> kept;  // most recent last
   {
-    std::lock_guard<std::mutex> g(lock);
+    std::lock_guard<std::mutex> g(g_work_lock);
     for (size_t i = 0; i < kept.size(); i++)
       if (kept[i].first == key) {
         auto hit = kept[i];
@@ -575,29 +635,77 @@ std::vector<int2> ragged_work(const AttentionProblem& p) {
   Mask hm = p.mask;
   hm.xlen = p.xlen_host.empty() ? nullptr : p.xlen_host.data();
   hm.jlen = p.jlen_host.empty() ? nullptr : p.jlen_host.data();
+  const bool ragged = hm.xlen || hm.jlen;
+  // A query tile's key tiles (0: it joins none); without lengths every
+  // batch has batch 0's.
+  auto key_tiles = [&](int64_t w, int64_t xt) -> int64_t {
+    const int64_t rows = hm.xlen ? hm.xlen[w] : p.lnx;
+    int64_t first = INT64_MAX, last = INT64_MIN;
+    for (int64_t r = xt * AM; r < std::min(rows, xt * AM + AM); r++) {
+      int64_t lo, hi;
+      allowed(hm, w * p.lnx + r, lo, hi);
+      if (lo < hi) {
+        first = std::min(first, lo - w * p.lnj);
+        last = std::max(last, hi - w * p.lnj);
+      }
+    }
+    return first < last ? (last + AJ - 1) / AJ - first / AJ : 0;
+  };
+  const int64_t n_xt = (p.lnx + AM - 1) / AM;
+  std::vector<int64_t> first_batch;
+  if (!ragged)
+    for (int64_t xt = 0; xt < n_xt; xt++) first_batch.push_back(key_tiles(0, xt));
   std::vector<std::pair<int64_t, int2>> work;
+  std::vector<std::pair<int64_t, int64_t>> batch_total;  // (key tiles, batch)
   for (int64_t w = 0; w < p.batches; w++) {
+    int64_t total = 0;
     const int64_t rows = hm.xlen ? hm.xlen[w] : p.lnx;
     for (int64_t xt = 0; xt * AM < rows; xt++) {
-      int64_t first = INT64_MAX, last = INT64_MIN;
-      for (int64_t r = xt * AM; r < std::min(rows, xt * AM + AM); r++) {
-        int64_t lo, hi;
-        allowed(hm, w * p.lnx + r, lo, hi);
-        if (lo < hi) {
-          first = std::min(first, lo - w * p.lnj);
-          last = std::max(last, hi - w * p.lnj);
-        }
-      }
-      if (first < last) work.push_back({(last + AJ - 1) / AJ - first / AJ, make_int2((int)xt, (int)w)});
+      const int64_t n = ragged ? key_tiles(w, xt) : first_batch[(size_t)xt];
+      if (n > 0) work.push_back({n, make_int2((int)xt, (int)w)});
+      total += n;
     }
+    batch_total.push_back({total, w});
   }
-  std::stable_sort(work.begin(), work.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-  std::vector<int2> list;
-  for (auto& x : work) list.push_back(x.second);
-  std::lock_guard<std::mutex> g(lock);
-  kept.emplace_back(std::move(key), list);
+  auto most_first = [](const auto& a, const auto& b) { return a.first > b.first; };
+  auto lists = std::make_shared<WorkLists>();
+  std::stable_sort(work.begin(), work.end(), most_first);
+  for (auto& x : work) lists->by_tiles.push_back(x.second);
+  std::stable_sort(batch_total.begin(), batch_total.end(), most_first);
+  std::vector<int64_t> place((size_t)p.batches);
+  for (size_t i = 0; i < batch_total.size(); i++) place[(size_t)batch_total[i].second] = (int64_t)i;
+  std::vector<int2> by_batch = lists->by_tiles;
+  std::stable_sort(by_batch.begin(), by_batch.end(),
+                   [&](const int2& a, const int2& b) { return place[(size_t)a.y] < place[(size_t)b.y]; });
+  lists->by_batch = std::move(by_batch);
+  std::lock_guard<std::mutex> g(g_work_lock);
+  kept.emplace_back(std::move(key), lists);
   if (kept.size() > 8) kept.erase(kept.begin());
-  return list;
+  return lists;
+}
+
+// EINFOLD_ATTENTION_SCHEDULE = grid | tiles | batches forces a schedule;
+// unset, the first call of a shape times them all.
+int forced_schedule() {
+  const char* s = std::getenv("EINFOLD_ATTENTION_SCHEDULE");
+  if (!s || !*s) return -1;
+  if (!std::strcmp(s, "grid")) return kGridSchedule;
+  if (!std::strcmp(s, "tiles")) return kTilesSchedule;
+  if (!std::strcmp(s, "batches")) return kBatchSchedule;
+  fail(EINFOLD_INVALID, "EINFOLD_ATTENTION_SCHEDULE is %s, not grid, tiles or batches", s);
+  return -1;
+}
+
+// EINFOLD_GRAPHS=0 launches directly instead of through CUDA graphs.
+bool graphs_enabled() {
+  const char* s = std::getenv("EINFOLD_GRAPHS");
+  return !(s && !std::strcmp(s, "0"));
+}
+
+template <class T>
+void put(std::vector<uint8_t>& key, const T& v) {
+  const uint8_t* b = (const uint8_t*)&v;
+  key.insert(key.end(), b, b + sizeof v);
 }
 
 }  // namespace
@@ -688,7 +796,6 @@ AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int sl
   args.lse = p.lse;
   args.status = status + 1;
   args.tiles = tiles;
-  dim3 grid((unsigned)(lnx_pad / AM), (unsigned)W);
   {
     // The query tiles whose rows join the most keys first: the last ones
     // under a causal mask, the first ones when the mask runs the other way.
@@ -699,32 +806,109 @@ AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int sl
     allowed(m, p.lnx - 1, lo1, hi1);
     args.reverse = hi1 - lo1 >= hi0 - lo0;
   }
-  // Ragged batches: one block per query tile that joins some key, the tiles
-  // with the most key tiles first.
-  DeviceBuffer<int2> items;
-  if (!p.xlen_host.empty() || !p.jlen_host.empty()) {
-    const std::vector<int2> list = ragged_work(p);
-    if (list.empty()) return ATTENTION_DONE;
-    items.allocate(list.size(), stream);
-    EF_CUDA(cudaMemcpyAsync(items.get(), list.data(), list.size() * sizeof(int2), cudaMemcpyHostToDevice, stream));
-    args.items = items.get();
-    grid = dim3((unsigned)list.size(), 1);
-  }
+  // The items that join some key, by key tiles and batch by batch.
+  const std::shared_ptr<WorkLists> lists = work_lists(p);
+  const int n_items = (int)lists->by_tiles.size();
+  if (n_items == 0) return ATTENTION_DONE;
+  const bool ragged = !p.xlen_host.empty() || !p.jlen_host.empty();
+  const int n_y = (int)((p.ny + AY - 1) / AY);
+  DeviceBuffer<int2> items((size_t)n_items * 2, stream);
+  EF_CUDA(cudaMemcpyAsync(items.get(), lists->by_tiles.data(), (size_t)n_items * sizeof(int2),
+                          cudaMemcpyHostToDevice, stream));
+  EF_CUDA(cudaMemcpyAsync(items.get() + n_items, lists->by_batch.data(), (size_t)n_items * sizeof(int2),
+                          cudaMemcpyHostToDevice, stream));
+  DeviceBuffer<unsigned> counters((size_t)n_y, stream);
+  int smem = 0;
+  const AttnKernel kernel = attn_kernel(KB, fast, &smem);
+  EF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  const int persistent_blocks = std::min(n_items, ctx.sm_count);
+  // The tile phase under a schedule: a launch per block of 64 value columns
+  // (persistent ones after zeroing their item counters).
+  auto enqueue = [&](int schedule, cudaStream_t st) {
+    AttnArgs ar = args;
+    dim3 grid((unsigned)(lnx_pad / AM), (unsigned)W);
+    if (schedule == kGridSchedule) {
+      if (ragged) {
+        ar.items = items.get();
+        ar.n_items = n_items;
+        grid = dim3((unsigned)n_items, 1);
+      }
+    } else {
+      ar.items = items.get() + (schedule == kBatchSchedule ? n_items : 0);
+      ar.n_items = n_items;
+      grid = dim3((unsigned)persistent_blocks, 1);
+      EF_CUDA(cudaMemsetAsync(counters.get(), 0, (size_t)n_y * sizeof(unsigned), st));
+    }
+    for (int yb = 0; yb < n_y; yb++) {
+      ar.y0 = yb * AY;
+      ar.next = schedule == kGridSchedule ? nullptr : counters.get() + yb;
+      kernel<<<grid, kAttnThreads, smem, st>>>(tq, tk, tv, ar);
+      EF_LAUNCH_CHECK();
+    }
+  };
   cudaEvent_t e0, e1;
   EF_CUDA(cudaEventCreate(&e0));
   EF_CUDA(cudaEventCreate(&e1));
-  EF_CUDA(cudaEventRecord(e0, stream));
-  for (int64_t y0 = 0; y0 < p.ny; y0 += AY) {
-    args.y0 = (int)y0;
-    if (KB == 1) {
-      if (fast) launch<6, 1, true>(tq, tk, tv, args, grid, stream);
-      else launch<6, 1, false>(tq, tk, tv, args, grid, stream);
-    } else {
-      if (fast) launch<6, 2, true>(tq, tk, tv, args, grid, stream);
-      else launch<6, 2, false>(tq, tk, tv, args, grid, stream);
-    }
-    ctx.kernels++;
+  int schedule = forced_schedule();
+  if (schedule < 0) {
+    std::lock_guard<std::mutex> g(g_work_lock);
+    schedule = lists->schedule;
   }
+  if (schedule < 0) {
+    // The first call of this shape: each schedule twice (the same results
+    // each time), the fastest by its shorter run.
+    float best = INFINITY;
+    for (int sc = 0; sc < kSchedules; sc++) {
+      for (int rep = 0; rep < 2; rep++) {
+        EF_CUDA(cudaEventRecord(e0, stream));
+        enqueue(sc, stream);
+        EF_CUDA(cudaEventRecord(e1, stream));
+        EF_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        EF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        ctx.kernels += (uint64_t)n_y;
+        if (ms < best) {
+          best = ms;
+          schedule = sc;
+        }
+      }
+    }
+    {
+      std::lock_guard<std::mutex> g(g_work_lock);
+      lists->schedule = schedule;
+    }
+    EF_CUDA(cudaMemsetAsync(tiles, 0, sizeof(unsigned long long), stream));
+  }
+  EF_CUDA(cudaEventRecord(e0, stream));
+  if (graphs_enabled()) {
+    // Replayed while every argument of the launches is the same (pointers
+    // included); else captured again and updated in place.
+    std::vector<uint8_t> shape, key;
+    put(shape, ctx.device);
+    put(shape, KB);
+    put(shape, fast);
+    put(shape, schedule);
+    put(shape, n_y);
+    put(shape, ragged);
+    put(shape, persistent_blocks);
+    for (const void* ptr : {(const void*)scratch.get(), (const void*)items.get(), (const void*)counters.get(),
+                            (const void*)rl, (const void*)p.out, (const void*)p.lse, (const void*)args.exp_table,
+                            (const void*)p.mask.xlen, (const void*)p.mask.jlen})
+      put(key, ptr);
+    for (int64_t x : {W, p.lnx, p.lnj, p.ne, p.ny, lnx_pad, lnj_pad, ny_pad, (int64_t)n_items, (int64_t)p.scale_kind,
+                      (int64_t)args.reverse, (int64_t)p.mask.n, p.mask.lnx, p.mask.lnj})
+      put(key, x);
+    put(key, p.scale_c);
+    for (int i = 0; i < p.mask.n; i++) {
+      put(key, p.mask.cmp[i]);
+      put(key, p.mask.off[i]);
+    }
+    ctx.graph = ctx.graphs.run(shape, key, stream, [&](cudaStream_t st) { enqueue(schedule, st); });
+  } else {
+    enqueue(schedule, stream);
+  }
+  ctx.kernels += (uint64_t)n_y;
+  ctx.schedule = schedule;
   EF_CUDA(cudaEventRecord(e1, stream));
   unsigned long long pairs = 0;
   EF_CUDA(cudaMemcpyAsync(st, status + 1, 4, cudaMemcpyDeviceToHost, stream));

@@ -9,6 +9,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -175,6 +176,27 @@ struct KeptScratch {
   }
 };
 
+// Instantiated CUDA graphs of a context's launch sequences. An entry is
+// replayed only when every argument its launches were captured with
+// (pointers included) is the same; otherwise the sequence is captured again
+// and, where an entry of the same shape (kernels, grids) exists, updated
+// into it.
+struct GraphCache {
+  struct Entry {
+    std::vector<uint8_t> shape, key;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t used = 0;
+  };
+  std::vector<Entry> entries;
+  uint64_t clock = 0;
+  static constexpr size_t kMaxEntries = 8;
+  // Launches `enqueue`'s work (queued on the stream it is given) on
+  // `stream` through a graph: 1 replayed, 2 updated, 3 instantiated.
+  int run(const std::vector<uint8_t>& shape, const std::vector<uint8_t>& key, cudaStream_t stream,
+          const std::function<void(cudaStream_t)>& enqueue);
+  void clear();
+};
+
 struct Context {
   // With EINFOLD_TRACE set, phase() synchronizes the stream and prints the
   // milliseconds since the previous phase to stderr.
@@ -189,6 +211,10 @@ struct Context {
   double product_ms = 0, product_ops = 0;  // the split products' kernels in the current call
   PinnedArena pinned;
   KeptScratch kept;  // the attention backward's exports
+  GraphCache graphs;
+  // The current call's attention forward: its schedule (-1: none) and how
+  // its tile phase ran (0 launched directly, else GraphCache::run's value).
+  int schedule = -1, graph = 0;
   // Device-resident scratch kept across calls.
   void* status_word = nullptr;  // int32 status set by bounded device waits
 };

@@ -362,6 +362,11 @@ class CallInfo:
     device_ms: float = 0.0
     product_ms: float = 0.0
     product_ops: float = 0.0
+    # Split attention forwards: the schedule (0 a block per item, 1
+    # persistent by key tiles, 2 persistent by batch; -1 other calls) and the
+    # graph launch (0 direct, 1 replayed, 2 updated, 3 instantiated).
+    schedule: int = -1
+    graph: int = 0
     message: str = ""
 
 
@@ -397,6 +402,8 @@ def _call(fn, *args) -> Optional[_lib.Result]:
     last_call.device_ms = res.device_ms
     last_call.product_ms = res.product_ms
     last_call.product_ops = res.product_ops
+    last_call.schedule = res.schedule
+    last_call.graph = res.graph
     last_call.message = msg
     if status == _lib.DECLINED:
         return None
