@@ -476,6 +476,9 @@ def run_ours(args):
     ranking = _ranking(hbm, basis) if not args.no_ranking else None
     ragged = _ragged() if not args.no_ragged else None
     sparse = _sparse(cpu=rank == 0 and world == 1 and not args.no_cpu) if not args.no_sparse else None
+    smoother = _smoother(cpu=rank == 0 and world == 1 and not args.no_cpu) if not args.no_smoother else None
+    config1 = _config1(cpu=rank == 0 and world == 1 and not args.no_cpu) if not args.no_configs else None
+    config5 = _config5() if not args.no_configs else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -509,6 +512,9 @@ def run_ours(args):
             "ranking": ranking,
             "ragged": ragged,
             "sparse": sparse,
+            "smoother": smoother,
+            "config1": config1,
+            "config5": config5,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "attention_forward_launch": fwd_launch,
@@ -720,6 +726,190 @@ def _sparse(cpu=False):
     return out
 
 
+def _smoother(cpu=False):
+    """Config 4's second part, the Gaussian smoother: per group (64), 2^20
+    query positions x and 256 key positions y uniform[0, 1) and values v
+    normal(0, 1); out(b, x) = sum_y w v / sum_y w with FP64 weights
+    w = exp(-power(x - y, 2) / h), h = 0.01, as a pipeline whose scores are
+    the row expression -power(q.x - k.x, 2) over one feature and whose
+    weight is exp(s / h) without a shift. The tables (b, t, d, x) are in
+    HBM (2.1 GB of q); the result stays there. Pairs per second, timed with
+    CUDA events; the error of group 0's first 4,096 rows against torch
+    float64."""
+    import pyarrow as pa
+    import torch
+
+    from einfold_b200 import cases as C
+    from einfold_b200 import kernels as K
+
+    groups, nx, ny, h = 64, 1 << 20, 256, 0.01
+    pipe = C.smoother_pipeline(h)
+    q, k, v, xs, ys, vs = C.smoother_tables(groups, nx, ny, SEED)
+    pairs = groups * nx * ny
+    opts = K.Options(result_on_device=True)
+    times, got = [], None
+    for _ in range(4):
+        if got is not None:
+            for batch in got.batches:
+                batch.release()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        got = K.pipeline(pipe, [q, k, v], options=opts)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = statistics.median(times[1:])
+    vals = got.batches[0].column(2)
+    rows = 4096
+    x0, y0, v0 = xs[:rows], ys[:ny], vs[:ny]
+    w = torch.exp(-(x0[:, None] - y0[None, :]) ** 2 / h)
+    want = (w @ v0) / w.sum(1)
+    err = ((vals[:rows] - want).abs().max() / want.abs().max()).item()
+    out = {"groups": groups, "x_per_group": nx, "y_per_group": ny, "h": h, "pairs": pairs, "ms": ms,
+           "gpairs_per_s": pairs / ms / 1e6, "rows_out": sum(b.rows for b in got.batches),
+           "tiles_visited": got.tiles_visited, "max_rel_err_vs_torch_f64": err,
+           "kernel": "fused_tiles (FP64 scores and weights on the CUDA cores)"}
+    for batch in got.batches:
+        batch.release()
+    if cpu:
+        # The CPU leg: the oracle's restatement of fused::pipeline on group
+        # 0's first 16,384 positions (one host thread a call).
+        from oracle import oracle
+
+        oracle.build()
+        n = 16384
+
+        def host(cols, names):
+            return [pa.record_batch([pa.array(c.cpu().numpy()) for c in cols], names=names)]
+
+        zeros = torch.zeros(n, dtype=torch.int64)
+        qa = host([zeros, torch.arange(n), zeros, xs[:n]], ["b", "t", "d", "x"])
+        ka = host([zeros[:ny], torch.arange(ny), zeros[:ny], ys[:ny]], ["b", "t", "d", "x"])
+        va = host([zeros[:ny], torch.arange(ny), vs[:ny]], ["b", "t", "x"])
+        schema = oracle.pipeline_schema(pipe, [qa[0].schema, ka[0].schema, va[0].schema])
+        t0 = time.perf_counter()
+        oracle.pipeline(pipe, qa, ka, va, schema, oracle.Options(threads=1))
+        sec = time.perf_counter() - t0
+        out["cpu_oracle"] = {"seconds": sec, "pairs": n * ny, "gpairs_per_s": n * ny / sec / 1e9, "cores": 1}
+    del q, k, v, xs, ys, vs
+    torch.cuda.empty_cache()
+    return out
+
+
+def _config1(cpu=False):
+    """The plain matmul fold at 512 x 512 . 512 x 256 (2·512·512·256 FLOP)
+    through einfold_fold from host Arrow tables (rows shuffled, four batches
+    an operand) to host results, timed end to end on the host clock around
+    each call (the copies in, the kernels, the copies out): with 1% of b's
+    values NULL (the reference sends that to its discrimination algorithm,
+    and so does this library) and complete (the dense product). The CPU leg
+    runs the oracle's restatement of the same fold on one host thread."""
+    import torch
+
+    from einfold_b200 import cases as C
+    from einfold_b200 import kernels as K
+
+    f = _matmul_fold()
+    flop = 2.0 * 512 * 512 * 256
+    out = {"flop": flop}
+    for name, nulls in (("nulls_in_b", True), ("complete", False)):
+        (sa, a), (sb, b) = C.config1_tables(nulls, SEED)
+        ra, rb = K.Relation(sa, a), K.Relation(sb, b)
+        times, device_ms, got = [], [], None
+        for _ in range(6):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            got = K.fold(f, ra, rb)
+            torch.cuda.synchronize()
+            times.append((time.perf_counter() - t0) * 1e3)
+            device_ms.append(K.last_call.device_ms)
+        ms = statistics.median(times[1:])
+        leg = {"algorithm": got.algorithm.name.lower(), "rows_out": sum(x.num_rows for x in got.batches),
+               "e2e_ms": ms, "e2e_gflop_per_s": flop / ms / 1e6, "device_ms": statistics.median(device_ms[1:])}
+        if cpu:
+            from oracle import oracle
+
+            oracle.build()
+            t0 = time.perf_counter()
+            want = oracle.fold(f, sa, a, sb, b, None, oracle.schema(f, [sa, sb]))
+            sec = time.perf_counter() - t0
+            leg["cpu_oracle"] = {"seconds": sec, "gflop_per_s": flop / sec / 1e9, "cores": 1,
+                                 "rows_out": sum(x.num_rows for x in want.batches)}
+        out[name] = leg
+    return out
+
+
+def _config5():
+    """The gradient shapes at their own sizes: the causal attention backward
+    at B=2 H=16 T=2048 d=64 (q, k, v normal(0, 1/8), d_out normal(0, 1);
+    FLOP 2.5 x the forward's 4·B·H·T²·d·(T+1)/(2T)) and the matmul fold's
+    forward and gradients at 4096² (dA = dC·Bᵀ, dB = Aᵀ·dC: 3 x 2·4096³
+    FLOP; a, b uniform[-1, 1], dC normal(0, 1)), each in the split form and
+    the FP64 forms, timed with CUDA events (median of 3 after a first call),
+    with the split results' normwise errors against the FP64 ones."""
+    import torch
+
+    from einfold_b200 import autograd as A
+    from einfold_b200 import synthetic as S
+    from einfold_b200.kernels import Precision
+
+    def timed(fn):
+        fn()
+        times = []
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            r = fn()
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        return statistics.median(times), r
+
+    def rel(x, y):
+        return ((x - y).norm() / y.norm()).item()
+
+    b_, h_, t_, d_ = 2, 16, 2048, 64
+    n = b_ * h_ * t_ * d_
+    q, k, v = (S.normal(SEED, salt, n, 1.0 / 8).view(b_, h_, t_, d_) for salt in (41, 42, 43))
+    d_out = S.normal(SEED, 44, n, 1.0).view(b_, h_, t_, d_)
+    causal = A.causal()
+    bwd_flop = 2.5 * 4.0 * b_ * h_ * t_ * t_ * d_ * (t_ + 1) / (2 * t_)
+    att = {"shape": {"B": b_, "H": h_, "T": t_, "d": d_}, "flop": bwd_flop}
+    grads = {}
+    for name, prec in (("split", Precision.SPLIT), ("fp64_tiles", Precision.FP64)):
+        out, lse = A.attention_forward(q, k, v, causal, 1.0, prec)
+        ms, g = timed(lambda: A.attention_backward(q, k, v, out, lse, d_out, causal, 1.0, prec))
+        grads[name] = g
+        att[name] = {"ms": ms, "tflop_per_s": bwd_flop / ms / 1e9}
+    att["split_norm_rel_err"] = {x: rel(a, b) for x, a, b in zip(("d_q", "d_k", "d_v"), grads["split"],
+                                                                   grads["fp64_tiles"])}
+    att["ratio_split_over_fp64"] = att["fp64_tiles"]["ms"] / att["split"]["ms"]
+    del q, k, v, d_out, grads
+    m = 4096
+    a = S.uniform(SEED, 45, m * m).view(m, m)
+    b = S.uniform(SEED, 46, m * m).view(m, m)
+    dc = S.normal(SEED, 47, m * m).view(m, m)
+    mm_flop = 3 * 2.0 * m ** 3
+    mm = {"n": m, "flop": mm_flop}
+    res = {}
+    for name, prec in (("split", Precision.SPLIT), ("fp64_reference_order", Precision.FP64), ("cublas_dgemm", None)):
+        def step():
+            x, y = a.clone().requires_grad_(), b.clone().requires_grad_()
+            c = A.matmul(x, y, prec) if prec is not None else x @ y
+            c.backward(dc)
+            return c.detach(), x.grad, y.grad
+        ms, r = timed(step)
+        res[name] = r
+        mm[name] = {"ms": ms, "tflop_per_s": mm_flop / ms / 1e9}
+    mm["split_norm_rel_err"] = {x: rel(p_, q_) for x, p_, q_ in zip(("c", "d_a", "d_b"), res["split"],
+                                                                     res["cublas_dgemm"])}
+    mm["ratio_split_over_dgemm"] = mm["cublas_dgemm"]["ms"] / mm["split"]["ms"]
+    del a, b, dc, res
+    torch.cuda.empty_cache()
+    return {"attention_backward": att, "matmul_gradients": mm}
+
+
 def _profiled_traffic(component):
     """DRAM bytes per step of a component's product kernel, from the committed
     ncu summary (`traffic_bytes_per_launch:` line), or None."""
@@ -747,6 +937,8 @@ def main():
     p.add_argument("--no-ranking", action="store_true")
     p.add_argument("--no-ragged", action="store_true")
     p.add_argument("--no-sparse", action="store_true")
+    p.add_argument("--no-smoother", action="store_true")
+    p.add_argument("--no-configs", action="store_true")
     args = p.parse_args()
     if args.impl == "reference":
         run_reference(args)

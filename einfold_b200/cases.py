@@ -5,6 +5,7 @@
     python -m einfold_b200.cases rank --n 67108864 [--repeat 3]
     python -m einfold_b200.cases ragged [--groups 64 --d 128 --window 512 --repeat 3]
     python -m einfold_b200.cases sparse
+    python -m einfold_b200.cases smoother [--groups 64 --x 1048576 --y 256]
 
 ``attention`` runs the split causal attention forward (and backward) over
 q, k, v normal(0, 1/8) and d_out normal(0, 1) (SplitMix64, seed 0);
@@ -15,8 +16,10 @@ per second of the last of `repeat` runs, timed with CUDA events;
 ``ragged`` runs the split attention forward over ragged batches (lengths
 log-uniform in [128, 8192], a window of |tq - tk| <= radius) and prints
 the FLOP rate on the allowed pairs; ``sparse`` runs the discrimination
-fold once on the sorting path's tables at 1/40 size (the bench's). Each
-prints one line and exits 0 when the kernels ran.
+fold once on the sorting path's tables at 1/40 size (the bench's);
+``smoother`` runs the Gaussian smoother pipeline (x positions a group, y
+key positions, h = 0.01) once. Each prints one line and exits 0 when the
+kernels ran.
 """
 from __future__ import annotations
 
@@ -141,6 +144,91 @@ def sparse() -> None:
     print(f"sparse: {pairs} pair products, {rows} groups ({got.algorithm.name.lower()})")
 
 
+def config1_tables(nulls: bool, seed: int = 0):
+    """The plain matmul fold's tables at 512 x 512 . 512 x 256: a(i, j, v)
+    with every (i, j) of 512 x 512 and b(j, k, v) with every (j, k) of
+    512 x 256, v uniform[-1, 1] (SplitMix64 salts 31, 32), with `nulls` 1%
+    of b's v NULL (independent draws, salt 33); rows shuffled (salts 34, 35)
+    and cut into four batches at random rows (salts 36, 37). Host Arrow
+    (schema, batches) pairs."""
+    import numpy as np
+    import pyarrow as pa
+
+    def table(names, extents, salt_v, salt_perm, salt_cut, null_salt=None):
+        n = int(np.prod(extents))
+        keys = np.indices(extents).reshape(len(extents), -1)
+        vals = S.uniform(seed, salt_v, n, device="cpu").numpy()
+        mask = S.units(seed, null_salt, n, device="cpu").numpy() < 0.01 if null_salt else None
+        order = np.argsort(S.u64(seed, salt_perm, n, device="cpu").numpy(), kind="stable")
+        cuts = np.sort((S.units(seed, salt_cut, 3, device="cpu").numpy() * n).astype(np.int64))
+        bounds = [0, *cuts.tolist(), n]
+        schema = pa.schema([(c, pa.int64()) for c in names] + [("v", pa.float64())])
+        batches = []
+        for lo, hi in zip(bounds[:-1], bounds[1:]):
+            rows = order[lo:hi]
+            cols = [pa.array(keys[c][rows]) for c in range(len(names))]
+            cols.append(pa.array(vals[rows], mask=mask[rows] if mask is not None else None))
+            batches.append(pa.record_batch(cols, schema=schema))
+        return schema, batches
+
+    a = table(["i", "j"], [512, 512], 31, 34, 36)
+    b = table(["j", "k"], [512, 256], 32, 35, 37, 33 if nulls else None)
+    return a, b
+
+
+def smoother_pipeline(h: float = 0.01):
+    """The Gaussian smoother as a pipeline over q(b, t, d, x), k(b, t, d, x)
+    and v(b, t, x): scores the row expression -power(q.x - k.x, 2) over one
+    feature d, FP64 weights exp(s / h) without a shift, normalised by the
+    kept groups, so out(b, t) = sum_y w v / sum_y w with
+    w = exp(-power(x - y, 2) / h)."""
+    from . import ir
+
+    E = ir.Dimension(ir.KeyEquality.EQUAL)
+    I, D, J, B = 0, 1, 2, 3
+    diff = ir.Expression.column(0, 3).binary(ir.Binary.SUBTRACT, ir.Expression.column(1, 3))
+    scores = diff.binary(ir.Binary.POWER, ir.Expression.literal(2.0)).unary(ir.Unary.NEGATE)
+    producer = ir.Fold([E, E, E, E], [ir.Operand([(B, 0), (I, 1), (D, 2)], 3),
+                                      ir.Operand([(B, 0), (J, 1), (D, 2)], 3)],
+                       [ir.Output(B), ir.Output(I), ir.Output(J)], ir.RowValue(scores))
+    return ir.Pipeline(producer, ir.Weight.exp(ir.Scale.over(h), ir.Shift.NONE), [], ir.Operand([(B, 0), (J, 1)], 2),
+                       [B, I], ir.Normalizer.KEPT_GROUPS)
+
+
+def smoother_tables(groups: int, nx: int, ny: int, seed: int = 0):
+    """Device relations q (groups x nx positions), k (groups x ny) with x
+    uniform[0, 1) (SplitMix64 salts 21, 22) and v (groups x ny) normal(0, 1)
+    (salt 23), keys b, t (and d = 0) int64; and the x, y, v tensors."""
+    import pyarrow as pa
+
+    from . import kernels as K
+
+    def table(n, salt, with_d=True):
+        b = torch.arange(groups, dtype=torch.int64, device="cuda").repeat_interleave(n)
+        t = torch.arange(n, dtype=torch.int64, device="cuda").repeat(groups)
+        cols = [b, t] + ([torch.zeros_like(t)] if with_d else [])
+        names = ["b", "t"] + (["d"] if with_d else []) + ["x"]
+        x = S.units(seed, salt, groups * n) if with_d else S.normal(seed, salt, groups * n)
+        schema = pa.schema([(c, pa.int64()) for c in names[:-1]] + [("x", pa.float64())])
+        return K.DeviceRelation(schema, cols + [x]), x
+
+    q, xs = table(nx, 21)
+    k, ys = table(ny, 22)
+    v, vs = table(ny, 23, with_d=False)
+    return q, k, v, xs, ys, vs
+
+
+def smoother(groups: int, nx: int, ny: int) -> None:
+    from . import kernels as K
+
+    q, k, v, _, _, _ = smoother_tables(groups, nx, ny)
+    got = K.pipeline(smoother_pipeline(), [q, k, v], options=K.Options(result_on_device=True))
+    rows = sum(batch.rows for batch in got.batches)
+    for batch in got.batches:
+        batch.release()
+    print(f"smoother: {groups} groups x {nx} x {ny}: {rows} rows, {got.tiles_visited} tile pairs")
+
+
 def main() -> None:
     p = argparse.ArgumentParser()
     sub = p.add_subparsers(dest="case", required=True)
@@ -157,6 +245,10 @@ def main() -> None:
     pg.add_argument("--window", type=int, default=512)
     pg.add_argument("--repeat", type=int, default=3)
     sub.add_parser("sparse")
+    ps = sub.add_parser("smoother")
+    ps.add_argument("--groups", type=int, default=64)
+    ps.add_argument("--x", type=int, default=1 << 20)
+    ps.add_argument("--y", type=int, default=256)
     pr = sub.add_parser("rank")
     pr.add_argument("--n", type=int, default=1 << 26)
     pr.add_argument("--repeat", type=int, default=3)
@@ -169,6 +261,8 @@ def main() -> None:
         ragged(args.groups, args.d, args.window, args.repeat)
     elif args.case == "sparse":
         sparse()
+    elif args.case == "smoother":
+        smoother(args.groups, args.x, args.y)
     else:
         product(args.n)
 

@@ -37,7 +37,10 @@ constexpr int kMaxSlots = 8;
 constexpr int kThreads = 256;
 
 // A postfix expression (expression.rs:61-120) over slots; column nodes
-// carry their slot in `a`. Every operation rounds once, as Rust's f64 does.
+// carry their slot in `a`. Every operation rounds once, as Rust's f64 does;
+// power(a, 2) is the product a·a, rounded once (the correctly rounded
+// square, which a power function returns up to its own rounding error; the
+// same NaN, infinities and signed zeros).
 __device__ double eval(const ExprNode* __restrict__ nodes, int n, const double* slots) {
   double st[64];
   int sp = 0;
@@ -58,7 +61,7 @@ __device__ double eval(const ExprNode* __restrict__ nodes, int n, const double* 
         case 1: r = __dsub_rn(a, b); break;
         case 2: r = __dmul_rn(a, b); break;
         case 3: r = __ddiv_rn(a, b); break;
-        default: r = pow(a, b); break;
+        default: r = b == 2.0 ? __dmul_rn(a, a) : pow(a, b); break;
       }
       st[sp - 1] = r;
     }
@@ -328,7 +331,8 @@ __global__ void __launch_bounds__(kThreads) fused_tiles(const TileArgs p) {
       const int r = ty + 16 * i;
       if (r >= rows) continue;
       const int lo = S.lo[r], hi = S.hi[r];
-      if (lo >= hi) continue;
+      // A thread whose outputs tx + 16 jj are all past the chunk's holds none.
+      if (lo >= hi || tx >= ycount) continue;
       if (S.pend[r]) {
         const double rescale = S.resc[r];
         for (int jj = 0; jj < 4; jj++) {

@@ -129,19 +129,43 @@ class _CudaArray:
                                          "strides": None}
 
 
+class _DeviceResult:
+    """A library result whose buffers are in HBM, released once."""
+
+    def __init__(self, res):
+        self.res = res
+
+    def release(self):
+        if self.res is not None:
+            _lib.load().einfold_result_release(ctypes.byref(self.res))
+            self.res = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
 class DeviceBatch:
-    """A result whose buffers are in HBM, owned until :meth:`release`."""
+    """A result batch whose buffers are in HBM, owned until :meth:`release`
+    (which frees every batch of the same result)."""
 
     _TYPESTR = {b"c": "|i1", b"C": "|u1", b"s": "<i2", b"S": "<u2", b"i": "<i4", b"I": "<u4", b"l": "<i8",
                 b"L": "<u8", b"f": "<f4", b"g": "<f8"}
 
-    def __init__(self, res):
-        self._res = res
-        self.rows = int(res.batches[0].length) if res.n_batches else 0
+    def __init__(self, res, index: int = 0, owner: Optional[_DeviceResult] = None):
+        self._owner = owner or _DeviceResult(res)
+        self._i = index
+        self.rows = int(res.batches[index].length) if index < res.n_batches else 0
         self.formats = []
         s = res.schema.contents
         for i in range(s.n_children):
             self.formats.append(s.children[i].contents.format)
+
+    @property
+    def _res(self):
+        return self._owner.res
 
     def column(self, i: int):
         """Column i's values as a CUDA tensor sharing the result's memory
@@ -150,7 +174,7 @@ class DeviceBatch:
 
         if self.formats[i] not in self._TYPESTR:
             raise TypeError(f"column {i} has Arrow format {self.formats[i]!r}: use strings({i})")
-        arr = self._res.batches[0].children[i].contents
+        arr = self._res.batches[self._i].children[i].contents
         ptr = arr.buffers[1]
         return torch.as_tensor(_CudaArray(ptr or 0, self.rows, self._TYPESTR[self.formats[i]], self), device="cuda")
 
@@ -163,7 +187,7 @@ class DeviceBatch:
         fmt = self.formats[i]
         if fmt not in (b"u", b"z", b"U", b"Z"):
             raise TypeError(f"column {i} has Arrow format {fmt!r}, not a string or binary one")
-        arr = self._res.batches[0].children[i].contents
+        arr = self._res.batches[self._i].children[i].contents
         wide = fmt in (b"U", b"Z")
         offsets = torch.as_tensor(_CudaArray(arr.buffers[1] or 0, self.rows + 1, "<i8" if wide else "<i4", self),
                                   device="cuda")
@@ -172,18 +196,16 @@ class DeviceBatch:
         return offsets, data
 
     def null_count(self, i: int) -> int:
-        return int(self._res.batches[0].children[i].contents.null_count)
+        return int(self._res.batches[self._i].children[i].contents.null_count)
 
     def release(self):
-        if self._res is not None:
-            _lib.load().einfold_result_release(ctypes.byref(self._res))
-            self._res = None
+        self._owner.release()
 
-    def __del__(self):
-        try:
-            self.release()
-        except Exception:
-            pass
+
+def _device_batches(res) -> List[DeviceBatch]:
+    """A result's batches left in HBM (at least one, perhaps of no rows)."""
+    owner = _DeviceResult(res)
+    return [DeviceBatch(res, i, owner) for i in range(max(1, int(res.n_batches)))]
 
 
 @dataclass
@@ -433,7 +455,7 @@ def fold(f: ir.Fold, a, b, domain=None, schema: Optional[pa.Schema] = None,
             raise ArrowComputeError("the fold declined")
         alg = Algorithm(_lib.ALGORITHMS[res.algorithm])
         if options.result_on_device:
-            return Folded(alg, [DeviceBatch(res)])
+            return Folded(alg, _device_batches(res))
         return Folded(alg, _collect(res))
     finally:
         keep.release()
@@ -450,7 +472,9 @@ def fold_dense(f: ir.Fold, a, b, domain=None, schema: Optional[pa.Schema] = None
                     ctypes.byref(_relation(a, keep)), ctypes.byref(_relation(b, keep)),
                     ctypes.byref(_relation(domain, keep)) if domain is not None else None,
                     ctypes.byref(_options(options, keep)), options.device)
-        return None if res is None else _collect(res)
+        if res is None:
+            return None
+        return _device_batches(res) if options.result_on_device else _collect(res)
     finally:
         keep.release()
 
@@ -465,7 +489,9 @@ def fold_chain(f: ir.Fold, operands: Sequence, schema: Optional[pa.Schema] = Non
         rels = keep.add(_array(_lib.Relation, [_relation(r, keep) for r in operands]))
         res = _call(_lib.load().einfold_fold_chain, ctypes.byref(_fold_desc(f, keep)), rels,
                     ctypes.byref(_options(options, keep)), options.device)
-        return None if res is None else _collect(res)
+        if res is None:
+            return None
+        return _device_batches(res) if options.result_on_device else _collect(res)
     finally:
         keep.release()
 
@@ -483,7 +509,7 @@ def pipeline(p: ir.Pipeline, operands: Sequence, schema: Optional[pa.Schema] = N
         if res is None:
             return None
         visited, tiles = int(res.tiles_visited), int(res.tiles)
-        return Piped(_collect(res), visited, tiles)
+        return Piped(_device_batches(res) if options.result_on_device else _collect(res), visited, tiles)
     finally:
         keep.release()
 

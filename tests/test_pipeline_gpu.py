@@ -204,3 +204,27 @@ def test_empty_relations():
     assert (got is None) == (want is None)
     if got is not None:
         assert rows_of(got.batches).num_rows == rows_of(want.batches).num_rows == 0
+
+
+def test_results_left_in_hbm_match_the_host_result():
+    # result_on_device: the same rows as the host result, as DeviceBatch
+    # columns (the Gaussian smoother's pipeline, two batches of positions).
+    import torch
+
+    case = P.attention(300, d=1, lk=90, nb=2, scores=P.gaussian_scores(),
+                       weight=ir.Weight.exp(ir.Scale.over(0.01), ir.Shift.NONE),
+                       q_value=lambda n: oracle.Rng.seeded(10, 3).units(n),
+                       k_value=lambda n: oracle.Rng.seeded(11, 3).units(n),
+                       v_value=lambda n: oracle.Rng.seeded(12, 3).units(n) * 2 - 1)
+    host = rows_of(_gpu(case).batches)
+    got = _gpu(case, K.Options(result_on_device=True))
+    try:
+        assert len(got.batches) == 1 and isinstance(got.batches[0], K.DeviceBatch)
+        dev = got.batches[0]
+        assert dev.rows == host.num_rows
+        for c in range(host.num_columns):
+            assert np.array_equal(dev.column(c).cpu().numpy(), host.column(c).to_numpy()), f"column {c}"
+        assert isinstance(dev.column(0), torch.Tensor)
+    finally:
+        for b in got.batches:
+            b.release()
