@@ -35,19 +35,23 @@ constexpr int XT = 64, JT = 64;  // fused.rs XT, JT: tiles visited count in thes
 constexpr int YC = 64;           // outputs per CTA along y
 constexpr int kMaxSlots = 8;
 constexpr int kThreads = 256;
+constexpr int kNarrow = 8;       // value columns up to which a chunk sums by half-warp reductions
 
 // A postfix expression (expression.rs:61-120) over slots; column nodes
 // carry their slot in `a`. Every operation rounds once, as Rust's f64 does;
 // power(a, 2) is the product a·a, rounded once (the correctly rounded
 // square, which a power function returns up to its own rounding error; the
 // same NaN, infinities and signed zeros).
-__device__ double eval(const ExprNode* __restrict__ nodes, int n, const double* slots) {
-  double st[64];
+// DEPTH bounds the stack (the host passes the expressions' deepest);
+// slot(i) reads slot i.
+template <int DEPTH, class Slot>
+__device__ __forceinline__ double eval(const ExprNode* __restrict__ nodes, int n, Slot slot) {
+  double st[DEPTH];
   int sp = 0;
   for (int i = 0; i < n; i++) {
     const ExprNode e = nodes[i];
     if (e.kind == 0) {
-      st[sp++] = slots[e.a];
+      st[sp++] = slot(e.a);
     } else if (e.kind == 1) {
       st[sp++] = e.value;
     } else if (e.kind == 2) {
@@ -69,16 +73,43 @@ __device__ double eval(const ExprNode* __restrict__ nodes, int n, const double* 
   return st[0];
 }
 
+// The interpreter out of line, once per kind of call (a row expression
+// over slots; a weight expression of the score).
+template <int DEPTH>
+__device__ __noinline__ double eval_slots(const ExprNode* __restrict__ nodes, int n, const double* slots) {
+  return eval<DEPTH>(nodes, n, [slots](int k) { return slots[k]; });
+}
+template <int DEPTH>
+__device__ __noinline__ double eval_score(const ExprNode* __restrict__ nodes, int n, double score) {
+  return eval<DEPTH>(nodes, n, [score](int) { return score; });
+}
+
 enum : uint8_t { J_FINITE = 1, J_INFINITE = 2 };
+
+// Expressions the tile kernel computes without the interpreter: the same
+// operations in the same order, so the same bits.
+enum ScoreShape : int {
+  SCORE_INTERPRETED = 0,
+  SCORE_NEG_SQUARED_DIFF = 1,  // -power(a - b, 2), a Gaussian kernel's exponent
+};
+enum WeightShape : int {
+  WEIGHT_INTERPRETED = 0,
+  WEIGHT_SIGMOID = 1,  // c1 / (c2 + exp(-s))
+  WEIGHT_CAUCHY = 2,   // c1 / (c2 + s * s)
+};
 
 struct TileArgs {
   int64_t nx, ne, nj, ny;
   Mask mask;
   int weight_expr, scale_kind, shifted, normalizer;
   double scale_c;
+  double wc1, wc2;  // the weight shape's constants
   const ExprNode* wnodes;
   int wn;
+  int weight_shape;  // WeightShape: a weight expression computed without the interpreter
   int score_expr;
+  int score_shape;   // ScoreShape, with the two slots it reads
+  int shape_a, shape_b;
   const double* q;  // [x][e]
   const double* k;  // [j][e]
   const ExprNode* snodes;
@@ -103,9 +134,23 @@ __device__ __forceinline__ double warp_min(double v) {
   for (int o = 16; o; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
-__device__ __forceinline__ double warp_sum(double v) {
-  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+// Reductions over the 16 lanes of a half-warp (every lane of the warp calls).
+__device__ __forceinline__ double half_max(double v) {
+  for (int o = 8; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
+}
+__device__ __forceinline__ double half_min(double v) {
+  for (int o = 8; o; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double half_sum(double v) {
+  for (int o = 8; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ bool half_or(bool b) {
+  int v = b;
+  for (int o = 8; o; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
+  return v != 0;
 }
 
 struct RowState {
@@ -118,6 +163,7 @@ struct RowState {
 constexpr int kStage = 32 * 65;  // doubles in one staged operand chunk (e rows of 64 + 1)
 constexpr size_t kTileSmem = sizeof(double) * (XT * (JT + 1) + 2 * kStage) + sizeof(RowState);
 
+template <int DEPTH>
 __global__ void __launch_bounds__(kThreads) fused_tiles(const TileArgs p) {
   extern __shared__ __align__(16) unsigned char smem[];
   double(*blk)[JT + 1] = reinterpret_cast<double(*)[JT + 1]>(smem);
@@ -125,7 +171,7 @@ __global__ void __launch_bounds__(kThreads) fused_tiles(const TileArgs p) {
   RowState& S = *reinterpret_cast<RowState*>(smem + sizeof(double) * (XT * (JT + 1) + 2 * kStage));
   __shared__ long long s_first, s_last;
 
-  const int t = threadIdx.x, tx = t & 15, ty = t >> 4, warp = t >> 5, lane = t & 31;
+  const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
   const int64_t x0 = (int64_t)blockIdx.x * XT;
   const int rows = (int)std::min<int64_t>(XT, p.nx - x0);
   const int64_t y0 = (int64_t)blockIdx.y * YC;
@@ -213,143 +259,274 @@ __global__ void __launch_bounds__(kThreads) fused_tiles(const TileArgs p) {
         }
         __syncthreads();
       }
+    } else if (p.score_shape == SCORE_NEG_SQUARED_DIFF) {
+      // -power(a - b, 2) summed over E, a row's and a column's values per
+      // slot loaded once for the thread's 4 rows and 4 columns.
+      const double* ma = p.mats[p.shape_a];
+      const double* mb = p.mats[p.shape_b];
+      const bool a_row = p.side[p.shape_a] == 0, b_row = p.side[p.shape_b] == 0;
+      for (int64_t e = 0; e < p.ne; e++) {
+        double ar[4], ac[4], br[4], bc[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          const int r = ty + 16 * i, j = tx + 16 * i;
+          const int64_t xr = (x0 + (r < rows ? r : 0)) * p.ne + e, jc = (j0 + (j < width ? j : 0)) * p.ne + e;
+          ar[i] = a_row ? ma[xr] : 0.0;
+          br[i] = b_row ? mb[xr] : 0.0;
+          ac[i] = a_row ? 0.0 : ma[jc];
+          bc[i] = b_row ? 0.0 : mb[jc];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+          for (int jj = 0; jj < 4; jj++) {
+            const double d = __dsub_rn(a_row ? ar[i] : ac[jj], b_row ? br[i] : bc[jj]);
+            const double val = -__dmul_rn(d, d);
+            s[i][jj] = e == 0 ? val : __dadd_rn(s[i][jj], val);
+          }
+      }
     } else {
+      // One interpreter call site (a rolled loop through shared memory):
+      // copies of it unrolled overflow the instruction cache.
       double slots[kMaxSlots];
+      for (int q = 0; q < 16; q++) {
+        const int r = ty + 16 * (q >> 2), j = tx + 16 * (q & 3);
+        double acc_s = 0.0;
+        if (r < rows && j < width) {
+          for (int64_t e = 0; e < p.ne; e++) {
+            for (int sl = 0; sl < p.n_slots; sl++)
+              slots[sl] = p.side[sl] == 0 ? p.mats[sl][(x0 + r) * p.ne + e] : p.mats[sl][(j0 + j) * p.ne + e];
+            const double val = eval_slots<DEPTH>(p.snodes, p.sn, slots);
+            acc_s = e == 0 ? val : __dadd_rn(acc_s, val);
+          }
+        }
+        blk[r][j] = acc_s;
+      }
+      __syncwarp();
+#pragma unroll
       for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int jj = 0; jj < 4; jj++) s[i][jj] = blk[ty + 16 * i][tx + 16 * jj];
+      __syncwarp();
+    }
+    // Weights and the row state (fused.rs:811-909). A thread weighs its
+    // 4 x 4 pairs (rows ty + 16 i, columns tx + 16 jj); a row's 64 columns
+    // are the 16 threads of a half-warp, whose reductions run over lane
+    // offsets 8, 4, 2, 1 (every lane takes part: rows outside the tile or
+    // with no pair here reduce neutral values). The thread with tx = 0
+    // keeps the row's state.
+    double w[4][4];
+    {
+      double lgc[4], smc[4];
+      uint8_t fc[4];
+      #pragma unroll
+      for (int jj = 0; jj < 4; jj++) {
+        const int j = tx + 16 * jj;
+        const bool live = j < width;
+        fc[jj] = live ? p.jflag[j0 + j] : J_FINITE;
+        lgc[jj] = live ? p.largest[j0 + j] : 0.0;
+        smc[jj] = live ? p.smallest[j0 + j] : POS_INF;
+      }
+      #pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int r = ty + 16 * i;
+        const bool row = r < rows;
+        const int lo = row ? S.lo[r] : 0, hi = row ? S.hi[r] : 0;
+        const bool active = lo < hi;  // the same for the half-warp
+        bool in[4];
+        #pragma unroll
+        for (int jj = 0; jj < 4; jj++) in[jj] = tx + 16 * jj >= lo && tx + 16 * jj < hi;
+        double lg = 0.0, sm = POS_INF;
+        #pragma unroll
         for (int jj = 0; jj < 4; jj++) {
-          const int r = ty + 16 * i, j = tx + 16 * jj;
-          double acc_s = 0.0;
-          if (r < rows && j < width) {
-            for (int64_t e = 0; e < p.ne; e++) {
-              for (int sl = 0; sl < p.n_slots; sl++)
-                slots[sl] = p.side[sl] == 0 ? p.mats[sl][(x0 + r) * p.ne + e] : p.mats[sl][(j0 + j) * p.ne + e];
-              const double val = eval(p.snodes, p.sn, slots);
-              acc_s = e == 0 ? val : __dadd_rn(acc_s, val);
+          lg = fmax(lg, in[jj] ? lgc[jj] : 0.0);
+          sm = fmin(sm, in[jj] ? smc[jj] : POS_INF);
+        }
+        lg = half_max(lg);
+        sm = half_min(sm);
+        // State read by the half-warp before its tx = 0 thread writes it.
+        const double m_old = row ? S.m[r] : 0.0;
+        __syncwarp();
+        if (map) {
+          double ha = NEG_INF, la = POS_INF, sum = 0.0;
+          bool bad = false;
+          #pragma unroll
+          for (int jj = 0; jj < 4; jj++) {
+            const double sc = s[i][jj];
+            double x = 0.0;
+            if (in[jj]) {
+              if (p.weight_shape == WEIGHT_SIGMOID) x = __ddiv_rn(p.wc1, __dadd_rn(p.wc2, exp(-sc)));
+              else if (p.weight_shape == WEIGHT_CAUCHY) x = __ddiv_rn(p.wc1, __dadd_rn(p.wc2, __dmul_rn(sc, sc)));
+              else x = eval_score<DEPTH>(p.wnodes, p.wn, sc);
+            }
+            w[i][jj] = x;
+            bad |= in[jj] && (!isfinite(x) || !(fc[jj] & J_FINITE));
+            const double ax = fabs(x);
+            ha = fmax(ha, in[jj] ? ax : NEG_INF);
+            la = fmin(la, in[jj] && ax != 0.0 ? ax : POS_INF);
+            sum += in[jj] ? x : 0.0;
+          }
+          ha = half_max(ha);
+          la = half_min(la);
+          sum = half_sum(sum);
+          bad = half_or(bad);
+          if (tx == 0 && active) {
+            S.terms[r] += hi - lo;
+            S.rl[r] = fmax(S.rl[r], lg);
+            S.rs[r] = fmin(S.rs[r], sm);
+            if (bad) over = true;
+            S.high[r] = fmax(S.high[r], ha);
+            S.light[r] = fmin(S.light[r], la);
+            S.z[r] += sum;
+          }
+        } else {
+          double sc[4];
+          double hs = NEG_INF, ls = POS_INF, lows = POS_INF, mx = NEG_INF;
+          bool any_nan = false, special_values = false;
+          #pragma unroll
+          for (int jj = 0; jj < 4; jj++) {
+            double x = s[i][jj];
+            if (in[jj]) {
+              if (p.scale_kind == 1) x = x * p.scale_c;
+              else if (p.scale_kind == 2) x = __ddiv_rn(x, p.scale_c);
+            }
+            sc[jj] = x;
+            const bool fin = in[jj] && isfinite(x);
+            hs = fmax(hs, fin ? x : NEG_INF);
+            ls = fmin(ls, fin ? x : POS_INF);
+            lows = fmin(lows, fin && (fc[jj] & J_INFINITE) ? x : POS_INF);
+            any_nan |= in[jj] && isnan(x);
+            mx = fmax(mx, in[jj] && !isnan(x) ? x : NEG_INF);
+            special_values |= in[jj] && !(fc[jj] & J_FINITE);
+          }
+          hs = half_max(hs);
+          ls = half_min(ls);
+          lows = half_min(lows);
+          mx = half_max(mx);
+          any_nan = half_or(any_nan);
+          special_values = half_or(special_values);
+          // The largest score so far, or NaN once any score is NaN.
+          const double shift = shifted ? ((isnan(m_old) || any_nan) ? NAN : fmax(m_old, mx)) : 0.0;
+          // Every score so far -inf: weights 0 here, and the row's state
+          // past its score bounds stays.
+          const bool none = shift == NEG_INF;
+          double sum = 0.0;
+          bool special_weights = false;
+          #pragma unroll
+          for (int jj = 0; jj < 4; jj++) {
+            const double x = in[jj] && !none ? exp(sc[jj] - shift) : 0.0;
+            w[i][jj] = x;
+            sum += x;
+            special_weights |= in[jj] && !none && !isfinite(x);
+          }
+          sum = half_sum(sum);
+          special_weights = half_or(special_weights);
+          if (tx == 0 && active) {
+            S.terms[r] += hi - lo;
+            S.rl[r] = fmax(S.rl[r], lg);
+            S.rs[r] = fmin(S.rs[r], sm);
+            S.high[r] = fmax(S.high[r], hs);
+            S.light[r] = fmin(S.light[r], ls);
+            S.low[r] = fmin(S.low[r], lows);
+            if (!none) {
+              const double rescale = exp(m_old - shift);
+              S.sw_before[r] = S.sw[r];
+              if (shifted && rescale != 1.0) {
+                // overflows(z, a, ...) before the rescale: z's part here,
+                // a's by the threads that hold a.
+                if (!S.sw[r] && !isfinite(S.z[r])) over = true;
+                S.z[r] *= rescale;
+                S.pend[r] = 1;
+                S.resc[r] = rescale;
+              }
+              S.sw[r] |= special_weights;
+              S.spv[r] = special_values;
+              if (unnormalized && (special_weights || special_values)) over = true;
+              S.z[r] += sum;
+              S.m[r] = shift;
             }
           }
-          s[i][jj] = acc_s;
         }
-    }
-    for (int i = 0; i < 4; i++)
-      for (int jj = 0; jj < 4; jj++) blk[ty + 16 * i][tx + 16 * jj] = s[i][jj];
-    __syncthreads();
-
-    // Weights and the row state (fused.rs:811-909), a warp per row.
-    for (int rr = 0; rr < XT / 8; rr++) {
-      const int r = warp * (XT / 8) + rr;
-      if (r >= rows) continue;
-      const int lo = S.lo[r], hi = S.hi[r];
-      if (lo >= hi) continue;
-      const int ja = lane, jb = lane + 32;
-      const bool ina = ja >= lo && ja < hi, inb = jb >= lo && jb < hi;
-      const uint8_t fa = ina ? p.jflag[j0 + ja] : J_FINITE, fb = inb ? p.jflag[j0 + jb] : J_FINITE;
-      {
-        const double lg = fmax(ina ? p.largest[j0 + ja] : 0.0, inb ? p.largest[j0 + jb] : 0.0);
-        const double sm = fmin(ina ? p.smallest[j0 + ja] : POS_INF, inb ? p.smallest[j0 + jb] : POS_INF);
-        const double wlg = warp_max(lg), wsm = warp_min(sm);
-        if (lane == 0) {
-          S.terms[r] += hi - lo;
-          S.rl[r] = fmax(S.rl[r], wlg);
-          S.rs[r] = fmin(S.rs[r], wsm);
-        }
-      }
-      double sa = ina ? blk[r][ja] : 0.0, sb = inb ? blk[r][jb] : 0.0;
-      if (map) {
-        if (ina) sa = eval(p.wnodes, p.wn, &sa);
-        if (inb) sb = eval(p.wnodes, p.wn, &sb);
-        const bool bad = (ina && (!isfinite(sa) || !(fa & J_FINITE))) || (inb && (!isfinite(sb) || !(fb & J_FINITE)));
-        if (__any_sync(0xffffffffu, bad)) over = true;
-        const double aa = fabs(sa), ab = fabs(sb);
-        const double hw = warp_max(fmax(ina ? aa : NEG_INF, inb ? ab : NEG_INF));
-        const double lw = warp_min(fmin(ina && aa != 0.0 ? aa : POS_INF, inb && ab != 0.0 ? ab : POS_INF));
-        const double sum = warp_sum((ina ? sa : 0.0) + (inb ? sb : 0.0));
-        if (ina) blk[r][ja] = sa;
-        if (inb) blk[r][jb] = sb;
-        if (lane == 0) {
-          S.high[r] = fmax(S.high[r], hw);
-          S.light[r] = fmin(S.light[r], lw);
-          S.z[r] += sum;
-        }
-        continue;
-      }
-      if (p.scale_kind == 1) { sa = sa * p.scale_c; sb = sb * p.scale_c; }
-      else if (p.scale_kind == 2) { sa = __ddiv_rn(sa, p.scale_c); sb = __ddiv_rn(sb, p.scale_c); }
-      const bool fina = ina && isfinite(sa), finb = inb && isfinite(sb);
-      const double hs = warp_max(fmax(fina ? sa : NEG_INF, finb ? sb : NEG_INF));
-      const double ls = warp_min(fmin(fina ? sa : POS_INF, finb ? sb : POS_INF));
-      const double lows = warp_min(fmin(fina && (fa & J_INFINITE) ? sa : POS_INF, finb && (fb & J_INFINITE) ? sb : POS_INF));
-      const bool any_nan = __any_sync(0xffffffffu, (ina && isnan(sa)) || (inb && isnan(sb)));
-      const double mx = warp_max(fmax(ina && !isnan(sa) ? sa : NEG_INF, inb && !isnan(sb) ? sb : NEG_INF));
-      const bool special_values = __any_sync(0xffffffffu, (ina && !(fa & J_FINITE)) || (inb && !(fb & J_FINITE)));
-      const double m_old = S.m[r];
-      // The largest score so far, or NaN once any score is NaN.
-      const double shift = shifted ? ((isnan(m_old) || any_nan) ? NAN : fmax(m_old, mx)) : 0.0;
-      if (lane == 0) {
-        S.high[r] = fmax(S.high[r], hs);
-        S.light[r] = fmin(S.light[r], ls);
-        S.low[r] = fmin(S.low[r], lows);
-      }
-      if (shift == NEG_INF) {
-        // Every score so far is -inf: weights 0 here.
-        if (ina) blk[r][ja] = 0.0;
-        if (inb) blk[r][jb] = 0.0;
-        continue;
-      }
-      const double rescale = exp(m_old - shift);
-      const double wa = ina ? exp(sa - shift) : 0.0, wb = inb ? exp(sb - shift) : 0.0;
-      const double sum = warp_sum(wa + wb);
-      const bool special_weights = __any_sync(0xffffffffu, (ina && !isfinite(wa)) || (inb && !isfinite(wb)));
-      if (ina) blk[r][ja] = wa;
-      if (inb) blk[r][jb] = wb;
-      if (lane == 0) {
-        S.sw_before[r] = S.sw[r];
-        if (shifted && rescale != 1.0) {
-          // overflows(z, a, ...) before the rescale: z's part here, a's by
-          // the threads that hold a.
-          if (!S.sw[r] && !isfinite(S.z[r])) over = true;
-          S.z[r] *= rescale;
-          S.pend[r] = 1;
-          S.resc[r] = rescale;
-        }
-        S.sw[r] |= special_weights;
-        S.spv[r] = special_values;
-        if (unnormalized && (special_weights || special_values)) over = true;
-        S.z[r] += sum;
-        S.m[r] = shift;
+        if (active)
+          #pragma unroll
+          for (int jj = 0; jj < 4; jj++)
+            if (in[jj]) blk[r][tx + 16 * jj] = w[i][jj];
       }
     }
     __syncthreads();
 
     // The weighted values: a += w · v over each row's allowed span.
     double* vs = stg;  // [j][y], rows of 65
+    const bool narrow = ycount <= kNarrow;
     for (int idx = t; idx < JT * YC; idx += kThreads) {
       const int j = idx >> 6, y = idx & 63;
+      if (narrow && y >= ycount) continue;
       vs[j * 65 + y] = (j < width && y < ycount) ? p.v[(j0 + j) * p.ny + y0 + y] : 0.0;
     }
     __syncthreads();
-    for (int i = 0; i < 4; i++) {
-      const int r = ty + 16 * i;
-      if (r >= rows) continue;
-      const int lo = S.lo[r], hi = S.hi[r];
-      // A thread whose outputs tx + 16 jj are all past the chunk's holds none.
-      if (lo >= hi || tx >= ycount) continue;
-      if (S.pend[r]) {
-        const double rescale = S.resc[r];
-        for (int jj = 0; jj < 4; jj++) {
-          const int y = tx + 16 * jj;
-          if (y < ycount && !S.sw_before[r] && !((sv >> (i * 4 + jj)) & 1) && !isfinite(acc[i][jj])) over = true;
-          acc[i][jj] *= rescale;
+    if (narrow) {
+      // A few value columns: a row's weighted sum over the tile is the
+      // half-warp's sum of its threads' four products, added to the output
+      // held by the thread with tx = y (its acc[i][0]).
+      #pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int r = ty + 16 * i;
+        const bool row = r < rows;
+        const int lo = row ? S.lo[r] : 0, hi = row ? S.hi[r] : 0;
+        const bool active = lo < hi;
+        if (active && tx < ycount && S.pend[r]) {
+          const double rescale = S.resc[r];
+          if (!S.sw_before[r] && !((sv >> (i * 4)) & 1) && !isfinite(acc[i][0])) over = true;
+          acc[i][0] *= rescale;
+        }
+        for (int y = 0; y < ycount; y++) {
+          double part = 0.0;
+          bool special = false;
+          #pragma unroll
+          for (int jj = 0; jj < 4; jj++) {
+            const int j = tx + 16 * jj;
+            const bool in = j >= lo && j < hi;
+            const double vj = vs[j * 65 + y];
+            part += in ? w[i][jj] * vj : 0.0;
+            special |= in && !isfinite(vj);
+          }
+          part = half_sum(part);
+          special = half_or(special);
+          if (active && tx == y) {
+            acc[i][0] += part;
+            if (special) sv |= 1u << (i * 4);
+          }
         }
       }
-      for (int j = lo; j < hi; j++) {
-        const double w = blk[r][j];
-        for (int jj = 0; jj < 4; jj++) acc[i][jj] = fma(w, vs[j * 65 + tx + 16 * jj], acc[i][jj]);
+    } else {
+      #pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int r = ty + 16 * i;
+        if (r >= rows) continue;
+        const int lo = S.lo[r], hi = S.hi[r];
+        // A thread whose outputs tx + 16 jj are all past the chunk's holds none.
+        if (lo >= hi || tx >= ycount) continue;
+        if (S.pend[r]) {
+          const double rescale = S.resc[r];
+          #pragma unroll
+          for (int jj = 0; jj < 4; jj++) {
+            const int y = tx + 16 * jj;
+            if (y < ycount && !S.sw_before[r] && !((sv >> (i * 4 + jj)) & 1) && !isfinite(acc[i][jj])) over = true;
+            acc[i][jj] *= rescale;
+          }
+        }
+        for (int j = lo; j < hi; j++) {
+          const double wt = blk[r][j];
+          #pragma unroll
+          for (int jj = 0; jj < 4; jj++) acc[i][jj] = fma(wt, vs[j * 65 + tx + 16 * jj], acc[i][jj]);
+        }
+        if (S.spv[r])
+          for (int j = lo; j < hi; j++)
+            if (!(p.jflag[j0 + j] & J_FINITE))
+              #pragma unroll
+              for (int jj = 0; jj < 4; jj++)
+                if (!isfinite(vs[j * 65 + tx + 16 * jj])) sv |= 1u << (i * 4 + jj);
       }
-      if (S.spv[r])
-        for (int j = lo; j < hi; j++)
-          if (!(p.jflag[j0 + j] & J_FINITE))
-            for (int jj = 0; jj < 4; jj++)
-              if (!isfinite(vs[j * 65 + tx + 16 * jj])) sv |= 1u << (i * 4 + jj);
     }
     __syncthreads();
   }
@@ -419,6 +596,27 @@ __global__ void __launch_bounds__(kThreads) fused_tiles(const TileArgs p) {
   }
   if (__syncthreads_or(over) && t == 0) atomicOr(p.overflowed, 1u);
   if (t == 0 && blockIdx.y == 0 && visited) atomicAdd(p.visited, visited);
+}
+
+// The deepest stack a postfix expression reaches.
+int stack_depth(const std::vector<ExprNode>& nodes) {
+  int depth = 0, deepest = 0;
+  for (const ExprNode& e : nodes) {
+    if (e.kind == 0 || e.kind == 1) depth++;
+    else if (e.kind != 2) depth--;
+    deepest = std::max(deepest, depth);
+  }
+  return deepest;
+}
+
+// fused_tiles with a stack for expressions `depth` deep (parsed expressions
+// are at most 60).
+void launch_tiles(const TileArgs& a, int depth, dim3 grid, cudaStream_t s) {
+  if (depth > 64) fail(EINFOLD_INVALID, "an expression deeper than 64");
+  auto kernel = depth <= 8 ? fused_tiles<8> : fused_tiles<64>;
+  EF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
+  kernel<<<grid, kThreads, kTileSmem, s>>>(a);
+  EF_LAUNCH_CHECK();
 }
 
 // Each J position's values: whether all are finite, whether any is
@@ -724,6 +922,22 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
       a.side[i] = read[i].first;
     }
   }
+  // Expressions of the shapes the kernel computes without the interpreter
+  // (binary ops 0 add, 1 sub, 2 mul, 3 div, 4 pow; unary 0 neg, 2 exp).
+  auto node = [](const ExprNode& e, int kind, int op) { return e.kind == kind && e.a == op; };
+  if (pr.row_expr && snodes.size() == 6 && snodes[0].kind == 0 && snodes[1].kind == 0 && node(snodes[2], 3, 1) &&
+      snodes[3].kind == 1 && snodes[3].value == 2.0 && node(snodes[4], 3, 4) && node(snodes[5], 2, 0)) {
+    a.score_shape = SCORE_NEG_SQUARED_DIFF;
+    a.shape_a = snodes[0].a;
+    a.shape_b = snodes[1].a;
+  }
+  if (p.weight_expr && wnodes.size() == 7 && wnodes[0].kind == 1 && wnodes[1].kind == 1 && wnodes[2].kind == 0 &&
+      node(wnodes[5], 3, 0) && node(wnodes[6], 3, 3)) {
+    if (node(wnodes[3], 2, 0) && node(wnodes[4], 2, 2)) a.weight_shape = WEIGHT_SIGMOID;
+    else if (wnodes[3].kind == 0 && node(wnodes[4], 3, 2)) a.weight_shape = WEIGHT_CAUCHY;
+    a.wc1 = wnodes[0].value;
+    a.wc2 = wnodes[1].value;
+  }
   a.v = matrices.back().get();
   a.jflag = jflag.get();
   a.largest = largest.get();
@@ -769,11 +983,9 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
     }
   }
   if (x_tiles && !split_done) {
-    EF_CUDA(cudaFuncSetAttribute(fused_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
     const dim3 grid((unsigned)x_tiles, (unsigned)std::max<uint64_t>((ny + YC - 1) / YC, 1));
-    fused_tiles<<<grid, kThreads, kTileSmem, s>>>(a);
+    launch_tiles(a, std::max(stack_depth(snodes), stack_depth(wnodes)), grid, s);
     ctx.kernels++;
-    EF_LAUNCH_CHECK();
   }
   unsigned long long n_visited = 0;
   unsigned of = 0;
@@ -910,11 +1122,9 @@ AttentionOutcome attention_forward(Context& ctx, AttentionProblem p, int precisi
   overflowed.zero();
   a.visited = visited.get();
   a.overflowed = overflowed.get();
-  EF_CUDA(cudaFuncSetAttribute(fused_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
   const dim3 grid((unsigned)((nx + XT - 1) / XT), (unsigned)((p.ny + YC - 1) / YC));
-  fused_tiles<<<grid, kThreads, kTileSmem, s>>>(a);
+  launch_tiles(a, 0, grid, s);
   ctx.kernels++;
-  EF_LAUNCH_CHECK();
   unsigned of = 0;
   EF_CUDA(cudaMemcpyAsync(&of, overflowed.get(), 4, cudaMemcpyDeviceToHost, s));
   EF_CUDA(cudaStreamSynchronize(s));

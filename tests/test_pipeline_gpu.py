@@ -228,3 +228,40 @@ def test_results_left_in_hbm_match_the_host_result():
     finally:
         for b in got.batches:
             b.release()
+
+
+def _bits(case: P.Case):
+    got = rows_of(_gpu(case).batches)
+    return got.column(got.num_columns - 1).to_numpy(zero_copy_only=False)
+
+
+@pytest.mark.parametrize("shape", ["gaussian", "sigmoid", "cauchy"])
+def test_named_shapes_give_the_interpreters_bits(shape):
+    # The kernel computes -power(a - b, 2) scores and the sigmoid and Cauchy
+    # weights without its expression interpreter; the same expressions
+    # written in another order of the same operations take the interpreter.
+    s = ir.Expression.column(0, 0)
+    one = ir.Expression.literal(1.0)
+    a, b = ir.Expression.column(0, -1), ir.Expression.column(1, -1)
+    diff = a.binary(ir.Binary.SUBTRACT, b)
+    kw = dict(q_value=lambda n: oracle.Rng.seeded(17, 2).units(n) * 2 - 1,
+              k_value=lambda n: oracle.Rng.seeded(18, 2).units(n) * 2 - 1,
+              v_value=lambda n: oracle.Rng.seeded(19, 2).units(n) * 2 - 1)
+    if shape == "gaussian":
+        fast = diff.binary(ir.Binary.POWER, ir.Expression.literal(2.0)).unary(ir.Unary.NEGATE)
+        slow = diff.unary(ir.Unary.NEGATE).binary(ir.Binary.MULTIPLY, diff)  # (-d)·d = -(d·d)
+        cases = [P.attention(200, d=3, lk=130, nb=2, scores=e, conditions=[(GE, -40)],
+                             weight=ir.Weight.exp(ir.Scale.over(0.05), ir.Shift.KEPT_MAXIMUM), **kw)
+                 for e in (fast, slow)]
+    else:
+        if shape == "sigmoid":
+            tail = s.unary(ir.Unary.NEGATE).unary(ir.Unary.EXP)
+        else:
+            tail = s.binary(ir.Binary.MULTIPLY, s)
+        fast = one.binary(ir.Binary.DIVIDE, one.binary(ir.Binary.ADD, tail))
+        slow = one.binary(ir.Binary.DIVIDE, tail.binary(ir.Binary.ADD, one))  # the sum's operands swapped
+        cases = [P.attention(150, d=5, nb=2, conditions=[(GE, 0), (LT, 90)], weight=ir.Weight.of_expression(e),
+                             **kw) for e in (fast, slow)]
+    got_fast, got_slow = (_bits(c) for c in cases)
+    assert np.array_equal(got_fast.view(np.uint64), got_slow.view(np.uint64))
+    _same(cases[0])
