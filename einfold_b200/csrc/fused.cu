@@ -402,8 +402,10 @@ __global__ void __launch_bounds__(kThreads) fused_tiles(const TileArgs p) {
           hs = half_max(hs);
           ls = half_min(ls);
           lows = half_min(lows);
-          mx = half_max(mx);
-          any_nan = half_or(any_nan);
+          if (shifted) {  // the same for the block: the running maximum's inputs
+            mx = half_max(mx);
+            any_nan = half_or(any_nan);
+          }
           special_values = half_or(special_values);
           // The largest score so far, or NaN once any score is NaN.
           const double shift = shifted ? ((isnan(m_old) || any_nan) ? NAN : fmax(m_old, mx)) : 0.0;
