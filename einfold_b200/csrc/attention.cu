@@ -43,6 +43,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 
@@ -600,18 +601,32 @@ enum Schedule : int {
   kSchedules = 3,
 };
 
-// A problem's work lists (the items that join some key) and the schedule
-// timed fastest for it (-1 until timed).
+// A problem's work lists (the items that join some key).
 struct WorkLists {
   std::vector<int2> by_tiles, by_batch;
-  int schedule = -1;
 };
 
 std::mutex g_work_lock;
 
+// The schedules timed fastest, by padded shape and conditions (not by the
+// ragged lengths, which a training loop may change at every step).
+std::vector<int64_t> tuning_key(const AttentionProblem& p, int kb, bool fast) {
+  std::vector<int64_t> key = {p.batches, p.lnx, p.lnj, p.ne, p.ny, kb, fast,
+                              (int64_t)(!p.xlen_host.empty() || !p.jlen_host.empty()), p.mask.n};
+  for (int i = 0; i < p.mask.n; i++) {
+    key.push_back(p.mask.cmp[i]);
+    key.push_back(p.mask.off[i]);
+  }
+  return key;
+}
+std::map<std::vector<int64_t>, int>& tuned_schedules() {
+  static std::map<std::vector<int64_t>, int> tuned;
+  return tuned;
+}
+
 // The work lists of a problem. Those of the last few shapes (lengths,
-// extents, conditions) are kept, with their timed schedule: a training
-// loop asks for the same ones at every step.
+// extents, conditions) are kept: a training loop over the same batches
+// asks for the same ones at every step.
 std::shared_ptr<WorkLists> work_lists(const AttentionProblem& p) {
   std::vector<int64_t> key = {p.batches, p.lnx, p.lnj, p.ne, p.ny, p.mask.n, (int64_t)p.xlen_host.size(),
                               (int64_t)p.jlen_host.size()};
@@ -850,9 +865,11 @@ AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int sl
   EF_CUDA(cudaEventCreate(&e0));
   EF_CUDA(cudaEventCreate(&e1));
   int schedule = forced_schedule();
+  const std::vector<int64_t> tkey = tuning_key(p, KB, fast);
   if (schedule < 0) {
     std::lock_guard<std::mutex> g(g_work_lock);
-    schedule = lists->schedule;
+    const auto it = tuned_schedules().find(tkey);
+    if (it != tuned_schedules().end()) schedule = it->second;
   }
   if (schedule < 0) {
     // The first call of this shape: each schedule twice (the same results
@@ -875,7 +892,9 @@ AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int sl
     }
     {
       std::lock_guard<std::mutex> g(g_work_lock);
-      lists->schedule = schedule;
+      auto& tuned = tuned_schedules();
+      if (tuned.size() >= 256) tuned.clear();
+      tuned[tkey] = schedule;
     }
     EF_CUDA(cudaMemsetAsync(tiles, 0, sizeof(unsigned long long), stream));
   }

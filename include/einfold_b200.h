@@ -211,7 +211,8 @@ typedef struct {
   /* Attention forwards in the split form: how the (query tile, batch) items
    * reached the SMs (0 a block per item, 1 persistent blocks claiming them by
    * key tiles, 2 persistent batch by batch; -1 other calls), picked by timing
-   * each on the first call of a shape unless EINFOLD_ATTENTION_SCHEDULE =
+   * each on the first call of a padded shape (extents and conditions, whatever
+   * the ragged lengths) unless EINFOLD_ATTENTION_SCHEDULE =
    * grid | tiles | batches forces one; and how the tile phase was launched
    * (0 directly, as with EINFOLD_GRAPHS=0; 1 a CUDA graph replayed, 2 one
    * updated with new arguments, 3 one captured and instantiated). */

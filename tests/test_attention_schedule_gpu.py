@@ -108,3 +108,22 @@ def test_an_unknown_schedule_is_refused(monkeypatch):
     monkeypatch.setenv("EINFOLD_ATTENTION_SCHEDULE", "sideways")
     with pytest.raises(ArrowInvalidArgumentError, match="EINFOLD_ATTENTION_SCHEDULE"):
         A.attention_forward(q, k, v, cond, scale, Precision.SPLIT)
+
+
+def test_new_lengths_of_a_timed_shape_are_not_timed_again(monkeypatch):
+    # The schedule is timed once per padded shape: a later call with other
+    # ragged lengths (a training loop's next batch) launches the tile kernel
+    # once, not the six timing runs again.
+    monkeypatch.delenv("EINFOLD_ATTENTION_SCHEDULE", raising=False)
+    lmax, d, dv = 512, 32, 40  # a shape no other test uses
+    runs = []
+    for lengths in ([300, 17, 512, 64, 200], [100, 512, 3, 250, 511]):
+        q, k, v = _ragged(lengths, lmax, d, dv, seed=len(runs) + 11)
+        ql = torch.tensor(lengths, dtype=torch.int64)
+        out, _ = A.attention_forward(q, k, v, A.window(30), 0.3, Precision.SPLIT, q_lengths=ql, k_lengths=ql)
+        runs.append((last_call.kernels_launched, last_call.schedule))
+        alone, _ = A.attention_forward(q[1:2, :lengths[1]], k[1:2, :lengths[1]], v[1:2, :lengths[1]], A.window(30),
+                                       0.3, Precision.SPLIT)
+        assert _equal(out[1, :lengths[1]], alone[0])
+    assert runs[0][1] == runs[1][1]
+    assert runs[0][0] - runs[1][0] == 6, runs
