@@ -711,15 +711,15 @@ __global__ void emit_rows(int64_t nx, int64_t ny, const uint8_t* __restrict__ fl
                           const int64_t* __restrict__ row_index, OutKeys keys, const int64_t* __restrict__ xtab,
                           const int64_t* __restrict__ ytab, const double* __restrict__ out,
                           double* __restrict__ val_out) {
-  for (int64_t x = blockIdx.y; x < nx; x += gridDim.y) {
+  // A thread per cell (x, y) of the row-major placed output.
+  const int64_t cells = nx * ny;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t x = ny == 1 ? c : c / ny, y = c - x * ny;
     if (!flags[x]) continue;
-    const int64_t base = row_index[x] * ny;
-    for (int64_t y = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; y < ny; y += (int64_t)gridDim.x * blockDim.x) {
-      const int64_t o = base + y;
-      for (int k = 0; k < keys.n; k++)
-        store_key(keys.out[k], keys.width[k], o, keys.key[k].in_x ? xtab[(int64_t)k * nx + x] : ytab[(int64_t)k * ny + y]);
-      val_out[o] = out[x * ny + y];
-    }
+    const int64_t o = row_index[x] * ny + y;
+    for (int k = 0; k < keys.n; k++)
+      store_key(keys.out[k], keys.width[k], o, keys.key[k].in_x ? xtab[(int64_t)k * nx + x] : ytab[(int64_t)k * ny + y]);
+    val_out[o] = out[c];
   }
 }
 
@@ -998,11 +998,19 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
   if (of) decline("a sum that overflowed or may have underflowed");
 
   // The pairs of tiles that share a batch (fused.rs:386-397).
+  // The batch of a tile's first row advances with the tiles (a division
+  // only for a tile whose rows reach past that batch).
   uint64_t tile_pairs = 0;
   const uint64_t lnx = (uint64_t)mask.lnx, lnj = (uint64_t)mask.lnj;
+  uint64_t w0 = 0, next_batch = lnx;  // x0's batch and the first row past it
   for (uint64_t t = 0; t < x_tiles; t++) {
     const uint64_t x0 = t * XT, x1 = std::min<uint64_t>((t + 1) * XT, nx);
-    const uint64_t start = x0 / lnx * lnj, end = (x1 - 1) / lnx * lnj + lnj;
+    while (x0 >= next_batch) {
+      w0++;
+      next_batch += lnx;
+    }
+    const uint64_t w1 = x1 - 1 < next_batch ? w0 : (x1 - 1) / lnx;
+    const uint64_t start = w0 * lnj, end = w1 * lnj + lnj;
     tile_pairs += (end + JT - 1) / JT - start / JT;
   }
 
@@ -1041,10 +1049,9 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
   }
   DeviceBuffer<double> vals((size_t)(n_out ? n_out : 1), s);
   if (n_out) {
-    const dim3 grid2((unsigned)std::max<uint64_t>(1, std::min<uint64_t>((ny + 255) / 256, 64)),
-                     (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(nx, 65535)));
-    emit_rows<<<grid2, 256, 0, s>>>((int64_t)nx, (int64_t)ny, flags.get(), row_index.get(), okeys, xtab.get(),
-                                    ytab.get(), out.get(), vals.get());
+    emit_rows<<<blocks_for((uint64_t)nx * ny, 256), 256, 0, s>>>((int64_t)nx, (int64_t)ny, flags.get(),
+                                                                  row_index.get(), okeys, xtab.get(), ytab.get(),
+                                                                  out.get(), vals.get());
     ctx.kernels++;
     EF_LAUNCH_CHECK();
   }
