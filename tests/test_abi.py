@@ -76,3 +76,42 @@ def test_pipeline_schema():
     v = pa.schema([("t", pa.int64()), ("c", pa.int32()), ("x", pa.float64())])
     s = K.pipeline_schema(p, [q, q, v])
     assert [f.type for f in s] == [pa.int64(), pa.int32(), pa.float64()]
+
+
+# The C structs of the header and their ctypes mirrors (einfold_b200/_lib.py).
+_MIRRORS = {
+    "einfold_key": "Key", "einfold_operand": "Operand", "einfold_output": "Output",
+    "einfold_condition": "Condition", "einfold_domain": "Domain", "einfold_expr_node": "ExprNode",
+    "einfold_expression": "Expression", "einfold_fold_desc": "FoldDesc", "einfold_pipeline_desc": "PipelineDesc",
+    "einfold_relation": "Relation", "einfold_options": "Options", "einfold_result": "Result",
+    "struct ArrowSchema": "ArrowSchema", "struct ArrowArray": "ArrowArray",
+}
+
+
+def test_ctypes_mirrors_have_the_headers_layout(tmp_path):
+    # Sizes and field offsets as a C compiler lays the header's structs out.
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "einfold_b200.h"', "int main(void) {"]
+    for cname, pyname in _MIRRORS.items():
+        cls = getattr(_lib, pyname)
+        lines.append(f'  printf("{pyname} %zu\\n", sizeof({cname}));')
+        for field in cls._fields_:
+            lines.append(f'  printf("{pyname}.{field[0]} %zu\\n", offsetof({cname}, {field[0]}));')
+    lines += ["  return 0;", "}"]
+    src, exe = tmp_path / "layout.c", tmp_path / "layout"
+    src.write_text("\n".join(lines))
+    subprocess.run([cc, "-std=c11", "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)], check=True)
+    c_layout = dict(line.split() for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                            text=True).stdout.splitlines())
+    import ctypes
+
+    for pyname in _MIRRORS.values():
+        cls = getattr(_lib, pyname)
+        assert int(c_layout[pyname]) == ctypes.sizeof(cls), f"sizeof {pyname}"
+        for field in cls._fields_:
+            assert int(c_layout[f"{pyname}.{field[0]}"]) == getattr(cls, field[0]).offset, f"{pyname}.{field[0]}"
