@@ -178,9 +178,10 @@ struct KeptScratch {
 
 // Instantiated CUDA graphs of a context's launch sequences. An entry is
 // replayed only when every argument its launches were captured with
-// (pointers included) is the same; otherwise the sequence is captured again
-// and, where an entry of the same shape (kernels, grids) exists, updated
-// into it.
+// (pointers included) is the same. Arguments seen for the first time are
+// launched directly, so that one-off arguments leave the cache alone; seen
+// again, the sequence is captured and updated into the entry of the same
+// shape (kernels, grids), or instantiated.
 struct GraphCache {
   struct Entry {
     std::vector<uint8_t> shape, key;
@@ -189,9 +190,12 @@ struct GraphCache {
   };
   std::vector<Entry> entries;
   uint64_t clock = 0;
+  cudaStream_t capture = nullptr;  // the stream graphs are captured on (the context's device)
+  std::vector<uint8_t> seen_shape, seen_key;  // the arguments last launched directly
   static constexpr size_t kMaxEntries = 8;
   // Launches `enqueue`'s work (queued on the stream it is given) on
-  // `stream` through a graph: 1 replayed, 2 updated, 3 instantiated.
+  // `stream`: 0 directly, else through a graph, 1 replayed, 2 updated,
+  // 3 instantiated.
   int run(const std::vector<uint8_t>& shape, const std::vector<uint8_t>& key, cudaStream_t stream,
           const std::function<void(cudaStream_t)>& enqueue);
   void clear();

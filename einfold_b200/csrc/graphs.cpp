@@ -12,28 +12,28 @@ int GraphCache::run(const std::vector<uint8_t>& shape, const std::vector<uint8_t
       EF_CUDA(cudaGraphLaunch(e.exec, stream));
       return 1;
     }
-  // Captured on a stream of its own: the caller's may be the legacy
-  // default stream, which cannot be captured.
-  cudaStream_t cs = nullptr;
-  EF_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-  cudaGraph_t graph = nullptr;
-  cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-  if (err != cudaSuccess) {
-    cudaStreamDestroy(cs);
-    EF_CUDA(err);
+  if (key != seen_key || shape != seen_shape) {
+    seen_shape = shape;
+    seen_key = key;
+    enqueue(stream);
+    return 0;
   }
+  // Captured on a stream of the cache's own: the caller's may be the
+  // legacy default stream, which cannot be captured. Capturing records the
+  // launches without running them.
+  if (!capture) EF_CUDA(cudaStreamCreateWithFlags(&capture, cudaStreamNonBlocking));
+  cudaStream_t cs = capture;
+  cudaGraph_t graph = nullptr;
+  EF_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
   try {
     enqueue(cs);
   } catch (...) {
     cudaStreamEndCapture(cs, &graph);
     if (graph) cudaGraphDestroy(graph);
-    cudaStreamDestroy(cs);
     cudaGetLastError();
     throw;
   }
-  err = cudaStreamEndCapture(cs, &graph);
-  cudaStreamDestroy(cs);
-  EF_CUDA(err);
+  EF_CUDA(cudaStreamEndCapture(cs, &graph));
   int how = 3;
   Entry* slot = nullptr;
   for (Entry& e : entries)
@@ -52,7 +52,7 @@ int GraphCache::run(const std::vector<uint8_t>& shape, const std::vector<uint8_t
     }
   if (!slot) {
     cudaGraphExec_t exec = nullptr;
-    err = cudaGraphInstantiate(&exec, graph, 0);
+    const cudaError_t err = cudaGraphInstantiate(&exec, graph, 0);
     if (err != cudaSuccess) cudaGraphDestroy(graph);
     EF_CUDA(err);
     for (size_t i = 0; i < entries.size();)
@@ -79,6 +79,8 @@ void GraphCache::clear() {
   for (Entry& e : entries)
     if (e.exec) cudaGraphExecDestroy(e.exec);
   entries.clear();
+  if (capture) cudaStreamDestroy(capture);
+  capture = nullptr;
 }
 
 }  // namespace ef

@@ -386,7 +386,8 @@ class CallInfo:
     product_ops: float = 0.0
     # Split attention forwards: the schedule (0 a block per item, 1
     # persistent by key tiles, 2 persistent by batch; -1 other calls) and the
-    # graph launch (0 direct, 1 replayed, 2 updated, 3 instantiated).
+    # graph launch (0 direct, arguments seen for the first time; 1 replayed;
+    # 2 updated, 3 instantiated, arguments seen a second time).
     schedule: int = -1
     graph: int = 0
     message: str = ""

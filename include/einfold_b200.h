@@ -214,8 +214,9 @@ typedef struct {
    * each on the first call of a padded shape (extents and conditions, whatever
    * the ragged lengths) unless EINFOLD_ATTENTION_SCHEDULE =
    * grid | tiles | batches forces one; and how the tile phase was launched
-   * (0 directly, as with EINFOLD_GRAPHS=0; 1 a CUDA graph replayed, 2 one
-   * updated with new arguments, 3 one captured and instantiated). */
+   * (0 directly: arguments seen for the first time, or EINFOLD_GRAPHS=0;
+   * 1 a CUDA graph replayed; seen a second time, 2 one updated with the new
+   * arguments or 3 one captured and instantiated). */
   int32_t schedule;
   int32_t graph;
   char message[480];

@@ -65,9 +65,9 @@ def test_every_schedule_gives_the_same_bits(monkeypatch, name):
 
 def test_the_tuned_schedule_and_graph_replays(monkeypatch):
     # The first call of a shape times the three schedules and keeps the
-    # fastest; with the same arguments the tile phase is then replayed from
-    # its graph, and new output buffers update the graph instead of
-    # capturing it again.
+    # fastest. Arguments seen for the first time launch directly; seen
+    # again, the tile phase is captured as a graph (new output buffers update
+    # the graph of that shape), and then replayed.
     monkeypatch.delenv("EINFOLD_ATTENTION_SCHEDULE", raising=False)
     monkeypatch.delenv("EINFOLD_GRAPHS", raising=False)
     q, k, v, _, cond, scale = _case("causal_24x1024_d64")
@@ -89,13 +89,13 @@ def test_the_tuned_schedule_and_graph_replays(monkeypatch):
 
     out, lse = buffers()
     schedule, graph = forward(out, lse)
-    assert schedule in SCHEDULES.values() and graph in (2, 3)
+    assert schedule in SCHEDULES.values() and graph == 0
     first = (out.clone(), lse.clone())
     graphs = [forward(out, lse)[1] for _ in range(3)]
-    assert graphs[-1] == 1, f"graph launches {graphs}: never replayed"
+    assert graphs[0] in (2, 3) and graphs[1:] == [1, 1], f"graph launches {graphs}"
     assert _equal(out, first[0]) and _equal(lse, first[1])
     out2, lse2 = buffers()
-    assert forward(out2, lse2) == (schedule, 2)
+    assert [forward(out2, lse2) for _ in range(3)] == [(schedule, 0), (schedule, 2), (schedule, 1)]
     assert _equal(out2, first[0]) and _equal(lse2, first[1])
     monkeypatch.setenv("EINFOLD_GRAPHS", "0")
     out3, lse3 = buffers()
