@@ -134,3 +134,43 @@ def test_fused_results_do_not_depend_on_threads_or_batches(threads):
 
     a, b = run(1, threads), run(2, 4)
     assert a.equals(b)
+
+
+def test_gaussian_smoother_against_numpy():
+    # Config 4's second part through the oracle's pipeline (the checker of the
+    # GPU's smoother): out(b, x) = sum_y w v / sum_y w with FP64 weights
+    # w = exp(-power(x - y, 2) / h), computed independently with numpy.
+    from einfold_b200 import cases as C
+
+    pipe = C.smoother_pipeline(0.01)
+    rng = np.random.default_rng(5)
+    g, n, ny = 3, 257, 70
+    x, y, v = rng.random(g * n), rng.random(g * ny), rng.standard_normal(g * ny)
+
+    def batch(cols, names):
+        return [pa.record_batch([pa.array(c) for c in cols], names=names)]
+
+    b, t = np.repeat(np.arange(g), n), np.tile(np.arange(n), g)
+    bk, tk = np.repeat(np.arange(g), ny), np.tile(np.arange(ny), g)
+    qa = batch([b, t, np.zeros_like(t), x], ["b", "t", "d", "x"])
+    ka = batch([bk, tk, np.zeros_like(tk), y], ["b", "t", "d", "x"])
+    va = batch([bk, tk, v], ["b", "t", "x"])
+    schema = oracle.pipeline_schema(pipe, [qa[0].schema, ka[0].schema, va[0].schema])
+    got = oracle.pipeline(pipe, qa, ka, va, schema, oracle.Options(threads=2))
+    table = rows_of(got.batches)
+    assert table.num_rows == g * n
+    assert np.array_equal(table.column(0).to_numpy(), b) and np.array_equal(table.column(1).to_numpy(), t)
+    X, Y, V = x.reshape(g, n), y.reshape(g, ny), v.reshape(g, ny)
+    w = np.exp(-(X[:, :, None] - Y[:, None, :]) ** 2 / 0.01)
+    want = (np.einsum("gnk,gk->gn", w, V) / w.sum(-1)).reshape(-1)
+    vals = table.column(2).to_numpy()
+    assert np.abs(vals - want).max() <= 1e-13 * np.abs(want).max()
+    # Tiles of 64 over the flattened positions (fused.rs:386-397): an X tile
+    # pairs with the J tiles of the groups its rows belong to; every pair
+    # here is allowed, so all are visited.
+    tiles = 0
+    for x0 in range(0, g * n, 64):
+        x1 = min(x0 + 64, g * n)
+        start, end = x0 // n * ny, (x1 - 1) // n * ny + ny
+        tiles += -(-end // 64) - start // 64
+    assert (got.tiles_visited, got.tiles) == (tiles, tiles)
