@@ -265,3 +265,25 @@ def test_named_shapes_give_the_interpreters_bits(shape):
     got_fast, got_slow = (_bits(c) for c in cases)
     assert np.array_equal(got_fast.view(np.uint64), got_slow.view(np.uint64))
     _same(cases[0])
+
+
+def test_gaussian_smoother_at_scale_against_torch_float64():
+    # Config 4's second part at 4 groups of 65,536 x and 256 y (67 M pairs,
+    # tables in HBM, result left there): every row against torch float64.
+    import torch
+
+    from einfold_b200 import cases as C
+
+    groups, nx, ny, h = 4, 1 << 16, 256, 0.01
+    q, k, v, xs, ys, vs = C.smoother_tables(groups, nx, ny, seed=3)
+    got = K.pipeline(C.smoother_pipeline(h), [q, k, v], options=K.Options(result_on_device=True))
+    try:
+        vals = got.batches[0].column(2).view(groups, nx)
+        X, Y, V = xs.view(groups, nx), ys.view(groups, ny), vs.view(groups, ny)
+        w = torch.exp(-(X[:, :, None] - Y[:, None, :]) ** 2 / h)
+        want = torch.einsum("gnk,gk->gn", w, V) / w.sum(-1)
+        assert got.batches[0].rows == groups * nx
+        assert ((vals - want).abs().max() / want.abs().max()).item() <= 1e-13
+    finally:
+        for b in got.batches:
+            b.release()
