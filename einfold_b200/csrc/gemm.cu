@@ -309,6 +309,23 @@ __global__ void __launch_bounds__(256) slice_short_rows(const double* __restrict
       ex += 2;
     }
     if (lane == 0) e_out[g] = ex;
+    if constexpr (S <= 6) {
+      // The digits from the bytes of the rounded values (digit_planes4:
+      // round to nearest, ties to even, as llrint below), x · 2^(8S - ex) in
+      // two exact factors.
+      if (lane * 4 < k_pad) {
+        const int shift = 8 * S - ex;
+        const double f1 = ptx::pow2(shift >> 1), f2 = ptx::pow2(shift - (shift >> 1));
+        double xs[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) xs[j] = (fabs(v[j]) <= 1.7976931348623157e308 ? v[j] : 0.0) * f1 * f2;
+        uint32_t planes[S];
+        digit_planes4<S>(xs, planes);
+#pragma unroll
+        for (int s = 0; s < S; s++) *(uint32_t*)(digits + (w * S + s) * slab + r * k_pad + lane * 4) = planes[s];
+      }
+      continue;
+    }
     if (lane * 4 < k_pad) {
       const int shift = 8 * S - ex;
       uint32_t word[S];
