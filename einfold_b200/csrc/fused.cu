@@ -624,11 +624,22 @@ void launch_tiles(const TileArgs& a, int depth, dim3 grid, cudaStream_t s) {
 // Each J position's values: whether all are finite, whether any is
 // infinite, the largest finite magnitude (0 if none) and the smallest
 // nonzero finite one (+inf if none) (fused.rs:371-385). A warp per J.
+// With jlen (ragged batches of lnj positions), a position past its batch's
+// length, which no row joins, is not read: it gets the statistics of zeros.
 __global__ void value_stats(int64_t nj, int64_t ny, const double* __restrict__ v, uint8_t* __restrict__ flag,
-                            double* __restrict__ largest, double* __restrict__ smallest, unsigned* nonfinite) {
+                            double* __restrict__ largest, double* __restrict__ smallest, unsigned* nonfinite,
+                            int64_t lnj = 1, const int64_t* __restrict__ jlen = nullptr) {
   const int lane = threadIdx.x & 31;
   for (int64_t j = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < nj;
        j += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    if (jlen && j % lnj >= jlen[j / lnj]) {
+      if (lane == 0) {
+        flag[j] = J_FINITE;
+        largest[j] = 0.0;
+        smallest[j] = INFINITY;
+      }
+      continue;
+    }
     bool fin = true, inf = false;
     double lg = 0.0, sm = INFINITY;
     for (int64_t y = lane; y < ny; y += 32) {
@@ -1094,7 +1105,7 @@ AttentionOutcome attention_forward(Context& ctx, AttentionProblem p, int precisi
   nonfinite.zero();
   if (nj) {
     value_stats<<<blocks_for(nj * 32, 256), 256, 0, s>>>(nj, p.ny, p.v, jflag.get(), largest.get(), smallest.get(),
-                                                         nonfinite.get());
+                                                         nonfinite.get(), p.lnj, p.mask.jlen);
     ctx.kernels++;
     EF_LAUNCH_CHECK();
   }
