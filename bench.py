@@ -477,8 +477,8 @@ def run_ours(args):
     ragged = _ragged() if not args.no_ragged else None
     sparse = _sparse(cpu=rank == 0 and world == 1 and not args.no_cpu) if not args.no_sparse else None
     smoother = _smoother(cpu=rank == 0 and world == 1 and not args.no_cpu) if not args.no_smoother else None
-    config1 = _config1(cpu=rank == 0 and world == 1 and not args.no_cpu) if not args.no_configs else None
-    config5 = _config5() if not args.no_configs else None
+    small_fold = _small_fold(cpu=rank == 0 and world == 1 and not args.no_cpu) if not args.no_small_fold else None
+    gradients = _gradients() if not args.no_gradients else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -513,8 +513,8 @@ def run_ours(args):
             "ragged": ragged,
             "sparse": sparse,
             "smoother": smoother,
-            "config1": config1,
-            "config5": config5,
+            "small_fold": small_fold,
+            "gradients": gradients,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "attention_forward_launch": fwd_launch,
@@ -728,7 +728,7 @@ def _sparse(cpu=False):
 
 
 def _smoother(cpu=False):
-    """Config 4's second part, the Gaussian smoother: per group (64), 2^20
+    """The Gaussian smoother: per group (64), 2^20
     query positions x and 256 key positions y uniform[0, 1) and values v
     normal(0, 1); out(b, x) = sum_y w v / sum_y w with FP64 weights
     w = exp(-power(x - y, 2) / h), h = 0.01, as a pipeline whose scores are
@@ -798,7 +798,7 @@ def _smoother(cpu=False):
     return out
 
 
-def _config1(cpu=False):
+def _small_fold(cpu=False):
     """The plain matmul fold at 512 x 512 . 512 x 256 (2·512·512·256 FLOP)
     through einfold_fold from host Arrow tables (rows shuffled, four batches
     an operand) to host results, timed end to end on the host clock around
@@ -815,7 +815,7 @@ def _config1(cpu=False):
     flop = 2.0 * 512 * 512 * 256
     out = {"flop": flop}
     for name, nulls in (("nulls_in_b", True), ("complete", False)):
-        (sa, a), (sb, b) = C.config1_tables(nulls, SEED)
+        (sa, a), (sb, b) = C.small_fold_tables(nulls, SEED)
         ra, rb = K.Relation(sa, a), K.Relation(sb, b)
         times, device_ms, got = [], [], None
         for _ in range(6):
@@ -841,7 +841,7 @@ def _config1(cpu=False):
     return out
 
 
-def _config5():
+def _gradients():
     """The gradient shapes at their own sizes: the causal attention backward
     at B=2 H=16 T=2048 d=64 (q, k, v normal(0, 1/8), d_out normal(0, 1);
     FLOP 2.5 x the forward's 4·B·H·T²·d·(T+1)/(2T)) and the matmul fold's
@@ -939,7 +939,8 @@ def main():
     p.add_argument("--no-ragged", action="store_true")
     p.add_argument("--no-sparse", action="store_true")
     p.add_argument("--no-smoother", action="store_true")
-    p.add_argument("--no-configs", action="store_true")
+    p.add_argument("--no-small-fold", action="store_true")
+    p.add_argument("--no-gradients", action="store_true")
     args = p.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -144,7 +144,7 @@ def sparse() -> None:
     print(f"sparse: {pairs} pair products, {rows} groups ({got.algorithm.name.lower()})")
 
 
-def config1_tables(nulls: bool, seed: int = 0):
+def small_fold_tables(nulls: bool, seed: int = 0):
     """The plain matmul fold's tables at 512 x 512 . 512 x 256: a(i, j, v)
     with every (i, j) of 512 x 512 and b(j, k, v) with every (j, k) of
     512 x 256, v uniform[-1, 1] (SplitMix64 salts 31, 32), with `nulls` 1%

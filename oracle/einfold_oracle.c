@@ -2,8 +2,8 @@
  * ORACLE — test infrastructure, not product code.
  *
  * A plain-C restatement of the inner loops of einfold's kernel layer
- * (crates/einfold-kernels), used only by tests/, by __graft_entry__.smoke() as
- * the checker, and by bench.py's CPU-baseline leg. Nothing in the product path
+ * (crates/einfold-kernels), used only by tests/, by __graft_entry__.smoke() to
+ * check its result, and by bench.py's CPU-baseline leg. Nothing in the product path
  * (einfold_b200/, include/) links or calls this file.
  *
  * Each function names the reference lines it follows. Floating-point sums are

@@ -5,7 +5,7 @@ control logic of ``dense::fold``, ``discriminate::fold``, ``fused::pipeline``,
 ``chain::fold`` and ``schema`` in Python over pyarrow and numpy, with the inner
 loops in ``einfold_oracle.c`` (built to ``oracle/libeinfold_oracle.so``).
 
-Only ``tests/``, ``__graft_entry__.smoke()`` (as the checker) and ``bench.py``'s
+Only ``tests/``, ``__graft_entry__.smoke()`` (to check its result) and ``bench.py``'s
 CPU-baseline leg may import this module. The product path never does.
 
 Parity pins: the SplitMix64 known answers (``rng.rs:66-78``), the tile-visit

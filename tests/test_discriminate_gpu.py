@@ -25,7 +25,7 @@ def _both(f, a, b, domain=None, options=None, float_keys=0):
 
 
 def test_nulls_in_b_send_the_matmul_fold_to_discrimination():
-    # Config 1's shape, scaled: 1% of b's factors NULL.
+    # The 512 x 512 . 512 x 256 fold's shape, scaled: 1% of b's factors NULL.
     rng = oracle.Rng.seeded(0, 0x5eedf01d)
     ni, nj, nk = 64, 64, 32
     sa, a = complete(["i", "j"], [ni, nj], rng.units(ni * nj) * 2 - 1, rng)

@@ -137,8 +137,8 @@ def test_fused_results_do_not_depend_on_threads_or_batches(threads):
 
 
 def test_gaussian_smoother_against_numpy():
-    # Config 4's second part through the oracle's pipeline (the checker of the
-    # GPU's smoother): out(b, x) = sum_y w v / sum_y w with FP64 weights
+    # The Gaussian smoother through the oracle's pipeline (against which the
+    # GPU's smoother is tested): out(b, x) = sum_y w v / sum_y w with FP64 weights
     # w = exp(-power(x - y, 2) / h), computed independently with numpy.
     from einfold_b200 import cases as C
 

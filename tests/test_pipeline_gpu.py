@@ -268,7 +268,7 @@ def test_named_shapes_give_the_interpreters_bits(shape):
 
 
 def test_gaussian_smoother_at_scale_against_torch_float64():
-    # Config 4's second part at 4 groups of 65,536 x and 256 y (67 M pairs,
+    # The Gaussian smoother at 4 groups of 65,536 x and 256 y (67 M pairs,
     # tables in HBM, result left there): every row against torch float64.
     import torch
 

@@ -68,7 +68,7 @@ def test_each_group_as_if_alone(name, precision):
 @pytest.mark.parametrize("precision", [Precision.SPLIT, Precision.FP64])
 @pytest.mark.parametrize("shape", [
     ([200, 64, 333, 1], 333, 64, 64, A.causal(), 0.125),
-    # d = 128 (config 4's width): the backward takes the FP64 tiles in either form.
+    # d = 128 (the ragged bench batches' width): the backward takes the FP64 tiles in either form.
     ([150, 40, 260], 260, 128, 64, A.window(50), 0.0884),
 ])
 def test_ragged_gradients(precision, shape):
