@@ -95,3 +95,31 @@ def test_lengths_outside_the_padding_are_refused():
     q, k, v = _ragged([5, 6], 6, 8, 8, seed=1)
     with pytest.raises(Exception, match="length"):
         A.attention_forward(q, k, v, q_lengths=torch.tensor([5, 7]), k_lengths=torch.tensor([5, 6]))
+
+
+@pytest.mark.parametrize("precision", [Precision.SPLIT, Precision.FP64])
+@pytest.mark.parametrize("lengths", [[0, 300, 0, 57], [0, 0]])
+def test_empty_groups(precision, lengths):
+    # A group of length 0 joins nothing: its rows are NaN and its gradients
+    # zero, and the other groups come out as if alone; a batch of only
+    # empty groups runs no tile at all.
+    lmax, d, dv, cond, scale = 300, 32, 16, A.causal(), 0.5
+    q, k, v = _ragged(lengths, lmax, d, dv, seed=13)
+    ql = torch.tensor(lengths, dtype=torch.int64)
+    qa, ka, va = (t.clone().requires_grad_(True) for t in (q, k, v))
+    out = A.attention(qa, ka, va, cond, scale, precision, q_lengths=ql, k_lengths=ql)
+    g = torch.Generator(device="cuda").manual_seed(6)
+    up = torch.randn(out.shape, dtype=torch.float64, device="cuda", generator=g)
+    (out.nan_to_num() * up).sum().backward()
+    for w, t in enumerate(lengths):
+        assert torch.isnan(out[w, t:]).all(), f"group {w}: rows past the length"
+        for name, grad in (("q", qa.grad), ("k", ka.grad), ("v", va.grad)):
+            assert (grad[w, t:] == 0).all(), f"d{name} past the length of group {w}"
+        if t == 0:
+            continue
+        qs, ks, vs = (x[w:w + 1, :t].clone().requires_grad_(True) for x in (q, k, v))
+        alone = A.attention(qs, ks, vs, cond, scale, precision)
+        assert _same(out[w, :t], alone[0], precision), f"group {w}"
+        (alone.nan_to_num() * up[w:w + 1, :t]).sum().backward()
+        for name, a, b in (("q", qa.grad, qs.grad), ("k", ka.grad, ks.grad), ("v", va.grad, vs.grad)):
+            assert _same(a[w, :t], b[0], precision, tol=1e-12), f"d{name} of group {w}"
