@@ -757,9 +757,14 @@ AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int sl
   EF_CUDA(cudaMemsetAsync(status, 0, 32, stream));
   const int init[4] = {INT_MIN, INT_MIN, INT_MIN, INT_MIN};
   EF_CUDA(cudaMemcpyAsync(status + 2, init, 16, cudaMemcpyHostToDevice, stream));
-  // Ragged batches: the padding rows are not read (their digits are zeros).
-  slice_rows_into(S, p.q, W, p.lnx, p.ne, p.ne, lnx_pad, d_pad, eq, qd, status, stream, p.mask.xlen);
-  slice_rows_into(S, p.k, W, p.lnj, p.ne, p.ne, lnj_pad, d_pad, ek, kd, status, stream, p.mask.jlen);
+  // Ragged batches: the padding rows are neither read nor given digits. A
+  // padding query joins no key and a padding key no query, so their digits
+  // only meet masked scores (weights exactly 0) in exact integer sums, and
+  // their rows' exponents (0) still bound the scores.
+  slice_rows_into(S, p.q, W, p.lnx, p.ne, p.ne, lnx_pad, d_pad, eq, qd, status, stream, p.mask.xlen,
+                  p.mask.xlen != nullptr);
+  slice_rows_into(S, p.k, W, p.lnj, p.ne, p.ne, lnj_pad, d_pad, ek, kd, status, stream, p.mask.jlen,
+                  p.mask.jlen != nullptr);
   slice_cols_into(S, p.v, W, p.lnj, p.ny, ny_pad, lnj_pad, colmax, ev, vd, status, stream, p.mask.jlen);
   exponent_range(eq, W * lnx_pad, status + 2, stream);
   exponent_range(ek, W * lnj_pad, status + 4, stream);

@@ -282,7 +282,8 @@ template <int S>
 __global__ void __launch_bounds__(256) slice_short_rows(const double* __restrict__ x, int64_t batches, int64_t rows,
                                                         int64_t k, int64_t ld, int64_t rows_pad, int64_t k_pad,
                                                         int32_t* __restrict__ e_out, int8_t* __restrict__ digits,
-                                                        int* status, const int64_t* __restrict__ lens) {
+                                                        int* status, const int64_t* __restrict__ lens,
+                                                        bool skip_padding) {
   const int lane = threadIdx.x & 31;
   const int64_t slab = rows_pad * k_pad;
   for (int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < batches * rows_pad;
@@ -312,8 +313,9 @@ __global__ void __launch_bounds__(256) slice_short_rows(const double* __restrict
     if constexpr (S <= 6) {
       // The digits from the bytes of the rounded values (digit_planes4:
       // round to nearest, ties to even, as llrint below), x · 2^(8S - ex) in
-      // two exact factors.
-      if (lane * 4 < k_pad) {
+      // two exact factors. Rows past their length keep their old digits
+      // when the caller never reads them (skip_padding).
+      if (lane * 4 < k_pad && (live || !skip_padding)) {
         const int shift = 8 * S - ex;
         const double f1 = ptx::pow2(shift >> 1), f2 = ptx::pow2(shift - (shift >> 1));
         double xs[4];
@@ -326,7 +328,7 @@ __global__ void __launch_bounds__(256) slice_short_rows(const double* __restrict
       }
       continue;
     }
-    if (lane * 4 < k_pad) {
+    if (lane * 4 < k_pad && (live || !skip_padding)) {
       const int shift = 8 * S - ex;
       uint32_t word[S];
 #pragma unroll
@@ -356,7 +358,8 @@ template <int S>
 __global__ void __launch_bounds__(256) slice_half_warp_rows(const double* __restrict__ x, int64_t batches,
                                                             int64_t rows, int64_t k, int64_t ld, int64_t rows_pad,
                                                             int32_t* __restrict__ e_out, int8_t* __restrict__ digits,
-                                                            int* status, const int64_t* __restrict__ lens) {
+                                                            int* status, const int64_t* __restrict__ lens,
+                                                            bool skip_padding) {
   constexpr int64_t kPad = 64;
   const int lane = threadIdx.x & 31, l16 = lane & 15, half = lane >> 4;
   const int64_t slab = rows_pad * kPad, total = batches * rows_pad;
@@ -402,8 +405,9 @@ __global__ void __launch_bounds__(256) slice_half_warp_rows(const double* __rest
       for (int j = 0; j < 4; j++) xs[j] = v[j] * f1 * f2;
       uint32_t planes[S];
       digit_planes4<S>(xs, planes);
+      if (live || !skip_padding)
 #pragma unroll
-      for (int s2 = 0; s2 < S; s2++) *(uint32_t*)(digits + (w * S + s2) * slab + r * kPad + c0) = planes[s2];
+        for (int s2 = 0; s2 < S; s2++) *(uint32_t*)(digits + (w * S + s2) * slab + r * kPad + c0) = planes[s2];
     }
   }
 }
@@ -412,17 +416,17 @@ __global__ void __launch_bounds__(256) slice_half_warp_rows(const double* __rest
 template <int S>
 void launch_slice_rows(const double* x, int64_t batches, int64_t rows, int64_t k, int64_t ld, int64_t rows_pad,
                        int64_t k_pad, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream,
-                       const int64_t* lens = nullptr) {
+                       const int64_t* lens = nullptr, bool skip_padding = false) {
   if constexpr (S <= 6) {
     if (k_pad == 64) {
       slice_half_warp_rows<S><<<blocks_for((uint64_t)(batches * rows_pad) * 16, 256), 256, 0, stream>>>(
-          x, batches, rows, k, ld, rows_pad, e_out, digits, status, lens);
+          x, batches, rows, k, ld, rows_pad, e_out, digits, status, lens, skip_padding);
       return;
     }
   }
   if (k_pad <= 128)
     slice_short_rows<S><<<blocks_for((uint64_t)(batches * rows_pad) * 32, 256), 256, 0, stream>>>(
-        x, batches, rows, k, ld, rows_pad, k_pad, e_out, digits, status, lens);
+        x, batches, rows, k, ld, rows_pad, k_pad, e_out, digits, status, lens, skip_padding);
   else
     slice_rows<S><<<blocks_for((uint64_t)(batches * rows_pad), 1, 148 * 8), 256, 0, stream>>>(
         x, batches, rows, k, ld, rows_pad, k_pad, e_out, digits, status, lens);
@@ -824,11 +828,11 @@ void exponent_range(const int32_t* e, int64_t n, int* out, cudaStream_t stream) 
 
 void slice_rows_into(int S, const double* x, int64_t batches, int64_t rows, int64_t k, int64_t ld, int64_t rows_pad,
                      int64_t k_pad, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream,
-                     const int64_t* lens) {
+                     const int64_t* lens, bool skip_padding) {
   if (batches <= 0 || rows_pad <= 0) return;
   dispatch_slices(S, [&](auto SS) {
     launch_slice_rows<decltype(SS)::value>(x, batches, rows, k, ld, rows_pad, k_pad, e_out, digits, status, stream,
-                                           lens);
+                                           lens, skip_padding);
   });
   EF_LAUNCH_CHECK();
 }

@@ -39,10 +39,12 @@ void fp64_gemm(Context& ctx, const double* a, const uint32_t* held, const double
 // (zeros beyond), each row under a power-of-two scale 2^e with e in
 // e_out[w·rows_pad + r]; status bit 1 if a value isn't finite. With
 // `lens` (device, one per batch), rows at or past lens[w] are not read and
-// slice to zeros.
+// slice to zeros; with skip_padding as well, their digits (rows at or past
+// `rows` too) are not written at all, for a caller that reads none of them
+// (their exponents are still 0).
 void slice_rows_into(int S, const double* x, int64_t batches, int64_t rows, int64_t k, int64_t ld, int64_t rows_pad,
                      int64_t k_pad, int32_t* e_out, int8_t* digits, int* status, cudaStream_t stream,
-                     const int64_t* lens = nullptr);
+                     const int64_t* lens = nullptr, bool skip_padding = false);
 // Columns of x [batches][k][n] become K-major digit planes
 // digits[(w·S + s)][col][kk] for col < n_pad and kk < k_pad (both multiples
 // of 64), each column under its own power of two, e_out[w·n_pad + col];
