@@ -115,3 +115,32 @@ def test_ctypes_mirrors_have_the_headers_layout(tmp_path):
         assert int(c_layout[pyname]) == ctypes.sizeof(cls), f"sizeof {pyname}"
         for field in cls._fields_:
             assert int(c_layout[f"{pyname}.{field[0]}"]) == getattr(cls, field[0]).offset, f"{pyname}.{field[0]}"
+
+
+def test_smoother_pipeline_schema():
+    # The Gaussian smoother's pipeline is valid and its output is (b, t, value).
+    from einfold_b200 import cases as C
+
+    q = pa.schema([("b", pa.int64()), ("t", pa.int64()), ("d", pa.int64()), ("x", pa.float64())])
+    v = pa.schema([("b", pa.int64()), ("t", pa.int64()), ("x", pa.float64())])
+    s = K.pipeline_schema(C.smoother_pipeline(0.01), [q, q, v])
+    assert [f.type for f in s] == [pa.int64(), pa.int64(), pa.float64()]
+
+
+def test_small_fold_tables_have_the_stated_shape():
+    # 512 x 512 and 512 x 256 rows, every key tuple once, in four batches,
+    # with about 1% of b's values NULL when asked (and none otherwise).
+    import numpy as np
+
+    from einfold_b200 import cases as C
+
+    for nulls in (True, False):
+        (sa, a), (sb, b) = C.small_fold_tables(nulls)
+        assert len(a) == 4 and len(b) == 4
+        ta, tb = pa.Table.from_batches(a), pa.Table.from_batches(b)
+        assert ta.num_rows == 512 * 512 and tb.num_rows == 512 * 256
+        keys = ta.column(0).to_numpy() * 512 + ta.column(1).to_numpy()
+        assert np.array_equal(np.sort(keys), np.arange(512 * 512))
+        n_null = tb.column(2).null_count
+        assert (0.008 * tb.num_rows < n_null < 0.012 * tb.num_rows) if nulls else n_null == 0
+        assert ta.column(2).null_count == 0
