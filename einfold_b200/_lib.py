@@ -140,6 +140,9 @@ SIGNATURES = {
     "einfold_result_release": (None, [ctypes.POINTER(Result)]),
     "einfold_rank_words": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                                             ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p]),
+    "einfold_rank_columns": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(Relation), ctypes.c_int32,
+                                              ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.POINTER(ctypes.c_int64)]),
     "einfold_split_gemm": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                             ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                             ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),

@@ -269,6 +269,22 @@ int32_t einfold_rank_words(einfold_context* ctx, const uint64_t* words, int64_t 
   });
 }
 
+int32_t einfold_rank_columns(einfold_context* ctx, const einfold_relation* relation, int32_t n_columns,
+                             const int32_t* columns, int32_t float_keys, uint32_t* rank, uint32_t* first,
+                             int64_t* n_ranks) {
+  einfold_result r;
+  const int32_t st = guarded(ctx, &r, [&](ef::Context& cx) -> int32_t {
+    if (!relation || n_columns < 0 || (n_columns && !columns)) ef::fail(EINFOLD_INVALID, "no relation or columns");
+    ef::Relation rel = ef::import_relation(relation);
+    std::vector<int> cols(columns, columns + n_columns);
+    const int64_t k = ef::rank_columns(cx, rel, cols, float_keys, rank, first, relation->device >= 0);
+    if (n_ranks) *n_ranks = k;
+    return EINFOLD_OK;
+  });
+  if (st != EINFOLD_OK) g_last_error = r.message;
+  return st;
+}
+
 int32_t einfold_fp64_gemm(einfold_context* ctx, const double* a, const double* b, double* c, int64_t batches,
                           int64_t m, int64_t n, int64_t k, int32_t b_transposed, void* stream) {
   einfold_result r;

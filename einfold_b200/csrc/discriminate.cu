@@ -5,12 +5,13 @@
 //    Arrow's default order and are equal exactly when the host calls the keys
 //    equal: per column a byte for NULL (0) or valid (1), then integers
 //    sign-flipped big-endian, floats by their total-order bits (-0.0 made 0.0
-//    first under SignedZerosEqual, keys.rs:61-76), strings as their bytes with
-//    0x00 escaped as 0x00 0xFF and two 0x00 after, zero-padded to the longest.
-//    A single non-NULL integer column is its sign-flipped value alone
-//    (discriminate.rs:244-272).
+//    first under SignedZerosEqual, keys.rs:61-76), strings as their bytes
+//    zero-padded to the longest, then their length. A single non-NULL
+//    integer column is its sign-flipped value alone (discriminate.rs:244-272).
 // 2. Ranks (rank.cu): the join's keys over a‖b, the outputs' over each
-//    operand with the domain's.
+//    operand with the domain's. Keys longer than four words are ranked over
+//    the words that vary between keys, in rounds that refine the previous
+//    round's ranks (any length, as by_bytes at :165-209).
 // 3. a's joining rows sorted by (x, z, NULL-first factor bits), b's by (z, y,
 //    factor bits): one stable radix sort each (the reference's two counting
 //    sorts and break_ties, :497-506).
@@ -31,29 +32,36 @@
 namespace ef {
 namespace {
 
-constexpr int kMaxWords = 4;
+constexpr int kMaxWords = 4;  // words one ranking pass orders a key by
 
+// One key column's block of bytes in the encoded key: a byte for NULL (0) or
+// valid (1), then the value. Fixed-width values take 8 bytes. A string or
+// binary value takes `max_len` bytes, its own bytes zero-padded, then its
+// length big-endian in `len_bytes` bytes: two values that differ first at
+// byte p order by that byte, a value that is a prefix of the other with only
+// zeros after it orders by its length, so the blocks order as Arrow's row
+// format orders the values (bytes, a prefix first), and are equal exactly
+// when the values are. Every byte's position is fixed, so any word of the key
+// is computed without the bytes before it.
 struct KeyCol {
   int kind;            // Kind
   int width;           // bytes of a fixed-width value
   const uint8_t* data; // fixed-width values, or var-length bytes
   const int64_t* off;  // var-length offsets
   const uint8_t* valid;
-  int pad_len;         // var-length: encoded bytes incl. the two terminators, padded
-  int start;           // first byte of this column in the key
+  int64_t start;       // first byte of this column's block in the key
+  int64_t block;       // bytes of the block
+  int64_t max_len;     // var-length: bytes of the value part
+  int len_bytes;       // var-length: bytes of the length part
   int canon_zero;      // SignedZerosEqual on a float column
 };
 
-struct KeyCols {
+// The word positions (absolute, within the key) a pass encodes, and where
+// the previous pass's ranks go (word 0) when refining.
+struct WordList {
   int n = 0;
-  KeyCol c[8];
-  int words = 1;
-  int fast_int = 0;    // one non-NULL integer column: sign-flipped value
+  int64_t pos[kMaxWords] = {};
 };
-
-__device__ __forceinline__ void put_byte(uint64_t* w, int pos, uint8_t b) {
-  w[pos >> 3] |= (uint64_t)b << (8 * (7 - (pos & 7)));
-}
 
 __device__ uint64_t ordered_bits(const KeyCol& c, int64_t r) {
   switch ((Kind)c.kind) {
@@ -85,44 +93,86 @@ __device__ uint64_t ordered_bits(const KeyCol& c, int64_t r) {
   }
 }
 
-__global__ void encode_keys(KeyCols k, int64_t rows, int64_t row0, uint64_t* __restrict__ out, int64_t ld) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
-    uint64_t w[kMaxWords] = {0, 0, 0, 0};
-    if (k.fast_int) {
-      w[0] = ordered_bits(k.c[0], r);
+// Word `wpos` of row r's key (bytes 8·wpos … 8·wpos + 7, most significant first).
+__device__ uint64_t key_word(const KeyCol* __restrict__ cols, int n_cols, int64_t r, int64_t wpos) {
+  const int64_t b0 = wpos * 8, b1 = b0 + 8;
+  uint64_t w = 0;
+  for (int i = 0; i < n_cols; i++) {
+    const KeyCol& c = cols[i];
+    const int64_t s = c.start, e = c.start + c.block;
+    if (e <= b0 || s >= b1) continue;
+    const bool v = !c.valid || c.valid[r];
+    const int64_t lo = s > b0 ? s : b0, hi = e < b1 ? e : b1;
+    if (!v) {
+      // NULL: the validity byte and everything after it are zero.
+      continue;
+    }
+    if (c.off) {
+      const int64_t o0 = c.off[r], len = c.off[r + 1] - o0;
+      for (int64_t p = lo; p < hi; p++) {
+        const int64_t q = p - s;
+        uint64_t byte;
+        if (q == 0) byte = 1;
+        else if (q <= c.max_len) byte = q - 1 < len ? c.data[o0 + q - 1] : 0;
+        else byte = ((uint64_t)len >> (8 * (c.len_bytes - 1 - (q - 1 - c.max_len)))) & 0xff;
+        w |= byte << (8 * (7 - (p - b0)));
+      }
     } else {
-      for (int i = 0; i < k.n; i++) {
-        const KeyCol& c = k.c[i];
-        const bool v = !c.valid || c.valid[r];
-        put_byte(w, c.start, v ? 1 : 0);
-        if (!v) continue;
-        if (c.off) {
-          const int64_t b0 = c.off[r], b1 = c.off[r + 1];
-          int pos = c.start + 1;
-          for (int64_t b = b0; b < b1; b++) {
-            const uint8_t ch = c.data[b];
-            put_byte(w, pos++, ch);
-            if (ch == 0) put_byte(w, pos++, 0xFF);
-          }
-          // two zero terminators and zero padding are already zero
-        } else {
-          const uint64_t bits = ordered_bits(c, r);
-          for (int b = 0; b < 8; b++) put_byte(w, c.start + 1 + b, (uint8_t)(bits >> (8 * (7 - b))));
-        }
+      const uint64_t bits = ordered_bits(c, r);
+      for (int64_t p = lo; p < hi; p++) {
+        const int64_t q = p - s;
+        const uint64_t byte = q == 0 ? 1 : (bits >> (8 * (8 - q))) & 0xff;
+        w |= byte << (8 * (7 - (p - b0)));
       }
     }
-    for (int i = 0; i < k.words; i++) out[(int64_t)i * ld + row0 + r] = w[i];
+  }
+  return w;
+}
+
+// The words of `list` for rows [row0, row0 + rows), after the previous
+// pass's rank (word 0) when `prefix` is given; word-major, stride ld.
+__global__ void encode_words(const KeyCol* __restrict__ cols, int n_cols, int fast_int, WordList list,
+                             const uint32_t* __restrict__ prefix, int64_t rows, int64_t row0,
+                             uint64_t* __restrict__ out, int64_t ld) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    int o = 0;
+    if (prefix) out[(int64_t)(o++) * ld + row0 + r] = prefix[row0 + r];
+    if (fast_int) {
+      out[(int64_t)o * ld + row0 + r] = ordered_bits(cols[0], r);
+      continue;
+    }
+    for (int i = 0; i < list.n; i++) out[(int64_t)(o + i) * ld + row0 + r] = key_word(cols, n_cols, r, list.pos[i]);
   }
 }
 
-// The longest escaped string of a column (bytes + one per 0x00).
-__global__ void escaped_max(const uint8_t* __restrict__ data, const int64_t* __restrict__ off,
-                            const uint8_t* __restrict__ valid, int64_t rows, unsigned long long* mx) {
+// For words [w0, w0 + gridDim.y) of every row: the OR and the AND over rows,
+// so that words no two keys differ in are known (and skipped).
+__global__ void word_spread(const KeyCol* __restrict__ cols, int n_cols, int64_t rows, int64_t w0,
+                            unsigned long long* __restrict__ any, unsigned long long* __restrict__ all) {
+  const int64_t wpos = w0 + blockIdx.y;
+  unsigned long long o = 0, a = ~0ull;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t w = key_word(cols, n_cols, r, wpos);
+    o |= w;
+    a &= w;
+  }
+  for (int s = 16; s; s >>= 1) {
+    o |= __shfl_xor_sync(0xffffffffu, o, s);
+    a &= __shfl_xor_sync(0xffffffffu, a, s);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicOr(&any[blockIdx.y], o);
+    atomicAnd(&all[blockIdx.y], a);
+  }
+}
+
+// The longest value of a var-length column.
+__global__ void longest(const int64_t* __restrict__ off, const uint8_t* __restrict__ valid, int64_t rows,
+                        unsigned long long* mx) {
   unsigned long long local = 0;
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
     if (valid && !valid[r]) continue;
-    unsigned long long len = 0;
-    for (int64_t b = off[r]; b < off[r + 1]; b++) len += data[b] == 0 ? 2 : 1;
+    const unsigned long long len = (unsigned long long)(off[r + 1] - off[r]);
     local = len > local ? len : local;
   }
   for (int o = 16; o; o >>= 1) {
@@ -386,81 +436,124 @@ StagedKeySet stage_set(Context& ctx, const Relation& r, const std::vector<int>& 
   StagedKeySet s;
   for (int c : cols) {
     const Field& f = r.fields[c];
-    if (f.dictionary) fail(EINFOLD_COMPUTE, "dictionary-encoded keys are not supported by the device fold");
+    if (f.dictionary) decline("dictionary-encoded keys are ranked by the host plan");
     s.cols.push_back(stage_column(ctx, r, c, true));
     s.kinds.push_back(f.kind);
   }
   return s;
 }
 
-// Encodes the rows of `sets` (same columns' types each, concatenated in order)
-// into words; returns the word count and the layout stride.
-int encode_sets(Context& ctx, const std::vector<const StagedKeySet*>& sets, int float_keys, int64_t total,
-                DeviceBuffer<uint64_t>& words, int64_t* ld_out) {
+// The encoded key's layout over the rows of `sets` (the same columns' types
+// each, concatenated in order), and each set's columns as the kernels read
+// them.
+struct KeyLayout {
+  int n_cols = 0;
+  bool fast = false;    // one integer column, no NULLs: its sign-flipped value alone
+  int64_t bytes = 0;    // of the whole key
+  int64_t words = 0;
+  std::vector<DeviceBuffer<KeyCol>> cols;  // per set
+};
+
+KeyLayout layout_of(Context& ctx, const std::vector<const StagedKeySet*>& sets, int float_keys) {
   cudaStream_t s = ctx.stream;
-  const int n_cols = sets.empty() ? 0 : (int)sets[0]->cols.size();
-  if (n_cols > 8) fail(EINFOLD_COMPUTE, "more than 8 key columns");
-  const int64_t ld = (total + 1) & ~(int64_t)1;
-  *ld_out = ld;
-  // Fast path: one integer column with no NULLs anywhere.
-  bool fast = n_cols == 1 && is_integer(sets[0]->kinds[0]);
-  if (fast)
-    for (auto* st : sets) fast = fast && st->cols[0].nulls == 0;
-  int bytes = 0;
-  std::vector<int> start(n_cols), pad(n_cols, 0);
+  KeyLayout L;
+  L.n_cols = sets.empty() ? 0 : (int)sets[0]->cols.size();
+  const int n_cols = L.n_cols;
+  L.fast = n_cols == 1 && is_integer(sets[0]->kinds[0]);
+  if (L.fast)
+    for (auto* st : sets) L.fast = L.fast && st->cols[0].nulls == 0;
+  std::vector<int64_t> start(n_cols), block(n_cols), max_len(n_cols, 0);
+  std::vector<int> len_bytes(n_cols, 0);
   for (int i = 0; i < n_cols; i++) {
-    start[i] = bytes;
-    const Kind k = sets[0]->kinds[i];
-    if (is_var(k)) {
-      unsigned long long mx = 0;
+    start[i] = L.bytes;
+    if (is_var(sets[0]->kinds[i])) {
       DeviceBuffer<unsigned long long> dmx(1, s);
       dmx.zero();
       for (auto* st : sets) {
         const DeviceColumn& c = st->cols[i];
-        if (c.rows)
-          escaped_max<<<blocks_for(c.rows, 256), 256, 0, s>>>(c.bytes.get(), c.offsets.get(), c.valid.get(), c.rows,
-                                                              dmx.get());
+        if (c.rows) longest<<<blocks_for(c.rows, 256), 256, 0, s>>>(c.offsets.get(), c.valid.get(), c.rows, dmx.get());
       }
+      unsigned long long mx = 0;
       EF_CUDA(cudaMemcpyAsync(&mx, dmx.get(), 8, cudaMemcpyDeviceToHost, s));
       EF_CUDA(cudaStreamSynchronize(s));
-      pad[i] = (int)mx + 2;
-      bytes += 1 + pad[i];
+      max_len[i] = (int64_t)mx;
+      while (len_bytes[i] < 8 && (mx >> (8 * len_bytes[i]))) len_bytes[i]++;
+      block[i] = 1 + max_len[i] + len_bytes[i];
     } else {
-      bytes += 1 + 8;
+      block[i] = 1 + 8;
     }
+    L.bytes += block[i];
   }
-  const int nwords = fast ? 1 : std::max(1, (bytes + 7) / 8);
-  if (nwords > kMaxWords) fail(EINFOLD_COMPUTE, "keys longer than %d bytes are not supported by the device fold", 8 * kMaxWords);
-  words.allocate((size_t)(nwords * ld ? nwords * ld : 1), s);
-  if (nwords * ld) words.zero();
-  int64_t row0 = 0;
+  L.words = L.fast ? 1 : std::max<int64_t>(1, (L.bytes + 7) / 8);
   for (auto* st : sets) {
-    KeyCols kc;
-    kc.n = n_cols;
-    kc.words = nwords;
-    kc.fast_int = fast;
-    int64_t rows = n_cols ? st->cols[0].rows : 0;
+    std::vector<KeyCol> kc(std::max(n_cols, 1));
     for (int i = 0; i < n_cols; i++) {
       const DeviceColumn& c = st->cols[i];
-      KeyCol& k = kc.c[i];
+      KeyCol& k = kc[i];
       k.kind = (int)c.kind;
       k.width = c.width;
       k.data = is_var(c.kind) ? c.bytes.get() : c.ptr();
       k.off = is_var(c.kind) ? c.offsets.get() : nullptr;
       k.valid = c.valid.get();
-      k.pad_len = pad[i];
       k.start = start[i];
+      k.block = block[i];
+      k.max_len = max_len[i];
+      k.len_bytes = len_bytes[i];
       k.canon_zero = float_keys == 1 && is_float(c.kind);
     }
+    DeviceBuffer<KeyCol> d(kc.size(), s);
+    EF_CUDA(cudaMemcpyAsync(d.get(), kc.data(), kc.size() * sizeof(KeyCol), cudaMemcpyHostToDevice, s));
+    EF_CUDA(cudaStreamSynchronize(s));  // kc leaves scope
+    L.cols.push_back(std::move(d));
+  }
+  return L;
+}
+
+// Writes the words of `list` (after `prefix`'s ranks as word 0, if given)
+// for every row of `sets`; returns the words per key.
+int encode_list(Context& ctx, const std::vector<const StagedKeySet*>& sets, const KeyLayout& L, const WordList& list,
+                const uint32_t* prefix, uint64_t* out, int64_t ld) {
+  cudaStream_t s = ctx.stream;
+  int64_t row0 = 0;
+  for (size_t i = 0; i < sets.size(); i++) {
+    const int64_t rows = L.n_cols ? sets[i]->cols[0].rows : 0;
     if (rows) {
-      encode_keys<<<blocks_for(rows, 256), 256, 0, s>>>(kc, rows, row0, words.get(), ld);
+      encode_words<<<blocks_for(rows, 256), 256, 0, s>>>(L.cols[i].get(), L.n_cols, L.fast, list, prefix, rows, row0,
+                                                         out, ld);
       ctx.kernels++;
     }
     row0 += rows;
   }
-  (void)total;
   EF_LAUNCH_CHECK();
-  return nwords;
+  return (prefix ? 1 : 0) + (L.fast ? 1 : list.n);
+}
+
+// The positions of the words that differ between two keys, in order.
+std::vector<int64_t> varying_words(Context& ctx, const std::vector<const StagedKeySet*>& sets, const KeyLayout& L) {
+  cudaStream_t s = ctx.stream;
+  std::vector<int64_t> out;
+  constexpr int64_t kSpan = 8192;  // word positions a launch covers
+  for (int64_t w0 = 0; w0 < L.words; w0 += kSpan) {
+    const int64_t span = std::min(kSpan, L.words - w0);
+    DeviceBuffer<unsigned long long> any((size_t)span, s), all((size_t)span, s);
+    any.zero();
+    EF_CUDA(cudaMemsetAsync(all.get(), 0xff, (size_t)span * 8, s));
+    for (size_t i = 0; i < sets.size(); i++) {
+      const int64_t rows = sets[i]->cols[0].rows;
+      if (!rows) continue;
+      const unsigned bx = blocks_for(rows, 256, std::max<unsigned>(1u, (unsigned)(148 * 32 / span)));
+      word_spread<<<dim3(bx, (unsigned)span), 256, 0, s>>>(L.cols[i].get(), L.n_cols, rows, w0, any.get(), all.get());
+      ctx.kernels++;
+    }
+    EF_LAUNCH_CHECK();
+    std::vector<unsigned long long> ha((size_t)span), hl((size_t)span);
+    EF_CUDA(cudaMemcpyAsync(ha.data(), any.get(), (size_t)span * 8, cudaMemcpyDeviceToHost, s));
+    EF_CUDA(cudaMemcpyAsync(hl.data(), all.get(), (size_t)span * 8, cudaMemcpyDeviceToHost, s));
+    EF_CUDA(cudaStreamSynchronize(s));
+    for (int64_t w = 0; w < span; w++)
+      if (ha[(size_t)w] != hl[(size_t)w]) out.push_back(w0 + w);
+  }
+  return out;
 }
 
 struct RankSet {
@@ -469,6 +562,15 @@ struct RankSet {
   int64_t count = 0;
 };
 
+// The ranks of the keys of `sets` (rows concatenated) in the order of their
+// bytes (discriminate.rs:212-292). Keys of up to four words are ranked in one
+// radix sort. Longer keys (long strings, many columns; the reference's
+// by_bytes, :165-209) are ranked over the words that differ between keys
+// only, four at a time: the first sort orders the first four such words, and
+// each further sort orders (the previous sort's rank, the next three words),
+// which refines the ranks of the keys that agreed so far. The ranks order the
+// keys as their bytes do, and the sorts are stable, so first[r] is the
+// smallest row of rank r. It stops once every key has its own rank.
 RankSet rank_sets(Context& ctx, const std::vector<const StagedKeySet*>& sets, int64_t total, int float_keys) {
   RankSet r;
   cudaStream_t s = ctx.stream;
@@ -476,21 +578,68 @@ RankSet rank_sets(Context& ctx, const std::vector<const StagedKeySet*>& sets, in
   r.first.allocate((size_t)(total ? total : 1), s);
   if (total == 0) return r;
   const int n_cols = sets.empty() ? 0 : (int)sets[0]->cols.size();
-  if (n_cols == 0) {
-    // No columns: every key is empty, one rank, first row 0.
+  auto all_equal = [&]() {
+    // Every key is the same: one rank, first row 0.
     EF_CUDA(cudaMemsetAsync(r.rank.get(), 0, (size_t)total * 4, s));
     EF_CUDA(cudaMemsetAsync(r.first.get(), 0, 4, s));
     r.count = 1;
+  };
+  if (n_cols == 0) {
+    all_equal();
     return r;
   }
-  DeviceBuffer<uint64_t> words;
-  int64_t ld = 0;
-  const int nw = encode_sets(ctx, sets, float_keys, total, words, &ld);
-  r.count = rank_keys(ctx, words.get(), nw, total, ld, r.rank.get(), r.first.get(), s);
+  KeyLayout L = layout_of(ctx, sets, float_keys);
+  const int64_t ld = (total + 1) & ~(int64_t)1;
+  if (L.words <= kMaxWords) {
+    WordList list;
+    list.n = (int)L.words;
+    for (int i = 0; i < list.n; i++) list.pos[i] = i;
+    DeviceBuffer<uint64_t> words((size_t)(list.n * ld), s);
+    const int nw = encode_list(ctx, sets, L, list, nullptr, words.get(), ld);
+    r.count = rank_keys(ctx, words.get(), nw, total, ld, r.rank.get(), r.first.get(), s);
+    return r;
+  }
+  const std::vector<int64_t> vary = varying_words(ctx, sets, L);
+  if (vary.empty()) {
+    all_equal();
+    return r;
+  }
+  DeviceBuffer<uint64_t> words((size_t)(kMaxWords * ld), s);
+  DeviceBuffer<uint32_t> prev((size_t)total, s);
+  size_t at = 0;
+  bool refining = false;
+  while (at < vary.size()) {
+    WordList list;
+    const int room = refining ? kMaxWords - 1 : kMaxWords;
+    while (list.n < room && at < vary.size()) list.pos[list.n++] = vary[at++];
+    if (refining) EF_CUDA(cudaMemcpyAsync(prev.get(), r.rank.get(), (size_t)total * 4, cudaMemcpyDeviceToDevice, s));
+    const int nw = encode_list(ctx, sets, L, list, refining ? prev.get() : nullptr, words.get(), ld);
+    r.count = rank_keys(ctx, words.get(), nw, total, ld, r.rank.get(), r.first.get(), s);
+    refining = true;
+    if (r.count == total) break;  // every key has its own rank already
+  }
   return r;
 }
 
 }  // namespace
+
+int64_t rank_columns(Context& ctx, const Relation& r, const std::vector<int>& cols, int float_keys, uint32_t* rank,
+                     uint32_t* first, bool device_out) {
+  cudaStream_t s = ctx.stream;
+  const int64_t n = r.rows();
+  if (n >= (int64_t)UINT32_MAX) fail(EINFOLD_COMPUTE, "EinFold's discrimination algorithm ranks at most 2^32 - 1 rows together");
+  for (int c : cols)
+    if (c < 0 || c >= (int)r.fields.size()) fail(EINFOLD_INVALID, "no column %d", c);
+  StagedKeySet ks = stage_set(ctx, r, cols);
+  RankSet rs = rank_sets(ctx, {&ks}, n, float_keys);
+  const cudaMemcpyKind kind = device_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (n) {
+    EF_CUDA(cudaMemcpyAsync(rank, rs.rank.get(), (size_t)n * 4, kind, s));
+    EF_CUDA(cudaMemcpyAsync(first, rs.first.get(), (size_t)rs.count * 4, kind, s));
+  }
+  EF_CUDA(cudaStreamSynchronize(s));
+  return rs.count;
+}
 
 FoldOutput discriminate_fold(Context& ctx, const FoldD& f, const Relation& a, const Relation& b,
                              const Relation* domain, const std::vector<Field>& schema, const einfold_options& o,

@@ -119,6 +119,12 @@ struct FoldOutput {
 
 FoldOutput dense_fold(Context& ctx, const FoldD& f, const Relation& a, const Relation& b, const Relation* domain,
                       const std::vector<Field>& schema, const einfold_options& o, Budget& budget);
+// The ranks of the keys in columns `cols` of `r` (rank_columns,
+// discriminate.rs:240-277): rank[i] per row, first[k] the smallest row of rank
+// k; returns the number of ranks. Outputs in host memory, or device memory
+// when `device_out`.
+int64_t rank_columns(Context& ctx, const Relation& r, const std::vector<int>& cols, int float_keys, uint32_t* rank,
+                     uint32_t* first, bool device_out);
 FoldOutput discriminate_fold(Context& ctx, const FoldD& f, const Relation& a, const Relation& b,
                              const Relation* domain, const std::vector<Field>& schema, const einfold_options& o,
                              Budget& budget);

@@ -903,20 +903,69 @@ constexpr size_t kStaticScratchBytes = (size_t)64 << 20;
 __device__ __align__(256) uint8_t g_split_scratch[kStaticScratchBytes];
 
 std::mutex g_static_lock;
-void* g_static_base[64] = {};
+struct StaticBase {
+  void* context = nullptr;  // the CUDA context the address belongs to
+  void* ptr = nullptr;
+};
+StaticBase g_static_base[64];
 
-// The array's device address on the current device. The first call on a
-// device looks it up (and sets the product kernels' shared-memory limit);
-// host code can't use the array's name as an address.
+// The calling thread's current CUDA context (the driver's cuCtxGetCurrent,
+// reached through the runtime's entry-point query).
+void* current_context() {
+  typedef int (*GetCurrent)(void**);
+  static GetCurrent fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (GetCurrent)p;
+  });
+  if (!fn) fail(EINFOLD_DEVICE, "cuCtxGetCurrent is unavailable");
+  void* c = nullptr;
+  if (fn(&c) != 0) fail(EINFOLD_DEVICE, "cuCtxGetCurrent failed");
+  return c;
+}
+
+// The array's device address in the current context of `device`. Host code
+// can't use the array's name as an address: the first call in a context
+// looks the address up with cudaGetSymbolAddress and keeps it with the
+// context's handle; a new context on the device (after cudaDeviceReset, say,
+// which reloads the module at another address) looks it up again.
 uint8_t* static_scratch(int device) {
-  std::lock_guard<std::mutex> lock(g_static_lock);
   if (device < 0 || device >= 64) fail(EINFOLD_INVALID, "device %d out of range", device);
-  if (!g_static_base[device]) {
+  void* ctx = current_context();
+  if (!ctx) {
+    // No context yet on this thread: the device's primary context, as the
+    // runtime would make current at its first call that needs one.
+    EF_CUDA(cudaSetDevice(device));
+    ctx = current_context();
+    if (!ctx) fail(EINFOLD_DEVICE, "no current CUDA context");
+  }
+  std::lock_guard<std::mutex> lock(g_static_lock);
+  StaticBase& b = g_static_base[device];
+  if (b.context != ctx || !b.ptr) {
     void* p = nullptr;
     EF_CUDA(cudaGetSymbolAddress(&p, g_split_scratch));
-    g_static_base[device] = p;
+    b.context = ctx;
+    b.ptr = p;
   }
-  return (uint8_t*)g_static_base[device];
+  return (uint8_t*)b.ptr;
+}
+
+// The scratch a product needs, saturating instead of wrapping: sizes whose
+// product would overflow 64 bits compare as larger than any array.
+uint64_t static_scratch_needed(int S, int64_t batches, int64_t m, int64_t n, int64_t k) {
+  const SplitDims d = split_dims(m, n, k);
+  auto al = [](uint64_t x) { return sat_add(x, 255) & ~(uint64_t)255; };
+  const uint64_t bs = sat_mul((uint64_t)batches, (uint64_t)S);
+  uint64_t t = al(sat_mul(sat_mul(bs, (uint64_t)d.m_pad), (uint64_t)d.k_pad));
+  t = sat_add(t, al(sat_mul(sat_mul(bs, (uint64_t)d.n_pad), (uint64_t)d.k_pad)));
+  t = sat_add(t, al(sat_mul(sat_mul((uint64_t)batches, (uint64_t)d.m_pad), 4)));
+  t = sat_add(t, al(sat_mul(sat_mul((uint64_t)batches, (uint64_t)d.n_pad), 4)));
+  t = sat_add(t, al(sat_mul(sat_mul((uint64_t)batches, (uint64_t)n), 8)));
+  return sat_add(t, 256);
 }
 
 }  // namespace
@@ -942,14 +991,15 @@ extern "C" int32_t einfold_split_gemm_static(const double* a, const double* b, d
       EF_CUDA(cudaStreamSynchronize(s));
       return EINFOLD_OK;
     }
+    if (k > INT64_MAX / 2) fail(EINFOLD_INVALID, "a product too large");
+    const uint64_t need = static_scratch_needed(S, batches, m, n, k);
+    if (need > kStaticScratchBytes)
+      fail(EINFOLD_INVALID,
+           "this product needs %llu bytes of scratch, more than the %zu einfold_split_gemm_static holds; "
+           "use einfold_split_gemm", (unsigned long long)need, kStaticScratchBytes);
+    // Within the array, so every size below fits in 64 bits.
     size_t sz[6];
     split_scratch_sizes(S, batches, m, n, k, sz);
-    size_t total = 0;
-    for (size_t x : sz) total += x;
-    if (total > kStaticScratchBytes)
-      fail(EINFOLD_INVALID,
-           "this product needs %zu bytes of scratch, more than the %zu einfold_split_gemm_static holds; "
-           "use einfold_split_gemm", total, kStaticScratchBytes);
     SplitScratch sc;
     uint8_t* p = base;
     sc.da = (int8_t*)p; p += sz[0];

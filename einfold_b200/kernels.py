@@ -17,6 +17,7 @@ import enum
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence
 
+import numpy as np
 import pyarrow as pa
 
 from . import _lib, ir
@@ -513,6 +514,38 @@ def pipeline(p: ir.Pipeline, operands: Sequence, schema: Optional[pa.Schema] = N
         return Piped(_device_batches(res) if options.result_on_device else _collect(res), visited, tiles)
     finally:
         keep.release()
+
+
+@dataclass
+class Ranks:
+    """Each row's rank among the distinct keys, and the first row of each rank."""
+
+    rank: np.ndarray  # uint32 per row
+    first: np.ndarray  # uint32 per distinct key
+
+
+def rank_columns(relation: Relation, columns: Sequence[int], float_keys: FloatKeys = FloatKeys.BITWISE,
+                 device: int = 0) -> Ranks:
+    """``rank_columns`` (discriminate.rs:240-277) on the device: the ranks of
+    the keys in ``columns`` of a host relation, in the order of Arrow's row
+    format, keys of any length."""
+    n = sum(b.num_rows for b in relation.batches)
+    rank = np.zeros(max(n, 1), dtype=np.uint32)
+    first = np.zeros(max(n, 1), dtype=np.uint32)
+    cols = np.asarray(list(columns), dtype=np.int32)
+    k = ctypes.c_int64(0)
+    keep = _Keep()
+    try:
+        st = _lib.load().einfold_rank_columns(_lib.context(device), ctypes.byref(_relation(relation, keep)),
+                                              len(cols), cols.ctypes.data if len(cols) else None, int(float_keys),
+                                              rank.ctypes.data, first.ctypes.data, ctypes.byref(k))
+    finally:
+        keep.release()
+    if st != _lib.OK:
+        if st == _lib.DECLINED:
+            raise ArrowComputeError("the ranking declined: " + _lib.load().einfold_last_error().decode())
+        _raise(st, _lib.load().einfold_last_error().decode())
+    return Ranks(rank[:n], first[: k.value].copy())
 
 
 def schema(f: ir.Fold, operands: Sequence[pa.Schema], domain: Optional[pa.Schema] = None) -> pa.Schema:

@@ -265,6 +265,20 @@ void einfold_result_release(einfold_result* result);
 int32_t einfold_rank_words(einfold_context* ctx, const uint64_t* words, int64_t n, uint32_t* rank,
                            uint32_t* first, int64_t* n_ranks, void* stream);
 
+/* The ranks of a relation's key columns (rank_columns,
+ * crates/einfold-kernels/src/discriminate.rs:240-277, with ranks and by_bytes
+ * at :165-235): rank[i] the number of distinct keys below row i's key in the
+ * order of Arrow's row format (NULL first, integers by value, floats in
+ * total order, strings and binaries by their bytes, a prefix first; -0.0 and
+ * 0.0 one key under float_keys = 1), first[r] the smallest row of rank r;
+ * *n_ranks the number of distinct keys. Keys of any length and any number of
+ * columns. rank has a slot per row and first one per distinct key (at most
+ * the rows); both are host memory for a relation in host memory, device
+ * memory of its device for one in HBM. */
+int32_t einfold_rank_columns(einfold_context* ctx, const einfold_relation* relation, int32_t n_columns,
+                             const int32_t* columns, int32_t float_keys, uint32_t* rank, uint32_t* first,
+                             int64_t* n_ranks);
+
 /* C[w] = A[w] · B[w] for w < batches, FP64, all row-major device arrays:
  * A [batches][m][k], B [batches][k][n] (b_transposed = 0) or
  * [batches][n][k] (b_transposed = 1), C [batches][m][n].
@@ -288,7 +302,8 @@ int32_t einfold_fp64_gemm(einfold_context* ctx, const double* a, const double* b
  * with the sizes in `message`, and einfold_split_gemm is the one to call.
  * No context: it runs on the calling thread's current device and `stream`
  * (NULL: the legacy default stream) and returns once the product is done.
- * It calls no cudaMalloc or cudaFree. Its first call on a device looks up
+ * It calls no cudaMalloc or cudaFree. Its first call on a device (in each
+ * CUDA context the device gets, e.g. again after cudaDeviceReset) looks up
  * the array's address, so make that call before any stream capture. Every
  * call shares the array: calls that overlap on the GPU, from two threads or
  * two streams, race and give wrong results; serialize them. */
