@@ -170,6 +170,44 @@ def _attention_inputs(device, groups=B * H):
     return q, k, v, d_out
 
 
+def _attention_pipeline(causal=True):
+    """Config 3 as einfold's pipeline: q(b, h, t, d, x), k(b, h, t, d, x),
+    v(b, h, t, c, x); scores SUM(q.x * k.x) over d, weights exp(s - MAX(s))
+    over (b, h, tq) normalised by their sum, out(b, h, tq, c) = SUM(w * v.x);
+    causal mask tq >= tk. Dimensions: 0 b, 1 h, 2 tq, 3 d, 4 tk, 5 c."""
+    from einfold_b200 import ir
+
+    e = ir.EQ
+    q = ir.Operand([(0, 0), (1, 1), (2, 2), (3, 3)], 4)
+    k = ir.Operand([(0, 0), (1, 1), (4, 2), (3, 3)], 4)
+    producer = ir.Fold([e] * 5, [q, k], [ir.Output(0), ir.Output(1), ir.Output(2), ir.Output(4)])
+    if causal:
+        producer = producer.with_conditions([ir.Condition(2, ir.Comparison.GREATER_OR_EQUAL, 4, 0)])
+    values = ir.Operand([(0, 0), (1, 1), (4, 2), (5, 3)], 4)
+    return ir.Pipeline(producer, ir.Weight.exp(), [e], values, [0, 1, 2, 5], ir.Normalizer.KEPT_GROUPS)
+
+
+def _host_table(names, extents, values, pinned):
+    """A host Arrow table in pinned memory: every key tuple of `extents`
+    (first slowest) and a value per row, from a device tensor."""
+    import pyarrow as pa
+    import torch
+
+    from einfold_b200 import synthetic as S
+
+    def col(t):
+        h = torch.empty(t.numel(), dtype=t.dtype, pin_memory=True)
+        h.copy_(t.reshape(-1))
+        pinned.append(h)
+        return pa.Array.from_buffers(pa.int64() if t.dtype == torch.int64 else pa.float64(), t.numel(),
+                                     [None, pa.foreign_buffer(h.data_ptr(), h.numel() * 8, base=h)])
+
+    keys = S.grid_keys(extents, values.device)
+    cols = [col(x) for x in keys] + [col(values)]
+    del keys
+    return pa.record_batch(cols, names=list(names) + ["x"])
+
+
 def _cpu_fold_sample(a_cols, b_cols, rows=1024, cols=2048):
     """A bounded sample of the fold for the CPU: a's first `rows` values of i
     against b's first `cols` values of k, every j: 2·rows·n·cols FLOP."""
@@ -279,6 +317,7 @@ def _rel(a, b):
 
 
 def run_ours(args):
+    import numpy as np
     import pyarrow as pa
     import torch
 
@@ -406,7 +445,11 @@ def run_ours(args):
     flops = FOLD + ATT_FWD + ATT_BWD
     value = replicas_value(world, flops, args.steps, ms)
 
-    # End to end: the public API from pinned host memory, results read back.
+    # End to end: the public API from pinned host memory, results read back:
+    # the fold through einfold_fold from host Arrow tables, attention through
+    # einfold_pipeline (forward) and einfold_pipeline_backward (gradients,
+    # which recomputes the forward for its log-sum-exp) from host Arrow
+    # tables q, k, v and d_out of 16.8M rows each.
     e2e = None
     if not args.no_e2e:
         pinned = []
@@ -420,39 +463,62 @@ def run_ours(args):
 
         ha = pa.record_batch([host_col(ai), host_col(aj), host_col(av)], schema=sa)
         hb = pa.record_batch([host_col(bj), host_col(bk), host_col(bv)], schema=sb)
-        hq, hk, hv, hd = (t.cpu().pin_memory() for t in (q, k, v, d_out))
-        back = [torch.empty(q.shape, dtype=torch.float64, pin_memory=True) for _ in range(4)]
+        ext = [B, H, T, D]
+        hq = _host_table(["b", "h", "t", "d"], ext, q, pinned)
+        hk = _host_table(["b", "h", "t", "d"], ext, k, pinned)
+        hv = _host_table(["b", "h", "t", "c"], ext, v, pinned)
+        hd = _host_table(["b", "h", "t", "c"], ext, d_out, pinned)
+        pipe = _attention_pipeline()
         hopts = K.Options(slices=args.slices, device=local)
+        rel = lambda t: K.Relation(t.schema, [t])
+        phases = {}
 
-        def e2e_step():
+        def e2e_step(record=False):
             res = K.fold(f, K.Relation(sa, [ha]), K.Relation(sb, [hb]), options=hopts)
-            dq, dk, dv_, dd = (t.to(dev, non_blocking=True) for t in (hq, hk, hv, hd))
-            out, lse = A.attention_forward(dq, dk, dv_, causal, 1.0, split)
-            grads = A.attention_backward(dq, dk, dv_, out, lse, dd, causal, 1.0, split)
-            for dst, src in zip(back, (out,) + tuple(grads)):
-                dst.copy_(src, non_blocking=True)
-            torch.cuda.synchronize()
-            return res
+            if record:
+                phases["fold_ms"] = K.last_call.device_ms
+            piped = K.pipeline(pipe, [rel(hq), rel(hk), rel(hv)], options=hopts)
+            if record:
+                phases["pipeline_ms"] = K.last_call.device_ms
+                phases["pipeline_product_ms"] = K.last_call.product_ms
+            grads = K.pipeline_backward(pipe, [rel(hq), rel(hk), rel(hv)], rel(hd), options=hopts)
+            if record:
+                phases["pipeline_backward_ms"] = K.last_call.device_ms
+                phases["pipeline_backward_product_ms"] = K.last_call.product_ms
+            return res, piped, grads
 
-        res = e2e_step()
-        d2h = sum(buf.size for batch in res.batches for col in batch.columns for buf in col.buffers() if buf)
-        d2h += sum(t.numel() * 8 for t in back)
-        h2d = sum(buf.size for batch in (ha, hb) for col in batch.columns for buf in col.buffers() if buf)
-        h2d += sum(t.numel() * 8 for t in (hq, hk, hv, hd))
-        del res
+        res, piped, grads = e2e_step(record=True)
+        assert piped is not None and grads is not None, K.last_call.message
+        outs = list(res.batches) + list(piped.batches) + [b for g in grads for b in g]
+        d2h = sum(buf.size for batch in outs for col in batch.columns for buf in col.buffers() if buf)
+        h2d = sum(buf.size for batch in (ha, hb, hq, hk, hv, hq, hk, hv, hd) for col in batch.columns
+                  for buf in col.buffers() if buf)
+        # Placement and staging against the product kernels, from the
+        # attention calls' device times.
+        phases["attention_staging_and_placement_ms"] = (phases["pipeline_ms"] - phases["pipeline_product_ms"] +
+                                                        phases["pipeline_backward_ms"] -
+                                                        phases["pipeline_backward_product_ms"])
+        # The same attention output as the device-array leg's (bits).
+        o_host = np.asarray(piped.batches[0].column(4).to_numpy(zero_copy_only=False))
+        o_dev = A.attention_forward(q, k, v, causal, 1.0, split)[0].reshape(-1).cpu().numpy()
+        same_as_kernel_leg = bool(np.array_equal(o_host.view(np.uint64), o_dev.view(np.uint64)))
+        del res, piped, grads, outs, o_host, o_dev
         e2e_steps = max(1, min(args.steps, 3))
         barrier()
         t0.record()
         for _ in range(e2e_steps):
-            del_res = e2e_step()
-            del del_res
+            out_ = e2e_step()
+            del out_
         t1.record()
         barrier()
         ems = max_over_ranks(t0.elapsed_time(t1), dist, dev)
         e2e = {"value": replicas_value(world, flops, e2e_steps, ems), "unit": "TFLOP/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
-               "ms_per_step": ems / e2e_steps}
-        del ha, hb, pinned, hq, hk, hv, hd, back
+               "ms_per_step": ems / e2e_steps,
+               "path": "einfold_fold + einfold_pipeline + einfold_pipeline_backward from host Arrow tables "
+                       "(a(i,j,v), b(j,k,v) 67.1M rows; q, k, v, d_out 16.8M rows), results to host Arrow",
+               "phases_ms": phases, "attention_out_same_bits_as_device_array_leg": same_as_kernel_leg}
+        del ha, hb, hq, hk, hv, hd, pinned
 
     # Rooflines of the three product kernels: digit ops executed on the
     # tensor cores per second against the int8 dense peak.
@@ -529,10 +595,14 @@ def run_ours(args):
 
 def _ranking(hbm, basis):
     """einfold_rank_words on random 64-bit keys (each drawn from a pool of
-    n/2), timed with CUDA events: 2^28 keys (8 GB-scale passes, beyond L2)
-    and 4M keys (the sorting path's join column). Bytes moved, per key: 8
-    read by the varying-byte scan; per 8-bit pass 8 (digit counts) + 12 read
-    + 12 written; then 9 (run heads) + 17 (ranks and first rows)."""
+    n/2), timed with CUDA events: 2^28 keys (passes of 6 GB, beyond L2) and
+    4M keys (the sorting path's join column over a and b). Two fractions of
+    HBM bandwidth: over the bytes the kernels move, per key 8 read for the
+    byte histograms, per 8-bit pass 12 read and 12 written (the first pass
+    reads no row numbers), then 12 read and 4 written for the ranks plus 4
+    per distinct key for the first rows; and over the algorithmic bytes of
+    the ranking itself, 8 B of key read, 4 B of rank and 4 B of first row
+    written per key."""
     import ctypes
 
     import torch
@@ -546,6 +616,12 @@ def _ranking(hbm, basis):
         pool = S.u64(SEED, 7, n // 2)
         words = pool[(S.u64(SEED, 8, n) % (n // 2)).to(torch.int64)].contiguous()
         del pool
+        w64 = words.view(torch.int64)
+        varying = 0
+        for b in range(8):
+            byte = (w64 >> (8 * b)) & 255
+            varying += int(byte.min().item() != byte.max().item())
+            del byte
         rank_ = torch.empty(n, dtype=torch.int32, device="cuda")
         first = torch.empty(n, dtype=torch.int32, device="cuda")
         k = ctypes.c_int64(0)
@@ -561,11 +637,14 @@ def _ranking(hbm, basis):
             assert st == _lib.OK
             times.append(e0.elapsed_time(e1))
         ms = statistics.median(times[1:])
-        passes = 8
-        moved = n * (8 + passes * 32 + 26)
+        passes = varying
+        moved = n * (8 + (20 + (passes - 1) * 24 if passes else 0) + 16) + k.value * 4
+        algorithmic = n * 16
         out[f"n{n}"] = {"keys": n, "distinct": k.value, "ms": ms, "gkeys_per_s": n / ms / 1e6, "passes": passes,
-                        "moved_gb_per_s": moved / ms / 1e6, "frac_of_hbm": moved / ms / 1e6 / hbm}
-        del words, rank_, first
+                        "moved_gb_per_s": moved / ms / 1e6, "frac_of_hbm": moved / ms / 1e6 / hbm,
+                        "algorithmic_gb_per_s": algorithmic / ms / 1e6,
+                        "frac_of_hbm_algorithmic": algorithmic / ms / 1e6 / hbm}
+        del words, rank_, first, w64
         torch.cuda.empty_cache()
     out["peak"] = {"hbm_gb_per_s": hbm, "basis": basis}
     return out
@@ -642,77 +721,61 @@ def _ragged():
 
 
 def _sparse_tables():
-    """The sorting path's tables at 1/40 of their size: a(i, j, v) and b(j,
-    k, v), 50,000 rows each; i and k 16-hex-digit strings from 50,000
-    distinct, j 63-bit hashes from a pool of 200,000 drawn with Zipf(1.1)
-    frequencies, v normal(0, 1); SplitMix64 (seed 0, salts 11-17)."""
-    import numpy as np
+    """The sorting path's tables at 1/40 of their size (synthetic.sorting_tables:
+    a(i, j, v) and b(j, k, v), 50,000 rows each; i and k 16-hex-digit strings
+    from 50,000 distinct, j 63-bit hashes from a pool of 200,000 drawn with
+    Zipf(1.1) frequencies, v normal(0, 1)), and the regridding variant's
+    weight table at 1/40 (w(src, dst, wt), 100,000 rows, src from the same
+    pool and law, dst from 50,000 int64 cells, wt uniform[0, 1))."""
     import pyarrow as pa
 
     from einfold_b200 import synthetic as S
 
-    n, pool, names = 50_000, 200_000, 50_000
-
-    def units(salt, m):
-        return S.units(SEED, salt, m, device="cpu").to(dtype=__import__("torch").float64).numpy()
-
-    def hexes(salt):
-        words = S.u64(SEED, salt, names, device="cpu").numpy().view(np.uint64)
-        return np.array([f"{int(x):016x}" for x in words], dtype=object)
-
-    hashes = S.u64(SEED, 13, pool, device="cpu").numpy().view(np.uint64) >> np.uint64(1)
-    cdf = np.cumsum(np.arange(1, pool + 1, dtype=np.float64) ** -1.1)
-    cdf /= cdf[-1]
-
-    def joins(salt):
-        return hashes[np.searchsorted(cdf, units(salt, n), side="right").clip(0, pool - 1)].astype(np.int64)
-
-    def normal(salt):
-        u1, u2 = units(salt, n), units(salt + 100, n)
-        return np.sqrt(-2.0 * np.log1p(-u1)) * np.cos(2 * np.pi * u2)
-
-    ia, kb = hexes(11), hexes(12)
-    pick_a = (units(14, n) * names).astype(np.int64).clip(0, names - 1)
-    pick_b = (units(15, n) * names).astype(np.int64).clip(0, names - 1)
-    ja, jb = joins(16), joins(17)
-    a = pa.record_batch([pa.array(ia[pick_a], pa.string()), pa.array(ja), pa.array(normal(18))], names=["i", "j", "v"])
-    b = pa.record_batch([pa.array(jb), pa.array(kb[pick_b], pa.string()), pa.array(normal(19))], names=["j", "k", "v"])
-    ua, ca = np.unique(ja, return_counts=True)
-    ub, cb = np.unique(jb, return_counts=True)
-    common, xa, xb = np.intersect1d(ua, ub, return_indices=True)
-    pairs = int((ca[xa].astype(np.int64) * cb[xb].astype(np.int64)).sum())
-    return a, b, pairs
+    a, b = S.sorting_tables(50_000, seed=SEED)
+    wt = S.regrid_table(100_000, seed=SEED)
+    w = pa.record_batch([wt.column(0), wt.column(1), wt.column(2)], names=["j", "k", "v"])
+    pairs = S.joined_pairs(a.column(1).to_numpy(), b.column(0).to_numpy())
+    regrid_pairs = S.joined_pairs(a.column(1).to_numpy(), w.column(0).to_numpy())
+    return a, b, pairs, w, regrid_pairs
 
 
 def _sparse(cpu=False):
     """The discrimination fold (ranking, counting sorts, the Gustavson
     product, grouped output) on the sorting path's tables scaled to 50,000
-    rows an operand, result left in HBM, timed with CUDA events: pair
-    products (one per pair of rows joining on j) per second."""
+    rows an operand, and on the regridding variant (a weighted by w on
+    j = src, grouped by i and dst), results left in HBM, timed with CUDA
+    events: pair products (one per pair of rows joining on j) per second."""
     import torch
 
     from einfold_b200 import kernels as K
 
-    a, b, pairs = _sparse_tables()
+    a, b, pairs, w, regrid_pairs = _sparse_tables()
     f = _matmul_fold()
     opts = K.Options(result_on_device=True)
-    ra, rb = K.Relation(a.schema, [a]), K.Relation(b.schema, [b])
-    times, groups, alg = [], 0, None
-    for _ in range(4):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record()
-        got = K.fold(f, ra, rb, options=opts)
-        e1.record()
-        torch.cuda.synchronize()
-        times.append(e0.elapsed_time(e1))
-        alg = got.algorithm.name.lower()
-        groups = sum(batch.rows for batch in got.batches)
-        for batch in got.batches:
-            batch.release()
-    ms = statistics.median(times[1:])
-    out = {"rows_per_operand": a.num_rows, "pairs": pairs, "groups": groups, "algorithm": alg, "ms": ms,
-           "gpairs_per_s": pairs / ms / 1e6, "host_to_device": "the Arrow tables are copied in each call"}
+
+    def run(left, right, n_pairs):
+        ra, rb = K.Relation(left.schema, [left]), K.Relation(right.schema, [right])
+        times, groups, alg = [], 0, None
+        for _ in range(4):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            got = K.fold(f, ra, rb, options=opts)
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+            alg = got.algorithm.name.lower()
+            groups = sum(batch.rows for batch in got.batches)
+            for batch in got.batches:
+                batch.release()
+        ms = statistics.median(times[1:])
+        return {"rows": [left.num_rows, right.num_rows], "pairs": n_pairs, "groups": groups, "algorithm": alg,
+                "ms": ms, "gpairs_per_s": n_pairs / ms / 1e6,
+                "host_to_device": "the Arrow tables are copied in each call"}
+
+    out = run(a, b, pairs)
+    out["rows_per_operand"] = a.num_rows
+    out["regrid"] = run(a, w, regrid_pairs)
     if cpu:
         # The CPU baseline leg: the oracle's restatement of discriminate::fold
         # (one host thread), on the same tables.

@@ -131,6 +131,9 @@ SIGNATURES = {
                                             ctypes.POINTER(Options), ctypes.POINTER(Result)]),
     "einfold_pipeline": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(PipelineDesc), ctypes.POINTER(Relation),
                                           ctypes.POINTER(Options), ctypes.POINTER(Result)]),
+    "einfold_pipeline_backward": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(PipelineDesc),
+                                                   ctypes.POINTER(Relation), ctypes.POINTER(Relation),
+                                                   ctypes.POINTER(Options), ctypes.POINTER(Result)]),
     "einfold_schema": (ctypes.c_int32, [ctypes.POINTER(FoldDesc), ctypes.POINTER(ctypes.POINTER(ArrowSchema)),
                                         ctypes.c_int32, ctypes.POINTER(ArrowSchema), ctypes.POINTER(ArrowSchema),
                                         ctypes.c_char_p, ctypes.c_int32]),
@@ -143,6 +146,9 @@ SIGNATURES = {
     "einfold_rank_columns": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(Relation), ctypes.c_int32,
                                               ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
                                               ctypes.POINTER(ctypes.c_int64)]),
+    "einfold_check_wait": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
+    "einfold_exp_weights": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                             ctypes.c_int32, ctypes.c_void_p]),
     "einfold_split_gemm": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                             ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                             ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),

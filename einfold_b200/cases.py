@@ -127,17 +127,15 @@ def ragged(groups: int, d: int, radius: int, repeat: int) -> None:
 
 
 def sparse() -> None:
-    import os
-    import sys
-
-    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
-    import bench
-
+    from . import ir
     from . import kernels as K
 
-    a, b, pairs = bench._sparse_tables()
-    got = K.fold(bench._matmul_fold(), K.Relation(a.schema, [a]), K.Relation(b.schema, [b]),
-                 options=K.Options(result_on_device=True))
+    a, b = S.sorting_tables(50_000)
+    pairs = S.joined_pairs(a.column(1).to_numpy(), b.column(0).to_numpy())
+    e = ir.EQ
+    f = ir.Fold([e, e, e], [ir.Operand([(0, 0), (1, 1)], 2), ir.Operand([(1, 0), (2, 1)], 2)],
+                [ir.Output(0), ir.Output(2)])
+    got = K.fold(f, K.Relation(a.schema, [a]), K.Relation(b.schema, [b]), options=K.Options(result_on_device=True))
     rows = sum(batch.rows for batch in got.batches)
     for batch in got.batches:
         batch.release()

@@ -147,8 +147,12 @@ void einfold_context_destroy(einfold_context* ctx) {
   {
     ef::DeviceGuard dev(ctx->device);
     if (ctx->stream) {
-      ctx->kept.release(ctx->stream);
       cudaStreamSynchronize(ctx->stream);
+      if (ctx->aux) {
+        cudaStreamSynchronize(ctx->aux);
+        ef::device_cache_forget(ctx->aux);
+        cudaStreamDestroy(ctx->aux);
+      }
       ctx->graphs.clear();
       ef::device_cache_forget(ctx->stream);
       cudaStreamDestroy(ctx->stream);
@@ -209,6 +213,36 @@ int32_t einfold_pipeline(einfold_context* ctx, const einfold_pipeline_desc* pipe
     ef::export_result(std::move(out.batches), schema, result);
     return EINFOLD_OK;
   });
+}
+
+int32_t einfold_pipeline_backward(einfold_context* ctx, const einfold_pipeline_desc* pipeline,
+                                  const einfold_relation* operands, const einfold_relation* d_out,
+                                  const einfold_options* options, einfold_result* results) {
+  if (results) std::memset(results + 1, 0, 2 * sizeof *results);
+  const int32_t st = guarded(ctx, results, [&](ef::Context& c) -> int32_t {
+    if (!pipeline || !operands || !d_out || !results) ef::fail(EINFOLD_INVALID, "a NULL argument");
+    einfold_options o = defaults(options);
+    ef::PipelineD p = ef::parse_pipeline(pipeline);
+    std::vector<ef::Relation> rels;
+    for (int i = 0; i < 3; i++) rels.push_back(ef::import_relation(&operands[i]));
+    ef::Relation rd = ef::import_relation(d_out);
+    std::vector<const std::vector<ef::Field>*> ins = {&rels[0].fields, &rels[1].fields, &rels[2].fields};
+    ef::pipeline_schema(p, ins);  // the forward pipeline's own validity rules
+    ef::GradientOutput g = ef::pipeline_backward(c, p, rels[0], rels[1], rels[2], rd, o);
+    for (int i = 0; i < 3; i++) {
+      results[i].algorithm = EINFOLD_ALG_FUSED;
+      ef::export_result(std::move(g.batches[i]), g.schemas[i], &results[i]);
+    }
+    return EINFOLD_OK;
+  });
+  if (results) {
+    for (int i = 1; i < 3; i++) {
+      if (st != EINFOLD_OK) ef::release_result(&results[i]);
+      results[i].status = st;
+      std::memcpy(results[i].message, results[0].message, sizeof results[i].message);
+    }
+  }
+  return st;
 }
 
 int32_t einfold_schema(const einfold_fold_desc* fold, const struct ArrowSchema* const* operands, int32_t n_operands,

@@ -23,6 +23,7 @@
 // the CUDA cores.
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 #include <cmath>
 #include <type_traits>
 
@@ -1145,41 +1146,74 @@ bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd,
     a.n_ct = a.lc_pad / GJ;
     a.reverse = last_rows_longest(a.mask, a.lr);
   }
-  // The tile path, while its exports fit in half the free memory (in chunks
-  // of batches): d_k first, exporting P's digits and dS; then d_v and d_q
-  // from them, one product a tile each. Otherwise the three kernels each
-  // recompute the scores.
+  // The tile path: d_k first, exporting P's digits and dS; then d_v and d_q
+  // from them, one product a tile each. The exports take 14 bytes a pair of
+  // a batch's padded square, so batches go in chunks whose exports fit the
+  // export limit (EINFOLD_BACKWARD_EXPORT_MB, 2048 by default), in two
+  // buffers: chunks alternate between the call's stream and the context's
+  // second stream, so that one chunk's kernels run beside the other's and a
+  // chunk's last wave of blocks leaves no SM idle. The buffers are freed at
+  // the end of the call. A batch whose exports alone exceed half the limit
+  // takes the three kernels that each recompute the scores.
   const int64_t n_kb = lk_pad / GM, n_qt = lq_pad / GJ;
   const size_t p_bytes = al((size_t)(lk_pad * lq_pad * S)), ds_bytes = al((size_t)(lk_pad * lq_pad) * 8),
                pe_bytes = al((size_t)(n_kb * n_qt * GM) * 4);
   const size_t per_batch = p_bytes + ds_bytes + pe_bytes;
-  // Free memory is asked only when the kept exports are too small.
-  int64_t chunk = W;
-  if (ctx.kept.bytes < (size_t)W * per_batch) {
-    size_t free_b = 0, total_b = 0;
-    EF_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    chunk = std::min<int64_t>(W, (int64_t)((free_b / 2 + ctx.kept.bytes) / per_batch));
+  static const size_t limit = [] {
+    const char* e = std::getenv("EINFOLD_BACKWARD_EXPORT_MB");
+    const long long mb = e ? std::atoll(e) : 2048;
+    return (size_t)std::max(0ll, mb) << 20;
+  }();
+  int64_t chunk = 0, buffers = 1;
+  if ((size_t)W * per_batch <= limit) {
+    chunk = W;
+  } else {
+    chunk = std::min<int64_t>(W, (int64_t)(limit / 2 / per_batch));
+    buffers = 2;
   }
-  uint8_t* p_tiles = chunk >= 1 ? (uint8_t*)ctx.kept.get((size_t)chunk * per_batch, s) : nullptr;
-  cudaEvent_t e0, e1;
+  DeviceBuffer<uint8_t> exports[2];
+  cudaStream_t streams[2] = {s, s};
+  cudaEvent_t e0, e1, joined = nullptr;
   EF_CUDA(cudaEventCreate(&e0));
   EF_CUDA(cudaEventCreate(&e1));
   EF_CUDA(cudaEventRecord(e0, s));
+  if (chunk >= 1 && buffers == 2) {
+    if (!ctx.aux) EF_CUDA(cudaStreamCreateWithFlags(&ctx.aux, cudaStreamNonBlocking));
+    streams[1] = ctx.aux;
+    EF_CUDA(cudaEventCreateWithFlags(&joined, cudaEventDisableTiming));
+    EF_CUDA(cudaEventRecord(joined, s));  // the slicing above, before the second stream starts
+    EF_CUDA(cudaStreamWaitEvent(ctx.aux, joined, 0));
+  }
   if (chunk >= 1) {
-    double* ds = (double*)(p_tiles + (size_t)chunk * p_bytes);
-    int32_t* p_exp = (int32_t*)((uint8_t*)ds + (size_t)chunk * ds_bytes);
-    const CUtensorMap tds = f64_boxes_map(ds, lk_pad, lq_pad, chunk, 16, GM);
-    for (int64_t w0 = 0; w0 < W; w0 += chunk) {
+    CUtensorMap tds[2];
+    double* ds[2] = {};
+    int32_t* p_exp[2] = {};
+    uint8_t* p_tiles[2] = {};
+    for (int b = 0; b < buffers; b++) {
+      exports[b].allocate((size_t)chunk * per_batch, streams[b]);
+      p_tiles[b] = exports[b].get();
+      ds[b] = (double*)(p_tiles[b] + (size_t)chunk * p_bytes);
+      p_exp[b] = (int32_t*)((uint8_t*)ds[b] + (size_t)chunk * ds_bytes);
+      tds[b] = f64_boxes_map(ds[b], lk_pad, lq_pad, chunk, 16, GM);
+    }
+    int c = 0;
+    for (int64_t w0 = 0; w0 < W; w0 += chunk, c++) {
+      const int b = c % buffers;
+      cudaStream_t st = streams[b];
       const unsigned wc = (unsigned)std::min<int64_t>(chunk, W - w0);
       GradArgs k = args[GRAD_K], v = args[GRAD_V], q = args[GRAD_Q];
       k.w0 = v.w0 = q.w0 = (int)w0;
-      k.p_tiles = v.p_tiles = p_tiles;
-      k.p_exp = v.p_exp = p_exp;
-      k.ds_out = ds;
-      launch_split<GRAD_K>(mode_maps[GRAD_K], k, dim3((unsigned)n_kb, wc), fast, s);
-      launch_tiles<GRAD_V>(tds, mode_maps[GRAD_V][4], v, dim3((unsigned)n_kb, wc), s);
-      launch_tiles<GRAD_Q>(tds, mode_maps[GRAD_Q][4], q, dim3((unsigned)(lq_pad / GM), wc), s);
+      k.p_tiles = v.p_tiles = p_tiles[b];
+      k.p_exp = v.p_exp = p_exp[b];
+      k.ds_out = ds[b];
+      launch_split<GRAD_K>(mode_maps[GRAD_K], k, dim3((unsigned)n_kb, wc), fast, st);
+      launch_tiles<GRAD_V>(tds[b], mode_maps[GRAD_V][4], v, dim3((unsigned)n_kb, wc), st);
+      launch_tiles<GRAD_Q>(tds[b], mode_maps[GRAD_Q][4], q, dim3((unsigned)(lq_pad / GM), wc), st);
       ctx.kernels += 3;
+    }
+    if (joined) {
+      EF_CUDA(cudaEventRecord(joined, ctx.aux));  // the second stream's chunks, before the call's stream goes on
+      EF_CUDA(cudaStreamWaitEvent(s, joined, 0));
     }
   } else {
     for (int mode = 0; mode < 3; mode++) {
@@ -1199,6 +1233,7 @@ bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd,
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (joined) cudaEventDestroy(joined);
   if (st & 2) fail(EINFOLD_TIMEOUT, "a bounded wait in the attention backward ran out");
   // Digit products executed: per pair of tiles, S(S+1)/2 digit pairs of a
   // 128 x 64 x 64 product, three for d_k, and for d_v and d_q one on the

@@ -155,27 +155,6 @@ struct PinnedArena {
   }
 };
 
-// Device scratch kept across calls: grown on demand (stream-ordered),
-// freed with the context. Calls that use it end synchronized, so the next
-// call may reuse it on any stream.
-struct KeptScratch {
-  void* ptr = nullptr;
-  size_t bytes = 0;
-  void* get(size_t n, cudaStream_t s) {
-    if (n > bytes) {
-      release(s);
-      EF_CUDA(cudaMallocAsync(&ptr, n, s));
-      bytes = n;
-    }
-    return ptr;
-  }
-  void release(cudaStream_t s) {
-    if (ptr) cudaFreeAsync(ptr, s);
-    ptr = nullptr;
-    bytes = 0;
-  }
-};
-
 // Instantiated CUDA graphs of a context's launch sequences. An entry is
 // replayed only when every argument its launches were captured with
 // (pointers included) is the same. Arguments seen for the first time are
@@ -214,7 +193,10 @@ struct Context {
   uint64_t kernels = 0;  // kernels launched by the current call
   double product_ms = 0, product_ops = 0;  // the split products' kernels in the current call
   PinnedArena pinned;
-  KeptScratch kept;  // the attention backward's exports
+  // A second stream of the context, for work that overlaps the main
+  // stream's within one call (created on first use, destroyed with the
+  // context).
+  cudaStream_t aux = nullptr;
   GraphCache graphs;
   // The current call's attention forward: its schedule (-1: none) and how
   // its tile phase ran (0 launched directly, else GraphCache::run's value).

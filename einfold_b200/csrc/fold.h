@@ -133,4 +133,15 @@ FoldOutput chain_fold(Context& ctx, const FoldD& f, const std::vector<const Rela
 FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, const Relation& k, const Relation& v,
                           const std::vector<Field>& schema, const einfold_options& o, Budget& budget);
 
+// The gradients of an attention-shaped pipeline's result (product scores,
+// weights exp(s - MAX(s)), normalised over the kept groups) with respect to
+// the factors of q, k and v, given d_out keyed as the result: per operand a
+// row per placed cell, its key columns and the gradient.
+struct GradientOutput {
+  std::vector<OutBatch> batches[3];
+  std::vector<Field> schemas[3];
+};
+GradientOutput pipeline_backward(Context& ctx, const PipelineD& p, const Relation& q, const Relation& k,
+                                 const Relation& v, const Relation& d_out, const einfold_options& o);
+
 }  // namespace ef

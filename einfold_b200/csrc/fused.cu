@@ -750,16 +750,46 @@ std::optional<uint64_t> size_of(const std::vector<int>& dims, const std::vector<
 
 }  // namespace
 
-FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, const Relation& k, const Relation& v,
-                          const std::vector<Field>& schema, const einfold_options& o, Budget& budget) {
-  (void)budget;  // the tile path asks no budget (fused.rs:151-489)
+// A pipeline's roles, mask and placed matrices (fused.rs:151-345, 624-664).
+struct PlacedPipeline {
+  std::vector<int> ws, xs, es, js, ys;  // xs and js lead with ws
+  Mask mask;
+  std::vector<std::pair<int, int>> read;  // the producer's columns, (operand, column)
+  std::vector<DeviceBuffer<double>> matrices;  // per read column, then the values
+  std::vector<int64_t> extent;
+  uint64_t nx = 0, ne = 0, nj = 0, ny = 0;
+  // Ragged groups (the reference declines them): per batch, the X and J
+  // positions present, as host vectors and device arrays; empty when every
+  // batch is complete.
+  std::vector<int64_t> xlen, jlen;
+  DeviceBuffer<int64_t> xlen_dev, jlen_dev;
+};
+
+// Rows of a placed matrix: 0 no cell held, 1 every cell, 2 some.
+__global__ void row_presence(const unsigned* __restrict__ held, int64_t rows, int64_t cols, uint8_t* __restrict__ state) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    int64_t n = 0;
+    for (int64_t c = r * cols; c < (r + 1) * cols; c++) n += (held[c >> 5] >> (c & 31)) & 1u;
+    state[r] = n == 0 ? 0 : (n == cols ? 1 : 2);
+  }
+}
+
+// The roles, conditions and placement of a pipeline. Where an operand
+// misses cells, its batches are taken as ragged groups when every batch's
+// present positions along X (for q) and J (for k and v, the same for both)
+// are a prefix 0 .. length - 1 with every cell of those rows present, and
+// `ragged_ok`; otherwise the pipeline declines, as the reference's
+// placement does for any missing cell.
+PlacedPipeline place_pipeline(Context& ctx, const PipelineD& p, const Relation& q, const Relation& k,
+                              const Relation& v, bool ragged_ok) {
   cudaStream_t s = ctx.stream;
+  PlacedPipeline P;
   const FoldD& pr = p.producer;
   if (pr.operands.size() != 2) decline("a pipeline's producer of other than two operands");
   const OperandD &op_q = pr.operands[0], &op_k = pr.operands[1], &values = p.values;
   const int own = pr.n_dims(), n = own + (int)p.equality.size();
   auto output = [&](int d) { return std::find(p.outputs.begin(), p.outputs.end(), d) != p.outputs.end(); };
-  std::vector<int> ws, xs, es, js;
+  std::vector<int>&ws = P.ws, &xs = P.xs, &es = P.es, &js = P.js, &ys = P.ys;
   for (int d = 0; d < own; d++) {
     const bool hq = op_q.holds(d), hk = op_k.holds(d), produced = pr.output_of(d) >= 0, out = output(d),
                hv = values.holds(d);
@@ -769,12 +799,11 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
     else if (!hq && hk && produced && !out && hv) js.push_back(d);
     else decline("a dimension of no pipeline role");
   }
-  std::vector<int> ys;
   for (int d = own; d < n; d++) {
     if (!output(d)) decline("a pipeline that sums its own dimension away");
     ys.push_back(d);
   }
-  Mask mask;
+  Mask& mask = P.mask;
   for (auto& c : pr.conditions) {
     if (xs.size() != 1 || js.size() != 1) decline("a condition without one X and one J dimension");
     ConditionD m;
@@ -796,7 +825,7 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
   js.insert(js.begin(), ws.begin(), ws.end());
 
   // The producer's columns: each operand's factor, or what its expression reads.
-  std::vector<std::pair<int, int>> read;
+  std::vector<std::pair<int, int>>& read = P.read;
   if (!pr.row_expr) {
     if (op_q.factor < 0 || op_k.factor < 0) decline("a product's operand without a factor");
     read = {{0, op_q.factor}, {1, op_k.factor}};
@@ -820,7 +849,8 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
   const Relation* rels[3] = {&q, &k, &v};
 
   // Keys and extents, each operand's staged once.
-  std::vector<int64_t> extent((size_t)n, 0);
+  std::vector<int64_t>& extent = P.extent;
+  extent.assign((size_t)n, 0);
   std::optional<StagedKeys> staged[3];
   for (auto& pl : placements) {
     if (staged[pl.operand]) continue;
@@ -832,13 +862,18 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
   auto nx_ = size_of(xs, extent), ne_ = size_of(es, extent), nj_ = size_of(js, extent), ny_ = size_of(ys, extent);
   auto lnx_ = size_of(local_xs, extent), lnj_ = size_of(local_js, extent);
   if (!nx_ || !ne_ || !nj_ || !ny_ || !lnx_ || !lnj_) decline("an extent product that overflows");
-  const uint64_t nx = *nx_, ne = *ne_, nj = *nj_, ny = *ny_;
+  P.nx = *nx_;
+  P.ne = *ne_;
+  P.nj = *nj_;
+  P.ny = *ny_;
   mask.lnx = (int64_t)std::max<uint64_t>(*lnx_, 1);
   mask.lnj = (int64_t)*lnj_;
   ctx.phase("fused: keys");
 
-  // Placement (fused.rs:624-664): exactly one non-NULL row per cell.
-  std::vector<DeviceBuffer<double>> matrices;
+  // Placement (fused.rs:624-664): exactly one non-NULL row per cell, or
+  // ragged groups.
+  bool ragged = false;
+  std::vector<std::vector<uint8_t>> presence;  // per placement: each row's state
   for (auto& pl : placements) {
     const Relation& r = *rels[pl.operand];
     const OperandD& op = *ops[pl.operand];
@@ -848,7 +883,9 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
     if (!checked_mul(*rows_n, *cols_n, &cells)) decline("an extent product that overflows");
     uint64_t total = 0;
     for (auto& b : r.batches) total += (uint64_t)b.rows;
-    if (total != cells || cells >= UINT32_MAX) decline("an operand without one row per cell");
+    if (cells >= UINT32_MAX || total > cells) decline("an operand without one row per cell");
+    const bool complete = total == cells;
+    if (!complete && !ragged_ok) decline("an operand without one row per cell");
     const Field& f = r.fields[pl.column];
     if (f.dictionary || f.kind != Kind::Float64) decline("a column that isn't DOUBLE");
     for (auto& b : r.batches)
@@ -859,10 +896,11 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
     DeviceBuffer<unsigned> dup(1, s);
     held.zero();
     dup.zero();
-    if (cells) {
+    if (!complete) mat.zero();  // missing cells (of ragged groups' padding) hold zeros
+    if (total) {
       const Role rr = role_of(*pl.rows, op, *staged[pl.operand], extent);
       const Role cr = role_of(*pl.cols, op, *staged[pl.operand], extent);
-      place_kernel<<<blocks_for((int64_t)cells, 256), 256, 0, s>>>(rr, cr, (int64_t)cells, (int64_t)*cols_n,
+      place_kernel<<<blocks_for((int64_t)total, 256), 256, 0, s>>>(rr, cr, (int64_t)total, (int64_t)*cols_n,
                                                                    (const double*)col.ptr(), mat.get(), held.get(),
                                                                    dup.get());
       ctx.kernels++;
@@ -872,11 +910,72 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
     EF_CUDA(cudaMemcpyAsync(&d, dup.get(), 4, cudaMemcpyDeviceToHost, s));
     EF_CUDA(cudaStreamSynchronize(s));
     if (d) decline("an operand with a repeated cell");
-    matrices.push_back(std::move(mat));
+    std::vector<uint8_t> state;
+    if (!complete) {
+      ragged = true;
+      DeviceBuffer<uint8_t> st((size_t)std::max<uint64_t>(*rows_n, 1), s);
+      row_presence<<<blocks_for(*rows_n, 256), 256, 0, s>>>(held.get(), (int64_t)*rows_n, (int64_t)*cols_n, st.get());
+      ctx.kernels++;
+      EF_LAUNCH_CHECK();
+      state.resize((size_t)*rows_n);
+      if (*rows_n) EF_CUDA(cudaMemcpyAsync(state.data(), st.get(), (size_t)*rows_n, cudaMemcpyDeviceToHost, s));
+      EF_CUDA(cudaStreamSynchronize(s));
+    }
+    presence.push_back(std::move(state));
+    P.matrices.push_back(std::move(mat));
   }
   uint64_t out_cells = 0;
-  if (!checked_mul(nx, ny, &out_cells) || out_cells >= UINT32_MAX) decline("an output of 2^32 cells or more");
+  if (!checked_mul(P.nx, P.ny, &out_cells) || out_cells >= UINT32_MAX) decline("an output of 2^32 cells or more");
+  if (ragged) {
+    // Ragged groups: per batch, a prefix of present rows along X (q's
+    // matrices) and along J (k's and v's, the same prefix).
+    if (pr.row_expr) decline("ragged groups with a row expression");
+    const int64_t W = mask.lnx > 0 ? (int64_t)P.nx / mask.lnx : 0;
+    if (W * mask.lnx != (int64_t)P.nx || W * mask.lnj != (int64_t)P.nj) decline("ragged groups that aren't batches");
+    auto lengths = [&](const std::vector<uint8_t>& st, int64_t per, std::vector<int64_t>& len) -> bool {
+      std::vector<int64_t> got((size_t)W, 0);
+      for (int64_t w = 0; w < W; w++) {
+        int64_t l = 0;
+        while (l < per && (st.empty() || st[(size_t)(w * per + l)] == 1)) l++;
+        for (int64_t r = l; r < per; r++)
+          if (!st.empty() && st[(size_t)(w * per + r)] != 0) return false;
+        got[(size_t)w] = l;
+      }
+      if (len.empty()) len = got;
+      return len == got;
+    };
+    for (size_t i = 0; i < placements.size(); i++) {
+      const bool along_x = placements[i].operand == 0;
+      if (!lengths(presence[i], along_x ? mask.lnx : mask.lnj, along_x ? P.xlen : P.jlen))
+        decline("an operand without one row per cell");
+    }
+    P.xlen_dev.allocate((size_t)std::max<int64_t>(W, 1), s);
+    P.jlen_dev.allocate((size_t)std::max<int64_t>(W, 1), s);
+    if (W) {
+      EF_CUDA(cudaMemcpyAsync(P.xlen_dev.get(), P.xlen.data(), (size_t)W * 8, cudaMemcpyHostToDevice, s));
+      EF_CUDA(cudaMemcpyAsync(P.jlen_dev.get(), P.jlen.data(), (size_t)W * 8, cudaMemcpyHostToDevice, s));
+    }
+    mask.xlen = P.xlen_dev.get();
+    mask.jlen = P.jlen_dev.get();
+  }
   ctx.phase("fused: place");
+  return P;
+}
+
+FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, const Relation& k, const Relation& v,
+                          const std::vector<Field>& schema, const einfold_options& o, Budget& budget) {
+  (void)budget;  // the tile path asks no budget (fused.rs:151-489)
+  cudaStream_t s = ctx.stream;
+  const FoldD& pr = p.producer;
+  PlacedPipeline P = place_pipeline(ctx, p, q, k, v, true);
+  const std::vector<int>&xs = P.xs, &ys = P.ys;
+  const std::vector<std::pair<int, int>>& read = P.read;
+  std::vector<DeviceBuffer<double>>& matrices = P.matrices;
+  const std::vector<int64_t>& extent = P.extent;
+  const uint64_t nx = P.nx, ne = P.ne, nj = P.nj, ny = P.ny;
+  const Mask mask = P.mask;
+  uint64_t out_cells = nx * ny;
+  (void)out_cells;
 
   DeviceBuffer<uint8_t> jflag((size_t)std::max<uint64_t>(nj, 1), s);
   DeviceBuffer<double> largest((size_t)std::max<uint64_t>(nj, 1), s), smallest((size_t)std::max<uint64_t>(nj, 1), s);
@@ -885,7 +984,7 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
   if (nj) {
     value_stats<<<blocks_for((int64_t)nj * 32, 256), 256, 0, s>>>((int64_t)nj, (int64_t)ny, matrices.back().get(),
                                                                   jflag.get(), largest.get(), smallest.get(),
-                                                                  nonfinite.get());
+                                                                  nonfinite.get(), mask.lnj, mask.jlen);
     ctx.kernels++;
     EF_LAUNCH_CHECK();
   }
@@ -985,6 +1084,8 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
     ap.largest = largest.get();
     ap.smallest = smallest.get();
     ap.out = out.get();
+    ap.xlen_host = P.xlen;
+    ap.jlen_host = P.jlen;
     const int slices = o.slices > 0 ? o.slices : 6;
     const AttentionOutcome r = attention_split(ctx, ap, slices, s);
     if (r == ATTENTION_GUARDED) decline("a sum that overflowed or may have underflowed");
@@ -1094,6 +1195,208 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
   result.tiles = tile_pairs;
   ctx.phase("fused: result");
   return result;
+}
+
+namespace {
+
+// Rows of a placed matrix that hold an operand's cells: all of them, or, in
+// ragged groups, row r of batch r / per when r % per < len[r / per].
+__global__ void length_flags(int64_t rows, int64_t per, const int64_t* __restrict__ len, uint8_t* __restrict__ flags) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x)
+    flags[r] = !len || r % per < len[r / per];
+}
+
+// One batch of rows from a placed matrix [rows][cols]: a row per cell of the
+// present rows, in order, with `op`'s key columns (as `fields` types them)
+// recomputed from the cell's position, then the cell's value.
+OutBatch emit_matrix(Context& ctx, const OperandD& op, const std::vector<Field>& fields,
+                     const std::vector<int>& row_dims, const std::vector<int>& col_dims,
+                     const std::vector<int64_t>& extent, const double* mat, int64_t rows, int64_t cols,
+                     int64_t per, const int64_t* len, bool on_device) {
+  cudaStream_t s = ctx.stream;
+  DeviceBuffer<uint8_t> flags((size_t)std::max<int64_t>(rows, 1), s);
+  DeviceBuffer<int64_t> row_index((size_t)std::max<int64_t>(rows, 1), s);
+  if (rows) {
+    length_flags<<<blocks_for((uint64_t)rows, 256), 256, 0, s>>>(rows, per, len, flags.get());
+    ctx.kernels++;
+    EF_LAUNCH_CHECK();
+  }
+  const int64_t n_rows = exclusive_scan_flags(ctx, flags.get(), rows, row_index.get());
+  const int64_t n_out = n_rows * cols;
+  if (op.keys.size() > (size_t)kMaxDims) decline("more than 8 keys");
+  OutKeys okeys;
+  for (auto& key : op.keys) {
+    const int d = key.dim;
+    const bool in_x = std::find(row_dims.begin(), row_dims.end(), d) != row_dims.end();
+    const std::vector<int>& role = in_x ? row_dims : col_dims;
+    const size_t slot = (size_t)(std::find(role.begin(), role.end(), d) - role.begin());
+    int64_t stride = 1;
+    for (size_t e = slot + 1; e < role.size(); e++) stride *= extent[role[e]];
+    okeys.key[okeys.n] = KeyAt{in_x ? 1 : 0, stride, std::max<int64_t>(extent[d], 1)};
+    okeys.width[okeys.n] = width_of(fields[key.col].kind);
+    okeys.n++;
+  }
+  DeviceBuffer<int64_t> xtab((size_t)std::max<int64_t>(okeys.n * rows, 1), s),
+      ytab((size_t)std::max<int64_t>(okeys.n * cols, 1), s);
+  if (rows) key_tables<<<blocks_for((uint64_t)rows, 256), 256, 0, s>>>(rows, okeys, 1, xtab.get());
+  if (cols) key_tables<<<blocks_for((uint64_t)cols, 256), 256, 0, s>>>(cols, okeys, 0, ytab.get());
+  ctx.kernels += 2;
+  std::vector<DeviceBuffer<uint8_t>> key_dev;
+  for (int i = 0; i < okeys.n; i++) {
+    key_dev.emplace_back((size_t)(n_out ? n_out * okeys.width[i] : 1), s);
+    okeys.out[i] = key_dev.back().get();
+  }
+  DeviceBuffer<double> vals((size_t)(n_out ? n_out : 1), s);
+  if (n_out) {
+    emit_rows<<<blocks_for((uint64_t)rows * cols, 256), 256, 0, s>>>(rows, cols, flags.get(), row_index.get(), okeys,
+                                                                      xtab.get(), ytab.get(), mat, vals.get());
+    ctx.kernels++;
+    EF_LAUNCH_CHECK();
+  }
+  OutBatch ob;
+  ob.rows = n_out;
+  for (int i = 0; i < okeys.n; i++) {
+    const Field& f = fields[op.keys[i].col];
+    OutColumn c;
+    c.format = f.format;
+    c.name = f.name;
+    c.kind = f.kind;
+    c.nullable = f.nullable;
+    c.length = n_out;
+    c.values = result_buffer(ctx, key_dev[i], (size_t)(n_out * okeys.width[i]), on_device);
+    ob.columns.push_back(std::move(c));
+  }
+  OutColumn val;
+  val.format = "g";
+  val.kind = Kind::Float64;
+  val.name = "grad";
+  val.nullable = true;
+  val.length = n_out;
+  val.values = result_buffer(ctx, vals, (size_t)n_out * 8, on_device);
+  ob.columns.push_back(std::move(val));
+  return ob;
+}
+
+}  // namespace
+
+std::vector<Field> gradient_schema(const OperandD& op, const std::vector<Field>& fields) {
+  std::vector<Field> out;
+  for (auto& key : op.keys) out.push_back(fields[key.col]);
+  Field g;
+  g.format = "g";
+  g.kind = Kind::Float64;
+  g.nullable = true;
+  g.name = "grad";
+  out.push_back(g);
+  return out;
+}
+
+GradientOutput pipeline_backward(Context& ctx, const PipelineD& p, const Relation& q, const Relation& k,
+                                 const Relation& v, const Relation& d_out, const einfold_options& o) {
+  cudaStream_t s = ctx.stream;
+  const FoldD& pr = p.producer;
+  if (pr.row_expr || p.weight_expr || p.shift != 1 || p.normalizer != 0 || p.scale_kind == 2)
+    decline("a backward pass only for product scores, exp(s - MAX(s)) weights, scaled by one or times c, "
+            "normalised over the kept groups");
+  PlacedPipeline P = place_pipeline(ctx, p, q, k, v, true);
+  const uint64_t nx = P.nx, ne = P.ne, nj = P.nj, ny = P.ny;
+  const int64_t W = P.mask.lnx > 0 ? (int64_t)nx / P.mask.lnx : 0;
+  if (W * P.mask.lnx != (int64_t)nx || W * P.mask.lnj != (int64_t)nj) decline("groups that aren't batches");
+  if (P.matrices.size() != 3) decline("a producer reading more than one column an operand");
+  // d_out: the result's keys (p.outputs, in order) and the gradient of each
+  // result row, placed as out is, [x][y]; rows of no d_out row have 0.
+  const int n_out_cols = (int)p.outputs.size();
+  if ((int)d_out.fields.size() != n_out_cols + 1) fail(EINFOLD_INVALID, "d_out needs the result's key columns and one gradient column");
+  const Field& gf = d_out.fields[(size_t)n_out_cols];
+  if (gf.dictionary || gf.kind != Kind::Float64) fail(EINFOLD_INVALID, "d_out's gradient column must be DOUBLE");
+  OperandD dop;
+  for (int i = 0; i < n_out_cols; i++) dop.keys.push_back(KeyD{p.outputs[(size_t)i], i});
+  dop.factor = n_out_cols;
+  StagedKeys dk = stage_keys(ctx, dop, d_out);
+  for (size_t i = 0; i < dop.keys.size(); i++)
+    if (dk.extent[i] > P.extent[(size_t)dop.keys[i].dim]) decline("a d_out row of no result row");
+  uint64_t cells = 0;
+  if (!checked_mul(nx, ny, &cells) || cells >= UINT32_MAX) decline("an output of 2^32 cells or more");
+  DeviceBuffer<double> g_out((size_t)std::max<uint64_t>(cells, 1), s);
+  g_out.zero();
+  {
+    int64_t rows = 0;
+    for (auto& b : d_out.batches) rows += b.rows;
+    for (auto& b : d_out.batches)
+      if (b.columns[(size_t)n_out_cols].nulls() > 0) decline("a NULL gradient");
+    DeviceColumn col = stage_column(ctx, d_out, n_out_cols, false);
+    DeviceBuffer<unsigned> held((size_t)std::max<uint64_t>((cells + 31) / 32, 1), s);
+    DeviceBuffer<unsigned> dup(1, s);
+    held.zero();
+    dup.zero();
+    if (rows) {
+      const Role rr = role_of(P.xs, dop, dk, P.extent);
+      const Role cr = role_of(P.ys, dop, dk, P.extent);
+      place_kernel<<<blocks_for((uint64_t)rows, 256), 256, 0, s>>>(rr, cr, rows, (int64_t)ny, (const double*)col.ptr(),
+                                                                   g_out.get(), held.get(), dup.get());
+      ctx.kernels++;
+      EF_LAUNCH_CHECK();
+    }
+    unsigned d = 0;
+    EF_CUDA(cudaMemcpyAsync(&d, dup.get(), 4, cudaMemcpyDeviceToHost, s));
+    EF_CUDA(cudaStreamSynchronize(s));
+    if (d) decline("d_out with a repeated row");
+  }
+  // The forward pass again, for out and the rows' log-sum-exp.
+  AttentionProblem ap;
+  ap.q = P.matrices[0].get();
+  ap.k = P.matrices[1].get();
+  ap.v = P.matrices[2].get();
+  ap.batches = W;
+  ap.lnx = P.mask.lnx;
+  ap.lnj = P.mask.lnj;
+  ap.ne = (int64_t)ne;
+  ap.ny = (int64_t)ny;
+  ap.mask = P.mask;
+  ap.scale_kind = p.scale_kind;
+  ap.scale_c = p.scale_c;
+  ap.xlen_host = P.xlen;
+  ap.jlen_host = P.jlen;
+  DeviceBuffer<double> out((size_t)std::max<uint64_t>(cells, 1), s), lse((size_t)std::max<uint64_t>(nx, 1), s);
+  out.zero();
+  lse.zero();
+  ap.out = out.get();
+  ap.lse = lse.get();
+  if (attention_forward(ctx, ap, o.precision, o.slices, s) == ATTENTION_GUARDED)
+    decline("a sum that overflowed or may have underflowed");
+  AttentionGradients g;
+  g.f = ap;
+  g.out = out.get();
+  g.lse = lse.get();
+  g.d_out = g_out.get();
+  DeviceBuffer<double> dq((size_t)std::max<uint64_t>(nx * ne, 1), s), dkm((size_t)std::max<uint64_t>(nj * ne, 1), s),
+      dv((size_t)std::max<uint64_t>(nj * ny, 1), s);
+  dq.zero();
+  dkm.zero();
+  dv.zero();
+  g.d_q = dq.get();
+  g.d_k = dkm.get();
+  g.d_v = dv.get();
+  attention_backward(ctx, g, o.precision, s);
+  ctx.phase("fused backward: gradients");
+  GradientOutput r;
+  const OperandD* ops[3] = {&pr.operands[0], &pr.operands[1], &p.values};
+  const Relation* rels[3] = {&q, &k, &v};
+  const double* mats[3] = {dq.get(), dkm.get(), dv.get()};
+  const std::vector<int>* rdims[3] = {&P.xs, &P.js, &P.js};
+  const std::vector<int>* cdims[3] = {&P.es, &P.es, &P.ys};
+  const uint64_t nrows[3] = {nx, nj, nj}, ncols[3] = {ne, ne, ny};
+  for (int i = 0; i < 3; i++) {
+    const bool along_x = i == 0;
+    const int64_t* len = P.xlen.empty() ? nullptr : (along_x ? P.xlen_dev.get() : P.jlen_dev.get());
+    r.schemas[i] = gradient_schema(*ops[i], rels[i]->fields);
+    r.batches[i].push_back(emit_matrix(ctx, *ops[i], rels[i]->fields, *rdims[i], *cdims[i], P.extent, mats[i],
+                                       (int64_t)nrows[i], (int64_t)ncols[i], along_x ? P.mask.lnx : P.mask.lnj, len,
+                                       o.result_on_device != 0));
+  }
+  EF_CUDA(cudaStreamSynchronize(s));
+  ctx.phase("fused backward: result");
+  return r;
 }
 
 AttentionOutcome attention_forward(Context& ctx, AttentionProblem p, int precision, int slices, cudaStream_t s) {

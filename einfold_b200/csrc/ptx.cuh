@@ -38,16 +38,21 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Waits for the phase of `parity` to complete, for at most kWaitNs; false if
-// the limit ran out. Patient waiters back off between polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, bool patient = false) {
+// Waits for the phase of `parity` to complete, for at most `limit_ns`; false
+// if the limit ran out. Patient waiters back off between polls.
+__device__ __forceinline__ bool mbar_wait_for(uint64_t* bar, uint32_t parity, uint64_t limit_ns, bool patient) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t start = now_ns();
   while (!mbar_try_wait(bar, parity)) {
-    if (now_ns() - start > kWaitNs) return false;
+    if (now_ns() - start > limit_ns) return false;
     if (patient) __nanosleep(128);
   }
   return true;
+}
+
+// The kernels' wait: at most kWaitNs.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, bool patient = false) {
+  return mbar_wait_for(bar, parity, kWaitNs, patient);
 }
 
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {

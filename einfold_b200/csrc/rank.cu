@@ -19,6 +19,8 @@
 // stable, so the result is the reference's bit for bit.
 #include <cub/cub.cuh>
 
+#include <cstdlib>
+
 #include "ptx.cuh"
 #include "rank.cuh"
 #include "stage.cuh"
@@ -238,6 +240,277 @@ __global__ void __launch_bounds__(kThreads) chunk_scatter(const uint64_t* __rest
   }
 }
 
+// ---- One-sweep passes --------------------------------------------------
+//
+// The histograms of every byte of the keys come from one read of them; each
+// pass is then one kernel. A block claims the next tile of keys from a
+// counter (so every earlier tile's block is already running), ranks its keys
+// among equal digits as the chunked downsweep does, publishes its per-digit
+// counts, and finds how many keys of each digit the earlier tiles hold by
+// looking back over their published counts (decoupled look-back): a tile
+// whose own offsets are known publishes them as inclusive prefixes, and a
+// look-back stops at the first prefix it meets. Waits are bounded. The
+// stable order, and so every rank, is the chunked passes' exactly.
+
+constexpr uint32_t kFlagAgg = 1u << 30, kFlagPre = 2u << 30, kValue = (1u << 30) - 1;
+
+__device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.volatile.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_volatile(uint32_t* p, uint32_t v) {
+  asm volatile("st.volatile.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Counts of every byte value at every byte position of the keys (word-major
+// W words), added into hist[8W][256] (zero on entry).
+template <int W>
+__global__ void __launch_bounds__(kThreads) byte_histograms(const uint64_t* __restrict__ keys, int64_t n, int64_t ld,
+                                                            unsigned long long* __restrict__ hist) {
+  __shared__ unsigned int h[8 * W][256];
+  for (int i = threadIdx.x; i < 8 * W * 256; i += kThreads) (&h[0][0])[i] = 0;
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+#pragma unroll
+    for (int w = 0; w < W; w++) {
+      const uint64_t k = __ldcs(&keys[(int64_t)w * ld + i]);
+#pragma unroll
+      for (int b = 0; b < 8; b++) atomicAdd(&h[8 * w + b][(k >> (8 * b)) & 255], 1u);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 8 * W * 256; i += kThreads) {
+    const unsigned int c = (&h[0][0])[i];
+    if (c) atomicAdd(&hist[i], (unsigned long long)c);
+  }
+}
+
+template <int W, int ITEMS>
+__global__ void __launch_bounds__(kThreads, 4) onesweep_pass(const uint64_t* __restrict__ kin,
+                                                          const uint32_t* __restrict__ vin,
+                                                          uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                          int64_t n, int64_t ldi, int64_t ldo, int word, int shift,
+                                                          const uint32_t* __restrict__ digit_start,
+                                                          uint32_t* __restrict__ status,
+                                                          unsigned int* __restrict__ tile_counter, int* err) {
+  constexpr int TILE = kThreads * ITEMS;
+  constexpr int WARPS = kThreads / 32;
+  static_assert(ITEMS <= 8, "a digit's counts of the warp's items fill one 64-bit word");
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint64_t* skeys = (uint64_t*)smem;                  // [W][TILE]
+  uint32_t* svals = (uint32_t*)(smem + TILE * 8 * W);  // [TILE]
+  __shared__ __align__(16) uint64_t counts[WARPS][256];
+  __shared__ long long dbase[256];
+  __shared__ unsigned int s_tile;
+  typedef cub::BlockScan<unsigned int, kThreads> Scan;
+  __shared__ typename Scan::TempStorage tmp;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
+#pragma unroll
+  for (int i = 0; i < 256 / 32; i++) counts[warp][i * 32 + lane] = 0;
+  __syncthreads();
+  const int64_t t = s_tile;
+  const int64_t base = t * TILE;
+  const int64_t count = min((int64_t)TILE, n - base);
+  const unsigned lt_mask = (1u << lane) - 1u;
+
+  uint64_t key[ITEMS][W];
+  uint32_t val[ITEMS];
+  int digit[ITEMS];
+  unsigned int local[ITEMS];
+#pragma unroll
+  for (int i = 0; i < ITEMS; i++) {
+    const int off = warp * 32 * ITEMS + i * 32 + lane;
+    if (off < count) {
+#pragma unroll
+      for (int w = 0; w < W; w++) key[i][w] = __ldcs(&kin[(int64_t)w * ldi + base + off]);
+      val[i] = vin ? __ldcs(&vin[base + off]) : (uint32_t)(base + off);
+      uint64_t wd = key[i][0];
+#pragma unroll
+      for (int w = 1; w < W; w++)
+        if (word == w) wd = key[i][w];
+      digit[i] = (int)((wd >> shift) & 255);
+    } else {
+      digit[i] = 256;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < ITEMS; i++) {
+    const int d = digit[i];
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const unsigned below = __popc(peers & lt_mask);
+    if (d < 256 && below == 0) ((uint8_t*)&counts[warp][d])[i] = (uint8_t)__popc(peers);
+    local[i] = below;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < ITEMS; i++) {
+    const int d = digit[i];
+    if (i > 0 && d < 256) {
+      const uint64_t c = counts[warp][d] & ((1ull << (8 * i)) - 1);  // items before i
+      local[i] += (unsigned)__dp4a((int)(uint32_t)c, 0x01010101, __dp4a((int)(uint32_t)(c >> 32), 0x01010101, 0));
+    }
+  }
+  __syncthreads();
+  unsigned int total = 0;
+#pragma unroll
+  for (int w = 0; w < WARPS; w++) {
+    const uint64_t c = counts[w][tid];
+    const unsigned cnt = (unsigned)__dp4a((int)(uint32_t)c, 0x01010101, __dp4a((int)(uint32_t)(c >> 32), 0x01010101, 0));
+    counts[w][tid] = total;
+    total += cnt;
+  }
+  // Publish this tile's count of digit `tid`, then look back for the
+  // earlier tiles' (thread tid owns digit tid).
+  uint32_t* my = status + t * 256 + tid;
+  if (t == 0) st_volatile(my, kFlagPre | total);
+  else st_volatile(my, kFlagAgg | total);
+  unsigned int ex;
+  Scan(tmp).ExclusiveSum(total, ex);
+  unsigned int before = 0;
+  if (t > 0) {
+    int64_t tt = t - 1;
+    uint64_t start = 0;
+    bool failed = false;
+    while (true) {
+      const uint32_t v = ld_volatile(status + tt * 256 + tid);
+      const uint32_t flag = v & ~kValue;
+      if (flag == 0) {
+        if (!start) start = ptx::now_ns();
+        else if (ptx::now_ns() - start > ptx::kWaitNs) {
+          failed = true;
+          break;
+        }
+        continue;
+      }
+      before += v & kValue;
+      if (flag == kFlagPre || tt == 0) break;
+      tt--;
+    }
+    if (failed) atomicOr(err, 1);
+    st_volatile(my, kFlagPre | (before + total));
+  }
+#pragma unroll
+  for (int w = 0; w < WARPS; w++) counts[w][tid] += ex;
+  dbase[tid] = (long long)digit_start[tid] + (long long)before - (long long)ex;
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < ITEMS; i++) {
+    const int d = digit[i];
+    if (d < 256) {
+      const unsigned pos = (unsigned)counts[warp][d] + local[i];
+#pragma unroll
+      for (int w = 0; w < W; w++) skeys[w * TILE + pos] = key[i][w];
+      svals[pos] = val[i];
+    }
+  }
+  __syncthreads();
+  for (int j = tid; j < count; j += kThreads) {
+    const uint64_t wd = skeys[word * TILE + j];
+    const int d = (int)((wd >> shift) & 255);
+    const long long dst = dbase[d] + j;
+#pragma unroll
+    for (int w = 0; w < W; w++) __stcs(&kout[(int64_t)w * ldo + dst], skeys[w * TILE + j]);
+    __stcs(&vout[dst], svals[j]);
+  }
+}
+
+// The ranks from the sorted pairs: a key heads its run when it differs from
+// the one before it; its run's rank is the number of heads before it. Tiles
+// are claimed in order and the heads counted before each tile come from a
+// look-back over the earlier tiles' counts, as in the passes. Each thread
+// takes ITEMS consecutive positions. rank[row] is written for every row and
+// first[r] by the head of run r; *distinct gets the number of runs.
+template <int W, int ITEMS>
+__global__ void __launch_bounds__(kThreads) rank_runs(const uint64_t* __restrict__ keys, int64_t ld,
+                                                      const uint32_t* __restrict__ rows, int64_t n,
+                                                      uint32_t* __restrict__ status,
+                                                      unsigned int* __restrict__ tile_counter,
+                                                      uint32_t* __restrict__ rank, uint32_t* __restrict__ first,
+                                                      unsigned long long* __restrict__ distinct, int* err) {
+  constexpr int TILE = kThreads * ITEMS;
+  typedef cub::BlockScan<unsigned int, kThreads> Scan;
+  __shared__ typename Scan::TempStorage tmp;
+  __shared__ unsigned int s_tile, s_before;
+  const int tid = threadIdx.x;
+  if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
+  __syncthreads();
+  const int64_t t = s_tile;
+  const int64_t p0 = t * TILE + (int64_t)tid * ITEMS;
+  unsigned int heads = 0;
+  unsigned int hmask = 0;
+  uint32_t r[ITEMS];
+  {
+    uint64_t prev[W];
+#pragma unroll
+    for (int w = 0; w < W; w++) prev[w] = p0 > 0 && p0 - 1 < n ? keys[(int64_t)w * ld + p0 - 1] : 0;
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+      const int64_t p = p0 + i;
+      if (p < n) {
+        bool h = p == 0;
+#pragma unroll
+        for (int w = 0; w < W; w++) {
+          const uint64_t k = keys[(int64_t)w * ld + p];
+          h |= k != prev[w];
+          prev[w] = k;
+        }
+        r[i] = rows[p];
+        if (h) {
+          hmask |= 1u << i;
+          heads++;
+        }
+      }
+    }
+  }
+  unsigned int ex, total;
+  Scan(tmp).ExclusiveSum(heads, ex, total);
+  if (tid == 0) {
+    uint32_t* my = status + t;
+    unsigned int before = 0;
+    if (t == 0) {
+      st_volatile(my, kFlagPre | total);
+    } else {
+      st_volatile(my, kFlagAgg | total);
+      int64_t tt = t - 1;
+      uint64_t start = 0;
+      while (true) {
+        const uint32_t v = ld_volatile(status + tt);
+        const uint32_t flag = v & ~kValue;
+        if (flag == 0) {
+          if (!start) start = ptx::now_ns();
+          else if (ptx::now_ns() - start > ptx::kWaitNs) {
+            atomicOr(err, 1);
+            break;
+          }
+          continue;
+        }
+        before += v & kValue;
+        if (flag == kFlagPre || tt == 0) break;
+        tt--;
+      }
+      st_volatile(my, kFlagPre | (before + total));
+    }
+    s_before = before;
+    if ((t + 1) * TILE >= n) *distinct = (unsigned long long)(before + total);
+  }
+  __syncthreads();
+  unsigned int cur = s_before + ex;
+#pragma unroll
+  for (int i = 0; i < ITEMS; i++) {
+    const int64_t p = p0 + i;
+    if (p < n) {
+      if (hmask >> i & 1u) {
+        first[cur] = r[i];
+        cur++;
+      }
+      rank[r[i]] = cur - 1;
+    }
+  }
+}
+
 template <int W>
 __global__ void head_flags(const uint64_t* __restrict__ keys, int64_t n, int64_t ld, uint8_t* __restrict__ head) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -288,6 +561,103 @@ void radix_pass(Context& ctx, const uint64_t* kin, int64_t ldi, const uint32_t* 
                                                                    chunk, (int)chunks, offsets.get(), err);
   EF_LAUNCH_CHECK();
   ctx.kernels += 3;
+}
+
+// The one-sweep ranking (n < 2^30, so that a status word holds a count
+// and its flag): one read of the keys for every byte's histogram, one kernel
+// per pass over the bytes that vary, and one for the ranks.
+template <int W>
+int64_t rank_keys_onesweep(Context& ctx, const uint64_t* keys, int64_t n, int64_t ld, uint32_t* rank,
+                           uint32_t* first, cudaStream_t s, uint32_t* sorted_rows) {
+  constexpr int ITEMS = W == 1 ? 8 : (W == 2 ? 6 : 4);
+  constexpr int TILE = kThreads * ITEMS;
+  constexpr int RITEMS = 8;
+  constexpr int RTILE = kThreads * RITEMS;
+  const int64_t tiles = (n + TILE - 1) / TILE;
+  const int64_t rtiles = (n + RTILE - 1) / RTILE;
+  DeviceBuffer<unsigned long long> hist((size_t)(8 * W * 256), s);
+  hist.zero();
+  byte_histograms<W><<<blocks_for((uint64_t)n, kThreads, (unsigned)ctx.sm_count * 8u), kThreads, 0, s>>>(keys, n, ld,
+                                                                                                       hist.get());
+  ctx.kernels++;
+  EF_LAUNCH_CHECK();
+  std::vector<unsigned long long> h((size_t)(8 * W * 256));
+  EF_CUDA(cudaMemcpyAsync(h.data(), hist.get(), h.size() * 8, cudaMemcpyDeviceToHost, s));
+  EF_CUDA(cudaStreamSynchronize(s));
+  // Passes: the least significant byte of the last word first; a byte whose
+  // values are all one (a bin holds every key) is skipped.
+  std::vector<int> pw, ps;
+  std::vector<uint32_t> starts;
+  for (int w = W - 1; w >= 0; w--)
+    for (int b = 0; b < 8; b++) {
+      const unsigned long long* c = &h[(size_t)(8 * w + b) * 256];
+      bool varies = true;
+      for (int d = 0; d < 256; d++)
+        if (c[d] == (unsigned long long)n) varies = false;
+      if (!varies) continue;
+      pw.push_back(w);
+      ps.push_back(8 * b);
+      uint32_t acc = 0;
+      for (int d = 0; d < 256; d++) {
+        starts.push_back(acc);
+        acc += (uint32_t)c[d];
+      }
+    }
+  const int passes = (int)pw.size();
+  DeviceBuffer<uint32_t> dstart((size_t)std::max(1, passes) * 256, s);
+  if (passes) EF_CUDA(cudaMemcpyAsync(dstart.get(), starts.data(), starts.size() * 4, cudaMemcpyHostToDevice, s));
+  const int64_t status_words = std::max(tiles * 256, rtiles);
+  DeviceBuffer<uint32_t> status((size_t)status_words, s);
+  DeviceBuffer<unsigned int> counters((size_t)passes + 1, s);
+  counters.zero();
+  DeviceBuffer<int> err(1, s);
+  err.zero();
+  DeviceBuffer<uint64_t> kb[2];
+  DeviceBuffer<uint32_t> vb[2];
+  const uint64_t* cur_k = keys;
+  int64_t cur_ld = ld;
+  const uint32_t* cur_v = nullptr;
+  const size_t smem = (size_t)TILE * (8 * W + 4);
+  if (passes) {
+    const int64_t ldb = (n + 1) & ~(int64_t)1;
+    for (int b = 0; b < 2; b++) {
+      kb[b].allocate((size_t)(W * ldb), s);
+      vb[b].allocate((size_t)n, s);
+    }
+    EF_CUDA(cudaFuncSetAttribute(onesweep_pass<W, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    for (int p = 0; p < passes; p++) {
+      EF_CUDA(cudaMemsetAsync(status.get(), 0, (size_t)tiles * 256 * 4, s));
+      onesweep_pass<W, ITEMS><<<(unsigned)tiles, kThreads, smem, s>>>(
+          cur_k, cur_v, kb[p & 1].get(), vb[p & 1].get(), n, cur_ld, ldb, pw[p], ps[p], dstart.get() + p * 256,
+          status.get(), counters.get() + p, err.get());
+      ctx.kernels++;
+      cur_k = kb[p & 1].get();
+      cur_ld = ldb;
+      cur_v = vb[p & 1].get();
+    }
+    EF_LAUNCH_CHECK();
+  }
+  DeviceBuffer<uint32_t> identity;
+  if (!cur_v) {
+    identity.allocate((size_t)n, s);
+    thrust_iota(ctx, identity.get(), n, s);
+    cur_v = identity.get();
+  }
+  DeviceBuffer<unsigned long long> distinct(1, s);
+  EF_CUDA(cudaMemsetAsync(status.get(), 0, (size_t)rtiles * 4, s));
+  rank_runs<W, RITEMS><<<(unsigned)rtiles, kThreads, 0, s>>>(cur_k, cur_ld, cur_v, n, status.get(),
+                                                             counters.get() + passes, rank, first, distinct.get(),
+                                                             err.get());
+  ctx.kernels++;
+  EF_LAUNCH_CHECK();
+  if (sorted_rows) EF_CUDA(cudaMemcpyAsync(sorted_rows, cur_v, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+  unsigned long long k = 0;
+  int e = 0;
+  EF_CUDA(cudaMemcpyAsync(&k, distinct.get(), 8, cudaMemcpyDeviceToHost, s));
+  EF_CUDA(cudaMemcpyAsync(&e, err.get(), 4, cudaMemcpyDeviceToHost, s));
+  EF_CUDA(cudaStreamSynchronize(s));
+  if (e) fail(EINFOLD_TIMEOUT, "a bounded wait in the radix sort ran out");
+  return (int64_t)k;
 }
 
 template <int W>
@@ -383,6 +753,19 @@ void thrust_iota(Context& ctx, uint32_t* out, int64_t n, cudaStream_t s) {
 
 int64_t rank_keys(Context& ctx, const uint64_t* keys, int words, int64_t n, int64_t ld, uint32_t* rank,
                   uint32_t* first, cudaStream_t s, uint32_t* sorted_rows) {
+  if (n <= 0) return 0;
+  // The one-sweep passes below 2^30 keys (a status word's count); the
+  // chunked passes beyond, or when EINFOLD_RANK_CHUNKED is set.
+  static const bool chunked = std::getenv("EINFOLD_RANK_CHUNKED") != nullptr;
+  if (n < ((int64_t)1 << 30) && !chunked) {
+    switch (words) {
+      case 1: return rank_keys_onesweep<1>(ctx, keys, n, ld, rank, first, s, sorted_rows);
+      case 2: return rank_keys_onesweep<2>(ctx, keys, n, ld, rank, first, s, sorted_rows);
+      case 3: return rank_keys_onesweep<3>(ctx, keys, n, ld, rank, first, s, sorted_rows);
+      case 4: return rank_keys_onesweep<4>(ctx, keys, n, ld, rank, first, s, sorted_rows);
+      default: fail(EINFOLD_INVALID, "keys of %d words", words);
+    }
+  }
   switch (words) {
     case 1: return rank_keys_w<1>(ctx, keys, n, ld, rank, first, s, sorted_rows);
     case 2: return rank_keys_w<2>(ctx, keys, n, ld, rank, first, s, sorted_rows);

@@ -516,6 +516,40 @@ def pipeline(p: ir.Pipeline, operands: Sequence, schema: Optional[pa.Schema] = N
         keep.release()
 
 
+def pipeline_backward(p: ir.Pipeline, operands: Sequence, d_out: Relation,
+                      options: Optional[Options] = None) -> Optional[List[List[pa.RecordBatch]]]:
+    """The gradients of ``pipeline``'s result with respect to q's, k's and v's
+    factors (``einfold_pipeline_backward``): ``d_out`` holds the result's key
+    columns and a DOUBLE gradient per result row; returns, per operand, its
+    key columns and a ``grad`` column, a row per placed cell; None where the
+    pipeline isn't attention-shaped."""
+    options = options or Options()
+    _after_torch(*operands, d_out)
+    keep = _Keep()
+    lib = _lib.load()
+    try:
+        rels = keep.add(_array(_lib.Relation, [_relation(r, keep) for r in operands]))
+        results = (_lib.Result * 3)()
+        status = lib.einfold_pipeline_backward(_lib.context(options.device), ctypes.byref(_pipeline_desc(p, keep)),
+                                               rels, ctypes.byref(_relation(d_out, keep)),
+                                               ctypes.byref(_options(options, keep)), results)
+        msg = results[0].message.decode(errors="replace")
+        last_call.kernels_launched = results[0].kernels_launched
+        last_call.device_ms = results[0].device_ms
+        last_call.product_ms = results[0].product_ms
+        last_call.product_ops = results[0].product_ops
+        last_call.message = msg
+        if status == _lib.DECLINED:
+            return None
+        if status != _lib.OK:
+            _raise(status, msg)
+        if options.result_on_device:
+            return [_device_batches(results[i]) for i in range(3)]
+        return [_collect(results[i]) for i in range(3)]
+    finally:
+        keep.release()
+
+
 @dataclass
 class Ranks:
     """Each row's rank among the distinct keys, and the first row of each rank."""

@@ -243,10 +243,34 @@ int32_t einfold_fold_dense(einfold_context* ctx, const einfold_fold_desc* fold, 
 /* einfold_kernels::fold_chain over three operands. */
 int32_t einfold_fold_chain(einfold_context* ctx, const einfold_fold_desc* fold, const einfold_relation* operands,
                            const einfold_options* options, einfold_result* result);
-/* einfold_kernels::pipeline over q, k and v. */
+/* einfold_kernels::pipeline over q, k and v. Where the reference's
+ * placement declines an operand that misses cells (fused.rs:624-664), this
+ * accepts ragged groups: every batch (the W dimensions) with its rows
+ * present from position 0 to a length of its own along X (q) and along J
+ * (k and v, the same length for both), each such row complete, and nothing
+ * after; the rows past a batch's length join nothing and give no result
+ * rows. Other missing cells decline, as the reference's placement does. */
 int32_t einfold_pipeline(einfold_context* ctx, const einfold_pipeline_desc* pipeline,
                          const einfold_relation* operands, const einfold_options* options,
                          einfold_result* result);
+/* The gradients of einfold_pipeline's result with respect to q's, k's and
+ * v's factor columns, for the attention-shaped pipelines (product scores,
+ * Weight::Exp{One or Times(c), KeptMaximum}, normalised over the kept
+ * groups; others return EINFOLD_DECLINED). The reference has no backward
+ * pass for its fused pipeline (docs/design.md:612); its gradients are
+ * gradient SQL the host plan runs, which this computes in one call:
+ * d_out holds the result's key columns (the pipeline's outputs, in order)
+ * and a DOUBLE gradient per result row (a result row with no d_out row has
+ * gradient 0). The forward pass is recomputed for its log-sum-exp, then the
+ * backward kernels run (scores recomputed tile by tile from it). results
+ * points at three results, d_q, d_k and d_v: a row per placed cell of the
+ * operand (ragged groups: the cells present), its key columns as the
+ * operand types them and a DOUBLE column "grad", rows in key order. Ragged
+ * groups (each batch's rows present from position 0 to its length along X
+ * for q, along J for k and v) are accepted, as by einfold_pipeline. */
+int32_t einfold_pipeline_backward(einfold_context* ctx, const einfold_pipeline_desc* pipeline,
+                                  const einfold_relation* operands, const einfold_relation* d_out,
+                                  const einfold_options* options, einfold_result* results);
 /* einfold_kernels::schema: the result schema of a fold over `operands`
  * (2 or 3) and an optional domain. On success *out is owned by the caller. */
 int32_t einfold_schema(const einfold_fold_desc* fold, const struct ArrowSchema* const* operands,
@@ -377,6 +401,24 @@ int32_t einfold_attention_backward_ragged(einfold_context* ctx, const double* q,
                                           int64_t d, int64_t dv, const int64_t* q_lengths, const int64_t* k_lengths,
                                           int32_t n_conditions, const int32_t* comparisons, const int64_t* offsets,
                                           double scale, int32_t precision, void* stream, einfold_result* info);
+
+/* ---- Device self-checks (no counterpart in the reference: they check two
+ * mechanisms the kernels rely on, for a caller's health check and the tests) ---- */
+
+/* One block waits on an mbarrier that nothing arrives on, with the bounded
+ * wait every kernel's mbarrier waits use, for at most limit_ns (at most the
+ * kernels' own 2 s): the wait runs out, the block records it in a status
+ * word and returns, and the call returns EINFOLD_TIMEOUT, as a call whose
+ * kernel's wait ran out does; the context stays usable. *waited_ns (may be
+ * NULL) gets how long the wait took. */
+int32_t einfold_check_wait(einfold_context* ctx, uint64_t limit_ns, uint64_t* waited_ns);
+
+/* y[i] = exp(x[i]) as the softmax weights compute it (Tang's table-driven
+ * method), for shift < 0; for 0 <= shift <= 64, 2^shift·exp(x[i]) with x
+ * clamped to [-708, 709], the weights' form. Device arrays; returns once
+ * done. */
+int32_t einfold_exp_weights(einfold_context* ctx, const double* x, double* y, int64_t n, int32_t shift,
+                            void* stream);
 
 #ifdef __cplusplus
 }

@@ -86,3 +86,18 @@ def test_more_than_4m_rows():
     pool = rng.u64s(n // 2)
     words = pool[(rng.u64s(n) % np.uint64(len(pool))).astype(np.int64)]
     _check(words)
+
+
+@pytest.mark.parametrize("order", ["ascending", "descending", "three_values"])
+def test_ordered_and_heavily_repeated_keys(order):
+    # Every tile of a pass holding one digit only, or the same few: the
+    # look-back across tiles carries whole runs.
+    n = 3_000_017
+    rng = oracle.Rng.seeded(10, 5)
+    if order == "three_values":
+        words = np.array([7, 1 << 40, (1 << 63) + 5], dtype=np.uint64)[(rng.u64s(n) % np.uint64(3)).astype(np.int64)]
+    else:
+        words = np.sort(rng.u64s(n))
+        if order == "descending":
+            words = words[::-1].copy()
+    _check(words)
