@@ -115,6 +115,19 @@ class Result(ctypes.Structure):
                 ("message", ctypes.c_char * 480)]
 
 
+
+class DenseShape(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("pad", ctypes.c_int32), ("batches", ctypes.c_int64),
+                ("rows", ctypes.c_int64), ("inner", ctypes.c_int64), ("columns", ctypes.c_int64),
+                ("keys", ctypes.c_int64)]
+
+
+class DenseWork(ctypes.Structure):
+    _fields_ = [("shape", DenseShape), ("a", ctypes.c_void_p), ("b", ctypes.c_void_p), ("q", ctypes.c_void_p),
+                ("kt", ctypes.c_void_p), ("v", ctypes.c_void_p), ("scale_kind", ctypes.c_int32),
+                ("precision", ctypes.c_int32), ("scale_c", ctypes.c_double), ("allowed", ctypes.c_void_p),
+                ("device", ctypes.c_int32), ("pad2", ctypes.c_int32)]
+
 # Every symbol the header declares, with its signature.
 SIGNATURES = {
     "einfold_context_create": (ctypes.c_void_p, [ctypes.c_int32]),
@@ -149,6 +162,9 @@ SIGNATURES = {
     "einfold_check_wait": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
     "einfold_exp_weights": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                              ctypes.c_int32, ctypes.c_void_p]),
+    "einfold_backend_may_run": (ctypes.c_int32, [ctypes.POINTER(DenseShape)]),
+    "einfold_backend_run": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(DenseWork), ctypes.c_void_p,
+                                             ctypes.POINTER(Result)]),
     "einfold_split_gemm": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                             ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                             ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),

@@ -336,6 +336,97 @@ int32_t einfold_fp64_gemm(einfold_context* ctx, const double* a, const double* b
   });
 }
 
+int32_t einfold_backend_may_run(const einfold_dense_shape* shape) {
+  if (!shape) return 0;
+  if (shape->batches < 0 || shape->rows < 0 || shape->inner < 0 || shape->columns < 0) return 0;
+  if (shape->kind == 0) return 1;
+  if (shape->kind == 1) return shape->keys >= 0 ? 1 : 0;
+  return 0;
+}
+
+int32_t einfold_backend_run(einfold_context* ctx, const einfold_dense_work* work, double* result,
+                            einfold_result* info) {
+  einfold_result local;
+  einfold_result* r = info ? info : &local;
+  const int32_t st = guarded(ctx, r, [&](ef::Context& c) -> int32_t {
+    if (!work || !result) ef::fail(EINFOLD_INVALID, "no work or no result");
+    const einfold_dense_shape& sh = work->shape;
+    if (!einfold_backend_may_run(&sh)) ef::decline("a kind of work this backend doesn't know");
+    cudaStream_t s = c.stream;
+    const bool host = work->device < 0;
+    if (!host && work->device != c.device)
+      ef::fail(EINFOLD_INVALID, "operands on device %d, the context on %d", work->device, c.device);
+    const int64_t W = sh.batches;
+    // Device copies of host operands (none for operands already in HBM).
+    std::vector<ef::DeviceBuffer<double>> keep;
+    keep.reserve(3);
+    auto on_device = [&](const double* p, int64_t n) -> const double* {
+      if (!host || n == 0) return p;
+      keep.emplace_back((size_t)n, s);
+      EF_CUDA(cudaMemcpyAsync(keep.back().get(), p, (size_t)n * 8, cudaMemcpyHostToDevice, s));
+      return keep.back().get();
+    };
+    ef::DeviceBuffer<double> out;
+    if (sh.kind == 0) {
+      const int64_t x = sh.rows, z = sh.inner, y = sh.columns;
+      const double* a = on_device(work->a, W * x * z);
+      const double* b = on_device(work->b, W * z * y);
+      double* o = result;
+      if (host) {
+        out.allocate((size_t)std::max<int64_t>(W * x * y, 1), s);
+        o = out.get();
+      }
+      if (W * x * y > 0) {
+        if (z == 0) EF_CUDA(cudaMemsetAsync(o, 0, (size_t)(W * x * y) * 8, s));
+        else if (work->precision == 1) ef::fp64_gemm(c, a, nullptr, b, o, W, x, y, z, 0, 0, false, s);
+        else ef::split_gemm(c, a, b, true, o, W, x, y, z, ef::kDefaultSlices, s);
+        if (host) EF_CUDA(cudaMemcpyAsync(result, o, (size_t)(W * x * y) * 8, cudaMemcpyDeviceToHost, s));
+      }
+      EF_CUDA(cudaStreamSynchronize(s));
+      return EINFOLD_OK;
+    }
+    // Attention.
+    const int64_t x = sh.rows, e = sh.inner, y = sh.columns, j = sh.keys;
+    if (!work->allowed && x > 0) ef::fail(EINFOLD_INVALID, "attention without its ranges");
+    if (work->scale_kind < 0 || work->scale_kind > 2) ef::fail(EINFOLD_INVALID, "a scale of kind %d", work->scale_kind);
+    ef::Mask mask;
+    if (!ef::ranges_as_mask(work->allowed, x, j, mask)) ef::decline("ranges that no conditions give");
+    const double* q = on_device(work->q, W * x * e);
+    const double* kt = on_device(work->kt, W * e * j);
+    const double* v = on_device(work->v, W * j * y);
+    ef::DeviceBuffer<double> k((size_t)std::max<int64_t>(W * j * e, 1), s);
+    if (W * j * e > 0) ef::transpose(kt, k.get(), W, e, j, s);
+    double* o = result;
+    if (host) {
+      out.allocate((size_t)std::max<int64_t>(W * x * y, 1), s);
+      o = out.get();
+    }
+    if (W * x * y > 0) EF_CUDA(cudaMemsetAsync(o, 0, (size_t)(W * x * y) * 8, s));
+    ef::AttentionProblem p;
+    p.q = q;
+    p.k = k.get();
+    p.v = v;
+    p.out = o;
+    p.batches = W;
+    p.lnx = x;
+    p.lnj = j;
+    p.ne = e;
+    p.ny = y;
+    p.mask = mask;
+    p.scale_kind = work->scale_kind;
+    p.scale_c = work->scale_c;
+    if (W > 0 && x > 0 && y > 0 && j > 0 && e > 0) {
+      if (ef::attention_forward(c, p, work->precision, 0, s) == ef::ATTENTION_GUARDED)
+        ef::decline("a sum that overflowed or may have underflowed");
+    }
+    if (host && W * x * y > 0) EF_CUDA(cudaMemcpyAsync(result, o, (size_t)(W * x * y) * 8, cudaMemcpyDeviceToHost, s));
+    EF_CUDA(cudaStreamSynchronize(s));
+    return EINFOLD_OK;
+  });
+  if (st != EINFOLD_OK) g_last_error = r->message;
+  return st;
+}
+
 static ef::AttentionProblem attention_problem(const double* q, const double* k, const double* v, double* out,
                                               double* lse, int64_t batches, int64_t lq, int64_t lk, int64_t d,
                                               int64_t dv, int32_t n_conditions, const int32_t* comparisons,

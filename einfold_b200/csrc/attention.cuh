@@ -56,6 +56,11 @@ __host__ __device__ inline void allowed(const Mask& m, int64_t x, int64_t& lo_ou
   hi_out = group_start + (int64_t)h;
 }
 
+// Per-query key ranges [lo, hi) (2·queries values, the same in every batch)
+// as conditions: true when every range is [x + a, x + b) clamped to
+// [0, keys) for constants a and b, as a pipeline's conditions give.
+bool ranges_as_mask(const int64_t* ranges, int64_t queries, int64_t keys, Mask& m);
+
 // A softmax-weighted average over placed matrices, batch by batch:
 // q [w][x][e], k [w][j][e], v [w][j][y] for w < batches, x < lnx, j < lnj,
 // e < ne, y < ny; out [w·lnx + x][y] = Σ_j exp(s_xj − m_x) v_jy / z_x over the

@@ -335,6 +335,51 @@ int32_t einfold_split_gemm_static(const double* a, const double* b, double* c, i
                                   int64_t n, int64_t k, int32_t b_transposed, int32_t slices, void* stream,
                                   char* message, int32_t message_len);
 
+/* ---- A dense backend (DenseBackend, crates/einfold-kernels/src/backend.rs:124-143) ----
+ * The two calls a Rust DenseBackend implementation forwards: may_run with a
+ * work's kind and shape before einfold packs its operands, run with the
+ * packed operands (DenseWork, backend.rs:46-96), which einfold has checked
+ * (keys in range, no duplicates, no NULLs, every factor finite). Operands
+ * are row-major, batch first, in host memory (device = -1, as the trait
+ * hands them; copied over and the result back) or already in the memory
+ * of CUDA device `device` (result there too). */
+typedef struct {
+  int32_t kind;    /* 0 DenseShape::Product, 1 DenseShape::Attention */
+  int32_t pad;
+  int64_t batches; /* w */
+  int64_t rows;    /* product: x, the rows of a and of the result; attention: queries x */
+  int64_t inner;   /* product: z, the summed dimension; attention: features e */
+  int64_t columns; /* product: y; attention: value columns y */
+  int64_t keys;    /* attention: key positions j */
+} einfold_dense_shape;
+typedef struct {
+  einfold_dense_shape shape;
+  const double* a;        /* product: a [w][x][z] */
+  const double* b;        /* product: b [w][z][y] */
+  const double* q;        /* attention: q [w][x][e] */
+  const double* kt;       /* attention: the keys transposed, kt [w][e][j] */
+  const double* v;        /* attention: v [w][j][y] */
+  int32_t scale_kind;     /* attention: 0 One, 1 Times(c), 2 Over(c) */
+  int32_t precision;      /* 0 split (int8 slices, exact sums, FP64 combine), 1 FP64 */
+  double scale_c;
+  const int64_t* allowed; /* attention: per query x, the keys [lo, hi) it joins, the same in every
+                           * batch (2·queries values, host memory) */
+  int32_t device;         /* -1 host memory; d >= 0 CUDA device d's memory */
+  int32_t pad2;
+} einfold_dense_work;
+
+/* Whether run may take work of this shape (DenseBackend::may_run): 1 for
+ * products and attention of non-negative extents, 0 otherwise. */
+int32_t einfold_backend_may_run(const einfold_dense_shape* shape);
+/* DenseBackend::run: writes the result [w][x][y] (row-major, batch first;
+ * attention rows with no keys are 0) and returns EINFOLD_OK, or
+ * EINFOLD_DECLINED (Ok(None): einfold computes the work itself) for a kind
+ * it doesn't know, attention ranges that aren't [x + a, x + b) clamped to
+ * the keys (the ranges einfold's conditions give), or attention whose sums
+ * the reference's guards would refuse. */
+int32_t einfold_backend_run(einfold_context* ctx, const einfold_dense_work* work, double* result,
+                            einfold_result* info);
+
 /* ---- Attention over device arrays ----
  * The pipeline einfold_pipeline runs for product scores, weights
  * exp(s - MAX(s)) over the kept groups and an average normalised by their

@@ -1,5 +1,6 @@
 """The C ABI library loads, exports what the header declares, and computes
 schemas on the host (no GPU needed)."""
+import ctypes
 import os
 
 import pyarrow as pa
@@ -85,6 +86,7 @@ _MIRRORS = {
     "einfold_expression": "Expression", "einfold_fold_desc": "FoldDesc", "einfold_pipeline_desc": "PipelineDesc",
     "einfold_relation": "Relation", "einfold_options": "Options", "einfold_result": "Result",
     "struct ArrowSchema": "ArrowSchema", "struct ArrowArray": "ArrowArray",
+    "einfold_dense_shape": "DenseShape", "einfold_dense_work": "DenseWork",
 }
 
 
@@ -144,3 +146,14 @@ def test_small_fold_tables_have_the_stated_shape():
         n_null = tb.column(2).null_count
         assert (0.008 * tb.num_rows < n_null < 0.012 * tb.num_rows) if nulls else n_null == 0
         assert ta.column(2).null_count == 0
+
+
+def test_backend_may_run_takes_products_and_attention_only():
+    # DenseBackend::may_run (backend.rs:124-132): the kinds this backend
+    # knows, with non-negative extents; no device is touched.
+    lib = _lib.load()
+    for kind, want in ((0, 1), (1, 1), (2, 0), (-1, 0)):
+        shape = _lib.DenseShape(kind, 0, 2, 3, 4, 5, 6)
+        assert lib.einfold_backend_may_run(ctypes.byref(shape)) == want
+    assert lib.einfold_backend_may_run(ctypes.byref(_lib.DenseShape(0, 0, 1, -1, 4, 5, 0))) == 0
+    assert lib.einfold_backend_may_run(None) == 0
