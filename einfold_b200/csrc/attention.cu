@@ -533,54 +533,6 @@ __global__ void __launch_bounds__(kAttnThreads, 1)
   }
 }
 
-// Each row's largest and smallest nonzero value magnitude over its allowed
-// keys (the bounds of Bounds::hold), from blocks of 64 keys' extrema.
-__global__ void block_extrema(int64_t nj, const double* __restrict__ largest, const double* __restrict__ smallest,
-                              double* __restrict__ bmax, double* __restrict__ bmin) {
-  const int lane = threadIdx.x & 31;
-  for (int64_t b = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b * 64 < nj;
-       b += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-    double mx = 0.0, mn = INFINITY;
-    for (int64_t j = b * 64 + lane; j < min(nj, b * 64 + 64); j += 32) {
-      mx = fmax(mx, largest[j]);
-      mn = fmin(mn, smallest[j]);
-    }
-    for (int o = 16; o; o >>= 1) {
-      mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-      mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-    }
-    if (lane == 0) {
-      bmax[b] = mx;
-      bmin[b] = mn;
-    }
-  }
-}
-
-__global__ void row_value_bounds(int64_t nx, Mask m, const double* __restrict__ largest,
-                                 const double* __restrict__ smallest, const double* __restrict__ bmax,
-                                 const double* __restrict__ bmin, double* __restrict__ rl, double* __restrict__ rs) {
-  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < nx; x += (int64_t)gridDim.x * blockDim.x) {
-    int64_t lo, hi;
-    allowed(m, x, lo, hi);
-    double mx = 0.0, mn = INFINITY;
-    int64_t j = lo;
-    for (; j < hi && (j & 63); j++) {
-      mx = fmax(mx, largest[j]);
-      mn = fmin(mn, smallest[j]);
-    }
-    for (; j + 64 <= hi; j += 64) {
-      mx = fmax(mx, bmax[j >> 6]);
-      mn = fmin(mn, bmin[j >> 6]);
-    }
-    for (; j < hi; j++) {
-      mx = fmax(mx, largest[j]);
-      mn = fmin(mn, smallest[j]);
-    }
-    rl[x] = mx;
-    rs[x] = mn;
-  }
-}
-
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
 // The kernel variant for d <= 64 (KB 1) or <= 128 (KB 2), with or without
@@ -724,6 +676,55 @@ void put(std::vector<uint8_t>& key, const T& v) {
 }
 
 }  // namespace
+
+// Each row's largest and smallest nonzero value magnitude over its allowed
+// keys (the bounds of Bounds::hold), from blocks of 64 keys' extrema.
+__global__ void block_extrema(int64_t nj, const double* __restrict__ largest, const double* __restrict__ smallest,
+                              double* __restrict__ bmax, double* __restrict__ bmin) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t b = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b * 64 < nj;
+       b += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    double mx = 0.0, mn = INFINITY;
+    for (int64_t j = b * 64 + lane; j < min(nj, b * 64 + 64); j += 32) {
+      mx = fmax(mx, largest[j]);
+      mn = fmin(mn, smallest[j]);
+    }
+    for (int o = 16; o; o >>= 1) {
+      mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    }
+    if (lane == 0) {
+      bmax[b] = mx;
+      bmin[b] = mn;
+    }
+  }
+}
+
+__global__ void row_value_bounds(int64_t nx, Mask m, const double* __restrict__ largest,
+                                 const double* __restrict__ smallest, const double* __restrict__ bmax,
+                                 const double* __restrict__ bmin, double* __restrict__ rl, double* __restrict__ rs) {
+  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < nx; x += (int64_t)gridDim.x * blockDim.x) {
+    int64_t lo, hi;
+    allowed(m, x, lo, hi);
+    double mx = 0.0, mn = INFINITY;
+    int64_t j = lo;
+    for (; j < hi && (j & 63); j++) {
+      mx = fmax(mx, largest[j]);
+      mn = fmin(mn, smallest[j]);
+    }
+    for (; j + 64 <= hi; j += 64) {
+      mx = fmax(mx, bmax[j >> 6]);
+      mn = fmin(mn, bmin[j >> 6]);
+    }
+    for (; j < hi; j++) {
+      mx = fmax(mx, largest[j]);
+      mn = fmin(mn, smallest[j]);
+    }
+    rl[x] = mx;
+    rs[x] = mn;
+  }
+}
+
 
 AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int slices, cudaStream_t stream) {
   // Six slices: their levels (384 TMEM columns) and the rows' FP64 sums

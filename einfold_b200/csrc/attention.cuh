@@ -61,6 +61,16 @@ __host__ __device__ inline void allowed(const Mask& m, int64_t x, int64_t& lo_ou
 // [0, keys) for constants a and b, as a pipeline's conditions give.
 bool ranges_as_mask(const int64_t* ranges, int64_t queries, int64_t keys, Mask& m);
 
+// Each row's largest and smallest nonzero value magnitude over its allowed
+// keys (the bounds of Bounds::hold, fused.rs:1058-1086): block_extrema takes
+// the extrema of blocks of 64 keys, row_value_bounds those of each row's
+// allowed range.
+__global__ void block_extrema(int64_t nj, const double* __restrict__ largest, const double* __restrict__ smallest,
+                              double* __restrict__ bmax, double* __restrict__ bmin);
+__global__ void row_value_bounds(int64_t nx, Mask m, const double* __restrict__ largest,
+                                 const double* __restrict__ smallest, const double* __restrict__ bmax,
+                                 const double* __restrict__ bmin, double* __restrict__ rl, double* __restrict__ rs);
+
 // A softmax-weighted average over placed matrices, batch by batch:
 // q [w][x][e], k [w][j][e], v [w][j][y] for w < batches, x < lnx, j < lnj,
 // e < ne, y < ny; out [w·lnx + x][y] = Σ_j exp(s_xj − m_x) v_jy / z_x over the
@@ -93,9 +103,18 @@ enum AttentionOutcome { ATTENTION_DONE = 0, ATTENTION_INELIGIBLE = 1, ATTENTION_
 // underflow guard fires on a row (the pipeline declines).
 AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int slices, cudaStream_t stream);
 
+// The FP64 form on the FP64 tensor pipe (mma.sync f64): product scores, the
+// online softmax and the weighted sums in FP64, with the reference's guards.
+// INELIGIBLE (nothing written) when q or k isn't finite, a score could
+// overflow, or d > 128; the caller's value statistics (largest, smallest)
+// must be set and v finite.
+AttentionOutcome attention_f64_mma(Context& ctx, const AttentionProblem& p, cudaStream_t stream);
+
 // The forward pass over placed matrices: the split form when `precision`
-// is 0 and it applies, else the FP64 tile kernel (fused.rs's tile, in FP64
-// on the CUDA cores). Computes each J position's value statistics itself.
+// is 0 and it applies, else the FP64 form on the FP64 tensor pipe where it
+// applies, else the FP64 tile kernel (fused.rs's tile, in FP64 on the CUDA
+// cores, for non-finite operands). Computes each J position's value
+// statistics itself.
 AttentionOutcome attention_forward(Context& ctx, AttentionProblem p, int precision, int slices, cudaStream_t stream);
 
 // The gradients of the forward pass's out, from its saved lse:

@@ -23,6 +23,7 @@
 #include <cub/cub.cuh>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "fold.h"
@@ -240,7 +241,8 @@ __global__ void __launch_bounds__(256) gustavson(int64_t nx, int64_t ny, const i
                                                  uint32_t* __restrict__ reached_all, uint32_t* __restrict__ valued_all,
                                                  int64_t* __restrict__ group_count, const int64_t* __restrict__ group_off,
                                                  uint32_t* __restrict__ gy, double* __restrict__ gsum,
-                                                 uint8_t* __restrict__ gvalued) {
+                                                 uint8_t* __restrict__ gvalued, int64_t x_begin, int64_t x_end,
+                                                 int64_t group_base) {
   const int64_t words = (ny + 31) / 32;
   double* acc = acc_all + (FILL ? (int64_t)blockIdx.x * ny : 0);
   uint32_t* reached = reached_all + (int64_t)blockIdx.x * words;
@@ -248,7 +250,8 @@ __global__ void __launch_bounds__(256) gustavson(int64_t nx, int64_t ny, const i
   __shared__ unsigned long long s_count;
   typedef cub::BlockScan<int, 256> BlockScanInt;
   __shared__ typename BlockScanInt::TempStorage scan_tmp;
-  for (int64_t x = blockIdx.x; x < nx; x += gridDim.x) {
+  (void)nx;
+  for (int64_t x = x_begin + blockIdx.x; x < x_end; x += gridDim.x) {
     for (int64_t i = a_start[x]; i < a_start[x + 1]; i++) {
       const uint32_t z = a_z[i];
       const double p = a_f[i];
@@ -299,7 +302,7 @@ __global__ void __launch_bounds__(256) gustavson(int64_t nx, int64_t ny, const i
       for (int64_t w = w0; w < w1; w++) cnt += __popc(reached[w]);
       int before;
       BlockScanInt(scan_tmp).ExclusiveSum(cnt, before);
-      int64_t pos = group_off[x] + before;
+      int64_t pos = group_off[x] - group_base + before;
       for (int64_t w = w0; w < w1; w++) {
         uint32_t bits = reached[w];
         const uint32_t vb = valued[w];
@@ -322,9 +325,10 @@ __global__ void __launch_bounds__(256) gustavson(int64_t nx, int64_t ny, const i
   }
 }
 
-__global__ void fill_x(const int64_t* __restrict__ off, int64_t nx, uint32_t* __restrict__ gx) {
-  for (int64_t x = blockIdx.x; x < nx; x += gridDim.x)
-    for (int64_t g = off[x] + threadIdx.x; g < off[x + 1]; g += blockDim.x) gx[g] = (uint32_t)x;
+__global__ void fill_x(const int64_t* __restrict__ off, int64_t x_begin, int64_t x_end, uint32_t* __restrict__ gx) {
+  const int64_t base = off[x_begin];
+  for (int64_t x = x_begin + blockIdx.x; x < x_end; x += gridDim.x)
+    for (int64_t g = off[x] + threadIdx.x; g < off[x + 1]; g += blockDim.x) gx[g - base] = (uint32_t)x;
 }
 
 // Fixed-width gather of a key column by row (take), with validity bytes.
@@ -799,7 +803,7 @@ FoldOutput discriminate_fold(Context& ctx, const FoldD& f, const Relation& a, co
   DeviceBuffer<int64_t> gcount((size_t)nx, s), goff((size_t)nx + 1, s);
   gustavson<false><<<count_blocks, 256, 0, s>>>(nx, ny, a_start.get(), a_z.get(), a_f.get(), a_v.get(), b_start.get(),
                                           b_y.get(), b_f.get(), b_v.get(), nullptr, reached.get(), valued.get(),
-                                          gcount.get(), nullptr, nullptr, nullptr, nullptr);
+                                          gcount.get(), nullptr, nullptr, nullptr, nullptr, 0, nx, 0);
   ctx.kernels++;
   EF_LAUNCH_CHECK();
   EF_CUDA(cudaMemsetAsync(goff.get(), 0, 8, s));
@@ -816,19 +820,24 @@ FoldOutput discriminate_fold(Context& ctx, const FoldD& f, const Relation& a, co
   budget.reserve(sat_add(sat_mul((uint64_t)groups, 24), out_bytes), "the discrimination algorithm's groups");
   DeviceBuffer<double> acc((size_t)blocks * ny, s);
   acc.zero();
-  DeviceBuffer<uint32_t> gy((size_t)(groups ? groups : 1), s), gx((size_t)(groups ? groups : 1), s);
-  DeviceBuffer<double> gsum((size_t)(groups ? groups : 1), s);
-  DeviceBuffer<uint8_t> gval((size_t)(groups ? groups : 1), s);
-  gustavson<true><<<blocks, 256, 0, s>>>(nx, ny, a_start.get(), a_z.get(), a_f.get(), a_v.get(), b_start.get(),
-                                         b_y.get(), b_f.get(), b_v.get(), acc.get(), reached.get(), valued.get(),
-                                         nullptr, goff.get(), gy.get(), gsum.get(), gval.get());
-  ctx.kernels++;
-  EF_LAUNCH_CHECK();
-  ctx.phase("discriminate: product");
+  // The groups of x in [x_begin, x_end), in (x, y) order, into arrays of
+  // their own (the accumulators and bitmaps are left cleared for the next).
+  auto fill = [&](int64_t x_begin, int64_t x_end, uint32_t* gy, double* gsum, uint8_t* gval, int64_t base) {
+    gustavson<true><<<blocks, 256, 0, s>>>(nx, ny, a_start.get(), a_z.get(), a_f.get(), a_v.get(), b_start.get(),
+                                           b_y.get(), b_f.get(), b_v.get(), acc.get(), reached.get(), valued.get(),
+                                           nullptr, goff.get(), gy, gsum, gval, x_begin, x_end, base);
+    ctx.kernels++;
+    EF_LAUNCH_CHECK();
+  };
 
   FoldOutput result;
   result.algorithm = EINFOLD_ALG_DISCRIMINATE;
   if (f.domain) {
+    DeviceBuffer<uint32_t> gy((size_t)(groups ? groups : 1), s);
+    DeviceBuffer<double> gsum((size_t)(groups ? groups : 1), s);
+    DeviceBuffer<uint8_t> gval((size_t)(groups ? groups : 1), s);
+    fill(0, nx, gy.get(), gsum.get(), gval.get(), 0);
+    ctx.phase("discriminate: product");
     if (!domain) fail(EINFOLD_INVALID, "a fold with a domain was given no domain relation");
     if (o.result_on_device) fail(EINFOLD_INVALID, "results in device memory are not supported with a domain");
     const DomainD& spec = *f.domain;
@@ -894,114 +903,143 @@ FoldOutput discriminate_fold(Context& ctx, const FoldD& f, const Relation& a, co
     return result;
   }
 
-  // Groups' keys from a row of a or b that has them (take of first rows).
-  if (groups) {
-    fill_x<<<std::min<int64_t>(nx, 65535), 256, 0, s>>>(goff.get(), nx, gx.get());
-    ctx.kernels++;
-  }
-  OutBatch out_batch;
-  out_batch.rows = groups;
-  for (size_t i = 0; i < f.outputs.size(); i++) {
-    const bool from_a = oa.holds(f.outputs[i].dim);
-    const std::vector<int>& outs = from_a ? a_out : b_out;
-    size_t j = 0;
-    while (outs[j] != (int)i) j++;
-    const DeviceColumn& src = (from_a ? a_o : b_o).cols[j];
-    const uint32_t* first = from_a ? x.first.get() : y.first.get();
-    const uint32_t* g = from_a ? gx.get() : gy.get();
-    OutColumn c;
-    c.format = schema[i].format;
-    c.name = schema[i].name;
-    c.kind = schema[i].kind;
-    c.nullable = schema[i].nullable;
-    c.length = groups;
-    DeviceBuffer<uint8_t> cvalid((size_t)(groups ? groups : 1), s);
-    DeviceBuffer<unsigned long long> cn(1, s);
-    cn.zero();
-    if (is_var(src.kind)) {
-      DeviceBuffer<int64_t> len((size_t)(groups ? groups : 1), s), offs((size_t)groups + 1, s);
-      if (groups) {
-        gather_lengths<<<blocks_for(groups, 256), 256, 0, s>>>(src.offsets.get(), first, g, groups, len.get());
-        EF_CUDA(cudaMemsetAsync(offs.get(), 0, 8, s));
-        size_t temp = 0;
-        EF_CUDA(cub::DeviceScan::InclusiveSum(nullptr, temp, len.get(), offs.get() + 1, (int)groups, s));
-        DeviceBuffer<uint8_t> t(temp ? temp : 1, s);
-        EF_CUDA(cub::DeviceScan::InclusiveSum(t.get(), temp, len.get(), offs.get() + 1, (int)groups, s));
-      } else {
-        EF_CUDA(cudaMemsetAsync(offs.get(), 0, 8, s));
-      }
-      int64_t total = 0;
-      EF_CUDA(cudaMemcpyAsync(&total, offs.get() + groups, 8, cudaMemcpyDeviceToHost, s));
-      EF_CUDA(cudaStreamSynchronize(s));
-      DeviceBuffer<uint8_t> bytes((size_t)(total ? total : 1), s);
-      if (groups) {
-        gather_bytes<<<blocks_for(groups, 256), 256, 0, s>>>(src.bytes.get(), src.offsets.get(), first, g, offs.get(),
-                                                             groups, bytes.get());
-        gather_valid<<<blocks_for(groups, 256), 256, 0, s>>>(src.valid.get(), first, g, groups, cvalid.get(), cn.get());
-      }
-      const bool large = src.kind == Kind::LargeUtf8 || src.kind == Kind::LargeBinary;
-      if (large) {
-        c.values = result_buffer(ctx, offs, (size_t)(groups + 1) * 8, o.result_on_device);
-      } else {
-        if (total > INT32_MAX) fail(EINFOLD_COMPUTE, "string output over 2 GiB");
-        DeviceBuffer<int32_t> o32((size_t)groups + 1, s);
-        narrow_offsets<<<blocks_for((uint64_t)groups + 1, 256), 256, 0, s>>>(offs.get(), groups + 1, o32.get());
-        ctx.kernels++;
-        c.values = result_buffer(ctx, o32, (size_t)(groups + 1) * 4, o.result_on_device);
-      }
-      c.data = result_buffer(ctx, bytes, (size_t)total, o.result_on_device);
-    } else {
-      const int width = width_of(src.kind) ? width_of(src.kind) : 1;
-      DeviceBuffer<uint8_t> vals((size_t)(groups ? groups * width : 1), s);
-      if (groups)
-        gather_fixed<<<blocks_for(groups, 256), 256, 0, s>>>(src.ptr(), src.valid.get(), width,
-                                                             o.float_keys == 1 && is_float(src.kind), first, g, groups,
-                                                             vals.get(), cvalid.get(), cn.get());
-      c.values = result_buffer(ctx, vals, (size_t)(groups * width), o.result_on_device);
-    }
-    unsigned long long cnulls = 0;
-    EF_CUDA(cudaMemcpyAsync(&cnulls, cn.get(), 8, cudaMemcpyDeviceToHost, s));
-    EF_CUDA(cudaStreamSynchronize(s));
-    c.null_count = (int64_t)cnulls;
-    if (cnulls) {
-      DeviceBuffer<uint8_t> bits((size_t)((groups + 7) / 8), s);
-      pack_bits(ctx, cvalid.get(), groups, bits.get());
-      c.validity = result_buffer(ctx, bits, (size_t)((groups + 7) / 8), o.result_on_device);
-    }
-    out_batch.columns.push_back(std::move(c));
-  }
-  OutColumn v;
-  v.format = "g";
-  v.kind = Kind::Float64;
-  v.name = schema.back().name;
-  v.length = groups;
-  DeviceBuffer<uint8_t> vbits((size_t)((groups + 7) / 8 ? (groups + 7) / 8 : 1), s);
-  unsigned long long vnulls = 0;
-  {
-    DeviceBuffer<unsigned long long> cnt(1, s);
-    cnt.zero();
-    // NULL where no product had a value.
-    DeviceBuffer<uint8_t> inv((size_t)(groups ? groups : 1), s);
-    if (groups) {
-      pack_bits(ctx, gval.get(), groups, vbits.get());
-      size_t temp = 0;
-      cub::TransformInputIterator<unsigned long long, cub::CastOp<unsigned long long>, const uint8_t*> it(
-          gval.get(), cub::CastOp<unsigned long long>());
-      EF_CUDA(cub::DeviceReduce::Sum(nullptr, temp, it, cnt.get(), (int)groups, s));
-      DeviceBuffer<uint8_t> t(temp ? temp : 1, s);
-      EF_CUDA(cub::DeviceReduce::Sum(t.get(), temp, it, cnt.get(), (int)groups, s));
-      unsigned long long valued_n = 0;
-      EF_CUDA(cudaMemcpyAsync(&valued_n, cnt.get(), 8, cudaMemcpyDeviceToHost, s));
-      EF_CUDA(cudaStreamSynchronize(s));
-      vnulls = (unsigned long long)groups - valued_n;
-    }
-  }
-  v.values = result_buffer(ctx, gsum, (size_t)groups * 8, o.result_on_device);
-  v.null_count = (int64_t)vnulls;
-  if (vnulls) v.validity = result_buffer(ctx, vbits, (size_t)((groups + 7) / 8), o.result_on_device);
-  out_batch.columns.push_back(std::move(v));
+  // The result in batches of at most EINFOLD_GROUPS_PER_BATCH groups (2^28
+  // by default): the groups of consecutive x blocks, each batch's product,
+  // keys and values computed, copied out and freed before the next, so that
+  // device memory holds one batch's groups at a time however many the fold
+  // makes. x blocks are independent (discriminate.rs:548-584), and the
+  // batches come out in (x, y) order.
+  static const int64_t per_batch = [] {
+    const char* e = std::getenv("EINFOLD_GROUPS_PER_BATCH");
+    const long long v = e ? std::atoll(e) : (1ll << 28);
+    return (int64_t)std::max(1ll, v);
+  }();
+  std::vector<int64_t> hoff((size_t)nx + 1);
+  EF_CUDA(cudaMemcpyAsync(hoff.data(), goff.get(), (size_t)(nx + 1) * 8, cudaMemcpyDeviceToHost, s));
   EF_CUDA(cudaStreamSynchronize(s));
-  result.batches.push_back(std::move(out_batch));
+  int64_t x_begin = 0;
+  do {
+    int64_t x_end = x_begin + 1;
+    while (x_end < nx && hoff[(size_t)x_end + 1] - hoff[(size_t)x_begin] <= per_batch) x_end++;
+    if (nx == 0) x_end = 0;
+    const int64_t base = nx ? hoff[(size_t)x_begin] : 0;
+    const int64_t groups = nx ? hoff[(size_t)x_end] - base : 0;
+    DeviceBuffer<uint32_t> gy((size_t)(groups ? groups : 1), s), gx((size_t)(groups ? groups : 1), s);
+    DeviceBuffer<double> gsum((size_t)(groups ? groups : 1), s);
+    DeviceBuffer<uint8_t> gval((size_t)(groups ? groups : 1), s);
+    if (groups) fill(x_begin, x_end, gy.get(), gsum.get(), gval.get(), base);
+    ctx.phase("discriminate: product");
+    // Groups' keys from a row of a or b that has them (take of first rows).
+    if (groups) {
+      fill_x<<<std::max<int64_t>(1, std::min<int64_t>(x_end - x_begin, 65535)), 256, 0, s>>>(goff.get(), x_begin,
+                                                                                            x_end, gx.get());
+      ctx.kernels++;
+    }
+    OutBatch out_batch;
+    out_batch.rows = groups;
+    for (size_t i = 0; i < f.outputs.size(); i++) {
+      const bool from_a = oa.holds(f.outputs[i].dim);
+      const std::vector<int>& outs = from_a ? a_out : b_out;
+      size_t j = 0;
+      while (outs[j] != (int)i) j++;
+      const DeviceColumn& src = (from_a ? a_o : b_o).cols[j];
+      const uint32_t* first = from_a ? x.first.get() : y.first.get();
+      const uint32_t* g = from_a ? gx.get() : gy.get();
+      OutColumn c;
+      c.format = schema[i].format;
+      c.name = schema[i].name;
+      c.kind = schema[i].kind;
+      c.nullable = schema[i].nullable;
+      c.length = groups;
+      DeviceBuffer<uint8_t> cvalid((size_t)(groups ? groups : 1), s);
+      DeviceBuffer<unsigned long long> cn(1, s);
+      cn.zero();
+      if (is_var(src.kind)) {
+        DeviceBuffer<int64_t> len((size_t)(groups ? groups : 1), s), offs((size_t)groups + 1, s);
+        if (groups) {
+          gather_lengths<<<blocks_for(groups, 256), 256, 0, s>>>(src.offsets.get(), first, g, groups, len.get());
+          EF_CUDA(cudaMemsetAsync(offs.get(), 0, 8, s));
+          size_t temp = 0;
+          EF_CUDA(cub::DeviceScan::InclusiveSum(nullptr, temp, len.get(), offs.get() + 1, (int)groups, s));
+          DeviceBuffer<uint8_t> t(temp ? temp : 1, s);
+          EF_CUDA(cub::DeviceScan::InclusiveSum(t.get(), temp, len.get(), offs.get() + 1, (int)groups, s));
+        } else {
+          EF_CUDA(cudaMemsetAsync(offs.get(), 0, 8, s));
+        }
+        int64_t total = 0;
+        EF_CUDA(cudaMemcpyAsync(&total, offs.get() + groups, 8, cudaMemcpyDeviceToHost, s));
+        EF_CUDA(cudaStreamSynchronize(s));
+        DeviceBuffer<uint8_t> bytes((size_t)(total ? total : 1), s);
+        if (groups) {
+          gather_bytes<<<blocks_for(groups, 256), 256, 0, s>>>(src.bytes.get(), src.offsets.get(), first, g, offs.get(),
+                                                               groups, bytes.get());
+          gather_valid<<<blocks_for(groups, 256), 256, 0, s>>>(src.valid.get(), first, g, groups, cvalid.get(), cn.get());
+        }
+        const bool large = src.kind == Kind::LargeUtf8 || src.kind == Kind::LargeBinary;
+        if (large) {
+          c.values = result_buffer(ctx, offs, (size_t)(groups + 1) * 8, o.result_on_device);
+        } else {
+          if (total > INT32_MAX) fail(EINFOLD_COMPUTE, "string output over 2 GiB");
+          DeviceBuffer<int32_t> o32((size_t)groups + 1, s);
+          narrow_offsets<<<blocks_for((uint64_t)groups + 1, 256), 256, 0, s>>>(offs.get(), groups + 1, o32.get());
+          ctx.kernels++;
+          c.values = result_buffer(ctx, o32, (size_t)(groups + 1) * 4, o.result_on_device);
+        }
+        c.data = result_buffer(ctx, bytes, (size_t)total, o.result_on_device);
+      } else {
+        const int width = width_of(src.kind) ? width_of(src.kind) : 1;
+        DeviceBuffer<uint8_t> vals((size_t)(groups ? groups * width : 1), s);
+        if (groups)
+          gather_fixed<<<blocks_for(groups, 256), 256, 0, s>>>(src.ptr(), src.valid.get(), width,
+                                                               o.float_keys == 1 && is_float(src.kind), first, g, groups,
+                                                               vals.get(), cvalid.get(), cn.get());
+        c.values = result_buffer(ctx, vals, (size_t)(groups * width), o.result_on_device);
+      }
+      unsigned long long cnulls = 0;
+      EF_CUDA(cudaMemcpyAsync(&cnulls, cn.get(), 8, cudaMemcpyDeviceToHost, s));
+      EF_CUDA(cudaStreamSynchronize(s));
+      c.null_count = (int64_t)cnulls;
+      if (cnulls) {
+        DeviceBuffer<uint8_t> bits((size_t)((groups + 7) / 8), s);
+        pack_bits(ctx, cvalid.get(), groups, bits.get());
+        c.validity = result_buffer(ctx, bits, (size_t)((groups + 7) / 8), o.result_on_device);
+      }
+      out_batch.columns.push_back(std::move(c));
+    }
+    OutColumn v;
+    v.format = "g";
+    v.kind = Kind::Float64;
+    v.name = schema.back().name;
+    v.length = groups;
+    DeviceBuffer<uint8_t> vbits((size_t)((groups + 7) / 8 ? (groups + 7) / 8 : 1), s);
+    unsigned long long vnulls = 0;
+    {
+      DeviceBuffer<unsigned long long> cnt(1, s);
+      cnt.zero();
+      // NULL where no product had a value.
+      DeviceBuffer<uint8_t> inv((size_t)(groups ? groups : 1), s);
+      if (groups) {
+        pack_bits(ctx, gval.get(), groups, vbits.get());
+        size_t temp = 0;
+        cub::TransformInputIterator<unsigned long long, cub::CastOp<unsigned long long>, const uint8_t*> it(
+            gval.get(), cub::CastOp<unsigned long long>());
+        EF_CUDA(cub::DeviceReduce::Sum(nullptr, temp, it, cnt.get(), (int)groups, s));
+        DeviceBuffer<uint8_t> t(temp ? temp : 1, s);
+        EF_CUDA(cub::DeviceReduce::Sum(t.get(), temp, it, cnt.get(), (int)groups, s));
+        unsigned long long valued_n = 0;
+        EF_CUDA(cudaMemcpyAsync(&valued_n, cnt.get(), 8, cudaMemcpyDeviceToHost, s));
+        EF_CUDA(cudaStreamSynchronize(s));
+        vnulls = (unsigned long long)groups - valued_n;
+      }
+    }
+    v.values = result_buffer(ctx, gsum, (size_t)groups * 8, o.result_on_device);
+    v.null_count = (int64_t)vnulls;
+    if (vnulls) v.validity = result_buffer(ctx, vbits, (size_t)((groups + 7) / 8), o.result_on_device);
+    out_batch.columns.push_back(std::move(v));
+    EF_CUDA(cudaStreamSynchronize(s));
+    result.batches.push_back(std::move(out_batch));
+    x_begin = x_end;
+  } while (x_begin < nx);
   ctx.phase("discriminate: result");
   return result;
 }

@@ -22,6 +22,7 @@
 // so the chunks' flags OR to the whole row's.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <optional>
 
 #include "attention.cuh"
@@ -734,6 +735,16 @@ __global__ void emit_rows(int64_t nx, int64_t ny, const uint8_t* __restrict__ fl
   }
 }
 
+// EINFOLD_FP64_TILES=1 keeps attention-shaped pipelines on the FP64 tile
+// kernel (the CUDA cores) instead of the FP64 tensor pipe.
+bool fp64_tiles_forced() {
+  static const bool forced = [] {
+    const char* e = std::getenv("EINFOLD_FP64_TILES");
+    return e && e[0] == '1';
+  }();
+  return forced;
+}
+
 struct Placement {
   int operand;                 // 0 q, 1 k, 2 v
   const std::vector<int>* rows;
@@ -1096,6 +1107,36 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
       EF_LAUNCH_CHECK();
     }
   }
+  if (!split_done && !pr.row_expr && !p.weight_expr && p.shift == 1 && p.normalizer == 0 && !v_nonfinite &&
+      nx > 0 && nj > 0 && ny > 0 && batches_w * mask.lnx == (int64_t)nx && batches_w * mask.lnj == (int64_t)nj &&
+      !fp64_tiles_forced()) {
+    // The FP64 form on the FP64 tensor pipe, for an attention-shaped
+    // pipeline the split form didn't take (precision = fp64, or scores it
+    // can't bound).
+    AttentionProblem ap;
+    ap.q = matrices[0].get();
+    ap.k = matrices[1].get();
+    ap.v = matrices.back().get();
+    ap.batches = batches_w;
+    ap.lnx = mask.lnx;
+    ap.lnj = mask.lnj;
+    ap.ne = (int64_t)ne;
+    ap.ny = (int64_t)ny;
+    ap.mask = mask;
+    ap.scale_kind = p.scale_kind;
+    ap.scale_c = p.scale_c;
+    ap.largest = largest.get();
+    ap.smallest = smallest.get();
+    ap.out = out.get();
+    const AttentionOutcome r = attention_f64_mma(ctx, ap, s);
+    if (r == ATTENTION_GUARDED) decline("a sum that overflowed or may have underflowed");
+    if (r == ATTENTION_DONE) {
+      split_done = true;
+      count_tiles<<<blocks_for(x_tiles * 32, 256), 256, 0, s>>>((int64_t)nx, (int64_t)nj, mask, visited.get());
+      ctx.kernels++;
+      EF_LAUNCH_CHECK();
+    }
+  }
   if (x_tiles && !split_done) {
     const dim3 grid((unsigned)x_tiles, (unsigned)std::max<uint64_t>((ny + YC - 1) / YC, 1));
     launch_tiles(a, std::max(stack_depth(snodes), stack_depth(wnodes)), grid, s);
@@ -1419,6 +1460,10 @@ AttentionOutcome attention_forward(Context& ctx, AttentionProblem p, int precisi
   p.smallest = smallest.get();
   if (precision == 0 && !v_nonfinite && nj > 0) {
     const AttentionOutcome r = attention_split(ctx, p, slices > 0 ? slices : 6, s);
+    if (r != ATTENTION_INELIGIBLE) return r;
+  }
+  if (!v_nonfinite && nj > 0 && !fp64_tiles_forced()) {
+    const AttentionOutcome r = attention_f64_mma(ctx, p, s);
     if (r != ATTENTION_INELIGIBLE) return r;
   }
   TileArgs a{};
