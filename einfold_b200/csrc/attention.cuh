@@ -110,6 +110,9 @@ AttentionOutcome attention_split(Context& ctx, const AttentionProblem& p, int sl
 // must be set and v finite.
 AttentionOutcome attention_f64_mma(Context& ctx, const AttentionProblem& p, cudaStream_t stream);
 
+// Whether EINFOLD_FP64_TILES=1 asks for the CUDA cores' FP64 tile kernels.
+bool fp64_tiles_requested();
+
 // The forward pass over placed matrices: the split form when `precision`
 // is 0 and it applies, else the FP64 form on the FP64 tensor pipe where it
 // applies, else the FP64 tile kernel (fused.rs's tile, in FP64 on the CUDA
@@ -130,6 +133,12 @@ struct AttentionGradients {
   double* d_k = nullptr;
   double* d_v = nullptr;
 };
+// The FP64 backward on the FP64 tensor pipe (d, dv <= 64, scale one or times
+// c; false, nothing written, otherwise): d_k and d_v from a kernel with keys
+// as rows (`keys_mask` the transposed mask), d_q from one with queries as
+// rows, scores recomputed from lse, D = rowsum(d_out∘out) given.
+bool backward_f64_mma(Context& ctx, const AttentionGradients& g, const Mask& keys_mask, const double* dd,
+                      cudaStream_t stream);
 void attention_backward(Context& ctx, const AttentionGradients& g, int precision, cudaStream_t stream);
 
 }  // namespace ef

@@ -21,13 +21,25 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <type_traits>
 
 #include "attention.cuh"
 #include "fastexp.cuh"
 #include "ptx.cuh"
 
 namespace ef {
+
+// EINFOLD_FP64_TILES=1 keeps the FP64 form on the CUDA cores' tile kernels.
+bool fp64_tiles_requested() {
+  static const bool on = [] {
+    const char* e = std::getenv("EINFOLD_FP64_TILES");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
 namespace {
 
 constexpr int FM = 64;   // query rows a block: four warps of 16
@@ -321,11 +333,246 @@ __global__ void finite_max(const double* __restrict__ x, int64_t n, int* bad, un
   if ((threadIdx.x & 31) == 0 && mx > 0.0) atomicMax(largest, (unsigned long long)__double_as_longlong(mx));
 }
 
+// ---- The backward pass on the FP64 tensor pipe -----------------------------
+//
+// Two kernels, as FlashAttention-2's backward: one with keys as rows (128 a
+// block, eight warps of 16) walking the query tiles of 32 its keys are
+// joined by, recomputing S^T = K·Q^T, P^T = exp(S^T - lse), dP^T = V·dO^T and
+// dS^T = P^T (dP^T - D), and summing dV += P^T·dO and dK += dS^T·Q in
+// registers; one with queries as rows walking their key tiles, recomputing
+// S, P, dP and dS and summing dQ += dS·K. P and dS feed the second products
+// from the accumulators (column 2t, 2t + 1 as the A operand's t, t + 4; the
+// B operand's rows read in that order). Every output row is summed by one
+// block, in tile order: no atomics. For d, dv <= 64.
+
+constexpr int BR = 128;  // rows a block: eight warps of 16
+constexpr int BC = 32;   // columns (queries or keys) a tile
+constexpr int kBwdThreads = 256;
+constexpr int RS = 68;   // shared-memory stride of the blocks' own rows
+constexpr int CS = 66;   // shared-memory stride of a tile's rows
+
+struct F64BwdArgs {
+  const double* a1;  // rows' operand of the first product (k or q), [w·lr + r][d1]
+  const double* a2;  // rows' operand of the second (v or d_out), [w·lr + r][d2]
+  const double* b1;  // tiles' operand of the first (q or k), [w·lc + c][d1]
+  const double* b2;  // tiles' operand of the second (d_out or v), [w·lc + c][d2]
+  const double* lse;  // per query
+  const double* dd;   // D per query
+  double* out1;  // kv: d_v [rows][d2]; q: d_q [rows][d1]
+  double* out2;  // kv: d_k [rows][d1]
+  int64_t lr, lc, d1, d2;
+  Mask mask;  // rows' allowed columns
+  double scale;
+  const double* exp_table;
+  int keys_rows;  // 1: rows are keys (lse, D per column); 0: rows are queries
+};
+
+// Rows [r0, r0 + n) of a row-major matrix of `cols` columns into shared
+// memory at `stride`, zeros past `valid` rows and `cols` columns, `width`
+// (a multiple of 8) columns wide.
+template <bool ASYNC>
+__device__ __forceinline__ void load_rows(double* dst, int stride, const double* src, int64_t r0, int n, int64_t valid,
+                                          int64_t cols, int width) {
+  if (ASYNC) {
+    const int kc = width / 2;
+    for (int i = threadIdx.x; i < n * kc; i += kBwdThreads) {
+      const int r = i / kc, c = 2 * (i - r * kc);
+      const bool in = r0 + r < valid && c < cols;
+      cp_async16(dst + r * stride + c, in ? src + (r0 + r) * cols + c : src, in ? 16 : 0);
+    }
+  } else {
+    for (int i = threadIdx.x; i < n * width; i += kBwdThreads) {
+      const int r = i / width, c = i - r * width;
+      dst[r * stride + c] = (r0 + r < valid && c < cols) ? src[(r0 + r) * cols + c] : 0.0;
+    }
+  }
+}
+
+// KV: rows are keys (out1 = d_v, out2 = d_k); else rows are queries (out1 = d_q).
+template <bool KV, bool ASYNC>
+__global__ void __launch_bounds__(kBwdThreads, 1) attn_bwd_f64(const F64BwdArgs a) {
+  extern __shared__ __align__(16) double sm[];
+  double* sA1 = sm;                  // [BR][RS]
+  double* sA2 = sA1 + BR * RS;       // [BR][RS]
+  double* sB = sA2 + BR * RS;        // [2][b1 | b2] tiles, [BC][CS] each
+  double* sLD = sB + 4 * BC * CS;    // [2][lse | D] of the tile's columns (KV)
+  __shared__ double texp[64];
+  __shared__ long long span[2];
+  __shared__ long long lo_s[BR], hi_s[BR];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+  const int64_t w = blockIdx.y;
+  const int64_t x0 = (int64_t)blockIdx.x * BR;
+  const int64_t r_base = w * a.lr, c_base = w * a.lc;
+  const int w1 = (int)((a.d1 + 7) & ~7LL), w2 = (int)((a.d2 + 7) & ~7LL);
+  if (tid < 64) texp[tid] = a.exp_table[tid];
+  if (tid == 0) {
+    span[0] = LLONG_MAX;
+    span[1] = LLONG_MIN;
+  }
+  __syncthreads();
+  if (tid < BR) {
+    const int64_t xl = x0 + tid;
+    int64_t lo = 0, hi = 0;
+    if (xl < a.lr) {
+      allowed(a.mask, r_base + xl, lo, hi);
+      lo -= c_base;
+      hi -= c_base;
+    }
+    if (lo >= hi) lo = hi = 0;
+    lo_s[tid] = lo;
+    hi_s[tid] = hi;
+    if (lo < hi) {
+      atomicMin(&span[0], lo);
+      atomicMax(&span[1], hi);
+    }
+  }
+  load_rows<ASYNC>(sA1, RS, a.a1 + r_base * a.d1, x0, BR, a.lr, a.d1, w1);
+  load_rows<ASYNC>(sA2, RS, a.a2 + r_base * a.d2, x0, BR, a.lr, a.d2, w2);
+  if (ASYNC) cp_commit();
+  __syncthreads();
+  const long long first = span[0], last = span[1];
+  const int64_t t0 = first < last ? first / BC : 0;
+  const int n_tiles = first < last ? (int)((last + BC - 1) / BC - t0) : 0;
+
+  auto load = [&](int it, int b) {
+    const int64_t j0 = (t0 + it) * BC;
+    double* b1 = sB + b * 2 * BC * CS;
+    double* b2 = b1 + BC * CS;
+    load_rows<ASYNC>(b1, CS, a.b1 + c_base * a.d1, j0, BC, a.lc, a.d1, w1);
+    load_rows<ASYNC>(b2, CS, a.b2 + c_base * a.d2, j0, BC, a.lc, a.d2, w2);
+    if (KV && tid < 2 * BC) {
+      // The tile's queries' lse and D.
+      const int c = tid & (BC - 1);
+      const int64_t q = j0 + c;
+      const double* srcp = tid < BC ? a.lse : a.dd;
+      sLD[b * 2 * BC + tid] = q < a.lc ? srcp[c_base + q] : 0.0;
+    }
+  };
+
+  const int r0 = warp * 16 + g, r1 = r0 + 8;
+  const long long lo0 = lo_s[r0], hi0 = hi_s[r0], lo1 = lo_s[r1], hi1 = hi_s[r1];
+  // Queries as rows: their own lse and D.
+  double lse_r[2] = {0.0, 0.0}, dd_r[2] = {0.0, 0.0};
+  if (!KV) {
+    if (x0 + r0 < a.lr) {
+      lse_r[0] = a.lse[r_base + x0 + r0];
+      dd_r[0] = a.dd[r_base + x0 + r0];
+    }
+    if (x0 + r1 < a.lr) {
+      lse_r[1] = a.lse[r_base + x0 + r1];
+      dd_r[1] = a.dd[r_base + x0 + r1];
+    }
+  }
+  double o1[8][4], o2[8][4];  // KV: d_v, d_k; else d_q in o1
+#pragma unroll
+  for (int n = 0; n < 8; n++)
+#pragma unroll
+    for (int i = 0; i < 4; i++) o1[n][i] = o2[n][i] = 0.0;
+
+  if (n_tiles > 0) {
+    load(0, 0);
+    if (ASYNC) cp_commit();
+  }
+  for (int it = 0; it < n_tiles; it++) {
+    const int b = it & 1;
+    if (it + 1 < n_tiles) {
+      load(it + 1, b ^ 1);
+      if (ASYNC) {
+        cp_commit();
+        cp_wait<1>();
+      }
+    } else if (ASYNC) {
+      cp_wait<0>();
+    }
+    __syncthreads();
+    const double* b1 = sB + b * 2 * BC * CS;
+    const double* b2 = b1 + BC * CS;
+    const double* ld = sLD + b * 2 * BC;
+    double s[BC / 8][4], dp[BC / 8][4];
+#pragma unroll
+    for (int n = 0; n < BC / 8; n++)
+#pragma unroll
+      for (int i = 0; i < 4; i++) s[n][i] = dp[n][i] = 0.0;
+    for (int kk = 0; kk < w1; kk += 8) {
+      const double x0a = sA1[r0 * RS + kk + t], x1a = sA1[r1 * RS + kk + t];
+      const double x2a = sA1[r0 * RS + kk + t + 4], x3a = sA1[r1 * RS + kk + t + 4];
+#pragma unroll
+      for (int n = 0; n < BC / 8; n++) {
+        const double* br = b1 + (n * 8 + g) * CS + kk;
+        dmma(s[n], x0a, x1a, x2a, x3a, br[t], br[t + 4]);
+      }
+    }
+    for (int kk = 0; kk < w2; kk += 8) {
+      const double x0a = sA2[r0 * RS + kk + t], x1a = sA2[r1 * RS + kk + t];
+      const double x2a = sA2[r0 * RS + kk + t + 4], x3a = sA2[r1 * RS + kk + t + 4];
+#pragma unroll
+      for (int n = 0; n < BC / 8; n++) {
+        const double* br = b2 + (n * 8 + g) * CS + kk;
+        dmma(dp[n], x0a, x1a, x2a, x3a, br[t], br[t + 4]);
+      }
+    }
+    // P = exp(scale·s - lse) on allowed pairs, dS = P (dP - D).
+    const long long j0 = (t0 + it) * BC;
+#pragma unroll
+    for (int n = 0; n < BC / 8; n++)
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int c = n * 8 + 2 * t + (i & 1);
+        const long long j = j0 + c;
+        const bool row1 = i >= 2;
+        const bool ok = row1 ? (j >= lo1 && j < hi1) : (j >= lo0 && j < hi0);
+        const double lse = KV ? ld[c] : lse_r[row1];
+        const double dd = KV ? ld[BC + c] : dd_r[row1];
+        const double p = ok ? exp_tang(a.scale * s[n][i] - lse, texp) : 0.0;
+        s[n][i] = p;
+        dp[n][i] = p * (dp[n][i] - dd);
+      }
+    // KV: d_v += P^T·dO (o1), d_k += dS^T·Q (o2); else d_q += dS·K (o1).
+#pragma unroll
+    for (int kk = 0; kk < BC / 8; kk++) {
+      if (KV) {
+        const double* v0 = b2 + (kk * 8 + 2 * t) * CS;
+        const double* v1 = v0 + CS;
+#pragma unroll
+        for (int n = 0; n < 8; n++)
+          if (n * 8 < w2) dmma(o1[n], s[kk][0], s[kk][2], s[kk][1], s[kk][3], v0[n * 8 + g], v1[n * 8 + g]);
+      }
+      const double* k0 = b1 + (kk * 8 + 2 * t) * CS;
+      const double* k1 = k0 + CS;
+#pragma unroll
+      for (int n = 0; n < 8; n++)
+        if (n * 8 < w1) {
+          if (KV) dmma(o2[n], dp[kk][0], dp[kk][2], dp[kk][1], dp[kk][3], k0[n * 8 + g], k1[n * 8 + g]);
+          else dmma(o1[n], dp[kk][0], dp[kk][2], dp[kk][1], dp[kk][3], k0[n * 8 + g], k1[n * 8 + g]);
+        }
+    }
+    __syncthreads();
+  }
+  // Store: rows of this block (zeros for rows that join nothing).
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const int64_t xl = x0 + (h ? r1 : r0);
+    if (xl >= a.lr) continue;
+#pragma unroll
+    for (int n = 0; n < 8; n++)
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int64_t c = n * 8 + 2 * t + e;
+        if (KV) {
+          if (c < a.d2) a.out1[(r_base + xl) * a.d2 + c] = o1[n][2 * h + e];
+          if (c < a.d1) a.out2[(r_base + xl) * a.d1 + c] = a.scale * o2[n][2 * h + e];
+        } else if (c < a.d1) {
+          a.out1[(r_base + xl) * a.d1 + c] = a.scale * o1[n][2 * h + e];
+        }
+      }
+  }
+}
+
 }  // namespace
 
 AttentionOutcome attention_f64_mma(Context& ctx, const AttentionProblem& p, cudaStream_t s) {
   const int64_t W = p.batches, nx = W * p.lnx, nj = W * p.lnj;
-  if (p.ne <= 0 || p.ne > kMaxFeatures || W > 65535 || p.ny <= 0) return ATTENTION_INELIGIBLE;
+  if (p.ne <= 0 || p.ne > kMaxFeatures || W > 65535 || p.ny <= 0 || fp64_tiles_requested()) return ATTENTION_INELIGIBLE;
   if ((p.ny + FY - 1) / FY > 65535) return ATTENTION_INELIGIBLE;
   // Finite q and k (v's finiteness the caller's statistics give): non-finite
   // scores take the FP64 tile kernel, which keeps their NaN and infinity rules.
@@ -400,6 +647,69 @@ AttentionOutcome attention_f64_mma(Context& ctx, const AttentionProblem& p, cuda
   EF_CUDA(cudaStreamSynchronize(s));
   ctx.phase("attention: fp64 mma");
   return (st & 1) ? ATTENTION_GUARDED : ATTENTION_DONE;
+}
+
+}  // namespace ef
+
+namespace ef {
+
+bool backward_f64_mma(Context& ctx, const AttentionGradients& g, const Mask& keys_mask, const double* dd,
+                      cudaStream_t s) {
+  const AttentionProblem& f = g.f;
+  const int64_t W = f.batches;
+  if (f.ne <= 0 || f.ne > 64 || f.ny <= 0 || f.ny > 64 || W > 65535) return false;
+  if (fp64_tiles_requested()) return false;
+  const double scale = f.scale_kind == 1 ? f.scale_c : 1.0;
+  if (f.scale_kind == 2) return false;
+  const size_t smem = (size_t)(2 * BR * RS + 4 * BC * CS + 4 * BC) * sizeof(double);
+  const bool async = f.ne % 2 == 0 && f.ny % 2 == 0 &&
+                     (((uintptr_t)f.q | (uintptr_t)f.k | (uintptr_t)f.v | (uintptr_t)g.d_out) & 15) == 0;
+  F64BwdArgs kv{};
+  kv.a1 = f.k;
+  kv.a2 = f.v;
+  kv.b1 = f.q;
+  kv.b2 = g.d_out;
+  kv.lse = g.lse;
+  kv.dd = dd;
+  kv.out1 = g.d_v;
+  kv.out2 = g.d_k;
+  kv.lr = f.lnj;
+  kv.lc = f.lnx;
+  kv.d1 = f.ne;
+  kv.d2 = f.ny;
+  kv.mask = keys_mask;
+  kv.scale = scale;
+  kv.exp_table = exp_table(ctx.device);
+  kv.keys_rows = 1;
+  F64BwdArgs qa = kv;
+  qa.a1 = f.q;
+  qa.a2 = g.d_out;
+  qa.b1 = f.k;
+  qa.b2 = f.v;
+  qa.out1 = g.d_q;
+  qa.out2 = nullptr;
+  qa.lr = f.lnx;
+  qa.lc = f.lnj;
+  qa.mask = f.mask;
+  qa.keys_rows = 0;
+  auto launch = [&](auto kvtag, auto asynctag, const F64BwdArgs& args) {
+    constexpr bool KVT = decltype(kvtag)::value, AS = decltype(asynctag)::value;
+    EF_CUDA(cudaFuncSetAttribute(attn_bwd_f64<KVT, AS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const dim3 grid((unsigned)((args.lr + BR - 1) / BR), (unsigned)W);
+    if (args.lr > 0) attn_bwd_f64<KVT, AS><<<grid, kBwdThreads, smem, s>>>(args);
+    EF_LAUNCH_CHECK();
+    ctx.kernels++;
+  };
+  if (async) {
+    launch(std::true_type{}, std::true_type{}, kv);
+    launch(std::false_type{}, std::true_type{}, qa);
+  } else {
+    launch(std::true_type{}, std::false_type{}, kv);
+    launch(std::false_type{}, std::false_type{}, qa);
+  }
+  EF_CUDA(cudaStreamSynchronize(s));
+  ctx.phase("attention backward: fp64 mma");
+  return true;
 }
 
 }  // namespace ef

@@ -1301,6 +1301,7 @@ void attention_backward(Context& ctx, const AttentionGradients& g, int precision
     ctx.kernels++;
   }
   if (precision == 0 && backward_split(ctx, g, dd.get(), s)) return;
+  if (backward_f64_mma(ctx, g, transposed(f.mask), dd.get(), s)) return;
   backward_fp64(ctx, g, dd.get(), s);
 }
 

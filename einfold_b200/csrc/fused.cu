@@ -735,16 +735,6 @@ __global__ void emit_rows(int64_t nx, int64_t ny, const uint8_t* __restrict__ fl
   }
 }
 
-// EINFOLD_FP64_TILES=1 keeps attention-shaped pipelines on the FP64 tile
-// kernel (the CUDA cores) instead of the FP64 tensor pipe.
-bool fp64_tiles_forced() {
-  static const bool forced = [] {
-    const char* e = std::getenv("EINFOLD_FP64_TILES");
-    return e && e[0] == '1';
-  }();
-  return forced;
-}
-
 struct Placement {
   int operand;                 // 0 q, 1 k, 2 v
   const std::vector<int>* rows;
@@ -1109,7 +1099,7 @@ FoldOutput fused_pipeline(Context& ctx, const PipelineD& p, const Relation& q, c
   }
   if (!split_done && !pr.row_expr && !p.weight_expr && p.shift == 1 && p.normalizer == 0 && !v_nonfinite &&
       nx > 0 && nj > 0 && ny > 0 && batches_w * mask.lnx == (int64_t)nx && batches_w * mask.lnj == (int64_t)nj &&
-      !fp64_tiles_forced()) {
+      !fp64_tiles_requested()) {
     // The FP64 form on the FP64 tensor pipe, for an attention-shaped
     // pipeline the split form didn't take (precision = fp64, or scores it
     // can't bound).
@@ -1462,7 +1452,7 @@ AttentionOutcome attention_forward(Context& ctx, AttentionProblem p, int precisi
     const AttentionOutcome r = attention_split(ctx, p, slices > 0 ? slices : 6, s);
     if (r != ATTENTION_INELIGIBLE) return r;
   }
-  if (!v_nonfinite && nj > 0 && !fp64_tiles_forced()) {
+  if (!v_nonfinite && nj > 0 && !fp64_tiles_requested()) {
     const AttentionOutcome r = attention_f64_mma(ctx, p, s);
     if (r != ATTENTION_INELIGIBLE) return r;
   }

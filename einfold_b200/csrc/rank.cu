@@ -253,6 +253,9 @@ __global__ void __launch_bounds__(kThreads) chunk_scatter(const uint64_t* __rest
 // stable order, and so every rank, is the chunked passes' exactly.
 
 constexpr uint32_t kFlagAgg = 1u << 30, kFlagPre = 2u << 30, kValue = (1u << 30) - 1;
+// Up to this many keys, the rank array (4 bytes a key) stays in L2 and ranks
+// are scattered straight to their rows.
+constexpr int64_t kScatterInL2 = (int64_t)1 << 22;
 
 __device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) {
   uint32_t v;
@@ -286,22 +289,34 @@ __global__ void __launch_bounds__(kThreads) byte_histograms(const uint64_t* __re
   }
 }
 
+// One pass, one tile of 256·ITEMS keys a block. The tile's keys and row
+// numbers stay in registers (item i of a lane is key warp·32·ITEMS + 32i +
+// lane of the tile). Each warp ranks its items among equal digits in order,
+// item by item: __match_any_sync groups the lanes of a digit, and a per-warp
+// counter of each digit in shared memory gives the group its first place,
+// so a key's place among its warp's equal digits counts every earlier key of
+// the warp. The warps' counters then become offsets (digit by digit, over
+// the warps), a block scan gives each digit's first place in the tile, and
+// the look-back each digit's keys in earlier tiles. The keys are reordered
+// by digit through one shared-memory buffer, a word at a time and then the
+// row numbers, and written out as runs of consecutive destinations.
 template <int W, int ITEMS>
-__global__ void __launch_bounds__(kThreads, 4) onesweep_pass(const uint64_t* __restrict__ kin,
-                                                          const uint32_t* __restrict__ vin,
-                                                          uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
-                                                          int64_t n, int64_t ldi, int64_t ldo, int word, int shift,
-                                                          const uint32_t* __restrict__ digit_start,
-                                                          uint32_t* __restrict__ status,
-                                                          unsigned int* __restrict__ tile_counter, int* err) {
+__global__ void __launch_bounds__(kThreads, 3) onesweep_pass(const uint64_t* __restrict__ kin,
+                                                             const uint32_t* __restrict__ vin,
+                                                             uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                             int64_t n, int64_t ldi, int64_t ldo, int word, int shift,
+                                                             const uint32_t* __restrict__ digit_start,
+                                                             uint32_t* __restrict__ status,
+                                                             unsigned int* __restrict__ tile_counter, int* err) {
   constexpr int TILE = kThreads * ITEMS;
   constexpr int WARPS = kThreads / 32;
-  static_assert(ITEMS <= 8, "a digit's counts of the warp's items fill one 64-bit word");
+  static_assert(TILE <= 65535, "a tile's places fit 16 bits");
   extern __shared__ __align__(16) uint8_t smem[];
-  uint64_t* skeys = (uint64_t*)smem;                  // [W][TILE]
-  uint32_t* svals = (uint32_t*)(smem + TILE * 8 * W);  // [TILE]
-  __shared__ __align__(16) uint64_t counts[WARPS][256];
-  __shared__ long long dbase[256];
+  uint64_t* xbuf = (uint64_t*)smem;               // [TILE]: one word of the reordered keys, or the rows
+  uint8_t* sdig = smem + TILE * 8;                // [TILE]: the reordered keys' digits
+  __shared__ uint16_t wcount[WARPS][256];         // per warp: a digit's keys so far, then its offset
+  __shared__ uint16_t dstart[256];                // a digit's first place in the tile
+  __shared__ long long dbase[256];                // a digit's destination minus its first place
   __shared__ unsigned int s_tile;
   typedef cub::BlockScan<unsigned int, kThreads> Scan;
   __shared__ typename Scan::TempStorage tmp;
@@ -309,7 +324,7 @@ __global__ void __launch_bounds__(kThreads, 4) onesweep_pass(const uint64_t* __r
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
 #pragma unroll
-  for (int i = 0; i < 256 / 32; i++) counts[warp][i * 32 + lane] = 0;
+  for (int d = lane; d < 256; d += 32) wcount[warp][d] = 0;
   __syncthreads();
   const int64_t t = s_tile;
   const int64_t base = t * TILE;
@@ -318,11 +333,11 @@ __global__ void __launch_bounds__(kThreads, 4) onesweep_pass(const uint64_t* __r
 
   uint64_t key[ITEMS][W];
   uint32_t val[ITEMS];
-  int digit[ITEMS];
-  unsigned int local[ITEMS];
+  uint32_t dp[ITEMS];  // digit (bits 16..24; 256: no key) and place among the warp's equal digits (bits 0..15)
 #pragma unroll
   for (int i = 0; i < ITEMS; i++) {
     const int off = warp * 32 * ITEMS + i * 32 + lane;
+    uint32_t d = 256;
     if (off < count) {
 #pragma unroll
       for (int w = 0; w < W; w++) key[i][w] = __ldcs(&kin[(int64_t)w * ldi + base + off]);
@@ -331,36 +346,27 @@ __global__ void __launch_bounds__(kThreads, 4) onesweep_pass(const uint64_t* __r
 #pragma unroll
       for (int w = 1; w < W; w++)
         if (word == w) wd = key[i][w];
-      digit[i] = (int)((wd >> shift) & 255);
-    } else {
-      digit[i] = 256;
+      d = (uint32_t)((wd >> shift) & 255);
     }
+    dp[i] = d << 16;
   }
 #pragma unroll
   for (int i = 0; i < ITEMS; i++) {
-    const int d = digit[i];
+    const uint32_t d = dp[i] >> 16;
     const unsigned peers = __match_any_sync(0xffffffffu, d);
-    const unsigned below = __popc(peers & lt_mask);
-    if (d < 256 && below == 0) ((uint8_t*)&counts[warp][d])[i] = (uint8_t)__popc(peers);
-    local[i] = below;
-  }
-  __syncwarp();
-#pragma unroll
-  for (int i = 0; i < ITEMS; i++) {
-    const int d = digit[i];
-    if (i > 0 && d < 256) {
-      const uint64_t c = counts[warp][d] & ((1ull << (8 * i)) - 1);  // items before i
-      local[i] += (unsigned)__dp4a((int)(uint32_t)c, 0x01010101, __dp4a((int)(uint32_t)(c >> 32), 0x01010101, 0));
-    }
+    const unsigned c = d < 256 ? wcount[warp][d] : 0u;
+    __syncwarp();
+    if (d < 256 && (peers & lt_mask) == 0) wcount[warp][d] = (uint16_t)(c + __popc(peers));
+    dp[i] |= c + __popc(peers & lt_mask);
+    __syncwarp();
   }
   __syncthreads();
   unsigned int total = 0;
 #pragma unroll
   for (int w = 0; w < WARPS; w++) {
-    const uint64_t c = counts[w][tid];
-    const unsigned cnt = (unsigned)__dp4a((int)(uint32_t)c, 0x01010101, __dp4a((int)(uint32_t)(c >> 32), 0x01010101, 0));
-    counts[w][tid] = total;
-    total += cnt;
+    const unsigned c = wcount[w][tid];
+    wcount[w][tid] = (uint16_t)total;
+    total += c;
   }
   // Publish this tile's count of digit `tid`, then look back for the
   // earlier tiles' (thread tid owns digit tid).
@@ -392,28 +398,36 @@ __global__ void __launch_bounds__(kThreads, 4) onesweep_pass(const uint64_t* __r
     if (failed) atomicOr(err, 1);
     st_volatile(my, kFlagPre | (before + total));
   }
-#pragma unroll
-  for (int w = 0; w < WARPS; w++) counts[w][tid] += ex;
+  dstart[tid] = (uint16_t)ex;
   dbase[tid] = (long long)digit_start[tid] + (long long)before - (long long)ex;
   __syncthreads();
+  // Each item's place in the reordered tile.
 #pragma unroll
   for (int i = 0; i < ITEMS; i++) {
-    const int d = digit[i];
+    const uint32_t d = dp[i] >> 16;
     if (d < 256) {
-      const unsigned pos = (unsigned)counts[warp][d] + local[i];
-#pragma unroll
-      for (int w = 0; w < W; w++) skeys[w * TILE + pos] = key[i][w];
-      svals[pos] = val[i];
+      const uint32_t pos = (uint32_t)dstart[d] + wcount[warp][d] + (dp[i] & 0xffffu);
+      dp[i] = (d << 16) | pos;
+      sdig[pos] = (uint8_t)d;
     }
   }
-  __syncthreads();
-  for (int j = tid; j < count; j += kThreads) {
-    const uint64_t wd = skeys[word * TILE + j];
-    const int d = (int)((wd >> shift) & 255);
-    const long long dst = dbase[d] + j;
 #pragma unroll
-    for (int w = 0; w < W; w++) __stcs(&kout[(int64_t)w * ldo + dst], skeys[w * TILE + j]);
-    __stcs(&vout[dst], svals[j]);
+  for (int w = 0; w <= W; w++) {
+    // Word w of the keys (w < W), then the rows, through the one buffer.
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++)
+      if ((dp[i] >> 16) < 256) {
+        const uint32_t pos = dp[i] & 0xffffu;
+        if (w < W) xbuf[pos] = key[i][w];
+        else ((uint32_t*)xbuf)[pos] = val[i];
+      }
+    __syncthreads();
+    for (int j = tid; j < count; j += kThreads) {
+      const long long dst = dbase[sdig[j]] + j;
+      if (w < W) __stcs(&kout[(int64_t)w * ldo + dst], xbuf[j]);
+      else __stcs(&vout[dst], ((const uint32_t*)xbuf)[j]);
+    }
+    __syncthreads();
   }
 }
 
@@ -511,6 +525,167 @@ __global__ void __launch_bounds__(kThreads) rank_runs(const uint64_t* __restrict
   }
 }
 
+// The ranks of the sorted pairs when the rank array is too large for L2:
+// each tile of 2048 sorted positions (claimed in order) finds its keys' run
+// heads and ranks (a look-back over the earlier tiles' head counts gives its
+// first rank), writes first[r] for its heads, and partitions its (row, rank)
+// pairs by bucket = row >> bshift, each bucket's pairs of all tiles in one
+// contiguous region (bucket b holds exactly the rows [b << bshift, (b + 1)
+// << bshift) of the n, so its region's start is known; a look-back over the
+// earlier tiles' bucket counts gives this tile's place in it). The order of
+// pairs within a bucket is of no consequence: scatter_ranks then writes
+// rank[row] for each pair, and the pairs of one bucket, read in order, fall
+// in one rank range of 2^bshift rows that stays in L2 while it is written.
+constexpr int kBuckets = 256;
+constexpr int kPartItems = 8;
+constexpr int kPartTile = kThreads * kPartItems;
+
+template <int W>
+__global__ void __launch_bounds__(kThreads) rank_partition(const uint64_t* __restrict__ keys, int64_t ld,
+                                                           const uint32_t* __restrict__ rows, int64_t n, int bshift,
+                                                           uint32_t* __restrict__ head_status,
+                                                           uint32_t* __restrict__ bucket_status,
+                                                           unsigned int* __restrict__ tile_counter,
+                                                           uint64_t* __restrict__ pairs, uint32_t* __restrict__ first,
+                                                           unsigned long long* __restrict__ distinct, int* err) {
+  typedef cub::BlockScan<unsigned int, kThreads> Scan;
+  __shared__ typename Scan::TempStorage tmp;
+  __shared__ unsigned int s_tile, s_before;
+  __shared__ unsigned int cnt[kBuckets];      // this tile's pairs of each bucket
+  __shared__ unsigned int at[kBuckets];       // a bucket's next slot in the tile's reordered pairs
+  __shared__ long long dbase[kBuckets];       // a bucket's destination minus its first slot in the tile
+  __shared__ __align__(16) uint64_t spairs[kPartTile];
+  const int tid = threadIdx.x;
+  if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
+  cnt[tid] = 0;
+  __syncthreads();
+  const int64_t t = s_tile;
+  const int64_t base = t * kPartTile;
+  const int64_t count = min((int64_t)kPartTile, n - base);
+  const int64_t p0 = base + (int64_t)tid * kPartItems;
+  unsigned int heads = 0, hmask = 0;
+  uint32_t r[kPartItems];
+  {
+    uint64_t prev[W];
+#pragma unroll
+    for (int w = 0; w < W; w++) prev[w] = p0 > 0 && p0 - 1 < n ? keys[(int64_t)w * ld + p0 - 1] : 0;
+#pragma unroll
+    for (int i = 0; i < kPartItems; i++) {
+      const int64_t p = p0 + i;
+      if (p < n) {
+        bool h = p == 0;
+#pragma unroll
+        for (int w = 0; w < W; w++) {
+          const uint64_t k = keys[(int64_t)w * ld + p];
+          h |= k != prev[w];
+          prev[w] = k;
+        }
+        r[i] = rows[p];
+        if (h) {
+          hmask |= 1u << i;
+          heads++;
+        }
+      }
+    }
+  }
+  unsigned int ex, total;
+  Scan(tmp).ExclusiveSum(heads, ex, total);
+  // The heads before this tile: a look-back over the earlier tiles' counts.
+  if (tid == 0) {
+    uint32_t* my = head_status + t;
+    unsigned int before = 0;
+    if (t == 0) {
+      st_volatile(my, kFlagPre | total);
+    } else {
+      st_volatile(my, kFlagAgg | total);
+      int64_t tt = t - 1;
+      uint64_t start = 0;
+      while (true) {
+        const uint32_t v = ld_volatile(head_status + tt);
+        const uint32_t flag = v & ~kValue;
+        if (flag == 0) {
+          if (!start) start = ptx::now_ns();
+          else if (ptx::now_ns() - start > ptx::kWaitNs) {
+            atomicOr(err, 1);
+            break;
+          }
+          continue;
+        }
+        before += v & kValue;
+        if (flag == kFlagPre || tt == 0) break;
+        tt--;
+      }
+      st_volatile(my, kFlagPre | (before + total));
+    }
+    s_before = before;
+    if (base + kPartTile >= n) *distinct = (unsigned long long)(before + total);
+  }
+  __syncthreads();
+  // Ranks; first rows; the pairs' bucket counts.
+  unsigned int cur = s_before + ex;
+  uint64_t pr[kPartItems];
+  unsigned int slot[kPartItems];
+#pragma unroll
+  for (int i = 0; i < kPartItems; i++) {
+    if (p0 + i < n) {
+      if (hmask >> i & 1u) {
+        first[cur] = r[i];
+        cur++;
+      }
+      pr[i] = ((uint64_t)r[i] << 32) | (cur - 1);
+      slot[i] = atomicAdd(&cnt[r[i] >> bshift], 1u);
+    }
+  }
+  __syncthreads();
+  const unsigned int mine = cnt[tid];
+  const int64_t bucket_rows = (int64_t)1 << bshift;
+  uint32_t* bst = bucket_status + t * kBuckets + tid;
+  if (t == 0) st_volatile(bst, kFlagPre | mine);
+  else st_volatile(bst, kFlagAgg | mine);
+  unsigned int bex;
+  Scan(tmp).ExclusiveSum(mine, bex);
+  unsigned int bbefore = 0;
+  if (t > 0) {
+    int64_t tt = t - 1;
+    uint64_t start = 0;
+    while (true) {
+      const uint32_t v = ld_volatile(bucket_status + tt * kBuckets + tid);
+      const uint32_t flag = v & ~kValue;
+      if (flag == 0) {
+        if (!start) start = ptx::now_ns();
+        else if (ptx::now_ns() - start > ptx::kWaitNs) {
+          atomicOr(err, 1);
+          break;
+        }
+        continue;
+      }
+      bbefore += v & kValue;
+      if (flag == kFlagPre || tt == 0) break;
+      tt--;
+    }
+    st_volatile(bst, kFlagPre | (bbefore + mine));
+  }
+  at[tid] = bex;
+  dbase[tid] = (long long)tid * bucket_rows + (long long)bbefore - (long long)bex;
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < kPartItems; i++)
+    if (p0 + i < n) spairs[at[(uint32_t)(pr[i] >> 32) >> bshift] + slot[i]] = pr[i];
+  __syncthreads();
+  for (int j = tid; j < count; j += kThreads) {
+    const uint64_t x = spairs[j];
+    const int b = (int)((uint32_t)(x >> 32) >> bshift);
+    __stcs(&pairs[dbase[b] + j], x);
+  }
+}
+
+__global__ void scatter_ranks(const uint64_t* __restrict__ pairs, int64_t n, uint32_t* __restrict__ rank) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t x = __ldcs(&pairs[i]);
+    rank[(uint32_t)(x >> 32)] = (uint32_t)x;
+  }
+}
+
 template <int W>
 __global__ void head_flags(const uint64_t* __restrict__ keys, int64_t n, int64_t ld, uint8_t* __restrict__ head) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -569,7 +744,7 @@ void radix_pass(Context& ctx, const uint64_t* kin, int64_t ldi, const uint32_t* 
 template <int W>
 int64_t rank_keys_onesweep(Context& ctx, const uint64_t* keys, int64_t n, int64_t ld, uint32_t* rank,
                            uint32_t* first, cudaStream_t s, uint32_t* sorted_rows) {
-  constexpr int ITEMS = W == 1 ? 8 : (W == 2 ? 6 : 4);
+  constexpr int ITEMS = W == 1 ? 12 : (W == 2 ? 8 : (W == 3 ? 6 : 4));
   constexpr int TILE = kThreads * ITEMS;
   constexpr int RITEMS = 8;
   constexpr int RTILE = kThreads * RITEMS;
@@ -606,7 +781,7 @@ int64_t rank_keys_onesweep(Context& ctx, const uint64_t* keys, int64_t n, int64_
   const int passes = (int)pw.size();
   DeviceBuffer<uint32_t> dstart((size_t)std::max(1, passes) * 256, s);
   if (passes) EF_CUDA(cudaMemcpyAsync(dstart.get(), starts.data(), starts.size() * 4, cudaMemcpyHostToDevice, s));
-  const int64_t status_words = std::max(tiles * 256, rtiles);
+  const int64_t status_words = std::max(tiles * 256, std::max(rtiles, (n + kPartTile - 1) / kPartTile));
   DeviceBuffer<uint32_t> status((size_t)status_words, s);
   DeviceBuffer<unsigned int> counters((size_t)passes + 1, s);
   counters.zero();
@@ -617,7 +792,7 @@ int64_t rank_keys_onesweep(Context& ctx, const uint64_t* keys, int64_t n, int64_
   const uint64_t* cur_k = keys;
   int64_t cur_ld = ld;
   const uint32_t* cur_v = nullptr;
-  const size_t smem = (size_t)TILE * (8 * W + 4);
+  const size_t smem = (size_t)TILE * (8 + 1);
   if (passes) {
     const int64_t ldb = (n + 1) & ~(int64_t)1;
     for (int b = 0; b < 2; b++) {
@@ -645,10 +820,26 @@ int64_t rank_keys_onesweep(Context& ctx, const uint64_t* keys, int64_t n, int64_
   }
   DeviceBuffer<unsigned long long> distinct(1, s);
   EF_CUDA(cudaMemsetAsync(status.get(), 0, (size_t)rtiles * 4, s));
-  rank_runs<W, RITEMS><<<(unsigned)rtiles, kThreads, 0, s>>>(cur_k, cur_ld, cur_v, n, status.get(),
-                                                             counters.get() + passes, rank, first, distinct.get(),
-                                                             err.get());
-  ctx.kernels++;
+  if (n <= kScatterInL2) {
+    // The rank array fits in L2: its scattered writes merge there.
+    rank_runs<W, RITEMS><<<(unsigned)rtiles, kThreads, 0, s>>>(cur_k, cur_ld, cur_v, n, status.get(),
+                                                               counters.get() + passes, rank, first, distinct.get(),
+                                                               err.get());
+    ctx.kernels++;
+  } else {
+    // Ranks partitioned by the rows' high bits, then scattered bucket by bucket.
+    int bshift = 0;
+    while ((((int64_t)1 << bshift) * kBuckets) < n) bshift++;
+    const int64_t ptiles = (n + kPartTile - 1) / kPartTile;
+    DeviceBuffer<uint32_t> bstatus((size_t)(ptiles * kBuckets), s);
+    DeviceBuffer<uint64_t> pairs((size_t)n, s);
+    EF_CUDA(cudaMemsetAsync(bstatus.get(), 0, (size_t)(ptiles * kBuckets) * 4, s));
+    rank_partition<W><<<(unsigned)ptiles, kThreads, 0, s>>>(cur_k, cur_ld, cur_v, n, bshift, status.get(),
+                                                            bstatus.get(), counters.get() + passes, pairs.get(),
+                                                            first, distinct.get(), err.get());
+    scatter_ranks<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, s>>>(pairs.get(), n, rank);
+    ctx.kernels += 2;
+  }
   EF_LAUNCH_CHECK();
   if (sorted_rows) EF_CUDA(cudaMemcpyAsync(sorted_rows, cur_v, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
   unsigned long long k = 0;

@@ -107,3 +107,28 @@ def test_fp64_and_split_forms_agree_and_both_guard_an_underflow():
                                            out.data_ptr(), None, 1, 64, 64, 8, 8, 0, None, None, 1.0, precision, 0,
                                            ctypes.c_void_p(1), None)  # stream 1: cudaStreamLegacy
         assert st == _lib.DECLINED
+
+
+@pytest.mark.parametrize("shape", [(2, 200, 64, 64, "causal"), (3, 77, 3, 5, "window"), (2, 130, 64, 40, "ragged")])
+def test_fp64_tensor_pipe_backward_matches_torch(shape):
+    # The FP64 backward (keys-as-rows and queries-as-rows kernels on the FP64
+    # tensor pipe) against torch float64 autograd of the same attention.
+    w, l, d, dv, kind = shape
+    g = torch.Generator(device="cuda").manual_seed(l)
+    q = torch.randn(w, l, d, dtype=torch.float64, device="cuda", generator=g) * 0.3
+    k = torch.randn(w, l, d, dtype=torch.float64, device="cuda", generator=g) * 0.3
+    v = torch.randn(w, l, dv, dtype=torch.float64, device="cuda", generator=g)
+    d_out = torch.randn(w, l, dv, dtype=torch.float64, device="cuda", generator=g)
+    cond = A.causal() if kind == "causal" else A.window(9)
+    lengths = torch.tensor([l, 57][:w], dtype=torch.int64, device="cuda") if kind == "ragged" else None
+    if lengths is not None:
+        pos = torch.arange(l, device="cuda")[None, :, None] < lengths[:, None, None]
+        q, k, v, d_out = q * pos, k * pos, v * pos, d_out * pos
+    out, lse = A.attention_forward(q, k, v, cond, 1.0, Precision.FP64, q_lengths=lengths, k_lengths=lengths)
+    dq, dk, dvv = A.attention_backward(q, k, v, out, lse, d_out, cond, 1.0, Precision.FP64, q_lengths=lengths,
+                                       k_lengths=lengths)
+    qr, kr, vr = (t.clone().requires_grad_(True) for t in (q, k, v))
+    want, some = _reference(qr, kr, vr, cond, 1.0, lengths, lengths)
+    gq, gk, gv = torch.autograd.grad(want, (qr, kr, vr), d_out * some)
+    for got, ref in ((dq, gq), (dk, gk), (dvv, gv)):
+        assert (got - ref).abs().max().item() <= 1e-11 * max(ref.abs().max().item(), 1e-300)
