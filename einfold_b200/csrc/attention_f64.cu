@@ -523,9 +523,11 @@ __global__ void __launch_bounds__(kBwdThreads, 1) attn_bwd_f64(const F64BwdArgs 
         const bool ok = row1 ? (j >= lo1 && j < hi1) : (j >= lo0 && j < hi0);
         const double lse = KV ? ld[c] : lse_r[row1];
         const double dd = KV ? ld[BC + c] : dd_r[row1];
+        // Pairs outside the mask weigh nothing, whatever lse and D hold there
+        // (rows that join no key have neither).
         const double p = ok ? exp_tang(a.scale * s[n][i] - lse, texp) : 0.0;
         s[n][i] = p;
-        dp[n][i] = p * (dp[n][i] - dd);
+        dp[n][i] = ok ? p * (dp[n][i] - dd) : 0.0;
       }
     // KV: d_v += P^T·dO (o1), d_k += dS^T·Q (o2); else d_q += dS·K (o1).
 #pragma unroll
