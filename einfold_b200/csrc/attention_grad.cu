@@ -87,15 +87,23 @@ struct GradArgs {
   unsigned long long* tiles;
   int w0;  // the first batch of this launch (blockIdx.y counts from it)
   int reverse;  // row blocks from the last one (whose rows join the most columns) down
-  // The d_k kernel's exports for the tile kernels (null: none), indexed by
-  // the launch's own batches: P's digit tiles as the d_v kernel cuts them,
-  // [batch][row block][column tile][S][128 rows][64 B] in the MMA's 64-byte
-  // swizzle, with their rows' powers of two [tile][128]; and dS, query-major,
-  // [batch][lq_pad][lk_pad].
+  // The d_k kernel's exports for the tile kernels (null: none), only for
+  // the tiles some pair of is allowed: P's digit tiles as the d_v kernel cuts
+  // them, [tile][S][128 rows][64 B] in the MMA's 64-byte swizzle, with their
+  // rows' powers of two [tile][128], a key block's tiles from p_off[batch ·
+  // n_rb + block] - p_base on, one a query tile it joins; and dS in tiles of
+  // 128 queries by 64 keys, [tile][128][64], a query block's from
+  // dq_off[batch · n_qb + block] - dq_base on, one a key tile from
+  // dq_ct0[...] on (dq_n of them). Batches count from the launch's first.
   uint8_t* p_tiles;
   int32_t* p_exp;
   double* ds_out;
-  int64_t n_rb, n_ct;  // row blocks and column tiles of a batch
+  const int64_t* p_off;
+  const int64_t* dq_off;
+  const int32_t* dq_ct0;
+  const int32_t* dq_n;
+  int64_t p_base, dq_base;
+  int64_t n_rb, n_qb;  // key blocks and query blocks of a batch
 };
 
 constexpr int kPTile = S * GM * 64;  // bytes of one tile of weight digits
@@ -338,10 +346,17 @@ __global__ void __launch_bounds__(kGradThreads, 1)
         }
       }
       if (kTwo) {
-        // d_k's export of dS: column c (a query) of this tile, the rows' keys contiguous.
-        double* ds_col = (MODE == GRAD_K && a.ds_out)
-                             ? a.ds_out + ((int64_t)blockIdx.y * a.lc_pad + cl0) * a.lr_pad + (int64_t)rt * GM + r
-                             : nullptr;
+        // d_k's export of dS: into the d_q kernel's tile of this tile's query
+        // block and the row's key tile, row (query) cl0 + c, the keys
+        // contiguous; nothing for a key tile the query block's rows don't join
+        // (every pair there is masked).
+        double* ds_col = nullptr;
+        if (MODE == GRAD_K && a.ds_out) {
+          const int64_t qbi = (int64_t)blockIdx.y * a.n_qb + cl0 / GM;
+          const int64_t kt = ((int64_t)rt * GM + r) / GJ - a.dq_ct0[qbi];
+          if (kt >= 0 && kt < a.dq_n[qbi])
+            ds_col = a.ds_out + ((a.dq_off[qbi] - a.dq_base + kt) * GM + cl0 % GM) * GJ + r % GJ;
+        }
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(t1_free);
@@ -358,7 +373,7 @@ __global__ void __launch_bounds__(kGradThreads, 1)
           ep = ep == INT_MIN ? 0 : ep;
           const int shift = 8 * S - ep;
           const double f1 = pow2(shift >> 1), f2 = pow2(shift - (shift >> 1));
-          const int64_t tile = ((int64_t)blockIdx.y * a.n_rb + rt) * a.n_ct + (ct0 + it);
+          const int64_t tile = a.p_off[(int64_t)blockIdx.y * a.n_rb + rt] - a.p_base + it;
           uint8_t* dst = a.p_tiles + tile * kPTile + sw64_offset((uint32_t)r, (uint32_t)(h * CW));
           uint32_t chunk[S][4];
 #pragma unroll
@@ -391,7 +406,7 @@ __global__ void __launch_bounds__(kGradThreads, 1)
             const double dp = FAST ? l * pow2(e2r + es[GJ + c]) : scale2(l, e2r + es[GJ + c]);
             const double t = wv[c] * (dp - (MODE == GRAD_Q ? dd_r : ls[GJ + c]));
             wv[c] = wv[c] != 0.0 ? t : 0.0;
-            if (ds_col) ds_col[(int64_t)c * a.lr_pad] = wv[c];
+            if (ds_col) ds_col[(int64_t)c * GJ] = wv[c];
           }
         }
       }
@@ -589,7 +604,11 @@ __global__ void __launch_bounds__(kGradThreads, 1)
   const int ct0 = first < last ? (int)(first / GJ) : 0;
   const int n_tiles = first < last ? (int)((last + GJ - 1) / GJ) - ct0 : 0;
   if (threadIdx.x == 0 && n_tiles > 0) atomicAdd(a.tiles, (unsigned long long)n_tiles);
-  auto tile_of = [&](int it) { return ((int64_t)blockIdx.y * a.n_rb + rt) * a.n_ct + (ct0 + it); };
+  // d_v: this key block's P tiles; d_q: this query block's dS tiles.
+  auto tile_of = [&](int it) {
+    return kQ ? a.dq_off[(int64_t)blockIdx.y * a.n_qb + rt] - a.dq_base + it
+              : a.p_off[(int64_t)blockIdx.y * a.n_rb + rt] - a.p_base + it;
+  };
 
   if (warp == 0) {
     if (lane == 0 && n_tiles > 0) {
@@ -608,8 +627,8 @@ __global__ void __launch_bounds__(kGradThreads, 1)
           if (ok) {
             mbar_expect_tx(&ds_full[st], (uint32_t)Sh::kDs);
             for (int j = 0; j < 4; j++)
-              tma_load_3d(sDs + st * Sh::kDs + j * GM * 128, &tds, &ds_full[st], cl0 + 16 * j, rt * GM,
-                          (int)blockIdx.y);
+              tma_load_3d(sDs + st * Sh::kDs + j * GM * 128, &tds, &ds_full[st], 16 * j, (int)(tile_of(it) * GM),
+                          0);
           }
           ok = ok && (it == 0 || mbar_wait(&kv_empty[0], (uint32_t)((it - 1) & 1)));
           if (ok) {
@@ -938,6 +957,30 @@ inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 // Whether a batch's last rows join more columns than its first (causal
 // queries do; causal keys as rows the other way round): the blocks with the
 // most work then go first.
+// Per block of 128 rows of each batch: the first column tile of 64 its rows
+// may pair with and how many, as the backward kernels find them (the span
+// of the rows' allowed intervals).
+__global__ void export_plan(Mask m, int64_t lr, int64_t lc, int64_t batches, int64_t blocks, int32_t* __restrict__ ct0,
+                            int32_t* __restrict__ n) {
+  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < batches * blocks;
+       x += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t w = x / blocks, b = x - w * blocks;
+    long long first = LLONG_MAX, last = LLONG_MIN;
+    for (int64_t r = b * GM; r < min(lr, b * GM + GM); r++) {
+      int64_t lo, hi;
+      allowed(m, w * lr + r, lo, hi);
+      lo -= w * lc;
+      hi -= w * lc;
+      if (lo < hi) {
+        first = min(first, (long long)lo);
+        last = max(last, (long long)hi);
+      }
+    }
+    ct0[x] = first < last ? (int32_t)(first / GJ) : 0;
+    n[x] = first < last ? (int32_t)((last + GJ - 1) / GJ - first / GJ) : 0;
+  }
+}
+
 bool last_rows_longest(Mask m, int64_t rows) {
   if (rows <= 0) return true;
   m.xlen = m.jlen = nullptr;
@@ -1143,72 +1186,121 @@ bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd,
     a.dy_pad = 64;
     a.y0 = 0;
     a.n_rb = a.lr_pad / GM;
-    a.n_ct = a.lc_pad / GJ;
     a.reverse = last_rows_longest(a.mask, a.lr);
   }
   // The tile path: d_k first, exporting P's digits and dS; then d_v and d_q
-  // from them, one product a tile each. The exports take 14 bytes a pair of
-  // a batch's padded square, so batches go in chunks whose exports fit the
-  // export limit (EINFOLD_BACKWARD_EXPORT_MB, 2048 by default), in two
-  // buffers: chunks alternate between the call's stream and the context's
-  // second stream, so that one chunk's kernels run beside the other's and a
-  // chunk's last wave of blocks leaves no SM idle. The buffers are freed at
-  // the end of the call. A batch whose exports alone exceed half the limit
-  // takes the three kernels that each recompute the scores.
-  const int64_t n_kb = lk_pad / GM, n_qt = lq_pad / GJ;
-  const size_t p_bytes = al((size_t)(lk_pad * lq_pad * S)), ds_bytes = al((size_t)(lk_pad * lq_pad) * 8),
-               pe_bytes = al((size_t)(n_kb * n_qt * GM) * 4);
-  const size_t per_batch = p_bytes + ds_bytes + pe_bytes;
+  // from them, one product a tile each. The exports cover only the tiles
+  // some pair of is allowed (export_plan counts them per block), 14 bytes a
+  // pair of those. Batches go in chunks whose exports fit the export limit
+  // (EINFOLD_BACKWARD_EXPORT_MB, 8192 by default): all in one when they fit,
+  // else in chunks of at most half of it in two buffers, the chunks
+  // alternating between the call's stream and the context's second stream,
+  // so that one chunk's kernels run beside the other's and a chunk's last
+  // wave of blocks leaves no SM idle. The buffers are freed at the end of
+  // the call. A batch whose exports alone exceed half the limit takes the
+  // three kernels that each recompute the scores.
+  const int64_t n_kb = lk_pad / GM, n_qb = lq_pad / GM;
   static const size_t limit = [] {
     const char* e = std::getenv("EINFOLD_BACKWARD_EXPORT_MB");
-    const long long mb = e ? std::atoll(e) : 2048;
+    const long long mb = e ? std::atoll(e) : 8192;
     return (size_t)std::max(0ll, mb) << 20;
   }();
-  int64_t chunk = 0, buffers = 1;
-  if ((size_t)W * per_batch <= limit) {
-    chunk = W;
+  DeviceBuffer<int32_t> plan((size_t)(2 * W * (n_kb + n_qb)), s);
+  int32_t* pk_ct0 = plan.get();
+  int32_t* pk_n = pk_ct0 + W * n_kb;
+  int32_t* pq_ct0 = pk_n + W * n_kb;
+  int32_t* pq_n = pq_ct0 + W * n_qb;
+  export_plan<<<blocks_for((uint64_t)(W * n_kb), 128), 128, 0, s>>>(keys_mask, lk, lq, W, n_kb, pk_ct0, pk_n);
+  export_plan<<<blocks_for((uint64_t)(W * n_qb), 128), 128, 0, s>>>(f.mask, lq, lk, W, n_qb, pq_ct0, pq_n);
+  ctx.kernels += 2;
+  EF_LAUNCH_CHECK();
+  std::vector<int32_t> hk_n((size_t)(W * n_kb)), hq_n((size_t)(W * n_qb));
+  EF_CUDA(cudaMemcpyAsync(hk_n.data(), pk_n, hk_n.size() * 4, cudaMemcpyDeviceToHost, s));
+  EF_CUDA(cudaMemcpyAsync(hq_n.data(), pq_n, hq_n.size() * 4, cudaMemcpyDeviceToHost, s));
+  EF_CUDA(cudaStreamSynchronize(s));
+  // Each block's first tile (exclusive over all batches), and each batch's tiles.
+  std::vector<int64_t> hp_off((size_t)(W * n_kb) + 1), hq_off((size_t)(W * n_qb) + 1);
+  for (size_t x = 0; x < hk_n.size(); x++) hp_off[x + 1] = hp_off[x] + hk_n[x];
+  for (size_t x = 0; x < hq_n.size(); x++) hq_off[x + 1] = hq_off[x] + hq_n[x];
+  constexpr size_t kPBytes = (size_t)kPTile + GM * 4, kDsBytes = (size_t)GM * GJ * 8;
+  auto bytes_of = [&](int64_t w0, int64_t w1) {
+    const int64_t np = hp_off[(size_t)(w1 * n_kb)] - hp_off[(size_t)(w0 * n_kb)];
+    const int64_t nq = hq_off[(size_t)(w1 * n_qb)] - hq_off[(size_t)(w0 * n_qb)];
+    return al((size_t)np * kPTile) + al((size_t)np * GM * 4) + (size_t)nq * kDsBytes;
+  };
+  std::vector<std::pair<int64_t, int64_t>> chunks;
+  int buffers = 1;
+  if (bytes_of(0, W) <= limit) {
+    chunks.push_back({0, W});
   } else {
-    chunk = std::min<int64_t>(W, (int64_t)(limit / 2 / per_batch));
     buffers = 2;
+    int64_t w0 = 0;
+    while (w0 < W) {
+      if (bytes_of(w0, w0 + 1) > limit / 2) {
+        chunks.clear();
+        break;
+      }
+      int64_t w1 = w0 + 1;
+      while (w1 < W && bytes_of(w0, w1 + 1) <= limit / 2) w1++;
+      chunks.push_back({w0, w1});
+      w0 = w1;
+    }
   }
+  (void)kPBytes;
+  DeviceBuffer<int64_t> offs;
+  if (!chunks.empty()) {
+    offs.allocate(hp_off.size() + hq_off.size(), s);
+    EF_CUDA(cudaMemcpyAsync(offs.get(), hp_off.data(), hp_off.size() * 8, cudaMemcpyHostToDevice, s));
+    EF_CUDA(cudaMemcpyAsync(offs.get() + hp_off.size(), hq_off.data(), hq_off.size() * 8, cudaMemcpyHostToDevice, s));
+  }
+  const int64_t* p_off = offs.get();
+  const int64_t* q_off = offs.get() + hp_off.size();
   DeviceBuffer<uint8_t> exports[2];
   cudaStream_t streams[2] = {s, s};
   cudaEvent_t e0, e1, joined = nullptr;
   EF_CUDA(cudaEventCreate(&e0));
   EF_CUDA(cudaEventCreate(&e1));
   EF_CUDA(cudaEventRecord(e0, s));
-  if (chunk >= 1 && buffers == 2) {
+  if (!chunks.empty() && buffers == 2) {
     if (!ctx.aux) EF_CUDA(cudaStreamCreateWithFlags(&ctx.aux, cudaStreamNonBlocking));
     streams[1] = ctx.aux;
     EF_CUDA(cudaEventCreateWithFlags(&joined, cudaEventDisableTiming));
     EF_CUDA(cudaEventRecord(joined, s));  // the slicing above, before the second stream starts
     EF_CUDA(cudaStreamWaitEvent(ctx.aux, joined, 0));
   }
-  if (chunk >= 1) {
-    CUtensorMap tds[2];
-    double* ds[2] = {};
-    int32_t* p_exp[2] = {};
-    uint8_t* p_tiles[2] = {};
-    for (int b = 0; b < buffers; b++) {
-      exports[b].allocate((size_t)chunk * per_batch, streams[b]);
-      p_tiles[b] = exports[b].get();
-      ds[b] = (double*)(p_tiles[b] + (size_t)chunk * p_bytes);
-      p_exp[b] = (int32_t*)((uint8_t*)ds[b] + (size_t)chunk * ds_bytes);
-      tds[b] = f64_boxes_map(ds[b], lk_pad, lq_pad, chunk, 16, GM);
-    }
-    int c = 0;
-    for (int64_t w0 = 0; w0 < W; w0 += chunk, c++) {
-      const int b = c % buffers;
+  if (!chunks.empty()) {
+    size_t biggest = 0;
+    for (auto& c : chunks) biggest = std::max(biggest, bytes_of(c.first, c.second));
+    for (int b = 0; b < buffers; b++) exports[b].allocate(std::max<size_t>(biggest, 256), streams[b]);
+    for (size_t c = 0; c < chunks.size(); c++) {
+      const int b = (int)(c % (size_t)buffers);
       cudaStream_t st = streams[b];
-      const unsigned wc = (unsigned)std::min<int64_t>(chunk, W - w0);
+      const int64_t w0 = chunks[c].first, w1 = chunks[c].second;
+      const int64_t np = hp_off[(size_t)(w1 * n_kb)] - hp_off[(size_t)(w0 * n_kb)];
+      const int64_t nq = hq_off[(size_t)(w1 * n_qb)] - hq_off[(size_t)(w0 * n_qb)];
+      uint8_t* p_tiles = exports[b].get();
+      int32_t* p_exp = (int32_t*)(p_tiles + al((size_t)np * kPTile));
+      double* ds = (double*)((uint8_t*)p_exp + al((size_t)np * GM * 4));
+      const CUtensorMap tds = f64_boxes_map(ds, GJ, std::max<int64_t>(nq, 1) * GM, 1, 16, GM);
+      const unsigned wc = (unsigned)(w1 - w0);
       GradArgs k = args[GRAD_K], v = args[GRAD_V], q = args[GRAD_Q];
-      k.w0 = v.w0 = q.w0 = (int)w0;
-      k.p_tiles = v.p_tiles = p_tiles[b];
-      k.p_exp = v.p_exp = p_exp[b];
-      k.ds_out = ds[b];
+      for (GradArgs* g2 : {&k, &v, &q}) {
+        g2->w0 = (int)w0;
+        g2->p_tiles = p_tiles;
+        g2->p_exp = p_exp;
+        g2->p_off = p_off + w0 * n_kb;
+        g2->p_base = hp_off[(size_t)(w0 * n_kb)];
+        g2->dq_off = q_off + w0 * n_qb;
+        g2->dq_ct0 = pq_ct0 + w0 * n_qb;
+        g2->dq_n = pq_n + w0 * n_qb;
+        g2->dq_base = hq_off[(size_t)(w0 * n_qb)];
+        g2->n_rb = n_kb;
+        g2->n_qb = n_qb;
+      }
+      k.ds_out = ds;
       launch_split<GRAD_K>(mode_maps[GRAD_K], k, dim3((unsigned)n_kb, wc), fast, st);
-      launch_tiles<GRAD_V>(tds[b], mode_maps[GRAD_V][4], v, dim3((unsigned)n_kb, wc), st);
-      launch_tiles<GRAD_Q>(tds[b], mode_maps[GRAD_Q][4], q, dim3((unsigned)(lq_pad / GM), wc), st);
+      launch_tiles<GRAD_V>(tds, mode_maps[GRAD_V][4], v, dim3((unsigned)n_kb, wc), st);
+      launch_tiles<GRAD_Q>(tds, mode_maps[GRAD_Q][4], q, dim3((unsigned)n_qb, wc), st);
       ctx.kernels += 3;
     }
     if (joined) {
@@ -1224,6 +1316,7 @@ bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd,
       ctx.kernels++;
     }
   }
+  const int64_t chunk = chunks.empty() ? 0 : 1;
   EF_CUDA(cudaEventRecord(e1, s));
   unsigned long long pairs[3] = {};
   EF_CUDA(cudaMemcpyAsync(&st, status + 1, 4, cudaMemcpyDeviceToHost, s));

@@ -1,5 +1,6 @@
 """The split attention backward under an export limit: batches go in chunks
-whose exports (P's digits and dS) fit EINFOLD_BACKWARD_EXPORT_MB, alternating
+whose exports (P's digits and dS, for the allowed tiles only) fit
+EINFOLD_BACKWARD_EXPORT_MB, alternating
 between two streams, and give the same bits as one chunk of every batch; a
 limit below one batch's exports takes the kernels that recompute the scores,
 with the same bits again (same digits, scales and order of summation)."""
@@ -45,12 +46,13 @@ def _grads(tmp_path, limit_mb):
 
 
 def test_chunked_exports_give_the_same_bits(tmp_path):
-    # A batch's exports at T = 1024: 1024² · 14 bytes, about 14 MB; 12 batches
-    # in one chunk by default, 2 a chunk (two buffers of 2) under 60 MB, and
-    # the recomputing kernels under 16 MB.
+    # A batch's exports at T = 1024, causal: the 72 allowed P tiles (48 KB
+    # each, and their rows' exponents) and 72 dS tiles (64 KB), about 8.3 MB;
+    # 12 batches in one chunk by default, 2 a chunk (two buffers) under
+    # 40 MB, and the recomputing kernels under 12 MB.
     whole = _grads(tmp_path, None)
-    chunked = _grads(tmp_path, 60)
-    recomputed = _grads(tmp_path, 16)
+    chunked = _grads(tmp_path, 40)
+    recomputed = _grads(tmp_path, 12)
     assert np.isfinite(whole).all()
     assert np.array_equal(whole.view(np.uint64), chunked.view(np.uint64))
     assert np.array_equal(whole.view(np.uint64), recomputed.view(np.uint64))

@@ -101,3 +101,25 @@ def test_ordered_and_heavily_repeated_keys(order):
         if order == "descending":
             words = words[::-1].copy()
     _check(words)
+
+
+def test_keys_not_16_byte_aligned():
+    # The passes read keys by TMA bulk copies, which want 16-byte aligned
+    # sources: keys starting 8 bytes past an alignment are copied first.
+    import torch
+
+    rng = oracle.Rng.seeded(12, 6)
+    n = 50_001
+    words = rng.u64s(n + 1) % np.uint64(7919)
+    lib = _lib.load()
+    w = torch.from_numpy(words.view(np.int64)).cuda()
+    rank = torch.zeros(n, dtype=torch.int32, device="cuda")
+    first = torch.zeros(n, dtype=torch.int32, device="cuda")
+    k = ctypes.c_int64(-1)
+    torch.cuda.synchronize()
+    st = lib.einfold_rank_words(_lib.context(0), w.data_ptr() + 8, n, rank.data_ptr(), first.data_ptr(),
+                                ctypes.byref(k), None)
+    assert st == _lib.OK, lib.einfold_last_error()
+    want = oracle.ranks_of_words(words[1:])
+    assert np.array_equal(rank.cpu().numpy().view(np.uint32), want.rank)
+    assert np.array_equal(first.cpu().numpy()[: k.value].view(np.uint32), want.first)
