@@ -289,192 +289,145 @@ __global__ void __launch_bounds__(kThreads) byte_histograms(const uint64_t* __re
   }
 }
 
-// One pass: persistent blocks (as many as fit at once), each claiming tiles
-// of 256·ITEMS keys from a counter, in order, so that every earlier tile's
-// block is running. A block fetches its next tile by TMA bulk copies into
-// the second of two shared-memory stages while it works on the current one,
-// so loads stay in flight through the ranking, look-back and writes. A tile's
-// keys and row numbers are read into registers (item i of a lane is key
-// warp·32·ITEMS + 32i + lane of the tile); each warp ranks its items among
-// equal digits in order, item by item: __match_any_sync groups the lanes of
-// a digit, and a per-warp counter of each digit in shared memory gives the
-// group its first place, so a key's place among its warp's equal digits
-// counts every earlier key of the warp. The warps' counters then become
-// offsets (digit by digit, over the warps), a block scan gives each digit's
-// first place in the tile, and the look-back each digit's keys in earlier
-// tiles. The keys are reordered by digit through one shared-memory buffer, a
-// word at a time and then the row numbers, and written out as runs of
-// consecutive destinations.
+// One pass, one tile of 256·ITEMS keys a block. The tile's keys and row
+// numbers stay in registers (item i of a lane is key warp·32·ITEMS + 32i +
+// lane of the tile). Each warp ranks its items among equal digits in order,
+// item by item: __match_any_sync groups the lanes of a digit, and a per-warp
+// counter of each digit in shared memory gives the group its first place,
+// so a key's place among its warp's equal digits counts every earlier key of
+// the warp. The warps' counters then become offsets (digit by digit, over
+// the warps), a block scan gives each digit's first place in the tile, and
+// the look-back each digit's keys in earlier tiles. The keys are reordered
+// by digit through one shared-memory buffer, a word at a time and then the
+// row numbers, and written out as runs of consecutive destinations.
 template <int W, int ITEMS>
-__global__ void __launch_bounds__(kThreads, 2) onesweep_pass(const uint64_t* __restrict__ kin,
+__global__ void __launch_bounds__(kThreads, 3) onesweep_pass(const uint64_t* __restrict__ kin,
                                                              const uint32_t* __restrict__ vin,
                                                              uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                              int64_t n, int64_t ldi, int64_t ldo, int word, int shift,
                                                              const uint32_t* __restrict__ digit_start,
                                                              uint32_t* __restrict__ status,
-                                                             unsigned int* __restrict__ tile_counter, int64_t tiles,
-                                                             int* err) {
+                                                             unsigned int* __restrict__ tile_counter, int* err) {
   constexpr int TILE = kThreads * ITEMS;
   constexpr int WARPS = kThreads / 32;
-  constexpr int STAGE = TILE * (8 * W + 4);
   static_assert(TILE <= 65535, "a tile's places fit 16 bits");
-  extern __shared__ __align__(128) uint8_t smem[];
-  uint64_t* xbuf = (uint64_t*)(smem + 2 * STAGE);  // [TILE]: one word of the reordered keys, or the rows
-  uint8_t* sdig = (uint8_t*)(xbuf + TILE);          // [TILE]: the reordered keys' digits
-  __shared__ __align__(8) uint64_t bar[2];
-  __shared__ long long s_tile[2];                   // the tile in each stage (-1: none)
-  __shared__ uint16_t wcount[WARPS][256];           // per warp: a digit's keys so far, then its offset
-  __shared__ uint16_t dstart[256];                  // a digit's first place in the tile
-  __shared__ long long dbase[256];                  // a digit's destination minus its first place
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint64_t* xbuf = (uint64_t*)smem;               // [TILE]: one word of the reordered keys, or the rows
+  uint8_t* sdig = smem + TILE * 8;                // [TILE]: the reordered keys' digits
+  __shared__ uint16_t wcount[WARPS][256];         // per warp: a digit's keys so far, then its offset
+  __shared__ uint16_t dstart[256];                // a digit's first place in the tile
+  __shared__ long long dbase[256];                // a digit's destination minus its first place
+  __shared__ unsigned int s_tile;
   typedef cub::BlockScan<unsigned int, kThreads> Scan;
   __shared__ typename Scan::TempStorage tmp;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
+#pragma unroll
+  for (int d = lane; d < 256; d += 32) wcount[warp][d] = 0;
+  __syncthreads();
+  const int64_t t = s_tile;
+  const int64_t base = t * TILE;
+  const int64_t count = min((int64_t)TILE, n - base);
   const unsigned lt_mask = (1u << lane) - 1u;
-  auto skeys = [&](int st) { return (uint64_t*)(smem + st * STAGE); };
-  auto svals = [&](int st) { return (uint32_t*)(smem + st * STAGE + TILE * 8 * W); };
-  // Claims the next tile and issues its copies into stage `st` (thread 0):
-  // whole 16-byte multiples by TMA, a ragged tail of the last tile by the
-  // threads when they read it.
-  auto claim = [&](int st) {
-    const long long t = (long long)atomicAdd(tile_counter, 1u);
-    if (t >= tiles) {
-      s_tile[st] = -1;
-      return;
+
+  uint64_t key[ITEMS][W];
+  uint32_t val[ITEMS];
+  uint32_t dp[ITEMS];  // digit (bits 16..24; 256: no key) and place among the warp's equal digits (bits 0..15)
+#pragma unroll
+  for (int i = 0; i < ITEMS; i++) {
+    const int off = warp * 32 * ITEMS + i * 32 + lane;
+    uint32_t d = 256;
+    if (off < count) {
+#pragma unroll
+      for (int w = 0; w < W; w++) key[i][w] = __ldcs(&kin[(int64_t)w * ldi + base + off]);
+      val[i] = vin ? __ldcs(&vin[base + off]) : (uint32_t)(base + off);
+      uint64_t wd = key[i][0];
+#pragma unroll
+      for (int w = 1; w < W; w++)
+        if (word == w) wd = key[i][w];
+      d = (uint32_t)((wd >> shift) & 255);
     }
-    s_tile[st] = t;
-    const int64_t base = t * TILE;
-    const int64_t bulk = min((int64_t)TILE, n - base) & ~(int64_t)3;
-    ptx::mbar_expect_tx(&bar[st], (uint32_t)(bulk * 8 * W + (vin ? bulk * 4 : 0)));
-    if (bulk) {
-      for (int w = 0; w < W; w++)
-        ptx::bulk_load(skeys(st) + w * TILE, kin + (int64_t)w * ldi + base, (uint32_t)(bulk * 8), &bar[st]);
-      if (vin) ptx::bulk_load(svals(st), vin + base, (uint32_t)(bulk * 4), &bar[st]);
-    }
-  };
-  if (tid == 0) {
-    ptx::mbar_init(&bar[0], 1);
-    ptx::mbar_init(&bar[1], 1);
-    ptx::mbar_fence_init();
-    claim(0);
+    dp[i] = d << 16;
+  }
+#pragma unroll
+  for (int i = 0; i < ITEMS; i++) {
+    const uint32_t d = dp[i] >> 16;
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const unsigned c = d < 256 ? wcount[warp][d] : 0u;
+    __syncwarp();
+    if (d < 256 && (peers & lt_mask) == 0) wcount[warp][d] = (uint16_t)(c + __popc(peers));
+    dp[i] |= c + __popc(peers & lt_mask);
+    __syncwarp();
   }
   __syncthreads();
-  for (int it = 0;; it++) {
-    const int st = it & 1;
-    const long long t = s_tile[st];
-    if (t < 0) break;
-    if (tid == 0) {
-      // The other stage was last read before the previous iteration's end.
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      claim(st ^ 1);
-    }
+  unsigned int total = 0;
 #pragma unroll
-    for (int d = lane; d < 256; d += 32) wcount[warp][d] = 0;
-    const int64_t base = t * TILE;
-    const int64_t count = min((int64_t)TILE, n - base);
-    const int64_t bulk = count & ~(int64_t)3;
-    if (!ptx::mbar_wait(&bar[st], (uint32_t)((it >> 1) & 1), true)) atomicOr(err, 1);
-
-    uint64_t key[ITEMS][W];
-    uint32_t val[ITEMS];
-    uint32_t dp[ITEMS];  // digit (bits 16..24; 256: no key) and place among the warp's equal digits
-#pragma unroll
-    for (int i = 0; i < ITEMS; i++) {
-      const int off = warp * 32 * ITEMS + i * 32 + lane;
-      uint32_t d = 256;
-      if (off < count) {
-        const bool in_smem = off < bulk;
-#pragma unroll
-        for (int w = 0; w < W; w++)
-          key[i][w] = in_smem ? skeys(st)[w * TILE + off] : kin[(int64_t)w * ldi + base + off];
-        val[i] = vin ? (in_smem ? svals(st)[off] : vin[base + off]) : (uint32_t)(base + off);
-        uint64_t wd = key[i][0];
-#pragma unroll
-        for (int w = 1; w < W; w++)
-          if (word == w) wd = key[i][w];
-        d = (uint32_t)((wd >> shift) & 255);
+  for (int w = 0; w < WARPS; w++) {
+    const unsigned c = wcount[w][tid];
+    wcount[w][tid] = (uint16_t)total;
+    total += c;
+  }
+  // Publish this tile's count of digit `tid`, then look back for the
+  // earlier tiles' (thread tid owns digit tid).
+  uint32_t* my = status + t * 256 + tid;
+  if (t == 0) st_volatile(my, kFlagPre | total);
+  else st_volatile(my, kFlagAgg | total);
+  unsigned int ex;
+  Scan(tmp).ExclusiveSum(total, ex);
+  unsigned int before = 0;
+  if (t > 0) {
+    int64_t tt = t - 1;
+    uint64_t start = 0;
+    bool failed = false;
+    while (true) {
+      const uint32_t v = ld_volatile(status + tt * 256 + tid);
+      const uint32_t flag = v & ~kValue;
+      if (flag == 0) {
+        if (!start) start = ptx::now_ns();
+        else if (ptx::now_ns() - start > ptx::kWaitNs) {
+          failed = true;
+          break;
+        }
+        continue;
       }
-      dp[i] = d << 16;
+      before += v & kValue;
+      if (flag == kFlagPre || tt == 0) break;
+      tt--;
     }
-    __syncwarp();
+    if (failed) atomicOr(err, 1);
+    st_volatile(my, kFlagPre | (before + total));
+  }
+  dstart[tid] = (uint16_t)ex;
+  dbase[tid] = (long long)digit_start[tid] + (long long)before - (long long)ex;
+  __syncthreads();
+  // Each item's place in the reordered tile.
 #pragma unroll
-    for (int i = 0; i < ITEMS; i++) {
-      const uint32_t d = dp[i] >> 16;
-      const unsigned peers = __match_any_sync(0xffffffffu, d);
-      const unsigned c = d < 256 ? wcount[warp][d] : 0u;
-      __syncwarp();
-      if (d < 256 && (peers & lt_mask) == 0) wcount[warp][d] = (uint16_t)(c + __popc(peers));
-      dp[i] |= c + __popc(peers & lt_mask);
-      __syncwarp();
+  for (int i = 0; i < ITEMS; i++) {
+    const uint32_t d = dp[i] >> 16;
+    if (d < 256) {
+      const uint32_t pos = (uint32_t)dstart[d] + wcount[warp][d] + (dp[i] & 0xffffu);
+      dp[i] = (d << 16) | pos;
+      sdig[pos] = (uint8_t)d;
+    }
+  }
+#pragma unroll
+  for (int w = 0; w <= W; w++) {
+    // Word w of the keys (w < W), then the rows, through the one buffer.
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++)
+      if ((dp[i] >> 16) < 256) {
+        const uint32_t pos = dp[i] & 0xffffu;
+        if (w < W) xbuf[pos] = key[i][w];
+        else ((uint32_t*)xbuf)[pos] = val[i];
+      }
+    __syncthreads();
+    for (int j = tid; j < count; j += kThreads) {
+      const long long dst = dbase[sdig[j]] + j;
+      if (w < W) __stcs(&kout[(int64_t)w * ldo + dst], xbuf[j]);
+      else __stcs(&vout[dst], ((const uint32_t*)xbuf)[j]);
     }
     __syncthreads();
-    unsigned int total = 0;
-#pragma unroll
-    for (int w = 0; w < WARPS; w++) {
-      const unsigned c = wcount[w][tid];
-      wcount[w][tid] = (uint16_t)total;
-      total += c;
-    }
-    // Publish this tile's count of digit `tid`, then look back for the
-    // earlier tiles' (thread tid owns digit tid).
-    uint32_t* my = status + t * 256 + tid;
-    if (t == 0) st_volatile(my, kFlagPre | total);
-    else st_volatile(my, kFlagAgg | total);
-    unsigned int ex;
-    Scan(tmp).ExclusiveSum(total, ex);
-    unsigned int before = 0;
-    if (t > 0) {
-      int64_t tt = t - 1;
-      uint64_t start = 0;
-      bool failed = false;
-      while (true) {
-        const uint32_t v = ld_volatile(status + tt * 256 + tid);
-        const uint32_t flag = v & ~kValue;
-        if (flag == 0) {
-          if (!start) start = ptx::now_ns();
-          else if (ptx::now_ns() - start > ptx::kWaitNs) {
-            failed = true;
-            break;
-          }
-          continue;
-        }
-        before += v & kValue;
-        if (flag == kFlagPre || tt == 0) break;
-        tt--;
-      }
-      if (failed) atomicOr(err, 1);
-      st_volatile(my, kFlagPre | (before + total));
-    }
-    dstart[tid] = (uint16_t)ex;
-    dbase[tid] = (long long)digit_start[tid] + (long long)before - (long long)ex;
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < ITEMS; i++) {
-      const uint32_t d = dp[i] >> 16;
-      if (d < 256) {
-        const uint32_t pos = (uint32_t)dstart[d] + wcount[warp][d] + (dp[i] & 0xffffu);
-        dp[i] = (d << 16) | pos;
-        sdig[pos] = (uint8_t)d;
-      }
-    }
-#pragma unroll
-    for (int w = 0; w <= W; w++) {
-      // Word w of the keys (w < W), then the rows, through the one buffer.
-#pragma unroll
-      for (int i = 0; i < ITEMS; i++)
-        if ((dp[i] >> 16) < 256) {
-          const uint32_t pos = dp[i] & 0xffffu;
-          if (w < W) xbuf[pos] = key[i][w];
-          else ((uint32_t*)xbuf)[pos] = val[i];
-        }
-      __syncthreads();
-      for (int j = tid; j < count; j += kThreads) {
-        const long long dst = dbase[sdig[j]] + j;
-        if (w < W) __stcs(&kout[(int64_t)w * ldo + dst], xbuf[j]);
-        else __stcs(&vout[dst], ((const uint32_t*)xbuf)[j]);
-      }
-      __syncthreads();
-    }
   }
 }
 
@@ -839,17 +792,7 @@ int64_t rank_keys_onesweep(Context& ctx, const uint64_t* keys, int64_t n, int64_
   const uint64_t* cur_k = keys;
   int64_t cur_ld = ld;
   const uint32_t* cur_v = nullptr;
-  const size_t smem = (size_t)TILE * (2 * (8 * W + 4) + 8 + 1);
-  // TMA bulk copies read 16-byte aligned words: copy keys that aren't.
-  DeviceBuffer<uint64_t> aligned;
-  if (passes && (((uintptr_t)keys & 15) || (W > 1 && (ld & 1)))) {
-    const int64_t lda = (n + 1) & ~(int64_t)1;
-    aligned.allocate((size_t)(W * lda), s);
-    EF_CUDA(cudaMemcpy2DAsync(aligned.get(), (size_t)lda * 8, keys, (size_t)ld * 8, (size_t)n * 8, W,
-                              cudaMemcpyDeviceToDevice, s));
-    cur_k = aligned.get();
-    cur_ld = lda;
-  }
+  const size_t smem = (size_t)TILE * (8 + 1);
   if (passes) {
     const int64_t ldb = (n + 1) & ~(int64_t)1;
     for (int b = 0; b < 2; b++) {
@@ -857,16 +800,11 @@ int64_t rank_keys_onesweep(Context& ctx, const uint64_t* keys, int64_t n, int64_
       vb[b].allocate((size_t)n, s);
     }
     EF_CUDA(cudaFuncSetAttribute(onesweep_pass<W, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    EF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_pass<W, ITEMS>, kThreads, smem));
-    // Persistent blocks, all resident at once (a look-back waits only on
-    // tiles that running blocks hold).
-    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)std::max(1, per_sm) * ctx.sm_count));
     for (int p = 0; p < passes; p++) {
       EF_CUDA(cudaMemsetAsync(status.get(), 0, (size_t)tiles * 256 * 4, s));
-      onesweep_pass<W, ITEMS><<<grid, kThreads, smem, s>>>(
+      onesweep_pass<W, ITEMS><<<(unsigned)tiles, kThreads, smem, s>>>(
           cur_k, cur_v, kb[p & 1].get(), vb[p & 1].get(), n, cur_ld, ldb, pw[p], ps[p], dstart.get() + p * 256,
-          status.get(), counters.get() + p, tiles, err.get());
+          status.get(), counters.get() + p, err.get());
       ctx.kernels++;
       cur_k = kb[p & 1].get();
       cur_ld = ldb;
