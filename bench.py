@@ -965,14 +965,14 @@ def _gradients():
     bwd_flop = 2.5 * 4.0 * b_ * h_ * t_ * t_ * d_ * (t_ + 1) / (2 * t_)
     att = {"shape": {"B": b_, "H": h_, "T": t_, "d": d_}, "flop": bwd_flop}
     grads = {}
-    for name, prec in (("split", Precision.SPLIT), ("fp64_tiles", Precision.FP64)):
+    for name, prec in (("split", Precision.SPLIT), ("fp64_tensor_pipe", Precision.FP64)):
         out, lse = A.attention_forward(q, k, v, causal, 1.0, prec)
         ms, g = timed(lambda: A.attention_backward(q, k, v, out, lse, d_out, causal, 1.0, prec))
         grads[name] = g
         att[name] = {"ms": ms, "tflop_per_s": bwd_flop / ms / 1e9}
     att["split_norm_rel_err"] = {x: rel(a, b) for x, a, b in zip(("d_q", "d_k", "d_v"), grads["split"],
-                                                                   grads["fp64_tiles"])}
-    att["ratio_split_over_fp64"] = att["fp64_tiles"]["ms"] / att["split"]["ms"]
+                                                                   grads["fp64_tensor_pipe"])}
+    att["ratio_split_over_fp64"] = att["fp64_tensor_pipe"]["ms"] / att["split"]["ms"]
     del q, k, v, d_out, grads
     m = 4096
     a = S.uniform(SEED, 45, m * m).view(m, m)

@@ -32,13 +32,13 @@ from . import synthetic as S
 from .kernels import Precision
 
 
-def attention(groups: int, t: int, d: int, backward: bool) -> None:
+def attention(groups: int, t: int, d: int, backward: bool, precision: Precision = Precision.SPLIT) -> None:
     n = groups * t * d
     q, k, v = (S.normal(0, salt, n, 1.0 / 8).view(groups, t, d) for salt in (3, 4, 5))
-    out, lse = A.attention_forward(q, k, v, A.causal(), 1.0, Precision.SPLIT)
+    out, lse = A.attention_forward(q, k, v, A.causal(), 1.0, precision)
     if backward:
         d_out = S.normal(0, 6, n, 1.0).view(groups, t, d)
-        A.attention_backward(q, k, v, out, lse, d_out, A.causal(), 1.0, Precision.SPLIT)
+        A.attention_backward(q, k, v, out, lse, d_out, A.causal(), 1.0, precision)
     torch.cuda.synchronize()
     print(f"attention groups={groups} t={t} d={d} backward={backward}: max|out| {out.abs().max().item():.6f}")
 
@@ -235,6 +235,7 @@ def main() -> None:
     pa.add_argument("--t", type=int, default=2048)
     pa.add_argument("--d", type=int, default=64)
     pa.add_argument("--backward", action="store_true")
+    pa.add_argument("--precision", choices=["split", "fp64"], default="split")
     pp = sub.add_parser("product")
     pp.add_argument("--n", type=int, default=4096)
     pg = sub.add_parser("ragged")
@@ -252,7 +253,8 @@ def main() -> None:
     pr.add_argument("--repeat", type=int, default=3)
     args = p.parse_args()
     if args.case == "attention":
-        attention(args.groups, args.t, args.d, args.backward)
+        attention(args.groups, args.t, args.d, args.backward,
+                  Precision.FP64 if args.precision == "fp64" else Precision.SPLIT)
     elif args.case == "rank":
         rank(args.n, args.repeat)
     elif args.case == "ragged":
