@@ -291,17 +291,22 @@ __global__ void __launch_bounds__(kThreads) byte_histograms(const uint64_t* __re
 
 // One pass, one tile of 256·ITEMS keys a block. The tile's keys and row
 // numbers stay in registers (item i of a lane is key warp·32·ITEMS + 32i +
-// lane of the tile). Each warp ranks its items among equal digits in order,
-// item by item: __match_any_sync groups the lanes of a digit, and a per-warp
-// counter of each digit in shared memory gives the group its first place,
-// so a key's place among its warp's equal digits counts every earlier key of
-// the warp. The warps' counters then become offsets (digit by digit, over
-// the warps), a block scan gives each digit's first place in the tile, and
-// the look-back each digit's keys in earlier tiles. The keys are reordered
-// by digit through one shared-memory buffer, a word at a time and then the
-// row numbers, and written out as runs of consecutive destinations.
-template <int W, int ITEMS>
-__global__ void __launch_bounds__(kThreads, 3) onesweep_pass(const uint64_t* __restrict__ kin,
+// lane of the tile). As soon as they arrive, the tile's count of each digit
+// (shared-memory atomics) is published, so that later tiles' look-backs can
+// pass this one while it ranks. Each warp then ranks its items among equal
+// digits in order: eight ballots over a digit's bits (and a ninth for the
+// padding past the last key) give each lane the lanes that hold its digit,
+// for every item before any counter is touched, and a per-warp counter of
+// each digit in shared memory, item by item, gives the group its first
+// place, so a key's place among its warp's equal digits counts every
+// earlier key of the warp. The warps' counters then become offsets (digit
+// by digit, over the warps), a block scan gives each digit's first place in
+// the tile, and the look-back each digit's keys in earlier tiles, reading
+// four earlier tiles' words at a time. The keys are reordered by digit
+// through one shared-memory buffer, a word at a time and then the row
+// numbers, and written out as runs of consecutive destinations.
+template <int W, int ITEMS, int MIN_BLOCKS>
+__global__ void __launch_bounds__(kThreads, MIN_BLOCKS) onesweep_pass(const uint64_t* __restrict__ kin,
                                                              const uint32_t* __restrict__ vin,
                                                              uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                              int64_t n, int64_t ldi, int64_t ldo, int word, int shift,
@@ -317,6 +322,7 @@ __global__ void __launch_bounds__(kThreads, 3) onesweep_pass(const uint64_t* __r
   __shared__ uint16_t wcount[WARPS][256];         // per warp: a digit's keys so far, then its offset
   __shared__ uint16_t dstart[256];                // a digit's first place in the tile
   __shared__ long long dbase[256];                // a digit's destination minus its first place
+  __shared__ unsigned int hcount[256];            // the tile's keys of each digit
   __shared__ unsigned int s_tile;
   typedef cub::BlockScan<unsigned int, kThreads> Scan;
   __shared__ typename Scan::TempStorage tmp;
@@ -325,6 +331,7 @@ __global__ void __launch_bounds__(kThreads, 3) onesweep_pass(const uint64_t* __r
   if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
 #pragma unroll
   for (int d = lane; d < 256; d += 32) wcount[warp][d] = 0;
+  hcount[tid] = 0;
   __syncthreads();
   const int64_t t = s_tile;
   const int64_t base = t * TILE;
@@ -350,50 +357,84 @@ __global__ void __launch_bounds__(kThreads, 3) onesweep_pass(const uint64_t* __r
     }
     dp[i] = d << 16;
   }
+  // The tile's count of each digit, published at once (thread tid owns
+  // digit tid): tile 0's counts are its inclusive prefixes.
+#pragma unroll
+  for (int i = 0; i < ITEMS; i++)
+    if ((dp[i] >> 16) < 256) atomicAdd(&hcount[dp[i] >> 16], 1u);
+  __syncthreads();
+  const unsigned int total = hcount[tid];
+  uint32_t* my = status + t * 256 + tid;
+  st_volatile(my, (t == 0 ? kFlagPre : kFlagAgg) | total);
+  // The lanes holding each item's digit (256 marks no key).
+  unsigned peers[ITEMS];
 #pragma unroll
   for (int i = 0; i < ITEMS; i++) {
     const uint32_t d = dp[i] >> 16;
-    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    unsigned m = 0xffffffffu;
+#pragma unroll
+    for (int b = 0; b < 9; b++) {
+      const bool bit = (d >> b) & 1u;
+      const unsigned set = __ballot_sync(0xffffffffu, bit);
+      m &= bit ? set : ~set;
+    }
+    peers[i] = m;
+  }
+#pragma unroll
+  for (int i = 0; i < ITEMS; i++) {
+    const uint32_t d = dp[i] >> 16;
     const unsigned c = d < 256 ? wcount[warp][d] : 0u;
     __syncwarp();
-    if (d < 256 && (peers & lt_mask) == 0) wcount[warp][d] = (uint16_t)(c + __popc(peers));
-    dp[i] |= c + __popc(peers & lt_mask);
+    if (d < 256 && (peers[i] & lt_mask) == 0) wcount[warp][d] = (uint16_t)(c + __popc(peers[i]));
+    dp[i] |= c + __popc(peers[i] & lt_mask);
     __syncwarp();
   }
   __syncthreads();
-  unsigned int total = 0;
+  {
+    unsigned int acc = 0;
 #pragma unroll
-  for (int w = 0; w < WARPS; w++) {
-    const unsigned c = wcount[w][tid];
-    wcount[w][tid] = (uint16_t)total;
-    total += c;
+    for (int w = 0; w < WARPS; w++) {
+      const unsigned c = wcount[w][tid];
+      wcount[w][tid] = (uint16_t)acc;
+      acc += c;
+    }
   }
-  // Publish this tile's count of digit `tid`, then look back for the
-  // earlier tiles' (thread tid owns digit tid).
-  uint32_t* my = status + t * 256 + tid;
-  if (t == 0) st_volatile(my, kFlagPre | total);
-  else st_volatile(my, kFlagAgg | total);
   unsigned int ex;
   Scan(tmp).ExclusiveSum(total, ex);
+  // The look-back, four earlier tiles' words at a time, in order: a count
+  // is added, a prefix ends it, and a word not yet published is read again
+  // (flags only go from none to count to prefix, so an early read of a
+  // count stays valid).
   unsigned int before = 0;
   if (t > 0) {
+    constexpr int kWindow = 4;
     int64_t tt = t - 1;
     uint64_t start = 0;
     bool failed = false;
     while (true) {
-      const uint32_t v = ld_volatile(status + tt * 256 + tid);
-      const uint32_t flag = v & ~kValue;
-      if (flag == 0) {
+      uint32_t v[kWindow];
+#pragma unroll
+      for (int k = 0; k < kWindow; k++) v[k] = tt - k >= 0 ? ld_volatile(status + (tt - k) * 256 + tid) : 0u;
+      bool done = false;
+      int used = 0;
+#pragma unroll
+      for (int k = 0; k < kWindow; k++) {
+        if (done || used < k || tt - k < 0) continue;
+        const uint32_t flag = v[k] & ~kValue;
+        if (flag == 0) continue;
+        before += v[k] & kValue;
+        used = k + 1;
+        if (flag == kFlagPre) done = true;
+      }
+      if (done) break;
+      if (used == 0) {
         if (!start) start = ptx::now_ns();
         else if (ptx::now_ns() - start > ptx::kWaitNs) {
           failed = true;
           break;
         }
-        continue;
       }
-      before += v & kValue;
-      if (flag == kFlagPre || tt == 0) break;
-      tt--;
+      tt -= used;
     }
     if (failed) atomicOr(err, 1);
     st_volatile(my, kFlagPre | (before + total));
@@ -744,7 +785,8 @@ void radix_pass(Context& ctx, const uint64_t* kin, int64_t ldi, const uint32_t* 
 template <int W>
 int64_t rank_keys_onesweep(Context& ctx, const uint64_t* keys, int64_t n, int64_t ld, uint32_t* rank,
                            uint32_t* first, cudaStream_t s, uint32_t* sorted_rows) {
-  constexpr int ITEMS = W == 1 ? 12 : (W == 2 ? 8 : (W == 3 ? 6 : 4));
+  constexpr int ITEMS = W == 1 ? 8 : (W == 2 ? 8 : (W == 3 ? 6 : 4));
+  constexpr int MIN_BLOCKS = W == 1 ? 4 : 3;
   constexpr int TILE = kThreads * ITEMS;
   constexpr int RITEMS = 8;
   constexpr int RTILE = kThreads * RITEMS;
@@ -799,10 +841,10 @@ int64_t rank_keys_onesweep(Context& ctx, const uint64_t* keys, int64_t n, int64_
       kb[b].allocate((size_t)(W * ldb), s);
       vb[b].allocate((size_t)n, s);
     }
-    EF_CUDA(cudaFuncSetAttribute(onesweep_pass<W, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    EF_CUDA(cudaFuncSetAttribute(onesweep_pass<W, ITEMS, MIN_BLOCKS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     for (int p = 0; p < passes; p++) {
       EF_CUDA(cudaMemsetAsync(status.get(), 0, (size_t)tiles * 256 * 4, s));
-      onesweep_pass<W, ITEMS><<<(unsigned)tiles, kThreads, smem, s>>>(
+      onesweep_pass<W, ITEMS, MIN_BLOCKS><<<(unsigned)tiles, kThreads, smem, s>>>(
           cur_k, cur_v, kb[p & 1].get(), vb[p & 1].get(), n, cur_ld, ldb, pw[p], ps[p], dstart.get() + p * 256,
           status.get(), counters.get() + p, err.get());
       ctx.kernels++;
