@@ -132,6 +132,10 @@ struct AttentionGradients {
   double* d_q = nullptr;
   double* d_k = nullptr;
   double* d_v = nullptr;
+  // The caller's budget (null: none): the split backward asks it for the
+  // export buffers, a smaller plan at each refusal, and gives them back at
+  // the end of the call; with nothing granted it recomputes the scores.
+  Budget* budget = nullptr;
 };
 // The FP64 backward on the FP64 tensor pipe (d, dv <= 64, scale one or times
 // c; false, nothing written, otherwise): d_k and d_v from a kernel with keys

@@ -1228,22 +1228,57 @@ bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd,
     const int64_t nq = hq_off[(size_t)(w1 * n_qb)] - hq_off[(size_t)(w0 * n_qb)];
     return al((size_t)np * kPTile) + al((size_t)np * GM * 4) + (size_t)nq * kDsBytes;
   };
+  // The chunks and buffers under a limit: one chunk when every batch's
+  // exports fit it, else chunks of at most half of it in two buffers; none
+  // when one batch's exports exceed half of it.
   std::vector<std::pair<int64_t, int64_t>> chunks;
   int buffers = 1;
-  if (bytes_of(0, W) <= limit) {
-    chunks.push_back({0, W});
-  } else {
+  auto plan_under = [&](size_t lim) {
+    chunks.clear();
+    buffers = 1;
+    if (bytes_of(0, W) <= lim) {
+      chunks.push_back({0, W});
+      return;
+    }
     buffers = 2;
     int64_t w0 = 0;
     while (w0 < W) {
-      if (bytes_of(w0, w0 + 1) > limit / 2) {
+      if (bytes_of(w0, w0 + 1) > lim / 2) {
         chunks.clear();
-        break;
+        return;
       }
       int64_t w1 = w0 + 1;
-      while (w1 < W && bytes_of(w0, w1 + 1) <= limit / 2) w1++;
+      while (w1 < W && bytes_of(w0, w1 + 1) <= lim / 2) w1++;
       chunks.push_back({w0, w1});
       w0 = w1;
+    }
+  };
+  auto biggest_chunk = [&]() {
+    size_t b = 0;
+    for (auto& c : chunks) b = std::max(b, bytes_of(c.first, c.second));
+    return std::max<size_t>(b, 256);
+  };
+  // With a budget, the plan's buffers are asked of it, and a refusal halves
+  // the limit until a plan is granted or none is left.
+  struct Granted {
+    Budget* budget = nullptr;
+    uint64_t bytes = 0;
+    ~Granted() {
+      if (budget && bytes) budget->release(bytes);
+    }
+  } granted;
+  for (size_t lim = limit;; lim /= 2) {
+    plan_under(lim);
+    if (chunks.empty() || !g.budget) break;
+    const uint64_t want = (uint64_t)buffers * biggest_chunk();
+    if (g.budget->try_reserve(want)) {
+      granted.budget = g.budget;
+      granted.bytes = want;
+      break;
+    }
+    if (lim == 0) {
+      chunks.clear();
+      break;
     }
   }
   (void)kPBytes;
@@ -1269,9 +1304,8 @@ bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd,
     EF_CUDA(cudaStreamWaitEvent(ctx.aux, joined, 0));
   }
   if (!chunks.empty()) {
-    size_t biggest = 0;
-    for (auto& c : chunks) biggest = std::max(biggest, bytes_of(c.first, c.second));
-    for (int b = 0; b < buffers; b++) exports[b].allocate(std::max<size_t>(biggest, 256), streams[b]);
+    const size_t biggest = biggest_chunk();
+    for (int b = 0; b < buffers; b++) exports[b].allocate(biggest, streams[b]);
     for (size_t c = 0; c < chunks.size(); c++) {
       const int b = (int)(c % (size_t)buffers);
       cudaStream_t st = streams[b];

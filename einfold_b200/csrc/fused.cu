@@ -1408,6 +1408,9 @@ GradientOutput pipeline_backward(Context& ctx, const PipelineD& p, const Relatio
   g.d_q = dq.get();
   g.d_k = dkm.get();
   g.d_v = dv.get();
+  Budget budget;
+  budget.o = &o;
+  g.budget = &budget;
   attention_backward(ctx, g, o.precision, s);
   ctx.phase("fused backward: gradients");
   GradientOutput r;

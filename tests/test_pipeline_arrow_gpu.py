@@ -240,3 +240,55 @@ def test_pipeline_backward_of_a_missing_d_out_row_is_zero_and_others_decline():
     p2 = ir.Pipeline(p.producer(), ir.Weight.of_expression(sig), [E], p.values(), [B, I, 4],
                      ir.Normalizer.KEPT_GROUPS)
     assert K.pipeline_backward(p2, ops, K.Relation(full.schema, [full])) is None
+
+
+class _Ledger(K.Budget):
+    """A budget that grants up to `cap` bytes at once and records what it was
+    asked, granted and given back."""
+
+    def __init__(self, cap):
+        self.cap, self.out, self.peak, self.asked = cap, 0, 0, []
+
+    def grow(self, n):
+        self.asked.append(n)
+        if self.out + n > self.cap:
+            return False
+        self.out += n
+        self.peak = max(self.peak, self.out)
+        return True
+
+    def shrink(self, n):
+        self.out -= n
+
+
+def test_pipeline_backward_asks_the_budget_for_its_exports():
+    # 4 causal batches of T = 1024, d = 64: about 8.3 MB of exports (P's digit
+    # tiles and dS over the allowed tiles) a batch. With the whole granted,
+    # one chunk; under 20 MB, two buffers of one batch each; with nothing
+    # granted, the kernels that recompute the scores. Same bits every time,
+    # and every granted byte given back.
+    nb, lmax, d, c = 4, 1024, 64, 64
+    Q, K_, V = _inputs(nb, lmax, d, c, 9)
+    dO = np.random.default_rng(10).normal(0, 1, (nb, lmax, c))
+    p = _pipeline(causal=True)
+    (sq, q), (sk, k), (sv, v) = _tables(Q, K_, V, [lmax] * nb)
+    dout = _d_out_table(dO, [lmax] * nb)
+    ops = [K.Relation(sq, q), K.Relation(sk, k), K.Relation(sv, v)]
+
+    def run(budget):
+        got = K.pipeline_backward(p, ops, K.Relation(dout.schema, [dout]), K.Options(budget=budget))
+        assert got is not None, K.last_call.message
+        return [rows_of(g).column(3).to_numpy(zero_copy_only=False) for g in got]
+
+    want = run(None)
+    for cap, granted in ((1 << 40, True), (20 << 20, True), (0, False)):
+        ledger = _Ledger(cap)
+        got = run(ledger)
+        for x, y in zip(got, want):
+            assert np.array_equal(x.view(np.uint64), y.view(np.uint64)), cap
+        assert ledger.out == 0, (cap, ledger.out)
+        assert ledger.asked, cap
+        assert (ledger.peak > 0) == granted, (cap, ledger.peak)
+        assert ledger.peak <= cap
+        if cap == 20 << 20:
+            assert ledger.peak > 8 << 20 and len(ledger.asked) > 1, ledger.asked
