@@ -289,22 +289,26 @@ __global__ void __launch_bounds__(kThreads) byte_histograms(const uint64_t* __re
   }
 }
 
-// One pass, one tile of 256·ITEMS keys a block. The tile's keys and row
-// numbers stay in registers (item i of a lane is key warp·32·ITEMS + 32i +
-// lane of the tile). As soon as they arrive, the tile's count of each digit
-// (shared-memory atomics) is published, so that later tiles' look-backs can
-// pass this one while it ranks. Each warp then ranks its items among equal
-// digits in order: eight ballots over a digit's bits (and a ninth for the
-// padding past the last key) give each lane the lanes that hold its digit,
-// for every item before any counter is touched, and a per-warp counter of
-// each digit in shared memory, item by item, gives the group its first
-// place, so a key's place among its warp's equal digits counts every
-// earlier key of the warp. The warps' counters then become offsets (digit
-// by digit, over the warps), a block scan gives each digit's first place in
-// the tile, and the look-back each digit's keys in earlier tiles, reading
-// four earlier tiles' words at a time. The keys are reordered by digit
-// through one shared-memory buffer, a word at a time and then the row
-// numbers, and written out as runs of consecutive destinations.
+// One pass, one tile of 256·ITEMS keys a block. The tile arrives in shared
+// memory by bulk copies (one a key word and one for the row numbers, whole
+// 16-byte multiples; a ragged tail of the last tile is read directly), so
+// that a block's loads take no load slots of its warps; its keys and row
+// numbers then stay in registers (item i of a lane is key warp·32·ITEMS +
+// 32i + lane of the tile). As soon as they arrive, the tile's count of each
+// digit (shared-memory atomics) is published, so that later tiles'
+// look-backs can pass this one while it ranks. Each warp then ranks its
+// items among equal digits in order: eight ballots over a digit's bits (and
+// a ninth for the padding past the last key) give each lane the lanes that
+// hold its digit, for every item before any counter is touched, and a
+// per-warp counter of each digit in shared memory, item by item, gives the
+// group its first place, so a key's place among its warp's equal digits
+// counts every earlier key of the warp. The warps' counters then become
+// offsets (digit by digit, over the warps), a block scan gives each digit's
+// first place in the tile, and the look-back each digit's keys in earlier
+// tiles, reading four earlier tiles' words at a time. The keys are
+// reordered by digit through the first key word's stage, a word at a time
+// and then the row numbers, and written out as runs of consecutive
+// destinations. Key words (ldi) and row numbers start 16-byte aligned.
 template <int W, int ITEMS, int MIN_BLOCKS>
 __global__ void __launch_bounds__(kThreads, MIN_BLOCKS) onesweep_pass(const uint64_t* __restrict__ kin,
                                                              const uint32_t* __restrict__ vin,
@@ -317,8 +321,11 @@ __global__ void __launch_bounds__(kThreads, MIN_BLOCKS) onesweep_pass(const uint
   constexpr int WARPS = kThreads / 32;
   static_assert(TILE <= 65535, "a tile's places fit 16 bits");
   extern __shared__ __align__(16) uint8_t smem[];
-  uint64_t* xbuf = (uint64_t*)smem;               // [TILE]: one word of the reordered keys, or the rows
-  uint8_t* sdig = smem + TILE * 8;                // [TILE]: the reordered keys' digits
+  uint64_t* kstage = (uint64_t*)smem;               // [W][TILE]: the tile's key words
+  uint32_t* vstage = (uint32_t*)(kstage + W * TILE);  // [TILE]: its row numbers
+  uint8_t* sdig = (uint8_t*)(vstage + TILE);        // [TILE]: the reordered keys' digits
+  uint64_t* xbuf = kstage;                          // [TILE]: one word of the reordered keys, or the rows
+  __shared__ __align__(8) uint64_t bar;
   __shared__ uint16_t wcount[WARPS][256];         // per warp: a digit's keys so far, then its offset
   __shared__ uint16_t dstart[256];                // a digit's first place in the tile
   __shared__ long long dbase[256];                // a digit's destination minus its first place
@@ -328,7 +335,11 @@ __global__ void __launch_bounds__(kThreads, MIN_BLOCKS) onesweep_pass(const uint
   __shared__ typename Scan::TempStorage tmp;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
+  if (tid == 0) {
+    s_tile = atomicAdd(tile_counter, 1u);
+    ptx::mbar_init(&bar, 1);
+    ptx::mbar_fence_init();
+  }
 #pragma unroll
   for (int d = lane; d < 256; d += 32) wcount[warp][d] = 0;
   hcount[tid] = 0;
@@ -337,6 +348,21 @@ __global__ void __launch_bounds__(kThreads, MIN_BLOCKS) onesweep_pass(const uint
   const int64_t base = t * TILE;
   const int64_t count = min((int64_t)TILE, n - base);
   const unsigned lt_mask = (1u << lane) - 1u;
+  const int kb = (int)(count & ~(int64_t)1);               // keys the bulk copies bring
+  const int vb = vin ? (int)(count & ~(int64_t)3) : 0;     // row numbers they bring
+  if (tid == 0) {
+    ptx::mbar_expect_tx(&bar, (uint32_t)(kb * 8 * W + vb * 4));
+    if (kb)
+#pragma unroll
+      for (int w = 0; w < W; w++) ptx::bulk_load(kstage + w * TILE, kin + (int64_t)w * ldi + base, (uint32_t)(kb * 8), &bar);
+    if (vb) ptx::bulk_load(vstage, vin + base, (uint32_t)(vb * 4), &bar);
+  }
+  if (!ptx::mbar_wait(&bar, 0)) {
+    // The copies didn't land in time: fail the sort, and wait once more for
+    // them before the block's shared memory goes.
+    atomicOr(err, 1);
+    ptx::mbar_wait(&bar, 0);
+  }
 
   uint64_t key[ITEMS][W];
   uint32_t val[ITEMS];
@@ -347,8 +373,8 @@ __global__ void __launch_bounds__(kThreads, MIN_BLOCKS) onesweep_pass(const uint
     uint32_t d = 256;
     if (off < count) {
 #pragma unroll
-      for (int w = 0; w < W; w++) key[i][w] = __ldcs(&kin[(int64_t)w * ldi + base + off]);
-      val[i] = vin ? __ldcs(&vin[base + off]) : (uint32_t)(base + off);
+      for (int w = 0; w < W; w++) key[i][w] = off < kb ? kstage[w * TILE + off] : kin[(int64_t)w * ldi + base + off];
+      val[i] = vin ? (off < vb ? vstage[off] : vin[base + off]) : (uint32_t)(base + off);
       uint64_t wd = key[i][0];
 #pragma unroll
       for (int w = 1; w < W; w++)
@@ -785,13 +811,23 @@ void radix_pass(Context& ctx, const uint64_t* kin, int64_t ldi, const uint32_t* 
 template <int W>
 int64_t rank_keys_onesweep(Context& ctx, const uint64_t* keys, int64_t n, int64_t ld, uint32_t* rank,
                            uint32_t* first, cudaStream_t s, uint32_t* sorted_rows) {
-  constexpr int ITEMS = W == 1 ? 8 : (W == 2 ? 8 : (W == 3 ? 6 : 4));
-  constexpr int MIN_BLOCKS = W == 1 ? 4 : 3;
+  constexpr int ITEMS = W == 1 ? 16 : (W == 2 ? 8 : (W == 3 ? 6 : 4));
+  constexpr int MIN_BLOCKS = W == 1 ? 2 : 3;
   constexpr int TILE = kThreads * ITEMS;
   constexpr int RITEMS = 8;
   constexpr int RTILE = kThreads * RITEMS;
   const int64_t tiles = (n + TILE - 1) / TILE;
   const int64_t rtiles = (n + RTILE - 1) / RTILE;
+  // The passes' bulk copies read 16-byte aligned words: copy keys that aren't.
+  DeviceBuffer<uint64_t> aligned;
+  if (((uintptr_t)keys & 15) || (W > 1 && (ld & 1))) {
+    const int64_t lda = (n + 1) & ~(int64_t)1;
+    aligned.allocate((size_t)(W * lda), s);
+    EF_CUDA(cudaMemcpy2DAsync(aligned.get(), (size_t)lda * 8, keys, (size_t)ld * 8, (size_t)n * 8, W,
+                              cudaMemcpyDeviceToDevice, s));
+    keys = aligned.get();
+    ld = lda;
+  }
   DeviceBuffer<unsigned long long> hist((size_t)(8 * W * 256), s);
   hist.zero();
   byte_histograms<W><<<blocks_for((uint64_t)n, kThreads, (unsigned)ctx.sm_count * 8u), kThreads, 0, s>>>(keys, n, ld,
@@ -834,7 +870,7 @@ int64_t rank_keys_onesweep(Context& ctx, const uint64_t* keys, int64_t n, int64_
   const uint64_t* cur_k = keys;
   int64_t cur_ld = ld;
   const uint32_t* cur_v = nullptr;
-  const size_t smem = (size_t)TILE * (8 + 1);
+  const size_t smem = (size_t)TILE * (8 * W + 4 + 1);
   if (passes) {
     const int64_t ldb = (n + 1) & ~(int64_t)1;
     for (int b = 0; b < 2; b++) {
