@@ -443,14 +443,26 @@ __global__ void col_max(const double* __restrict__ x, int64_t batches, int64_t k
   const int64_t rows_per = (k + gridDim.y - 1) / gridDim.y;
   const int64_t r0 = (int64_t)blockIdx.y * rows_per, r1 = min(lens ? min(k, lens[w]) : k, r0 + rows_per);
   if (col >= n) return;
-  double m = 0.0;
+  // Eight rows at a time into independent maxima, so that eight loads are
+  // in flight per thread.
+  double mx[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   bool bad = false;
   const double* p = x + w * k * n + col;
-  for (int64_t r = r0; r < r1; r++) {
+  int64_t r = r0;
+  for (; r + 8 <= r1; r += 8) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const double v = fabs(p[(r + i) * n]);
+      bad |= !(v <= 1.7976931348623157e308);
+      mx[i] = fmax(mx[i], v);
+    }
+  }
+  for (; r < r1; r++) {
     const double v = fabs(p[r * n]);
     bad |= !(v <= 1.7976931348623157e308);
-    m = fmax(m, v);
+    mx[0] = fmax(mx[0], v);
   }
+  const double m = fmax(fmax(fmax(mx[0], mx[1]), fmax(mx[2], mx[3])), fmax(fmax(mx[4], mx[5]), fmax(mx[6], mx[7])));
   if (bad) atomicOr(status, 1);
   if (m > 0.0) atomicMax(&colmax[w * n + col], (unsigned long long)__double_as_longlong(m));
 }

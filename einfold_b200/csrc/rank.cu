@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(kThreads, MIN_BLOCKS) onesweep_pass(const uint
   constexpr int TILE = kThreads * ITEMS;
   constexpr int WARPS = kThreads / 32;
   static_assert(TILE <= 65535, "a tile's places fit 16 bits");
-  extern __shared__ __align__(16) uint8_t smem[];
+  extern __shared__ __align__(128) uint8_t smem[];
   uint64_t* kstage = (uint64_t*)smem;               // [W][TILE]: the tile's key words
   uint32_t* vstage = (uint32_t*)(kstage + W * TILE);  // [TILE]: its row numbers
   uint8_t* sdig = (uint8_t*)(vstage + TILE);        // [TILE]: the reordered keys' digits
@@ -593,113 +593,161 @@ __global__ void __launch_bounds__(kThreads) rank_runs(const uint64_t* __restrict
 }
 
 // The ranks of the sorted pairs when the rank array is too large for L2:
-// each tile of 2048 sorted positions (claimed in order) finds its keys' run
-// heads and ranks (a look-back over the earlier tiles' head counts gives its
-// first rank), writes first[r] for its heads, and partitions its (row, rank)
-// pairs by bucket = row >> bshift, each bucket's pairs of all tiles in one
-// contiguous region (bucket b holds exactly the rows [b << bshift, (b + 1)
-// << bshift) of the n, so its region's start is known; a look-back over the
-// earlier tiles' bucket counts gives this tile's place in it). The order of
-// pairs within a bucket is of no consequence: scatter_ranks then writes
-// rank[row] for each pair, and the pairs of one bucket, read in order, fall
-// in one rank range of 2^bshift rows that stays in L2 while it is written.
+// each tile of sorted positions (claimed in order; it arrives in shared
+// memory by bulk copies) finds its keys' run heads and ranks (ballots count
+// the heads before each position within a warp, the warps' counts give the
+// tile's own, published at once, and a look-back by one warp over 32 earlier
+// tiles' counts at a time gives its first rank), writes first[r] for its
+// heads, and partitions its (row, rank) pairs by bucket = row >> bshift, each
+// bucket's pairs of all tiles in one contiguous region (bucket b holds
+// exactly the rows [b << bshift, (b + 1) << bshift) of the n, so its region's
+// start is known; a look-back over the earlier tiles' bucket counts, four
+// tiles at a time, gives this tile's place in it). The order of pairs within
+// a bucket is of no consequence: scatter_ranks then writes rank[row] for each
+// pair, and the pairs of one bucket, read in order, fall in one rank range of
+// 2^bshift rows that stays in L2 while it is written. Item i of a lane is
+// position warp·32·ITEMS + 32i + lane of the tile.
 constexpr int kBuckets = 256;
-constexpr int kPartItems = 8;
-constexpr int kPartTile = kThreads * kPartItems;
-
 template <int W>
-__global__ void __launch_bounds__(kThreads) rank_partition(const uint64_t* __restrict__ keys, int64_t ld,
-                                                           const uint32_t* __restrict__ rows, int64_t n, int bshift,
-                                                           uint32_t* __restrict__ head_status,
-                                                           uint32_t* __restrict__ bucket_status,
-                                                           unsigned int* __restrict__ tile_counter,
-                                                           uint64_t* __restrict__ pairs, uint32_t* __restrict__ first,
-                                                           unsigned long long* __restrict__ distinct, int* err) {
+constexpr int part_items() { return W == 1 ? 16 : (W == 2 ? 8 : (W == 3 ? 6 : 4)); }
+
+// Sums a value over a warp.
+__device__ __forceinline__ unsigned int warp_sum(unsigned int v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <int W, int ITEMS>
+__global__ void __launch_bounds__(kThreads, 2) rank_partition(const uint64_t* __restrict__ keys, int64_t ld,
+                                                              const uint32_t* __restrict__ rows, int64_t n, int bshift,
+                                                              uint32_t* __restrict__ head_status,
+                                                              uint32_t* __restrict__ bucket_status,
+                                                              unsigned int* __restrict__ tile_counter,
+                                                              uint64_t* __restrict__ pairs, uint32_t* __restrict__ first,
+                                                              unsigned long long* __restrict__ distinct, int* err) {
+  constexpr int TILE = kThreads * ITEMS;
+  constexpr int WARPS = kThreads / 32;
   typedef cub::BlockScan<unsigned int, kThreads> Scan;
   __shared__ typename Scan::TempStorage tmp;
+  extern __shared__ __align__(128) uint8_t smem[];
+  uint64_t* kstage = (uint64_t*)smem;                 // [W][TILE]: the tile's key words; then its reordered pairs
+  uint32_t* rstage = (uint32_t*)(kstage + W * TILE);  // [TILE]: its rows
+  uint64_t* spairs = kstage;
+  __shared__ __align__(8) uint64_t bar;
   __shared__ unsigned int s_tile, s_before;
+  __shared__ unsigned int wheads[WARPS];      // each warp's heads
   __shared__ unsigned int cnt[kBuckets];      // this tile's pairs of each bucket
-  __shared__ unsigned int at[kBuckets];       // a bucket's next slot in the tile's reordered pairs
+  __shared__ unsigned int at[kBuckets];       // a bucket's first slot in the tile's reordered pairs
   __shared__ long long dbase[kBuckets];       // a bucket's destination minus its first slot in the tile
-  __shared__ __align__(16) uint64_t spairs[kPartTile];
-  const int tid = threadIdx.x;
-  if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  if (tid == 0) {
+    s_tile = atomicAdd(tile_counter, 1u);
+    ptx::mbar_init(&bar, 1);
+    ptx::mbar_fence_init();
+  }
   cnt[tid] = 0;
   __syncthreads();
   const int64_t t = s_tile;
-  const int64_t base = t * kPartTile;
-  const int64_t count = min((int64_t)kPartTile, n - base);
-  const int64_t p0 = base + (int64_t)tid * kPartItems;
-  unsigned int heads = 0, hmask = 0;
-  uint32_t r[kPartItems];
-  {
-    uint64_t prev[W];
-#pragma unroll
-    for (int w = 0; w < W; w++) prev[w] = p0 > 0 && p0 - 1 < n ? keys[(int64_t)w * ld + p0 - 1] : 0;
-#pragma unroll
-    for (int i = 0; i < kPartItems; i++) {
-      const int64_t p = p0 + i;
-      if (p < n) {
-        bool h = p == 0;
-#pragma unroll
-        for (int w = 0; w < W; w++) {
-          const uint64_t k = keys[(int64_t)w * ld + p];
-          h |= k != prev[w];
-          prev[w] = k;
-        }
-        r[i] = rows[p];
-        if (h) {
-          hmask |= 1u << i;
-          heads++;
-        }
-      }
-    }
-  }
-  unsigned int ex, total;
-  Scan(tmp).ExclusiveSum(heads, ex, total);
-  // The heads before this tile: a look-back over the earlier tiles' counts.
+  const int64_t base = t * TILE;
+  const int count = (int)min((int64_t)TILE, n - base);
+  const int kb = count & ~1, rb = count & ~3;  // keys and rows the bulk copies bring
   if (tid == 0) {
+    ptx::mbar_expect_tx(&bar, (uint32_t)(kb * 8 * W + rb * 4));
+    if (kb)
+#pragma unroll
+      for (int w = 0; w < W; w++) ptx::bulk_load(kstage + w * TILE, keys + (int64_t)w * ld + base, (uint32_t)(kb * 8), &bar);
+    if (rb) ptx::bulk_load(rstage, rows + base, (uint32_t)(rb * 4), &bar);
+  }
+  if (!ptx::mbar_wait(&bar, 0)) {
+    // The copies didn't land in time: fail the sort, and wait once more for
+    // them before the block's shared memory goes.
+    atomicOr(err, 1);
+    ptx::mbar_wait(&bar, 0);
+  }
+  auto key_at = [&](int j, int w) -> uint64_t {
+    return j < kb ? kstage[w * TILE + j] : keys[(int64_t)w * ld + base + j];
+  };
+  // Heads, rows, and the heads at or before each item within the warp.
+  uint32_t r[ITEMS];
+  uint32_t hrank[ITEMS];  // that count (bit 31: the item is a head); then the item's rank
+  unsigned int wcount = 0;
+#pragma unroll
+  for (int i = 0; i < ITEMS; i++) {
+    const int j = warp * 32 * ITEMS + i * 32 + lane;
+    bool h = false;
+    if (j < count) {
+      h = base + j == 0;
+#pragma unroll
+      for (int w = 0; w < W; w++) {
+        const uint64_t prev = j > 0 ? key_at(j - 1, w) : (base > 0 ? keys[(int64_t)w * ld + base - 1] : 0);
+        h |= key_at(j, w) != prev;
+      }
+      r[i] = j < rb ? rstage[j] : rows[base + j];
+    }
+    const unsigned heads = __ballot_sync(0xffffffffu, h);
+    hrank[i] = (wcount + __popc(heads & lt_mask) + (h ? 1u : 0u)) | (h ? 0x80000000u : 0u);
+    wcount += __popc(heads);
+  }
+  if (lane == 0) wheads[warp] = wcount;
+  __syncthreads();
+  unsigned int woff = 0, total = 0;
+#pragma unroll
+  for (int w = 0; w < WARPS; w++) {
+    woff += w < warp ? wheads[w] : 0u;
+    total += wheads[w];
+  }
+  // The heads before this tile: published at once, then a look-back by
+  // warp 0 over 32 earlier tiles' counts at a time (flags only go from none
+  // to count to prefix, so an early read of a count stays valid).
+  if (warp == 0) {
     uint32_t* my = head_status + t;
+    if (lane == 0) st_volatile(my, (t == 0 ? kFlagPre : kFlagAgg) | total);
     unsigned int before = 0;
-    if (t == 0) {
-      st_volatile(my, kFlagPre | total);
-    } else {
-      st_volatile(my, kFlagAgg | total);
+    if (t > 0) {
       int64_t tt = t - 1;
       uint64_t start = 0;
       while (true) {
-        const uint32_t v = ld_volatile(head_status + tt);
+        const int64_t idx = tt - lane;
+        const uint32_t v = idx >= 0 ? ld_volatile(head_status + idx) : kFlagPre;
         const uint32_t flag = v & ~kValue;
-        if (flag == 0) {
+        const unsigned waiting = __ballot_sync(0xffffffffu, flag == 0);
+        const unsigned prefix = __ballot_sync(0xffffffffu, flag == kFlagPre);
+        const int f0 = waiting ? __ffs(waiting) - 1 : 32, p = prefix ? __ffs(prefix) - 1 : 32;
+        if (p < f0) {
+          before += warp_sum(lane <= p ? v & kValue : 0u);
+          break;
+        }
+        before += warp_sum(lane < f0 ? v & kValue : 0u);
+        tt -= f0;
+        if (f0 == 0) {
+          // Lane 0's clock decides, so that the warp leaves together.
           if (!start) start = ptx::now_ns();
-          else if (ptx::now_ns() - start > ptx::kWaitNs) {
-            atomicOr(err, 1);
+          if (__shfl_sync(0xffffffffu, ptx::now_ns() - start > ptx::kWaitNs ? 1 : 0, 0)) {
+            if (lane == 0) atomicOr(err, 1);
             break;
           }
-          continue;
         }
-        before += v & kValue;
-        if (flag == kFlagPre || tt == 0) break;
-        tt--;
       }
-      st_volatile(my, kFlagPre | (before + total));
+      if (lane == 0) st_volatile(my, kFlagPre | (before + total));
     }
-    s_before = before;
-    if (base + kPartTile >= n) *distinct = (unsigned long long)(before + total);
+    if (lane == 0) {
+      s_before = before;
+      if (base + TILE >= n) *distinct = (unsigned long long)(before + total);
+    }
   }
   __syncthreads();
   // Ranks; first rows; the pairs' bucket counts.
-  unsigned int cur = s_before + ex;
-  uint64_t pr[kPartItems];
-  unsigned int slot[kPartItems];
+  const unsigned int first_rank = s_before + woff;
+  uint32_t slot[ITEMS];
 #pragma unroll
-  for (int i = 0; i < kPartItems; i++) {
-    if (p0 + i < n) {
-      if (hmask >> i & 1u) {
-        first[cur] = r[i];
-        cur++;
-      }
-      pr[i] = ((uint64_t)r[i] << 32) | (cur - 1);
+  for (int i = 0; i < ITEMS; i++) {
+    const int j = warp * 32 * ITEMS + i * 32 + lane;
+    if (j < count) {
+      const unsigned int rk = first_rank + (hrank[i] & 0x7fffffffu) - 1u;
+      if (hrank[i] >> 31) first[rk] = r[i];
+      hrank[i] = rk;
       slot[i] = atomicAdd(&cnt[r[i] >> bshift], 1u);
     }
   }
@@ -707,37 +755,51 @@ __global__ void __launch_bounds__(kThreads) rank_partition(const uint64_t* __res
   const unsigned int mine = cnt[tid];
   const int64_t bucket_rows = (int64_t)1 << bshift;
   uint32_t* bst = bucket_status + t * kBuckets + tid;
-  if (t == 0) st_volatile(bst, kFlagPre | mine);
-  else st_volatile(bst, kFlagAgg | mine);
+  st_volatile(bst, (t == 0 ? kFlagPre : kFlagAgg) | mine);
   unsigned int bex;
   Scan(tmp).ExclusiveSum(mine, bex);
   unsigned int bbefore = 0;
   if (t > 0) {
+    constexpr int kWindow = 4;
     int64_t tt = t - 1;
     uint64_t start = 0;
+    bool failed = false;
     while (true) {
-      const uint32_t v = ld_volatile(bucket_status + tt * kBuckets + tid);
-      const uint32_t flag = v & ~kValue;
-      if (flag == 0) {
+      uint32_t v[kWindow];
+#pragma unroll
+      for (int k = 0; k < kWindow; k++) v[k] = tt - k >= 0 ? ld_volatile(bucket_status + (tt - k) * kBuckets + tid) : 0u;
+      bool done = false;
+      int used = 0;
+#pragma unroll
+      for (int k = 0; k < kWindow; k++) {
+        if (done || used < k || tt - k < 0) continue;
+        const uint32_t flag = v[k] & ~kValue;
+        if (flag == 0) continue;
+        bbefore += v[k] & kValue;
+        used = k + 1;
+        if (flag == kFlagPre) done = true;
+      }
+      if (done) break;
+      if (used == 0) {
         if (!start) start = ptx::now_ns();
         else if (ptx::now_ns() - start > ptx::kWaitNs) {
-          atomicOr(err, 1);
+          failed = true;
           break;
         }
-        continue;
       }
-      bbefore += v & kValue;
-      if (flag == kFlagPre || tt == 0) break;
-      tt--;
+      tt -= used;
     }
+    if (failed) atomicOr(err, 1);
     st_volatile(bst, kFlagPre | (bbefore + mine));
   }
   at[tid] = bex;
   dbase[tid] = (long long)tid * bucket_rows + (long long)bbefore - (long long)bex;
   __syncthreads();
 #pragma unroll
-  for (int i = 0; i < kPartItems; i++)
-    if (p0 + i < n) spairs[at[(uint32_t)(pr[i] >> 32) >> bshift] + slot[i]] = pr[i];
+  for (int i = 0; i < ITEMS; i++) {
+    const int j = warp * 32 * ITEMS + i * 32 + lane;
+    if (j < count) spairs[at[r[i] >> bshift] + slot[i]] = ((uint64_t)r[i] << 32) | hrank[i];
+  }
   __syncthreads();
   for (int j = tid; j < count; j += kThreads) {
     const uint64_t x = spairs[j];
@@ -859,7 +921,8 @@ int64_t rank_keys_onesweep(Context& ctx, const uint64_t* keys, int64_t n, int64_
   const int passes = (int)pw.size();
   DeviceBuffer<uint32_t> dstart((size_t)std::max(1, passes) * 256, s);
   if (passes) EF_CUDA(cudaMemcpyAsync(dstart.get(), starts.data(), starts.size() * 4, cudaMemcpyHostToDevice, s));
-  const int64_t status_words = std::max(tiles * 256, std::max(rtiles, (n + kPartTile - 1) / kPartTile));
+  constexpr int PTILE = kThreads * part_items<W>();
+  const int64_t status_words = std::max(tiles * 256, std::max(rtiles, (n + PTILE - 1) / PTILE));
   DeviceBuffer<uint32_t> status((size_t)status_words, s);
   DeviceBuffer<unsigned int> counters((size_t)passes + 1, s);
   counters.zero();
@@ -897,7 +960,8 @@ int64_t rank_keys_onesweep(Context& ctx, const uint64_t* keys, int64_t n, int64_
     cur_v = identity.get();
   }
   DeviceBuffer<unsigned long long> distinct(1, s);
-  EF_CUDA(cudaMemsetAsync(status.get(), 0, (size_t)rtiles * 4, s));
+  // The finish's per-tile head counts start unpublished (either finish's tiles).
+  EF_CUDA(cudaMemsetAsync(status.get(), 0, (size_t)std::max(rtiles, (n + PTILE - 1) / PTILE) * 4, s));
   if (n <= kScatterInL2) {
     // The rank array fits in L2: its scattered writes merge there.
     rank_runs<W, RITEMS><<<(unsigned)rtiles, kThreads, 0, s>>>(cur_k, cur_ld, cur_v, n, status.get(),
@@ -908,13 +972,16 @@ int64_t rank_keys_onesweep(Context& ctx, const uint64_t* keys, int64_t n, int64_
     // Ranks partitioned by the rows' high bits, then scattered bucket by bucket.
     int bshift = 0;
     while ((((int64_t)1 << bshift) * kBuckets) < n) bshift++;
-    const int64_t ptiles = (n + kPartTile - 1) / kPartTile;
+    const int64_t ptiles = (n + PTILE - 1) / PTILE;
     DeviceBuffer<uint32_t> bstatus((size_t)(ptiles * kBuckets), s);
     DeviceBuffer<uint64_t> pairs((size_t)n, s);
     EF_CUDA(cudaMemsetAsync(bstatus.get(), 0, (size_t)(ptiles * kBuckets) * 4, s));
-    rank_partition<W><<<(unsigned)ptiles, kThreads, 0, s>>>(cur_k, cur_ld, cur_v, n, bshift, status.get(),
-                                                            bstatus.get(), counters.get() + passes, pairs.get(),
-                                                            first, distinct.get(), err.get());
+    const size_t psmem = (size_t)PTILE * (8 * W + 4);
+    EF_CUDA(cudaFuncSetAttribute(rank_partition<W, part_items<W>()>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)psmem));
+    rank_partition<W, part_items<W>()><<<(unsigned)ptiles, kThreads, psmem, s>>>(
+        cur_k, cur_ld, cur_v, n, bshift, status.get(), bstatus.get(), counters.get() + passes, pairs.get(), first,
+        distinct.get(), err.get());
     scatter_ranks<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, s>>>(pairs.get(), n, rank);
     ctx.kernels += 2;
   }

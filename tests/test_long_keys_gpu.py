@@ -135,3 +135,30 @@ def test_fold_joined_on_long_url_keys():
                 [ir.Output(0), ir.Output(2)])
     got, want = _fold_both(f, a, b)
     assert_same_rows(rows_of(got.batches), rows_of(want.batches), exact=True)
+
+
+def test_two_column_keys_beyond_4m_rows():
+    # Keys of two int64 columns (more than one word) over 4.4M rows: the
+    # ranks go back to rows by bucket (beyond L2's share), as the one-word
+    # case does; the order of non-NULL integer keys is their signed
+    # lexicographic order, checked against the oracle on a prefix of rows.
+    n = 4_400_000
+    rng = oracle.Rng.seeded(14, 2)
+    c1 = (rng.u64s(n) % np.uint64(3000)).astype(np.int64) - 1500
+    c2 = (rng.u64s(n) >> np.uint64(1)).astype(np.int64) * np.where(rng.u64s(n) & np.uint64(1), 1, -1)
+    dup = np.arange(7, n, 7)  # every seventh row repeats an earlier row's key
+    c1[dup], c2[dup] = c1[dup // 2], c2[dup // 2]
+    batch = pa.record_batch([pa.array(c1), pa.array(c2)], names=["c0", "c1"])
+    got = K.rank_columns(K.Relation(batch.schema, [batch]), [0, 1], K.FloatKeys(0))
+    order = np.lexsort((c2, c1))
+    s1, s2 = c1[order], c2[order]
+    head = np.r_[True, (s1[1:] != s1[:-1]) | (s2[1:] != s2[:-1])]
+    want_rank = np.empty(n, np.int64)
+    want_rank[order] = np.cumsum(head) - 1
+    assert np.array_equal(got.rank.astype(np.int64), want_rank)
+    assert np.array_equal(got.first.astype(np.int64), order[head])
+    m = 60_000
+    small = _rank_both([pa.array(c1[:m]), pa.array(c2[:m])])
+    o = np.lexsort((c2[:m], c1[:m]))
+    h = np.r_[True, (c1[:m][o][1:] != c1[:m][o][:-1]) | (c2[:m][o][1:] != c2[:m][o][:-1])]
+    assert np.array_equal(small.first.astype(np.int64), o[h])
