@@ -623,8 +623,10 @@ def _ranking(hbm, basis):
     4M keys (the sorting path's join column over a and b). Two fractions of
     HBM bandwidth: over the bytes the kernels move, per key 8 read for the
     byte histograms, per 8-bit pass 12 read and 12 written (the first pass
-    reads no row numbers), then 12 read and 4 written for the ranks plus 4
-    per distinct key for the first rows; and over the algorithmic bytes of
+    reads no row numbers), then 12 read and 4 written for the ranks (beyond
+    4M keys 8 more written and read again: the (row, rank) pairs partitioned
+    by row bucket) plus 4 per distinct key for the first rows; and over the
+    algorithmic bytes of
     the ranking itself, 8 B of key read, 4 B of rank and 4 B of first row
     written per key."""
     import ctypes
@@ -662,7 +664,8 @@ def _ranking(hbm, basis):
             times.append(e0.elapsed_time(e1))
         ms = statistics.median(times[1:])
         passes = varying
-        moved = n * (8 + (20 + (passes - 1) * 24 if passes else 0) + 16) + k.value * 4
+        finish = 32 if n > (1 << 22) else 16
+        moved = n * (8 + (20 + (passes - 1) * 24 if passes else 0) + finish) + k.value * 4
         algorithmic = n * 16
         out[f"n{n}"] = {"keys": n, "distinct": k.value, "ms": ms, "gkeys_per_s": n / ms / 1e6, "passes": passes,
                         "moved_gb_per_s": moved / ms / 1e6, "frac_of_hbm": moved / ms / 1e6 / hbm,
