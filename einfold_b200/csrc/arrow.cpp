@@ -255,6 +255,8 @@ struct ArrayPrivate {
   std::vector<ArrowArray*> child_ptrs;
   std::vector<std::vector<const void*>> child_buffers;
   std::vector<const void*> buffers;
+  std::vector<ArrowArray> dicts;  // dictionary columns' values
+  std::vector<std::vector<const void*>> dict_buffers;
 };
 
 static void release_child(ArrowArray* a) { a->release = nullptr; }
@@ -272,19 +274,27 @@ static void fill_array(OutBatch&& batch, ArrowArray* out) {
   p->children.resize(n);
   p->child_ptrs.resize(n);
   p->child_buffers.resize(n);
-  for (size_t i = 0; i < n; i++) {
-    OutColumn& c = p->columns[i];
-    auto& bufs = p->child_buffers[i];
+  p->dicts.resize(n);
+  p->dict_buffers.resize(n);
+  auto fill = [](OutColumn& c, std::vector<const void*>& bufs, ArrowArray& a) {
     bufs.push_back(c.null_count ? c.validity.ptr : nullptr);
     bufs.push_back(c.values.ptr);
     if (is_var(c.kind)) bufs.push_back(c.data.ptr);
-    ArrowArray& a = p->children[i];
     std::memset(&a, 0, sizeof a);
     a.length = c.length;
     a.null_count = c.null_count;
     a.n_buffers = (int64_t)bufs.size();
     a.buffers = bufs.data();
     a.release = release_child;
+  };
+  for (size_t i = 0; i < n; i++) {
+    OutColumn& c = p->columns[i];
+    ArrowArray& a = p->children[i];
+    fill(c, p->child_buffers[i], a);
+    if (c.dictionary) {
+      fill(*c.dictionary, p->dict_buffers[i], p->dicts[i]);
+      a.dictionary = &p->dicts[i];
+    }
     p->child_ptrs[i] = &a;
   }
   p->buffers.push_back(nullptr);
@@ -303,6 +313,8 @@ struct SchemaPrivate {
   std::vector<std::string> formats, names;
   std::vector<ArrowSchema> children;
   std::vector<ArrowSchema*> child_ptrs;
+  std::vector<std::string> dict_formats;  // dictionary fields' value types
+  std::vector<ArrowSchema> dicts;
 };
 
 static void release_child_schema(ArrowSchema* s) { s->release = nullptr; }
@@ -320,6 +332,8 @@ void export_schema(const std::vector<Field>& fields, ArrowSchema* out) {
   p->names.resize(n);
   p->children.resize(n);
   p->child_ptrs.resize(n);
+  p->dict_formats.resize(n);
+  p->dicts.resize(n);
   for (size_t i = 0; i < n; i++) {
     p->formats[i] = fields[i].format;
     p->names[i] = fields[i].name;
@@ -329,6 +343,16 @@ void export_schema(const std::vector<Field>& fields, ArrowSchema* out) {
     s.name = p->names[i].c_str();
     s.flags = fields[i].nullable ? ARROW_FLAG_NULLABLE : 0;
     s.release = release_child_schema;
+    if (fields[i].dictionary) {
+      p->dict_formats[i] = fields[i].dictionary->format;
+      ArrowSchema& d = p->dicts[i];
+      std::memset(&d, 0, sizeof d);
+      d.format = p->dict_formats[i].c_str();
+      d.name = "";
+      d.flags = ARROW_FLAG_NULLABLE;
+      d.release = release_child_schema;
+      s.dictionary = &d;
+    }
     p->child_ptrs[i] = &s;
   }
   std::memset(out, 0, sizeof *out);
@@ -364,13 +388,77 @@ void release_result(einfold_result* r) {
   r->n_batches = 0;
 }
 
+// Dictionary indices of any integer type.
+static int64_t read_index(const uint8_t* p, Kind k, int64_t i) {
+  switch (k) {
+    case Kind::Int8: return ((const int8_t*)p)[i];
+    case Kind::UInt8: return ((const uint8_t*)p)[i];
+    case Kind::Int16: return ((const int16_t*)p)[i];
+    case Kind::UInt16: return ((const uint16_t*)p)[i];
+    case Kind::Int32: return ((const int32_t*)p)[i];
+    case Kind::UInt32: return ((const uint32_t*)p)[i];
+    case Kind::Int64: return ((const int64_t*)p)[i];
+    case Kind::UInt64: {
+      const uint64_t v = ((const uint64_t*)p)[i];
+      return v > (uint64_t)INT64_MAX ? -1 : (int64_t)v;
+    }
+    default: fail(EINFOLD_INVALID, "a dictionary whose indices aren't integers");
+  }
+  return -1;
+}
+
+static int64_t largest_index(Kind k) {
+  switch (k) {
+    case Kind::Int8: return INT8_MAX;
+    case Kind::UInt8: return UINT8_MAX;
+    case Kind::Int16: return INT16_MAX;
+    case Kind::UInt16: return UINT16_MAX;
+    case Kind::Int32: return INT32_MAX;
+    case Kind::UInt32: return UINT32_MAX;
+    case Kind::Int64:
+    case Kind::UInt64: return INT64_MAX;
+    default: fail(EINFOLD_INVALID, "a dictionary whose indices aren't integers");
+  }
+  return 0;
+}
+
+static void write_index(uint8_t* p, Kind k, int64_t i, int64_t v) {
+  switch (k) {
+    case Kind::Int8: ((int8_t*)p)[i] = (int8_t)v; break;
+    case Kind::UInt8: ((uint8_t*)p)[i] = (uint8_t)v; break;
+    case Kind::Int16: ((int16_t*)p)[i] = (int16_t)v; break;
+    case Kind::UInt16: ((uint16_t*)p)[i] = (uint16_t)v; break;
+    case Kind::Int32: ((int32_t*)p)[i] = (int32_t)v; break;
+    case Kind::UInt32: ((uint32_t*)p)[i] = (uint32_t)v; break;
+    default: ((int64_t*)p)[i] = v; break;
+  }
+}
+
 OutColumn copy_column(const Column& c, const Field& f) {
   if (c.device) fail(EINFOLD_INVALID, "carrying a device column is not supported");
   OutColumn o;
   o.format = f.format;
   o.nullable = f.nullable;
   o.length = c.length;
-  if (c.dictionary) fail(EINFOLD_INVALID, "carrying a dictionary column is not supported");
+  if (c.dictionary) {
+    // The indices as they are, and the dictionary's values.
+    if (!f.dictionary) fail(EINFOLD_INVALID, "a dictionary column of a field without a dictionary");
+    o.kind = c.index_kind;
+    const int w = width_of(c.index_kind);
+    const int64_t nulls = c.nulls();
+    o.null_count = nulls;
+    if (nulls) {
+      o.validity = Buffer(HostBuffer((size_t)((c.length + 7) / 8)));
+      std::memset(o.validity.ptr, 0, o.validity.bytes);
+      uint8_t* v = o.validity.as<uint8_t>();
+      for (int64_t i = 0; i < c.length; i++)
+        if (c.valid(i)) v[i >> 3] |= (uint8_t)(1u << (i & 7));
+    }
+    o.values = Buffer(HostBuffer((size_t)(c.length * w)));
+    if (c.length) std::memcpy(o.values.ptr, c.values + c.offset * w, (size_t)(c.length * w));
+    o.dictionary = std::make_shared<OutColumn>(copy_column(*c.dictionary, *f.dictionary));
+    return o;
+  }
   o.kind = c.kind;
   int64_t nulls = c.nulls();
   o.null_count = nulls;
@@ -412,6 +500,190 @@ OutColumn copy_column(const Column& c, const Field& f) {
     if (c.length) std::memcpy(o.values.ptr, c.values + c.offset * w, (size_t)(c.length * w));
   }
   return o;
+}
+
+// A row's value as bytes, for hashing and copying (`width` bytes of a
+// fixed-width kind, or the var-length bytes).
+static std::string value_bytes(const OutColumn& v, int64_t i, int width) {
+  if (is_var(v.kind)) {
+    const bool large = v.kind == Kind::LargeUtf8 || v.kind == Kind::LargeBinary;
+    const int64_t a = large ? v.values.as<int64_t>()[i] : v.values.as<int32_t>()[i];
+    const int64_t b = large ? v.values.as<int64_t>()[i + 1] : v.values.as<int32_t>()[i + 1];
+    return std::string((const char*)v.data.as<uint8_t>() + a, (size_t)(b - a));
+  }
+  if (v.kind == Kind::Bool) return std::string(1, (char)((v.values.as<uint8_t>()[i >> 3] >> (i & 7)) & 1));
+  return std::string((const char*)v.values.as<uint8_t>() + i * width, (size_t)width);
+}
+
+OutColumn dictionary_encode(OutColumn&& v, const Field& f) {
+  if (!f.dictionary) fail(EINFOLD_INVALID, "dictionary_encode of a field without a dictionary");
+  if (v.values.device >= 0 || v.data.device >= 0 || v.validity.device >= 0)
+    fail(EINFOLD_INVALID, "dictionary-encoded key columns of results left in device memory are not supported");
+  const Kind ik = kind_of(f.format.c_str());
+  const int64_t cap = largest_index(ik);
+  const int iw = width_of(ik);
+  const int w = is_var(v.kind) || v.kind == Kind::Bool ? 0 : width_of(v.kind);
+  const int64_t n = v.length;
+  auto valid = [&](int64_t i) { return !v.null_count || ((v.validity.as<uint8_t>()[i >> 3] >> (i & 7)) & 1); };
+  // Distinct values in the order of their first rows; NULL is one of them.
+  std::unordered_map<std::string, int64_t> seen;
+  std::vector<int64_t> rep;  // each distinct value's first row
+  int64_t null_at = -1;
+  OutColumn o;
+  o.format = f.format;
+  o.name = v.name;
+  o.nullable = f.nullable;
+  o.kind = ik;
+  o.length = n;
+  o.values = Buffer(HostBuffer((size_t)(n ? n * iw : 1)));
+  for (int64_t i = 0; i < n; i++) {
+    int64_t d;
+    if (!valid(i)) {
+      if (null_at < 0) {
+        null_at = (int64_t)rep.size();
+        rep.push_back(-1);
+      }
+      d = null_at;
+    } else {
+      auto it = seen.emplace(value_bytes(v, i, w), (int64_t)rep.size());
+      if (it.second) rep.push_back(i);
+      d = it.first->second;
+    }
+    if (d > cap) fail(EINFOLD_COMPUTE, "%lld distinct keys exceed the dictionary's index type", (long long)(d + 1));
+    write_index(o.values.as<uint8_t>(), ik, i, d);
+  }
+  auto dict = std::make_shared<OutColumn>();
+  dict->format = f.dictionary->format;
+  dict->kind = v.kind;
+  dict->length = (int64_t)rep.size();
+  const int64_t m = dict->length;
+  if (null_at >= 0) {
+    dict->null_count = 1;
+    dict->validity = Buffer(HostBuffer((size_t)((m + 7) / 8)));
+    std::memset(dict->validity.ptr, 0xff, dict->validity.bytes);
+    dict->validity.as<uint8_t>()[null_at >> 3] &= (uint8_t)~(1u << (null_at & 7));
+  }
+  if (is_var(v.kind)) {
+    const bool large = v.kind == Kind::LargeUtf8 || v.kind == Kind::LargeBinary;
+    int64_t total = 0;
+    for (int64_t r : rep) total += r < 0 ? 0 : (int64_t)value_bytes(v, r, 0).size();
+    dict->values = Buffer(HostBuffer((size_t)(m + 1) * (large ? 8 : 4)));
+    dict->data = Buffer(HostBuffer((size_t)(total ? total : 1)));
+    int64_t pos = 0;
+    for (int64_t j = 0; j < m; j++) {
+      if (large) dict->values.as<int64_t>()[j] = pos; else dict->values.as<int32_t>()[j] = (int32_t)pos;
+      if (rep[(size_t)j] < 0) continue;
+      const std::string b = value_bytes(v, rep[(size_t)j], 0);
+      std::memcpy(dict->data.as<uint8_t>() + pos, b.data(), b.size());
+      pos += (int64_t)b.size();
+    }
+    if (large) dict->values.as<int64_t>()[m] = pos; else dict->values.as<int32_t>()[m] = (int32_t)pos;
+  } else if (v.kind == Kind::Bool) {
+    dict->values = Buffer(HostBuffer((size_t)((m + 7) / 8 ? (m + 7) / 8 : 1)));
+    std::memset(dict->values.ptr, 0, dict->values.bytes);
+    for (int64_t j = 0; j < m; j++)
+      if (rep[(size_t)j] >= 0 && value_bytes(v, rep[(size_t)j], 0)[0])
+        dict->values.as<uint8_t>()[j >> 3] |= (uint8_t)(1u << (j & 7));
+  } else {
+    dict->values = Buffer(HostBuffer((size_t)(m ? m * w : 1)));
+    std::memset(dict->values.ptr, 0, dict->values.bytes);
+    for (int64_t j = 0; j < m; j++)
+      if (rep[(size_t)j] >= 0)
+        std::memcpy(dict->values.as<uint8_t>() + j * w, v.values.as<uint8_t>() + rep[(size_t)j] * w, (size_t)w);
+  }
+  o.dictionary = std::move(dict);
+  return o;
+}
+
+Relation decode_dictionaries(const Relation& r, const std::vector<int>& cols, std::vector<HostBuffer>& keep) {
+  Relation out = r;
+  for (int c : cols) {
+    if (c < 0 || c >= (int)r.fields.size() || !r.fields[c].dictionary) continue;
+    if (r.device >= 0) fail(EINFOLD_INVALID, "dictionary columns in device memory are not decoded here");
+    Field vf = *r.fields[c].dictionary;
+    vf.name = r.fields[c].name;
+    vf.nullable = true;
+    out.fields[c] = vf;
+    for (size_t bi = 0; bi < r.batches.size(); bi++) {
+      const Column& col = r.batches[bi].columns[c];
+      if (!col.dictionary) fail(EINFOLD_INVALID, "a dictionary column without its dictionary");
+      const Column& d = *col.dictionary;
+      const int64_t n = col.length;
+      Column nc;
+      nc.kind = d.kind;
+      nc.length = n;
+      nc.offset = 0;
+      // Each row's dictionary entry, or -1 for a NULL row.
+      std::vector<int64_t> at((size_t)n);
+      int64_t nulls = 0;
+      for (int64_t i = 0; i < n; i++) {
+        int64_t j = -1;
+        if (col.valid(i)) {
+          j = read_index(col.values, col.index_kind, col.offset + i);
+          if (j < 0 || j >= d.length) fail(EINFOLD_INVALID, "a dictionary index out of range");
+          if (!d.valid(j)) j = -1;
+        }
+        at[(size_t)i] = j;
+        nulls += j < 0;
+      }
+      nc.null_count = nulls;
+      if (nulls) {
+        HostBuffer bits((size_t)((n + 7) / 8));
+        std::memset(bits.ptr, 0, bits.bytes);
+        for (int64_t i = 0; i < n; i++)
+          if (at[(size_t)i] >= 0) bits.as<uint8_t>()[i >> 3] |= (uint8_t)(1u << (i & 7));
+        nc.validity = bits.as<uint8_t>();
+        keep.push_back(std::move(bits));
+      }
+      if (is_var(d.kind)) {
+        const bool large = d.kind == Kind::LargeUtf8 || d.kind == Kind::LargeBinary;
+        int64_t total = 0;
+        for (int64_t i = 0; i < n; i++)
+          if (at[(size_t)i] >= 0) {
+            int64_t l;
+            d.bytes(at[(size_t)i], &l);
+            total += l;
+          }
+        if (!large && total > INT32_MAX) fail(EINFOLD_COMPUTE, "decoded dictionary keys over 2 GiB in one batch");
+        HostBuffer offs((size_t)(n + 1) * (large ? 8 : 4)), data((size_t)(total ? total : 1));
+        int64_t pos = 0;
+        for (int64_t i = 0; i < n; i++) {
+          if (large) offs.as<int64_t>()[i] = pos; else offs.as<int32_t>()[i] = (int32_t)pos;
+          if (at[(size_t)i] < 0) continue;
+          int64_t l;
+          const uint8_t* src = d.bytes(at[(size_t)i], &l);
+          std::memcpy(data.as<uint8_t>() + pos, src, (size_t)l);
+          pos += l;
+        }
+        if (large) offs.as<int64_t>()[n] = pos; else offs.as<int32_t>()[n] = (int32_t)pos;
+        nc.values = offs.as<uint8_t>();
+        nc.data = data.as<uint8_t>();
+        keep.push_back(std::move(offs));
+        keep.push_back(std::move(data));
+      } else if (d.kind == Kind::Bool) {
+        HostBuffer bits((size_t)((n + 7) / 8 ? (n + 7) / 8 : 1));
+        std::memset(bits.ptr, 0, bits.bytes);
+        for (int64_t i = 0; i < n; i++) {
+          const int64_t j = at[(size_t)i];
+          if (j >= 0 && ((d.values[(d.offset + j) >> 3] >> ((d.offset + j) & 7)) & 1))
+            bits.as<uint8_t>()[i >> 3] |= (uint8_t)(1u << (i & 7));
+        }
+        nc.values = bits.as<uint8_t>();
+        keep.push_back(std::move(bits));
+      } else {
+        const int w = width_of(d.kind);
+        HostBuffer vals((size_t)(n ? n * w : 1));
+        std::memset(vals.ptr, 0, vals.bytes);
+        for (int64_t i = 0; i < n; i++)
+          if (at[(size_t)i] >= 0)
+            std::memcpy(vals.as<uint8_t>() + i * w, d.values + (d.offset + at[(size_t)i]) * w, (size_t)w);
+        nc.values = vals.as<uint8_t>();
+        keep.push_back(std::move(vals));
+      }
+      out.batches[bi].columns[c] = nc;
+    }
+  }
+  return out;
 }
 
 }  // namespace ef

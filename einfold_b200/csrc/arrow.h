@@ -159,6 +159,9 @@ struct OutColumn {
   Buffer values;
   Buffer data;      // var-length kinds only
   Kind kind = Kind::Other;
+  // A dictionary column: `values` holds the indices (of `kind`), and this
+  // the dictionary's values.
+  std::shared_ptr<OutColumn> dictionary;
 };
 
 struct OutBatch {
@@ -171,7 +174,18 @@ void export_result(std::vector<OutBatch>&& batches, const std::vector<Field>& sc
 void export_schema(const std::vector<Field>& fields, ArrowSchema* out);
 void release_result(einfold_result* r);
 
-// A deep copy of rows [0, length) of a column, for carried domain columns.
+// A deep copy of rows [0, length) of a column, for carried domain columns
+// (a dictionary column with its dictionary).
 OutColumn copy_column(const Column& c, const Field& f);
+
+// A host column of values as a column of the dictionary field `f`: the
+// distinct values (a NULL among them once, where any row is NULL) in the
+// order of their first rows, and each row's index into them.
+OutColumn dictionary_encode(OutColumn&& values, const Field& f);
+
+// `r` with its dictionary-encoded columns among `cols` replaced by their
+// values, row by row (a row is NULL where its index or its value is), in
+// host buffers `keep` holds. Host relations only.
+Relation decode_dictionaries(const Relation& r, const std::vector<int>& cols, std::vector<HostBuffer>& keep);
 
 }  // namespace ef

@@ -434,16 +434,33 @@ __global__ void domain_lookup(int64_t rows, const uint32_t* __restrict__ xr, con
 struct StagedKeySet {
   std::vector<DeviceColumn> cols;
   std::vector<Kind> kinds;
+  // Decoded from a dictionary: compared by bits whatever the host's float
+  // keys (DataFusion takes -0.0 and 0.0 as one key in float columns, not in
+  // dictionary-encoded ones; options.rs:19-22).
+  std::vector<bool> dictionary;
 };
 
+// Dictionary-encoded key columns are staged as their values, row by row
+// (decoded on the host; a NULL index or a NULL dictionary value is a NULL
+// key), so that they rank, join and group as the plain columns of their
+// values do.
 StagedKeySet stage_set(Context& ctx, const Relation& r, const std::vector<int>& cols) {
   StagedKeySet s;
+  bool dictionary = false;
   for (int c : cols) {
-    const Field& f = r.fields[c];
-    if (f.dictionary) decline("dictionary-encoded keys are ranked by the host plan");
-    s.cols.push_back(stage_column(ctx, r, c, true));
-    s.kinds.push_back(f.kind);
+    if (c < 0 || c >= (int)r.fields.size()) fail(EINFOLD_INVALID, "no column %d", c);
+    dictionary = dictionary || r.fields[c].dictionary;
   }
+  if (dictionary && r.device >= 0) decline("dictionary-encoded keys in device memory are ranked by the host plan");
+  std::vector<HostBuffer> keep;
+  const Relation decoded = dictionary ? decode_dictionaries(r, cols, keep) : Relation();
+  const Relation& src = dictionary ? decoded : r;
+  for (int c : cols) {
+    s.cols.push_back(stage_column(ctx, src, c, true));
+    s.kinds.push_back(src.fields[c].kind);
+    s.dictionary.push_back((bool)r.fields[c].dictionary);
+  }
+  if (dictionary) EF_CUDA(cudaStreamSynchronize(ctx.stream));  // the decoded buffers go on return
   return s;
 }
 
@@ -503,7 +520,7 @@ KeyLayout layout_of(Context& ctx, const std::vector<const StagedKeySet*>& sets, 
       k.block = block[i];
       k.max_len = max_len[i];
       k.len_bytes = len_bytes[i];
-      k.canon_zero = float_keys == 1 && is_float(c.kind);
+      k.canon_zero = float_keys == 1 && is_float(c.kind) && !st->dictionary[i];
     }
     DeviceBuffer<KeyCol> d(kc.size(), s);
     EF_CUDA(cudaMemcpyAsync(d.get(), kc.data(), kc.size() * sizeof(KeyCol), cudaMemcpyHostToDevice, s));
@@ -943,6 +960,7 @@ FoldOutput discriminate_fold(Context& ctx, const FoldD& f, const Relation& a, co
       size_t j = 0;
       while (outs[j] != (int)i) j++;
       const DeviceColumn& src = (from_a ? a_o : b_o).cols[j];
+      const bool src_dict = (from_a ? a_o : b_o).dictionary[j];
       const uint32_t* first = from_a ? x.first.get() : y.first.get();
       const uint32_t* g = from_a ? gx.get() : gy.get();
       OutColumn c;
@@ -991,7 +1009,8 @@ FoldOutput discriminate_fold(Context& ctx, const FoldD& f, const Relation& a, co
         DeviceBuffer<uint8_t> vals((size_t)(groups ? groups * width : 1), s);
         if (groups)
           gather_fixed<<<blocks_for(groups, 256), 256, 0, s>>>(src.ptr(), src.valid.get(), width,
-                                                               o.float_keys == 1 && is_float(src.kind), first, g, groups,
+                                                               o.float_keys == 1 && is_float(src.kind) && !src_dict,
+                                                               first, g, groups,
                                                                vals.get(), cvalid.get(), cn.get());
         c.values = result_buffer(ctx, vals, (size_t)(groups * width), o.result_on_device);
       }
@@ -1003,6 +1022,11 @@ FoldOutput discriminate_fold(Context& ctx, const FoldD& f, const Relation& a, co
         DeviceBuffer<uint8_t> bits((size_t)((groups + 7) / 8), s);
         pack_bits(ctx, cvalid.get(), groups, bits.get());
         c.validity = result_buffer(ctx, bits, (size_t)((groups + 7) / 8), o.result_on_device);
+      }
+      if (schema[i].dictionary) {
+        // A dictionary-encoded key: the gathered values, encoded again.
+        c.format = schema[i].dictionary->format;
+        c = dictionary_encode(std::move(c), schema[i]);
       }
       out_batch.columns.push_back(std::move(c));
     }
