@@ -1192,7 +1192,7 @@ bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd,
   // from them, one product a tile each. The exports cover only the tiles
   // some pair of is allowed (export_plan counts them per block), 14 bytes a
   // pair of those. Batches go in chunks whose exports fit the export limit
-  // (EINFOLD_BACKWARD_EXPORT_MB, 8192 by default): all in one when they fit,
+  // (EINFOLD_BACKWARD_EXPORT_MB, 4096 by default): all in one when they fit,
   // else in chunks of at most half of it in two buffers, the chunks
   // alternating between the call's stream and the context's second stream,
   // so that one chunk's kernels run beside the other's and a chunk's last
@@ -1202,7 +1202,7 @@ bool backward_split(Context& ctx, const AttentionGradients& g, const double* dd,
   const int64_t n_kb = lk_pad / GM, n_qb = lq_pad / GM;
   static const size_t limit = [] {
     const char* e = std::getenv("EINFOLD_BACKWARD_EXPORT_MB");
-    const long long mb = e ? std::atoll(e) : 8192;
+    const long long mb = e ? std::atoll(e) : 4096;
     return (size_t)std::max(0ll, mb) << 20;
   }();
   DeviceBuffer<int32_t> plan((size_t)(2 * W * (n_kb + n_qb)), s);
