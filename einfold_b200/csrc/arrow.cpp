@@ -11,6 +11,16 @@ namespace ef {
 
 Kind kind_of(const char* f) {
   if (!f) return Kind::Other;
+  if (f[0] == 't' && f[1]) {
+    // Temporal types: dates (tdD, tdm), times (tts, ttm, ttu, ttn),
+    // timestamps (ts?:zone), durations (tD?).
+    if (f[1] == 'd' && f[2] && !f[3]) return f[2] == 'D' ? Kind::Date32 : (f[2] == 'm' ? Kind::Date64 : Kind::Other);
+    if (f[1] == 't' && f[2] && !f[3])
+      return (f[2] == 's' || f[2] == 'm') ? Kind::Time32 : ((f[2] == 'u' || f[2] == 'n') ? Kind::Time64 : Kind::Other);
+    if (f[1] == 's' && f[2] && f[3] == ':') return Kind::Timestamp;
+    if (f[1] == 'D' && f[2] && !f[3]) return Kind::Duration;
+    return Kind::Other;
+  }
   if (f[0] && f[1] == 0) {
     switch (f[0]) {
       case 'c': return Kind::Int8;
@@ -41,6 +51,8 @@ int width_of(Kind k) {
     case Kind::Int16: case Kind::UInt16: case Kind::Float16: return 2;
     case Kind::Int32: case Kind::UInt32: case Kind::Float32: return 4;
     case Kind::Int64: case Kind::UInt64: case Kind::Float64: return 8;
+    case Kind::Date32: case Kind::Time32: return 4;
+    case Kind::Date64: case Kind::Time64: case Kind::Timestamp: case Kind::Duration: return 8;
     default: return 0;
   }
 }
@@ -211,7 +223,6 @@ static Column column_of(const ArrowArray* a, const ArrowSchema* s, int64_t paren
     return c;
   }
   c.kind = kind_of(s->format);
-  if (c.kind == Kind::Other) fail(EINFOLD_INVALID, "unsupported Arrow format '%s'", s->format);
   if (c.kind == Kind::Null) {
     c.null_count = c.length;
     return c;
@@ -459,6 +470,7 @@ OutColumn copy_column(const Column& c, const Field& f) {
     o.dictionary = std::make_shared<OutColumn>(copy_column(*c.dictionary, *f.dictionary));
     return o;
   }
+  if (c.kind == Kind::Other) decline("carrying a column of type '" + f.format + "' is left to the host plan");
   o.kind = c.kind;
   int64_t nulls = c.nulls();
   o.null_count = nulls;

@@ -13,9 +13,15 @@
 namespace ef {
 
 // A column's logical type, from its Arrow format string.
+// Dates, times, timestamps and durations are signed integers underneath (32
+// or 64 bits) but not integer types: they rank, join and group by their
+// values, and the dense and fused algorithms, which take integer keys only,
+// decline them as the reference's do. Other: a type the library can't read,
+// allowed in columns no call uses.
 enum class Kind : uint8_t {
   Int8, UInt8, Int16, UInt16, Int32, UInt32, Int64, UInt64,
-  Float16, Float32, Float64, Bool, Utf8, LargeUtf8, Binary, LargeBinary, Null, Other
+  Float16, Float32, Float64, Bool, Utf8, LargeUtf8, Binary, LargeBinary, Null, Other,
+  Date32, Date64, Time32, Time64, Timestamp, Duration
 };
 
 Kind kind_of(const char* format);
@@ -24,6 +30,7 @@ inline bool is_integer(Kind k) { return k <= Kind::UInt64; }
 inline bool is_signed(Kind k) { return k == Kind::Int8 || k == Kind::Int16 || k == Kind::Int32 || k == Kind::Int64; }
 inline bool is_float(Kind k) { return k == Kind::Float16 || k == Kind::Float32 || k == Kind::Float64; }
 inline bool is_var(Kind k) { return k == Kind::Utf8 || k == Kind::LargeUtf8 || k == Kind::Binary || k == Kind::LargeBinary; }
+inline bool is_temporal(Kind k) { return k >= Kind::Date32; }
 const char* format_of(Kind k);
 
 struct Field {

@@ -70,6 +70,12 @@ __device__ uint64_t ordered_bits(const KeyCol& c, int64_t r) {
     case Kind::Int16: return (uint64_t)(int64_t)((const int16_t*)c.data)[r] ^ (1ull << 63);
     case Kind::Int32: return (uint64_t)(int64_t)((const int32_t*)c.data)[r] ^ (1ull << 63);
     case Kind::Int64: return (uint64_t)((const int64_t*)c.data)[r] ^ (1ull << 63);
+    case Kind::Date32:
+    case Kind::Time32: return (uint64_t)(int64_t)((const int32_t*)c.data)[r] ^ (1ull << 63);
+    case Kind::Date64:
+    case Kind::Time64:
+    case Kind::Timestamp:
+    case Kind::Duration: return (uint64_t)((const int64_t*)c.data)[r] ^ (1ull << 63);
     case Kind::UInt8: return ((const uint8_t*)c.data)[r];
     case Kind::UInt16: return ((const uint16_t*)c.data)[r];
     case Kind::UInt32: return ((const uint32_t*)c.data)[r];
@@ -450,6 +456,8 @@ StagedKeySet stage_set(Context& ctx, const Relation& r, const std::vector<int>& 
   for (int c : cols) {
     if (c < 0 || c >= (int)r.fields.size()) fail(EINFOLD_INVALID, "no column %d", c);
     dictionary = dictionary || r.fields[c].dictionary;
+    if (r.fields[c].kind == Kind::Other || (r.fields[c].dictionary && r.fields[c].dictionary->kind == Kind::Other))
+      decline("keys of type '" + r.fields[c].format + "' are ranked by the host plan");
   }
   if (dictionary && r.device >= 0) decline("dictionary-encoded keys in device memory are ranked by the host plan");
   std::vector<HostBuffer> keep;
