@@ -21,6 +21,26 @@ Kind kind_of(const char* f) {
     if (f[1] == 'D' && f[2] && !f[3]) return Kind::Duration;
     return Kind::Other;
   }
+  if (f[0] == 'd' && f[1] == ':') {
+    // Decimals: d:precision,scale, or d:precision,scale,bits (128 bits when
+    // the bits are left out).
+    int commas = 0;
+    const char* bits = nullptr;
+    for (const char* p = f + 2; *p; p++)
+      if (*p == ',' && ++commas == 2) bits = p + 1;
+    if (!bits) return commas == 1 ? Kind::Decimal128 : Kind::Other;
+    if (!std::strcmp(bits, "32")) return Kind::Decimal32;
+    if (!std::strcmp(bits, "64")) return Kind::Decimal64;
+    if (!std::strcmp(bits, "128")) return Kind::Decimal128;
+    if (!std::strcmp(bits, "256")) return Kind::Decimal256;
+    return Kind::Other;
+  }
+  if (f[0] == 'w' && f[1] == ':') {
+    // Fixed-size binary of n bytes, n > 0.
+    char* end = nullptr;
+    const long n = std::strtol(f + 2, &end, 10);
+    return (end != f + 2 && !*end && n > 0 && n <= (1L << 20)) ? Kind::FixedBinary : Kind::Other;
+  }
   if (f[0] && f[1] == 0) {
     switch (f[0]) {
       case 'c': return Kind::Int8;
@@ -53,8 +73,18 @@ int width_of(Kind k) {
     case Kind::Int64: case Kind::UInt64: case Kind::Float64: return 8;
     case Kind::Date32: case Kind::Time32: return 4;
     case Kind::Date64: case Kind::Time64: case Kind::Timestamp: case Kind::Duration: return 8;
+    case Kind::Decimal32: return 4;
+    case Kind::Decimal64: return 8;
+    case Kind::Decimal128: return 16;
+    case Kind::Decimal256: return 32;
     default: return 0;
   }
+}
+
+int fixed_width(const std::string& format) {
+  const Kind k = kind_of(format.c_str());
+  if (k == Kind::FixedBinary) return (int)std::strtol(format.c_str() + 2, nullptr, 10);
+  return width_of(k);
 }
 
 const char* format_of(Kind k) {
@@ -507,7 +537,7 @@ OutColumn copy_column(const Column& c, const Field& f) {
   } else if (c.kind == Kind::Null) {
     o.null_count = c.length;
   } else {
-    int w = width_of(c.kind);
+    const int w = fixed_width(f.format);
     o.values = Buffer(HostBuffer((size_t)(c.length * w)));
     if (c.length) std::memcpy(o.values.ptr, c.values + c.offset * w, (size_t)(c.length * w));
   }
@@ -534,7 +564,7 @@ OutColumn dictionary_encode(OutColumn&& v, const Field& f) {
   const Kind ik = kind_of(f.format.c_str());
   const int64_t cap = largest_index(ik);
   const int iw = width_of(ik);
-  const int w = is_var(v.kind) || v.kind == Kind::Bool ? 0 : width_of(v.kind);
+  const int w = fixed_width(v.format);  // 0 for var-length and Bool values
   const int64_t n = v.length;
   auto valid = [&](int64_t i) { return !v.null_count || ((v.validity.as<uint8_t>()[i >> 3] >> (i & 7)) & 1); };
   // Distinct values in the order of their first rows; NULL is one of them.
@@ -683,7 +713,7 @@ Relation decode_dictionaries(const Relation& r, const std::vector<int>& cols, st
         nc.values = bits.as<uint8_t>();
         keep.push_back(std::move(bits));
       } else {
-        const int w = width_of(d.kind);
+        const int w = fixed_width(vf.format);
         HostBuffer vals((size_t)(n ? n * w : 1));
         std::memset(vals.ptr, 0, vals.bytes);
         for (int64_t i = 0; i < n; i++)

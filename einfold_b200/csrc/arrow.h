@@ -16,21 +16,30 @@ namespace ef {
 // Dates, times, timestamps and durations are signed integers underneath (32
 // or 64 bits) but not integer types: they rank, join and group by their
 // values, and the dense and fused algorithms, which take integer keys only,
-// decline them as the reference's do. Other: a type the library can't read,
-// allowed in columns no call uses.
+// decline them as the reference's do. Decimals (32, 64, 128 and 256 bits,
+// two's complement, little-endian) rank by their values within one type, and
+// fixed-size binary by its bytes; they aren't integer types either. Other: a
+// type the library can't read, allowed in columns no call uses.
 enum class Kind : uint8_t {
   Int8, UInt8, Int16, UInt16, Int32, UInt32, Int64, UInt64,
   Float16, Float32, Float64, Bool, Utf8, LargeUtf8, Binary, LargeBinary, Null, Other,
-  Date32, Date64, Time32, Time64, Timestamp, Duration
+  Date32, Date64, Time32, Time64, Timestamp, Duration,
+  Decimal32, Decimal64, Decimal128, Decimal256, FixedBinary
 };
 
 Kind kind_of(const char* format);
-int width_of(Kind k);  // bytes per value of a fixed-width kind (Bool: 0)
+int width_of(Kind k);  // bytes per value of a fixed-width kind (Bool and FixedBinary: 0)
+// Bytes per value of a fixed-width format, fixed-size binary (w:n) included;
+// 0 for Bool, var-length and unreadable formats.
+int fixed_width(const std::string& format);
 inline bool is_integer(Kind k) { return k <= Kind::UInt64; }
 inline bool is_signed(Kind k) { return k == Kind::Int8 || k == Kind::Int16 || k == Kind::Int32 || k == Kind::Int64; }
 inline bool is_float(Kind k) { return k == Kind::Float16 || k == Kind::Float32 || k == Kind::Float64; }
 inline bool is_var(Kind k) { return k == Kind::Utf8 || k == Kind::LargeUtf8 || k == Kind::Binary || k == Kind::LargeBinary; }
-inline bool is_temporal(Kind k) { return k >= Kind::Date32; }
+inline bool is_temporal(Kind k) { return k >= Kind::Date32 && k <= Kind::Duration; }
+// Keys wider than 8 bytes, encoded byte by byte: 128- and 256-bit decimals
+// and fixed-size binary.
+inline bool is_wide(Kind k) { return k == Kind::Decimal128 || k == Kind::Decimal256 || k == Kind::FixedBinary; }
 const char* format_of(Kind k);
 
 struct Field {

@@ -36,7 +36,10 @@ namespace {
 constexpr int kMaxWords = 4;  // words one ranking pass orders a key by
 
 // One key column's block of bytes in the encoded key: a byte for NULL (0) or
-// valid (1), then the value. Fixed-width values take 8 bytes. A string or
+// valid (1), then the value. Fixed-width values up to 8 bytes take 8, as
+// order-preserving 64-bit words. 128- and 256-bit decimals take their 16 or
+// 32 bytes big-endian with the sign bit flipped, fixed-size binary its bytes
+// as they are, so both order bytewise as Arrow's row format orders them. A string or
 // binary value takes `max_len` bytes, its own bytes zero-padded, then its
 // length big-endian in `len_bytes` bytes: two values that differ first at
 // byte p order by that byte, a value that is a prefix of the other with only
@@ -55,6 +58,7 @@ struct KeyCol {
   int64_t max_len;     // var-length: bytes of the value part
   int len_bytes;       // var-length: bytes of the length part
   int canon_zero;      // SignedZerosEqual on a float column
+  int wide;            // 1: a 128/256-bit decimal, 2: fixed-size binary (bytes in the block); 0 otherwise
 };
 
 // The word positions (absolute, within the key) a pass encodes, and where
@@ -71,11 +75,13 @@ __device__ uint64_t ordered_bits(const KeyCol& c, int64_t r) {
     case Kind::Int32: return (uint64_t)(int64_t)((const int32_t*)c.data)[r] ^ (1ull << 63);
     case Kind::Int64: return (uint64_t)((const int64_t*)c.data)[r] ^ (1ull << 63);
     case Kind::Date32:
-    case Kind::Time32: return (uint64_t)(int64_t)((const int32_t*)c.data)[r] ^ (1ull << 63);
+    case Kind::Time32:
+    case Kind::Decimal32: return (uint64_t)(int64_t)((const int32_t*)c.data)[r] ^ (1ull << 63);
     case Kind::Date64:
     case Kind::Time64:
     case Kind::Timestamp:
-    case Kind::Duration: return (uint64_t)((const int64_t*)c.data)[r] ^ (1ull << 63);
+    case Kind::Duration:
+    case Kind::Decimal64: return (uint64_t)((const int64_t*)c.data)[r] ^ (1ull << 63);
     case Kind::UInt8: return ((const uint8_t*)c.data)[r];
     case Kind::UInt16: return ((const uint16_t*)c.data)[r];
     case Kind::UInt32: return ((const uint32_t*)c.data)[r];
@@ -122,6 +128,18 @@ __device__ uint64_t key_word(const KeyCol* __restrict__ cols, int n_cols, int64_
         if (q == 0) byte = 1;
         else if (q <= c.max_len) byte = q - 1 < len ? c.data[o0 + q - 1] : 0;
         else byte = ((uint64_t)len >> (8 * (c.len_bytes - 1 - (q - 1 - c.max_len)))) & 0xff;
+        w |= byte << (8 * (7 - (p - b0)));
+      }
+    } else if (c.wide) {
+      // Decimals: little-endian two's complement, taken most significant
+      // byte first with the sign bit flipped; fixed-size binary as it is.
+      const uint8_t* v = c.data + r * c.width;
+      for (int64_t p = lo; p < hi; p++) {
+        const int64_t q = p - s;
+        uint64_t byte;
+        if (q == 0) byte = 1;
+        else if (c.wide == 1) byte = v[c.width - q] ^ (q == 1 ? 0x80 : 0);
+        else byte = v[q - 1];
         w |= byte << (8 * (7 - (p - b0)));
       }
     } else {
@@ -357,11 +375,14 @@ __global__ void gather_fixed(const uint8_t* __restrict__ data, const uint8_t* __
         ((uint32_t*)out)[i] = u;
         break;
       }
-      default: {
+      case 8: {
         uint64_t u = ((const uint64_t*)data)[r];
         if (canon_zero && u == 0x8000000000000000ull) u = 0;
         ((uint64_t*)out)[i] = u;
+        break;
       }
+      default:  // wide decimals and fixed-size binary
+        for (int b = 0; b < width; b++) out[i * width + b] = data[r * width + b];
     }
   }
   if (local) atomicAdd(nulls, local);
@@ -508,6 +529,8 @@ KeyLayout layout_of(Context& ctx, const std::vector<const StagedKeySet*>& sets, 
       max_len[i] = (int64_t)mx;
       while (len_bytes[i] < 8 && (mx >> (8 * len_bytes[i]))) len_bytes[i]++;
       block[i] = 1 + max_len[i] + len_bytes[i];
+    } else if (is_wide(sets[0]->kinds[i])) {
+      block[i] = 1 + sets[0]->cols[i].width;
     } else {
       block[i] = 1 + 8;
     }
@@ -529,6 +552,7 @@ KeyLayout layout_of(Context& ctx, const std::vector<const StagedKeySet*>& sets, 
       k.max_len = max_len[i];
       k.len_bytes = len_bytes[i];
       k.canon_zero = float_keys == 1 && is_float(c.kind) && !st->dictionary[i];
+      k.wide = c.kind == Kind::FixedBinary ? 2 : (is_wide(c.kind) ? 1 : 0);
     }
     DeviceBuffer<KeyCol> d(kc.size(), s);
     EF_CUDA(cudaMemcpyAsync(d.get(), kc.data(), kc.size() * sizeof(KeyCol), cudaMemcpyHostToDevice, s));
@@ -1013,7 +1037,7 @@ FoldOutput discriminate_fold(Context& ctx, const FoldD& f, const Relation& a, co
         }
         c.data = result_buffer(ctx, bytes, (size_t)total, o.result_on_device);
       } else {
-        const int width = width_of(src.kind) ? width_of(src.kind) : 1;
+        const int width = src.width ? src.width : 1;
         DeviceBuffer<uint8_t> vals((size_t)(groups ? groups * width : 1), s);
         if (groups)
           gather_fixed<<<blocks_for(groups, 256), 256, 0, s>>>(src.ptr(), src.valid.get(), width,

@@ -142,7 +142,7 @@ DeviceColumn stage_column(Context& ctx, const Relation& r, int col, bool with_va
     if (d.rows) expand_validity<<<blocks_for(d.rows, 256), 256, 0, s>>>(bits.get(), dseg.get(), (int)seg.size(), d.rows, d.data.get());
     EF_CUDA(cudaStreamSynchronize(s));
   } else if (d.kind != Kind::Null) {
-    d.width = width_of(d.kind);
+    d.width = fixed_width(r.fields[col].format);
     if (!d.width) fail(EINFOLD_INVALID, "a column of an unsupported type");
     if (r.device >= 0 && r.batches.size() == 1) {
       // One batch already in HBM: read in place.

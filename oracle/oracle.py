@@ -607,6 +607,24 @@ def _encode_column(c: pa.Array) -> List[bytes]:
     t = c.type
     valid = _valid(c)
     n = len(c)
+    if pa.types.is_temporal(t) and not pa.types.is_interval(t):
+        # Dates, times, timestamps and durations order as their integers.
+        c = c.cast(pa.int32() if t.bit_width == 32 else pa.int64())
+        t = c.type
+    if pa.types.is_decimal(t) or pa.types.is_fixed_size_binary(t):
+        # Arrow's row format: a decimal's two's complement big-endian with
+        # the sign bit flipped; fixed-size binary as its bytes.
+        w = t.byte_width
+        raw = c.buffers()[1].to_pybytes() if n else b""
+        vals = []
+        for i in range(n):
+            b = raw[(c.offset + i) * w:(c.offset + i + 1) * w]
+            if pa.types.is_decimal(t):
+                b = bytearray(b[::-1])
+                b[0] ^= 0x80
+                b = bytes(b)
+            vals.append(b)
+        return [(b"\x01" + vals[i]) if valid[i] else b"\x00" for i in range(n)]
     if pa.types.is_integer(t):
         v = c.fill_null(0).to_numpy(zero_copy_only=False)
         if pa.types.is_signed_integer(t):

@@ -104,6 +104,21 @@ def test_keys_with_long_shared_prefixes_sort_as_their_bytes():
     assert np.array_equal(r.rank, np.argsort(np.argsort(strings, kind="stable"), kind="stable").astype(np.uint32))
 
 
+@pytest.mark.parametrize("bits", [32, 64, 128, 256])
+def test_decimal_keys_sort_as_their_values(bits):
+    # Arrow's row format for decimals: big-endian, sign bit flipped.
+    t = {32: pa.decimal32(9, 2), 64: pa.decimal64(18, 0), 128: pa.decimal128(38, 4), 256: pa.decimal256(76, 1)}[bits]
+    top = 10 ** t.precision - 1
+    vals = [0, -1, 1, top, -top, 255, -256, 256, 1 << 20, -(1 << 20), top // 3, -top // 7, None, 5, 0]
+    data = b"".join((0 if v is None else v).to_bytes(t.byte_width, "little", signed=True) for v in vals)
+    valid = pa.array([v is not None for v in vals]).buffers()[1]
+    col = pa.Array.from_buffers(t, len(vals), [valid, pa.py_buffer(data)], null_count=1)
+    r = oracle.ranks_of_bytes(oracle._encode_column(col))
+    distinct = [None] + sorted({v for v in vals if v is not None})
+    assert [vals[f] for f in r.first] == distinct
+    assert [distinct[k] for k in r.rank] == vals
+
+
 def test_dense_product_within_the_rounding_bound_and_repeatable():
     rng = oracle.Rng.seeded(11, 0)
     ni, nj, nk = 24, 300, 17
