@@ -293,8 +293,9 @@ __global__ void __launch_bounds__(kThreads) byte_histograms(const uint64_t* __re
 // memory by bulk copies (one a key word and one for the row numbers, whole
 // 16-byte multiples; a ragged tail of the last tile is read directly), so
 // that a block's loads take no load slots of its warps; its keys and row
-// numbers then stay in registers (item i of a lane is key warp·32·ITEMS +
-// 32i + lane of the tile). As soon as they arrive, the tile's count of each
+// numbers stay there, and each lane keeps only its items' digits and places
+// in registers (item i of a lane is key warp·32·ITEMS + 32i + lane of the
+// tile), so that three blocks fit an SM. As soon as they arrive, the tile's count of each
 // digit (shared-memory atomics) is published, so that later tiles'
 // look-backs can pass this one while it ranks. Each warp then ranks its
 // items among equal digits in order: eight ballots over a digit's bits (and
@@ -307,8 +308,8 @@ __global__ void __launch_bounds__(kThreads) byte_histograms(const uint64_t* __re
 // first place in the tile, and the look-back each digit's keys in earlier
 // tiles, reading four earlier tiles' words at a time. The keys are
 // reordered by digit through the first key word's stage, a word at a time
-// and then the row numbers, and written out as runs of consecutive
-// destinations. Key words (ldi) and row numbers start 16-byte aligned.
+// (read from the stage into registers first) and then the row numbers, and
+// written out as runs of consecutive destinations. Key words (ldi) and row numbers start 16-byte aligned.
 template <int W, int ITEMS, int MIN_BLOCKS>
 __global__ void __launch_bounds__(kThreads, MIN_BLOCKS) onesweep_pass(const uint64_t* __restrict__ kin,
                                                              const uint32_t* __restrict__ vin,
@@ -364,21 +365,14 @@ __global__ void __launch_bounds__(kThreads, MIN_BLOCKS) onesweep_pass(const uint
     ptx::mbar_wait(&bar, 0);
   }
 
-  uint64_t key[ITEMS][W];
-  uint32_t val[ITEMS];
+  // Keys and row numbers stay in the stage until the reorder reads them.
   uint32_t dp[ITEMS];  // digit (bits 16..24; 256: no key) and place among the warp's equal digits (bits 0..15)
 #pragma unroll
   for (int i = 0; i < ITEMS; i++) {
     const int off = warp * 32 * ITEMS + i * 32 + lane;
     uint32_t d = 256;
     if (off < count) {
-#pragma unroll
-      for (int w = 0; w < W; w++) key[i][w] = off < kb ? kstage[w * TILE + off] : kin[(int64_t)w * ldi + base + off];
-      val[i] = vin ? (off < vb ? vstage[off] : vin[base + off]) : (uint32_t)(base + off);
-      uint64_t wd = key[i][0];
-#pragma unroll
-      for (int w = 1; w < W; w++)
-        if (word == w) wd = key[i][w];
+      const uint64_t wd = off < kb ? kstage[word * TILE + off] : kin[(int64_t)word * ldi + base + off];
       d = (uint32_t)((wd >> shift) & 255);
     }
     dp[i] = d << 16;
@@ -480,14 +474,28 @@ __global__ void __launch_bounds__(kThreads, MIN_BLOCKS) onesweep_pass(const uint
   }
 #pragma unroll
   for (int w = 0; w <= W; w++) {
-    // Word w of the keys (w < W), then the rows, through the one buffer.
+    // Word w of the keys (w < W), then the rows, through the one buffer
+    // (word 0's stage: its keys are read before any is overwritten).
+    if (w < W) {
+      uint64_t kw[ITEMS];
 #pragma unroll
-    for (int i = 0; i < ITEMS; i++)
-      if ((dp[i] >> 16) < 256) {
-        const uint32_t pos = dp[i] & 0xffffu;
-        if (w < W) xbuf[pos] = key[i][w];
-        else ((uint32_t*)xbuf)[pos] = val[i];
+      for (int i = 0; i < ITEMS; i++) {
+        const int off = warp * 32 * ITEMS + i * 32 + lane;
+        if ((dp[i] >> 16) < 256) kw[i] = off < kb ? kstage[w * TILE + off] : kin[(int64_t)w * ldi + base + off];
       }
+      if (w == 0) __syncthreads();
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++)
+        if ((dp[i] >> 16) < 256) xbuf[dp[i] & 0xffffu] = kw[i];
+    } else {
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++)
+        if ((dp[i] >> 16) < 256) {
+          const int off = warp * 32 * ITEMS + i * 32 + lane;
+          ((uint32_t*)xbuf)[dp[i] & 0xffffu] =
+              vin ? (off < vb ? vstage[off] : vin[base + off]) : (uint32_t)(base + off);
+        }
+    }
     __syncthreads();
     for (int j = tid; j < count; j += kThreads) {
       const long long dst = dbase[sdig[j]] + j;
@@ -606,10 +614,12 @@ __global__ void __launch_bounds__(kThreads) rank_runs(const uint64_t* __restrict
 // a bucket is of no consequence: scatter_ranks then writes rank[row] for each
 // pair, and the pairs of one bucket, read in order, fall in one rank range of
 // 2^bshift rows that stays in L2 while it is written. Item i of a lane is
-// position warp·32·ITEMS + 32i + lane of the tile.
+// position warp·32·ITEMS + 32i + lane of the tile; the rows stay in shared
+// memory and a lane keeps only its items' ranks and bucket slots, so that
+// three blocks fit an SM.
 constexpr int kBuckets = 256;
 template <int W>
-constexpr int part_items() { return W == 1 ? 16 : (W == 2 ? 8 : (W == 3 ? 6 : 4)); }
+constexpr int part_items() { return W == 1 ? 20 : (W == 2 ? 8 : (W == 3 ? 6 : 4)); }
 
 // Sums a value over a warp.
 __device__ __forceinline__ unsigned int warp_sum(unsigned int v) {
@@ -619,7 +629,7 @@ __device__ __forceinline__ unsigned int warp_sum(unsigned int v) {
 }
 
 template <int W, int ITEMS>
-__global__ void __launch_bounds__(kThreads, 2) rank_partition(const uint64_t* __restrict__ keys, int64_t ld,
+__global__ void __launch_bounds__(kThreads, 3) rank_partition(const uint64_t* __restrict__ keys, int64_t ld,
                                                               const uint32_t* __restrict__ rows, int64_t n, int bshift,
                                                               uint32_t* __restrict__ head_status,
                                                               uint32_t* __restrict__ bucket_status,
@@ -669,8 +679,9 @@ __global__ void __launch_bounds__(kThreads, 2) rank_partition(const uint64_t* __
   auto key_at = [&](int j, int w) -> uint64_t {
     return j < kb ? kstage[w * TILE + j] : keys[(int64_t)w * ld + base + j];
   };
-  // Heads, rows, and the heads at or before each item within the warp.
-  uint32_t r[ITEMS];
+  auto row_at = [&](int j) -> uint32_t { return j < rb ? rstage[j] : rows[base + j]; };
+  // Heads, and the heads at or before each item within the warp (the rows
+  // stay in the stage).
   uint32_t hrank[ITEMS];  // that count (bit 31: the item is a head); then the item's rank
   unsigned int wcount = 0;
 #pragma unroll
@@ -684,7 +695,6 @@ __global__ void __launch_bounds__(kThreads, 2) rank_partition(const uint64_t* __
         const uint64_t prev = j > 0 ? key_at(j - 1, w) : (base > 0 ? keys[(int64_t)w * ld + base - 1] : 0);
         h |= key_at(j, w) != prev;
       }
-      r[i] = j < rb ? rstage[j] : rows[base + j];
     }
     const unsigned heads = __ballot_sync(0xffffffffu, h);
     hrank[i] = (wcount + __popc(heads & lt_mask) + (h ? 1u : 0u)) | (h ? 0x80000000u : 0u);
@@ -745,10 +755,11 @@ __global__ void __launch_bounds__(kThreads, 2) rank_partition(const uint64_t* __
   for (int i = 0; i < ITEMS; i++) {
     const int j = warp * 32 * ITEMS + i * 32 + lane;
     if (j < count) {
+      const uint32_t ri = row_at(j);
       const unsigned int rk = first_rank + (hrank[i] & 0x7fffffffu) - 1u;
-      if (hrank[i] >> 31) first[rk] = r[i];
+      if (hrank[i] >> 31) first[rk] = ri;
       hrank[i] = rk;
-      slot[i] = atomicAdd(&cnt[r[i] >> bshift], 1u);
+      slot[i] = atomicAdd(&cnt[ri >> bshift], 1u);
     }
   }
   __syncthreads();
@@ -798,7 +809,10 @@ __global__ void __launch_bounds__(kThreads, 2) rank_partition(const uint64_t* __
 #pragma unroll
   for (int i = 0; i < ITEMS; i++) {
     const int j = warp * 32 * ITEMS + i * 32 + lane;
-    if (j < count) spairs[at[r[i] >> bshift] + slot[i]] = ((uint64_t)r[i] << 32) | hrank[i];
+    if (j < count) {
+      const uint32_t ri = row_at(j);
+      spairs[at[ri >> bshift] + slot[i]] = ((uint64_t)ri << 32) | hrank[i];
+    }
   }
   __syncthreads();
   for (int j = tid; j < count; j += kThreads) {
@@ -873,8 +887,8 @@ void radix_pass(Context& ctx, const uint64_t* kin, int64_t ldi, const uint32_t* 
 template <int W>
 int64_t rank_keys_onesweep(Context& ctx, const uint64_t* keys, int64_t n, int64_t ld, uint32_t* rank,
                            uint32_t* first, cudaStream_t s, uint32_t* sorted_rows) {
-  constexpr int ITEMS = W == 1 ? 16 : (W == 2 ? 8 : (W == 3 ? 6 : 4));
-  constexpr int MIN_BLOCKS = W == 1 ? 2 : 3;
+  constexpr int ITEMS = W == 1 ? 20 : (W == 2 ? 8 : (W == 3 ? 6 : 4));
+  constexpr int MIN_BLOCKS = 3;
   constexpr int TILE = kThreads * ITEMS;
   constexpr int RITEMS = 8;
   constexpr int RTILE = kThreads * RITEMS;
