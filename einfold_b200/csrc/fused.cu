@@ -163,6 +163,51 @@ struct RowState {
 
 constexpr int kStage = 32 * 65;  // doubles in one staged operand chunk (e rows of 64 + 1)
 constexpr size_t kTileSmem = sizeof(double) * (XT * (JT + 1) + 2 * kStage) + sizeof(RowState);
+constexpr size_t kUnshiftedSmem = sizeof(double) * 2 * kStage + sizeof(RowState);
+
+// The guards of row r after its last tile (fused.rs:941-1013): whether the
+// call overflowed, and the row's check of each output against the terms
+// lost below the smallest normal (S.check, S.lost).
+__device__ bool row_guards(RowState& S, int r, bool map, bool shifted, bool unnormalized) {
+  const double NEG_INF = -INFINITY, POS_INF = INFINITY;
+  const double normal = 2.0 * 2.2250738585072014e-308;
+  bool over = false;
+  const bool zp = !unnormalized;
+  const double z = S.z[r], m = S.m[r];
+  if (zp && !S.sw[r] && !isfinite(z)) over = true;
+  S.check[r] = 0;
+  auto weight = [&](double bound) { return map ? bound : shifted ? exp(bound - m) : exp(bound); };
+  const double heaviest = weight(S.high[r]);
+  if (!(S.sw[r] || S.high[r] == NEG_INF || heaviest == 0.0)) {
+    const double lightest = weight(S.light[r]);
+    const double largest = S.rl[r], smallest = S.rs[r];
+    const double terms = 2.0 * (double)S.terms[r];
+    bool finite = isfinite(__dmul_rn(__dmul_rn(heaviest, largest), terms));
+    if (finite && zp) {
+      const double quotient = __ddiv_rn(heaviest, fabs(z));
+      finite = isfinite(quotient) && isfinite(__dmul_rn(__dmul_rn(quotient, largest), terms));
+    }
+    const double inverse = zp ? __ddiv_rn(1.0, fabs(z)) : 1.0;
+    const double tiniest = 4.9406564584124654e-324;
+    S.lost[r] = __dmul_rn(__dmul_rn(terms, tiniest), __dadd_rn(__dadd_rn(inverse, largest), 1.0));
+    bool no_underflow = smallest == POS_INF;
+    if (!no_underflow) {
+      no_underflow = __dmul_rn(lightest, smallest) >= normal;
+      if (no_underflow && zp) {
+        const double quotient = __ddiv_rn(lightest, fabs(z));
+        no_underflow = quotient >= normal && __dmul_rn(quotient, smallest) >= normal;
+      }
+    }
+    if (!finite) over = true;
+    else if (!no_underflow) S.check[r] = 1;
+    if (S.low[r] != POS_INF) {
+      const double lw = shifted ? exp(S.low[r] - m) : exp(S.low[r]);
+      const bool ok = lw >= normal && (!zp || __ddiv_rn(lw, fabs(z)) >= normal);
+      if (!ok) over = true;
+    }
+  }
+  return over;
+}
 
 template <int DEPTH>
 __global__ void __launch_bounds__(kThreads) fused_tiles(const TileArgs p) {
@@ -535,44 +580,7 @@ __global__ void __launch_bounds__(kThreads) fused_tiles(const TileArgs p) {
   }
 
   // Normalisation and the row guards (fused.rs:941-1013).
-  const double normal = 2.0 * 2.2250738585072014e-308;
-  if (t < rows) {
-    const int r = t;
-    const bool zp = !unnormalized;
-    const double z = S.z[r], m = S.m[r];
-    if (zp && !S.sw[r] && !isfinite(z)) over = true;
-    S.check[r] = 0;
-    auto weight = [&](double bound) { return map ? bound : shifted ? exp(bound - m) : exp(bound); };
-    const double heaviest = weight(S.high[r]);
-    if (!(S.sw[r] || S.high[r] == NEG_INF || heaviest == 0.0)) {
-      const double lightest = weight(S.light[r]);
-      const double largest = S.rl[r], smallest = S.rs[r];
-      const double terms = 2.0 * (double)S.terms[r];
-      bool finite = isfinite(__dmul_rn(__dmul_rn(heaviest, largest), terms));
-      if (finite && zp) {
-        const double quotient = __ddiv_rn(heaviest, fabs(z));
-        finite = isfinite(quotient) && isfinite(__dmul_rn(__dmul_rn(quotient, largest), terms));
-      }
-      const double inverse = zp ? __ddiv_rn(1.0, fabs(z)) : 1.0;
-      const double tiniest = 4.9406564584124654e-324;
-      S.lost[r] = __dmul_rn(__dmul_rn(terms, tiniest), __dadd_rn(__dadd_rn(inverse, largest), 1.0));
-      bool no_underflow = smallest == POS_INF;
-      if (!no_underflow) {
-        no_underflow = __dmul_rn(lightest, smallest) >= normal;
-        if (no_underflow && zp) {
-          const double quotient = __ddiv_rn(lightest, fabs(z));
-          no_underflow = quotient >= normal && __dmul_rn(quotient, smallest) >= normal;
-        }
-      }
-      if (!finite) over = true;
-      else if (!no_underflow) S.check[r] = 1;
-      if (S.low[r] != POS_INF) {
-        const double lw = shifted ? exp(S.low[r] - m) : exp(S.low[r]);
-        const bool ok = lw >= normal && (!zp || __ddiv_rn(lw, fabs(z)) >= normal);
-        if (!ok) over = true;
-      }
-    }
-  }
+  if (t < rows && row_guards(S, t, map, shifted, unnormalized)) over = true;
   __syncthreads();
   const double rounding = 2.220446049250313e-16 / 4.0;
   for (int i = 0; i < 4; i++) {
@@ -601,6 +609,251 @@ __global__ void __launch_bounds__(kThreads) fused_tiles(const TileArgs p) {
   if (t == 0 && blockIdx.y == 0 && visited) atomicAdd(p.visited, visited);
 }
 
+// fused_tiles for exp weights without a shift (a smoother's exp(s / h))
+// and at most kNarrow value columns. No weight then depends on another
+// tile's scores, so no row needs its statistics before its last tile: a
+// thread keeps its row's running statistics, weight sum, weighted sums and
+// flags over all its tiles, and the four threads of a row combine them once
+// at the end, where fused_tiles reduces over a half-warp at every tile. A
+// thread owns row t % 64 and columns 16·(t / 64) .. + 15 of each 64 x 64
+// tile of pairs. Scores are computed as fused_tiles computes them (the same
+// operations in the same order, so the same bits); the sums add the same
+// terms in another order (a thread's columns in order over the tiles, then
+// the row's four threads in order). The row guards and outputs follow
+// fused.rs:941-1013 as in fused_tiles.
+// SHAPE: 0 product scores, 1 -power(a - b, 2) (SCORE_NEG_SQUARED_DIFF), 2 the
+// interpreter.
+// NY: the value columns the kernel sums at most (1 or kNarrow).
+template <int DEPTH, int SHAPE, int NY>
+__global__ void __launch_bounds__(kThreads, 2) fused_unshifted(const TileArgs p) {
+  constexpr int CPT = JT / 4;          // columns a thread
+  constexpr int RS = 6 + kNarrow;      // a thread's partials: z, high, light, low, largest, smallest, sums
+  extern __shared__ __align__(16) unsigned char smem[];
+  double* stg = reinterpret_cast<double*>(smem);  // staged q and k; after the last tile the partials
+  RowState& S = *reinterpret_cast<RowState*>(smem + sizeof(double) * 2 * kStage);
+  __shared__ long long s_first, s_last;
+  __shared__ int s_lo[XT], s_hi[XT];
+  __shared__ uint8_t s_fc[JT];
+  __shared__ double s_lg[JT], s_sm[JT];
+  __shared__ double vsm[JT * kNarrow];
+  __shared__ long long s_terms[4][XT];
+  __shared__ unsigned s_flags[4][XT];  // bit 0: a weight not finite; 1: a value not finite; 8 + y: column y's
+
+  const int t = threadIdx.x, row = t % XT, cg = t / XT;
+  const int64_t x0 = (int64_t)blockIdx.x * XT;
+  const int rows = (int)std::min<int64_t>(XT, p.nx - x0);
+  const int ycount = (int)std::min<int64_t>(NY, p.ny);
+  const bool unnormalized = p.normalizer == 2;
+  const double NEG_INF = -INFINITY, POS_INF = INFINITY;
+
+  if (t == 0) { s_first = p.nj; s_last = 0; }
+  __syncthreads();
+  if (t < rows) {
+    int64_t lo, hi;
+    allowed(p.mask, x0 + t, lo, hi);
+    if (lo < hi) {
+      atomicMin(&s_first, (long long)lo);
+      atomicMax(&s_last, (long long)hi);
+    }
+  }
+  __syncthreads();
+  const int64_t first = s_first, last = s_last;
+
+  double z = 0.0, high = NEG_INF, light = POS_INF, low = POS_INF, rl = 0.0, rs = POS_INF;
+  double acc[NY];
+#pragma unroll
+  for (int y = 0; y < NY; y++) acc[y] = 0.0;
+  long long terms = 0;
+  unsigned flags = 0;
+  unsigned long long visited = 0;
+
+  for (int64_t j0 = first - first % JT; j0 < last; j0 += JT) {
+    const int width = (int)std::min<int64_t>(JT, p.nj - j0);
+    bool has = false;
+    if (t < XT) {
+      int lo = 0, hi = 0;
+      if (t < rows) {
+        int64_t l, h;
+        allowed(p.mask, x0 + t, l, h);
+        l = l < j0 ? j0 : (l > j0 + width ? j0 + width : l);
+        h = h < j0 ? j0 : (h > j0 + width ? j0 + width : h);
+        lo = (int)(l - j0);
+        hi = (int)(h - j0);
+      }
+      s_lo[t] = lo;
+      s_hi[t] = hi;
+      has = lo < hi;
+      const bool live = t < width;
+      s_fc[t] = live ? p.jflag[j0 + t] : J_FINITE;
+      s_lg[t] = live ? p.largest[j0 + t] : 0.0;
+      s_sm[t] = live ? p.smallest[j0 + t] : POS_INF;
+    }
+    for (int idx = t; idx < JT * ycount; idx += kThreads) {
+      const int j = idx / ycount, y = idx % ycount;
+      vsm[j * kNarrow + y] = j < width ? p.v[(j0 + j) * p.ny + y] : 0.0;
+    }
+    if (!__syncthreads_or(has)) continue;
+    visited++;
+
+    // Product and -power(a - b, 2) scores for the thread's 16 columns at
+    // once; interpreted scores pair by pair in the weights' loop.
+    double s[SHAPE == 2 ? 1 : CPT];
+    if constexpr (SHAPE == 0) {
+#pragma unroll
+      for (int c = 0; c < CPT; c++) s[c] = 0.0;
+      double* qs = stg;           // [e][r], rows of 65
+      double* ks = stg + kStage;  // [e][j]
+      for (int64_t e0 = 0; e0 < p.ne; e0 += 32) {
+        const int ec = (int)std::min<int64_t>(32, p.ne - e0);
+        for (int idx = t; idx < XT * 32; idx += kThreads) {
+          const int r = idx >> 5, e = idx & 31;
+          qs[e * 65 + r] = (r < rows && e < ec) ? p.q[(x0 + r) * p.ne + e0 + e] : 0.0;
+          ks[e * 65 + r] = (r < width && e < ec) ? p.k[(j0 + r) * p.ne + e0 + e] : 0.0;
+        }
+        __syncthreads();
+        for (int e = 0; e < ec; e++) {
+          const double qv = qs[e * 65 + row];
+#pragma unroll
+          for (int c = 0; c < CPT; c++) s[c] = fma(qv, ks[e * 65 + cg * CPT + c], s[c]);
+        }
+        __syncthreads();
+      }
+    } else if constexpr (SHAPE == 1) {
+      // -power(a - b, 2) summed over E.
+      const double* ma = p.mats[p.shape_a];
+      const double* mb = p.mats[p.shape_b];
+      const bool a_row = p.side[p.shape_a] == 0, b_row = p.side[p.shape_b] == 0;
+      const int64_t xr0 = (x0 + (row < rows ? row : 0)) * p.ne;
+      for (int64_t e = 0; e < p.ne; e++) {
+        const double ar = a_row ? ma[xr0 + e] : 0.0, br = b_row ? mb[xr0 + e] : 0.0;
+#pragma unroll
+        for (int c = 0; c < CPT; c++) {
+          const int j = cg * CPT + c;
+          const int64_t jc = (j0 + (j < width ? j : 0)) * p.ne + e;
+          const double d = __dsub_rn(a_row ? ar : ma[jc], b_row ? br : mb[jc]);
+          const double val = -__dmul_rn(d, d);
+          s[c] = e == 0 ? val : __dadd_rn(s[c], val);
+        }
+      }
+    }
+    auto score = [&](int c) -> double {
+      if constexpr (SHAPE != 2) {
+        return s[c];
+      } else {
+        double slots[kMaxSlots];
+        const int j = cg * CPT + c;
+        double acc_s = 0.0;
+        if (row < rows && j < width) {
+          for (int64_t e = 0; e < p.ne; e++) {
+            for (int sl = 0; sl < p.n_slots; sl++)
+              slots[sl] = p.side[sl] == 0 ? p.mats[sl][(x0 + row) * p.ne + e] : p.mats[sl][(j0 + j) * p.ne + e];
+            const double val = eval_slots<DEPTH>(p.snodes, p.sn, slots);
+            acc_s = e == 0 ? val : __dadd_rn(acc_s, val);
+          }
+        }
+        return acc_s;
+      }
+    };
+
+    // Weights exp(scale(s)) on the row's allowed columns, and the row's
+    // running state (fused.rs:811-909 with no shift).
+    const int lo = s_lo[row], hi = s_hi[row];
+#pragma unroll
+    for (int c = 0; c < CPT; c++) {
+      const int j = cg * CPT + c;
+      const bool in = j >= lo && j < hi;
+      double x = score(c);
+      if (in) {
+        if (p.scale_kind == 1) x = x * p.scale_c;
+        else if (p.scale_kind == 2) x = __ddiv_rn(x, p.scale_c);
+      }
+      const uint8_t fc = s_fc[j];
+      const bool fin = in && isfinite(x);
+      high = fmax(high, fin ? x : NEG_INF);
+      light = fmin(light, fin ? x : POS_INF);
+      low = fmin(low, fin && (fc & J_INFINITE) ? x : POS_INF);
+      rl = fmax(rl, in ? s_lg[j] : 0.0);
+      rs = fmin(rs, in ? s_sm[j] : POS_INF);
+      const double w = in ? exp(x) : 0.0;
+      z += w;
+      terms += in;
+      flags |= (in && !isfinite(w) ? 1u : 0u) | (in && !(fc & J_FINITE) ? 2u : 0u);
+#pragma unroll
+      for (int y = 0; y < NY; y++)
+        if (y < ycount) {
+          const double vj = vsm[j * kNarrow + y];
+          acc[y] += in ? w * vj : 0.0;
+          flags |= in && !isfinite(vj) ? 1u << (8 + y) : 0u;
+        }
+    }
+    __syncthreads();
+  }
+
+  // The row's four threads' partials, combined in order.
+  double* mine = stg + (cg * XT + row) * RS;
+  mine[0] = z;
+  mine[1] = high;
+  mine[2] = light;
+  mine[3] = low;
+  mine[4] = rl;
+  mine[5] = rs;
+#pragma unroll
+  for (int y = 0; y < NY; y++) mine[6 + y] = acc[y];
+  s_terms[cg][row] = terms;
+  s_flags[cg][row] = flags;
+  __syncthreads();
+  bool over = false;
+  if (t < XT) {
+    const int r = t;
+    double* p0 = stg + r * RS;
+    unsigned f = s_flags[0][r];
+    long long n = s_terms[0][r];
+    for (int g = 1; g < 4; g++) {
+      const double* pg = stg + (g * XT + r) * RS;
+      p0[0] += pg[0];
+      p0[1] = fmax(p0[1], pg[1]);
+      p0[2] = fmin(p0[2], pg[2]);
+      p0[3] = fmin(p0[3], pg[3]);
+      p0[4] = fmax(p0[4], pg[4]);
+      p0[5] = fmin(p0[5], pg[5]);
+      for (int y = 0; y < ycount; y++) p0[6 + y] += pg[6 + y];
+      f |= s_flags[g][r];
+      n += s_terms[g][r];
+    }
+    s_flags[0][r] = f;
+    S.m[r] = 0.0;
+    S.z[r] = p0[0];
+    S.high[r] = p0[1];
+    S.light[r] = p0[2];
+    S.low[r] = p0[3];
+    S.rl[r] = p0[4];
+    S.rs[r] = p0[5];
+    S.terms[r] = n;
+    S.sw[r] = f & 1u;
+    if (unnormalized && (f & 3u)) over = true;
+    if (r < rows && row_guards(S, r, false, false, unnormalized)) over = true;
+  }
+  __syncthreads();
+  const double rounding = 2.220446049250313e-16 / 4.0;
+  for (int idx = t; idx < rows * ycount; idx += kThreads) {
+    const int r = idx / ycount, y = idx % ycount;
+    const double z_r = S.z[r];
+    const bool swr = S.sw[r] != 0;
+    const bool spec = (s_flags[0][r] >> (8 + y)) & 1u;
+    double a = stg[r * RS + 6 + y];
+    if (!unnormalized) {
+      if (!swr && !spec && !isfinite(a)) over = true;
+      a = __ddiv_rn(a, z_r);
+      if (z_r != 0.0 && !swr && !spec && !isfinite(a)) over = true;
+    }
+    if (S.check[r] && !spec && !(S.lost[r] <= rounding * fabs(a))) over = true;
+    p.out[(x0 + r) * p.ny + y] = a;
+  }
+  if (p.lse && !unnormalized && t < rows) p.lse[x0 + t] = S.m[t] + log(S.z[t]);
+  if (__syncthreads_or(over) && t == 0) atomicOr(p.overflowed, 1u);
+  if (t == 0 && visited) atomicAdd(p.visited, visited);
+}
+
 // The deepest stack a postfix expression reaches.
 int stack_depth(const std::vector<ExprNode>& nodes) {
   int depth = 0, deepest = 0;
@@ -616,6 +869,20 @@ int stack_depth(const std::vector<ExprNode>& nodes) {
 // are at most 60).
 void launch_tiles(const TileArgs& a, int depth, dim3 grid, cudaStream_t s) {
   if (depth > 64) fail(EINFOLD_INVALID, "an expression deeper than 64");
+  const char* general = std::getenv("EINFOLD_TILES_GENERAL");
+  if (!a.weight_expr && !a.shifted && a.ny <= kNarrow && !(general && std::atoi(general) != 0)) {
+    // Unshifted exp weights and few value columns: no per-tile reductions.
+    // The interpreter's stack depth matters to its kernels only.
+    const int shape = !a.score_expr ? 0 : (a.score_shape == SCORE_NEG_SQUARED_DIFF ? 1 : 2);
+    const bool one = a.ny <= 1;
+    auto kernel = shape == 0 ? (one ? fused_unshifted<8, 0, 1> : fused_unshifted<8, 0, kNarrow>)
+                  : shape == 1 ? (one ? fused_unshifted<8, 1, 1> : fused_unshifted<8, 1, kNarrow>)
+                               : (depth <= 8 ? fused_unshifted<8, 2, kNarrow> : fused_unshifted<64, 2, kNarrow>);
+    EF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUnshiftedSmem));
+    kernel<<<dim3(grid.x, 1), kThreads, kUnshiftedSmem, s>>>(a);
+    EF_LAUNCH_CHECK();
+    return;
+  }
   auto kernel = depth <= 8 ? fused_tiles<8> : fused_tiles<64>;
   EF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
   kernel<<<grid, kThreads, kTileSmem, s>>>(a);
