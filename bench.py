@@ -513,6 +513,8 @@ def run_ours(args):
         o_host = np.asarray(piped.batches[0].column(4).to_numpy(zero_copy_only=False))
         o_dev = A.attention_forward(q, k, v, causal, 1.0, split)[0].reshape(-1).cpu().numpy()
         same_as_kernel_leg = bool(np.array_equal(o_host.view(np.uint64), o_dev.view(np.uint64)))
+        # (no view of a result may outlive this: it would keep the result's
+        # pinned buffers from the library's pool while the timed steps run)
         del res, piped, grads, outs, o_host, o_dev
         e2e_steps = max(1, min(args.steps, 3))
         barrier()

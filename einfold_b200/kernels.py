@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import ctypes
 import enum
+import threading
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence
 
@@ -85,6 +86,42 @@ class Options:
     # Leave the result's buffers in HBM: the functions then return DeviceBatch
     # objects instead of pyarrow record batches.
     result_on_device: bool = False
+    # The context the call runs on (None: the device's shared one). Calls on
+    # one context are serialized; calls on different contexts of a device
+    # may run at the same time from different threads.
+    context: Optional["Context"] = None
+
+
+class Context:
+    """A context of its own on ``device`` (``einfold_context_create``): its
+    own stream and scratch; calls on it are serialized, while calls on other
+    contexts run beside them from other threads."""
+
+    def __init__(self, device: int = 0):
+        lib = _lib.load()
+        self.device = device
+        self.handle = lib.einfold_context_create(device)
+        if not self.handle:
+            raise RuntimeError("einfold_context_create failed: " + lib.einfold_last_error().decode())
+
+    def close(self) -> None:
+        if self.handle:
+            _lib.load().einfold_context_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self) -> "Context":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
+
+
+def _ctx(options: "Options"):
+    if options.context is not None:
+        if not options.context.handle:
+            raise ValueError("a closed context")
+        return options.context.handle
+    return _lib.context(options.device)
 
 
 class Algorithm(enum.Enum):
@@ -394,7 +431,24 @@ class CallInfo:
     message: str = ""
 
 
-last_call = CallInfo()
+class _ThreadCalls(threading.local):
+    def __init__(self):
+        self.info = CallInfo()
+
+
+class _LastCall:
+    """``CallInfo`` of the last call on the calling thread."""
+
+    _calls = _ThreadCalls()
+
+    def __getattr__(self, name):
+        return getattr(self._calls.info, name)
+
+    def __setattr__(self, name, value):
+        setattr(self._calls.info, name, value)
+
+
+last_call = _LastCall()
 
 
 def _collect(res: _lib.Result) -> List[pa.RecordBatch]:
@@ -420,7 +474,7 @@ def _after_torch(*relations) -> None:
 
 def _call(fn, *args) -> Optional[_lib.Result]:
     res = _lib.Result()
-    status = fn(_lib.context(args[-1]), *args[:-1], ctypes.byref(res))
+    status = fn(args[-1], *args[:-1], ctypes.byref(res))
     msg = res.message.decode(errors="replace")
     last_call.kernels_launched = res.kernels_launched
     last_call.device_ms = res.device_ms
@@ -452,7 +506,7 @@ def fold(f: ir.Fold, a, b, domain=None, schema: Optional[pa.Schema] = None,
         res = _call(_lib.load().einfold_fold, ctypes.byref(_fold_desc(f, keep)), ctypes.byref(_relation(a, keep)),
                     ctypes.byref(_relation(b, keep)),
                     ctypes.byref(_relation(domain, keep)) if domain is not None else None,
-                    ctypes.byref(_options(options, keep)), options.device)
+                    ctypes.byref(_options(options, keep)), _ctx(options))
         if res is None:
             raise ArrowComputeError("the fold declined")
         alg = Algorithm(_lib.ALGORITHMS[res.algorithm])
@@ -473,7 +527,7 @@ def fold_dense(f: ir.Fold, a, b, domain=None, schema: Optional[pa.Schema] = None
         res = _call(_lib.load().einfold_fold_dense, ctypes.byref(_fold_desc(f, keep)),
                     ctypes.byref(_relation(a, keep)), ctypes.byref(_relation(b, keep)),
                     ctypes.byref(_relation(domain, keep)) if domain is not None else None,
-                    ctypes.byref(_options(options, keep)), options.device)
+                    ctypes.byref(_options(options, keep)), _ctx(options))
         if res is None:
             return None
         return _device_batches(res) if options.result_on_device else _collect(res)
@@ -490,7 +544,7 @@ def fold_chain(f: ir.Fold, operands: Sequence, schema: Optional[pa.Schema] = Non
     try:
         rels = keep.add(_array(_lib.Relation, [_relation(r, keep) for r in operands]))
         res = _call(_lib.load().einfold_fold_chain, ctypes.byref(_fold_desc(f, keep)), rels,
-                    ctypes.byref(_options(options, keep)), options.device)
+                    ctypes.byref(_options(options, keep)), _ctx(options))
         if res is None:
             return None
         return _device_batches(res) if options.result_on_device else _collect(res)
@@ -507,7 +561,7 @@ def pipeline(p: ir.Pipeline, operands: Sequence, schema: Optional[pa.Schema] = N
     try:
         rels = keep.add(_array(_lib.Relation, [_relation(r, keep) for r in operands]))
         res = _call(_lib.load().einfold_pipeline, ctypes.byref(_pipeline_desc(p, keep)), rels,
-                    ctypes.byref(_options(options, keep)), options.device)
+                    ctypes.byref(_options(options, keep)), _ctx(options))
         if res is None:
             return None
         visited, tiles = int(res.tiles_visited), int(res.tiles)
@@ -530,7 +584,7 @@ def pipeline_backward(p: ir.Pipeline, operands: Sequence, d_out: Relation,
     try:
         rels = keep.add(_array(_lib.Relation, [_relation(r, keep) for r in operands]))
         results = (_lib.Result * 3)()
-        status = lib.einfold_pipeline_backward(_lib.context(options.device), ctypes.byref(_pipeline_desc(p, keep)),
+        status = lib.einfold_pipeline_backward(_ctx(options), ctypes.byref(_pipeline_desc(p, keep)),
                                                rels, ctypes.byref(_relation(d_out, keep)),
                                                ctypes.byref(_options(options, keep)), results)
         msg = results[0].message.decode(errors="replace")

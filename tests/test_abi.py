@@ -157,3 +157,22 @@ def test_backend_may_run_takes_products_and_attention_only():
         assert lib.einfold_backend_may_run(ctypes.byref(shape)) == want
     assert lib.einfold_backend_may_run(ctypes.byref(_lib.DenseShape(0, 0, 1, -1, 4, 5, 0))) == 0
     assert lib.einfold_backend_may_run(None) == 0
+
+
+def test_last_call_is_per_thread():
+    import threading
+
+    from einfold_b200 import kernels as K
+
+    K.last_call.message = "main"
+    seen = []
+
+    def other():
+        seen.append(K.last_call.message)
+        K.last_call.message = "other"
+        seen.append(K.last_call.message)
+
+    t = threading.Thread(target=other)
+    t.start()
+    t.join()
+    assert seen == ["", "other"] and K.last_call.message == "main"
