@@ -862,7 +862,7 @@ def _smoother(cpu=False):
     out = {"groups": groups, "x_per_group": nx, "y_per_group": ny, "h": h, "pairs": pairs, "ms": ms,
            "gpairs_per_s": pairs / ms / 1e6, "rows_out": sum(b.rows for b in got.batches),
            "tiles_visited": got.tiles_visited, "max_rel_err_vs_torch_f64": err,
-           "kernel": "fused_tiles (FP64 scores and weights on the CUDA cores)"}
+           "kernel": "fused_unshifted (FP64 scores and weights on the CUDA cores, no per-tile reductions)"}
     for batch in got.batches:
         batch.release()
     if cpu:
