@@ -436,19 +436,14 @@ class _ThreadCalls(threading.local):
         self.info = CallInfo()
 
 
-class _LastCall:
-    """``CallInfo`` of the last call on the calling thread."""
-
-    _calls = _ThreadCalls()
-
-    def __getattr__(self, name):
-        return getattr(self._calls.info, name)
-
-    def __setattr__(self, name, value):
-        setattr(self._calls.info, name, value)
+_calls = _ThreadCalls()
 
 
-last_call = _LastCall()
+def __getattr__(name):
+    # ``last_call``: the calling thread's CallInfo.
+    if name == "last_call":
+        return _calls.info
+    raise AttributeError(f"module {__name__!r} has no attribute {name!r}")
 
 
 def _collect(res: _lib.Result) -> List[pa.RecordBatch]:
@@ -476,13 +471,13 @@ def _call(fn, *args) -> Optional[_lib.Result]:
     res = _lib.Result()
     status = fn(args[-1], *args[:-1], ctypes.byref(res))
     msg = res.message.decode(errors="replace")
-    last_call.kernels_launched = res.kernels_launched
-    last_call.device_ms = res.device_ms
-    last_call.product_ms = res.product_ms
-    last_call.product_ops = res.product_ops
-    last_call.schedule = res.schedule
-    last_call.graph = res.graph
-    last_call.message = msg
+    _calls.info.kernels_launched = res.kernels_launched
+    _calls.info.device_ms = res.device_ms
+    _calls.info.product_ms = res.product_ms
+    _calls.info.product_ops = res.product_ops
+    _calls.info.schedule = res.schedule
+    _calls.info.graph = res.graph
+    _calls.info.message = msg
     if status == _lib.DECLINED:
         return None
     if status != _lib.OK:
@@ -588,11 +583,11 @@ def pipeline_backward(p: ir.Pipeline, operands: Sequence, d_out: Relation,
                                                rels, ctypes.byref(_relation(d_out, keep)),
                                                ctypes.byref(_options(options, keep)), results)
         msg = results[0].message.decode(errors="replace")
-        last_call.kernels_launched = results[0].kernels_launched
-        last_call.device_ms = results[0].device_ms
-        last_call.product_ms = results[0].product_ms
-        last_call.product_ops = results[0].product_ops
-        last_call.message = msg
+        _calls.info.kernels_launched = results[0].kernels_launched
+        _calls.info.device_ms = results[0].device_ms
+        _calls.info.product_ms = results[0].product_ms
+        _calls.info.product_ops = results[0].product_ops
+        _calls.info.message = msg
         if status == _lib.DECLINED:
             return None
         if status != _lib.OK:
