@@ -162,6 +162,10 @@ SIGNATURES = {
     "einfold_check_wait": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
     "einfold_exp_weights": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                              ctypes.c_int32, ctypes.c_void_p]),
+    "einfold_evaluate_pairs": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(Expression), ctypes.c_void_p,
+                                                ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                                                ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                                ctypes.c_void_p]),
     "einfold_backend_may_run": (ctypes.c_int32, [ctypes.POINTER(DenseShape)]),
     "einfold_backend_run": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(DenseWork), ctypes.c_void_p,
                                              ctypes.POINTER(Result)]),

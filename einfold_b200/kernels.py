@@ -607,6 +607,37 @@ class Ranks:
     first: np.ndarray  # uint32 per distinct key
 
 
+def evaluate_pairs(e: ir.Expression, a, a_valid, b, b_valid, options: Optional[Options] = None):
+    """``Expression::evaluate`` (expression.rs) on the device, as the tile
+    kernels evaluate row expressions (``einfold_evaluate_pairs``), for every
+    pair of a row of ``a`` and a row of ``b``: CUDA float64 tensors of
+    ``cols`` values a row, with uint8 validity tensors of the same shape
+    (1: valid). Returns the values and their validity, ``[len(a)][len(b)]``
+    (0 and 0 where a column the expression reads is NULL)."""
+    import torch
+
+    options = options or Options()
+    if a.dim() != 2 or b.dim() != 2 or a.shape[1] != b.shape[1]:
+        raise ValueError("a and b must be [rows][cols] with the same cols")
+    a, b = a.contiguous(), b.contiguous()
+    a_valid, b_valid = a_valid.contiguous().to(torch.uint8), b_valid.contiguous().to(torch.uint8)
+    na, nb, cols = a.shape[0], b.shape[0], a.shape[1]
+    out = torch.empty((na, nb), dtype=torch.float64, device=a.device)
+    valid = torch.empty((na, nb), dtype=torch.uint8, device=a.device)
+    keep = _Keep()
+    try:
+        expr = _expression(e, keep)
+        torch.cuda.current_stream(a.device).synchronize()
+        st = _lib.load().einfold_evaluate_pairs(_ctx(options), ctypes.byref(expr), a.data_ptr(), a_valid.data_ptr(),
+                                                na, b.data_ptr(), b_valid.data_ptr(), nb, cols, out.data_ptr(),
+                                                valid.data_ptr(), None)
+    finally:
+        keep.release()
+    if st != _lib.OK:
+        _raise(st, _lib.load().einfold_last_error().decode())
+    return out, valid
+
+
 def rank_columns(relation: Relation, columns: Sequence[int], float_keys: FloatKeys = FloatKeys.BITWISE,
                  device: int = 0) -> Ranks:
     """``rank_columns`` (discriminate.rs:240-277) on the device: the ranks of

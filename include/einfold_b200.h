@@ -465,6 +465,19 @@ int32_t einfold_check_wait(einfold_context* ctx, uint64_t limit_ns, uint64_t* wa
 int32_t einfold_exp_weights(einfold_context* ctx, const double* x, double* y, int64_t n, int32_t shift,
                             void* stream);
 
+/* A row expression's value as the pipelines' tile kernels evaluate it
+ * (Expression::evaluate, crates/einfold-ir/src/expression.rs), for every
+ * pair of a row i of `a` and a row j of `b`: out[i·nb + j], with
+ * out_valid[i·nb + j] = 0 (and out 0) where a column the expression reads is
+ * NULL. a and b hold `cols` DOUBLE values a row, row-major, with a validity
+ * byte each (1: valid); a column node (operand o, column c) reads value c of
+ * a's row (o = 0) or b's (o = 1). Device arrays; returns once done. Replaces
+ * the host evaluation the reference's row expressions get
+ * (tests/expression_vs_sql.rs checks it against SQL). */
+int32_t einfold_evaluate_pairs(einfold_context* ctx, const einfold_expression* expression, const double* a,
+                               const uint8_t* a_valid, int64_t na, const double* b, const uint8_t* b_valid,
+                               int64_t nb, int32_t cols, double* out, uint8_t* out_valid, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
