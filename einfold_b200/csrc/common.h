@@ -224,7 +224,7 @@ inline void Context::phase(const char* name) {
   if (!tracing) return;
   cudaStreamSynchronize(stream);
   double t = now_ms();
-  std::fprintf(stderr, "[einfold] %-28s %9.3f ms\n", name, last_phase ? t - last_phase : 0.0);
+  std::fprintf(stderr, "[einfold %p] %-28s %9.3f ms\n", (void*)stream, name, last_phase ? t - last_phase : 0.0);
   last_phase = t;
 }
 
