@@ -36,6 +36,28 @@ def test_schema_follows_the_key_types():
     assert [f.name for f in s] == ["0", "1", "2"]
 
 
+@pytest.mark.parametrize("i_type,k_type", [
+    (pa.decimal32(9, 2), pa.decimal64(18, 3)),
+    (pa.decimal128(38, 4), pa.decimal256(76, 5)),
+    (pa.binary(12), pa.binary(1)),
+    (pa.date32(), pa.timestamp("us", tz="UTC")),
+    (pa.time64("ns"), pa.duration("ms")),
+    (pa.dictionary(pa.int8(), pa.decimal256(76, 5)), pa.dictionary(pa.int32(), pa.binary(4))),
+])
+def test_schema_keeps_every_key_type(i_type, k_type):
+    sa = pa.schema([("i", i_type), ("j", pa.int64()), ("v", pa.float64())])
+    sb = pa.schema([("j", pa.int64()), ("k", k_type), ("v", pa.float64())])
+    s = K.schema(_matmul(), [sa, sb])
+    assert [f.type for f in s] == [i_type, k_type, pa.float64()]
+
+
+def test_schema_rejects_decimals_of_another_scale_on_one_dimension():
+    sa = pa.schema([("i", pa.int64()), ("j", pa.decimal128(10, 2)), ("v", pa.float64())])
+    sb = pa.schema([("j", pa.decimal128(10, 3)), ("k", pa.int64()), ("v", pa.float64())])
+    with pytest.raises(K.ArrowInvalidArgumentError):
+        K.schema(_matmul(), [sa, sb])
+
+
 def test_schema_rejects_mismatched_keys_and_non_float_values():
     sa = pa.schema([("i", pa.int64()), ("j", pa.int64()), ("v", pa.float64())])
     sb = pa.schema([("j", pa.int32()), ("k", pa.int64()), ("v", pa.float64())])
