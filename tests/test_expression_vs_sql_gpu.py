@@ -20,50 +20,12 @@ import numpy as np
 import pytest
 
 from einfold_b200 import ir, kernels as K
-from oracle import oracle
+from tests import expression_cases as X
 
 pytestmark = pytest.mark.gpu
 
-SEED, CASES = 0xE4E5, 300
 U = 2.0 ** -53
 TINY = 5e-324  # the least subnormal
-SPECIAL = [math.nan, math.inf, -math.inf, 0.0, -0.0, 1.0, -1.0, 800.0, -800.0, 1e-300, 1e300]
-
-
-def _value(rng):
-    r = rng.below(10)
-    if r == 0:
-        return None
-    if r in (1, 2):
-        return SPECIAL[rng.below(len(SPECIAL))]
-    return (rng.unit() - 0.5) * 20.0
-
-
-def _expression(rng, depth):
-    leaf = depth == 0 or rng.below(4) == 0
-    if leaf:
-        n = rng.below(5)
-        if n == 0:
-            return ir.Expression.literal([0.0, 1.0, 2.0, -0.5, 0.25, 3.5][rng.below(6)])
-        operand = [0, 1][n % 2]
-        column = [1, 2][n // 3]
-        return ir.Expression.column(operand, column)
-    n = rng.below(9)
-    if n <= 3:
-        op = [ir.Binary.ADD, ir.Binary.SUBTRACT, ir.Binary.MULTIPLY, ir.Binary.DIVIDE][rng.below(4)]
-        a = _expression(rng, depth - 1)
-        b = _expression(rng, depth - 1)
-        return a.binary(op, b)
-    if n == 4:
-        a = _expression(rng, depth - 1)
-        p = [1.0, 2.0, 3.0, 0.5, 1.5][rng.below(5)]
-        return a.binary(ir.Binary.POWER, ir.Expression.literal(p))
-    op = [ir.Unary.NEGATE, ir.Unary.ABS, ir.Unary.EXP, ir.Unary.LN][n - 5]
-    return _expression(rng, depth - 1).unary(op)
-
-
-def _table(rows, rng):
-    return [[_value(rng), _value(rng)] for _ in range(rows)]
 
 
 def _bound(e, column):
@@ -168,12 +130,7 @@ def _check(e, rows_a, rows_b, where):
 
 def test_row_expressions_compute_what_evaluate_does():
     exact = bounded = pairs = 0
-    for i in range(CASES):
-        seed = (SEED + i) & ((1 << 64) - 1)
-        rng = oracle.Rng.seeded(seed, 0)
-        rows_a = _table(rng.below(9), rng)
-        rows_b = _table(rng.below(9), rng)
-        e = _expression(rng, 5)
+    for seed, rows_a, rows_b, e in X.cases():
         pairs += len(rows_a) * len(rows_b)
         if not rows_a or not rows_b:
             continue  # either table may be empty, and so the cross join

@@ -3,8 +3,10 @@ SplitMix64 outputs of crates/einfold-testkit/src/rng.rs:66-78, the tile
 counts of crates/einfold-kernels/tests/pipeline_vs_sql.rs:731-760, the
 Bounds cases of crates/einfold-kernels/src/fused.rs:1116-1177, the signed
 zero keys of keys.rs:83-93, the long shared prefixes of
-discriminate.rs:663-683, and the rounding bound and repeatability of the
-dense product (kernels_vs_sql.rs:21-23, gemm.rs:52-89)."""
+discriminate.rs:663-683, the rounding bound and repeatability of the dense
+product (kernels_vs_sql.rs:21-23, gemm.rs:52-89), the row-format order of
+decimal keys, and the row-expression restatement held to SQL on the
+reference's expression cases (expression_vs_sql.rs)."""
 import math
 
 import numpy as np
@@ -189,3 +191,107 @@ def test_gaussian_smoother_against_numpy():
         start, end = x0 // n * ny, (x1 - 1) // n * ny + ny
         tiles += -(-end // 64) - start // 64
     assert (got.tiles_visited, got.tiles) == (tiles, tiles)
+
+
+def _sql(e, a, b):
+    """SELECT <e> FROM a CROSS JOIN b, column by column, as SQL computes it:
+    NULL wherever an operand is NULL, IEEE arithmetic on DOUBLE (division by
+    zero gives ±inf or NaN), exp and ln with SQL's special values (exp's
+    overflow +inf, ln of a negative NaN, of zero -inf), power as libm's pow.
+    a and b: (values,
+    nulls) arrays of [rows][2] for the columns x and y."""
+    (av, an), (bv, bn) = a, b
+    na, nb = av.shape[0], bv.shape[0]
+    if e.kind == "column":
+        src_v, src_n = (av, an) if e.operand == 0 else (bv, bn)
+        v, n = src_v[:, e.col - 1], src_n[:, e.col - 1]
+        shape = (na, 1) if e.operand == 0 else (1, nb)
+        return np.broadcast_to(v.reshape(shape), (na, nb)), np.broadcast_to(n.reshape(shape), (na, nb))
+    if e.kind == "literal":
+        return np.full((na, nb), e.value), np.zeros((na, nb), dtype=bool)
+    if e.kind == "unary":
+        x, xn = _sql(e.args[0], a, b)
+        with np.errstate(all="ignore"):
+            if e.op is ir.Unary.NEGATE:
+                v = -x
+            elif e.op is ir.Unary.ABS:
+                v = np.abs(x)
+            elif e.op is ir.Unary.EXP:
+                def exp(t):
+                    try:
+                        return math.exp(t)
+                    except OverflowError:
+                        return math.inf
+                v = np.vectorize(exp, otypes=[float])(x) if x.size else x
+            else:
+                def ln(t):
+                    if math.isnan(t) or t < 0:
+                        return math.nan
+                    if t == 0:
+                        return -math.inf
+                    return math.inf if math.isinf(t) else math.log(t)
+                v = np.vectorize(ln, otypes=[float])(x) if x.size else x
+        return v, xn
+    x, xn = _sql(e.args[0], a, b)
+    y, yn = _sql(e.args[1], a, b)
+    with np.errstate(all="ignore"):
+        op = e.op
+        if op is ir.Binary.ADD:
+            v = x + y
+        elif op is ir.Binary.SUBTRACT:
+            v = x - y
+        elif op is ir.Binary.MULTIPLY:
+            v = x * y
+        elif op is ir.Binary.DIVIDE:
+            v = np.divide(x, y)
+        else:
+            # libm's pow, as DataFusion's power (numpy's vectorised pow may
+            # round otherwise): a domain error is NaN, an overflow ±inf.
+            def power(p, q):
+                try:
+                    return math.pow(p, q)
+                except ValueError:
+                    return math.nan
+                except OverflowError:
+                    odd = q == math.floor(q) and math.fmod(q, 2.0) != 0.0
+                    return -math.inf if p < 0 and odd else math.inf
+            v = np.vectorize(power, otypes=[float])(x, y) if x.size else x
+    return v, xn | yn
+
+
+def test_evaluate_is_sqls_on_the_reference_expression_cases():
+    # The reference holds Expression::evaluate to DataFusion's SQL bit for
+    # bit on these cases (expression_vs_sql.rs); ir.Expression.evaluate,
+    # which the device interpreter is held to, is held here to the SQL
+    # evaluated column by column above.
+    from tests import expression_cases as X
+
+    def table(rows):
+        v = np.zeros((len(rows), 2))
+        n = np.zeros((len(rows), 2), dtype=bool)
+        for i, r in enumerate(rows):
+            for c in range(2):
+                if r[c] is None:
+                    n[i, c] = True
+                else:
+                    v[i, c] = r[c]
+        return v, n
+
+    pairs = 0
+    for seed, rows_a, rows_b, e in X.cases():
+        if not rows_a or not rows_b:
+            continue
+        got_v, got_n = _sql(e, table(rows_a), table(rows_b))
+        for i, ra in enumerate(rows_a):
+            for j, rb in enumerate(rows_b):
+                rows = [ra, rb]
+                want = e.evaluate(lambda o, c: rows[o][c - 1])
+                pairs += 1
+                assert bool(got_n[i, j]) == (want is None), (seed, i, j)
+                if want is None:
+                    continue
+                g = float(got_v[i, j])
+                same = (math.isnan(g) and math.isnan(want)) or \
+                    np.float64(g).view(np.uint64) == np.float64(want).view(np.uint64)
+                assert same, (seed, i, j, g, want, repr(e))
+    assert pairs > 3000
