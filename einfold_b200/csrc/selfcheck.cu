@@ -80,6 +80,7 @@ extern "C" int32_t einfold_evaluate_pairs(einfold_context* ctx, const einfold_ex
     if (!expression || expression->n_nodes < 1 || expression->n_nodes > 4096 || !expression->nodes)
       fail(EINFOLD_INVALID, "no expression, or one of more than 4096 nodes");
     if (na < 0 || nb < 0 || cols < 1 || cols > 32) fail(EINFOLD_INVALID, "na or nb < 0, or cols outside 1..32");
+    if (na > 0 && nb > INT64_MAX / na) fail(EINFOLD_INVALID, "na·nb overflows");
     // The postfix nodes, checked as a pipeline's are: every operation finds
     // its operands, one value is left, the stack never deeper than 60.
     std::vector<ExprNode> nodes;
