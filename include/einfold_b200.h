@@ -328,9 +328,9 @@ int32_t einfold_fp64_gemm(einfold_context* ctx, const double* a, const double* b
  * (NULL: the legacy default stream) and returns once the product is done.
  * It calls no cudaMalloc or cudaFree. Its first call on a device (in each
  * CUDA context the device gets, e.g. again after cudaDeviceReset) looks up
- * the array's address, so make that call before any stream capture. Every
- * call shares the array: calls that overlap on the GPU, from two threads or
- * two streams, race and give wrong results; serialize them. */
+ * the array's address. Every call shares the array: calls that overlap on
+ * the GPU, from two threads or two streams, race and give wrong results;
+ * serialize them. */
 int32_t einfold_split_gemm_static(const double* a, const double* b, double* c, int64_t batches, int64_t m,
                                   int64_t n, int64_t k, int32_t b_transposed, int32_t slices, void* stream,
                                   char* message, int32_t message_len);
