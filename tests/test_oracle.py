@@ -1,13 +1,17 @@
-"""The oracle pinned to the reference's own known answers, on the CPU: the
+"""The oracle pinned to the reference's own known answers, on the CPU. The
 SplitMix64 outputs of crates/einfold-testkit/src/rng.rs:66-78, the tile
 counts of crates/einfold-kernels/tests/pipeline_vs_sql.rs:731-760, the
-Bounds cases of crates/einfold-kernels/src/fused.rs:1116-1177, the signed
-zero keys of keys.rs:83-93, the long shared prefixes of
-discriminate.rs:663-683, the rounding bound and repeatability of the dense
-product (kernels_vs_sql.rs:21-23, gemm.rs:52-89), the row-format order of
-decimal keys, and the row-expression restatement held to SQL on the
+Bounds cases of crates/einfold-kernels/src/fused.rs:1116-1177, the long
+shared prefix of discriminate.rs:663-683 and the property tests' seeds and
+case counts are read from tests/golden/reference_facts.json, which
+tests/golden/make_golden.py extracts from the reference's sources. Also: the
+signed zero keys of keys.rs:83-93, the rounding bound and repeatability of
+the dense product (kernels_vs_sql.rs:21-23, gemm.rs:52-89), the row-format
+order of decimal keys, and the row-expression restatement held to SQL on the
 reference's expression cases (expression_vs_sql.rs)."""
+import json
 import math
+import os
 
 import numpy as np
 import pyarrow as pa
@@ -20,15 +24,23 @@ from tests.tables import complete, matmul_fold, rows_of
 
 GE, GT, LE, LT = (ir.Comparison.GREATER_OR_EQUAL, ir.Comparison.GREATER, ir.Comparison.LESS_OR_EQUAL,
                   ir.Comparison.LESS)
+COMPARISONS = {"ge": GE, "gt": GT, "le": LE, "lt": LT}
+
+with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_facts.json")) as _f:
+    FACTS = json.load(_f)
+
+
+def _f64(x):
+    return float(x) if isinstance(x, str) else x
 
 
 def test_splitmix64_seed_zero_gives_the_reference_outputs():
+    want = FACTS["splitmix64_seed0"]["outputs"]
+    assert len(want) == 4
     rng = oracle.Rng.seeded(0, 0)
-    assert [rng.next_u64() for _ in range(4)] == [0xE220A8397B1DCDAF, 0x6E789E6AA1B965F4, 0x06C45D188009454F,
-                                                  0xF88BB8A8724C81EC]
+    assert [rng.next_u64() for _ in range(4)] == want
     # The vectorised stream is the same stream.
-    assert list(oracle.Rng.seeded(0, 0).u64s(4)) == [0xE220A8397B1DCDAF, 0x6E789E6AA1B965F4, 0x06C45D188009454F,
-                                                     0xF88BB8A8724C81EC]
+    assert list(oracle.Rng.seeded(0, 0).u64s(4)) == want
     a, b = oracle.Rng.seeded(5, 1), oracle.Rng.seeded(5, 2)
     assert a.next_u64() != b.next_u64()
 
@@ -41,16 +53,13 @@ def _tiles(l, nb=None, conditions=()):
     return r.tiles_visited, r.tiles
 
 
-def test_causal_masks_skip_half_the_tiles():
-    assert _tiles(64 * 16, conditions=[(GE, 0)]) == (16 * 17 // 2, 256)
+@pytest.mark.parametrize("case", FACTS["tile_counts"], ids=lambda c: c["test"])
+def test_masked_pipelines_visit_the_reference_tile_counts(case):
+    conditions = [(COMPARISONS[c], o) for c, o in case["conditions"]]
+    assert _tiles(case["length"], nb=case["batches"], conditions=conditions) == (case["visited"], case["tiles"])
 
 
-def test_sliding_windows_visit_a_band_of_tiles():
-    assert _tiles(64 * 16, conditions=[(GE, 0), (LT, 64)]) == (16 + 15, 256)
-
-
-def test_batches_visit_only_their_own_tiles():
-    assert _tiles(64 * 4, nb=8, conditions=[(GE, 0)]) == (8 * 10, 8 * 16)
+def test_batches_not_a_multiple_of_the_tile_visit_at_most_their_tiles():
     visited, tiles = _tiles(100, nb=8, conditions=[(GE, 0)])
     assert tiles <= 13 * 4 and visited <= tiles
 
@@ -68,22 +77,14 @@ def _hold(b, z, results, special):
                               special)
 
 
-def test_bounds_cases():
-    assert _hold(_normal(1.0, 0.25, 2.0, 0.5), 1.5, [0.0, 1.0], [False, False])
-    assert _hold(_normal(1.0, 0.25, 2.0, 0.5), None, [0.0], [False])
-    assert _hold(_normal(1.0, 0.25, 0.0, math.inf), 1.5, [0.0], [False])
-    assert not _hold(_normal(1.0, 1.0, 1.0, 1e-300), 1e10, [0.0], [False])
-    assert not _hold(_normal(1.0, 1e-300, 1.0, 1e-10), None, [0.0], [False])
-    assert _hold(_bounds(1.0, 1e5), 1.5, [0.3, -2.0], [False, False])
-    assert _hold(_bounds(1.0, 1e5), None, [0.3, -2.0], [False, False])
-    assert _hold(_bounds(1.1e188, 1.0), 1.1e188, [0.4], [False])
-    assert not _hold(_bounds(1e-323, 0.125), 2e-323, [0.0], [False])
-    assert not _hold(_bounds(2.0, 1e300), 2.0, [2.5e-24], [False])
-    assert not _hold(_bounds(1.0, 1e100), 1e-309, [1e100], [False])
-    assert _hold(_bounds(1.0, 1e100), None, [1e100], [False])
-    assert not _hold(_bounds(1.0, 1e308), None, [1e308], [False])
-    assert _hold(_bounds(1.0, 1.0), 1.0, [0.0, math.inf], [True, True])
-    assert not _hold(_bounds(1.0, 1.0), 1.0, [0.0], [False])
+@pytest.mark.parametrize("case", FACTS["bounds_cases"], ids=lambda c: c["source"].rsplit(":", 1)[1])
+def test_bounds_cases(case):
+    assert len(FACTS["bounds_cases"]) == 15
+    z = _f64(case["z"]) if case["z"] is not None else None
+    got = oracle.bounds_hold(_f64(case["heaviest"]), _f64(case["lightest"]), _f64(case["largest"]),
+                             _f64(case["smallest"]), case["terms"], z, [_f64(r) for r in case["results"]],
+                             case["special"])
+    assert got == case["holds"]
 
 
 def test_signed_zeros_are_one_key_only_when_the_host_says_so():
@@ -98,10 +99,12 @@ def test_signed_zeros_are_one_key_only_when_the_host_says_so():
 
 
 def test_keys_with_long_shared_prefixes_sort_as_their_bytes():
-    prefix = "p" * 100_000
-    strings = [f"{prefix}{i:03}" for i in reversed(range(200))]
+    lp = FACTS["long_prefix"]
+    prefix = lp["char"] * lp["prefix_bytes"]
+    n = lp["keys"]
+    strings = [f"{prefix}{i:0{lp['digits']}}" for i in reversed(range(n))]
     r = oracle.ranks_of_bytes(oracle._encode_column(pa.array(strings)))
-    order = sorted(range(200), key=lambda i: strings[i])
+    order = sorted(range(n), key=lambda i: strings[i])
     assert [strings[r.first[k]] for k in range(len(r.first))] == [strings[i] for i in order]
     assert np.array_equal(r.rank, np.argsort(np.argsort(strings, kind="stable"), kind="stable").astype(np.uint32))
 
@@ -295,3 +298,14 @@ def test_evaluate_is_sqls_on_the_reference_expression_cases():
                     np.float64(g).view(np.uint64) == np.float64(want).view(np.uint64)
                 assert same, (seed, i, j, g, want, repr(e))
     assert pairs > 3000
+
+
+def test_the_restated_property_tests_draw_the_reference_cases():
+    # Each restated property test starts from the reference's seed and runs
+    # its number of cases.
+    from tests import expression_cases, test_dense_metamorphic_gpu, test_kernels_vs_sql_gpu, test_pipeline_vs_sql_gpu
+
+    ours = {"kernels_vs_sql": test_kernels_vs_sql_gpu, "pipeline_vs_sql": test_pipeline_vs_sql_gpu,
+            "expression_vs_sql": expression_cases, "dense_metamorphic": test_dense_metamorphic_gpu}
+    for name, facts in FACTS["property_tests"].items():
+        assert (ours[name].SEED, ours[name].CASES) == (facts["seed"], facts["cases"]), name
