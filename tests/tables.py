@@ -2,6 +2,8 @@
 from __future__ import annotations
 
 import itertools
+import json
+import os
 from typing import Callable, List, Optional, Sequence, Tuple
 
 import numpy as np
@@ -101,3 +103,10 @@ def assert_same_rows(got: pa.Table, want: pa.Table, tol: Optional[np.ndarray] = 
         t = np.broadcast_to(tol, w.shape)[fin]
         bad = err > t
         assert not bad.any(), f"{bad.sum()} values outside tolerance; worst {np.max(err - t)}"
+
+
+def reference_facts() -> dict:
+    """The reference's known answers, extracted from its sources by
+    tests/golden/make_golden.py into tests/golden/reference_facts.json."""
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_facts.json")) as f:
+        return json.load(f)

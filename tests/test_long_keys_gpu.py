@@ -9,7 +9,7 @@ import pytest
 
 from einfold_b200 import ir, kernels as K
 from oracle import oracle
-from tests.tables import assert_same_rows, rows_of
+from tests.tables import assert_same_rows, reference_facts, rows_of
 
 pytestmark = pytest.mark.gpu
 
@@ -29,12 +29,14 @@ def _rank_both(columns, float_keys=0):
 def test_keys_with_a_100000_byte_shared_prefix():
     # discriminate.rs:663-683: 200 keys sharing a 100,000-byte prefix, in
     # reverse order, sort as their bytes.
-    prefix = "p" * 100_000
-    strings = [f"{prefix}{i:03}" for i in reversed(range(200))]
+    lp = reference_facts()["long_prefix"]
+    n = lp["keys"]
+    prefix = lp["char"] * lp["prefix_bytes"]
+    strings = [f"{prefix}{i:0{lp['digits']}}" for i in reversed(range(n))]
     got = _rank_both([pa.array(strings)])
-    assert len(got.first) == 200
-    assert [strings[got.first[r]] for r in range(200)] == sorted(strings)
-    assert np.array_equal(got.rank, np.arange(199, -1, -1, dtype=np.uint32))
+    assert len(got.first) == n
+    assert [strings[got.first[r]] for r in range(n)] == sorted(strings)
+    assert np.array_equal(got.rank, np.arange(n - 1, -1, -1, dtype=np.uint32))
 
 
 def test_long_strings_with_prefixes_zeros_and_nulls():

@@ -9,9 +9,7 @@ signed zero keys of keys.rs:83-93, the rounding bound and repeatability of
 the dense product (kernels_vs_sql.rs:21-23, gemm.rs:52-89), the row-format
 order of decimal keys, and the row-expression restatement held to SQL on the
 reference's expression cases (expression_vs_sql.rs)."""
-import json
 import math
-import os
 
 import numpy as np
 import pyarrow as pa
@@ -20,14 +18,13 @@ import pytest
 from einfold_b200 import ir
 from oracle import oracle
 from tests import pipelines as P
-from tests.tables import complete, matmul_fold, rows_of
+from tests.tables import complete, matmul_fold, reference_facts, rows_of
 
 GE, GT, LE, LT = (ir.Comparison.GREATER_OR_EQUAL, ir.Comparison.GREATER, ir.Comparison.LESS_OR_EQUAL,
                   ir.Comparison.LESS)
 COMPARISONS = {"ge": GE, "gt": GT, "le": LE, "lt": LT}
 
-with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_facts.json")) as _f:
-    FACTS = json.load(_f)
+FACTS = reference_facts()
 
 
 def _f64(x):

@@ -10,7 +10,7 @@ import pytest
 from einfold_b200 import ir, kernels as K
 from oracle import oracle
 from tests import pipelines as P
-from tests.tables import rows_of
+from tests.tables import reference_facts, rows_of
 
 pytestmark = pytest.mark.gpu
 
@@ -66,15 +66,15 @@ def _magnitudes(case: P.Case) -> np.ndarray:
     return np.abs(t.column(t.num_columns - 1).to_numpy(zero_copy_only=False))
 
 
-@pytest.mark.parametrize("conditions,want", [([(GE, 0)], (136, 256)), ([(GE, 0), (LT, 64)], (31, 256))])
-def test_masks_visit_the_reference_tile_counts(conditions, want):
-    got = _same(P.attention(64 * 16, conditions=conditions))
-    assert (got.tiles_visited, got.tiles) == want
+@pytest.mark.parametrize("case", reference_facts()["tile_counts"], ids=lambda c: c["test"])
+def test_masks_and_batches_visit_the_reference_tile_counts(case):
+    comparisons = {"ge": GE, "gt": GT, "le": LE, "lt": LT}
+    conditions = [(comparisons[c], o) for c, o in case["conditions"]]
+    got = _same(P.attention(case["length"], nb=case["batches"], conditions=conditions))
+    assert (got.tiles_visited, got.tiles) == (case["visited"], case["tiles"])
 
 
-def test_batches_visit_only_their_own_tiles():
-    got = _same(P.attention(64 * 4, nb=8, conditions=[(GE, 0)]))
-    assert (got.tiles_visited, got.tiles) == (80, 128)
+def test_batches_not_a_multiple_of_the_tile():
     _same(P.attention(100, nb=8, conditions=[(GE, 0)]))
 
 
